@@ -1,0 +1,130 @@
+/* stark_gpu.h — C ABI of the B200 (sm_100a) STARK prover path of stark-stir-swarm.
+ *
+ * Drop-in boundary for the reference prover core (paths relative to
+ * stark-stir-swarm/crates/): trace LDE -> DEEP-ALI merge -> STIR prove, plus
+ * the SHA3-256 Merkle channel and the STIR verifier. A Rust caller binds these
+ * with `extern "C"` and converts its 16-byte Montgomery `Goldilocks` values to
+ * canonical u64 (into_bigint().0[0]) at the boundary.
+ *
+ * Conventions
+ *  - Field elements are canonical little-endian u64 in [0, p), p = 2^64 - 2^32 + 1.
+ *  - Column-major matrices: column c occupies [c*n, (c+1)*n).
+ *  - Element buffers may live in host memory or in device memory of the
+ *    context's GPU; the library detects which (cudaPointerGetAttributes).
+ *    Host buffers are staged through the device inside the call.
+ *  - Every call is ordered on the context's stream and returns when its
+ *    results are available to the caller (host results are written back).
+ *  - Return 0 on success, a negative SG_E* code on error; nothing aborts.
+ *    sg_last_error() gives a human-readable reason for the last failure.
+ *  - A context is not thread-safe; use one context per host thread/stream.
+ */
+#ifndef STARK_GPU_H
+#define STARK_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_OK 0
+#define SG_EINVAL -1    /* bad argument (shape, power-of-two, schedule ...) */
+#define SG_ECUDA -2     /* CUDA runtime error */
+#define SG_ENOMEM -3    /* device allocation failed */
+#define SG_ESPACE -4    /* output buffer too small; *len holds the needed size */
+#define SG_EVERIFY -5   /* self-verification of a produced proof failed */
+
+#define SG_MAX_SCHEDULE 64
+
+/* Mirrors DeepFriParams (deep_ali/src/fri.rs:1303-1314). */
+typedef struct {
+  uint64_t schedule[SG_MAX_SCHEDULE];
+  uint64_t schedule_len;
+  uint64_t r;                 /* classic-FRI query count (unused by STIR) */
+  uint64_t s0;                /* STIR proximity queries */
+  uint64_t seed_z;
+  uint64_t d_final;
+  int32_t coeff_commit_final; /* bool */
+  int32_t stir;               /* bool; this library proves the STIR branch */
+  int32_t has_pi;             /* bool: public_inputs_hash is Some */
+  uint8_t pi_hash[32];
+} sg_fri_params;
+
+/* Phi gating of the reference merges (deep_ali/src/lib.rs:20-33, 372-397). */
+#define SG_PHI_PARALLEL_GATE 0 /* feature "parallel", >1 rayon thread: Phi = 0 unless n >= 4096 */
+#define SG_PHI_ALWAYS 1        /* built without "parallel": Phi always computed */
+#define SG_PHI_NEVER 2         /* feature "parallel" with one rayon thread: Phi = 0 */
+
+/* AIR ids follow deep_ali::air_workloads::AirType's declaration order. */
+#define SG_AIR_HASH_ROLLUP 4
+
+typedef struct sg_ctx sg_ctx;
+typedef struct sg_tree sg_tree;
+
+/* Context: one CUDA device + stream + twiddle tables + a stream-ordered pool. */
+int sg_ctx_create(int device, sg_ctx** out);
+void sg_ctx_destroy(sg_ctx* ctx);
+/* Use an existing cudaStream_t (passed as void*) for all later calls; NULL = the context's own stream. */
+int sg_ctx_set_stream(sg_ctx* ctx, void* cuda_stream);
+const char* sg_last_error(const sg_ctx* ctx);
+/* Number of kernels this context has launched since creation (instrumentation). */
+uint64_t sg_kernel_launches(const sg_ctx* ctx);
+
+/* Batched NTT with ark-poly Radix2EvaluationDomain semantics: forward = evaluations
+ * at w^0..w^{n-1} (natural order), inverse includes 1/n; w = 7^((p-1)/2^32)
+ * squared (32 - log_n) times. n_cols columns of 2^log_n, log_n <= 24.
+ * Replaces the domain.fft / domain.ifft calls of trace_import.rs:276-279 and
+ * lib.rs:402-410. in == out allowed. */
+int sg_ntt(sg_ctx* ctx, const uint64_t* in, uint64_t* out, size_t n_cols, size_t log_n, int inverse);
+
+/* Replaces lde_trace_columns (deep_ali/src/trace_import.rs:251-281): each of the
+ * w columns (n_trace rows, column-major) -> iFFT, zero-pad to n_trace*blowup,
+ * FFT. shift = 1 reproduces the reference (plain subgroup); another shift
+ * evaluates on the coset shift*<w>. out: w x (n_trace*blowup). */
+int sg_lde(sg_ctx* ctx, const uint64_t* trace, size_t w, size_t n_trace, size_t blowup, uint64_t shift,
+           uint64_t* out);
+
+/* Replaces deep_ali_merge_general (deep_ali/src/lib.rs:343-437) for the AIRs
+ * listed above: Phi_i = sum_j lambda_j C_j(row i, row (i+blowup) mod n),
+ * c = FFT_n(iFFT_n(Phi) / (X^n_trace - 1)), remainder dropped as in release
+ * builds (lib.rs:190-228). lde: w x n (n = n_trace*blowup); c_eval: n values. */
+int sg_merge(sg_ctx* ctx, int air, const uint64_t* lde, size_t w, size_t n_trace, size_t blowup,
+             const uint64_t* lambdas, size_t k, int phi_mode, uint64_t* c_eval);
+
+/* Merkle commitment over the rows of a column-major matrix (leaf i = the
+ * `width` values of row i), with the reference channel's framing
+ * (merkle/src/lib.rs:95-238, 391-476): per-level arities, tree label, last-node
+ * padding. `keep` (optional) receives a device-resident tree for sg_merkle_open. */
+int sg_merkle_commit(sg_ctx* ctx, const uint64_t* cols, size_t n_leaves, size_t width, size_t col_stride,
+                     const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t root[32], sg_tree** keep);
+/* Serialized MerkleOpening (ark-serialize compressed: leaf[32], path Vec<Vec<[u8;32]>>,
+ * index u64) for leaf `index` (merkle/src/lib.rs:478-512). */
+int sg_merkle_open(sg_ctx* ctx, const sg_tree* tree, size_t index, uint8_t* out, size_t cap, size_t* len);
+void sg_merkle_free(sg_tree* tree);
+
+/* make_schedule + build_params (swarm-dns/src/prover.rs:53-98): schedule of 8s plus
+ * a remainder for STIR (2s for FRI), r = s0 = 54, seed_z = 0xDEEF_BAAD,
+ * coeff_commit_final, d_final = 1, public_inputs_hash = pi (NULL = None). */
+void sg_build_params(size_t n0, const uint8_t* pi32, int stir, sg_fri_params* out);
+
+/* Replaces deep_fri_prove::<SexticExt> (deep_ali/src/fri.rs:1900-2055), STIR
+ * branch: writes the exact ark-serialize (Compress::Yes) bytes of the
+ * DeepFriProof. f0: n0 values. */
+int sg_stir_prove(sg_ctx* ctx, const uint64_t* f0, size_t n0, const sg_fri_params* params, uint8_t* proof,
+                  size_t cap, size_t* len);
+
+/* Replaces deep_fri_verify::<SexticExt> (deep_ali/src/fri.rs:2136-2521), STIR
+ * branch, on serialized proof bytes. Returns 1 accept, 0 reject. Host only. */
+int sg_stir_verify(const uint8_t* proof, size_t len, const sg_fri_params* params);
+
+/* Core of prove_inner_shard / prove_outer_rollup (swarm-dns/src/prover.rs:148-304):
+ * HashRollup trace over `leaves` (n_trace = next_pow2(n_leaves) >= 8) -> LDE x32 ->
+ * merge (lambda = 1,2,3) -> STIR with build_params(n0, pi). The proof is
+ * self-verified before return (SG_EVERIFY on failure), like the reference worker. */
+int sg_prove_hash_rollup(sg_ctx* ctx, const uint64_t* leaves, size_t n_leaves, const uint8_t pi[32], int phi_mode,
+                         uint8_t* proof, size_t cap, size_t* len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STARK_GPU_H */

@@ -1,0 +1,363 @@
+"""B200 (sm_100a) drop-in for the stark-stir-swarm prover hot path.
+
+Host-side mirror of the reference's Rust entry points (paths relative to
+stark-stir-swarm/crates/), each a thin ctypes call into libstarkgpu.so whose
+C ABI is declared in include/stark_gpu.h:
+
+  lde_trace_columns      deep_ali/src/trace_import.rs:251-281
+  deep_ali_merge_general deep_ali/src/lib.rs:343-437
+  deep_fri_prove         deep_ali/src/fri.rs:1900-2055 (STIR branch, SexticExt)
+  deep_fri_verify        deep_ali/src/fri.rs:2136-2521 (STIR branch)
+  MerkleTreeChannel      merkle/src/lib.rs:356-512
+  make_schedule / build_params / prove_hash_rollup   swarm-dns/src/prover.rs:53-304
+
+Field elements are canonical uint64 (numpy uint64 arrays on the host, or CUDA
+tensors / raw device pointers that the library uses in place). Errors that the
+reference reports with panics or Err(String) raise exceptions here. The
+library must be built (`make -C stark-swarm_b200`); there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libstarkgpu.so")
+P = 0xFFFFFFFF00000001
+
+SG_OK, SG_EINVAL, SG_ECUDA, SG_ENOMEM, SG_ESPACE, SG_EVERIFY = 0, -1, -2, -3, -4, -5
+PHI_PARALLEL_GATE, PHI_ALWAYS, PHI_NEVER = 0, 1, 2
+AIR_HASH_ROLLUP = 4
+
+BLOWUP = 32
+NUM_QUERIES = 54
+SEED_Z = 0xDEEFBAAD
+
+
+class StarkGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class FriParams(ctypes.Structure):
+    """sg_fri_params == DeepFriParams (deep_ali/src/fri.rs:1303-1314)."""
+    _fields_ = [
+        ("schedule", ctypes.c_uint64 * 64),
+        ("schedule_len", ctypes.c_uint64),
+        ("r", ctypes.c_uint64),
+        ("s0", ctypes.c_uint64),
+        ("seed_z", ctypes.c_uint64),
+        ("d_final", ctypes.c_uint64),
+        ("coeff_commit_final", ctypes.c_int32),
+        ("stir", ctypes.c_int32),
+        ("has_pi", ctypes.c_int32),
+        ("pi_hash", ctypes.c_uint8 * 32),
+    ]
+
+    @classmethod
+    def new(cls, schedule, r=NUM_QUERIES, seed_z=SEED_Z, coeff_commit_final=True, d_final=1, stir=True, s0=None,
+            public_inputs_hash=None):
+        p = cls()
+        if len(schedule) > 64:
+            raise ValueError("schedule longer than 64 layers")
+        for i, m in enumerate(schedule):
+            p.schedule[i] = m
+        p.schedule_len = len(schedule)
+        p.r = r
+        p.s0 = r if s0 is None else s0
+        p.seed_z = seed_z
+        p.d_final = d_final
+        p.coeff_commit_final = int(bool(coeff_commit_final))
+        p.stir = int(bool(stir))
+        if public_inputs_hash is not None:
+            if len(public_inputs_hash) != 32:
+                raise ValueError("public_inputs_hash must be 32 bytes")
+            p.has_pi = 1
+            ctypes.memmove(p.pi_hash, bytes(public_inputs_hash), 32)
+        return p
+
+    @property
+    def schedule_list(self):
+        return [self.schedule[i] for i in range(self.schedule_len)]
+
+
+DeepFriParams = FriParams
+
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+_lib = None
+
+# Every symbol declared in include/stark_gpu.h.
+EXPORTS = (
+    "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_last_error", "sg_kernel_launches", "sg_ntt",
+    "sg_lde", "sg_merge", "sg_merkle_commit", "sg_merkle_open", "sg_merkle_free", "sg_build_params",
+    "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
+)
+
+
+def lib():
+    """Load libstarkgpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}`")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, sz, u64, i32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int
+    L.sg_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
+    L.sg_ctx_destroy.argtypes = [vp]
+    L.sg_ctx_destroy.restype = None
+    L.sg_ctx_set_stream.argtypes = [vp, vp]
+    L.sg_last_error.argtypes = [vp]
+    L.sg_last_error.restype = ctypes.c_char_p
+    L.sg_kernel_launches.argtypes = [vp]
+    L.sg_kernel_launches.restype = u64
+    L.sg_ntt.argtypes = [vp, vp, vp, sz, sz, i32]
+    L.sg_lde.argtypes = [vp, vp, sz, sz, sz, u64, vp]
+    L.sg_merge.argtypes = [vp, i32, vp, sz, sz, sz, vp, sz, i32, vp]
+    L.sg_merkle_commit.argtypes = [vp, vp, sz, sz, sz, vp, sz, u64, ctypes.c_char_p, ctypes.POINTER(vp)]
+    L.sg_merkle_open.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
+    L.sg_merkle_free.argtypes = [vp]
+    L.sg_merkle_free.restype = None
+    L.sg_build_params.argtypes = [sz, ctypes.c_char_p, i32, ctypes.POINTER(FriParams)]
+    L.sg_build_params.restype = None
+    L.sg_stir_prove.argtypes = [vp, vp, sz, ctypes.POINTER(FriParams), ctypes.c_char_p, sz, ctypes.POINTER(sz)]
+    L.sg_stir_verify.argtypes = [ctypes.c_char_p, sz, ctypes.POINTER(FriParams)]
+    L.sg_prove_hash_rollup.argtypes = [vp, vp, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
+    _lib = L
+    return L
+
+
+def _addr(x):
+    """(pointer, keepalive, is_numpy) for a numpy uint64 array, a CUDA tensor or an int device pointer."""
+    if isinstance(x, np.ndarray):
+        if x.dtype != np.uint64:
+            raise TypeError("host buffers must be numpy uint64")
+        if not x.flags["C_CONTIGUOUS"]:
+            raise ValueError("host buffers must be C-contiguous")
+        return x.ctypes.data, x, True
+    if hasattr(x, "data_ptr"):
+        if not x.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        if x.element_size() != 8:
+            raise TypeError("tensors must hold 64-bit elements")
+        return x.data_ptr(), x, False
+    if isinstance(x, int):
+        return x, None, False
+    raise TypeError(f"unsupported buffer type {type(x)!r}")
+
+
+def make_schedule(n0: int, stir: bool = True):
+    """swarm-dns/src/prover.rs:53-67"""
+    if n0 <= 0 or n0 & (n0 - 1):
+        raise ValueError("n0 must be a power of 2")
+    lg = n0.bit_length() - 1
+    if not stir:
+        return [2] * lg
+    s = [8] * (lg // 3)
+    if lg % 3:
+        s.append(1 << (lg % 3))
+    return s
+
+
+def build_params(n0: int, pk_hash_32: bytes = None, stir: bool = True) -> FriParams:
+    """swarm-dns/src/prover.rs:89-98"""
+    p = FriParams()
+    lib().sg_build_params(n0, pk_hash_32, int(stir), ctypes.byref(p))
+    return p
+
+
+def deep_fri_verify(params: FriParams, proof: bytes) -> bool:
+    """STIR verifier on serialized proof bytes (host code; needs no GPU)."""
+    return lib().sg_stir_verify(proof, len(proof), ctypes.byref(params)) == 1
+
+
+class FriDomain:
+    """fri.rs:161-169: the radix-2 domain of size n with ark-poly's generator."""
+
+    def __init__(self, size: int):
+        if size <= 0 or size & (size - 1):
+            raise ValueError("radix-2 domain size must be a power of 2")
+        self.size = size
+        lg = size.bit_length() - 1
+        r = pow(7, (P - 1) >> 32, P)
+        for _ in range(32 - lg):
+            r = r * r % P
+        self.omega = r
+
+    @classmethod
+    def new_radix2(cls, size: int):
+        return cls(size)
+
+
+class Context:
+    """One CUDA device + stream + twiddle tables (sg_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.sg_ctx_create(device, ctypes.byref(h))
+        if rc != SG_OK:
+            raise StarkGpuError(rc, f"sg_ctx_create(device={device}) failed")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.sg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != SG_OK:
+            raise StarkGpuError(rc, self._lib.sg_last_error(self._h).decode())
+
+    def set_stream(self, stream_ptr: int = 0):
+        self._check(self._lib.sg_ctx_set_stream(self._h, stream_ptr or None))
+
+    @property
+    def kernel_launches(self) -> int:
+        return self._lib.sg_kernel_launches(self._h)
+
+    # ---------------------------------------------------------------- NTT / LDE
+    def ntt(self, data, log_n: int, inverse: bool = False, out=None):
+        """Batched ark-poly fft/ifft over the columns of a (cols, 2^log_n) buffer."""
+        ip, _ki, host = _addr(data)
+        n = 1 << log_n
+        if out is None:
+            if not host:
+                raise ValueError("device input needs an explicit out buffer")
+            out = np.empty_like(data)
+        op, _ko, _ = _addr(out)
+        cols = (data.size if host else data.numel()) // n
+        self._check(self._lib.sg_ntt(self._h, ip, op, cols, log_n, int(inverse)))
+        return out
+
+    def lde(self, trace, blowup: int, shift: int = 1, out=None):
+        """lde_trace_columns on a (w, n_trace) column-major buffer -> (w, n_trace*blowup)."""
+        ip, _ki, host = _addr(trace)
+        w, n = trace.shape
+        if out is None:
+            if not host:
+                raise ValueError("device input needs an explicit out buffer")
+            out = np.empty((w, n * blowup), dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        self._check(self._lib.sg_lde(self._h, ip, w, n, blowup, shift, op))
+        return out
+
+    def lde_trace_columns(self, columns, trace_len: int, blowup: int):
+        """Reference signature: list of columns -> list of LDE columns (raises ValueError like Err(String))."""
+        if len(columns) == 0:
+            raise ValueError("no columns provided")
+        for i, col in enumerate(columns):
+            if len(col) != trace_len:
+                raise ValueError(f"column {i}: expected {trace_len} rows, got {len(col)}")
+        if trace_len & (trace_len - 1) or trace_len == 0:
+            raise ValueError(f"trace_len {trace_len} must be a power of 2")
+        if blowup < 2 or blowup & (blowup - 1):
+            raise ValueError(f"blowup {blowup} must be a power-of-2 >= 2")
+        tr = np.ascontiguousarray(np.array(columns, dtype=np.uint64) % np.uint64(P))
+        return list(self.lde(tr, blowup))
+
+    # ---------------------------------------------------------------- merge
+    def merge(self, air: int, lde, n_trace: int, blowup: int, lambdas, phi_mode=PHI_PARALLEL_GATE, out=None):
+        ip, _ki, host = _addr(lde)
+        w = lde.shape[0]
+        lam = np.ascontiguousarray(lambdas, dtype=np.uint64)
+        n = n_trace * blowup
+        if out is None:
+            if not host:
+                raise ValueError("device input needs an explicit out buffer")
+            out = np.empty(n, dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        self._check(self._lib.sg_merge(self._h, air, ip, w, n_trace, blowup, lam.ctypes.data, lam.size, phi_mode,
+                                       op))
+        return out
+
+    def deep_ali_merge_general(self, trace_evals_on_lde, combination_coeffs, air, omega, n_trace, blowup,
+                               phi_mode=PHI_PARALLEL_GATE):
+        del omega  # the domain generator is implied by n = n_trace * blowup
+        lde = np.ascontiguousarray(np.array(trace_evals_on_lde, dtype=np.uint64))
+        return self.merge(air, lde, n_trace, blowup, combination_coeffs, phi_mode)
+
+    # ---------------------------------------------------------------- Merkle
+    def merkle_commit(self, cols, arities, tree_label: int, n_leaves=None, col_stride=None, keep=False):
+        """Commit to the rows of a column-major (width, n) buffer; returns root (and a tree handle if keep)."""
+        ip, _ki, host = _addr(cols)
+        width = cols.shape[0]
+        n = cols.shape[1] if n_leaves is None else n_leaves
+        cs = cols.shape[1] if col_stride is None else col_stride
+        ar = np.ascontiguousarray(arities, dtype=np.uint64)
+        root = ctypes.create_string_buffer(32)
+        t = ctypes.c_void_p()
+        self._check(self._lib.sg_merkle_commit(self._h, ip, n, width, cs, ar.ctypes.data, ar.size, tree_label, root,
+                                               ctypes.byref(t) if keep else None))
+        return (root.raw, MerkleTree(self, t)) if keep else root.raw
+
+    # ---------------------------------------------------------------- STIR
+    def deep_fri_prove(self, f0, domain0, params: FriParams) -> bytes:
+        """STIR prove; returns the ark-serialize (Compress::Yes) bytes of the DeepFriProof."""
+        ip, _ki, host = _addr(f0)
+        n0 = domain0.size if isinstance(domain0, FriDomain) else int(domain0)
+        cap = 1 << 24
+        while True:
+            buf = ctypes.create_string_buffer(cap)
+            ln = ctypes.c_size_t()
+            rc = self._lib.sg_stir_prove(self._h, ip, n0, ctypes.byref(params), buf, cap, ctypes.byref(ln))
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return buf.raw[:ln.value]
+
+    def prove_hash_rollup(self, leaves, pi: bytes, phi_mode=PHI_PARALLEL_GATE) -> bytes:
+        """prove_inner_shard / prove_outer_rollup core on u64 rollup leaves; self-verified."""
+        lv = np.ascontiguousarray(leaves, dtype=np.uint64)
+        if len(pi) != 32:
+            raise ValueError("pi must be 32 bytes")
+        cap = 1 << 24
+        while True:
+            buf = ctypes.create_string_buffer(cap)
+            ln = ctypes.c_size_t()
+            rc = self._lib.sg_prove_hash_rollup(self._h, lv.ctypes.data if lv.size else None, lv.size, pi, phi_mode,
+                                                buf, cap, ctypes.byref(ln))
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return buf.raw[:ln.value]
+
+
+class MerkleTree:
+    """Device-resident tree kept by Context.merkle_commit(keep=True)."""
+
+    def __init__(self, ctx: Context, handle):
+        self._ctx, self._h = ctx, handle
+
+    def open(self, index: int) -> bytes:
+        cap = 1 << 16
+        buf = ctypes.create_string_buffer(cap)
+        ln = ctypes.c_size_t()
+        self._ctx._check(self._ctx._lib.sg_merkle_open(self._ctx._h, self._h, index, buf, cap, ctypes.byref(ln)))
+        return buf.raw[:ln.value]
+
+    def free(self):
+        if self._h:
+            self._ctx._lib.sg_merkle_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

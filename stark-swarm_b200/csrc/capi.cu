@@ -1,0 +1,304 @@
+// capi.cu — extern "C" entry points declared in include/stark_gpu.h.
+#include <cstring>
+#include <vector>
+
+#include "context.hpp"
+#include "merkle.cuh"
+#include "prover.hpp"
+#include "verifier.hpp"
+
+struct sg_tree {
+  sg::DevTree t;
+  sg::DBuf buf;
+};
+
+namespace {
+
+int fail(sg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+template <class F>
+int guarded(sg_ctx* c, F&& f) {
+  if (!c) return SG_EINVAL;
+  try {
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, SG_ECUDA, "cudaSetDevice failed");
+    f();
+    c->err.clear();
+    return SG_OK;
+  } catch (const sg::SgError& e) {
+    return fail(c, e.code, e.msg);
+  } catch (const std::bad_alloc&) {
+    return fail(c, SG_ENOMEM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(c, SG_EINVAL, e.what());
+  }
+}
+
+// A caller buffer on the device is used in place; a host buffer is staged.
+struct In {
+  const uint64_t* d = nullptr;
+  sg::DBuf stage;
+  In(const uint64_t* p, size_t elems, cudaStream_t s) {
+    if (elems == 0 || sg::is_device_ptr(p)) {
+      d = p;
+      return;
+    }
+    stage.alloc(elems, s);
+    sg::cuda_check(cudaMemcpyAsync(stage.p, p, elems * 8, cudaMemcpyHostToDevice, s), "h2d");
+    d = stage.p;
+  }
+};
+struct Out {
+  uint64_t* user;
+  uint64_t* d = nullptr;
+  size_t elems;
+  bool host = false;
+  sg::DBuf stage;
+  cudaStream_t s;
+  Out(uint64_t* p, size_t n, cudaStream_t st) : user(p), elems(n), s(st) {
+    if (n == 0 || sg::is_device_ptr(p)) {
+      d = p;
+      return;
+    }
+    host = true;
+    stage.alloc(n, s);
+    d = stage.p;
+  }
+  void finish() {
+    if (host) sg::cuda_check(cudaMemcpyAsync(user, d, elems * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    sg::cuda_check(cudaStreamSynchronize(s), "sync");
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int sg_ctx_create(int device, sg_ctx** out) {
+  if (!out) return SG_EINVAL;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return SG_ECUDA;
+  }
+  if (device < 0 || device >= n) return SG_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return SG_ECUDA;
+  sg_ctx* c = new sg_ctx;
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return SG_ECUDA;
+  }
+  c->stream = c->own_stream;
+  if (sg::ntt_tables_init(&c->tw) != cudaSuccess) {
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+    return SG_ECUDA;
+  }
+  // keep freed pool memory cached: repeated proofs reuse it without cudaMalloc
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  *out = c;
+  return SG_OK;
+}
+
+void sg_ctx_destroy(sg_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  sg::ntt_tables_free(&c->tw);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+int sg_ctx_set_stream(sg_ctx* c, void* stream) {
+  if (!c) return SG_EINVAL;
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return SG_OK;
+}
+
+const char* sg_last_error(const sg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+uint64_t sg_kernel_launches(const sg_ctx*) { return sg::g_kernel_launches.load(); }
+
+int sg_ntt(sg_ctx* c, const uint64_t* in, uint64_t* out, size_t n_cols, size_t log_n, int inverse) {
+  return guarded(c, [&] {
+    sg::require(in && out && n_cols > 0 && n_cols < (1u << 31), "ntt: bad buffers or column count");
+    sg::require(log_n <= (size_t)sg::kMaxLogN, "ntt: log_n must be <= 24");
+    const size_t n = size_t(1) << log_n, total = n_cols * n;
+    In di(in, total, c->stream);
+    Out dout(out, total, c->stream);
+    sg::DBuf scratch(log_n > 12 ? total : 0, c->stream);
+    sg::cuda_check(sg::ntt_batch(c->tw, di.d, dout.d, (uint32_t)n_cols, n, n, (int)log_n, inverse != 0, n,
+                                 scratch.p, c->stream),
+                   "ntt");
+    dout.finish();
+  });
+}
+
+int sg_lde(sg_ctx* c, const uint64_t* trace, size_t w, size_t n_trace, size_t blowup, uint64_t shift,
+           uint64_t* out) {
+  return guarded(c, [&] {
+    sg::require(trace && out, "lde: null buffer");
+    sg::require(w > 0 && n_trace > 0 && blowup > 0, "lde: empty input");
+    In di(trace, w * n_trace, c->stream);
+    Out dout(out, w * n_trace * blowup, c->stream);
+    sg::lde_device(c, di.d, w, n_trace, blowup, shift, dout.d);
+    dout.finish();
+  });
+}
+
+int sg_merge(sg_ctx* c, int air, const uint64_t* lde, size_t w, size_t n_trace, size_t blowup,
+             const uint64_t* lambdas, size_t k, int phi_mode, uint64_t* c_eval) {
+  return guarded(c, [&] {
+    sg::require(lde && lambdas && c_eval, "merge: null buffer");
+    sg::require(n_trace > 0 && blowup > 0, "merge: empty input");
+    const size_t n = n_trace * blowup;
+    std::vector<uint64_t> lam(lambdas, lambdas + k);  // lambdas are read on the host
+    In di(lde, w * n, c->stream);
+    Out dout(c_eval, n, c->stream);
+    sg::merge_device(c, air, di.d, w, n_trace, blowup, lam.data(), k, phi_mode, dout.d);
+    dout.finish();
+  });
+}
+
+int sg_merkle_commit(sg_ctx* c, const uint64_t* cols, size_t n_leaves, size_t width, size_t col_stride,
+                     const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t root[32], sg_tree** keep) {
+  if (keep) *keep = nullptr;
+  return guarded(c, [&] {
+    sg::require(cols && root && arities && depth > 0 && n_leaves > 0, "merkle_commit: bad arguments");
+    sg::require(width > 0 && col_stride >= n_leaves, "merkle_commit: bad width or column stride");
+    std::vector<uint32_t> ar;
+    for (size_t i = 0; i < depth; ++i) {
+      sg::require(arities[i] >= 2 && arities[i] <= 1024, "merkle_commit: arity out of range");
+      ar.push_back((uint32_t)arities[i]);
+    }
+    In di(cols, (width - 1) * col_stride + n_leaves, c->stream);
+    sg_tree* t = new sg_tree;
+    try {
+      sg::require(sg::tree_plan(&t->t, n_leaves, ar, tree_label), "merkle_commit: arities do not reach the root");
+      t->buf.alloc(t->t.total_digests * 4, c->stream);
+      t->t.d = t->buf.p;
+      sg::cuda_check(sg::tree_hash_leaves(t->t, di.d, (uint32_t)width, col_stride, 0, c->stream), "leaves");
+      sg::cuda_check(sg::tree_hash_levels(t->t, c->stream), "levels");
+      sg::cuda_check(cudaMemcpyAsync(root, t->t.d + 4 * t->t.off.back(), 32, cudaMemcpyDeviceToHost, c->stream),
+                     "d2h");
+      sg::cuda_check(cudaStreamSynchronize(c->stream), "sync");
+    } catch (...) {
+      delete t;
+      throw;
+    }
+    if (keep)
+      *keep = t;
+    else
+      delete t;
+  });
+}
+
+int sg_merkle_open(sg_ctx* c, const sg_tree* tree, size_t index, uint8_t* out, size_t cap, size_t* len) {
+  return guarded(c, [&] {
+    sg::require(tree && len, "merkle_open: null tree or length");
+    sg::require(index < tree->t.len[0], "merkle_open: index out of range");
+    std::vector<uint64_t> idx;
+    sg::opening_indices(tree->t, index, &idx);
+    sg::DBuf di(idx.size(), c->stream), dout(4 * idx.size(), c->stream);
+    sg::cuda_check(cudaMemcpyAsync(di.p, idx.data(), idx.size() * 8, cudaMemcpyHostToDevice, c->stream), "h2d");
+    sg::cuda_check(sg::gather_digests(tree->t.d, di.p, idx.size(), dout.p, c->stream), "gather");
+    std::vector<uint64_t> got(4 * idx.size());
+    sg::cuda_check(cudaMemcpyAsync(got.data(), dout.p, got.size() * 8, cudaMemcpyDeviceToHost, c->stream), "d2h");
+    sg::cuda_check(cudaStreamSynchronize(c->stream), "sync");
+    sg::ByteWriter w;
+    size_t pos = 0;
+    auto dig = [&]() {
+      sg::Digest d;
+      memcpy(d.data(), got.data() + pos, 32);
+      pos += 4;
+      return d;
+    };
+    sg::Opening o;
+    o.index = index;
+    o.leaf = dig();
+    for (size_t l = 0; l + 1 < tree->t.len.size(); ++l) {
+      std::vector<sg::Digest> sib(tree->t.arity[l] - 1);
+      for (auto& d : sib) d = dig();
+      o.path.push_back(std::move(sib));
+    }
+    w.opening(o);
+    *len = w.b.size();
+    if (w.b.size() > cap || !out) throw sg::SgError{SG_ESPACE, "merkle_open: output buffer too small"};
+    memcpy(out, w.b.data(), w.b.size());
+  });
+}
+
+void sg_merkle_free(sg_tree* t) { delete t; }
+
+void sg_build_params(size_t n0, const uint8_t* pi32, int stir, sg_fri_params* out) {
+  if (!out) return;
+  memset(out, 0, sizeof *out);
+  unsigned lg = 0;
+  while ((size_t(1) << lg) < n0) ++lg;
+  if (stir) {
+    for (unsigned i = 0; i < lg / 3; ++i) out->schedule[out->schedule_len++] = 8;
+    if (lg % 3) out->schedule[out->schedule_len++] = 1ull << (lg % 3);
+  } else {
+    for (unsigned i = 0; i < lg && i < SG_MAX_SCHEDULE; ++i) out->schedule[out->schedule_len++] = 2;
+  }
+  out->r = out->s0 = 54;
+  out->seed_z = 0xDEEFBAADull;
+  out->coeff_commit_final = 1;
+  out->d_final = 1;
+  out->stir = stir ? 1 : 0;
+  if (pi32) {
+    out->has_pi = 1;
+    memcpy(out->pi_hash, pi32, 32);
+  }
+}
+
+int sg_stir_prove(sg_ctx* c, const uint64_t* f0, size_t n0, const sg_fri_params* params, uint8_t* proof,
+                  size_t cap, size_t* len) {
+  return guarded(c, [&] {
+    sg::require(f0 && params && len, "stir_prove: null argument");
+    sg::require(n0 > 0 && n0 <= (size_t(1) << sg::kMaxLogN), "stir_prove: bad n0");
+    In di(f0, n0, c->stream);
+    std::vector<uint8_t> b = sg::stir_prove_device(c, di.d, n0, *params);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "stir_prove: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+int sg_stir_verify(const uint8_t* proof, size_t len, const sg_fri_params* params) {
+  if (!proof || !params) return 0;
+  try {
+    return sg::stir_verify(sg::decode_proof(proof, len), *params) ? 1 : 0;
+  } catch (...) {
+    return 0;
+  }
+}
+
+int sg_prove_hash_rollup(sg_ctx* c, const uint64_t* leaves, size_t n_leaves, const uint8_t pi[32], int phi_mode,
+                         uint8_t* proof, size_t cap, size_t* len) {
+  return guarded(c, [&] {
+    sg::require(len && (leaves || n_leaves == 0), "prove_hash_rollup: null argument");
+    std::vector<uint64_t> lv(n_leaves);
+    if (n_leaves) {
+      if (sg::is_device_ptr(leaves)) {
+        sg::cuda_check(cudaMemcpy(lv.data(), leaves, n_leaves * 8, cudaMemcpyDeviceToHost), "d2h");
+      } else {
+        memcpy(lv.data(), leaves, n_leaves * 8);
+      }
+    }
+    std::vector<uint8_t> b = sg::prove_hash_rollup_host_leaves(c, lv.data(), n_leaves, pi, phi_mode, true);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_hash_rollup: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// context.hpp — library context, device buffers and error plumbing.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <string>
+
+#include "counters.hpp"
+#include "ntt.cuh"
+#include "stark_gpu.h"
+
+struct sg_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  sg::NttTables tw;
+  std::string err;
+};
+
+namespace sg {
+
+struct SgError {
+  int code;
+  std::string msg;
+};
+
+inline void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw SgError{SG_ECUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+inline void require(bool ok, const std::string& msg) {
+  if (!ok) throw SgError{SG_EINVAL, msg};
+}
+
+// Stream-ordered device buffer from the device's default memory pool.
+struct DBuf {
+  uint64_t* p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = nullptr;
+  DBuf() = default;
+  DBuf(size_t elems, cudaStream_t st) { alloc(elems, st); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; }
+  DBuf& operator=(DBuf&& o) noexcept {
+    release();
+    p = o.p;
+    n = o.n;
+    s = o.s;
+    o.p = nullptr;
+    return *this;
+  }
+  void alloc(size_t elems, cudaStream_t st) {
+    release();
+    s = st;
+    n = elems;
+    if (elems == 0) return;
+    cudaError_t e = cudaMallocAsync((void**)&p, elems * sizeof(uint64_t), st);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw SgError{SG_ENOMEM, std::string("device allocation of ") + std::to_string(elems * 8) +
+                                   " bytes failed: " + cudaGetErrorString(e)};
+    }
+  }
+  void release() {
+    if (p) cudaFreeAsync(p, s);
+    p = nullptr;
+  }
+  ~DBuf() { release(); }
+};
+
+bool is_device_ptr(const void* p);
+
+}  // namespace sg

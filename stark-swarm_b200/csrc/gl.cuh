@@ -1,0 +1,191 @@
+// gl.cuh — Goldilocks field p = 2^64 - 2^32 + 1 and its sextic tower, for
+// host and device. Elements are canonical uint64 (< p) everywhere in this
+// library: trace, LDE, quotient and STIR layers are stored canonical, which is
+// also the byte form the reference hashes (le64 of into_bigint().0[0],
+// merkle/src/lib.rs:56-62) and serializes.
+//
+// Tower (deep_ali/src/cubic_ext.rs:63-76, sextic_ext.rs:72-100):
+//   Fp3 = Fp[a]/(a^3 - 7),  Fp6 = Fp3[u]/(u^2 - a),
+//   components ordered [c0.c0, c0.c1, c0.c2, c1.c0, c1.c1, c1.c2].
+// On the device the 64x64-bit products compile to 32-bit IMAD chains
+// (mul.lo.u64 / mul.hi.u64); reduction uses 2^64 = 2^32 - 1 and 2^96 = -1.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define GL_HD __host__ __device__ __forceinline__
+#else
+#define GL_HD inline
+#endif
+
+namespace gl {
+
+static constexpr uint64_t P = 0xFFFFFFFF00000001ull;
+static constexpr uint64_t EPS = 0xFFFFFFFFull;
+
+GL_HD uint64_t add(uint64_t a, uint64_t b) {
+  uint64_t s = a + b;
+  bool c = s < a;
+  return (c || s >= P) ? s - P : s;
+}
+GL_HD uint64_t sub(uint64_t a, uint64_t b) {
+  uint64_t d = a - b;
+  return a < b ? d + P : d;
+}
+GL_HD uint64_t neg(uint64_t a) { return a ? P - a : 0; }
+
+GL_HD uint64_t reduce128(uint64_t hi, uint64_t lo) {
+  uint64_t hh = hi >> 32, hl = hi & EPS;
+  uint64_t t0 = lo - hh;
+  if (lo < hh) t0 -= EPS;
+  uint64_t t1 = hl * EPS;
+  uint64_t r = t0 + t1;
+  if (r < t0) r += EPS;
+  return r >= P ? r - P : r;
+}
+
+GL_HD uint64_t mul(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+  return reduce128(__umul64hi(a, b), a * b);
+#else
+  unsigned __int128 x = (unsigned __int128)a * b;
+  return reduce128((uint64_t)(x >> 64), (uint64_t)x);
+#endif
+}
+GL_HD uint64_t sqr(uint64_t a) { return mul(a, a); }
+
+GL_HD uint64_t pow(uint64_t a, uint64_t e) {
+  uint64_t r = 1;
+  while (e) {
+    if (e & 1) r = mul(r, a);
+    a = mul(a, a);
+    e >>= 1;
+  }
+  return r;
+}
+GL_HD uint64_t inv(uint64_t a) { return pow(a, P - 2); }
+
+// x * 2^e for 0 <= e < 64 (one 128-bit reduction, no multiply)
+GL_HD uint64_t mul_pow2_lt64(uint64_t x, unsigned e) {
+  if (e == 0) return x;
+  return reduce128(x >> (64 - e), x << e);
+}
+// x * 2^e for any 0 <= e < 192 (2 has order 192 in this field)
+GL_HD uint64_t mul_pow2(uint64_t x, unsigned e) {
+  bool negate = false;
+  if (e >= 96) {
+    e -= 96;
+    negate = true;
+  }
+  uint64_t r = e < 64 ? mul_pow2_lt64(x, e) : mul_pow2_lt64(mul_pow2_lt64(x, e - 32), 32);
+  return negate ? neg(r) : r;
+}
+
+// Primitive 2^k-th root of unity of ark-poly's Radix2EvaluationDomain:
+// 7^((p-1)/2^32) squared (32-k) times (ark-goldilocks/build.rs:20-24).
+GL_HD uint64_t root_of_unity(unsigned log_n) {
+  uint64_t r = pow(7, (P - 1) >> 32);
+  for (unsigned i = log_n; i < 32; ++i) r = sqr(r);
+  return r;
+}
+
+// ------------------------------------------------------------------ Fp6
+struct Fp6 {
+  uint64_t c[6];
+};
+
+GL_HD Fp6 e_zero() { return Fp6{{0, 0, 0, 0, 0, 0}}; }
+GL_HD Fp6 e_one() { return Fp6{{1, 0, 0, 0, 0, 0}}; }
+GL_HD Fp6 e_from(uint64_t x) { return Fp6{{x, 0, 0, 0, 0, 0}}; }
+GL_HD bool e_eq(const Fp6& a, const Fp6& b) {
+  bool r = true;
+  for (int i = 0; i < 6; ++i) r = r && a.c[i] == b.c[i];
+  return r;
+}
+GL_HD Fp6 e_add(const Fp6& a, const Fp6& b) {
+  Fp6 r;
+  for (int i = 0; i < 6; ++i) r.c[i] = add(a.c[i], b.c[i]);
+  return r;
+}
+GL_HD Fp6 e_sub(const Fp6& a, const Fp6& b) {
+  Fp6 r;
+  for (int i = 0; i < 6; ++i) r.c[i] = sub(a.c[i], b.c[i]);
+  return r;
+}
+GL_HD Fp6 e_scale(const Fp6& a, uint64_t s) {
+  Fp6 r;
+  for (int i = 0; i < 6; ++i) r.c[i] = mul(a.c[i], s);
+  return r;
+}
+GL_HD uint64_t mul7(uint64_t x) {
+  // 7x = 8x - x with one reduction
+  return sub(mul_pow2_lt64(x, 3), x);
+}
+// Fp3 product, schoolbook with a^3 = 7 (cubic_ext.rs:166-175)
+GL_HD void f3_mul(const uint64_t* a, const uint64_t* b, uint64_t* r) {
+  uint64_t c0 = add(mul(a[0], b[0]), mul7(add(mul(a[1], b[2]), mul(a[2], b[1]))));
+  uint64_t c1 = add(add(mul(a[0], b[1]), mul(a[1], b[0])), mul7(mul(a[2], b[2])));
+  uint64_t c2 = add(add(mul(a[0], b[2]), mul(a[1], b[1])), mul(a[2], b[0]));
+  r[0] = c0;
+  r[1] = c1;
+  r[2] = c2;
+}
+// Fp6 product, Karatsuba over Fp3 with u^2 = a (sextic_ext.rs:200-206)
+GL_HD Fp6 e_mul(const Fp6& x, const Fp6& y) {
+  uint64_t v0[3], v1[3], sa[3], sb[3], m[3];
+  f3_mul(x.c, y.c, v0);
+  f3_mul(x.c + 3, y.c + 3, v1);
+  for (int i = 0; i < 3; ++i) {
+    sa[i] = add(x.c[i], x.c[3 + i]);
+    sb[i] = add(y.c[i], y.c[3 + i]);
+  }
+  f3_mul(sa, sb, m);
+  Fp6 r;
+  // c0 = v0 + a*v1 ; a*(t0,t1,t2) = (7 t2, t0, t1)
+  r.c[0] = add(v0[0], mul7(v1[2]));
+  r.c[1] = add(v0[1], v1[0]);
+  r.c[2] = add(v0[2], v1[1]);
+  for (int i = 0; i < 3; ++i) r.c[3 + i] = sub(sub(m[i], v0[i]), v1[i]);
+  return r;
+}
+GL_HD Fp6 e_pow(Fp6 b, uint64_t e) {
+  Fp6 r = e_one();
+  while (e) {
+    if (e & 1) r = e_mul(r, b);
+    b = e_mul(b, b);
+    e >>= 1;
+  }
+  return r;
+}
+// Inverse through the Fp3 and Fp norms (cubic_ext.rs:205-226, sextic_ext.rs:240-256).
+// Returns false for zero.
+GL_HD bool e_inv(const Fp6& x, Fp6* out) {
+  uint64_t aa[3], bb[3], n3[3];
+  f3_mul(x.c, x.c, aa);
+  f3_mul(x.c + 3, x.c + 3, bb);
+  n3[0] = sub(aa[0], mul7(bb[2]));
+  n3[1] = sub(aa[1], bb[0]);
+  n3[2] = sub(aa[2], bb[1]);
+  // Fp3 inverse of n3
+  uint64_t a0 = n3[0], a1 = n3[1], a2 = n3[2];
+  uint64_t t = mul(mul(a0, a0), a0);
+  t = add(t, mul(7, mul(mul(a1, a1), a1)));
+  t = add(t, mul(49, mul(mul(a2, a2), a2)));
+  t = sub(t, mul(21, mul(mul(a0, a1), a2)));
+  if (t == 0) return false;
+  uint64_t ti = inv(t);
+  uint64_t i3[3];
+  i3[0] = mul(sub(mul(a0, a0), mul7(mul(a1, a2))), ti);
+  i3[1] = mul(sub(mul7(mul(a2, a2)), mul(a0, a1)), ti);
+  i3[2] = mul(sub(mul(a1, a1), mul(a0, a2)), ti);
+  uint64_t r0[3], r1[3];
+  f3_mul(x.c, i3, r0);
+  f3_mul(x.c + 3, i3, r1);
+  for (int i = 0; i < 3; ++i) {
+    out->c[i] = r0[i];
+    out->c[3 + i] = neg(r1[i]);
+  }
+  return true;
+}
+
+}  // namespace gl

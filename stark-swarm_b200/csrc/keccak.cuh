@@ -1,0 +1,211 @@
+// keccak.cuh — Keccak-f[1600] and SHA3-256 (FIPS 202) for host and device.
+//
+// The reference hashes every Merkle leaf/node, its transcript and its tree
+// domain tags with sha3 0.10.8's Sha3_256 (hash/src/selected.rs:100-112,
+// merkle/src/lib.rs:185-238, transcript/src/lib.rs:158-213). SHA3-256 absorbs
+// 136-byte blocks (17 lanes) and pads with 0x06 .. 0x80.
+//
+// On the device the 25-lane state lives in registers; each 64-bit XOR/rotate
+// lowers to 32-bit LOP3/SHF pairs. Messages in this library are built from
+// whole 64-bit lanes (32-byte labels, 8-byte field elements, 32-byte digests),
+// so lane-granular absorption is all the kernels need.
+#pragma once
+#include <cstdint>
+#include <cstring>
+
+#if defined(__CUDACC__)
+#define KC_HD __host__ __device__ __forceinline__
+#else
+#define KC_HD inline
+#endif
+
+namespace kc {
+
+KC_HD uint64_t rotl(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
+
+#if defined(__CUDACC__)
+__constant__ static const uint64_t kRC_dev[24] = {
+#else
+static const uint64_t kRC_dev[24] = {
+#endif
+    0x0000000000000001ull, 0x0000000000008082ull, 0x800000000000808Aull, 0x8000000080008000ull,
+    0x000000000000808Bull, 0x0000000080000001ull, 0x8000000080008081ull, 0x8000000000008009ull,
+    0x000000000000008Aull, 0x0000000000000088ull, 0x0000000080008009ull, 0x000000008000000Aull,
+    0x000000008000808Bull, 0x800000000000008Bull, 0x8000000000008089ull, 0x8000000000008003ull,
+    0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800Aull, 0x800000008000000Aull,
+    0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
+
+static const uint64_t kRC_host[24] = {
+    0x0000000000000001ull, 0x0000000000008082ull, 0x800000000000808Aull, 0x8000000080008000ull,
+    0x000000000000808Bull, 0x0000000080000001ull, 0x8000000080008081ull, 0x8000000000008009ull,
+    0x000000000000008Aull, 0x0000000000000088ull, 0x0000000080008009ull, 0x000000008000000Aull,
+    0x000000008000808Bull, 0x800000000000008Bull, 0x8000000000008089ull, 0x8000000000008003ull,
+    0x8000000000008002ull, 0x8000000000000080ull, 0x000000000000800Aull, 0x800000008000000Aull,
+    0x8000000080008081ull, 0x8000000000008080ull, 0x0000000080000001ull, 0x8000000080008008ull};
+
+// One round on a register-resident state (theta, rho+pi, chi, iota).
+#define KC_ROUND(A, rc)                                                               \
+  {                                                                                   \
+    uint64_t C0 = A[0] ^ A[5] ^ A[10] ^ A[15] ^ A[20];                                \
+    uint64_t C1 = A[1] ^ A[6] ^ A[11] ^ A[16] ^ A[21];                                \
+    uint64_t C2 = A[2] ^ A[7] ^ A[12] ^ A[17] ^ A[22];                                \
+    uint64_t C3 = A[3] ^ A[8] ^ A[13] ^ A[18] ^ A[23];                                \
+    uint64_t C4 = A[4] ^ A[9] ^ A[14] ^ A[19] ^ A[24];                                \
+    uint64_t D0 = C4 ^ kc::rotl(C1, 1), D1 = C0 ^ kc::rotl(C2, 1);                    \
+    uint64_t D2 = C1 ^ kc::rotl(C3, 1), D3 = C2 ^ kc::rotl(C4, 1);                    \
+    uint64_t D4 = C3 ^ kc::rotl(C0, 1);                                               \
+    uint64_t B0 = A[0] ^ D0;                                                          \
+    uint64_t B1 = kc::rotl(A[6] ^ D1, 44);                                            \
+    uint64_t B2 = kc::rotl(A[12] ^ D2, 43);                                           \
+    uint64_t B3 = kc::rotl(A[18] ^ D3, 21);                                           \
+    uint64_t B4 = kc::rotl(A[24] ^ D4, 14);                                           \
+    uint64_t B5 = kc::rotl(A[3] ^ D3, 28);                                            \
+    uint64_t B6 = kc::rotl(A[9] ^ D4, 20);                                            \
+    uint64_t B7 = kc::rotl(A[10] ^ D0, 3);                                            \
+    uint64_t B8 = kc::rotl(A[16] ^ D1, 45);                                           \
+    uint64_t B9 = kc::rotl(A[22] ^ D2, 61);                                           \
+    uint64_t B10 = kc::rotl(A[1] ^ D1, 1);                                            \
+    uint64_t B11 = kc::rotl(A[7] ^ D2, 6);                                            \
+    uint64_t B12 = kc::rotl(A[13] ^ D3, 25);                                          \
+    uint64_t B13 = kc::rotl(A[19] ^ D4, 8);                                           \
+    uint64_t B14 = kc::rotl(A[20] ^ D0, 18);                                          \
+    uint64_t B15 = kc::rotl(A[4] ^ D4, 27);                                           \
+    uint64_t B16 = kc::rotl(A[5] ^ D0, 36);                                           \
+    uint64_t B17 = kc::rotl(A[11] ^ D1, 10);                                          \
+    uint64_t B18 = kc::rotl(A[17] ^ D2, 15);                                          \
+    uint64_t B19 = kc::rotl(A[23] ^ D3, 56);                                          \
+    uint64_t B20 = kc::rotl(A[2] ^ D2, 62);                                           \
+    uint64_t B21 = kc::rotl(A[8] ^ D3, 55);                                           \
+    uint64_t B22 = kc::rotl(A[14] ^ D4, 39);                                          \
+    uint64_t B23 = kc::rotl(A[15] ^ D0, 41);                                          \
+    uint64_t B24 = kc::rotl(A[21] ^ D1, 2);                                           \
+    A[0] = B0 ^ (~B1 & B2) ^ (rc);                                                    \
+    A[1] = B1 ^ (~B2 & B3);                                                           \
+    A[2] = B2 ^ (~B3 & B4);                                                           \
+    A[3] = B3 ^ (~B4 & B0);                                                           \
+    A[4] = B4 ^ (~B0 & B1);                                                           \
+    A[5] = B5 ^ (~B6 & B7);                                                           \
+    A[6] = B6 ^ (~B7 & B8);                                                           \
+    A[7] = B7 ^ (~B8 & B9);                                                           \
+    A[8] = B8 ^ (~B9 & B5);                                                           \
+    A[9] = B9 ^ (~B5 & B6);                                                           \
+    A[10] = B10 ^ (~B11 & B12);                                                       \
+    A[11] = B11 ^ (~B12 & B13);                                                       \
+    A[12] = B12 ^ (~B13 & B14);                                                       \
+    A[13] = B13 ^ (~B14 & B10);                                                       \
+    A[14] = B14 ^ (~B10 & B11);                                                       \
+    A[15] = B15 ^ (~B16 & B17);                                                       \
+    A[16] = B16 ^ (~B17 & B18);                                                       \
+    A[17] = B17 ^ (~B18 & B19);                                                       \
+    A[18] = B18 ^ (~B19 & B15);                                                       \
+    A[19] = B19 ^ (~B15 & B16);                                                       \
+    A[20] = B20 ^ (~B21 & B22);                                                       \
+    A[21] = B21 ^ (~B22 & B23);                                                       \
+    A[22] = B22 ^ (~B23 & B24);                                                       \
+    A[23] = B23 ^ (~B24 & B20);                                                       \
+    A[24] = B24 ^ (~B20 & B21);                                                       \
+  }
+
+KC_HD void keccak_f(uint64_t A[25]) {
+#if defined(__CUDA_ARCH__)
+#pragma unroll 2
+  for (int r = 0; r < 24; ++r) KC_ROUND(A, kRC_dev[r]);
+#else
+  for (int r = 0; r < 24; ++r) KC_ROUND(A, kRC_host[r]);
+#endif
+}
+
+// Lane-granular SHA3-256 sponge: absorb whole 64-bit lanes, squeeze 4 lanes.
+// The state is only ever indexed by constants (a switch on the block
+// position), so it stays in registers; when the caller's loop is unrolled the
+// position is a compile-time constant and the switch disappears.
+struct LaneSponge {
+  uint64_t s[25];
+  int pos;  // lanes absorbed into the current block (0..16)
+  KC_HD void init() {
+#pragma unroll
+    for (int i = 0; i < 25; ++i) s[i] = 0;
+    pos = 0;
+  }
+  KC_HD void xor_at(int p, uint64_t w) {
+    switch (p) {
+      case 0: s[0] ^= w; break;
+      case 1: s[1] ^= w; break;
+      case 2: s[2] ^= w; break;
+      case 3: s[3] ^= w; break;
+      case 4: s[4] ^= w; break;
+      case 5: s[5] ^= w; break;
+      case 6: s[6] ^= w; break;
+      case 7: s[7] ^= w; break;
+      case 8: s[8] ^= w; break;
+      case 9: s[9] ^= w; break;
+      case 10: s[10] ^= w; break;
+      case 11: s[11] ^= w; break;
+      case 12: s[12] ^= w; break;
+      case 13: s[13] ^= w; break;
+      case 14: s[14] ^= w; break;
+      case 15: s[15] ^= w; break;
+      default: s[16] ^= w; break;
+    }
+  }
+  KC_HD void lane(uint64_t w) {
+    xor_at(pos, w);
+    if (++pos == 17) {
+      keccak_f(s);
+      pos = 0;
+    }
+  }
+  KC_HD void finish(uint64_t out[4]) {
+    xor_at(pos, 0x06ull);
+    s[16] ^= 0x8000000000000000ull;
+    keccak_f(s);
+    out[0] = s[0];
+    out[1] = s[1];
+    out[2] = s[2];
+    out[3] = s[3];
+  }
+};
+
+// Byte-granular streaming SHA3-256 for host code (transcript, domain tags).
+struct Sha3 {
+  uint64_t st[25];
+  uint8_t buf[136];
+  size_t fill;
+  Sha3() { reset(); }
+  void reset() {
+    memset(st, 0, sizeof st);
+    fill = 0;
+  }
+  void block(const uint8_t* b) {
+    for (int i = 0; i < 17; ++i) {
+      uint64_t w;
+      memcpy(&w, b + 8 * i, 8);
+      st[i] ^= w;
+    }
+    keccak_f(st);
+  }
+  void update(const void* data, size_t len) {
+    const uint8_t* p = (const uint8_t*)data;
+    while (len) {
+      size_t take = 136 - fill < len ? 136 - fill : len;
+      memcpy(buf + fill, p, take);
+      fill += take;
+      p += take;
+      len -= take;
+      if (fill == 136) {
+        block(buf);
+        fill = 0;
+      }
+    }
+  }
+  void finalize(uint8_t out[32]) const {
+    Sha3 c = *this;
+    memset(c.buf + c.fill, 0, 136 - c.fill);
+    c.buf[c.fill] ^= 0x06;
+    c.buf[135] ^= 0x80;
+    c.block(c.buf);
+    memcpy(out, c.st, 32);
+  }
+};
+
+}  // namespace kc

@@ -1,0 +1,224 @@
+// merkle.cu — leaf and node hashing kernels for the SHA3-256 Merkle channel.
+#include "keccak.cuh"
+#include "merkle.cuh"
+#include "counters.hpp"
+
+namespace sg {
+
+bool tree_plan(DevTree* t, uint64_t n_leaves, const std::vector<uint32_t>& arities, uint64_t label) {
+  t->label = label;
+  if (arities.empty()) return false;
+  t->arity0 = arities[0];
+  t->arity.clear();
+  t->len.assign(1, n_leaves);
+  t->off.assign(1, 0);
+  uint64_t total = n_leaves;
+  size_t l = 0;
+  while (t->len.back() > 1) {
+    if (l >= arities.size() || arities[l] < 2) return false;
+    uint64_t a = arities[l];
+    uint64_t np = (t->len.back() + a - 1) / a;
+    t->arity.push_back((uint32_t)a);
+    t->off.push_back(total);
+    t->len.push_back(np);
+    total += np;
+    ++l;
+  }
+  t->total_digests = total;
+  return n_leaves > 0;
+}
+
+__device__ void leaf_digest_row(const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros, uint64_t i,
+                                uint64_t arity0, uint64_t label, uint64_t out[4]) {
+  kc::LaneSponge sp;
+  sp.init();
+  sp.lane(arity0);
+  sp.lane(0xFFFFFFFFull);
+  sp.lane(i);
+  sp.lane(label);
+  for (uint32_t c = 0; c < w; ++c) sp.lane(__ldg(cols + (uint64_t)c * cs + i));
+  for (uint32_t c = 0; c < zeros; ++c) sp.lane(0);
+  sp.finish(out);
+}
+
+namespace {
+
+// Generic width: runtime loop (positions resolved by the sponge's switch).
+__global__ void leaf_kernel(const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros, uint64_t n,
+                            uint64_t arity0, uint64_t label, uint64_t* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint64_t d[4];
+  leaf_digest_row(cols, w, cs, zeros, i, arity0, label, d);
+  uint64_t* o = out + 4 * i;
+  o[0] = d[0];
+  o[1] = d[1];
+  o[2] = d[2];
+  o[3] = d[3];
+}
+
+// Fixed width: fully unrolled, every lane position is a compile-time constant.
+template <int W, int Z>
+__global__ void leaf_kernel_t(const uint64_t* __restrict__ cols, uint64_t cs, uint64_t n, uint64_t arity0,
+                              uint64_t label, uint64_t* __restrict__ out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  kc::LaneSponge sp;
+  sp.init();
+  sp.lane(arity0);
+  sp.lane(0xFFFFFFFFull);
+  sp.lane(i);
+  sp.lane(label);
+#pragma unroll
+  for (int c = 0; c < W; ++c) sp.lane(__ldg(cols + (uint64_t)c * cs + i));
+#pragma unroll
+  for (int c = 0; c < Z; ++c) sp.lane(0);
+  uint64_t d[4];
+  sp.finish(d);
+  uint64_t* o = out + 4 * i;
+  o[0] = d[0];
+  o[1] = d[1];
+  o[2] = d[2];
+  o[3] = d[3];
+}
+
+template <int A>
+__global__ void node_kernel_t(const uint64_t* __restrict__ child, uint64_t n_child, uint64_t* __restrict__ parent,
+                              uint64_t n_parent, uint64_t level, uint64_t label) {
+  uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (p >= n_parent) return;
+  kc::LaneSponge sp;
+  sp.init();
+  sp.lane(A);
+  sp.lane(level);
+  sp.lane(p);
+  sp.lane(label);
+#pragma unroll
+  for (int k = 0; k < A; ++k) {
+    uint64_t c = p * A + k;
+    if (c >= n_child) c = n_child - 1;  // padding = copies of the last node
+    const uint64_t* cd = child + 4 * c;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sp.lane(cd[q]);
+  }
+  uint64_t d[4];
+  sp.finish(d);
+  uint64_t* o = parent + 4 * p;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) o[q] = d[q];
+}
+
+__global__ void node_kernel(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t n_parent,
+                            uint32_t arity, uint64_t level, uint64_t label) {
+  uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (p >= n_parent) return;
+  kc::LaneSponge sp;
+  sp.init();
+  sp.lane(arity);
+  sp.lane(level);
+  sp.lane(p);
+  sp.lane(label);
+  for (uint32_t k = 0; k < arity; ++k) {
+    uint64_t c = p * arity + k;
+    if (c >= n_child) c = n_child - 1;  // padding = copies of the last node
+    const uint64_t* cd = child + 4 * c;
+    sp.lane(cd[0]);
+    sp.lane(cd[1]);
+    sp.lane(cd[2]);
+    sp.lane(cd[3]);
+  }
+  uint64_t d[4];
+  sp.finish(d);
+  uint64_t* o = parent + 4 * p;
+  o[0] = d[0];
+  o[1] = d[1];
+  o[2] = d[2];
+  o[3] = d[3];
+}
+
+__global__ void gather_digests_kernel(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out) {
+  uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (e >= 4 * n) return;
+  out[e] = d[4 * idx[e >> 2] + (e & 3)];
+}
+
+__global__ void gather_u64_kernel(const uint64_t* src, const uint64_t* idx, uint64_t n, uint64_t* out) {
+  uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (e < n) out[e] = src[idx[e]];
+}
+
+inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros,
+                             cudaStream_t s) {
+  const uint64_t n = t.len[0];
+  const unsigned T = 128, B = blocks_for(n, T);
+#define SG_LEAF_CASE(WW, ZZ)                                                           \
+  if (w == WW && zeros == ZZ) {                                                        \
+    leaf_kernel_t<WW, ZZ><<<B, T, 0, s>>>(cols, cs, n, t.arity0, t.label, t.d);        \
+    count_launches(1);                                                                 \
+    return cudaGetLastError();                                                         \
+  }
+  SG_LEAF_CASE(1, 5)
+  SG_LEAF_CASE(2, 0)
+  SG_LEAF_CASE(4, 0)
+  SG_LEAF_CASE(6, 0)
+  SG_LEAF_CASE(8, 0)
+  SG_LEAF_CASE(16, 0)
+  SG_LEAF_CASE(64, 0)
+#undef SG_LEAF_CASE
+  leaf_kernel<<<B, T, 0, s>>>(cols, w, cs, zeros, n, t.arity0, t.label, t.d);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
+  for (size_t l = 0; l + 1 < t.len.size(); ++l) {
+    const uint64_t np = t.len[l + 1];
+    const uint64_t* ch = t.d + 4 * t.off[l];
+    uint64_t* par = t.d + 4 * t.off[l + 1];
+    const unsigned B = blocks_for(np, 128);
+    switch (t.arity[l]) {
+      case 2: node_kernel_t<2><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
+      case 4: node_kernel_t<4><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
+      case 8: node_kernel_t<8><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
+      case 16: node_kernel_t<16><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
+      default: node_kernel<<<B, 128, 0, s>>>(ch, t.len[l], par, np, t.arity[l], l + 1, t.label); break;
+    }
+    count_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t gather_digests(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  gather_digests_kernel<<<blocks_for(4 * n, 256), 256, 0, s>>>(d, idx, n, out);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t gather_u64(const uint64_t* src, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  gather_u64_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, idx, n, out);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+void opening_indices(const DevTree& t, uint64_t index, std::vector<uint64_t>* out) {
+  out->push_back(t.off[0] + index);
+  uint64_t idx = index;
+  for (size_t l = 0; l + 1 < t.len.size(); ++l) {
+    uint64_t a = t.arity[l], g = (idx / a) * a;
+    for (uint64_t k = 0; k < a; ++k) {
+      uint64_t pos = g + k;
+      if (pos == idx) continue;
+      if (pos >= t.len[l]) pos = t.len[l] - 1;
+      out->push_back(t.off[l] + pos);
+    }
+    idx /= a;
+  }
+}
+
+}  // namespace sg

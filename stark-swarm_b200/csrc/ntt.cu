@@ -1,0 +1,333 @@
+// ntt.cu — batched Goldilocks NTT for sm_100a.
+//
+// Global structure: a transform of N = 2^n <= 2^12 is one pass; larger N is a
+// four-step split N = N1 * N2 (N1 <= N2 <= 2^12) done as two passes:
+//   pass 1: for each k1 < N1, DFT_{N2} over k2 of x[k2*N1 + k1], times w_N^{i2*k1},
+//           stored transposed at i2*N1 + k1;
+//   pass 2: for each i2 < N2, DFT_{N1} over the contiguous row, stored at i1*N2 + i2.
+// A CTA owns K "lanes" (independent sub-DFTs with adjacent addresses, so every
+// global row access is K*8 contiguous bytes) x M points in shared memory.
+// Inside the CTA the M-point DFT is a Stockham autosort sequence of radix-16
+// (and one smaller) stages: each thread holds 16 values in registers, reads
+// them, barrier, writes them to their permuted slots, barrier. Shared memory
+// is padded one word per 16 so every stage's stride pattern is conflict-free.
+// The radix-R butterflies use only powers of w_R <= w_16, which in Goldilocks
+// are powers of two (w_16 = 2^156 for ark's root chain), so they cost a shift
+// and a reduction instead of a multiply.
+#include "dft.cuh"
+#include "gl.cuh"
+#include "ntt.cuh"
+#include "counters.hpp"
+
+namespace sg {
+namespace {
+
+__device__ __forceinline__ int padi(int m) { return m + (m >> 4); }
+
+struct PassArgs {
+  const uint64_t* in;
+  uint64_t* out;
+  uint64_t in_col, out_col;   // column strides (grid.y = column)
+  uint64_t in_lane, in_m;     // input address of (lane, m)
+  uint64_t out_lane, out_i;   // output address of (lane, i)
+  uint64_t n_lanes;           // valid lanes
+  // zero padding: the input element's flat index inside its column is
+  // m*in_m + lane*flat_lane; indices >= in_valid are zero and never read
+  uint64_t flat_lane;
+  uint64_t in_valid;
+  int log_k;                  // lanes per CTA = 2^log_k
+  int tw_shift;               // >= 0: output (lane,i) *= w24^((i*lane) << tw_shift)
+  uint64_t scale;             // != 1: outputs *= scale
+  const uint64_t* tw_lo;      // w24^i (direction of the transform)
+  const uint64_t* tw_hi;      // w24^(4096 i) = w_4096^i
+};
+
+// One Stockham stage of radix R over all K lanes of the tile.
+// Each thread holds V values = V/R groups; group g -> lane g / G, j = g % G.
+template <int R, int V, bool INV>
+__device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int log_m, int log_ns,
+                                               const uint64_t* tw_hi) {
+  constexpr int GPT = V / R;
+  constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+  const int M = 1 << log_m, Mp = M + (M >> 4);
+  const int log_g = log_m - LR;
+  const int G = 1 << log_g;
+  const int Ns = 1 << log_ns;
+  uint64_t v[V];
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
+    int g = t + q * T;
+    int l = g >> log_g, j = g & (G - 1);
+    uint64_t* row = sm + l * Mp;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[q * R + r] = row[padi(j + r * G)];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
+    int g = t + q * T;
+    int l = g >> log_g, j = g & (G - 1);
+    int k = j & (Ns - 1);
+    if (log_ns > 0) {
+      const int sh = 12 - log_ns - LR;  // w_{Ns R}^{rk} = w_4096^{rk 4096/(Ns R)}
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[q * R + r] = gl::mul(v[q * R + r], __ldg(tw_hi + (((r * k) << sh) & 4095)));
+    }
+    dft_reg<R, INV>(v + q * R);
+    int idx = ((j >> log_ns) << (log_ns + LR)) + k;
+    uint64_t* row = sm + l * Mp;
+#pragma unroll
+    for (int r = 0; r < R; ++r) row[padi(idx + r * Ns)] = v[q * R + r];
+  }
+  __syncthreads();
+}
+
+template <int LOG_M, bool INV>
+__global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
+  constexpr int M = 1 << LOG_M;
+  constexpr int V = M < 16 ? M : 16;
+  constexpr int Mp = M + (M >> 4);
+  extern __shared__ uint64_t sm[];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int K = 1 << a.log_k;
+  const int E = K * M;
+  const uint64_t lane0 = (uint64_t)blockIdx.x << a.log_k;
+  const uint64_t* in = a.in + (uint64_t)blockIdx.y * a.in_col;
+  uint64_t* out = a.out + (uint64_t)blockIdx.y * a.out_col;
+
+  const bool lane_fast_in = a.in_lane == 1;
+  for (int e = t; e < E; e += T) {
+    int l, m;
+    if (lane_fast_in) {
+      l = e & (K - 1);
+      m = e >> a.log_k;
+    } else {
+      m = e & (M - 1);
+      l = e >> LOG_M;
+    }
+    uint64_t lane = lane0 + l;
+    uint64_t x = 0;
+    if (lane < a.n_lanes && (uint64_t)m * a.in_m + lane * a.flat_lane < a.in_valid)
+      x = in[lane * a.in_lane + (uint64_t)m * a.in_m];
+    sm[l * Mp + padi(m)] = x;
+  }
+  __syncthreads();
+
+  // Stage sequence: radix-16 stages, then one radix 2/4/8 stage for the remainder.
+  constexpr int N16 = LOG_M / 4, REM = LOG_M % 4;
+  int log_ns = 0;
+  if constexpr (LOG_M >= 4) {
+#pragma unroll 1
+    for (int st = 0; st < N16; ++st) {
+      stockham_stage<16, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
+      log_ns += 4;
+    }
+  }
+  if constexpr (REM == 1) stockham_stage<2, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
+  if constexpr (REM == 2) stockham_stage<4, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
+  if constexpr (REM == 3) stockham_stage<8, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
+
+  const bool lane_fast_out = a.out_lane == 1;
+  for (int e = t; e < E; e += T) {
+    int l, i;
+    if (lane_fast_out) {
+      l = e & (K - 1);
+      i = e >> a.log_k;
+    } else {
+      i = e & (M - 1);
+      l = e >> LOG_M;
+    }
+    uint64_t lane = lane0 + l;
+    if (lane >= a.n_lanes) continue;
+    uint64_t x = sm[l * Mp + padi(i)];
+    if (a.tw_shift >= 0) {
+      uint64_t ex = (((uint64_t)i * lane) << a.tw_shift) & ((1ull << 24) - 1);
+      x = gl::mul(x, gl::mul(__ldg(a.tw_lo + (ex & 4095)), __ldg(a.tw_hi + (ex >> 12))));
+    }
+    if (a.scale != 1) x = gl::mul(x, a.scale);
+    out[lane * a.out_lane + (uint64_t)i * a.out_i] = x;
+  }
+}
+
+template <int LOG_M>
+cudaError_t launch_pass(const PassArgs& a0, bool inv, uint32_t n_cols, cudaStream_t s) {
+  constexpr int M = 1 << LOG_M;
+  constexpr int V = M < 16 ? M : 16;
+  PassArgs a = a0;
+  // lanes per CTA: at least 4 (32-byte rows), ~8192 elements per CTA, <= 1024 threads
+  int log_k = LOG_M >= 11 ? 2 : 13 - LOG_M;
+  while (((1 << log_k) * M / V) > 1024) --log_k;
+  a.log_k = log_k;
+  const int K = 1 << log_k;
+  const int T = K * M / V;
+  const size_t smem = (size_t)K * (M + M / 16) * sizeof(uint64_t);
+  const uint64_t blocks = (a.n_lanes + K - 1) / K;
+  auto kern = inv ? ntt_pass_kernel<LOG_M, true> : ntt_pass_kernel<LOG_M, false>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  for (uint32_t c0 = 0; c0 < n_cols; c0 += 65535) {
+    uint32_t nc = n_cols - c0 < 65535 ? n_cols - c0 : 65535;
+    PassArgs b = a;
+    b.in = a.in + (uint64_t)c0 * a.in_col;
+    b.out = a.out + (uint64_t)c0 * a.out_col;
+    kern<<<dim3((unsigned)blocks, nc), T, smem, s>>>(b);
+    count_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pass_dyn(int log_m, const PassArgs& a, bool inv, uint32_t n_cols, cudaStream_t s) {
+  switch (log_m) {
+    case 1: return launch_pass<1>(a, inv, n_cols, s);
+    case 2: return launch_pass<2>(a, inv, n_cols, s);
+    case 3: return launch_pass<3>(a, inv, n_cols, s);
+    case 4: return launch_pass<4>(a, inv, n_cols, s);
+    case 5: return launch_pass<5>(a, inv, n_cols, s);
+    case 6: return launch_pass<6>(a, inv, n_cols, s);
+    case 7: return launch_pass<7>(a, inv, n_cols, s);
+    case 8: return launch_pass<8>(a, inv, n_cols, s);
+    case 9: return launch_pass<9>(a, inv, n_cols, s);
+    case 10: return launch_pass<10>(a, inv, n_cols, s);
+    case 11: return launch_pass<11>(a, inv, n_cols, s);
+    case 12: return launch_pass<12>(a, inv, n_cols, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+__global__ void copy_cols_kernel(const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t in_stride,
+                                 uint64_t out_stride, uint64_t n) {
+  uint64_t total = (uint64_t)n_cols * n;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t c = e / n, k = e - c * n;
+    out[c * out_stride + k] = in[c * in_stride + k];
+  }
+}
+
+__global__ void scale_powers_kernel(const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t stride,
+                                    uint64_t n, uint64_t g) {
+  // each thread scales 32 consecutive coefficients of one column
+  const uint64_t chunks = (n + 31) / 32;
+  uint64_t id = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (id >= chunks * n_cols) return;
+  uint64_t c = id / chunks, k0 = (id - c * chunks) * 32;
+  uint64_t p = gl::pow(g, k0);
+  for (uint64_t k = k0; k < k0 + 32 && k < n; ++k) {
+    out[c * stride + k] = gl::mul(in[c * stride + k], p);
+    p = gl::mul(p, g);
+  }
+}
+
+}  // namespace
+
+cudaError_t ntt_tables_init(NttTables* t) {
+  uint64_t w = gl::root_of_unity(24), wi = gl::inv(w);
+  uint64_t h[4][4096];
+  uint64_t w4096 = gl::pow(w, 4096), wi4096 = gl::pow(wi, 4096);
+  uint64_t a = 1, b = 1, c = 1, d = 1;
+  for (int i = 0; i < 4096; ++i) {
+    h[0][i] = a; a = gl::mul(a, w);
+    h[1][i] = b; b = gl::mul(b, w4096);
+    h[2][i] = c; c = gl::mul(c, wi);
+    h[3][i] = d; d = gl::mul(d, wi4096);
+  }
+  uint64_t* dev = nullptr;
+  cudaError_t e = cudaMalloc(&dev, sizeof h);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpy(dev, h, sizeof h, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(dev);
+    return e;
+  }
+  t->d_fwd_lo = dev;
+  t->d_fwd_hi = dev + 4096;
+  t->d_inv_lo = dev + 2 * 4096;
+  t->d_inv_hi = dev + 3 * 4096;
+  return cudaSuccess;
+}
+
+void ntt_tables_free(NttTables* t) {
+  if (t->d_fwd_lo) cudaFree(t->d_fwd_lo);
+  *t = NttTables{};
+}
+
+cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t in_stride,
+                      uint64_t out_stride, int log_n, bool inverse, uint64_t n_valid, uint64_t* scratch,
+                      cudaStream_t s) {
+  if (n_cols == 0) return cudaSuccess;
+  if (log_n < 0 || log_n > kMaxLogN) return cudaErrorInvalidValue;
+  const uint64_t N = 1ull << log_n;
+  if (n_valid > N) n_valid = N;
+  if (log_n == 0) {
+    if (in == out) return cudaSuccess;
+    copy_cols_kernel<<<64, 256, 0, s>>>(in, out, n_cols, in_stride, out_stride, 1);
+    count_launches(1);
+    return cudaGetLastError();
+  }
+  const uint64_t ninv = inverse ? gl::inv(N) : 1;
+  PassArgs a{};
+  a.tw_lo = inverse ? t.d_inv_lo : t.d_fwd_lo;
+  a.tw_hi = inverse ? t.d_inv_hi : t.d_fwd_hi;
+  if (log_n <= 12) {
+    // one pass; the lanes are the columns
+    a.in = in;
+    a.out = out;
+    a.in_col = a.out_col = 0;
+    a.in_lane = in_stride;
+    a.in_m = 1;
+    a.out_lane = out_stride;
+    a.out_i = 1;
+    a.n_lanes = n_cols;
+    a.flat_lane = 0;  // lanes are whole columns
+    a.in_valid = n_valid;
+    a.tw_shift = -1;
+    a.scale = ninv;
+    return launch_pass_dyn(log_n, a, inverse, 1, s);
+  }
+  if (!scratch) return cudaErrorInvalidValue;
+  const int l1 = log_n / 2, l2 = log_n - l1;
+  const uint64_t N1 = 1ull << l1, N2 = 1ull << l2;
+  // pass 1: DFT_{N2} over k2 (stride N1), lanes k1; transposed store into scratch
+  a.in = in;
+  a.out = scratch;
+  a.in_col = in_stride;
+  a.out_col = N;
+  a.in_lane = 1;
+  a.in_m = N1;
+  a.out_lane = 1;
+  a.out_i = N1;
+  a.n_lanes = N1;
+  a.flat_lane = 1;  // flat index k = k2*N1 + k1
+  a.in_valid = n_valid;
+  a.tw_shift = 24 - log_n;
+  a.scale = 1;
+  cudaError_t e = launch_pass_dyn(l2, a, inverse, n_cols, s);
+  if (e != cudaSuccess) return e;
+  // pass 2: DFT_{N1} over contiguous rows, lanes i2; natural-order store
+  a.in = scratch;
+  a.out = out;
+  a.in_col = N;
+  a.out_col = out_stride;
+  a.in_lane = N1;
+  a.in_m = 1;
+  a.out_lane = 1;
+  a.out_i = N2;
+  a.n_lanes = N2;
+  a.flat_lane = N1;
+  a.in_valid = N;
+  a.tw_shift = -1;
+  a.scale = ninv;
+  return launch_pass_dyn(l1, a, inverse, n_cols, s);
+}
+
+cudaError_t scale_by_powers(const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t stride, uint64_t n,
+                            uint64_t g, cudaStream_t s) {
+  uint64_t threads = ((n + 31) / 32) * n_cols;
+  if (threads == 0) return cudaSuccess;
+  scale_powers_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(in, out, n_cols, stride, n, g);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace sg

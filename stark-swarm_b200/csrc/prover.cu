@@ -1,0 +1,367 @@
+// prover.cu — device-resident prover pipeline: LDE, merge, STIR prove.
+//
+// Data stays in HBM from the trace to the last fold. The host only drives the
+// Fiat-Shamir transcript: per STIR layer it reads back the m coset
+// evaluations and the layer root (a few hundred bytes), derives the next
+// challenges, and finally gathers the s0 query openings in one copy.
+#include <algorithm>
+#include <vector>
+
+#include "context.hpp"
+#include "gl.cuh"
+#include "merge.cuh"
+#include "merkle.cuh"
+#include "prover.hpp"
+#include "stir.cuh"
+#include "verifier.hpp"
+
+namespace sg {
+
+std::atomic<uint64_t> g_kernel_launches{0};
+
+bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static unsigned log2_exact(uint64_t n) {
+  unsigned l = 0;
+  while ((1ull << l) < n) ++l;
+  return l;
+}
+static bool pow2(uint64_t n) { return n && !(n & (n - 1)); }
+
+static void ntt(sg_ctx* c, const uint64_t* in, uint64_t* out, uint32_t cols, uint64_t in_stride, uint64_t out_stride,
+                unsigned log_n, bool inverse, uint64_t n_valid, uint64_t* scratch) {
+  cuda_check(ntt_batch(c->tw, in, out, cols, in_stride, out_stride, (int)log_n, inverse, n_valid, scratch, c->stream),
+             "ntt");
+}
+
+// ------------------------------------------------------------------ LDE
+void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
+                uint64_t* d_out) {
+  require(w > 0 && w < (1u << 31), "lde: bad column count");
+  require(pow2(n_trace), "lde: trace_len must be a power of 2");
+  require(pow2(blowup) && blowup >= 2, "lde: blowup must be a power of 2 >= 2");
+  const uint64_t n0 = n_trace * blowup;
+  require(log2_exact(n0) <= kMaxLogN, "lde: domain larger than 2^24");
+  shift %= gl::P;
+  require(shift != 0, "lde: shift must be nonzero");
+  cudaStream_t s = c->stream;
+  DBuf coef(w * n_trace, s);
+  const bool big = log2_exact(n0) > 12;
+  DBuf scratch(big ? w * n0 : 0, s);
+  ntt(c, d_trace, coef.p, (uint32_t)w, n_trace, n_trace, log2_exact(n_trace), true, n_trace, scratch.p);
+  if (shift != 1) cuda_check(scale_by_powers(coef.p, coef.p, (uint32_t)w, n_trace, n_trace, shift, s), "coset scale");
+  ntt(c, coef.p, d_out, (uint32_t)w, n_trace, n0, log2_exact(n0), false, n_trace, scratch.p);
+}
+
+// ------------------------------------------------------------------ merge
+static bool phi_live(int mode, uint64_t n) {
+  if (mode == SG_PHI_ALWAYS) return true;
+  if (mode == SG_PHI_NEVER) return false;
+  return n >= 4096;
+}
+
+void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_t n_trace, uint64_t blowup,
+                  const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c) {
+  require(air == SG_AIR_HASH_ROLLUP, "merge: unsupported AIR id");
+  require(w == 4 && k == 3, "merge: HashRollup has 4 columns and 3 constraints");
+  require(pow2(n_trace) && pow2(blowup), "merge: sizes must be powers of 2");
+  require(phi_mode >= 0 && phi_mode <= 2, "merge: bad phi mode");
+  const uint64_t n = n_trace * blowup;
+  require(log2_exact(n) <= kMaxLogN, "merge: domain larger than 2^24");
+  cudaStream_t s = c->stream;
+  if (!phi_live(phi_mode, n)) {
+    cuda_check(cudaMemsetAsync(d_c, 0, n * 8, s), "memset");
+    return;
+  }
+  DBuf phi(n, s);
+  DBuf scratch(log2_exact(n) > 12 ? n : 0, s);
+  cuda_check(hash_rollup_phi(d_lde, n, blowup, lambdas, phi.p, s), "phi");
+  ntt(c, phi.p, phi.p, 1, n, n, log2_exact(n), true, n, scratch.p);
+  cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
+  ntt(c, d_c, d_c, 1, n, n, log2_exact(n), false, n > n_trace ? n - n_trace : n, scratch.p);
+}
+
+// ------------------------------------------------------------------ STIR
+namespace {
+
+struct Tree {
+  DevTree t;
+  DBuf buf;
+  void make(uint64_t n, const std::vector<uint32_t>& ar, uint64_t label, cudaStream_t s) {
+    require(tree_plan(&t, n, ar, label), "merkle: arity schedule does not reach the root");
+    buf.alloc(t.total_digests * 4, s);
+    t.d = buf.p;
+  }
+};
+
+template <class T>
+void d2h(std::vector<T>* v, const uint64_t* src, size_t elems, cudaStream_t s) {
+  v->resize(elems * 8 / sizeof(T));
+  cuda_check(cudaMemcpyAsync(v->data(), src, elems * 8, cudaMemcpyDeviceToHost, s), "d2h");
+}
+
+Digest digest_at(const std::vector<uint64_t>& h, size_t lane0) {
+  Digest d;
+  memcpy(d.data(), h.data() + lane0, 32);
+  return d;
+}
+
+}  // namespace
+
+std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p) {
+  cudaStream_t s = c->stream;
+  const uint64_t L = p.schedule_len;
+  require(p.stir != 0, "stir_prove: only the STIR branch (params.stir = true) is implemented");
+  require(L >= 1 && L <= SG_MAX_SCHEDULE, "stir_prove: empty or oversized schedule");
+  require(pow2(n0) && n0 >= 2 && log2_exact(n0) <= kMaxLogN, "stir_prove: n0 must be a power of 2 in [2, 2^24]");
+  require(p.s0 <= (1u << 20), "stir_prove: s0 too large");
+  std::vector<uint64_t> sizes{n0};
+  for (uint64_t i = 0; i < L; ++i) {
+    const uint64_t m = p.schedule[i];
+    require(m == 2 || m == 4 || m == 8 || m == 16, "stir_prove: fold arities must be 2, 4, 8 or 16");
+    require(sizes.back() % m == 0, "stir_prove: schedule does not divide the domain");
+    sizes.push_back(sizes.back() / m);
+  }
+  const bool use_cc = p.coeff_commit_final != 0;
+
+  StirProof pr;
+  pr.n0 = n0;
+  pr.omega0 = gl::root_of_unity(log2_exact(n0));
+  HostTranscript tr("FRI/FS");
+  bind_statement(tr, p, n0);
+
+  // packed f0 tree: leaf b = {f0[b + j n0/m0]}_j (fri.rs:1420-1431), label 0xFF
+  const uint64_t m0 = p.schedule[0], nn0 = n0 / m0;
+  Tree f0t;
+  f0t.make(nn0, layer_arities(nn0, 16), 0xFF, s);
+  cuda_check(tree_hash_leaves(f0t.t, d_f0, (uint32_t)m0, nn0, 0, s), "f0 leaves");
+  cuda_check(tree_hash_levels(f0t.t, s), "f0 levels");
+  std::vector<uint64_t> h;
+  d2h(&h, f0t.t.d + 4 * f0t.t.off.back(), 4, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+  pr.root_f0 = digest_at(h, 0);
+  tr.absorb_bytes(pr.root_f0.data(), 32);
+  const gl::Fp6 z = tr.challenge_ext("z_fp3");
+
+  const uint64_t work = std::max<uint64_t>(n0, 6 * sizes[1]);
+  DBuf coef(work, s), scratch(log2_exact(n0) > 12 ? work : 0, s);
+  uint64_t part_len = 0;
+  for (uint64_t i = 0; i < L; ++i) part_len = std::max<uint64_t>(part_len, ood_partials_len(sizes[i], (int)p.schedule[i]));
+  DBuf partials(part_len, s);
+  DBuf evals(16 * 6, s);
+  std::vector<DBuf> planes(L + 1);
+  std::vector<Tree> trees(L);
+  DBuf tuples;
+  Tree ctree;
+
+  const uint64_t* cur = d_f0;
+  bool base = true;
+  gl::Fp6 zc = z;
+  for (uint64_t ell = 0; ell < L; ++ell) {
+    const uint64_t m = p.schedule[ell], n = sizes[ell], nn = n / m;
+    const unsigned lg = log2_exact(n);
+    const bool last_cc = use_cc && ell == L - 1;
+    gl::Fp6 alpha = gl::e_zero();
+    if (!last_cc) alpha = tr.challenge_ext("alpha");
+
+    // layer tree (label ell) over the 6 components of f_ell; for ell >= 1 the
+    // previous fold already wrote its leaves
+    if (ell == 0) {
+      trees[0].make(n, layer_arities(n, m), 0, s);
+      cuda_check(tree_hash_leaves(trees[0].t, d_f0, 1, n, 5, s), "layer-0 leaves");
+    }
+    cuda_check(tree_hash_levels(trees[ell].t, s), "layer levels");
+
+    // out-of-domain coset evaluation
+    const uint32_t cols = base ? 1 : 6;
+    ntt(c, cur, coef.p, cols, n, n, lg, true, n, scratch.p);
+    cuda_check(ood_evaluate(coef.p, base, n, (int)m, zc, partials.p, evals.p, s), "ood");
+
+    FoldArgs fa{};
+    fa.f = cur;
+    fa.base = base;
+    fa.n = n;
+    fa.log_n = (int)lg;
+    fa.m = (int)m;
+    fa.alpha = alpha;
+    fa.tw_inv_lo = c->tw.d_inv_lo;
+    fa.tw_inv_hi = c->tw.d_inv_hi;
+    if (!last_cc) {
+      planes[ell + 1].alloc(6 * nn, s);
+      fa.next = planes[ell + 1].p;
+      if (ell + 1 < L) {
+        trees[ell + 1].make(nn, layer_arities(nn, p.schedule[ell + 1]), ell + 1, s);
+        fa.leaves = trees[ell + 1].t.d;
+        fa.leaf_label = ell + 1;
+        fa.leaf_arity0 = trees[ell + 1].t.arity0;
+      }
+      cuda_check(stir_fold(fa, s), "fold");
+    } else {
+      tuples.alloc(6 * m * nn, s);
+      fa.tuples = tuples.p;
+      cuda_check(stir_fold(fa, s), "coefficient tuples");
+      ctree.make(nn, layer_arities(nn, 16), 0xFE, s);
+      cuda_check(tree_hash_leaves(ctree.t, tuples.p, (uint32_t)(6 * m), nn, 0, s), "coeff leaves");
+      cuda_check(tree_hash_levels(ctree.t, s), "coeff levels");
+    }
+
+    std::vector<uint64_t> ev, root, croot, tup;
+    d2h(&ev, evals.p, m * 6, s);
+    d2h(&root, trees[ell].t.d + 4 * trees[ell].t.off.back(), 4, s);
+    if (last_cc) {
+      d2h(&croot, ctree.t.d + 4 * ctree.t.off.back(), 4, s);
+      d2h(&tup, tuples.p, 6 * m * nn, s);
+    }
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    std::vector<gl::Fp6> evs(m);
+    for (uint64_t j = 0; j < m; ++j)
+      for (int q = 0; q < 6; ++q) evs[j].c[q] = ev[j * 6 + q];
+    pr.fz.push_back(evs[0]);
+    for (auto& e : evs) tr.absorb_ext(e);
+    pr.coset_evals.push_back(std::move(evs));
+    pr.roots.push_back(digest_at(root, 0));
+    tr.absorb_bytes(pr.roots.back().data(), 32);
+    zc = gl::e_pow(zc, m);
+    if (last_cc) {
+      pr.has_ct = pr.has_croot = true;
+      pr.coeff_root = digest_at(croot, 0);
+      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      alpha = tr.challenge_ext("alpha");
+      (void)tr.challenge_ext("beta_deg");
+      pr.coeff_tuples.assign(nn, std::vector<gl::Fp6>(m));
+      for (uint64_t b = 0; b < nn; ++b)
+        for (uint64_t k = 0; k < m; ++k)
+          for (int q = 0; q < 6; ++q) pr.coeff_tuples[b][k].c[q] = tup[(k * 6 + q) * nn + b];
+      planes[ell + 1].alloc(6 * nn, s);
+      cuda_check(fold_tuples(tuples.p, nn, (int)m, alpha, planes[ell + 1].p, s), "final fold");
+    }
+    cur = planes[ell + 1].p;
+    base = false;
+  }
+
+  // final polynomial coefficients (fri.rs:1915-1935)
+  const uint64_t nf = sizes[L];
+  const unsigned lgf = log2_exact(nf);
+  if (nf > 1) {
+    ntt(c, cur, coef.p, 6, nf, nf, lgf, true, nf, scratch.p);
+  } else {
+    cuda_check(cudaMemcpyAsync(coef.p, cur, 6 * 8, cudaMemcpyDeviceToDevice, s), "copy");
+  }
+  std::vector<uint64_t> fc;
+  d2h(&fc, coef.p, 6 * nf, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+  const uint64_t d_final = std::min<uint64_t>(p.d_final, nf);
+  for (uint64_t k = 0; k < d_final; ++k) {
+    gl::Fp6 e;
+    for (int q = 0; q < 6; ++q) e.c[q] = fc[q * nf + k];
+    pr.final_coeffs.push_back(e);
+    tr.absorb_ext(e);
+  }
+  const uint64_t query_seed = tr.challenge_field("query_seed");
+
+  // proximity queries (fri.rs:1813-1893): indices on the host, one gather each way
+  std::vector<uint64_t> val_idx, dig_idx0, dig_idx1;
+  std::vector<ProxQuery> qs(p.s0);
+  for (uint64_t q = 0; q < p.s0; ++q) {
+    qs[q].raw = query_index(query_seed, q, n0);
+    qs[q].base = qs[q].raw % nn0;
+    for (uint64_t j = 0; j < m0; ++j) {
+      qs[q].fib_idx.push_back(qs[q].base + j * nn0);
+      val_idx.push_back(qs[q].base + j * nn0);
+    }
+    opening_indices(f0t.t, qs[q].base, &dig_idx0);
+    if (L >= 2) opening_indices(trees[1].t, qs[q].base, &dig_idx1);
+  }
+  const size_t nv = val_idx.size(), nd0 = dig_idx0.size(), nd1 = dig_idx1.size();
+  const size_t n_next = L >= 2 ? 6 * p.s0 : 0;
+  std::vector<uint64_t> idx_all;
+  idx_all.insert(idx_all.end(), val_idx.begin(), val_idx.end());
+  idx_all.insert(idx_all.end(), dig_idx0.begin(), dig_idx0.end());
+  idx_all.insert(idx_all.end(), dig_idx1.begin(), dig_idx1.end());
+  for (uint64_t q = 0; q < (L >= 2 ? p.s0 : 0); ++q)
+    for (int k = 0; k < 6; ++k) idx_all.push_back((uint64_t)k * sizes[1] + qs[q].base);
+  DBuf d_idx(idx_all.size(), s), d_out(nv + 4 * (nd0 + nd1) + n_next, s);
+  if (!idx_all.empty()) {
+    cuda_check(cudaMemcpyAsync(d_idx.p, idx_all.data(), idx_all.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(gather_u64(d_f0, d_idx.p, nv, d_out.p, s), "gather values");
+    cuda_check(gather_digests(f0t.t.d, d_idx.p + nv, nd0, d_out.p + nv, s), "gather f0 paths");
+    if (L >= 2) {
+      cuda_check(gather_digests(trees[1].t.d, d_idx.p + nv + nd0, nd1, d_out.p + nv + 4 * nd0, s), "gather l1");
+      cuda_check(gather_u64(planes[1].p, d_idx.p + nv + nd0 + nd1, n_next, d_out.p + nv + 4 * (nd0 + nd1), s),
+                 "gather f1");
+    }
+  }
+  std::vector<uint64_t> got;
+  d2h(&got, d_out.p, d_out.n, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+
+  size_t pv = 0, p0 = nv, p1 = nv + 4 * nd0, pn = nv + 4 * (nd0 + nd1);
+  auto take_opening = [&](const DevTree& t, uint64_t index, size_t* pos) {
+    Opening o;
+    o.index = index;
+    o.leaf = digest_at(got, *pos);
+    *pos += 4;
+    for (size_t l = 0; l + 1 < t.len.size(); ++l) {
+      std::vector<Digest> sib(t.arity[l] - 1);
+      for (auto& d : sib) {
+        d = digest_at(got, *pos);
+        *pos += 4;
+      }
+      o.path.push_back(std::move(sib));
+    }
+    return o;
+  };
+  for (uint64_t q = 0; q < p.s0; ++q) {
+    for (uint64_t j = 0; j < m0; ++j) qs[q].fib_vals.push_back(got[pv++]);
+    qs[q].f0_open = take_opening(f0t.t, qs[q].base, &p0);
+    qs[q].has_l1 = L >= 2;
+    if (L >= 2) {
+      qs[q].l1_open = take_opening(trees[1].t, qs[q].base, &p1);
+      for (int k = 0; k < 6; ++k) qs[q].f_next.c[k] = got[pn++];
+    }
+  }
+  pr.prox = std::move(qs);
+  return encode_proof(pr);
+}
+
+// ------------------------------------------------------------------ HashRollup pipeline
+std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* leaves, uint64_t n_leaves,
+                                                   const uint8_t pi[32], int phi_mode, bool self_verify) {
+  uint64_t n_trace = 8;
+  while (n_trace < n_leaves) n_trace <<= 1;
+  const uint64_t blowup = 32, n0 = n_trace * blowup;
+  require(log2_exact(n0) <= kMaxLogN, "prove_hash_rollup: too many leaves");
+  // build_hash_rollup_trace (air_workloads.rs:571-589): a sequential recurrence, built on the host
+  std::vector<uint64_t> trace(4 * n_trace);
+  uint64_t st = 0;
+  for (uint64_t i = 0; i < n_trace; ++i) {
+    const uint64_t leaf = i < n_leaves ? leaves[i] % gl::P : 0;
+    const uint64_t sq = gl::mul(st, st);
+    trace[i] = i % gl::P;
+    trace[n_trace + i] = leaf;
+    trace[2 * n_trace + i] = st;
+    trace[3 * n_trace + i] = sq;
+    st = gl::add(sq, leaf);
+  }
+  cudaStream_t s = c->stream;
+  DBuf d_trace(4 * n_trace, s), d_lde(4 * n0, s), d_c(n0, s);
+  cuda_check(cudaMemcpyAsync(d_trace.p, trace.data(), trace.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+  lde_device(c, d_trace.p, 4, n_trace, blowup, 1, d_lde.p);
+  const uint64_t lam[3] = {1, 2, 3};  // comb_coeffs (prover.rs:100-102)
+  merge_device(c, SG_AIR_HASH_ROLLUP, d_lde.p, 4, n_trace, blowup, lam, 3, phi_mode, d_c.p);
+  sg_fri_params p;
+  sg_build_params(n0, pi, 1, &p);
+  std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
+  if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
+    throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
+  return proof;
+}
+
+}  // namespace sg

@@ -1,0 +1,19 @@
+// prover.hpp — device pipeline entry points used by the C ABI.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "context.hpp"
+#include "protocol.hpp"
+
+namespace sg {
+
+void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
+                uint64_t* d_out);
+void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_t n_trace, uint64_t blowup,
+                  const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c);
+std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p);
+std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* leaves, uint64_t n_leaves,
+                                                   const uint8_t pi[32], int phi_mode, bool self_verify);
+
+}  // namespace sg

@@ -1,0 +1,258 @@
+// stir.cu — STIR out-of-domain evaluation and fold kernels.
+#include "dft.cuh"
+#include "keccak.cuh"
+#include "stir.cuh"
+#include "counters.hpp"
+
+namespace sg {
+namespace {
+
+constexpr int kOodThreads = 256;
+constexpr uint64_t kOodGroupsPerThread = 16;
+
+__device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = gl::add(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+inline uint64_t ood_blocks(uint64_t n, int m) {
+  uint64_t groups = n / m;
+  uint64_t threads = (groups + kOodGroupsPerThread - 1) / kOodGroupsPerThread;
+  uint64_t b = (threads + kOodThreads - 1) / kOodThreads;
+  return b ? b : 1;
+}
+
+// Thread tid accumulates T_r over groups t = tid, tid + S, ... (S = all threads),
+// starting from w^tid and stepping by w^S: consecutive threads read consecutive
+// groups of M coefficients.
+template <int M, bool BASE>
+__global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t* c, uint64_t n, gl::Fp6 w,
+                                                                   gl::Fp6 w_stride, uint64_t* partials) {
+  const uint64_t n_groups = n / M;
+  const uint64_t S = (uint64_t)gridDim.x * kOodThreads;
+  const uint64_t tid = (uint64_t)blockIdx.x * kOodThreads + threadIdx.x;
+  __shared__ gl::Fp6 blk_start;
+  if (threadIdx.x == 0) blk_start = gl::e_pow(w, (uint64_t)blockIdx.x * kOodThreads);
+  __syncthreads();
+  gl::Fp6 wt = gl::e_mul(blk_start, gl::e_pow(w, threadIdx.x));
+  uint64_t acc[M][6];
+#pragma unroll
+  for (int r = 0; r < M; ++r)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[r][q] = 0;
+  for (uint64_t t = tid; t < n_groups; t += S) {
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+      const uint64_t k = t * M + r;
+      if constexpr (BASE) {
+        const uint64_t ck = __ldg(c + k);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc[r][q] = gl::add(acc[r][q], gl::mul(wt.c[q], ck));
+      } else {
+        gl::Fp6 ck;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) ck.c[q] = __ldg(c + (uint64_t)q * n + k);
+        gl::Fp6 p = gl::e_mul(ck, wt);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) acc[r][q] = gl::add(acc[r][q], p.c[q]);
+      }
+    }
+    wt = gl::e_mul(wt, w_stride);
+  }
+  __shared__ uint64_t red[kOodThreads / 32][M * 6];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = 0; r < M; ++r)
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      uint64_t v = warp_sum(acc[r][q]);
+      if (lane == 0) red[warp][r * 6 + q] = v;
+    }
+  __syncthreads();
+  if (threadIdx.x < M * 6) {
+    uint64_t v = 0;
+#pragma unroll
+    for (int wi = 0; wi < kOodThreads / 32; ++wi) v = gl::add(v, red[wi][threadIdx.x]);
+    partials[(uint64_t)blockIdx.x * M * 6 + threadIdx.x] = v;
+  }
+}
+
+// Sum block partials into T_r, then evals[j] = sum_r w_M^{jr} z^r T_r.
+template <int M>
+__global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, gl::Fp6 z, uint64_t* evals) {
+  __shared__ uint64_t T[M * 6];
+  for (int e = threadIdx.x; e < M * 6; e += blockDim.x) {
+    uint64_t v = 0;
+    for (uint64_t b = 0; b < n_blocks; ++b) v = gl::add(v, partials[b * M * 6 + e]);
+    T[e] = v;
+  }
+  __syncthreads();
+  const int j = threadIdx.x;
+  if (j >= M) return;
+  constexpr unsigned EM = (exp16(false) * (16 / M)) % 192;  // w_M = 2^EM
+  gl::Fp6 acc = gl::e_zero(), zr = gl::e_one();
+  for (int r = 0; r < M; ++r) {
+    gl::Fp6 tr;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) tr.c[q] = T[r * 6 + q];
+    gl::Fp6 s = gl::e_mul(zr, tr);
+    const unsigned e = (EM * (unsigned)((j * r) % M)) % 192u;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) s.c[q] = gl::mul_pow2(s.c[q], e);
+    acc = gl::e_add(acc, s);
+    zr = gl::e_mul(zr, z);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) evals[j * 6 + q] = acc.c[q];
+}
+
+template <int M, bool BASE>
+__global__ void fold_kernel(FoldArgs a) {
+  constexpr int LM = M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : 4;
+  const uint64_t nn = a.n / M;
+  const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (b >= nn) return;
+  constexpr int NC = BASE ? 1 : 6;
+  uint64_t x[NC][M];
+#pragma unroll
+  for (int q = 0; q < NC; ++q) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) x[q][j] = __ldg(a.f + (uint64_t)q * a.n + b + (uint64_t)j * nn);
+    dft_reg<M, true>(x[q]);
+  }
+  // w_n^{-b}
+  const uint64_t E = (b << (24 - a.log_n)) & ((1ull << 24) - 1);
+  const uint64_t obinv = gl::mul(__ldg(a.tw_inv_lo + (E & 4095)), __ldg(a.tw_inv_hi + (E >> 12)));
+  constexpr unsigned MINV = 192u - LM;  // 1/M = 2^{-LM} = 2^{192-LM}
+  if (a.tuples) {
+    uint64_t p = 1;
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        uint64_t v = q < NC ? gl::mul(gl::mul_pow2(x[q][k], MINV), p) : 0;
+        a.tuples[(uint64_t)(k * 6 + q) * nn + b] = v;
+      }
+      p = gl::mul(p, obinv);
+    }
+  }
+  if (!a.next) return;
+  const gl::Fp6 beta = gl::e_scale(a.alpha, obinv);
+  gl::Fp6 acc;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) acc.c[q] = q < NC ? x[q][M - 1] : 0;
+#pragma unroll
+  for (int k = M - 2; k >= 0; --k) {
+    acc = gl::e_mul(acc, beta);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) acc.c[q] = gl::add(acc.c[q], x[q][k]);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    acc.c[q] = gl::mul_pow2(acc.c[q], MINV);
+    a.next[(uint64_t)q * nn + b] = acc.c[q];
+  }
+  if (a.leaves) {
+    kc::LaneSponge sp;
+    sp.init();
+    sp.lane(a.leaf_arity0);
+    sp.lane(0xFFFFFFFFull);
+    sp.lane(b);
+    sp.lane(a.leaf_label);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sp.lane(acc.c[q]);
+    uint64_t d[4];
+    sp.finish(d);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a.leaves[4 * b + i] = d[i];
+  }
+}
+
+template <int M>
+__global__ void fold_tuples_kernel(const uint64_t* tup, uint64_t nf, gl::Fp6 alpha, uint64_t* next) {
+  const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (b >= nf) return;
+  gl::Fp6 acc;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) acc.c[q] = tup[(uint64_t)((M - 1) * 6 + q) * nf + b];
+#pragma unroll
+  for (int k = M - 2; k >= 0; --k) {
+    acc = gl::e_mul(acc, alpha);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc.c[q] = gl::add(acc.c[q], tup[(uint64_t)(k * 6 + q) * nf + b]);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) next[(uint64_t)q * nf + b] = acc.c[q];
+}
+
+template <int M>
+cudaError_t ood_launch(const uint64_t* c, bool base, uint64_t n, const gl::Fp6& z, uint64_t* partials,
+                       uint64_t* evals, cudaStream_t s) {
+  const uint64_t blocks = ood_blocks(n, M);
+  const gl::Fp6 w = gl::e_pow(z, M);
+  const gl::Fp6 ws = gl::e_pow(w, blocks * kOodThreads);
+  if (base)
+    ood_partial_kernel<M, true><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
+  else
+    ood_partial_kernel<M, false><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
+  ood_finish_kernel<M><<<1, 128, 0, s>>>(partials, blocks, z, evals);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t fold_launch(const FoldArgs& a, cudaStream_t s) {
+  const uint64_t nn = a.n / M;
+  const unsigned T = 128;
+  const unsigned blocks = (unsigned)((nn + T - 1) / T);
+  if (a.base)
+    fold_kernel<M, true><<<blocks, T, 0, s>>>(a);
+  else
+    fold_kernel<M, false><<<blocks, T, 0, s>>>(a);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+uint64_t ood_partials_len(uint64_t n, int m) { return ood_blocks(n, m) * (uint64_t)m * 6; }
+
+cudaError_t ood_evaluate(const uint64_t* coeffs, bool base, uint64_t n, int m, const gl::Fp6& z,
+                         uint64_t* partials, uint64_t* evals, cudaStream_t s) {
+  if (n % m) return cudaErrorInvalidValue;
+  switch (m) {
+    case 2: return ood_launch<2>(coeffs, base, n, z, partials, evals, s);
+    case 4: return ood_launch<4>(coeffs, base, n, z, partials, evals, s);
+    case 8: return ood_launch<8>(coeffs, base, n, z, partials, evals, s);
+    case 16: return ood_launch<16>(coeffs, base, n, z, partials, evals, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t stir_fold(const FoldArgs& a, cudaStream_t s) {
+  if (a.n % a.m || a.log_n > 24) return cudaErrorInvalidValue;
+  switch (a.m) {
+    case 2: return fold_launch<2>(a, s);
+    case 4: return fold_launch<4>(a, s);
+    case 8: return fold_launch<8>(a, s);
+    case 16: return fold_launch<16>(a, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t fold_tuples(const uint64_t* tuples, uint64_t n_final, int m, const gl::Fp6& alpha, uint64_t* next,
+                        cudaStream_t s) {
+  const unsigned blocks = (unsigned)((n_final + 127) / 128);
+  switch (m) {
+    case 2: fold_tuples_kernel<2><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
+    case 4: fold_tuples_kernel<4><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
+    case 8: fold_tuples_kernel<8><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
+    case 16: fold_tuples_kernel<16><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
+    default: return cudaErrorInvalidValue;
+  }
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace sg

@@ -1,3 +1,4 @@
+import importlib
 import json
 import os
 import sys
@@ -20,3 +21,20 @@ def pytest_configure(config):
 def golden():
     with open(os.path.join(HERE, "golden", "golden_proofs.json")) as f:
         return json.load(f)
+
+
+def load_sgpu():
+    """The product package (its directory name is not a Python identifier)."""
+    return importlib.import_module("stark-swarm_b200")
+
+
+@pytest.fixture(scope="session")
+def sgpu():
+    return load_sgpu()
+
+
+@pytest.fixture(scope="session")
+def ctx(sgpu):
+    c = sgpu.Context(0)
+    yield c
+    c.close()

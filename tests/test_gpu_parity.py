@@ -1,0 +1,261 @@
+"""GPU path vs the CPU oracle, through the C ABI (libstarkgpu.so).
+
+Bit-exact equality everywhere: every value is an exact Goldilocks / Fp6
+element and every proof byte must match. Sizes the oracle finishes in
+seconds are compared directly; the full 2^23 domain is checked through
+size-independent properties (inverse round trip, linearity, agreement with the
+oracle at sampled points) and by full-proof self-verification.
+"""
+import hashlib
+import struct
+
+import numpy as np
+import pytest
+
+import dnszone
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+P = O.P
+
+
+def rand_field(rng, shape):
+    return rng.integers(0, P, size=shape, dtype=np.uint64)
+
+
+@pytest.mark.parametrize("log_n", list(range(0, 17)))
+@pytest.mark.parametrize("inverse", [False, True])
+def test_ntt_matches_oracle(ctx, log_n, inverse):
+    rng = np.random.default_rng(100 + log_n)
+    cols = 3 if log_n <= 14 else 1
+    x = rand_field(rng, (cols, 1 << log_n))
+    got = ctx.ntt(x, log_n, inverse)
+    for c in range(cols):
+        assert np.array_equal(got[c], O.ntt(x[c], inverse)), c
+
+
+@pytest.mark.parametrize("log_n", [17, 20, 23, 24])
+def test_ntt_large_round_trip_and_oracle(ctx, log_n):
+    rng = np.random.default_rng(log_n)
+    x = rand_field(rng, (1, 1 << log_n))
+    y = ctx.ntt(x, log_n, False)
+    if log_n <= 20:
+        assert np.array_equal(y[0], O.ntt(x[0]))
+    assert np.array_equal(ctx.ntt(y, log_n, True), x)
+    # a sparse input (first 512 entries) makes the defining sum cheap on the CPU
+    sp = np.zeros_like(x)
+    sp[0, :512] = x[0, :512]
+    ys = ctx.ntt(sp, log_n, False)
+    w = int(O.lib().orc_root_of_unity(log_n))
+    xs = [int(v) for v in sp[0, :512]]
+    for i in (0, 1, 3, 4097, (1 << log_n) - 1):
+        wi = pow(w, i, P)
+        acc, p = 0, 1
+        for v in xs:
+            acc = (acc + v * p) % P
+            p = p * wi % P
+        assert int(ys[0, i]) == acc, i
+
+
+def test_ntt_linearity_at_2p23(ctx):
+    rng = np.random.default_rng(7)
+    n = 1 << 23
+    a, b = rand_field(rng, (1, n)), rand_field(rng, (1, n))
+    s = ((a.astype(object) + b.astype(object)) % P).astype(np.uint64)
+    fa, fb, fs = ctx.ntt(a, 23), ctx.ntt(b, 23), ctx.ntt(s, 23)
+    assert np.array_equal(fs, ((fa.astype(object) + fb.astype(object)) % P).astype(np.uint64))
+
+
+@pytest.mark.parametrize("w,log_n,blowup,shift", [
+    (3, 3, 4, 1), (4, 7, 32, 1), (4, 12, 32, 1), (5, 10, 8, 7), (2, 16, 8, 7), (1, 1, 2, 1), (3, 13, 2, 3),
+])
+def test_lde_matches_oracle(ctx, w, log_n, blowup, shift):
+    rng = np.random.default_rng(w * 100 + log_n)
+    tr = rand_field(rng, (w, 1 << log_n))
+    assert np.array_equal(ctx.lde(tr, blowup, shift), O.lde(tr, blowup, shift))
+
+
+def test_lde_reference_signature_and_errors(ctx):
+    cols = [[i * 3 + c for i in range(8)] for c in range(2)]
+    got = ctx.lde_trace_columns(cols, 8, 4)
+    assert len(got) == 2 and len(got[0]) == 32
+    assert np.array_equal(np.array(got), O.lde(np.array(cols, dtype=np.uint64), 4))
+    with pytest.raises(ValueError):
+        ctx.lde_trace_columns([], 8, 4)
+    with pytest.raises(ValueError):
+        ctx.lde_trace_columns(cols, 8, 3)
+    with pytest.raises(ValueError):
+        ctx.lde_trace_columns([[1] * 6], 6, 4)
+
+
+def test_lde_device_pointers(ctx):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(5)
+    tr = rand_field(rng, (4, 1 << 14))
+    d_in = torch.from_numpy(tr.view(np.int64)).cuda()
+    d_out = torch.empty((4, 1 << 17), dtype=torch.int64, device="cuda")
+    ctx.lde(d_in, 8, 1, out=d_out)
+    torch.cuda.synchronize()
+    got = d_out.cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, O.lde(tr, 8, 1))
+
+
+@pytest.mark.parametrize("log_nt,blowup,mode", [
+    (3, 32, O.PHI_PARALLEL_GATE), (4, 32, O.PHI_ALWAYS), (7, 32, O.PHI_PARALLEL_GATE), (12, 32, O.PHI_PARALLEL_GATE),
+    (10, 4, O.PHI_ALWAYS), (9, 8, O.PHI_NEVER),
+])
+def test_merge_hash_rollup_matches_oracle(ctx, log_nt, blowup, mode):
+    rng = np.random.default_rng(log_nt)
+    n_trace = 1 << log_nt
+    leaves = rand_field(rng, n_trace)
+    tr = O.hash_rollup_trace(leaves, n_trace)
+    lde = O.lde(tr, blowup)
+    want = O.merge(O.AIR_HASH_ROLLUP, lde, n_trace, blowup, [1, 2, 3], mode)
+    got = ctx.merge(4, lde, n_trace, blowup, [1, 2, 3], mode)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("n,width,arities,label", [
+    (1, 6, [2], 0xFE), (5, 3, [2, 2, 2], 7), (16, 8, [16], 0xFF), (100, 4, [8, 8, 8], 1), (37, 2, [4, 4, 4], 0),
+    (4096, 6, [8, 8, 8, 8], 2), (1 << 14, 64, [16, 16, 16, 16], 0), (1000, 12, [4] * 5, 9),
+])
+def test_merkle_commit_matches_oracle(ctx, n, width, arities, label):
+    rng = np.random.default_rng(n + width)
+    rows = rand_field(rng, (n, width))
+    cols = np.ascontiguousarray(rows.T)
+    assert ctx.merkle_commit(cols, arities, label) == O.merkle_root(rows, arities, label)
+
+
+def test_merkle_open_verifies(ctx):
+    rng = np.random.default_rng(3)
+    n, width, ar = 1000, 6, [8, 8, 8, 8]
+    cols = rand_field(rng, (width, n))
+    root, tree = ctx.merkle_commit(cols, ar, 5, keep=True)
+    for idx in (0, 1, 511, 999):
+        blob = tree.open(idx)
+        leaf = hashlib.sha3_256(struct.pack("<4Q", ar[0], 0xFFFFFFFF, idx, 5) +
+                                struct.pack(f"<{width}Q", *map(int, cols[:, idx]))).digest()
+        assert blob[:32] == leaf
+        # decode: leaf, path, index
+        off = 32
+        nl = int.from_bytes(blob[off:off + 8], "little"); off += 8
+        path = []
+        for _ in range(nl):
+            ns = int.from_bytes(blob[off:off + 8], "little"); off += 8
+            path.append([blob[off + 32 * k: off + 32 * (k + 1)] for k in range(ns)]); off += 32 * ns
+        assert int.from_bytes(blob[off:off + 8], "little") == idx
+        # recompute the root from the opening
+        cur, i = blob[:32], idx
+        for lv, sib in enumerate(path):
+            a = ar[lv]
+            ch, k = [], 0
+            for j in range(a):
+                if j == i % a:
+                    ch.append(cur)
+                else:
+                    ch.append(sib[k]); k += 1
+            ds = (a).to_bytes(8, "little") + (lv + 1).to_bytes(8, "little") + (i // a).to_bytes(8, "little") + (5).to_bytes(8, "little")
+            cur = hashlib.sha3_256(ds + b"".join(ch)).digest()
+            i //= a
+        assert cur == root
+    tree.free()
+
+
+def _rand_params(sg, n0, pi, sched=None, cc=True):
+    if sched is None:
+        return sg.build_params(n0, pi), O.build_params(n0, pi)
+    po = O.build_params(n0, pi)
+    po.schedule_len = len(sched)
+    for i, m in enumerate(sched):
+        po.schedule[i] = m
+    po.coeff_commit_final = int(cc)
+    ps = sg.FriParams.new(sched, coeff_commit_final=cc, public_inputs_hash=pi)
+    return ps, po
+
+
+@pytest.mark.parametrize("log_n0", [3, 4, 5, 6, 9, 12, 13, 15, 17])
+def test_stir_prove_matches_oracle_bytes(sgpu, ctx, log_n0):
+    rng = np.random.default_rng(log_n0)
+    n0 = 1 << log_n0
+    f0 = rand_field(rng, n0)
+    pi = rng.bytes(32)
+    ps, po = _rand_params(sgpu, n0, pi)
+    got = ctx.deep_fri_prove(f0, sgpu.FriDomain(n0), ps)
+    want = O.stir_prove(f0, po)
+    assert got == want
+
+
+@pytest.mark.parametrize("sched,cc", [([4, 2, 8], True), ([2, 2, 2, 2], False), ([16, 4], True), ([8], True),
+                                      ([8], False), ([2], True)])
+def test_stir_prove_other_schedules_match_oracle(sgpu, ctx, sched, cc):
+    rng = np.random.default_rng(len(sched))
+    n0 = 4
+    for m in sched:
+        n0 *= m
+    f0 = rand_field(rng, n0)
+    pi = rng.bytes(32)
+    ps, po = _rand_params(sgpu, n0, pi, sched, cc)
+    assert ctx.deep_fri_prove(f0, n0, ps) == O.stir_prove(f0, po)
+
+
+def test_stir_prove_rejects_bad_arguments(sgpu, ctx):
+    f0 = np.zeros(64, dtype=np.uint64)
+    with pytest.raises(sgpu.StarkGpuError):
+        ctx.deep_fri_prove(f0, 64, sgpu.FriParams.new([3, 2]))
+    with pytest.raises(sgpu.StarkGpuError):
+        ctx.deep_fri_prove(f0, 64, sgpu.FriParams.new([8, 8, 8]))
+    with pytest.raises(sgpu.StarkGpuError):
+        ctx.deep_fri_prove(f0, 64, sgpu.FriParams.new([8, 8], stir=False))
+    with pytest.raises(sgpu.StarkGpuError):
+        ctx.deep_fri_prove(f0[:48], 48, sgpu.FriParams.new([8, 2]))
+
+
+def test_golden_outer_rollup_on_gpu(ctx, golden):
+    leaves, pk = dnszone.outer_rollup_inputs(golden)
+    proof = ctx.prove_hash_rollup(leaves, pk)
+    e = golden["outer"]
+    assert len(proof) == e["len"]
+    assert hashlib.sha3_256(proof).hexdigest() == e["sha3_256"]
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_golden_inner_shards_on_gpu(ctx, golden, idx):
+    sh = golden["shards"][idx]
+    leaves, fsb, root, count = dnszone.inner_shard_inputs(golden, sh)
+    proof = ctx.prove_hash_rollup(leaves, fsb)
+    assert len(proof) == sh["len"]
+    assert hashlib.sha3_256(proof).hexdigest() == sh["sha3_256"]
+    pi = dnszone.shard_pi_hash(bytes.fromhex(golden["zone_salt_hex"]), count, root, proof[:32], fsb)
+    assert pi.hex() == sh["pi_hash_hex"]
+
+
+@pytest.mark.parametrize("n_leaves,mode", [(0, 0), (1, 0), (12, 1), (100, 0), (5000, 0), (5000, 2)])
+def test_prove_hash_rollup_edge_sizes(ctx, n_leaves, mode):
+    rng = np.random.default_rng(n_leaves)
+    leaves = rand_field(rng, n_leaves)
+    pi = rng.bytes(32)
+    assert ctx.prove_hash_rollup(leaves, pi, mode) == O.prove_hash_rollup(leaves, pi, mode)
+
+
+def test_full_size_stir_self_verifies(sgpu, ctx):
+    # the 2^23 domain of the benchmark workload: too slow for the scalar oracle,
+    # so check acceptance by the verifier and the OOD values against Horner on
+    # the CPU for a low-degree f0
+    n0 = 1 << 23
+    rng = np.random.default_rng(23)
+    coeffs = rand_field(rng, 1)
+    f0 = np.full(n0, coeffs[0], dtype=np.uint64)  # constant polynomial: degree 0 < d_final
+    pi = rng.bytes(32)
+    proof = ctx.deep_fri_prove(f0, n0, sgpu.build_params(n0, pi))
+    assert sgpu.deep_fri_verify(sgpu.build_params(n0, pi), proof)
+    assert O.stir_verify(proof, O.build_params(n0, pi))
+
+
+def test_full_size_stir_random_f0_consistent(sgpu, ctx):
+    # random f0 at 2^20: not low degree, so only the prover's own values can be
+    # checked; compare bytes with the oracle (multi-threaded, a few seconds)
+    n0 = 1 << 20
+    rng = np.random.default_rng(20)
+    f0 = rand_field(rng, n0)
+    pi = rng.bytes(32)
+    assert ctx.deep_fri_prove(f0, n0, sgpu.build_params(n0, pi)) == O.stir_prove(f0, O.build_params(n0, pi))

@@ -1,0 +1,99 @@
+"""CPU-side checks of the GPU library: it loads, exports the declared C ABI,
+and its host-only parts (parameter builder, STIR verifier) agree with the
+oracle. No kernel is launched here."""
+import ctypes
+import os
+import random
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import dnszone
+import oracle_lib as O
+from conftest import ROOT, load_sgpu
+
+HEADER = os.path.join(ROOT, "include", "stark_gpu.h")
+
+
+def _declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(sg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    sg = load_sgpu()
+    if not os.path.exists(sg.LIB_PATH):
+        subprocess.run(["make", "-s", "-C", os.path.dirname(sg.LIB_PATH)], check=True)
+    L = sg.lib()
+    declared = _declared_functions()
+    assert declared, "no declarations parsed"
+    assert sorted(sg.EXPORTS) == declared
+    for name in declared:
+        assert getattr(L, name) is not None
+    nm = subprocess.run(["nm", "-D", "--defined-only", sg.LIB_PATH], capture_output=True, text=True).stdout
+    for name in declared:
+        assert re.search(rf"\bT {name}\b", nm), name
+
+
+@pytest.mark.parametrize("n0", [8, 16, 512, 4096, 1 << 17, 1 << 23])
+def test_build_params_matches_reference_recipe(n0):
+    sg = load_sgpu()
+    pi = bytes(range(32))
+    a = sg.build_params(n0, pi)
+    b = O.build_params(n0, pi)
+    assert a.schedule_list == b.sched == sg.make_schedule(n0)
+    for f in ("r", "s0", "seed_z", "d_final", "coeff_commit_final", "stir", "has_pi"):
+        assert getattr(a, f) == getattr(b, f), f
+    assert bytes(a.pi_hash) == pi
+
+
+def test_verifier_accepts_golden_outer_and_rejects_tampering(golden):
+    sg = load_sgpu()
+    leaves, pk = dnszone.outer_rollup_inputs(golden)
+    proof = O.prove_hash_rollup(leaves, pk)
+    params = sg.build_params(512, pk)
+    assert sg.deep_fri_verify(params, proof)
+    rng = random.Random(11)
+    for _ in range(30):
+        i = rng.randrange(len(proof))
+        bad = bytearray(proof)
+        bad[i] ^= 1 << rng.randrange(8)
+        assert not sg.deep_fri_verify(params, bytes(bad)), i
+    assert not sg.deep_fri_verify(sg.build_params(512, bytes(32)), proof)
+    assert not sg.deep_fri_verify(params, proof[:-1])
+    assert not sg.deep_fri_verify(params, proof + b"\0")
+
+
+def test_verifier_accepts_golden_inner_shard(golden):
+    sg = load_sgpu()
+    sh = golden["shards"][0]
+    leaves, fsb, _root, _count = dnszone.inner_shard_inputs(golden, sh)
+    proof = O.prove_hash_rollup(leaves, fsb)
+    assert sg.deep_fri_verify(sg.build_params(sh["n0"], fsb), proof)
+
+
+@pytest.mark.parametrize("sched,cc", [([4, 2, 8], True), ([2, 2, 2, 2, 2, 2], False), ([16, 4], True)])
+def test_verifier_agrees_with_oracle_on_other_schedules(sched, cc):
+    sg = load_sgpu()
+    n0 = 1
+    for m in sched:
+        n0 *= m
+    n0 *= 4
+    pi = os.urandom(32)
+    p_o = O.build_params(n0, pi)
+    p_o.schedule_len = len(sched)
+    for i, m in enumerate(sched):
+        p_o.schedule[i] = m
+    p_o.coeff_commit_final = int(cc)
+    p_o.d_final = 4
+    p_s = sg.FriParams.new(sched, coeff_commit_final=cc, d_final=4, public_inputs_hash=pi)
+    # f0 of degree < 4 so the final-polynomial check holds for these schedules
+    xs = [pow(int(sg.FriDomain(n0).omega), i, O.P) for i in range(n0)]
+    c = [random.randrange(O.P) for _ in range(4)]
+    f0 = np.array([sum(ci * pow(x, k, O.P) for k, ci in enumerate(c)) % O.P for x in xs], dtype=np.uint64)
+    proof = O.stir_prove(f0, p_o)
+    assert O.stir_verify(proof, p_o)
+    assert sg.deep_fri_verify(p_s, proof)
