@@ -67,8 +67,21 @@ void sg_ctx_destroy(sg_ctx* ctx);
 /* Use an existing cudaStream_t (passed as void*) for all later calls; NULL = the context's own stream. */
 int sg_ctx_set_stream(sg_ctx* ctx, void* cuda_stream);
 const char* sg_last_error(const sg_ctx* ctx);
-/* Number of kernels this context has launched since creation (instrumentation). */
+/* Number of kernels this library has launched in this process (instrumentation). */
 uint64_t sg_kernel_launches(const sg_ctx* ctx);
+
+/* Per-kernel-family timing (instrumentation, no reference counterpart): while
+ * enabled, every launch is bracketed by a CUDA event pair on its own stream.
+ * sg_profile_read waits for the pending events and reports, per family, the
+ * number of launches and the summed device time since the last reset. */
+typedef struct {
+  char name[48];
+  uint64_t launches;
+  double total_ms;
+} sg_profile_entry;
+int sg_profile_enable(int on);
+int sg_profile_read(sg_profile_entry* out, size_t cap, size_t* n);
+void sg_profile_reset(void);
 
 /* Batched NTT with ark-poly Radix2EvaluationDomain semantics: forward = evaluations
  * at w^0..w^{n-1} (natural order), inverse includes 1/n; w = 7^((p-1)/2^32)

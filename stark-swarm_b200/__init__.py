@@ -87,9 +87,14 @@ DeepFriParams = FriParams
 _U64P = ctypes.POINTER(ctypes.c_uint64)
 _lib = None
 
+class ProfileEntry(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_uint64), ("total_ms", ctypes.c_double)]
+
+
 # Every symbol declared in include/stark_gpu.h.
 EXPORTS = (
-    "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_last_error", "sg_kernel_launches", "sg_ntt",
+    "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_last_error", "sg_kernel_launches",
+    "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt",
     "sg_lde", "sg_merge", "sg_merkle_commit", "sg_merkle_open", "sg_merkle_free", "sg_build_params",
     "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
 )
@@ -112,6 +117,10 @@ def lib():
     L.sg_last_error.restype = ctypes.c_char_p
     L.sg_kernel_launches.argtypes = [vp]
     L.sg_kernel_launches.restype = u64
+    L.sg_profile_enable.argtypes = [i32]
+    L.sg_profile_read.argtypes = [ctypes.POINTER(ProfileEntry), sz, ctypes.POINTER(sz)]
+    L.sg_profile_reset.argtypes = []
+    L.sg_profile_reset.restype = None
     L.sg_ntt.argtypes = [vp, vp, vp, sz, sz, i32]
     L.sg_lde.argtypes = [vp, vp, sz, sz, sz, u64, vp]
     L.sg_merge.argtypes = [vp, i32, vp, sz, sz, sz, vp, sz, i32, vp]
@@ -165,6 +174,22 @@ def build_params(n0: int, pk_hash_32: bytes = None, stir: bool = True) -> FriPar
     p = FriParams()
     lib().sg_build_params(n0, pk_hash_32, int(stir), ctypes.byref(p))
     return p
+
+
+def profile_enable(on: bool = True):
+    lib().sg_profile_enable(int(on))
+
+
+def profile_reset():
+    lib().sg_profile_reset()
+
+
+def profile_read():
+    """{kernel family: (launches, total device ms)} since the last reset."""
+    arr = (ProfileEntry * 64)()
+    n = ctypes.c_size_t()
+    lib().sg_profile_read(arr, 64, ctypes.byref(n))
+    return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(min(n.value, 64))}
 
 
 def deep_fri_verify(params: FriParams, proof: bytes) -> bool:

@@ -127,6 +127,25 @@ const char* sg_last_error(const sg_ctx* c) { return c ? c->err.c_str() : "null c
 
 uint64_t sg_kernel_launches(const sg_ctx*) { return sg::g_kernel_launches.load(); }
 
+int sg_profile_enable(int on) {
+  sg::Profiler::get().enable(on != 0);
+  return SG_OK;
+}
+
+int sg_profile_read(sg_profile_entry* out, size_t cap, size_t* n) {
+  std::vector<sg::ProfStat> st = sg::Profiler::get().read();
+  if (n) *n = st.size();
+  for (size_t i = 0; i < st.size() && i < cap && out; ++i) {
+    memset(out[i].name, 0, sizeof out[i].name);
+    strncpy(out[i].name, st[i].name.c_str(), sizeof out[i].name - 1);
+    out[i].launches = st[i].launches;
+    out[i].total_ms = st[i].total_ms;
+  }
+  return SG_OK;
+}
+
+void sg_profile_reset(void) { sg::Profiler::get().reset(); }
+
 int sg_ntt(sg_ctx* c, const uint64_t* in, uint64_t* out, size_t n_cols, size_t log_n, int inverse) {
   return guarded(c, [&] {
     sg::require(in && out && n_cols > 0 && n_cols < (1u << 31), "ntt: bad buffers or column count");

@@ -39,9 +39,9 @@ __global__ void quotient_kernel(const uint64_t* __restrict__ d, uint64_t n, uint
 cudaError_t hash_rollup_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, const uint64_t* lambdas,
                             uint64_t* phi, cudaStream_t s) {
   const unsigned T = 256;
+  SG_LAUNCH_SCOPE("merge_phi", s);
   hash_rollup_phi_kernel<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(lde, n, blowup, lambdas[0] % gl::P,
                                                                     lambdas[1] % gl::P, lambdas[2] % gl::P, phi);
-  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -49,8 +49,8 @@ cudaError_t quotient_zh(const uint64_t* d, uint64_t n, uint64_t m, uint64_t* q, 
   if (n <= m) return cudaMemsetAsync(q, 0, n * sizeof(uint64_t), s);
   if (n % m) return cudaErrorInvalidValue;
   const unsigned T = 256;
+  SG_LAUNCH_SCOPE("merge_quotient", s);
   quotient_kernel<<<(unsigned)((m + T - 1) / T), T, 0, s>>>(d, n, m, q);
-  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -157,8 +157,8 @@ cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w,
   const unsigned T = 128, B = blocks_for(n, T);
 #define SG_LEAF_CASE(WW, ZZ)                                                           \
   if (w == WW && zeros == ZZ) {                                                        \
+    SG_LAUNCH_SCOPE("merkle_leaves", s);                                               \
     leaf_kernel_t<WW, ZZ><<<B, T, 0, s>>>(cols, cs, n, t.arity0, t.label, t.d);        \
-    count_launches(1);                                                                 \
     return cudaGetLastError();                                                         \
   }
   SG_LEAF_CASE(1, 5)
@@ -169,8 +169,8 @@ cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w,
   SG_LEAF_CASE(16, 0)
   SG_LEAF_CASE(64, 0)
 #undef SG_LEAF_CASE
+  SG_LAUNCH_SCOPE("merkle_leaves", s);
   leaf_kernel<<<B, T, 0, s>>>(cols, w, cs, zeros, n, t.arity0, t.label, t.d);
-  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -180,6 +180,7 @@ cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
     const uint64_t* ch = t.d + 4 * t.off[l];
     uint64_t* par = t.d + 4 * t.off[l + 1];
     const unsigned B = blocks_for(np, 128);
+    SG_LAUNCH_SCOPE("merkle_nodes", s);
     switch (t.arity[l]) {
       case 2: node_kernel_t<2><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
       case 4: node_kernel_t<4><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
@@ -187,22 +188,21 @@ cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
       case 16: node_kernel_t<16><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
       default: node_kernel<<<B, 128, 0, s>>>(ch, t.len[l], par, np, t.arity[l], l + 1, t.label); break;
     }
-    count_launches(1);
   }
   return cudaGetLastError();
 }
 
 cudaError_t gather_digests(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
+  SG_LAUNCH_SCOPE("gather", s);
   gather_digests_kernel<<<blocks_for(4 * n, 256), 256, 0, s>>>(d, idx, n, out);
-  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t gather_u64(const uint64_t* src, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
+  SG_LAUNCH_SCOPE("gather", s);
   gather_u64_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, idx, n, out);
-  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -172,8 +172,8 @@ cudaError_t launch_pass(const PassArgs& a0, bool inv, uint32_t n_cols, cudaStrea
     PassArgs b = a;
     b.in = a.in + (uint64_t)c0 * a.in_col;
     b.out = a.out + (uint64_t)c0 * a.out_col;
+    SG_LAUNCH_SCOPE("ntt_pass", s);
     kern<<<dim3((unsigned)blocks, nc), T, smem, s>>>(b);
-    count_launches(1);
   }
   return cudaGetLastError();
 }
@@ -261,8 +261,8 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
   if (n_valid > N) n_valid = N;
   if (log_n == 0) {
     if (in == out) return cudaSuccess;
+    SG_LAUNCH_SCOPE("copy_cols", s);
     copy_cols_kernel<<<64, 256, 0, s>>>(in, out, n_cols, in_stride, out_stride, 1);
-    count_launches(1);
     return cudaGetLastError();
   }
   const uint64_t ninv = inverse ? gl::inv(N) : 1;
@@ -325,8 +325,8 @@ cudaError_t scale_by_powers(const uint64_t* in, uint64_t* out, uint32_t n_cols, 
                             uint64_t g, cudaStream_t s) {
   uint64_t threads = ((n + 31) / 32) * n_cols;
   if (threads == 0) return cudaSuccess;
+  SG_LAUNCH_SCOPE("coset_scale", s);
   scale_powers_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(in, out, n_cols, stride, n, g);
-  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -17,8 +17,6 @@
 
 namespace sg {
 
-std::atomic<uint64_t> g_kernel_launches{0};
-
 bool is_device_ptr(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {

@@ -192,12 +192,15 @@ cudaError_t ood_launch(const uint64_t* c, bool base, uint64_t n, const gl::Fp6& 
   const uint64_t blocks = ood_blocks(n, M);
   const gl::Fp6 w = gl::e_pow(z, M);
   const gl::Fp6 ws = gl::e_pow(w, blocks * kOodThreads);
-  if (base)
-    ood_partial_kernel<M, true><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
-  else
-    ood_partial_kernel<M, false><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
+  {
+    SG_LAUNCH_SCOPE("stir_ood", s);
+    if (base)
+      ood_partial_kernel<M, true><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
+    else
+      ood_partial_kernel<M, false><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
+  }
+  SG_LAUNCH_SCOPE("stir_ood_finish", s);
   ood_finish_kernel<M><<<1, 128, 0, s>>>(partials, blocks, z, evals);
-  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -206,11 +209,11 @@ cudaError_t fold_launch(const FoldArgs& a, cudaStream_t s) {
   const uint64_t nn = a.n / M;
   const unsigned T = 128;
   const unsigned blocks = (unsigned)((nn + T - 1) / T);
+  SG_LAUNCH_SCOPE("stir_fold", s);
   if (a.base)
     fold_kernel<M, true><<<blocks, T, 0, s>>>(a);
   else
     fold_kernel<M, false><<<blocks, T, 0, s>>>(a);
-  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -244,6 +247,7 @@ cudaError_t stir_fold(const FoldArgs& a, cudaStream_t s) {
 cudaError_t fold_tuples(const uint64_t* tuples, uint64_t n_final, int m, const gl::Fp6& alpha, uint64_t* next,
                         cudaStream_t s) {
   const unsigned blocks = (unsigned)((n_final + 127) / 128);
+  SG_LAUNCH_SCOPE("stir_fold_tuples", s);
   switch (m) {
     case 2: fold_tuples_kernel<2><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
     case 4: fold_tuples_kernel<4><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
@@ -251,7 +255,6 @@ cudaError_t fold_tuples(const uint64_t* tuples, uint64_t n_final, int m, const g
     case 16: fold_tuples_kernel<16><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
     default: return cudaErrorInvalidValue;
   }
-  count_launches(1);
   return cudaGetLastError();
 }
 
