@@ -33,6 +33,7 @@ extern "C" {
 #define SG_ENOMEM -3    /* device allocation failed */
 #define SG_ESPACE -4    /* output buffer too small; *len holds the needed size */
 #define SG_EVERIFY -5   /* self-verification of a produced proof failed */
+#define SG_ELIMIT -6    /* request exceeds the fixed scratch of sg_ntt_noalloc */
 
 #define SG_MAX_SCHEDULE 64
 
@@ -89,6 +90,29 @@ void sg_profile_reset(void);
  * Replaces the domain.fft / domain.ifft calls of trace_import.rs:276-279 and
  * lib.rs:402-410. in == out allowed. */
 int sg_ntt(sg_ctx* ctx, const uint64_t* in, uint64_t* out, size_t n_cols, size_t log_n, int inverse);
+
+/* sg_ntt for callers that must not have this library allocate device memory
+ * (no counterpart in the reference, which allocates freely on the host): for
+ * example a serving process that has already split all of HBM between its
+ * jobs, a host framework whose own allocator owns every device buffer, or a
+ * latency-critical loop that cannot afford cudaMalloc's device-wide sync.
+ * Same transform and results as sg_ntt, but no context and no allocation:
+ * the buffer between the two passes of a transform longer than 2^12 and the
+ * twiddle table are static device arrays (8 MiB + 128 KiB, held by every GPU
+ * that loads the library until exit).
+ *  - in/out: device pointers on the current device (in == out allowed);
+ *    host pointers are rejected with SG_EINVAL.
+ *  - limit: for log_n > 12, n_cols * 2^log_n must be <= 2^20, else SG_ELIMIT;
+ *    log_n <= 12 needs no scratch and has no limit.
+ *  - the first call on a device sets it up (cudaGetSymbolAddress of the static
+ *    arrays and a synchronous copy of the twiddle table), so make that first
+ *    call before any stream capture.
+ *  - every call shares the one static buffer: calls whose kernels can overlap
+ *    on the GPU (different streams, no ordering between them) race; order
+ *    them on one stream or synchronize between them.
+ *  - cuda_stream: a cudaStream_t as void*, NULL for the legacy default stream.
+ *    The call returns after enqueueing; results are ordered on that stream. */
+int sg_ntt_noalloc(const uint64_t* in, uint64_t* out, size_t n_cols, size_t log_n, int inverse, void* cuda_stream);
 
 /* Replaces lde_trace_columns (deep_ali/src/trace_import.rs:251-281): each of the
  * w columns (n_trace rows, column-major) -> iFFT, zero-pad to n_trace*blowup,

@@ -25,7 +25,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libstarkgpu.so")
 P = 0xFFFFFFFF00000001
 
-SG_OK, SG_EINVAL, SG_ECUDA, SG_ENOMEM, SG_ESPACE, SG_EVERIFY = 0, -1, -2, -3, -4, -5
+SG_OK, SG_EINVAL, SG_ECUDA, SG_ENOMEM, SG_ESPACE, SG_EVERIFY, SG_ELIMIT = 0, -1, -2, -3, -4, -5, -6
+NOALLOC_MAX_ELEMS = 1 << 20  # sg_ntt_noalloc: n_cols * 2^log_n limit for log_n > 12
 PHI_PARALLEL_GATE, PHI_ALWAYS, PHI_NEVER = 0, 1, 2
 AIR_HASH_ROLLUP = 4
 
@@ -94,7 +95,7 @@ class ProfileEntry(ctypes.Structure):
 # Every symbol declared in include/stark_gpu.h.
 EXPORTS = (
     "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_last_error", "sg_kernel_launches",
-    "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt",
+    "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
     "sg_lde", "sg_merge", "sg_merkle_commit", "sg_merkle_open", "sg_merkle_free", "sg_build_params",
     "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
 )
@@ -122,6 +123,7 @@ def lib():
     L.sg_profile_reset.argtypes = []
     L.sg_profile_reset.restype = None
     L.sg_ntt.argtypes = [vp, vp, vp, sz, sz, i32]
+    L.sg_ntt_noalloc.argtypes = [vp, vp, sz, sz, i32, vp]
     L.sg_lde.argtypes = [vp, vp, sz, sz, sz, u64, vp]
     L.sg_merge.argtypes = [vp, i32, vp, sz, sz, sz, vp, sz, i32, vp]
     L.sg_merkle_commit.argtypes = [vp, vp, sz, sz, sz, vp, sz, u64, ctypes.c_char_p, ctypes.POINTER(vp)]
@@ -190,6 +192,17 @@ def profile_read():
     n = ctypes.c_size_t()
     lib().sg_profile_read(arr, 64, ctypes.byref(n))
     return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(min(n.value, 64))}
+
+
+def ntt_noalloc(d_in, d_out, log_n: int, inverse: bool = False, stream_ptr: int = 0) -> int:
+    """sg_ntt_noalloc on device buffers (CUDA tensors or raw device pointers), for
+    callers that must not let the library allocate device memory. Returns the
+    SG_* code; the transform is ordered on `stream_ptr` (0 = default stream)."""
+    ip, _ki, host_in = _addr(d_in)
+    op, _ko, host_out = _addr(d_out)
+    n = 1 << log_n
+    count = d_in.size if host_in else (d_in.numel() if hasattr(d_in, "numel") else n)
+    return lib().sg_ntt_noalloc(ip, op, max(1, count // n), log_n, int(inverse), stream_ptr or None)
 
 
 def deep_fri_verify(params: FriParams, proof: bytes) -> bool:
