@@ -58,6 +58,7 @@ typedef struct {
 
 /* AIR ids follow deep_ali::air_workloads::AirType's declaration order. */
 #define SG_AIR_HASH_ROLLUP 4
+#define SG_AIR_SHA256 6 /* Sha256DsKsk: 756 columns, 766 constraints */
 
 typedef struct sg_ctx sg_ctx;
 typedef struct sg_tree sg_tree;
@@ -127,6 +128,26 @@ int sg_lde(sg_ctx* ctx, const uint64_t* trace, size_t w, size_t n_trace, size_t 
  * builds (lib.rs:190-228). lde: w x n (n = n_trace*blowup); c_eval: n values. */
 int sg_merge(sg_ctx* ctx, int air, const uint64_t* lde, size_t w, size_t n_trace, size_t blowup,
              const uint64_t* lambdas, size_t k, int phi_mode, uint64_t* c_eval);
+
+/* Replaces deep_ali_merge_sha256 (deep_ali/src/lib.rs:453-545): the SHA-256 AIR
+ * (eval_sha256_constraints, sha256_air.rs:956-1294) with an explicit block count
+ * gating its phases. lde: 756 x (n_trace*blowup); lambdas: 766 values (host). */
+int sg_merge_sha256(sg_ctx* ctx, const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas,
+                    size_t n_blocks, int phi_mode, uint64_t* c_eval);
+
+/* Replaces build_sha256_trace_multi (deep_ali/src/sha256_air.rs:429-472), host only:
+ * FIPS 180-4 padding, 128 rows per block, height = next power of two, last useful
+ * row replicated. Writes 756 x height column-major into `trace` (cap in elements),
+ * the block count, and the 32-byte digest carried in the H-state. */
+int sg_sha256_trace(const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height, size_t* n_blocks,
+                    uint8_t digest[32]);
+
+/* Core of prove_ds_ksk_binding (swarm-dns/src/prover.rs:512-585): SHA-256 AIR trace
+ * of `msg` -> LDE x32 -> merge (lambda_j = j+1) -> STIR with
+ * build_params(n0, fs_binding). Self-verified before return; `digest` receives the
+ * asserted SHA-256 digest read from the trace's H-state. */
+int sg_prove_sha256(sg_ctx* ctx, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,
+                    uint8_t* proof, size_t cap, size_t* len_out, uint8_t digest[32]);
 
 /* Merkle commitment over the rows of a column-major matrix (leaf i = the
  * `width` values of row i), with the reference channel's framing

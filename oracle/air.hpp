@@ -10,6 +10,7 @@
 #pragma once
 #include <cstddef>
 #include "gl.hpp"
+#include "sha256_air.hpp"
 
 namespace orc {
 
@@ -18,12 +19,14 @@ enum { AIR_HASH_ROLLUP = 4, AIR_SHA256 = 6 };
 inline size_t air_width(int air) {
   switch (air) {
     case AIR_HASH_ROLLUP: return 4;
+    case AIR_SHA256: return sha::WIDTH;
     default: return 0;
   }
 }
 inline size_t air_num_constraints(int air) {
   switch (air) {
     case AIR_HASH_ROLLUP: return 3;
+    case AIR_SHA256: return sha::NUM_CONSTRAINTS;
     default: return 0;
   }
 }
@@ -44,14 +47,13 @@ inline void build_hash_rollup_trace(const uint64_t* leaves, size_t n_leaves, siz
 }
 
 inline void eval_constraints(int air, const Fp* cur, const Fp* nxt, size_t row, size_t n_blocks, Fp* out) {
-  (void)row;
-  (void)n_blocks;
   switch (air) {
     case AIR_HASH_ROLLUP:
       out[0] = nxt[0] - cur[0] - Fp::raw(1);
       out[1] = cur[3] - cur[2] * cur[2];
       out[2] = nxt[2] - cur[3] - cur[1];
       break;
+    case AIR_SHA256: sha::eval(cur, nxt, row, n_blocks, out); break;
     default: break;
   }
 }

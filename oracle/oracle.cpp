@@ -68,7 +68,7 @@ bool phi_live(int mode, size_t n) {
 // Constraint j at LDE point i uses cur = row i, nxt = row (i+blowup) mod n and
 // trace_row = i / blowup (lib.rs:270-319).
 std::vector<Fp> merge(int air, const Fp* lde, size_t w, size_t n_trace, size_t blowup, const Fp* lambdas,
-                      size_t k, int phi_mode) {
+                      size_t k, int phi_mode, size_t n_blocks) {
   size_t n = n_trace * blowup;
   std::vector<Fp> phi(n);
   if (phi_live(phi_mode, n)) {
@@ -82,7 +82,7 @@ std::vector<Fp> merge(int air, const Fp* lde, size_t w, size_t n_trace, size_t b
           cur[c] = lde[c * n + i];
           nxt[c] = lde[c * n + ni];
         }
-        eval_constraints(air, cur.data(), nxt.data(), i / blowup, n_trace / 128, cv.data());
+        eval_constraints(air, cur.data(), nxt.data(), i / blowup, n_blocks, cv.data());
         Fp acc;
         for (size_t j = 0; j < k; ++j) acc = acc + lambdas[j] * cv[j];
         phi[i] = acc;
@@ -804,9 +804,59 @@ int orc_merge(int air, const uint64_t* lde, size_t w, size_t n_trace, size_t blo
               size_t k, int phi_mode, uint64_t* c_eval) {
   if (air_width(air) != w || air_num_constraints(air) != k) return -1;
   if (n_trace == 0 || (n_trace & (n_trace - 1)) || blowup == 0 || (blowup & (blowup - 1))) return -2;
-  auto c = merge(air, (const Fp*)lde, w, n_trace, blowup, (const Fp*)lambdas, k, phi_mode);
+  auto c = merge(air, (const Fp*)lde, w, n_trace, blowup, (const Fp*)lambdas, k, phi_mode, 1);
   memcpy(c_eval, c.data(), c.size() * 8);
   return 0;
+}
+
+// deep_ali_merge_sha256 (lib.rs:453-545): the SHA-256 AIR with an explicit block count.
+int orc_merge_sha256(const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas, size_t n_blocks,
+                     int phi_mode, uint64_t* c_eval) {
+  if (n_trace == 0 || (n_trace & (n_trace - 1)) || blowup == 0 || (blowup & (blowup - 1))) return -2;
+  auto c = merge(ORC_AIR_SHA256, (const Fp*)lde, sha::WIDTH, n_trace, blowup, (const Fp*)lambdas,
+                 sha::NUM_CONSTRAINTS, phi_mode, n_blocks);
+  memcpy(c_eval, c.data(), c.size() * 8);
+  return 0;
+}
+
+// build_sha256_trace_multi (sha256_air.rs:429-472): WIDTH x height column-major.
+int orc_sha256_trace(const uint8_t* msg, size_t len, uint64_t* out, size_t cap_elems, size_t* height,
+                     size_t* n_blocks) {
+  std::vector<Fp> tr;
+  *height = sha::build_trace_multi(msg, len, &tr, n_blocks);
+  if (tr.size() > cap_elems) return -3;
+  memcpy(out, tr.data(), tr.size() * 8);
+  return 0;
+}
+
+// eval_sha256_constraints at one row (for known-answer / tamper tests).
+int orc_sha256_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_blocks, uint64_t* out) {
+  sha::eval((const Fp*)cur, (const Fp*)nxt, row, n_blocks, (Fp*)out);
+  return 0;
+}
+
+// prove_ds_ksk_binding core (swarm-dns/src/prover.rs:512-585): multi-block trace ->
+// LDE x32 -> merge_sha256 (lambda_j = j+1) -> STIR with build_params(n0, fs_binding).
+// digest receives the asserted SHA-256 digest read from the H-state.
+int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
+                     size_t cap, size_t* out_len, uint8_t digest[32]) {
+  std::vector<Fp> tr;
+  size_t n_blocks = 0;
+  const size_t n_trace = sha::build_trace_multi(msg, len, &tr, &n_blocks);
+  const size_t digest_row = sha::ROWS_PER_BLOCK * (n_blocks - 1) + 65;
+  for (int k = 0; k < 8; ++k) {
+    uint32_t wd = (uint32_t)tr[(sha::H0 + k) * n_trace + digest_row].v;
+    for (int b = 0; b < 4; ++b) digest[4 * k + b] = (uint8_t)(wd >> (24 - 8 * b));
+  }
+  const size_t blowup = 32, n0 = n_trace * blowup;
+  std::vector<uint64_t> lde(sha::WIDTH * n0), c(n0);
+  orc_lde((const uint64_t*)tr.data(), sha::WIDTH, n_trace, blowup, 1, lde.data());
+  std::vector<uint64_t> lam(sha::NUM_CONSTRAINTS);
+  for (size_t j = 0; j < lam.size(); ++j) lam[j] = j + 1;
+  orc_merge_sha256(lde.data(), n_trace, blowup, lam.data(), n_blocks, phi_mode, c.data());
+  orc_fri_params p;
+  orc_build_params(n0, fs_binding, 1, &p);
+  return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
 }
 
 int orc_poly_div_zh(const uint64_t* coeffs, size_t n, size_t m, uint64_t* q) {

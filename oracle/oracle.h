@@ -65,6 +65,13 @@ int orc_hash_rollup_trace(const uint64_t* leaves, size_t n_leaves, size_t n_trac
 int orc_merge(int air, const uint64_t* lde, size_t w, size_t n_trace, size_t blowup, const uint64_t* lambdas,
               size_t k, int phi_mode, uint64_t* c_eval);
 int orc_poly_div_zh(const uint64_t* coeffs, size_t n, size_t m, uint64_t* q);
+int orc_merge_sha256(const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas, size_t n_blocks,
+                     int phi_mode, uint64_t* c_eval);
+int orc_sha256_trace(const uint8_t* msg, size_t len, uint64_t* out, size_t cap_elems, size_t* height,
+                     size_t* n_blocks);
+int orc_sha256_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_blocks, uint64_t* out);
+int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
+                     size_t cap, size_t* out_len, uint8_t digest[32]);
 void orc_build_params(size_t n0, const uint8_t pi[32], int stir, orc_fri_params* out);
 int orc_stir_prove(const uint64_t* f0, size_t n0, const orc_fri_params* p, uint8_t* out, size_t cap, size_t* len);
 int orc_stir_verify(const uint8_t* proof, size_t len, const orc_fri_params* p);

@@ -96,9 +96,11 @@ class ProfileEntry(ctypes.Structure):
 EXPORTS = (
     "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_last_error", "sg_kernel_launches",
     "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
-    "sg_lde", "sg_merge", "sg_merkle_commit", "sg_merkle_open", "sg_merkle_free", "sg_build_params",
-    "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
+    "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_prove_sha256", "sg_merkle_commit",
+    "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
 )
+AIR_SHA256 = 6
+SHA256_WIDTH, SHA256_CONSTRAINTS = 756, 766
 
 
 def lib():
@@ -126,6 +128,11 @@ def lib():
     L.sg_ntt_noalloc.argtypes = [vp, vp, sz, sz, i32, vp]
     L.sg_lde.argtypes = [vp, vp, sz, sz, sz, u64, vp]
     L.sg_merge.argtypes = [vp, i32, vp, sz, sz, sz, vp, sz, i32, vp]
+    L.sg_merge_sha256.argtypes = [vp, vp, sz, sz, vp, sz, i32, vp]
+    L.sg_sha256_trace.argtypes = [ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz),
+                                  ctypes.c_char_p]
+    L.sg_prove_sha256.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz,
+                                  ctypes.POINTER(sz), ctypes.c_char_p]
     L.sg_merkle_commit.argtypes = [vp, vp, sz, sz, sz, vp, sz, u64, ctypes.c_char_p, ctypes.POINTER(vp)]
     L.sg_merkle_open.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
     L.sg_merkle_free.argtypes = [vp]
@@ -203,6 +210,22 @@ def ntt_noalloc(d_in, d_out, log_n: int, inverse: bool = False, stream_ptr: int 
     n = 1 << log_n
     count = d_in.size if host_in else (d_in.numel() if hasattr(d_in, "numel") else n)
     return lib().sg_ntt_noalloc(ip, op, max(1, count // n), log_n, int(inverse), stream_ptr or None)
+
+
+def build_sha256_trace_multi(message: bytes):
+    """sha256_air.rs:429-472 on the host -> ((756, height) uint64 trace, n_blocks, asserted digest)."""
+    nb = (len(message) + 9 + 63) // 64
+    height = 128
+    while height < 128 * nb:
+        height *= 2
+    out = np.zeros(SHA256_WIDTH * height, dtype=np.uint64)
+    h, n = ctypes.c_size_t(), ctypes.c_size_t()
+    dg = ctypes.create_string_buffer(32)
+    rc = lib().sg_sha256_trace(message, len(message), out.ctypes.data, out.size, ctypes.byref(h), ctypes.byref(n),
+                               dg)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_sha256_trace failed")
+    return out[: SHA256_WIDTH * h.value].reshape(SHA256_WIDTH, h.value), n.value, dg.raw
 
 
 def deep_fri_verify(params: FriParams, proof: bytes) -> bool:
@@ -321,6 +344,39 @@ class Context:
         self._check(self._lib.sg_merge(self._h, air, ip, w, n_trace, blowup, lam.ctypes.data, lam.size, phi_mode,
                                        op))
         return out
+
+    def merge_sha256(self, lde, n_trace: int, blowup: int, lambdas, n_blocks: int, phi_mode=PHI_PARALLEL_GATE,
+                     out=None):
+        """deep_ali_merge_sha256 on a (756, n_trace*blowup) LDE."""
+        ip, _ki, host = _addr(lde)
+        lam = np.ascontiguousarray(lambdas, dtype=np.uint64)
+        if lam.size != SHA256_CONSTRAINTS:
+            raise ValueError("need one combination coefficient per constraint (766)")
+        n = n_trace * blowup
+        if out is None:
+            if not host:
+                raise ValueError("device input needs an explicit out buffer")
+            out = np.empty(n, dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        self._check(self._lib.sg_merge_sha256(self._h, ip, n_trace, blowup, lam.ctypes.data, n_blocks, phi_mode, op))
+        return out
+
+    def prove_sha256(self, message: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
+        """prove_ds_ksk_binding core -> (proof bytes, asserted SHA-256 digest); self-verified."""
+        if len(fs_binding) != 32:
+            raise ValueError("fs_binding must be 32 bytes")
+        cap = 1 << 24
+        while True:
+            buf = ctypes.create_string_buffer(cap)
+            ln = ctypes.c_size_t()
+            dg = ctypes.create_string_buffer(32)
+            rc = self._lib.sg_prove_sha256(self._h, message, len(message), fs_binding, phi_mode, buf, cap,
+                                           ctypes.byref(ln), dg)
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return buf.raw[:ln.value], dg.raw
 
     def deep_ali_merge_general(self, trace_evals_on_lde, combination_coeffs, air, omega, n_trace, blowup,
                                phi_mode=PHI_PARALLEL_GATE):

@@ -5,6 +5,7 @@
 #include "context.hpp"
 #include "merkle.cuh"
 #include "prover.hpp"
+#include "sha256_air.cuh"
 #include "verifier.hpp"
 
 struct sg_tree {
@@ -184,6 +185,50 @@ int sg_merge(sg_ctx* c, int air, const uint64_t* lde, size_t w, size_t n_trace, 
     Out dout(c_eval, n, c->stream);
     sg::merge_device(c, air, di.d, w, n_trace, blowup, lam.data(), k, phi_mode, dout.d);
     dout.finish();
+  });
+}
+
+int sg_merge_sha256(sg_ctx* c, const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas,
+                    size_t n_blocks, int phi_mode, uint64_t* c_eval) {
+  return guarded(c, [&] {
+    sg::require(lde && lambdas && c_eval, "merge_sha256: null buffer");
+    sg::require(n_trace > 0 && blowup > 0 && n_blocks > 0, "merge_sha256: empty input");
+    const size_t n = n_trace * blowup;
+    std::vector<uint64_t> lam(lambdas, lambdas + sg::sha::NUM_CONSTRAINTS);
+    In di(lde, (size_t)sg::sha::WIDTH * n, c->stream);
+    Out dout(c_eval, n, c->stream);
+    sg::merge_device(c, SG_AIR_SHA256, di.d, sg::sha::WIDTH, n_trace, blowup, lam.data(), lam.size(), phi_mode,
+                     dout.d, n_blocks);
+    dout.finish();
+  });
+}
+
+int sg_sha256_trace(const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height, size_t* n_blocks,
+                    uint8_t digest[32]) {
+  if ((!msg && len) || !height || !n_blocks || !digest) return SG_EINVAL;
+  try {
+    std::vector<uint64_t> tr;
+    uint64_t nb = 0;
+    uint8_t dg[32];
+    *height = (size_t)sg::sha256_build_trace(msg, len, &tr, &nb, dg);
+    *n_blocks = (size_t)nb;
+    memcpy(digest, dg, 32);
+    if (!trace || tr.size() > cap) return SG_ESPACE;
+    memcpy(trace, tr.data(), tr.size() * 8);
+    return SG_OK;
+  } catch (const std::bad_alloc&) {
+    return SG_ENOMEM;
+  }
+}
+
+int sg_prove_sha256(sg_ctx* c, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,
+                    uint8_t* proof, size_t cap, size_t* len_out, uint8_t digest[32]) {
+  return guarded(c, [&] {
+    sg::require((msg || !len) && fs_binding && len_out && digest, "prove_sha256: null argument");
+    std::vector<uint8_t> b = sg::prove_sha256_message(c, msg, len, fs_binding, phi_mode, true, digest);
+    *len_out = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_sha256: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
   });
 }
 

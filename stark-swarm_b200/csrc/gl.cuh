@@ -23,18 +23,71 @@ namespace gl {
 static constexpr uint64_t P = 0xFFFFFFFF00000001ull;
 static constexpr uint64_t EPS = 0xFFFFFFFFull;
 
-GL_HD uint64_t add(uint64_t a, uint64_t b) {
+#if defined(__CUDA_ARCH__)
+// Device versions: 32-bit carry chains in hand-written PTX. A 64-bit add or
+// compare costs the compiler several ALU instructions each; with explicit
+// carries the canonical add is 9, sub 5 and the 128-bit reduction 20 ALU
+// instructions, and the 64x64 product is 9 IMADs on the (otherwise idle) FMA pipe.
+__device__ __forceinline__ uint64_t add(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("{\n\t.reg .u32 a0, a1, b0, b1, s0, s1, t0, t1, c;\n\t.reg .pred p;\n\t"
+      "mov.b64 {a0, a1}, %1;\n\tmov.b64 {b0, b1}, %2;\n\t"
+      "add.cc.u32 s0, a0, b0;\n\taddc.cc.u32 s1, a1, b1;\n\taddc.u32 c, 0, 0;\n\t"
+      "add.cc.u32 t0, s0, 0xFFFFFFFF;\n\taddc.cc.u32 t1, s1, 0;\n\taddc.u32 c, c, 0;\n\t"
+      "setp.ne.u32 p, c, 0;\n\tselp.b32 s0, t0, s0, p;\n\tselp.b32 s1, t1, s1, p;\n\t"
+      "mov.b64 %0, {s0, s1};\n\t}"
+      : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t sub(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("{\n\t.reg .u32 a0, a1, b0, b1, d0, d1, bw;\n\t"
+      "mov.b64 {a0, a1}, %1;\n\tmov.b64 {b0, b1}, %2;\n\t"
+      "sub.cc.u32 d0, a0, b0;\n\tsubc.cc.u32 d1, a1, b1;\n\tsubc.u32 bw, 0, 0;\n\t"
+      "sub.cc.u32 d0, d0, bw;\n\tsubc.u32 d1, d1, 0;\n\t"
+      "mov.b64 %0, {d0, d1};\n\t}"
+      : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+// x = x0 + x1 2^32 + x2 2^64 + x3 2^96 = (lo) + x2 (2^32 - 1) - x3  (mod p), canonical result
+__device__ __forceinline__ uint64_t reduce128(uint64_t hi, uint64_t lo) {
+  uint64_t r;
+  asm("{\n\t.reg .u32 x0, x1, x2, x3, t0, t1, u0, u1, c, m;\n\t.reg .pred p;\n\t"
+      "mov.b64 {x0, x1}, %1;\n\tmov.b64 {x2, x3}, %2;\n\t"
+      "sub.cc.u32 t0, x0, x3;\n\tsubc.cc.u32 t1, x1, 0;\n\tsubc.u32 c, 0, 0;\n\t"
+      "sub.cc.u32 t0, t0, c;\n\tsubc.u32 t1, t1, 0;\n\t"
+      "sub.cc.u32 u0, 0, x2;\n\tsubc.u32 u1, x2, 0;\n\t"
+      "add.cc.u32 t0, t0, u0;\n\taddc.cc.u32 t1, t1, u1;\n\taddc.u32 c, 0, 0;\n\t"
+      "sub.u32 m, 0, c;\n\tadd.cc.u32 t0, t0, m;\n\taddc.u32 t1, t1, 0;\n\t"
+      "add.cc.u32 u0, t0, 0xFFFFFFFF;\n\taddc.cc.u32 u1, t1, 0;\n\taddc.u32 c, 0, 0;\n\t"
+      "setp.ne.u32 p, c, 0;\n\tselp.b32 t0, u0, t0, p;\n\tselp.b32 t1, u1, t1, p;\n\t"
+      "mov.b64 %0, {t0, t1};\n\t}"
+      : "=l"(r) : "l"(lo), "l"(hi));
+  return r;
+}
+__device__ __forceinline__ uint64_t mul(uint64_t a, uint64_t b) {
+  uint64_t lo, hi;
+  asm("{\n\t.reg .u32 a0, a1, b0, b1, x0, x1, x2, x3;\n\t"
+      "mov.b64 {a0, a1}, %2;\n\tmov.b64 {b0, b1}, %3;\n\t"
+      "mul.lo.u32 x0, a0, b0;\n\tmul.hi.u32 x1, a0, b0;\n\t"
+      "mad.lo.cc.u32 x1, a0, b1, x1;\n\tmadc.hi.u32 x2, a0, b1, 0;\n\t"
+      "mad.lo.cc.u32 x1, a1, b0, x1;\n\tmadc.hi.cc.u32 x2, a1, b0, x2;\n\taddc.u32 x3, 0, 0;\n\t"
+      "mad.lo.cc.u32 x2, a1, b1, x2;\n\tmadc.hi.u32 x3, a1, b1, x3;\n\t"
+      "mov.b64 %0, {x0, x1};\n\tmov.b64 %1, {x2, x3};\n\t}"
+      : "=l"(lo), "=l"(hi) : "l"(a), "l"(b));
+  return reduce128(hi, lo);
+}
+#else
+inline uint64_t add(uint64_t a, uint64_t b) {
   uint64_t s = a + b;
   bool c = s < a;
   return (c || s >= P) ? s - P : s;
 }
-GL_HD uint64_t sub(uint64_t a, uint64_t b) {
+inline uint64_t sub(uint64_t a, uint64_t b) {
   uint64_t d = a - b;
   return a < b ? d + P : d;
 }
-GL_HD uint64_t neg(uint64_t a) { return a ? P - a : 0; }
-
-GL_HD uint64_t reduce128(uint64_t hi, uint64_t lo) {
+inline uint64_t reduce128(uint64_t hi, uint64_t lo) {
   uint64_t hh = hi >> 32, hl = hi & EPS;
   uint64_t t0 = lo - hh;
   if (lo < hh) t0 -= EPS;
@@ -43,15 +96,12 @@ GL_HD uint64_t reduce128(uint64_t hi, uint64_t lo) {
   if (r < t0) r += EPS;
   return r >= P ? r - P : r;
 }
-
-GL_HD uint64_t mul(uint64_t a, uint64_t b) {
-#if defined(__CUDA_ARCH__)
-  return reduce128(__umul64hi(a, b), a * b);
-#else
+inline uint64_t mul(uint64_t a, uint64_t b) {
   unsigned __int128 x = (unsigned __int128)a * b;
   return reduce128((uint64_t)(x >> 64), (uint64_t)x);
-#endif
 }
+#endif
+GL_HD uint64_t neg(uint64_t a) { return a ? P - a : 0; }
 GL_HD uint64_t sqr(uint64_t a) { return mul(a, a); }
 
 GL_HD uint64_t pow(uint64_t a, uint64_t e) {

@@ -12,6 +12,7 @@
 #include "merge.cuh"
 #include "merkle.cuh"
 #include "prover.hpp"
+#include "sha256_air.cuh"
 #include "stir.cuh"
 #include "verifier.hpp"
 
@@ -66,9 +67,11 @@ static bool phi_live(int mode, uint64_t n) {
 }
 
 void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_t n_trace, uint64_t blowup,
-                  const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c) {
-  require(air == SG_AIR_HASH_ROLLUP, "merge: unsupported AIR id");
-  require(w == 4 && k == 3, "merge: HashRollup has 4 columns and 3 constraints");
+                  const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c, uint64_t n_blocks) {
+  require(air == SG_AIR_HASH_ROLLUP || air == SG_AIR_SHA256, "merge: unsupported AIR id");
+  if (air == SG_AIR_HASH_ROLLUP) require(w == 4 && k == 3, "merge: HashRollup has 4 columns and 3 constraints");
+  if (air == SG_AIR_SHA256)
+    require(w == sha::WIDTH && k == sha::NUM_CONSTRAINTS, "merge: the SHA-256 AIR has 756 columns and 766 constraints");
   require(pow2(n_trace) && pow2(blowup), "merge: sizes must be powers of 2");
   require(phi_mode >= 0 && phi_mode <= 2, "merge: bad phi mode");
   const uint64_t n = n_trace * blowup;
@@ -80,7 +83,16 @@ void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_
   }
   DBuf phi(n, s);
   DBuf scratch(log2_exact(n) > 12 ? n : 0, s);
-  cuda_check(hash_rollup_phi(d_lde, n, blowup, lambdas, phi.p, s), "phi");
+  if (air == SG_AIR_HASH_ROLLUP) {
+    cuda_check(hash_rollup_phi(d_lde, n, blowup, lambdas, phi.p, s), "phi");
+  } else {
+    std::vector<uint64_t> lam(lambdas, lambdas + k);
+    for (auto& x : lam) x %= gl::P;
+    DBuf d_lam(k, s);
+    cuda_check(cudaMemcpyAsync(d_lam.p, lam.data(), k * 8, cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(sha256_phi(d_lde, n, blowup, n_blocks, d_lam.p, phi.p, s), "sha256 phi");
+    cuda_check(cudaStreamSynchronize(s), "sync");  // lam (host) must outlive the copy
+  }
   ntt(c, phi.p, phi.p, 1, n, n, log2_exact(n), true, n, scratch.p);
   cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
   ntt(c, d_c, d_c, 1, n, n, log2_exact(n), false, n > n_trace ? n - n_trace : n, scratch.p);
@@ -356,6 +368,33 @@ std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* le
   merge_device(c, SG_AIR_HASH_ROLLUP, d_lde.p, 4, n_trace, blowup, lam, 3, phi_mode, d_c.p);
   sg_fri_params p;
   sg_build_params(n0, pi, 1, &p);
+  std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
+  if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
+    throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
+  return proof;
+}
+
+// ------------------------------------------------------------------ SHA-256 pipeline
+// prove_ds_ksk_binding (swarm-dns/src/prover.rs:512-585): multi-block trace on the
+// host (sha256_air.rs:429-472), then LDE x32 -> deep_ali_merge_sha256 with
+// lambda_j = j + 1 -> STIR with build_params(n0, fs_binding) on the device.
+std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
+                                          int phi_mode, bool self_verify, uint8_t digest[32]) {
+  std::vector<uint64_t> trace;
+  uint64_t n_blocks = 0;
+  const uint64_t n_trace = sha256_build_trace(msg, len, &trace, &n_blocks, digest);
+  const uint64_t blowup = 32, n0 = n_trace * blowup;
+  require(log2_exact(n0) <= kMaxLogN, "prove_sha256: message too long for a 2^24 domain");
+  cudaStream_t s = c->stream;
+  DBuf d_trace(trace.size(), s), d_lde((uint64_t)sha::WIDTH * n0, s), d_c(n0, s);
+  cuda_check(cudaMemcpyAsync(d_trace.p, trace.data(), trace.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+  lde_device(c, d_trace.p, sha::WIDTH, n_trace, blowup, 1, d_lde.p);
+  std::vector<uint64_t> lam(sha::NUM_CONSTRAINTS);
+  for (uint64_t j = 0; j < lam.size(); ++j) lam[j] = j + 1;  // comb_coeffs (prover.rs:100-102)
+  merge_device(c, SG_AIR_SHA256, d_lde.p, sha::WIDTH, n_trace, blowup, lam.data(), lam.size(), phi_mode, d_c.p,
+               n_blocks);
+  sg_fri_params p;
+  sg_build_params(n0, fs_binding, 1, &p);
   std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
   if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
     throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};

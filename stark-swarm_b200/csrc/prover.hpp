@@ -10,8 +10,12 @@ namespace sg {
 
 void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
                 uint64_t* d_out);
+// lambdas are host values; n_blocks gates the SHA-256 AIR (the AIR registry uses 1)
 void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_t n_trace, uint64_t blowup,
-                  const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c);
+                  const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c, uint64_t n_blocks = 1);
+// prove_ds_ksk_binding core: message -> SHA-256 AIR trace -> LDE x32 -> merge -> STIR.
+std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
+                                          int phi_mode, bool self_verify, uint8_t digest[32]);
 std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p);
 std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* leaves, uint64_t n_leaves,
                                                    const uint8_t pi[32], int phi_mode, bool self_verify);

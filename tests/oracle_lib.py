@@ -80,6 +80,14 @@ def lib():
                                                 ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
             L.orc_chacha_block.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_uint32)]
+            L.orc_merge_sha256.argtypes = [U64P, ctypes.c_size_t, ctypes.c_size_t, U64P, ctypes.c_size_t,
+                                           ctypes.c_int, U64P]
+            L.orc_sha256_trace.argtypes = [ctypes.c_char_p, ctypes.c_size_t, U64P, ctypes.c_size_t,
+                                           ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+            L.orc_sha256_eval.argtypes = [U64P, U64P, ctypes.c_size_t, ctypes.c_size_t, U64P]
+            L.orc_prove_sha256.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_int,
+                                           ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                                           ctypes.c_char_p]
             _lib = L
     return _lib
 
@@ -165,6 +173,51 @@ def prove_hash_rollup(leaves, pi: bytes, phi_mode=PHI_PARALLEL_GATE) -> bytes:
     rc = lib().orc_prove_hash_rollup(_ptr(lv), lv.size, pi, phi_mode, buf, cap, ctypes.byref(ln))
     assert rc == 0, rc
     return buf.raw[:ln.value]
+
+
+SHA_WIDTH, SHA_K = 756, 766
+SHA_H0 = 534
+
+
+def sha256_trace(msg: bytes):
+    """build_sha256_trace_multi -> ((756, height) uint64, n_blocks)"""
+    n_blocks_max = (len(msg) + 9 + 63) // 64
+    height = 128
+    while height < 128 * n_blocks_max:
+        height *= 2
+    out = np.zeros(SHA_WIDTH * height, dtype=np.uint64)
+    h, nb = ctypes.c_size_t(), ctypes.c_size_t()
+    rc = lib().orc_sha256_trace(msg, len(msg), _ptr(out), out.size, ctypes.byref(h), ctypes.byref(nb))
+    assert rc == 0, rc
+    return out[: SHA_WIDTH * h.value].reshape(SHA_WIDTH, h.value), nb.value
+
+
+def sha256_eval(cur, nxt, row, n_blocks):
+    cur = np.ascontiguousarray(cur, dtype=np.uint64)
+    nxt = np.ascontiguousarray(nxt, dtype=np.uint64)
+    out = np.zeros(SHA_K, dtype=np.uint64)
+    lib().orc_sha256_eval(_ptr(cur), _ptr(nxt), row, n_blocks, _ptr(out))
+    return out
+
+
+def merge_sha256(lde_cols, n_trace, blowup, lambdas, n_blocks, phi_mode=PHI_PARALLEL_GATE):
+    lde_cols = np.ascontiguousarray(lde_cols, dtype=np.uint64)
+    lam = np.ascontiguousarray(lambdas, dtype=np.uint64)
+    out = np.zeros(n_trace * blowup, dtype=np.uint64)
+    rc = lib().orc_merge_sha256(_ptr(lde_cols), n_trace, blowup, _ptr(lam), n_blocks, phi_mode, _ptr(out))
+    assert rc == 0, rc
+    return out
+
+
+def prove_sha256(msg: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
+    """prove_ds_ksk_binding core -> (proof bytes, asserted digest)"""
+    cap = 1 << 26
+    buf = ctypes.create_string_buffer(cap)
+    ln = ctypes.c_size_t()
+    dg = ctypes.create_string_buffer(32)
+    rc = lib().orc_prove_sha256(msg, len(msg), fs_binding, phi_mode, buf, cap, ctypes.byref(ln), dg)
+    assert rc == 0, rc
+    return buf.raw[:ln.value], dg.raw
 
 
 def sha3_256(msg: bytes) -> bytes:

@@ -97,3 +97,15 @@ def test_verifier_agrees_with_oracle_on_other_schedules(sched, cc):
     proof = O.stir_prove(f0, p_o)
     assert O.stir_verify(proof, p_o)
     assert sg.deep_fri_verify(p_s, proof)
+
+
+@pytest.mark.parametrize("msg", [b"abc", b"", bytes(range(64)), b"c" * 120, bytes(range(200))])
+def test_sha256_trace_builder_matches_oracle(msg):
+    # host-side trace builder (build_sha256_trace_multi) of the library vs the oracle
+    import hashlib
+    sg = load_sgpu()
+    tr, nb, digest = sg.build_sha256_trace_multi(msg)
+    otr, onb = O.sha256_trace(msg)
+    assert nb == onb
+    assert np.array_equal(tr, otr)
+    assert digest == hashlib.sha256(msg).digest()
