@@ -182,6 +182,47 @@ int sg_stir_verify(const uint8_t* proof, size_t len, const sg_fri_params* params
 int sg_prove_hash_rollup(sg_ctx* ctx, const uint64_t* leaves, size_t n_leaves, const uint8_t pi[32], int phi_mode,
                          uint8_t* proof, size_t cap, size_t* len);
 
+/* ---------------------------------------------------------------- batched / served proving
+ * No single reference function: the reference scales by running one proof per
+ * worker process (swarm-worker/src/main.rs:341-355, driven by swarm-ctrl). Here
+ * many proofs share one GPU: N worker threads, each with its own stream, take
+ * jobs FIFO as soon as they are free (continuous batching); a job starts only
+ * while the estimated device footprint of the running jobs plus its own fits
+ * the HBM budget (0 = unlimited; a job larger than the budget runs alone).
+ * Every proof is self-verified and byte-identical to the single-proof call. */
+#define SG_JOB_SHA256 1      /* input = message bytes, input_len = bytes (sg_prove_sha256) */
+#define SG_JOB_HASH_ROLLUP 2 /* input = u64 rollup leaves, input_len = count (sg_prove_hash_rollup) */
+
+typedef struct {
+  int32_t kind;
+  int32_t phi_mode;
+  const void* input;
+  size_t input_len;
+  uint8_t pi[32]; /* fs_binding / public_inputs_hash */
+} sg_job;
+
+typedef struct {
+  int32_t status; /* SG_OK or an SG_E* code */
+  uint32_t reserved;
+  size_t proof_len;
+  uint8_t digest[32]; /* SHA-256 jobs: the asserted digest */
+  double queue_ms;    /* submit -> start */
+  double run_ms;      /* start -> proof ready */
+  double latency_ms;  /* submit -> proof ready */
+} sg_job_result;
+
+typedef struct sg_server sg_server;
+int sg_server_create(sg_ctx* ctx, int n_streams, uint64_t hbm_budget_bytes, sg_server** out);
+void sg_server_destroy(sg_server* srv); /* waits for running jobs; queued jobs are dropped */
+int sg_server_submit(sg_server* srv, const sg_job* job, uint64_t* ticket); /* copies the input */
+int sg_server_poll(sg_server* srv, uint64_t ticket);                       /* 1 done, 0 pending */
+/* Blocks until the job is done; copies the proof (cap bytes available) and releases
+ * the ticket, except on SG_ESPACE, which keeps it so the caller can retry. */
+int sg_server_wait(sg_server* srv, uint64_t ticket, sg_job_result* res, uint8_t* proof, size_t cap);
+/* Proves n jobs with n_streams proofs in flight; proof i goes to proofs + i*cap_per_job. */
+int sg_prove_batch(sg_ctx* ctx, const sg_job* jobs, size_t n, int n_streams, uint64_t hbm_budget_bytes,
+                   uint8_t* proofs, size_t cap_per_job, sg_job_result* results);
+
 #ifdef __cplusplus
 }
 #endif

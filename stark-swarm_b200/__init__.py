@@ -98,7 +98,20 @@ EXPORTS = (
     "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
     "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_prove_sha256", "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
+    "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
 )
+JOB_SHA256, JOB_HASH_ROLLUP = 1, 2
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("phi_mode", ctypes.c_int32), ("input", ctypes.c_void_p),
+                ("input_len", ctypes.c_size_t), ("pi", ctypes.c_uint8 * 32)]
+
+
+class JobResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("reserved", ctypes.c_uint32), ("proof_len", ctypes.c_size_t),
+                ("digest", ctypes.c_uint8 * 32), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double)]
 AIR_SHA256 = 6
 SHA256_WIDTH, SHA256_CONSTRAINTS = 756, 766
 
@@ -129,6 +142,14 @@ def lib():
     L.sg_lde.argtypes = [vp, vp, sz, sz, sz, u64, vp]
     L.sg_merge.argtypes = [vp, i32, vp, sz, sz, sz, vp, sz, i32, vp]
     L.sg_merge_sha256.argtypes = [vp, vp, sz, sz, vp, sz, i32, vp]
+    L.sg_server_create.argtypes = [vp, i32, u64, ctypes.POINTER(vp)]
+    L.sg_server_destroy.argtypes = [vp]
+    L.sg_server_destroy.restype = None
+    L.sg_server_submit.argtypes = [vp, ctypes.POINTER(Job), ctypes.POINTER(u64)]
+    L.sg_server_poll.argtypes = [vp, u64]
+    L.sg_server_wait.argtypes = [vp, u64, ctypes.POINTER(JobResult), ctypes.c_char_p, sz]
+    L.sg_prove_batch.argtypes = [vp, ctypes.POINTER(Job), sz, i32, u64, ctypes.c_char_p, sz,
+                                 ctypes.POINTER(JobResult)]
     L.sg_sha256_trace.argtypes = [ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz),
                                   ctypes.c_char_p]
     L.sg_prove_sha256.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz,
@@ -378,6 +399,18 @@ class Context:
             self._check(rc)
             return buf.raw[:ln.value], dg.raw
 
+    def prove_batch(self, jobs, n_streams: int = 8, hbm_budget_bytes: int = 0, cap_per_job: int = 1 << 21):
+        """jobs: list of (kind, data, pi[, phi_mode]) -> list of (proof bytes, JobResult)."""
+        made = [make_job(*j) for j in jobs]
+        arr = (Job * len(made))(*[m[0] for m in made])
+        res = (JobResult * len(made))()
+        buf = ctypes.create_string_buffer(cap_per_job * max(1, len(made)))
+        rc = self._lib.sg_prove_batch(self._h, arr, len(made), n_streams, hbm_budget_bytes, buf, cap_per_job, res)
+        if rc != SG_OK:
+            raise StarkGpuError(rc, "sg_prove_batch failed")
+        raw = buf.raw
+        return [(raw[i * cap_per_job: i * cap_per_job + res[i].proof_len], res[i]) for i in range(len(made))]
+
     def deep_ali_merge_general(self, trace_evals_on_lde, combination_coeffs, air, omega, n_trace, blowup,
                                phi_mode=PHI_PARALLEL_GATE):
         del omega  # the domain generator is implied by n = n_trace * blowup
@@ -430,6 +463,80 @@ class Context:
                 continue
             self._check(rc)
             return buf.raw[:ln.value]
+
+
+def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
+    """A sg_job plus the buffer it points to (keep both alive until submitted)."""
+    if len(pi) != 32:
+        raise ValueError("pi must be 32 bytes")
+    if kind == JOB_SHA256:
+        buf = ctypes.create_string_buffer(bytes(data), max(1, len(data)))
+        n = len(data)
+    elif kind == JOB_HASH_ROLLUP:
+        buf = np.ascontiguousarray(data, dtype=np.uint64)
+        n = buf.size
+    else:
+        raise ValueError("unknown job kind")
+    j = Job()
+    j.kind, j.phi_mode = kind, phi_mode
+    j.input = ctypes.addressof(buf) if kind == JOB_SHA256 else (buf.ctypes.data if n else None)
+    j.input_len = n
+    ctypes.memmove(j.pi, pi, 32)
+    return j, buf
+
+
+class Server:
+    """Continuous-batching proof server (sg_server): submit() any time, wait() per ticket."""
+
+    def __init__(self, ctx: "Context", n_streams: int = 8, hbm_budget_bytes: int = 0):
+        self._ctx = ctx
+        h = ctypes.c_void_p()
+        rc = ctx._lib.sg_server_create(ctx._h, n_streams, hbm_budget_bytes, ctypes.byref(h))
+        if rc != SG_OK:
+            raise StarkGpuError(rc, "sg_server_create failed")
+        self._h = h
+
+    def submit(self, kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE) -> int:
+        j, _keep = make_job(kind, data, pi, phi_mode)
+        t = ctypes.c_uint64()
+        rc = self._ctx._lib.sg_server_submit(self._h, ctypes.byref(j), ctypes.byref(t))
+        if rc != SG_OK:
+            raise StarkGpuError(rc, "sg_server_submit failed")
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        return self._ctx._lib.sg_server_poll(self._h, ticket) == 1
+
+    def wait(self, ticket: int):
+        """-> (proof bytes, JobResult)"""
+        cap = 1 << 22
+        while True:
+            res = JobResult()
+            buf = ctypes.create_string_buffer(cap)
+            rc = self._ctx._lib.sg_server_wait(self._h, ticket, ctypes.byref(res), buf, cap)
+            if rc == SG_ESPACE:
+                cap = res.proof_len
+                continue
+            if rc != SG_OK:
+                raise StarkGpuError(rc, f"job {ticket} failed")
+            return buf.raw[:res.proof_len], res
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._ctx._lib.sg_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class MerkleTree:

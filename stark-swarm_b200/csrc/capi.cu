@@ -113,7 +113,7 @@ void sg_ctx_destroy(sg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  sg::ntt_tables_free(&c->tw);
+  if (c->owns_tables) sg::ntt_tables_free(&c->tw);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }

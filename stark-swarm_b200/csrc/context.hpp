@@ -15,6 +15,7 @@ struct sg_ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
   sg::NttTables tw;
+  bool owns_tables = true;  // worker contexts of a server borrow the parent's tables
   std::string err;
 };
 

@@ -1,0 +1,251 @@
+// server.cu — continuous-batching proof server (many proofs in flight on one GPU).
+//
+// The reference proves one shard per worker process and scales across
+// processes (swarm-worker, swarm-ctrl). On one B200 a single small proof
+// (n0 = 2^12..2^17) occupies a few SMs and spends most of its latency in
+// Fiat-Shamir round trips, so throughput comes from keeping many proofs in
+// flight: N worker threads, each with its own CUDA stream and context
+// (sharing the parent's twiddle tables), take jobs from a FIFO queue as soon
+// as they finish the previous one. Admission is by HBM footprint: a job starts
+// only while the footprints of the running jobs plus its own stay within the
+// budget (a job larger than the whole budget runs alone). Results are byte
+// for byte those of the single-proof entry points.
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "context.hpp"
+#include "prover.hpp"
+#include "sha256_air.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Entry {
+  int32_t kind = 0;
+  int32_t phi_mode = 0;
+  std::vector<uint8_t> input;
+  uint8_t pi[32];
+  uint64_t footprint = 0;
+  bool done = false;
+  int status = SG_OK;
+  std::string err;
+  std::vector<uint8_t> proof;
+  uint8_t digest[32] = {0};
+  Clock::time_point t_submit, t_start, t_end;
+};
+
+uint64_t next_pow2(uint64_t x) {
+  uint64_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// Device bytes a job holds at its peak (LDE + trace + quotient + STIR buffers), estimated.
+uint64_t footprint_bytes(const sg_job& j) {
+  if (j.kind == SG_JOB_SHA256) {
+    const uint64_t blocks = (j.input_len + 9 + 63) / 64;
+    const uint64_t nt = next_pow2(128 * blocks), n0 = nt * 32;
+    return 8 * ((uint64_t)sg::sha::WIDTH * (n0 + 2 * nt) + 16 * n0);
+  }
+  const uint64_t nt = next_pow2(j.input_len < 8 ? 8 : j.input_len), n0 = nt * 32;
+  return 8 * (4 * n0 + 8 * nt + 16 * n0);
+}
+
+}  // namespace
+
+struct sg_server {
+  sg_ctx* parent = nullptr;
+  uint64_t budget = 0;
+  uint64_t in_flight = 0;
+  int running = 0;
+  bool stop = false;
+  uint64_t next_ticket = 1;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<uint64_t> queue;
+  std::map<uint64_t, Entry> entries;
+  std::vector<sg_ctx*> wctx;
+  std::vector<std::thread> threads;
+
+  void worker(sg_ctx* c) {
+    cudaSetDevice(c->device);
+    for (;;) {
+      uint64_t ticket = 0;
+      Entry* e = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] {
+          if (stop) return true;
+          if (queue.empty()) return false;
+          const Entry& f = entries.at(queue.front());
+          return running == 0 || in_flight + f.footprint <= budget;
+        });
+        if (stop) return;
+        ticket = queue.front();
+        queue.pop_front();
+        e = &entries.at(ticket);
+        in_flight += e->footprint;
+        ++running;
+        e->t_start = Clock::now();
+      }
+      run(c, e);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        e->t_end = Clock::now();
+        e->done = true;
+        in_flight -= e->footprint;
+        --running;
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+
+  static void run(sg_ctx* c, Entry* e) {
+    try {
+      if (e->kind == SG_JOB_SHA256) {
+        e->proof = sg::prove_sha256_message(c, e->input.data(), e->input.size(), e->pi, e->phi_mode, true, e->digest);
+      } else {
+        const uint64_t n = e->input.size() / 8;
+        e->proof = sg::prove_hash_rollup_host_leaves(c, (const uint64_t*)e->input.data(), n, e->pi, e->phi_mode, true);
+      }
+      e->status = SG_OK;
+    } catch (const sg::SgError& x) {
+      e->status = x.code;
+      e->err = x.msg;
+    } catch (const std::exception& x) {
+      e->status = SG_EINVAL;
+      e->err = x.what();
+    }
+  }
+};
+
+extern "C" {
+
+int sg_server_create(sg_ctx* ctx, int n_streams, uint64_t hbm_budget_bytes, sg_server** out) {
+  if (!ctx || !out || n_streams < 1 || n_streams > 256) return SG_EINVAL;
+  *out = nullptr;
+  sg_server* s = new sg_server;
+  s->parent = ctx;
+  s->budget = hbm_budget_bytes ? hbm_budget_bytes : UINT64_MAX;
+  cudaSetDevice(ctx->device);
+  for (int i = 0; i < n_streams; ++i) {
+    sg_ctx* w = new sg_ctx;
+    w->device = ctx->device;
+    w->tw = ctx->tw;
+    w->owns_tables = false;
+    if (cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete w;
+      sg_server_destroy(s);
+      return SG_ECUDA;
+    }
+    w->stream = w->own_stream;
+    s->wctx.push_back(w);
+  }
+  for (sg_ctx* w : s->wctx) s->threads.emplace_back([s, w] { s->worker(w); });
+  *out = s;
+  return SG_OK;
+}
+
+void sg_server_destroy(sg_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  for (auto& t : s->threads) t.join();
+  for (sg_ctx* w : s->wctx) sg_ctx_destroy(w);
+  delete s;
+}
+
+int sg_server_submit(sg_server* s, const sg_job* job, uint64_t* ticket) {
+  if (!s || !job || !ticket) return SG_EINVAL;
+  if (job->kind != SG_JOB_SHA256 && job->kind != SG_JOB_HASH_ROLLUP) return SG_EINVAL;
+  if (job->input_len && !job->input) return SG_EINVAL;
+  Entry e;
+  e.kind = job->kind;
+  e.phi_mode = job->phi_mode;
+  const size_t bytes = job->kind == SG_JOB_SHA256 ? job->input_len : job->input_len * 8;
+  e.input.assign((const uint8_t*)job->input, (const uint8_t*)job->input + bytes);
+  memcpy(e.pi, job->pi, 32);
+  e.footprint = footprint_bytes(*job);
+  e.t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    *ticket = s->next_ticket++;
+    s->entries.emplace(*ticket, std::move(e));
+    s->queue.push_back(*ticket);
+  }
+  s->cv_work.notify_one();
+  return SG_OK;
+}
+
+int sg_server_poll(sg_server* s, uint64_t ticket) {
+  if (!s) return SG_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->entries.find(ticket);
+  if (it == s->entries.end()) return SG_EINVAL;
+  return it->second.done ? 1 : 0;
+}
+
+int sg_server_wait(sg_server* s, uint64_t ticket, sg_job_result* res, uint8_t* proof, size_t cap) {
+  if (!s || !res) return SG_EINVAL;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->entries.find(ticket);
+  if (it == s->entries.end()) return SG_EINVAL;
+  s->cv_done.wait(lk, [&] { return it->second.done; });
+  Entry& e = it->second;
+  auto ms = [](Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  memset(res, 0, sizeof *res);
+  res->status = e.status;
+  res->proof_len = e.proof.size();
+  memcpy(res->digest, e.digest, 32);
+  res->queue_ms = ms(e.t_submit, e.t_start);
+  res->run_ms = ms(e.t_start, e.t_end);
+  res->latency_ms = ms(e.t_submit, e.t_end);
+  int rc = e.status;
+  if (rc == SG_OK) {
+    if (!proof || e.proof.size() > cap) return SG_ESPACE;  // entry kept: the caller may retry with a larger buffer
+    memcpy(proof, e.proof.data(), e.proof.size());
+  }
+  s->entries.erase(it);
+  return rc;
+}
+
+int sg_prove_batch(sg_ctx* ctx, const sg_job* jobs, size_t n, int n_streams, uint64_t hbm_budget_bytes,
+                   uint8_t* proofs, size_t cap_per_job, sg_job_result* results) {
+  if (!ctx || (n && (!jobs || !results))) return SG_EINVAL;
+  sg_server* s = nullptr;
+  int rc = sg_server_create(ctx, n_streams, hbm_budget_bytes, &s);
+  if (rc != SG_OK) return rc;
+  std::vector<uint64_t> tickets(n);
+  int first_err = SG_OK;
+  for (size_t i = 0; i < n; ++i) {
+    rc = sg_server_submit(s, &jobs[i], &tickets[i]);
+    if (rc != SG_OK) {
+      tickets[i] = 0;
+      results[i] = sg_job_result{};
+      results[i].status = rc;
+      if (first_err == SG_OK) first_err = rc;
+    }
+  }
+  for (size_t i = 0; i < n; ++i) {
+    if (!tickets[i]) continue;
+    rc = sg_server_wait(s, tickets[i], &results[i], proofs ? proofs + i * cap_per_job : nullptr, cap_per_job);
+    if (rc != SG_OK && first_err == SG_OK) first_err = rc;
+  }
+  sg_server_destroy(s);
+  return first_err;
+}
+
+}  // extern "C"

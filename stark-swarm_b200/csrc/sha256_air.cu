@@ -8,6 +8,7 @@
 // no constraint matrix is ever materialised. The emission order below is the
 // reference's (sha256_air.rs:956-1294) because lambda_j multiplies the j-th value.
 #include <cstring>
+#include <mutex>
 
 #include "counters.hpp"
 #include "gl.cuh"
@@ -308,6 +309,7 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
 }
 
 bool g_k_uploaded[64] = {false};
+std::mutex g_k_mu;
 
 }  // namespace
 
@@ -348,10 +350,14 @@ cudaError_t sha256_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, uint64_
                        uint64_t* phi, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !g_k_uploaded[dev]) {
-    cudaError_t e = cudaMemcpyToSymbol(kK, kK_host, sizeof kK_host);
-    if (e != cudaSuccess) return e;
-    g_k_uploaded[dev] = true;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  {
+    std::lock_guard<std::mutex> g(g_k_mu);
+    if (!g_k_uploaded[dev]) {
+      cudaError_t e = cudaMemcpyToSymbol(kK, kK_host, sizeof kK_host);
+      if (e != cudaSuccess) return e;
+      g_k_uploaded[dev] = true;
+    }
   }
   const unsigned T = 128;
   SG_LAUNCH_SCOPE("merge_phi", s);

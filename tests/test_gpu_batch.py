@@ -1,0 +1,56 @@
+"""Batched and served proving: every proof made in a mix of concurrent jobs is
+byte-identical to the same job proved alone (oracle), under several stream
+counts and an HBM budget tight enough to serialise admission; the server
+accepts submissions while earlier jobs are running."""
+import hashlib
+import time
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix(n, seed):
+    rng = np.random.default_rng(seed)
+    jobs, want = [], []
+    for i in range(n):
+        pi = hashlib.sha3_256(b"job%d" % i).digest()
+        if i % 3 == 2:
+            leaves = rng.integers(0, O.P, int(rng.integers(1, 3000)), dtype=np.uint64)
+            jobs.append((2, leaves, pi))
+            want.append((O.prove_hash_rollup(leaves, pi), None))
+        else:
+            ln = int(np.clip(rng.lognormal(np.log(120), 0.6), 40, 600))
+            msg = rng.integers(0, 256, ln, dtype=np.uint8).tobytes()
+            jobs.append((1, msg, pi))
+            proof, dg = O.prove_sha256(msg, pi)
+            want.append((proof, dg))
+    return jobs, want
+
+
+@pytest.mark.parametrize("streams,budget", [(1, 0), (4, 0), (16, 0), (8, 64 << 20)])
+def test_batch_matches_single_proofs(ctx, streams, budget):
+    jobs, want = _mix(12, streams)
+    out = ctx.prove_batch(jobs, n_streams=streams, hbm_budget_bytes=budget)
+    for (proof, res), (wproof, wdg) in zip(out, want):
+        assert res.status == 0
+        assert proof == wproof
+        if wdg is not None:
+            assert bytes(res.digest) == wdg
+        assert res.latency_ms >= res.run_ms >= 0
+
+
+def test_server_admits_while_running(sgpu, ctx):
+    jobs, want = _mix(10, 99)
+    with sgpu.Server(ctx, n_streams=4) as srv:
+        tickets = [srv.submit(*jobs[i]) for i in range(5)]
+        first, _ = srv.wait(tickets[0])
+        assert first == want[0][0]
+        time.sleep(0.01)
+        tickets += [srv.submit(*jobs[i]) for i in range(5, 10)]  # arrive while others are on the GPU
+        for i, t in enumerate(tickets[1:], start=1):
+            proof, res = srv.wait(t)
+            assert res.status == 0 and proof == want[i][0]
