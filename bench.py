@@ -218,6 +218,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sha256-jobs", type=int, default=256,
+                    help="SHA-256 AIR proofs for the plain-vs-batched section (0 skips it)")
     ap.add_argument("--columns", type=int, default=64,
                     help="trace columns (64 = the benchmark workload; fewer for small profiling captures)")
     args = ap.parse_args()
@@ -239,6 +241,12 @@ def main():
     ctx = sg.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    # The Merkle commitment over the LDE rows and the STIR proof of column 0 are
+    # independent once the LDE exists: they run concurrently from two host
+    # threads, each on its own context/stream (ctypes releases the GIL).
+    ctx2 = sg.Context(local)
+    from concurrent.futures import ThreadPoolExecutor
+    pool = ThreadPoolExecutor(max_workers=1)
 
     trace = make_trace(rank)
     h_trace = torch.from_numpy(trace.view(np.int64)).pin_memory()
@@ -246,17 +254,18 @@ def main():
     d_lde = torch.empty((W, N0), dtype=torch.int64, device="cuda")
     params = sg.build_params(N0, PI_HASH)
 
-    def step_device():
-        ctx.lde(d_trace, BLOWUP, SHIFT, out=d_lde)
+    def commit_and_prove():
+        fut = pool.submit(ctx2.deep_fri_prove, d_lde[0], N0, params)
         root = ctx.merkle_commit(d_lde, ARITIES, TREE_LABEL)
-        proof = ctx.deep_fri_prove(d_lde[0], N0, params)
-        return root, proof
+        return root, fut.result()
+
+    def step_device():
+        ctx.lde(d_trace, BLOWUP, SHIFT, out=d_lde)  # returns once the LDE is complete
+        return commit_and_prove()
 
     def step_e2e():
         ctx.lde(h_trace, BLOWUP, SHIFT, out=d_lde)  # host (pinned) input: H2D inside the call
-        root = ctx.merkle_commit(d_lde, ARITIES, TREE_LABEL)
-        proof = ctx.deep_fri_prove(d_lde[0], N0, params)
-        return root, proof
+        return commit_and_prove()
 
     # warm-up, and a determinism check: every step must give the same bytes
     ref = None
@@ -342,6 +351,26 @@ def main():
                     "launches_per_step": launches_per_step}
     kernels = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps} for k, v in prof.items()}
 
+    # SHA-256 AIR proofs of seeded 64-byte messages (prove_ds_ksk_binding shape:
+    # 2 blocks, n_trace 256, n0 8192): one proof at a time vs 16 in flight
+    cfg1 = None
+    if args.sha256_jobs > 0:
+        rng = np.random.default_rng(1)
+        jobs = [(sg.JOB_SHA256, rng.integers(0, 256, 64, dtype=np.uint8).tobytes(),
+                 hashlib.sha3_256(b"cfg1-%d" % i).digest()) for i in range(args.sha256_jobs)]
+        ctx.prove_batch(jobs[:16], n_streams=16)
+        cfg1 = {"workload": "SHA-256 AIR proof of a 64-byte message (2 blocks, n_trace 256, n0 8192, 756 cols, "
+                            "766 constraints), self-verified", "jobs": len(jobs)}
+        for label, streams in (("plain", 1), ("batched", 16)):
+            t0 = time.perf_counter()
+            out = ctx.prove_batch(jobs, n_streams=streams)
+            dt = time.perf_counter() - t0
+            lat = sorted(r.latency_ms for _, r in out)
+            assert all(r.status == 0 for _, r in out)
+            cfg1[label] = {"streams": streams, "proofs_per_s": len(jobs) / dt,
+                           "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
+        cfg1["batched_over_plain"] = cfg1["batched"]["proofs_per_s"] / cfg1["plain"]["proofs_per_s"]
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -364,10 +393,13 @@ def main():
             "kernels": kernels,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "sha256_proofs": cfg1,
             "proof_bytes": len(ref[1]),
             "root": ref[0].hex(),
         }
         print(json.dumps(line), flush=True)
+    pool.shutdown()
+    ctx2.close()
     ctx.close()
     if ws > 1:
         import torch.distributed as dist

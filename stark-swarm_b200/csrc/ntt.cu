@@ -35,6 +35,9 @@ struct PassArgs {
   // m*in_m + lane*flat_lane; indices >= in_valid are zero and never read
   uint64_t flat_lane;
   uint64_t in_valid;
+  // 1 or 2 when only the first `sparse_nz` of the 16 inputs of every first-stage
+  // radix-16 group can be non-zero (zero-padded forward transform); 0 = dense
+  int sparse_nz;
   int log_k;                  // lanes per CTA = 2^log_k
   int tw_shift;               // >= 0: output (lane,i) *= w24^((i*lane) << tw_shift)
   uint64_t scale;             // != 1: outputs *= scale
@@ -82,6 +85,47 @@ __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int l
   __syncthreads();
 }
 
+// First Stockham stage (Ns = 1, radix 16) when only inputs r < NZ of each group
+// can be non-zero: X[k] = sum_{r<NZ} x_r w_16^{rk}. NZ = 1 is a broadcast,
+// NZ = 2 is X[k], X[k+8] = x0 +- w_16^k x1 (7 shift-multiplies, no full DFT).
+template <int NZ, bool INV>
+__device__ __forceinline__ void stockham_first_sparse(uint64_t* sm, int t, int T, int K, int log_m) {
+  const int M = 1 << log_m, Mp = M + (M >> 4);
+  const int log_g = log_m - 4, G = 1 << log_g;
+  const int groups = K << log_g;
+  constexpr unsigned E16 = exp16(INV);
+  for (int g0 = 0; g0 < groups; g0 += T) {
+    const int g = g0 + t;
+    uint64_t x0 = 0, x1 = 0;
+    int l = 0, j = 0;
+    if (g < groups) {
+      l = g >> log_g;
+      j = g & (G - 1);
+      x0 = sm[l * Mp + padi(j)];
+      if (NZ == 2) x1 = sm[l * Mp + padi(j + G)];
+    }
+    __syncthreads();
+    if (g < groups) {
+      uint64_t* row = sm + l * Mp;
+      const int base = j << 4;
+      if (NZ == 1) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) row[padi(base + k)] = x0;
+      } else {
+        row[padi(base)] = gl::add(x0, x1);
+        row[padi(base + 8)] = gl::sub(x0, x1);
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+          const uint64_t w = gl::mul_pow2(x1, (E16 * (unsigned)k) % 192u);
+          row[padi(base + k)] = gl::add(x0, w);
+          row[padi(base + k + 8)] = gl::sub(x0, w);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <int LOG_M, bool INV>
 __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   constexpr int M = 1 << LOG_M;
@@ -96,7 +140,10 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   uint64_t* out = a.out + (uint64_t)blockIdx.y * a.out_col;
 
   const bool lane_fast_in = a.in_lane == 1;
-  for (int e = t; e < E; e += T) {
+  // a sparse first stage reads only points m < nz * M/16: skip the rest
+  const int sparse = (LOG_M >= 4 && lane_fast_in) ? a.sparse_nz : 0;
+  const int E_load = sparse ? K * sparse * (M >> 4) : E;
+  for (int e = t; e < E_load; e += T) {
     int l, m;
     if (lane_fast_in) {
       l = e & (K - 1);
@@ -117,8 +164,17 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   constexpr int N16 = LOG_M / 4, REM = LOG_M % 4;
   int log_ns = 0;
   if constexpr (LOG_M >= 4) {
+    int st0 = 0;
+    if (sparse == 1 || sparse == 2) {
+      if (sparse == 1)
+        stockham_first_sparse<1, INV>(sm, t, T, K, LOG_M);
+      else
+        stockham_first_sparse<2, INV>(sm, t, T, K, LOG_M);
+      log_ns = 4;
+      st0 = 1;
+    }
 #pragma unroll 1
-    for (int st = 0; st < N16; ++st) {
+    for (int st = st0; st < N16; ++st) {
       stockham_stage<16, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
       log_ns += 4;
     }
@@ -300,6 +356,13 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
   a.n_lanes = N1;
   a.flat_lane = 1;  // flat index k = k2*N1 + k1
   a.in_valid = n_valid;
+  {
+    // points k2 >= ceil(n_valid / N1) are zero; the first radix-16 stage reads
+    // k2 = j + r*N2/16, so at most ceil(.. / (N2/16)) of its 16 inputs are non-zero
+    const uint64_t m_nz = (n_valid + N1 - 1) / N1, G = N2 / 16;
+    const uint64_t nz = (m_nz + G - 1) / G;
+    a.sparse_nz = (n_valid < N && nz <= 2) ? (int)(nz ? nz : 1) : 0;
+  }
   a.tw_shift = 24 - log_n;
   a.scale = 1;
   cudaError_t e = launch_pass_dyn(l2, a, inverse, n_cols, s);
@@ -316,6 +379,7 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
   a.n_lanes = N2;
   a.flat_lane = N1;
   a.in_valid = N;
+  a.sparse_nz = 0;
   a.tw_shift = -1;
   a.scale = ninv;
   return launch_pass_dyn(l1, a, inverse, n_cols, s);
