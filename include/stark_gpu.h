@@ -69,6 +69,22 @@ void sg_ctx_destroy(sg_ctx* ctx);
 /* Use an existing cudaStream_t (passed as void*) for all later calls; NULL = the context's own stream. */
 int sg_ctx_set_stream(sg_ctx* ctx, void* cuda_stream);
 const char* sg_last_error(const sg_ctx* ctx);
+/* Context options.
+ * SG_OPT_WIDE_MERGE selects how sg_prove_sha256 evaluates the SHA-256 AIR over the LDE:
+ *   SG_WIDE_MERGE_LDE     materialise the 756-column LDE, then evaluate (fewest launches);
+ *   SG_WIDE_MERGE_COSETS  never store the LDE: for each of the `blowup` cosets r, evaluate
+ *                         all columns on r*<w_n0^blowup> (coefficients twisted by w_n0^{rk},
+ *                         one n_trace-point NTT per column) and fold the constraints of that
+ *                         coset straight into Phi (row i+blowup of the LDE is the next point
+ *                         of the same coset) -- memory 3 x trace instead of blowup x trace;
+ *   SG_WIDE_MERGE_AUTO    (default) cosets once the LDE would exceed 2 GiB.
+ * Both give bit-identical results. */
+#define SG_OPT_WIDE_MERGE 1
+#define SG_WIDE_MERGE_AUTO 0
+#define SG_WIDE_MERGE_LDE 1
+#define SG_WIDE_MERGE_COSETS 2
+int sg_ctx_set_option(sg_ctx* ctx, int option, int64_t value);
+
 /* Number of kernels this library has launched in this process (instrumentation). */
 uint64_t sg_kernel_launches(const sg_ctx* ctx);
 
@@ -99,7 +115,7 @@ int sg_ntt(sg_ctx* ctx, const uint64_t* in, uint64_t* out, size_t n_cols, size_t
  * latency-critical loop that cannot afford cudaMalloc's device-wide sync.
  * Same transform and results as sg_ntt, but no context and no allocation:
  * the buffer between the two passes of a transform longer than 2^12 and the
- * twiddle table are static device arrays (8 MiB + 128 KiB, held by every GPU
+ * twiddle table are static device arrays (8 MiB + 576 KiB, held by every GPU
  * that loads the library until exit).
  *  - in/out: device pointers on the current device (in == out allowed);
  *    host pointers are rejected with SG_EINVAL.

@@ -94,13 +94,16 @@ class ProfileEntry(ctypes.Structure):
 
 # Every symbol declared in include/stark_gpu.h.
 EXPORTS = (
-    "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_last_error", "sg_kernel_launches",
+    "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_ctx_set_option", "sg_last_error",
+    "sg_kernel_launches",
     "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
     "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_prove_sha256", "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
 )
 JOB_SHA256, JOB_HASH_ROLLUP = 1, 2
+OPT_WIDE_MERGE = 1
+WIDE_MERGE_AUTO, WIDE_MERGE_LDE, WIDE_MERGE_COSETS = 0, 1, 2
 
 
 class Job(ctypes.Structure):
@@ -129,6 +132,7 @@ def lib():
     L.sg_ctx_destroy.argtypes = [vp]
     L.sg_ctx_destroy.restype = None
     L.sg_ctx_set_stream.argtypes = [vp, vp]
+    L.sg_ctx_set_option.argtypes = [vp, i32, ctypes.c_int64]
     L.sg_last_error.argtypes = [vp]
     L.sg_last_error.restype = ctypes.c_char_p
     L.sg_kernel_launches.argtypes = [vp]
@@ -306,6 +310,9 @@ class Context:
 
     def set_stream(self, stream_ptr: int = 0):
         self._check(self._lib.sg_ctx_set_stream(self._h, stream_ptr or None))
+
+    def set_option(self, option: int, value: int):
+        self._check(self._lib.sg_ctx_set_option(self._h, option, value))
 
     @property
     def kernel_launches(self) -> int:

@@ -126,6 +126,16 @@ int sg_ctx_set_stream(sg_ctx* c, void* stream) {
 
 const char* sg_last_error(const sg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
+int sg_ctx_set_option(sg_ctx* c, int option, int64_t value) {
+  if (!c) return SG_EINVAL;
+  if (option == SG_OPT_WIDE_MERGE) {
+    if (value < SG_WIDE_MERGE_AUTO || value > SG_WIDE_MERGE_COSETS) return SG_EINVAL;
+    c->wide_merge = (int)value;
+    return SG_OK;
+  }
+  return SG_EINVAL;
+}
+
 uint64_t sg_kernel_launches(const sg_ctx*) { return sg::g_kernel_launches.load(); }
 
 int sg_profile_enable(int on) {
@@ -150,11 +160,11 @@ void sg_profile_reset(void) { sg::Profiler::get().reset(); }
 int sg_ntt(sg_ctx* c, const uint64_t* in, uint64_t* out, size_t n_cols, size_t log_n, int inverse) {
   return guarded(c, [&] {
     sg::require(in && out && n_cols > 0 && n_cols < (1u << 31), "ntt: bad buffers or column count");
-    sg::require(log_n <= (size_t)sg::kMaxLogN, "ntt: log_n must be <= 24");
+    sg::require(log_n <= (size_t)sg::kMaxLogN, "ntt: log_n must be <= 28");
     const size_t n = size_t(1) << log_n, total = n_cols * n;
     In di(in, total, c->stream);
     Out dout(out, total, c->stream);
-    sg::DBuf scratch(log_n > 12 ? total : 0, c->stream);
+    sg::DBuf scratch(sg::ntt_scratch_elems(n_cols, (int)log_n), c->stream);
     sg::cuda_check(sg::ntt_batch(c->tw, di.d, dout.d, (uint32_t)n_cols, n, n, (int)log_n, inverse != 0, n,
                                  scratch.p, c->stream),
                    "ntt");

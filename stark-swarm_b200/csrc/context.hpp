@@ -16,6 +16,7 @@ struct sg_ctx {
   cudaStream_t stream = nullptr;
   sg::NttTables tw;
   bool owns_tables = true;  // worker contexts of a server borrow the parent's tables
+  int wide_merge = SG_WIDE_MERGE_AUTO;  // SG_OPT_WIDE_MERGE
   std::string err;
 };
 

@@ -1,10 +1,15 @@
 // ntt.cu — batched Goldilocks NTT for sm_100a.
 //
-// Global structure: a transform of N = 2^n <= 2^12 is one pass; larger N is a
-// four-step split N = N1 * N2 (N1 <= N2 <= 2^12) done as two passes:
+// Global structure: a transform of N = 2^n <= 2^12 is one pass; up to 2^24 it
+// is a four-step split N = N1 * N2 (N1 <= N2 <= 2^12) done as two passes:
 //   pass 1: for each k1 < N1, DFT_{N2} over k2 of x[k2*N1 + k1], times w_N^{i2*k1},
 //           stored transposed at i2*N1 + k1;
 //   pass 2: for each i2 < N2, DFT_{N1} over the contiguous row, stored at i1*N2 + i2.
+// Up to 2^28 the second step is itself split (N = A*B*C, three passes):
+//   pass 1 as above with N1 = A*B, N2 = C;
+//   pass 2: inside each block i3, DFT_B over k2 of rows k1 < A, times
+//           w_{AB}^{i2*k1}, written to row (i2*C + i3) so that
+//   pass 3: DFT_A over each contiguous row, stored at i1*BC + (i2*C + i3).
 // A CTA owns K "lanes" (independent sub-DFTs with adjacent addresses, so every
 // global row access is K*8 contiguous bytes) x M points in shared memory.
 // Inside the CTA the M-point DFT is a Stockham autosort sequence of radix-16
@@ -12,12 +17,13 @@
 // them, barrier, writes them to their permuted slots, barrier. Shared memory
 // is padded one word per 16 so every stage's stride pattern is conflict-free.
 // The radix-R butterflies use only powers of w_R <= w_16, which in Goldilocks
-// are powers of two (w_16 = 2^156 for ark's root chain), so they cost a shift
-// and a reduction instead of a multiply.
+// are powers of two (w_16 = 2^156 for ark's root chain).
+#include <vector>
+
+#include "counters.hpp"
 #include "dft.cuh"
 #include "gl.cuh"
 #include "ntt.cuh"
-#include "counters.hpp"
 
 namespace sg {
 namespace {
@@ -27,7 +33,11 @@ __device__ __forceinline__ int padi(int m) { return m + (m >> 4); }
 struct PassArgs {
   const uint64_t* in;
   uint64_t* out;
-  uint64_t in_col, out_col;   // column strides (grid.y = column)
+  // grid row y = blockIdx.y + y_base -> (c, s) = (y / y_sub, y % y_sub); the
+  // tile's base is in + c*in_col + s*in_sub (same for out)
+  uint64_t in_col, out_col, in_sub, out_sub;
+  uint32_t y_sub;
+  uint32_t y_base;
   uint64_t in_lane, in_m;     // input address of (lane, m)
   uint64_t out_lane, out_i;   // output address of (lane, i)
   uint64_t n_lanes;           // valid lanes
@@ -39,17 +49,18 @@ struct PassArgs {
   // radix-16 group can be non-zero (zero-padded forward transform); 0 = dense
   int sparse_nz;
   int log_k;                  // lanes per CTA = 2^log_k
-  int tw_shift;               // >= 0: output (lane,i) *= w24^((i*lane) << tw_shift)
+  int tw_log;                 // > 0: output (lane, i) *= w_{2^tw_log}^(i*lane)
   uint64_t scale;             // != 1: outputs *= scale
-  const uint64_t* tw_lo;      // w24^i (direction of the transform)
-  const uint64_t* tw_hi;      // w24^(4096 i) = w_4096^i
+  const uint64_t* tw_st;      // w_4096^i (direction of the transform)
+  const uint64_t* tw_lo;      // w28^i
+  const uint64_t* tw_hi;      // w28^(2^14 i)
 };
 
 // One Stockham stage of radix R over all K lanes of the tile.
 // Each thread holds V values = V/R groups; group g -> lane g / G, j = g % G.
 template <int R, int V, bool INV>
 __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int log_m, int log_ns,
-                                               const uint64_t* tw_hi) {
+                                               const uint64_t* tw_st) {
   constexpr int GPT = V / R;
   constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
   const int M = 1 << log_m, Mp = M + (M >> 4);
@@ -74,7 +85,7 @@ __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int l
     if (log_ns > 0) {
       const int sh = 12 - log_ns - LR;  // w_{Ns R}^{rk} = w_4096^{rk 4096/(Ns R)}
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[q * R + r] = gl::mul(v[q * R + r], __ldg(tw_hi + (((r * k) << sh) & 4095)));
+      for (int r = 1; r < R; ++r) v[q * R + r] = gl::mul(v[q * R + r], __ldg(tw_st + (((r * k) << sh) & 4095)));
     }
     dft_reg<R, INV>(v + q * R);
     int idx = ((j >> log_ns) << (log_ns + LR)) + k;
@@ -136,8 +147,10 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   const int K = 1 << a.log_k;
   const int E = K * M;
   const uint64_t lane0 = (uint64_t)blockIdx.x << a.log_k;
-  const uint64_t* in = a.in + (uint64_t)blockIdx.y * a.in_col;
-  uint64_t* out = a.out + (uint64_t)blockIdx.y * a.out_col;
+  const uint64_t y = (uint64_t)blockIdx.y + a.y_base;
+  const uint64_t yc = y / a.y_sub, ys = y - yc * a.y_sub;
+  const uint64_t* in = a.in + yc * a.in_col + ys * a.in_sub;
+  uint64_t* out = a.out + yc * a.out_col + ys * a.out_sub;
 
   const bool lane_fast_in = a.in_lane == 1;
   // a sparse first stage reads only points m < nz * M/16: skip the rest
@@ -175,13 +188,13 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
     }
 #pragma unroll 1
     for (int st = st0; st < N16; ++st) {
-      stockham_stage<16, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
+      stockham_stage<16, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
       log_ns += 4;
     }
   }
-  if constexpr (REM == 1) stockham_stage<2, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
-  if constexpr (REM == 2) stockham_stage<4, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
-  if constexpr (REM == 3) stockham_stage<8, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_hi);
+  if constexpr (REM == 1) stockham_stage<2, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
+  if constexpr (REM == 2) stockham_stage<4, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
+  if constexpr (REM == 3) stockham_stage<8, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
 
   const bool lane_fast_out = a.out_lane == 1;
   for (int e = t; e < E; e += T) {
@@ -196,17 +209,14 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
     uint64_t lane = lane0 + l;
     if (lane >= a.n_lanes) continue;
     uint64_t x = sm[l * Mp + padi(i)];
-    if (a.tw_shift >= 0) {
-      uint64_t ex = (((uint64_t)i * lane) << a.tw_shift) & ((1ull << 24) - 1);
-      x = gl::mul(x, gl::mul(__ldg(a.tw_lo + (ex & 4095)), __ldg(a.tw_hi + (ex >> 12))));
-    }
+    if (a.tw_log > 0) x = gl::mul(x, tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * lane, a.tw_log));
     if (a.scale != 1) x = gl::mul(x, a.scale);
     out[lane * a.out_lane + (uint64_t)i * a.out_i] = x;
   }
 }
 
 template <int LOG_M>
-cudaError_t launch_pass(const PassArgs& a0, bool inv, uint32_t n_cols, cudaStream_t s) {
+cudaError_t launch_pass(const PassArgs& a0, bool inv, uint64_t n_rows, cudaStream_t s) {
   constexpr int M = 1 << LOG_M;
   constexpr int V = M < 16 ? M : 16;
   PassArgs a = a0;
@@ -223,31 +233,30 @@ cudaError_t launch_pass(const PassArgs& a0, bool inv, uint32_t n_cols, cudaStrea
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  for (uint32_t c0 = 0; c0 < n_cols; c0 += 65535) {
-    uint32_t nc = n_cols - c0 < 65535 ? n_cols - c0 : 65535;
+  for (uint64_t y0 = 0; y0 < n_rows; y0 += 65535) {
+    const uint32_t ny = (uint32_t)(n_rows - y0 < 65535 ? n_rows - y0 : 65535);
     PassArgs b = a;
-    b.in = a.in + (uint64_t)c0 * a.in_col;
-    b.out = a.out + (uint64_t)c0 * a.out_col;
+    b.y_base = (uint32_t)y0;
     SG_LAUNCH_SCOPE("ntt_pass", s);
-    kern<<<dim3((unsigned)blocks, nc), T, smem, s>>>(b);
+    kern<<<dim3((unsigned)blocks, ny), T, smem, s>>>(b);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_pass_dyn(int log_m, const PassArgs& a, bool inv, uint32_t n_cols, cudaStream_t s) {
+cudaError_t launch_pass_dyn(int log_m, const PassArgs& a, bool inv, uint64_t n_rows, cudaStream_t s) {
   switch (log_m) {
-    case 1: return launch_pass<1>(a, inv, n_cols, s);
-    case 2: return launch_pass<2>(a, inv, n_cols, s);
-    case 3: return launch_pass<3>(a, inv, n_cols, s);
-    case 4: return launch_pass<4>(a, inv, n_cols, s);
-    case 5: return launch_pass<5>(a, inv, n_cols, s);
-    case 6: return launch_pass<6>(a, inv, n_cols, s);
-    case 7: return launch_pass<7>(a, inv, n_cols, s);
-    case 8: return launch_pass<8>(a, inv, n_cols, s);
-    case 9: return launch_pass<9>(a, inv, n_cols, s);
-    case 10: return launch_pass<10>(a, inv, n_cols, s);
-    case 11: return launch_pass<11>(a, inv, n_cols, s);
-    case 12: return launch_pass<12>(a, inv, n_cols, s);
+    case 1: return launch_pass<1>(a, inv, n_rows, s);
+    case 2: return launch_pass<2>(a, inv, n_rows, s);
+    case 3: return launch_pass<3>(a, inv, n_rows, s);
+    case 4: return launch_pass<4>(a, inv, n_rows, s);
+    case 5: return launch_pass<5>(a, inv, n_rows, s);
+    case 6: return launch_pass<6>(a, inv, n_rows, s);
+    case 7: return launch_pass<7>(a, inv, n_rows, s);
+    case 8: return launch_pass<8>(a, inv, n_rows, s);
+    case 9: return launch_pass<9>(a, inv, n_rows, s);
+    case 10: return launch_pass<10>(a, inv, n_rows, s);
+    case 11: return launch_pass<11>(a, inv, n_rows, s);
+    case 12: return launch_pass<12>(a, inv, n_rows, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -275,37 +284,87 @@ __global__ void scale_powers_kernel(const uint64_t* in, uint64_t* out, uint32_t 
   }
 }
 
+PassArgs base_args(const NttTables& t, bool inverse) {
+  PassArgs a{};
+  a.tw_st = inverse ? t.d_inv_st : t.d_fwd_st;
+  a.tw_lo = inverse ? t.d_inv_lo : t.d_fwd_lo;
+  a.tw_hi = inverse ? t.d_inv_hi : t.d_fwd_hi;
+  a.y_sub = 1;
+  a.scale = 1;
+  return a;
+}
+
+// sparse first stage for pass 1 over k_hi: points m >= ceil(n_valid / n_lo) are zero
+int sparse_nz_for(uint64_t n_valid, uint64_t N, uint64_t n_lo, uint64_t M) {
+  const uint64_t m_nz = (n_valid + n_lo - 1) / n_lo, G = M / 16;
+  const uint64_t nz = (m_nz + G - 1) / G;
+  return (n_valid < N && M >= 16 && nz <= 2) ? (int)(nz ? nz : 1) : 0;
+}
+
 }  // namespace
 
-cudaError_t ntt_tables_init(NttTables* t) {
-  uint64_t w = gl::root_of_unity(24), wi = gl::inv(w);
-  uint64_t h[4][4096];
-  uint64_t w4096 = gl::pow(w, 4096), wi4096 = gl::pow(wi, 4096);
-  uint64_t a = 1, b = 1, c = 1, d = 1;
-  for (int i = 0; i < 4096; ++i) {
-    h[0][i] = a; a = gl::mul(a, w);
-    h[1][i] = b; b = gl::mul(b, w4096);
-    h[2][i] = c; c = gl::mul(c, wi);
-    h[3][i] = d; d = gl::mul(d, wi4096);
+void ntt_tables_host(uint64_t* out) {
+  for (int dir = 0; dir < 2; ++dir) {
+    uint64_t* st = out + dir * kTwDirElems;
+    uint64_t* lo = st + 4096;
+    uint64_t* hi = lo + kTwEntries;
+    uint64_t w28 = gl::root_of_unity(kTwBaseLog);
+    uint64_t w4096 = gl::root_of_unity(12);
+    if (dir == 1) {
+      w28 = gl::inv(w28);
+      w4096 = gl::inv(w4096);
+    }
+    const uint64_t wstep = gl::pow(w28, kTwEntries);
+    uint64_t a = 1, b = 1, c = 1;
+    for (int i = 0; i < 4096; ++i) {
+      st[i] = c;
+      c = gl::mul(c, w4096);
+    }
+    for (int i = 0; i < kTwEntries; ++i) {
+      lo[i] = a;
+      a = gl::mul(a, w28);
+      hi[i] = b;
+      b = gl::mul(b, wstep);
+    }
   }
+}
+
+NttTables ntt_tables_view(uint64_t* dev) {
+  NttTables t;
+  t.d_fwd_st = dev;
+  t.d_fwd_lo = dev + 4096;
+  t.d_fwd_hi = dev + 4096 + kTwEntries;
+  t.d_inv_st = dev + kTwDirElems;
+  t.d_inv_lo = dev + kTwDirElems + 4096;
+  t.d_inv_hi = dev + kTwDirElems + 4096 + kTwEntries;
+  return t;
+}
+
+cudaError_t ntt_tables_init(NttTables* t) {
+  std::vector<uint64_t> h(2 * kTwDirElems);
+  ntt_tables_host(h.data());
   uint64_t* dev = nullptr;
-  cudaError_t e = cudaMalloc(&dev, sizeof h);
+  cudaError_t e = cudaMalloc(&dev, h.size() * 8);
   if (e != cudaSuccess) return e;
-  e = cudaMemcpy(dev, h, sizeof h, cudaMemcpyHostToDevice);
+  e = cudaMemcpy(dev, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(dev);
     return e;
   }
-  t->d_fwd_lo = dev;
-  t->d_fwd_hi = dev + 4096;
-  t->d_inv_lo = dev + 2 * 4096;
-  t->d_inv_hi = dev + 3 * 4096;
+  *t = ntt_tables_view(dev);
+  t->owned = true;
   return cudaSuccess;
 }
 
 void ntt_tables_free(NttTables* t) {
-  if (t->d_fwd_lo) cudaFree(t->d_fwd_lo);
+  if (t->owned && t->d_fwd_st) cudaFree(t->d_fwd_st);
   *t = NttTables{};
+}
+
+uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n) {
+  if (log_n <= 12) return 0;
+  const uint64_t N = 1ull << log_n;
+  return (log_n <= 24 ? 1 : 2) * n_cols * N;
 }
 
 cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t in_stride,
@@ -322,14 +381,11 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
     return cudaGetLastError();
   }
   const uint64_t ninv = inverse ? gl::inv(N) : 1;
-  PassArgs a{};
-  a.tw_lo = inverse ? t.d_inv_lo : t.d_fwd_lo;
-  a.tw_hi = inverse ? t.d_inv_hi : t.d_fwd_hi;
   if (log_n <= 12) {
     // one pass; the lanes are the columns
+    PassArgs a = base_args(t, inverse);
     a.in = in;
     a.out = out;
-    a.in_col = a.out_col = 0;
     a.in_lane = in_stride;
     a.in_m = 1;
     a.out_lane = out_stride;
@@ -337,52 +393,103 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
     a.n_lanes = n_cols;
     a.flat_lane = 0;  // lanes are whole columns
     a.in_valid = n_valid;
-    a.tw_shift = -1;
     a.scale = ninv;
     return launch_pass_dyn(log_n, a, inverse, 1, s);
   }
   if (!scratch) return cudaErrorInvalidValue;
-  const int l1 = log_n / 2, l2 = log_n - l1;
-  const uint64_t N1 = 1ull << l1, N2 = 1ull << l2;
-  // pass 1: DFT_{N2} over k2 (stride N1), lanes k1; transposed store into scratch
+  if (log_n <= 24) {
+    const int l1 = log_n / 2, l2 = log_n - l1;
+    const uint64_t N1 = 1ull << l1, N2 = 1ull << l2;
+    // pass 1: DFT_{N2} over k2 (stride N1), lanes k1; transposed store into scratch
+    PassArgs a = base_args(t, inverse);
+    a.in = in;
+    a.out = scratch;
+    a.in_col = in_stride;
+    a.out_col = N;
+    a.in_lane = 1;
+    a.in_m = N1;
+    a.out_lane = 1;
+    a.out_i = N1;
+    a.n_lanes = N1;
+    a.flat_lane = 1;  // flat index k = k2*N1 + k1
+    a.in_valid = n_valid;
+    a.sparse_nz = sparse_nz_for(n_valid, N, N1, N2);
+    a.tw_log = log_n;
+    cudaError_t e = launch_pass_dyn(l2, a, inverse, n_cols, s);
+    if (e != cudaSuccess) return e;
+    // pass 2: DFT_{N1} over contiguous rows, lanes i2; natural-order store
+    PassArgs b = base_args(t, inverse);
+    b.in = scratch;
+    b.out = out;
+    b.in_col = N;
+    b.out_col = out_stride;
+    b.in_lane = N1;
+    b.in_m = 1;
+    b.out_lane = 1;
+    b.out_i = N2;
+    b.n_lanes = N2;
+    b.flat_lane = N1;
+    b.in_valid = N;
+    b.scale = ninv;
+    return launch_pass_dyn(l1, b, inverse, n_cols, s);
+  }
+  // three passes: N = A * B * C
+  const int lc = (log_n + 2) / 3, lb = (log_n - lc + 1) / 2, la = log_n - lc - lb;
+  const uint64_t A = 1ull << la, B = 1ull << lb, C = 1ull << lc, AB = A * B, BC = B * C;
+  uint64_t* s1 = scratch;
+  uint64_t* s2 = scratch + (uint64_t)n_cols * N;
+  // pass 1: DFT_C over k3 (stride AB), lanes k1' < AB, twiddle w_N^{i3 k1'} -> s1[i3*AB + k1']
+  PassArgs a = base_args(t, inverse);
   a.in = in;
-  a.out = scratch;
+  a.out = s1;
   a.in_col = in_stride;
   a.out_col = N;
   a.in_lane = 1;
-  a.in_m = N1;
+  a.in_m = AB;
   a.out_lane = 1;
-  a.out_i = N1;
-  a.n_lanes = N1;
-  a.flat_lane = 1;  // flat index k = k2*N1 + k1
+  a.out_i = AB;
+  a.n_lanes = AB;
+  a.flat_lane = 1;
   a.in_valid = n_valid;
-  {
-    // points k2 >= ceil(n_valid / N1) are zero; the first radix-16 stage reads
-    // k2 = j + r*N2/16, so at most ceil(.. / (N2/16)) of its 16 inputs are non-zero
-    const uint64_t m_nz = (n_valid + N1 - 1) / N1, G = N2 / 16;
-    const uint64_t nz = (m_nz + G - 1) / G;
-    a.sparse_nz = (n_valid < N && nz <= 2) ? (int)(nz ? nz : 1) : 0;
-  }
-  a.tw_shift = 24 - log_n;
-  a.scale = 1;
-  cudaError_t e = launch_pass_dyn(l2, a, inverse, n_cols, s);
+  a.sparse_nz = sparse_nz_for(n_valid, N, AB, C);
+  a.tw_log = log_n;
+  cudaError_t e = launch_pass_dyn(lc, a, inverse, n_cols, s);
   if (e != cudaSuccess) return e;
-  // pass 2: DFT_{N1} over contiguous rows, lanes i2; natural-order store
-  a.in = scratch;
-  a.out = out;
-  a.in_col = N;
-  a.out_col = out_stride;
-  a.in_lane = N1;
-  a.in_m = 1;
-  a.out_lane = 1;
-  a.out_i = N2;
-  a.n_lanes = N2;
-  a.flat_lane = N1;
-  a.in_valid = N;
-  a.sparse_nz = 0;
-  a.tw_shift = -1;
-  a.scale = ninv;
-  return launch_pass_dyn(l1, a, inverse, n_cols, s);
+  // pass 2: per (column, i3): DFT_B over k2 (stride A) of lanes k1 < A, twiddle
+  // w_{AB}^{i2 k1}, stored at s2[col*N + (i2*C + i3)*A + k1]
+  PassArgs b = base_args(t, inverse);
+  b.in = s1;
+  b.out = s2;
+  b.y_sub = (uint32_t)C;
+  b.in_col = N;
+  b.in_sub = AB;
+  b.out_col = N;
+  b.out_sub = A;
+  b.in_lane = 1;
+  b.in_m = A;
+  b.out_lane = 1;
+  b.out_i = C * A;
+  b.n_lanes = A;
+  b.flat_lane = 1;
+  b.in_valid = AB;
+  b.tw_log = la + lb;
+  e = launch_pass_dyn(lb, b, inverse, (uint64_t)n_cols * C, s);
+  if (e != cudaSuccess) return e;
+  // pass 3: DFT_A over each contiguous row h' = i2*C + i3, stored at i1*BC + h'
+  PassArgs c = base_args(t, inverse);
+  c.in = s2;
+  c.out = out;
+  c.in_col = N;
+  c.out_col = out_stride;
+  c.in_lane = A;
+  c.in_m = 1;
+  c.out_lane = 1;
+  c.out_i = BC;
+  c.n_lanes = BC;
+  c.flat_lane = A;
+  c.in_valid = N;
+  c.scale = ninv;
+  return launch_pass_dyn(la, c, inverse, n_cols, s);
 }
 
 cudaError_t scale_by_powers(const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t stride, uint64_t n,

@@ -10,26 +10,41 @@
 
 namespace sg {
 
+static constexpr int kMaxLogN = 28;     // largest transform (three passes above 2^24)
+static constexpr int kTwBaseLog = 28;   // global twiddles are powers of w28 = w_{2^28}
+static constexpr int kTwSplit = 14;     // w28^E = lo[E & (2^14-1)] * hi[E >> 14]
+static constexpr int kTwEntries = 1 << kTwSplit;
+
 struct NttTables {
-  // w24 = primitive 2^24-th root; lo[i] = w24^i, hi[i] = w24^(4096 i), i < 4096,
-  // and the same for w24^-1. Any w_N^e with N <= 2^24 is lo[E & 4095] * hi[E >> 12]
-  // with E = e * 2^(24 - log N) mod 2^24.
+  // Per direction (forward: w, inverse: w^-1):
+  //   st[i] = w_4096^i (i < 4096)       — in-CTA Stockham stage twiddles
+  //   lo[i] = w28^i, hi[i] = w28^(2^14 i) (i < 2^14) — any w_N^e, N <= 2^28
+  uint64_t* d_fwd_st = nullptr;
   uint64_t* d_fwd_lo = nullptr;
   uint64_t* d_fwd_hi = nullptr;
+  uint64_t* d_inv_st = nullptr;
   uint64_t* d_inv_lo = nullptr;
   uint64_t* d_inv_hi = nullptr;
+  bool owned = false;
 };
 
-static constexpr int kMaxLogN = 24;
+// Elements of one direction's block: st (4096) + lo + hi.
+static constexpr uint64_t kTwDirElems = 4096 + 2 * kTwEntries;
 
+// Host: fill `out` (2 * kTwDirElems u64: forward block, then inverse block).
+void ntt_tables_host(uint64_t* out);
+// Point a table struct at a device copy of ntt_tables_host's layout.
+NttTables ntt_tables_view(uint64_t* dev);
 cudaError_t ntt_tables_init(NttTables* t);
 void ntt_tables_free(NttTables* t);
+
+// Scratch (in elements) ntt_batch needs for n_cols columns of 2^log_n.
+uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n);
 
 // Transform `n_cols` columns of length 2^log_n. Column c of the input starts at
 // in + c*in_stride, of the output at out + c*out_stride. Input entries at index
 // >= n_valid are treated as zero (zero-padded forward transform). `scratch`
-// must hold n_cols * 2^log_n elements when log_n > 12 (two-pass transform);
-// in == out is allowed. Returns cudaSuccess or the launch error.
+// must hold ntt_scratch_elems(n_cols, log_n) elements; in == out is allowed.
 cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t in_stride,
                       uint64_t out_stride, int log_n, bool inverse, uint64_t n_valid, uint64_t* scratch,
                       cudaStream_t s);
@@ -39,3 +54,14 @@ cudaError_t scale_by_powers(const uint64_t* in, uint64_t* out, uint32_t n_cols, 
                             uint64_t g, cudaStream_t s);
 
 }  // namespace sg
+
+#if defined(__CUDACC__)
+#include "gl.cuh"
+namespace sg {
+// w_N^e for N = 2^log_n <= 2^28 (any e; reduced mod N) from the two-level tables.
+__device__ __forceinline__ uint64_t tw_pow(const uint64_t* lo, const uint64_t* hi, uint64_t e, int log_n) {
+  const uint64_t E = (e << (kTwBaseLog - log_n)) & ((1ull << kTwBaseLog) - 1);
+  return gl::mul(__ldg(lo + (E & (kTwEntries - 1))), __ldg(hi + (E >> kTwSplit)));
+}
+}  // namespace sg
+#endif

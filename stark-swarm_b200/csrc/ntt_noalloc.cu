@@ -9,7 +9,7 @@
 // transpose buffer between the passes and the twiddle tables live in
 // file-scope static device arrays of fixed size, so nothing is allocated per
 // call. The arrays are created when the library is loaded and every GPU that
-// loads it keeps them (kNoAllocScratchElems * 8 bytes + 128 KiB) until exit.
+// loads it keeps them (kNoAllocScratchElems * 8 bytes + 576 KiB) until exit.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -27,7 +27,7 @@ constexpr size_t kNoAllocScratchElems = size_t(1) << 20;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) uint64_t g_noalloc_scratch[kNoAllocScratchElems];
-static __device__ __align__(256) uint64_t g_noalloc_twiddles[4 * 4096];
+static __device__ __align__(256) uint64_t g_noalloc_twiddles[2 * sg::kTwDirElems];
 
 struct DeviceSlot {
   bool ready = false;
@@ -36,7 +36,7 @@ struct DeviceSlot {
 };
 DeviceSlot g_slots[kMaxDevices];
 std::mutex g_mu;
-uint64_t g_host_twiddles[4 * 4096];  // same layout as sg::NttTables: fwd lo, fwd hi, inv lo, inv hi
+uint64_t g_host_twiddles[2 * sg::kTwDirElems];  // layout of sg::ntt_tables_host
 bool g_host_twiddles_ready = false;
 
 // Once per device, with that device current: resolve the device addresses of
@@ -47,19 +47,7 @@ int setup_device(int dev) {
   DeviceSlot& s = g_slots[dev];
   if (s.ready) return SG_OK;
   if (!g_host_twiddles_ready) {
-    const uint64_t w = gl::root_of_unity(24), wi = gl::inv(w);
-    const uint64_t w4096 = gl::pow(w, 4096), wi4096 = gl::pow(wi, 4096);
-    uint64_t a = 1, b = 1, c = 1, d = 1;
-    for (int i = 0; i < 4096; ++i) {
-      g_host_twiddles[i] = a;
-      a = gl::mul(a, w);
-      g_host_twiddles[4096 + i] = b;
-      b = gl::mul(b, w4096);
-      g_host_twiddles[2 * 4096 + i] = c;
-      c = gl::mul(c, wi);
-      g_host_twiddles[3 * 4096 + i] = d;
-      d = gl::mul(d, wi4096);
-    }
+    sg::ntt_tables_host(g_host_twiddles);
     g_host_twiddles_ready = true;
   }
   uint64_t* scratch = nullptr;
@@ -90,7 +78,7 @@ extern "C" int sg_ntt_noalloc(const uint64_t* d_in, uint64_t* d_out, size_t n_co
   if (!d_in || !d_out || n_cols == 0 || n_cols >= (size_t(1) << 31) || log_n > (size_t)sg::kMaxLogN)
     return SG_EINVAL;
   const size_t n = size_t(1) << log_n;
-  if (log_n > 12 && n_cols > kNoAllocScratchElems / n) return SG_ELIMIT;
+  if (sg::ntt_scratch_elems(n_cols, (int)log_n) > kNoAllocScratchElems) return SG_ELIMIT;
   if (!on_device(d_in) || !on_device(d_out)) return SG_EINVAL;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return SG_ECUDA;
@@ -98,11 +86,7 @@ extern "C" int sg_ntt_noalloc(const uint64_t* d_in, uint64_t* d_out, size_t n_co
   const int rc = setup_device(dev);
   if (rc != SG_OK) return rc;
   const DeviceSlot& s = g_slots[dev];
-  sg::NttTables t;
-  t.d_fwd_lo = s.twiddles;
-  t.d_fwd_hi = s.twiddles + 4096;
-  t.d_inv_lo = s.twiddles + 2 * 4096;
-  t.d_inv_hi = s.twiddles + 3 * 4096;
+  const sg::NttTables t = sg::ntt_tables_view(s.twiddles);
   // Pass 1 writes every scratch element that pass 2 reads, so the scratch left
   // by an earlier call needs no clearing.
   const cudaError_t e = sg::ntt_batch(t, d_in, d_out, (uint32_t)n_cols, n, n, (int)log_n, inverse != 0, n,

@@ -47,13 +47,12 @@ void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace
   require(pow2(n_trace), "lde: trace_len must be a power of 2");
   require(pow2(blowup) && blowup >= 2, "lde: blowup must be a power of 2 >= 2");
   const uint64_t n0 = n_trace * blowup;
-  require(log2_exact(n0) <= kMaxLogN, "lde: domain larger than 2^24");
+  require(log2_exact(n0) <= kMaxLogN, "lde: domain larger than 2^28");
   shift %= gl::P;
   require(shift != 0, "lde: shift must be nonzero");
   cudaStream_t s = c->stream;
   DBuf coef(w * n_trace, s);
-  const bool big = log2_exact(n0) > 12;
-  DBuf scratch(big ? w * n0 : 0, s);
+  DBuf scratch(std::max(ntt_scratch_elems(w, log2_exact(n0)), ntt_scratch_elems(w, log2_exact(n_trace))), s);
   ntt(c, d_trace, coef.p, (uint32_t)w, n_trace, n_trace, log2_exact(n_trace), true, n_trace, scratch.p);
   if (shift != 1) cuda_check(scale_by_powers(coef.p, coef.p, (uint32_t)w, n_trace, n_trace, shift, s), "coset scale");
   ntt(c, coef.p, d_out, (uint32_t)w, n_trace, n0, log2_exact(n0), false, n_trace, scratch.p);
@@ -75,14 +74,14 @@ void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_
   require(pow2(n_trace) && pow2(blowup), "merge: sizes must be powers of 2");
   require(phi_mode >= 0 && phi_mode <= 2, "merge: bad phi mode");
   const uint64_t n = n_trace * blowup;
-  require(log2_exact(n) <= kMaxLogN, "merge: domain larger than 2^24");
+  require(log2_exact(n) <= kMaxLogN, "merge: domain larger than 2^28");
   cudaStream_t s = c->stream;
   if (!phi_live(phi_mode, n)) {
     cuda_check(cudaMemsetAsync(d_c, 0, n * 8, s), "memset");
     return;
   }
   DBuf phi(n, s);
-  DBuf scratch(log2_exact(n) > 12 ? n : 0, s);
+  DBuf scratch(ntt_scratch_elems(1, log2_exact(n)), s);
   if (air == SG_AIR_HASH_ROLLUP) {
     cuda_check(hash_rollup_phi(d_lde, n, blowup, lambdas, phi.p, s), "phi");
   } else {
@@ -130,7 +129,7 @@ std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t
   const uint64_t L = p.schedule_len;
   require(p.stir != 0, "stir_prove: only the STIR branch (params.stir = true) is implemented");
   require(L >= 1 && L <= SG_MAX_SCHEDULE, "stir_prove: empty or oversized schedule");
-  require(pow2(n0) && n0 >= 2 && log2_exact(n0) <= kMaxLogN, "stir_prove: n0 must be a power of 2 in [2, 2^24]");
+  require(pow2(n0) && n0 >= 2 && log2_exact(n0) <= kMaxLogN, "stir_prove: n0 must be a power of 2 in [2, 2^28]");
   require(p.s0 <= (1u << 20), "stir_prove: s0 too large");
   std::vector<uint64_t> sizes{n0};
   for (uint64_t i = 0; i < L; ++i) {
@@ -161,7 +160,9 @@ std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t
   const gl::Fp6 z = tr.challenge_ext("z_fp3");
 
   const uint64_t work = std::max<uint64_t>(n0, 6 * sizes[1]);
-  DBuf coef(work, s), scratch(log2_exact(n0) > 12 ? work : 0, s);
+  uint64_t scratch_len = ntt_scratch_elems(1, log2_exact(n0));
+  for (uint64_t i = 1; i <= L; ++i) scratch_len = std::max(scratch_len, ntt_scratch_elems(6, log2_exact(sizes[i])));
+  DBuf coef(work, s), scratch(scratch_len, s);
   uint64_t part_len = 0;
   for (uint64_t i = 0; i < L; ++i) part_len = std::max<uint64_t>(part_len, ood_partials_len(sizes[i], (int)p.schedule[i]));
   DBuf partials(part_len, s);
@@ -378,21 +379,68 @@ std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* le
 // prove_ds_ksk_binding (swarm-dns/src/prover.rs:512-585): multi-block trace on the
 // host (sha256_air.rs:429-472), then LDE x32 -> deep_ali_merge_sha256 with
 // lambda_j = j + 1 -> STIR with build_params(n0, fs_binding) on the device.
+// deep_ali_merge_sha256 without materialising the LDE: LDE point i = r + blowup a
+// lies on coset r, whose evaluations are NTT_{n_trace}(c_k w_n0^{rk}), and point
+// i + blowup is point a + 1 of the same coset. Each coset is produced, folded into
+// Phi[r + blowup a] by the constraint kernel, and dropped.
+void merge_sha256_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, uint64_t blowup, uint64_t n_blocks,
+                         const uint64_t* lambdas, int phi_mode, uint64_t* d_c) {
+  const uint64_t W = sha::WIDTH, n = n_trace * blowup;
+  const unsigned lt = log2_exact(n_trace), ln = log2_exact(n);
+  require(pow2(n_trace) && pow2(blowup) && ln <= kMaxLogN, "merge: bad sizes");
+  cudaStream_t s = c->stream;
+  if (!phi_live(phi_mode, n)) {
+    cuda_check(cudaMemsetAsync(d_c, 0, n * 8, s), "memset");
+    return;
+  }
+  std::vector<uint64_t> lam(lambdas, lambdas + sha::NUM_CONSTRAINTS);
+  for (auto& x : lam) x %= gl::P;
+  DBuf d_lam(lam.size(), s), phi(n, s), coef(W * n_trace, s), ev(W * n_trace, s);
+  DBuf scratch(std::max(ntt_scratch_elems(W, lt), ntt_scratch_elems(1, ln)), s);
+  cuda_check(cudaMemcpyAsync(d_lam.p, lam.data(), lam.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+  ntt(c, d_trace, coef.p, (uint32_t)W, n_trace, n_trace, lt, true, n_trace, scratch.p);
+  const uint64_t w_n = gl::root_of_unity(ln);
+  for (uint64_t r = 0; r < blowup; ++r) {
+    const uint64_t* evals = d_trace;  // coset 0 holds the trace values themselves
+    if (r > 0) {
+      cuda_check(scale_by_powers(coef.p, ev.p, (uint32_t)W, n_trace, n_trace, gl::pow(w_n, r), s), "coset twist");
+      ntt(c, ev.p, ev.p, (uint32_t)W, n_trace, n_trace, lt, false, n_trace, scratch.p);
+      evals = ev.p;
+    }
+    cuda_check(sha256_phi_points(evals, n_trace, 1, 1, n_blocks, d_lam.p, phi.p, blowup, r, s), "coset phi");
+  }
+  ntt(c, phi.p, phi.p, 1, n, n, ln, true, n, scratch.p);
+  cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
+  ntt(c, d_c, d_c, 1, n, n, ln, false, n > n_trace ? n - n_trace : n, scratch.p);
+  cuda_check(cudaStreamSynchronize(s), "sync");  // lam (host) must outlive the copy
+}
+
 std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
                                           int phi_mode, bool self_verify, uint8_t digest[32]) {
   std::vector<uint64_t> trace;
   uint64_t n_blocks = 0;
   const uint64_t n_trace = sha256_build_trace(msg, len, &trace, &n_blocks, digest);
   const uint64_t blowup = 32, n0 = n_trace * blowup;
-  require(log2_exact(n0) <= kMaxLogN, "prove_sha256: message too long for a 2^24 domain");
+  require(log2_exact(n0) <= kMaxLogN, "prove_sha256: message too long for a 2^28 domain");
   cudaStream_t s = c->stream;
-  DBuf d_trace(trace.size(), s), d_lde((uint64_t)sha::WIDTH * n0, s), d_c(n0, s);
+  const uint64_t lde_bytes = (uint64_t)sha::WIDTH * n0 * 8;
+  const bool cosets = c->wide_merge == SG_WIDE_MERGE_COSETS ||
+                      (c->wide_merge == SG_WIDE_MERGE_AUTO && lde_bytes > (2ull << 30));
+  DBuf d_trace(trace.size(), s), d_c(n0, s);
   cuda_check(cudaMemcpyAsync(d_trace.p, trace.data(), trace.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
-  lde_device(c, d_trace.p, sha::WIDTH, n_trace, blowup, 1, d_lde.p);
   std::vector<uint64_t> lam(sha::NUM_CONSTRAINTS);
   for (uint64_t j = 0; j < lam.size(); ++j) lam[j] = j + 1;  // comb_coeffs (prover.rs:100-102)
-  merge_device(c, SG_AIR_SHA256, d_lde.p, sha::WIDTH, n_trace, blowup, lam.data(), lam.size(), phi_mode, d_c.p,
-               n_blocks);
+  if (cosets) {
+    merge_sha256_cosets(c, d_trace.p, n_trace, blowup, n_blocks, lam.data(), phi_mode, d_c.p);
+  } else {
+    DBuf d_lde((uint64_t)sha::WIDTH * n0, s);
+    lde_device(c, d_trace.p, sha::WIDTH, n_trace, blowup, 1, d_lde.p);
+    merge_device(c, SG_AIR_SHA256, d_lde.p, sha::WIDTH, n_trace, blowup, lam.data(), lam.size(), phi_mode, d_c.p,
+                 n_blocks);
+  }
+  cuda_check(cudaStreamSynchronize(s), "sync");
+  trace.clear();
+  trace.shrink_to_fit();
   sg_fri_params p;
   sg_build_params(n0, fs_binding, 1, &p);
   std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);

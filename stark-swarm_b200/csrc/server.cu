@@ -141,6 +141,7 @@ int sg_server_create(sg_ctx* ctx, int n_streams, uint64_t hbm_budget_bytes, sg_s
     w->device = ctx->device;
     w->tw = ctx->tw;
     w->owns_tables = false;
+    w->wide_merge = ctx->wide_merge;
     if (cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
       delete w;
       sg_server_destroy(s);

@@ -161,16 +161,22 @@ __device__ __forceinline__ uint64_t xor_poly(uint64_t x, uint64_t y) {
   return gl::sub(gl::add(x, y), gl::add(gl::mul(x, y), gl::mul(x, y)));
 }
 
-__global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n,
-                                                         uint64_t blowup, uint64_t n_blocks,
-                                                         const uint64_t* __restrict__ lam, uint64_t* __restrict__ phi) {
+// Point i of a column-major evaluation buffer (n points per column): cur = point
+// i, nxt = point (i + step) mod n, trace_row = i / row_div, result to
+// phi[out_off + i * out_stride]. The full LDE uses (step, row_div) = (blowup,
+// blowup); one coset r of it (points r + blowup a) uses (1, 1) with
+// out_off = r, out_stride = blowup.
+__global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n, uint64_t step,
+                                                         uint64_t row_div, uint64_t n_blocks,
+                                                         const uint64_t* __restrict__ lam, uint64_t* __restrict__ phi,
+                                                         uint64_t out_stride, uint64_t out_off) {
   using namespace sha;
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint64_t j = (i + blowup) & (n - 1);
+  const uint64_t j = (i + step) & (n - 1);
   auto C = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + i); };
   auto X = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + j); };
-  const uint64_t row = i / blowup, blk = row / ROWS_PER_BLOCK, br = row % ROWS_PER_BLOCK;
+  const uint64_t row = i / row_div, blk = row / ROWS_PER_BLOCK, br = row % ROWS_PER_BLOCK;
   const bool past = blk >= n_blocks;
   const bool comp = !past && br < 64, fin = !past && br == 64, sched = !past && br >= 15 && br <= 62;
   Acc acc{lam, 0, 0};
@@ -305,7 +311,7 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
   } else {
     acc.zeros(4);
   }
-  phi[i] = acc.phi;
+  phi[out_off + i * out_stride] = acc.phi;
 }
 
 bool g_k_uploaded[64] = {false};
@@ -348,6 +354,12 @@ uint64_t sha256_build_trace(const uint8_t* msg, uint64_t len, std::vector<uint64
 
 cudaError_t sha256_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, uint64_t n_blocks, const uint64_t* lambdas,
                        uint64_t* phi, cudaStream_t s) {
+  return sha256_phi_points(lde, n, blowup, blowup, n_blocks, lambdas, phi, 1, 0, s);
+}
+
+cudaError_t sha256_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, uint64_t row_div, uint64_t n_blocks,
+                              const uint64_t* lambdas, uint64_t* phi, uint64_t out_stride, uint64_t out_off,
+                              cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
@@ -361,7 +373,8 @@ cudaError_t sha256_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, uint64_
   }
   const unsigned T = 128;
   SG_LAUNCH_SCOPE("merge_phi", s);
-  sha256_phi_kernel<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(lde, n, blowup, n_blocks, lambdas, phi);
+  sha256_phi_kernel<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(evals, n, step, row_div, n_blocks, lambdas, phi,
+                                                                out_stride, out_off);
   return cudaGetLastError();
 }
 

@@ -1,6 +1,7 @@
 // stir.cu — STIR out-of-domain evaluation and fold kernels.
 #include "dft.cuh"
 #include "keccak.cuh"
+#include "ntt.cuh"
 #include "stir.cuh"
 #include "counters.hpp"
 
@@ -122,8 +123,7 @@ __global__ void fold_kernel(FoldArgs a) {
     dft_reg<M, true>(x[q]);
   }
   // w_n^{-b}
-  const uint64_t E = (b << (24 - a.log_n)) & ((1ull << 24) - 1);
-  const uint64_t obinv = gl::mul(__ldg(a.tw_inv_lo + (E & 4095)), __ldg(a.tw_inv_hi + (E >> 12)));
+  const uint64_t obinv = tw_pow(a.tw_inv_lo, a.tw_inv_hi, b, a.log_n);
   constexpr unsigned MINV = 192u - LM;  // 1/M = 2^{-LM} = 2^{192-LM}
   if (a.tuples) {
     uint64_t p = 1;
@@ -234,7 +234,7 @@ cudaError_t ood_evaluate(const uint64_t* coeffs, bool base, uint64_t n, int m, c
 }
 
 cudaError_t stir_fold(const FoldArgs& a, cudaStream_t s) {
-  if (a.n % a.m || a.log_n > 24) return cudaErrorInvalidValue;
+  if (a.n % a.m || a.log_n > kMaxLogN) return cudaErrorInvalidValue;
   switch (a.m) {
     case 2: return fold_launch<2>(a, s);
     case 4: return fold_launch<4>(a, s);

@@ -34,7 +34,7 @@ def test_ntt_matches_oracle(ctx, log_n, inverse):
         assert np.array_equal(got[c], O.ntt(x[c], inverse)), c
 
 
-@pytest.mark.parametrize("log_n", [17, 20, 23, 24])
+@pytest.mark.parametrize("log_n", [17, 20, 23, 24, 25, 26])
 def test_ntt_large_round_trip_and_oracle(ctx, log_n):
     rng = np.random.default_rng(log_n)
     x = rand_field(rng, (1, 1 << log_n))
@@ -259,3 +259,20 @@ def test_full_size_stir_random_f0_consistent(sgpu, ctx):
     f0 = rand_field(rng, n0)
     pi = rng.bytes(32)
     assert ctx.deep_fri_prove(f0, n0, sgpu.build_params(n0, pi)) == O.stir_prove(f0, O.build_params(n0, pi))
+
+
+def test_lde_into_three_pass_domain(ctx):
+    # 2 x 2^13 -> blowup 4096 = 2^25 points: zero-padded forward three-pass transform
+    rng = np.random.default_rng(25)
+    tr = rand_field(rng, (2, 1 << 13))
+    out = ctx.lde(tr, 1 << 12, 1)
+    L = O.lib()
+    w = int(L.orc_root_of_unity(25))
+    for c in range(2):
+        coeffs = [int(v) for v in O.ntt(tr[c], inverse=True)]
+        for i in (0, 1, 4095, 4096, (1 << 25) - 1):
+            x, acc = pow(w, i, P), 0
+            for cf in reversed(coeffs):
+                acc = (acc * x + cf) % P
+            assert int(out[c, i]) == acc, (c, i)
+    assert np.array_equal(out[:, ::4096], tr)  # coset 0 of the LDE is the trace itself

@@ -47,3 +47,29 @@ def test_prove_sha256_matches_oracle(sgpu, ctx, msg):
     n0 = tr.shape[1] * 32
     assert sgpu.deep_fri_verify(sgpu.build_params(n0, fsb), proof)
     assert O.stir_verify(proof, O.build_params(n0, fsb))
+
+
+@pytest.mark.parametrize("msg", [b"abc", bytes(range(200)), b"w" * 2000])
+def test_coset_sliced_merge_matches_materialised(sgpu, ctx, msg):
+    fsb = hashlib.sha3_256(b"coset" + msg).digest()
+    want, wd = O.prove_sha256(msg, fsb)
+    try:
+        ctx.set_option(sgpu.OPT_WIDE_MERGE, sgpu.WIDE_MERGE_COSETS)
+        got, gd = ctx.prove_sha256(msg, fsb)
+    finally:
+        ctx.set_option(sgpu.OPT_WIDE_MERGE, sgpu.WIDE_MERGE_AUTO)
+    assert got == want and gd == wd
+
+
+def test_large_sha256_trace_proof(sgpu, ctx):
+    # 2^14-row trace (128 blocks): n0 = 2^19, taken by the coset path; digest and
+    # self-verification (inside the call) and acceptance by the oracle verifier
+    msg = bytes(np.random.default_rng(14).integers(0, 256, 128 * 64 - 9, dtype=np.uint8))
+    fsb = hashlib.sha3_256(b"large").digest()
+    ctx.set_option(sgpu.OPT_WIDE_MERGE, sgpu.WIDE_MERGE_COSETS)
+    try:
+        proof, digest = ctx.prove_sha256(msg, fsb)
+    finally:
+        ctx.set_option(sgpu.OPT_WIDE_MERGE, sgpu.WIDE_MERGE_AUTO)
+    assert digest == hashlib.sha256(msg).digest()
+    assert O.stir_verify(proof, O.build_params(1 << 19, fsb))
