@@ -158,6 +158,14 @@ int sg_merge_sha256(sg_ctx* ctx, const uint64_t* lde, size_t n_trace, size_t blo
 int sg_sha256_trace(const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height, size_t* n_blocks,
                     uint8_t digest[32]);
 
+/* The same trace (build_sha256_trace_multi, sha256_air.rs:429-472) with the
+ * column expansion on the device: the host runs only the compressions and ships
+ * one 2368-byte witness per block; `trace` (756 x height elements, host or device)
+ * receives the cells. SG_ESPACE (height, n_blocks, digest still set) when cap is
+ * too small. */
+int sg_sha256_trace_gpu(sg_ctx* ctx, const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height,
+                        size_t* n_blocks, uint8_t digest[32]);
+
 /* Core of prove_ds_ksk_binding (swarm-dns/src/prover.rs:512-585): SHA-256 AIR trace
  * of `msg` -> LDE x32 -> merge (lambda_j = j+1) -> STIR with
  * build_params(n0, fs_binding). Self-verified before return; `digest` receives the

@@ -97,7 +97,8 @@ EXPORTS = (
     "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_ctx_set_option", "sg_last_error",
     "sg_kernel_launches",
     "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
-    "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_prove_sha256", "sg_merkle_commit",
+    "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_sha256_trace_gpu", "sg_prove_sha256",
+    "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
 )
@@ -156,6 +157,7 @@ def lib():
                                  ctypes.POINTER(JobResult)]
     L.sg_sha256_trace.argtypes = [ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz),
                                   ctypes.c_char_p]
+    L.sg_sha256_trace_gpu.argtypes = [vp] + L.sg_sha256_trace.argtypes
     L.sg_prove_sha256.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz,
                                   ctypes.POINTER(sz), ctypes.c_char_p]
     L.sg_merkle_commit.argtypes = [vp, vp, sz, sz, sz, vp, sz, u64, ctypes.c_char_p, ctypes.POINTER(vp)]
@@ -372,6 +374,24 @@ class Context:
         self._check(self._lib.sg_merge(self._h, air, ip, w, n_trace, blowup, lam.ctypes.data, lam.size, phi_mode,
                                        op))
         return out
+
+    def sha256_trace(self, message: bytes, out=None):
+        """build_sha256_trace_multi with the column expansion on the GPU ->
+        ((756, height) trace, n_blocks, asserted digest). `out`, if given, is a
+        device tensor of at least 756 * height elements and receives the trace."""
+        nb = (len(message) + 9 + 63) // 64
+        height = 128
+        while height < 128 * nb:
+            height *= 2
+        if out is None:
+            out = np.empty((SHA256_WIDTH, height), dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        cap = SHA256_WIDTH * height
+        h, n = ctypes.c_size_t(), ctypes.c_size_t()
+        dg = ctypes.create_string_buffer(32)
+        self._check(self._lib.sg_sha256_trace_gpu(self._h, message, len(message), op, cap, ctypes.byref(h),
+                                                  ctypes.byref(n), dg))
+        return out, n.value, dg.raw
 
     def merge_sha256(self, lde, n_trace: int, blowup: int, lambdas, n_blocks: int, phi_mode=PHI_PARALLEL_GATE,
                      out=None):

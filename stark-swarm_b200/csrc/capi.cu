@@ -217,18 +217,38 @@ int sg_sha256_trace(const uint8_t* msg, size_t len, uint64_t* trace, size_t cap,
                     uint8_t digest[32]) {
   if ((!msg && len) || !height || !n_blocks || !digest) return SG_EINVAL;
   try {
-    std::vector<uint64_t> tr;
-    uint64_t nb = 0;
+    std::vector<sg::sha::BlockWitness> wit;
     uint8_t dg[32];
-    *height = (size_t)sg::sha256_build_trace(msg, len, &tr, &nb, dg);
-    *n_blocks = (size_t)nb;
+    const uint64_t h = sg::sha256_witness(msg, len, &wit, dg);
+    *height = (size_t)h;
+    *n_blocks = wit.size();
     memcpy(digest, dg, 32);
-    if (!trace || tr.size() > cap) return SG_ESPACE;
-    memcpy(trace, tr.data(), tr.size() * 8);
+    if (!trace || (uint64_t)sg::sha::WIDTH * h > cap) return SG_ESPACE;
+    sg::sha256_fill_host(wit.data(), wit.size(), h, trace);
     return SG_OK;
   } catch (const std::bad_alloc&) {
     return SG_ENOMEM;
   }
+}
+
+int sg_sha256_trace_gpu(sg_ctx* c, const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height,
+                        size_t* n_blocks, uint8_t digest[32]) {
+  return guarded(c, [&] {
+    sg::require((msg || !len) && height && n_blocks && digest, "sha256_trace_gpu: null argument");
+    std::vector<sg::sha::BlockWitness> wit;
+    const uint64_t h = sg::sha256_witness(msg, len, &wit, digest);
+    *height = (size_t)h;
+    *n_blocks = wit.size();
+    const uint64_t cells = (uint64_t)sg::sha::WIDTH * h;
+    if (!trace || cells > cap) throw sg::SgError{SG_ESPACE, "sha256_trace_gpu: trace buffer too small"};
+    Out dout(trace, cells, c->stream);
+    sg::DBuf d_wit((wit.size() * sizeof(sg::sha::BlockWitness) + 7) / 8, c->stream);
+    sg::cuda_check(cudaMemcpyAsync(d_wit.p, wit.data(), wit.size() * sizeof(sg::sha::BlockWitness),
+                                   cudaMemcpyHostToDevice, c->stream), "h2d");
+    sg::cuda_check(sg::sha256_expand((const sg::sha::BlockWitness*)d_wit.p, wit.size(), h, dout.d, c->stream),
+                   "sha256_expand");
+    dout.finish();
+  });
 }
 
 int sg_prove_sha256(sg_ctx* c, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,

@@ -54,6 +54,7 @@ struct PassArgs {
   const uint64_t* tw_st;      // w_4096^i (direction of the transform)
   const uint64_t* tw_lo;      // w28^i
   const uint64_t* tw_hi;      // w28^(2^14 i)
+  PowSpec pre;                // lo != nullptr: input at flat index k times g^k
 };
 
 // One Stockham stage of radix R over all K lanes of the tile.
@@ -167,8 +168,11 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
     }
     uint64_t lane = lane0 + l;
     uint64_t x = 0;
-    if (lane < a.n_lanes && (uint64_t)m * a.in_m + lane * a.flat_lane < a.in_valid)
+    const uint64_t flat = (uint64_t)m * a.in_m + lane * a.flat_lane;
+    if (lane < a.n_lanes && flat < a.in_valid) {
       x = in[lane * a.in_lane + (uint64_t)m * a.in_m];
+      if (a.pre.lo) x = gl::mul(x, pow_at(a.pre, flat));
+    }
     sm[l * Mp + padi(m)] = x;
   }
   __syncthreads();
@@ -270,20 +274,6 @@ __global__ void copy_cols_kernel(const uint64_t* in, uint64_t* out, uint32_t n_c
   }
 }
 
-__global__ void scale_powers_kernel(const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t stride,
-                                    uint64_t n, uint64_t g) {
-  // each thread scales 32 consecutive coefficients of one column
-  const uint64_t chunks = (n + 31) / 32;
-  uint64_t id = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (id >= chunks * n_cols) return;
-  uint64_t c = id / chunks, k0 = (id - c * chunks) * 32;
-  uint64_t p = gl::pow(g, k0);
-  for (uint64_t k = k0; k < k0 + 32 && k < n; ++k) {
-    out[c * stride + k] = gl::mul(in[c * stride + k], p);
-    p = gl::mul(p, g);
-  }
-}
-
 PassArgs base_args(const NttTables& t, bool inverse) {
   PassArgs a{};
   a.tw_st = inverse ? t.d_inv_st : t.d_fwd_st;
@@ -329,6 +319,19 @@ void ntt_tables_host(uint64_t* out) {
   }
 }
 
+void pow_tables_host(uint64_t g, uint64_t scale, uint64_t* out) {
+  uint64_t* lo = out;
+  uint64_t* hi = out + kTwEntries;
+  const uint64_t gstep = gl::pow(g, kTwEntries);
+  uint64_t a = scale % gl::P, b = 1;
+  for (int i = 0; i < kTwEntries; ++i) {
+    lo[i] = a;
+    a = gl::mul(a, g);
+    hi[i] = b;
+    b = gl::mul(b, gstep);
+  }
+}
+
 NttTables ntt_tables_view(uint64_t* dev) {
   NttTables t;
   t.d_fwd_st = dev;
@@ -369,21 +372,24 @@ uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n) {
 
 cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t in_stride,
                       uint64_t out_stride, int log_n, bool inverse, uint64_t n_valid, uint64_t* scratch,
-                      cudaStream_t s) {
+                      cudaStream_t s, const PowSpec* pre) {
   if (n_cols == 0) return cudaSuccess;
   if (log_n < 0 || log_n > kMaxLogN) return cudaErrorInvalidValue;
   const uint64_t N = 1ull << log_n;
   if (n_valid > N) n_valid = N;
-  if (log_n == 0) {
+  if (log_n == 0 && !pre) {
     if (in == out) return cudaSuccess;
     SG_LAUNCH_SCOPE("copy_cols", s);
     copy_cols_kernel<<<64, 256, 0, s>>>(in, out, n_cols, in_stride, out_stride, 1);
     return cudaGetLastError();
   }
   const uint64_t ninv = inverse ? gl::inv(N) : 1;
+  const PowSpec none{};
   if (log_n <= 12) {
-    // one pass; the lanes are the columns
+    // one pass; the lanes are the columns (a length-1 "transform" is the identity
+    // pass, used only to apply pre)
     PassArgs a = base_args(t, inverse);
+    a.pre = pre ? *pre : none;
     a.in = in;
     a.out = out;
     a.in_lane = in_stride;
@@ -394,7 +400,7 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
     a.flat_lane = 0;  // lanes are whole columns
     a.in_valid = n_valid;
     a.scale = ninv;
-    return launch_pass_dyn(log_n, a, inverse, 1, s);
+    return log_n == 0 ? launch_pass<0>(a, inverse, 1, s) : launch_pass_dyn(log_n, a, inverse, 1, s);
   }
   if (!scratch) return cudaErrorInvalidValue;
   if (log_n <= 24) {
@@ -415,6 +421,7 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
     a.in_valid = n_valid;
     a.sparse_nz = sparse_nz_for(n_valid, N, N1, N2);
     a.tw_log = log_n;
+    a.pre = pre ? *pre : none;
     cudaError_t e = launch_pass_dyn(l2, a, inverse, n_cols, s);
     if (e != cudaSuccess) return e;
     // pass 2: DFT_{N1} over contiguous rows, lanes i2; natural-order store
@@ -453,6 +460,7 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
   a.in_valid = n_valid;
   a.sparse_nz = sparse_nz_for(n_valid, N, AB, C);
   a.tw_log = log_n;
+  a.pre = pre ? *pre : none;
   cudaError_t e = launch_pass_dyn(lc, a, inverse, n_cols, s);
   if (e != cudaSuccess) return e;
   // pass 2: per (column, i3): DFT_B over k2 (stride A) of lanes k1 < A, twiddle
@@ -490,15 +498,6 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
   c.in_valid = N;
   c.scale = ninv;
   return launch_pass_dyn(la, c, inverse, n_cols, s);
-}
-
-cudaError_t scale_by_powers(const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t stride, uint64_t n,
-                            uint64_t g, cudaStream_t s) {
-  uint64_t threads = ((n + 31) / 32) * n_cols;
-  if (threads == 0) return cudaSuccess;
-  SG_LAUNCH_SCOPE("coset_scale", s);
-  scale_powers_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(in, out, n_cols, stride, n, g);
-  return cudaGetLastError();
 }
 
 }  // namespace sg

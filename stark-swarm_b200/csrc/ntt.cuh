@@ -38,6 +38,20 @@ NttTables ntt_tables_view(uint64_t* dev);
 cudaError_t ntt_tables_init(NttTables* t);
 void ntt_tables_free(NttTables* t);
 
+// Element-wise powers x[k] *= g^k (k = natural index inside the column), applied
+// to the input by the transform itself as pass 1 loads it. g^k = lo[E & (2^14-1)] * hi[E >> 14] with
+// E = ((k * mult) << shl) mod 2^28:
+//   g = w_{2^L}^r, a root of unity: the w28 tables of NttTables, mult = r, shl = 28 - L;
+//   any other g (the LDE shift): pow_tables_host(g), mult = 1, shl = 0, k < 2^28.
+struct PowSpec {
+  const uint64_t* lo = nullptr;
+  const uint64_t* hi = nullptr;
+  uint64_t mult = 1;
+  int shl = 0;
+};
+// Host: lo[i] = scale * g^i, hi[i] = g^(2^14 i) for i < 2^14 (out: 2 * 2^14 u64).
+void pow_tables_host(uint64_t g, uint64_t scale, uint64_t* out);
+
 // Scratch (in elements) ntt_batch needs for n_cols columns of 2^log_n.
 uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n);
 
@@ -45,13 +59,10 @@ uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n);
 // in + c*in_stride, of the output at out + c*out_stride. Input entries at index
 // >= n_valid are treated as zero (zero-padded forward transform). `scratch`
 // must hold ntt_scratch_elems(n_cols, log_n) elements; in == out is allowed.
+// `pre` (optional) multiplies input element k by g^k first.
 cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t in_stride,
                       uint64_t out_stride, int log_n, bool inverse, uint64_t n_valid, uint64_t* scratch,
-                      cudaStream_t s);
-
-// out[c*stride + k] = in[c*stride + k] * g^k for k < n (coset scaling of coefficients).
-cudaError_t scale_by_powers(const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t stride, uint64_t n,
-                            uint64_t g, cudaStream_t s);
+                      cudaStream_t s, const PowSpec* pre = nullptr);
 
 }  // namespace sg
 
@@ -62,6 +73,10 @@ namespace sg {
 __device__ __forceinline__ uint64_t tw_pow(const uint64_t* lo, const uint64_t* hi, uint64_t e, int log_n) {
   const uint64_t E = (e << (kTwBaseLog - log_n)) & ((1ull << kTwBaseLog) - 1);
   return gl::mul(__ldg(lo + (E & (kTwEntries - 1))), __ldg(hi + (E >> kTwSplit)));
+}
+__device__ __forceinline__ uint64_t pow_at(const PowSpec& p, uint64_t k) {
+  const uint64_t E = ((k * p.mult) << p.shl) & ((1ull << kTwBaseLog) - 1);
+  return gl::mul(__ldg(p.lo + (E & (kTwEntries - 1))), __ldg(p.hi + (E >> kTwSplit)));
 }
 }  // namespace sg
 #endif

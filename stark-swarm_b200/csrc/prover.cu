@@ -35,8 +35,9 @@ static unsigned log2_exact(uint64_t n) {
 static bool pow2(uint64_t n) { return n && !(n & (n - 1)); }
 
 static void ntt(sg_ctx* c, const uint64_t* in, uint64_t* out, uint32_t cols, uint64_t in_stride, uint64_t out_stride,
-                unsigned log_n, bool inverse, uint64_t n_valid, uint64_t* scratch) {
-  cuda_check(ntt_batch(c->tw, in, out, cols, in_stride, out_stride, (int)log_n, inverse, n_valid, scratch, c->stream),
+                unsigned log_n, bool inverse, uint64_t n_valid, uint64_t* scratch, const PowSpec* pre = nullptr) {
+  cuda_check(ntt_batch(c->tw, in, out, cols, in_stride, out_stride, (int)log_n, inverse, n_valid, scratch, c->stream,
+                       pre),
              "ntt");
 }
 
@@ -54,8 +55,21 @@ void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace
   DBuf coef(w * n_trace, s);
   DBuf scratch(std::max(ntt_scratch_elems(w, log2_exact(n0)), ntt_scratch_elems(w, log2_exact(n_trace))), s);
   ntt(c, d_trace, coef.p, (uint32_t)w, n_trace, n_trace, log2_exact(n_trace), true, n_trace, scratch.p);
-  if (shift != 1) cuda_check(scale_by_powers(coef.p, coef.p, (uint32_t)w, n_trace, n_trace, shift, s), "coset scale");
-  ntt(c, coef.p, d_out, (uint32_t)w, n_trace, n0, log2_exact(n0), false, n_trace, scratch.p);
+  // coset shift: coefficient k times shift^k, applied as the forward transform loads it
+  PowSpec pre;
+  DBuf tab;
+  std::vector<uint64_t> h_tab;
+  if (shift != 1) {
+    h_tab.resize(2 * kTwEntries);
+    pow_tables_host(shift, 1, h_tab.data());
+    tab.alloc(h_tab.size(), s);
+    cuda_check(cudaMemcpyAsync(tab.p, h_tab.data(), h_tab.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+    pre.lo = tab.p;
+    pre.hi = tab.p + kTwEntries;
+  }
+  ntt(c, coef.p, d_out, (uint32_t)w, n_trace, n0, log2_exact(n0), false, n_trace, scratch.p,
+      shift != 1 ? &pre : nullptr);
+  if (shift != 1) cuda_check(cudaStreamSynchronize(s), "sync");  // h_tab must outlive its copy
 }
 
 // ------------------------------------------------------------------ merge
@@ -399,12 +413,16 @@ void merge_sha256_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, u
   DBuf scratch(std::max(ntt_scratch_elems(W, lt), ntt_scratch_elems(1, ln)), s);
   cuda_check(cudaMemcpyAsync(d_lam.p, lam.data(), lam.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
   ntt(c, d_trace, coef.p, (uint32_t)W, n_trace, n_trace, lt, true, n_trace, scratch.p);
-  const uint64_t w_n = gl::root_of_unity(ln);
   for (uint64_t r = 0; r < blowup; ++r) {
     const uint64_t* evals = d_trace;  // coset 0 holds the trace values themselves
     if (r > 0) {
-      cuda_check(scale_by_powers(coef.p, ev.p, (uint32_t)W, n_trace, n_trace, gl::pow(w_n, r), s), "coset twist");
-      ntt(c, ev.p, ev.p, (uint32_t)W, n_trace, n_trace, lt, false, n_trace, scratch.p);
+      // coefficient k times w_n^(r k), applied as the transform loads it
+      PowSpec twist;
+      twist.lo = c->tw.d_fwd_lo;
+      twist.hi = c->tw.d_fwd_hi;
+      twist.mult = r;
+      twist.shl = kTwBaseLog - (int)ln;
+      ntt(c, coef.p, ev.p, (uint32_t)W, n_trace, n_trace, lt, false, n_trace, scratch.p, &twist);
       evals = ev.p;
     }
     cuda_check(sha256_phi_points(evals, n_trace, 1, 1, n_blocks, d_lam.p, phi.p, blowup, r, s), "coset phi");
@@ -417,17 +435,23 @@ void merge_sha256_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, u
 
 std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
                                           int phi_mode, bool self_verify, uint8_t digest[32]) {
-  std::vector<uint64_t> trace;
-  uint64_t n_blocks = 0;
-  const uint64_t n_trace = sha256_build_trace(msg, len, &trace, &n_blocks, digest);
+  // the host runs the compressions; the 756 trace columns are expanded on the device
+  std::vector<sha::BlockWitness> wit;
+  const uint64_t n_trace = sha256_witness(msg, len, &wit, digest);
+  const uint64_t n_blocks = wit.size();
   const uint64_t blowup = 32, n0 = n_trace * blowup;
   require(log2_exact(n0) <= kMaxLogN, "prove_sha256: message too long for a 2^28 domain");
   cudaStream_t s = c->stream;
   const uint64_t lde_bytes = (uint64_t)sha::WIDTH * n0 * 8;
   const bool cosets = c->wide_merge == SG_WIDE_MERGE_COSETS ||
                       (c->wide_merge == SG_WIDE_MERGE_AUTO && lde_bytes > (2ull << 30));
-  DBuf d_trace(trace.size(), s), d_c(n0, s);
-  cuda_check(cudaMemcpyAsync(d_trace.p, trace.data(), trace.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+  DBuf d_trace((uint64_t)sha::WIDTH * n_trace, s), d_c(n0, s);
+  {
+    DBuf d_wit((n_blocks * sizeof(sha::BlockWitness) + 7) / 8, s);
+    cuda_check(cudaMemcpyAsync(d_wit.p, wit.data(), n_blocks * sizeof(sha::BlockWitness), cudaMemcpyHostToDevice, s),
+               "h2d");
+    cuda_check(sha256_expand((const sha::BlockWitness*)d_wit.p, n_blocks, n_trace, d_trace.p, s), "sha256_expand");
+  }
   std::vector<uint64_t> lam(sha::NUM_CONSTRAINTS);
   for (uint64_t j = 0; j < lam.size(); ++j) lam[j] = j + 1;  // comb_coeffs (prover.rs:100-102)
   if (cosets) {
@@ -438,9 +462,7 @@ std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_
     merge_device(c, SG_AIR_SHA256, d_lde.p, sha::WIDTH, n_trace, blowup, lam.data(), lam.size(), phi_mode, d_c.p,
                  n_blocks);
   }
-  cuda_check(cudaStreamSynchronize(s), "sync");
-  trace.clear();
-  trace.shrink_to_fit();
+  cuda_check(cudaStreamSynchronize(s), "sync");  // wit (host) must outlive its copy
   sg_fri_params p;
   sg_build_params(n0, fs_binding, 1, &p);
   std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);

@@ -7,8 +7,10 @@
 // every column) and folds the 766 constraint values into Phi(w^i) as it goes;
 // no constraint matrix is ever materialised. The emission order below is the
 // reference's (sha256_air.rs:956-1294) because lambda_j multiplies the j-th value.
+#include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <thread>
 
 #include "counters.hpp"
 #include "gl.cuh"
@@ -30,21 +32,25 @@ __constant__ uint32_t kK[64];
 static const uint32_t kIV[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
                                 0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
 
-// ------------------------------------------------------------------ host trace
-inline uint32_t rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
-inline uint32_t Sig0(uint32_t x) { return rotr(x, 2) ^ rotr(x, 13) ^ rotr(x, 22); }
-inline uint32_t Sig1(uint32_t x) { return rotr(x, 6) ^ rotr(x, 11) ^ rotr(x, 25); }
-inline uint32_t sig0(uint32_t x) { return rotr(x, 7) ^ rotr(x, 18) ^ (x >> 3); }
-inline uint32_t sig1(uint32_t x) { return rotr(x, 17) ^ rotr(x, 19) ^ (x >> 10); }
-inline uint32_t chf(uint32_t x, uint32_t y, uint32_t z) { return (x & y) ^ (~x & z); }
-inline uint32_t majf(uint32_t x, uint32_t y, uint32_t z) { return (x & y) ^ (x & z) ^ (y & z); }
+// ------------------------------------------------------------------ trace
+// Witness generation is split: the host runs the compressions (message schedule
+// and the 65 working states of every block, sha::BlockWitness, 2368 bytes a
+// block) and the 756 cells of each row are expanded from them by
+// sha256_row_cells, the same code on the host (sg_sha256_trace) and on the
+// device (sha256_expand_kernel), so a 2^20-row trace crosses PCIe as 19 MB of
+// block witnesses instead of 6.3 GB of cells.
+__host__ __device__ __forceinline__ uint32_t rotr(uint32_t x, int n) { return (x >> n) | (x << (32 - n)); }
+__host__ __device__ __forceinline__ uint32_t Sig0(uint32_t x) { return rotr(x, 2) ^ rotr(x, 13) ^ rotr(x, 22); }
+__host__ __device__ __forceinline__ uint32_t Sig1(uint32_t x) { return rotr(x, 6) ^ rotr(x, 11) ^ rotr(x, 25); }
+__host__ __device__ __forceinline__ uint32_t sig0(uint32_t x) { return rotr(x, 7) ^ rotr(x, 18) ^ (x >> 3); }
+__host__ __device__ __forceinline__ uint32_t sig1(uint32_t x) { return rotr(x, 17) ^ rotr(x, 19) ^ (x >> 10); }
+__host__ __device__ __forceinline__ uint32_t chf(uint32_t x, uint32_t y, uint32_t z) { return (x & y) ^ (~x & z); }
+__host__ __device__ __forceinline__ uint32_t majf(uint32_t x, uint32_t y, uint32_t z) {
+  return (x & y) ^ (x & z) ^ (y & z);
+}
 
-struct BlockState {
-  uint32_t w[64];
-  uint32_t st[65][8];  // working state before round t (st[64] = post-compression)
-};
-
-void run_block(const uint8_t* blk, const uint32_t iv[8], BlockState* b) {
+void run_block(const uint8_t* blk, const uint32_t iv[8], sha::BlockWitness* b) {
+  memcpy(b->iv, iv, 32);
   for (int i = 0; i < 16; ++i)
     b->w[i] = (uint32_t)blk[4 * i] << 24 | (uint32_t)blk[4 * i + 1] << 16 | (uint32_t)blk[4 * i + 2] << 8 |
               blk[4 * i + 3];
@@ -60,88 +66,84 @@ void run_block(const uint8_t* blk, const uint32_t iv[8], BlockState* b) {
   }
 }
 
-// fill_block (sha256_air.rs:648-937): one 128-row segment starting at `base`
-void fill_rows(uint64_t* tr, uint64_t h, uint64_t base, const BlockState& B, const uint32_t iv[8]) {
+// fill_block (sha256_air.rs:648-937), one row: block row `br` of the block whose
+// witness is B; kt = K[br] for compression rows, 0 otherwise. put(column, value).
+template <class Put>
+__host__ __device__ __forceinline__ void sha256_row_cells(const sha::BlockWitness& B, uint32_t br, uint32_t kt,
+                                                          Put&& put) {
   using namespace sha;
-  uint32_t digest[8];
-  for (int k = 0; k < 8; ++k) digest[k] = iv[k] + B.st[64][k];
-  auto W = [&](long t) -> uint32_t { return (t >= 0 && t < 64) ? B.w[t] : 0u; };
-  for (uint64_t br = 0; br < ROWS_PER_BLOCK; ++br) {
-    uint64_t* col0 = tr + base + br;  // cell (c) at col0[c * h]
-    auto put = [&](uint32_t c, uint64_t v) { col0[(uint64_t)c * h] = v; };
-    const uint32_t* s = B.st[br <= 64 ? br : 64];
-    const uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], hh = s[7];
-    for (int k = 0; k < 8; ++k) put(A_a + k, s[k]);
-    for (int i = 0; i < 32; ++i) {
-      put(BIT_A + i, (a >> i) & 1);
-      put(BIT_B + i, (b >> i) & 1);
-      put(BIT_C + i, (c >> i) & 1);
-      put(BIT_E + i, (e >> i) & 1);
-      put(BIT_F + i, (f >> i) & 1);
-      put(BIT_G + i, (g >> i) & 1);
-    }
-    for (int i = 0; i < 32; ++i) {
-      uint32_t p = (a >> ((i + 2) & 31)) & 1, q = (a >> ((i + 13) & 31)) & 1, r = (a >> ((i + 22) & 31)) & 1;
-      put(S0_T + i, p ^ q);
-      put(S0_BIT + i, p ^ q ^ r);
-      p = (e >> ((i + 6) & 31)) & 1, q = (e >> ((i + 11) & 31)) & 1, r = (e >> ((i + 25) & 31)) & 1;
-      put(S1_T + i, p ^ q);
-      put(S1_BIT + i, p ^ q ^ r);
-    }
-    put(S0_W, Sig0(a));
-    put(S1_W, Sig1(e));
-    const uint32_t chw = chf(e, f, g), mjw = majf(a, b, c);
-    for (int i = 0; i < 32; ++i) {
-      put(CH_BIT + i, (chw >> i) & 1);
-      uint32_t ai = (a >> i) & 1, bi = (b >> i) & 1, ci = (c >> i) & 1;
-      uint32_t ab = ai & bi, ac = ai & ci, bc = bi & ci;
-      put(MAJ_AB + i, ab);
-      put(MAJ_AC + i, ac);
-      put(MAJ_BC + i, bc);
-      put(MAJ_U + i, ab ^ ac);
-      put(MAJ_BIT + i, ab ^ ac ^ bc);
-    }
-    put(CH_W, chw);
-    put(MAJ_W, mjw);
-    const uint32_t wt = br < 64 ? B.w[br] : 0, kt = br < 64 ? kK_host[br] : 0;
-    put(W_, wt);
-    const uint64_t t1 = (uint64_t)hh + Sig1(e) + chw + kt + wt, t2 = (uint64_t)Sig0(a) + mjw;
-    const uint32_t t1c = (uint32_t)(t1 >> 32), t2c = (uint32_t)(t2 >> 32);
-    put(T1_LO, t1 & 0xFFFFFFFFu);
-    put(T1_C0, t1c & 1);
-    put(T1_C1, (t1c >> 1) & 1);
-    put(T1_C2, (t1c >> 2) & 1);
-    put(T1_CW, t1c);
-    put(T2_LO, t2 & 0xFFFFFFFFu);
-    put(T2_C0, t2c & 1);
-    put(T2_C1, (t2c >> 1) & 1);
-    put(T2_CW, t2c);
-    for (int k = 0; k < 8; ++k) put(H0 + k, br <= 64 ? iv[k] : digest[k]);
-    for (int k = 0; k < 15; ++k) put(WW0 + k, W((long)br - 15 + k));
-    const uint32_t w14 = W((long)br - 1), w1 = W((long)br - 14);
-    for (int i = 0; i < 32; ++i) {
-      put(BIT_WW14 + i, (w14 >> i) & 1);
-      put(BIT_WW1 + i, (w1 >> i) & 1);
-      uint32_t p = (w1 >> ((i + 7) & 31)) & 1, q = (w1 >> ((i + 18) & 31)) & 1, r = i + 3 < 32 ? (w1 >> (i + 3)) & 1 : 0;
-      put(SS0_T + i, p ^ q);
-      put(SS0_BIT + i, p ^ q ^ r);
-      p = (w14 >> ((i + 17) & 31)) & 1, q = (w14 >> ((i + 19) & 31)) & 1, r = i + 10 < 32 ? (w14 >> (i + 10)) & 1 : 0;
-      put(SS1_T + i, p ^ q);
-      put(SS1_BIT + i, p ^ q ^ r);
-    }
-    put(SS0_W, sig0(w1));
-    put(SS1_W, sig1(w14));
-    const uint64_t sum = (uint64_t)W((long)br - 15) + sig0(w1) + W((long)br - 6) + sig1(w14);
-    const uint32_t sc = (uint32_t)(sum >> 32);
-    put(WS_C0, sc & 1);
-    put(WS_C1, (sc >> 1) & 1);
-    put(WS_CW, sc);
-    if (br < 64) {
-      const uint64_t t1lo = t1 & 0xFFFFFFFFu, t2lo = t2 & 0xFFFFFFFFu;
-      put(NA_C, (t1lo + t2lo) >> 32);
-      put(NE_C, ((uint64_t)d + t1lo) >> 32);
-    }
-  }
+  auto W = [&](int t) -> uint32_t { return (t >= 0 && t < 64) ? B.w[t] : 0u; };
+  const uint32_t* s = B.st[br <= 64 ? br : 64];
+  const uint32_t a = s[0], b = s[1], c = s[2], d = s[3], e = s[4], f = s[5], g = s[6], hh = s[7];
+  for (int k = 0; k < 8; ++k) put(A_a + k, s[k]);
+  for (int i = 0; i < 32; ++i) put(BIT_A + i, (a >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(BIT_B + i, (b >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(BIT_C + i, (c >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(BIT_E + i, (e >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(BIT_F + i, (f >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(BIT_G + i, (g >> i) & 1);
+  const uint32_t s0a = rotr(a, 2) ^ rotr(a, 13), s1e = rotr(e, 6) ^ rotr(e, 11);
+  for (int i = 0; i < 32; ++i) put(S0_T + i, (s0a >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(S0_BIT + i, (Sig0(a) >> i) & 1);
+  put(S0_W, Sig0(a));
+  for (int i = 0; i < 32; ++i) put(S1_T + i, (s1e >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(S1_BIT + i, (Sig1(e) >> i) & 1);
+  put(S1_W, Sig1(e));
+  const uint32_t chw = chf(e, f, g), mjw = majf(a, b, c), ab = a & b, ac = a & c, bc = b & c;
+  for (int i = 0; i < 32; ++i) put(CH_BIT + i, (chw >> i) & 1);
+  put(CH_W, chw);
+  for (int i = 0; i < 32; ++i) put(MAJ_AB + i, (ab >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(MAJ_AC + i, (ac >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(MAJ_BC + i, (bc >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(MAJ_U + i, ((ab ^ ac) >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(MAJ_BIT + i, (mjw >> i) & 1);
+  put(MAJ_W, mjw);
+  const uint32_t wt = br < 64 ? B.w[br] : 0;
+  put(W_, wt);
+  const uint64_t t1 = (uint64_t)hh + Sig1(e) + chw + kt + wt, t2 = (uint64_t)Sig0(a) + mjw;
+  const uint32_t t1c = (uint32_t)(t1 >> 32), t2c = (uint32_t)(t2 >> 32);
+  put(T1_LO, t1 & 0xFFFFFFFFu);
+  put(T1_C0, t1c & 1);
+  put(T1_C1, (t1c >> 1) & 1);
+  put(T1_C2, (t1c >> 2) & 1);
+  put(T1_CW, t1c);
+  put(T2_LO, t2 & 0xFFFFFFFFu);
+  put(T2_C0, t2c & 1);
+  put(T2_C1, (t2c >> 1) & 1);
+  put(T2_CW, t2c);
+  for (int k = 0; k < 8; ++k) put(H0 + k, br <= 64 ? B.iv[k] : B.iv[k] + B.st[64][k]);
+  for (int k = 0; k < 15; ++k) put(WW0 + k, W((int)br - 15 + k));
+  const uint32_t w14 = W((int)br - 1), w1 = W((int)br - 14);
+  for (int i = 0; i < 32; ++i) put(BIT_WW14 + i, (w14 >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(BIT_WW1 + i, (w1 >> i) & 1);
+  // sigma0 / sigma1: two rotations, then the shift (zero-filled above bit 31 - n)
+  const uint32_t ss0t = rotr(w1, 7) ^ rotr(w1, 18), ss1t = rotr(w14, 17) ^ rotr(w14, 19);
+  for (int i = 0; i < 32; ++i) put(SS0_T + i, (ss0t >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(SS0_BIT + i, (sig0(w1) >> i) & 1);
+  put(SS0_W, sig0(w1));
+  for (int i = 0; i < 32; ++i) put(SS1_T + i, (ss1t >> i) & 1);
+  for (int i = 0; i < 32; ++i) put(SS1_BIT + i, (sig1(w14) >> i) & 1);
+  put(SS1_W, sig1(w14));
+  const uint64_t sum = (uint64_t)W((int)br - 15) + sig0(w1) + W((int)br - 6) + sig1(w14);
+  const uint32_t sc = (uint32_t)(sum >> 32);
+  put(WS_C0, sc & 1);
+  put(WS_C1, (sc >> 1) & 1);
+  put(WS_CW, sc);
+  const uint64_t t1lo = t1 & 0xFFFFFFFFu, t2lo = t2 & 0xFFFFFFFFu;
+  put(NA_C, br < 64 ? (t1lo + t2lo) >> 32 : 0);
+  put(NE_C, br < 64 ? ((uint64_t)d + t1lo) >> 32 : 0);
+}
+
+// One thread per trace row; padding rows repeat the last useful row. Consecutive
+// threads write consecutive addresses of every column.
+__global__ void __launch_bounds__(256) sha256_expand_kernel(const sha::BlockWitness* __restrict__ wit,
+                                                            uint64_t useful, uint64_t h, uint64_t* __restrict__ out) {
+  const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= h) return;
+  const uint64_t rr = r < useful ? r : useful - 1;
+  const uint32_t br = (uint32_t)(rr % sha::ROWS_PER_BLOCK);
+  sha256_row_cells(wit[rr / sha::ROWS_PER_BLOCK], br, br < 64 ? kK[br] : 0u,
+                   [&](uint32_t c, uint64_t v) { out[(uint64_t)c * h + r] = v; });
 }
 
 // ------------------------------------------------------------------ device Phi
@@ -317,10 +319,23 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
 bool g_k_uploaded[64] = {false};
 std::mutex g_k_mu;
 
+// K lives in constant memory; it is copied once per device.
+cudaError_t upload_k() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> g(g_k_mu);
+  if (!g_k_uploaded[dev]) {
+    cudaError_t e = cudaMemcpyToSymbol(kK, kK_host, sizeof kK_host);
+    if (e != cudaSuccess) return e;
+    g_k_uploaded[dev] = true;
+  }
+  return cudaSuccess;
+}
+
 }  // namespace
 
-uint64_t sha256_build_trace(const uint8_t* msg, uint64_t len, std::vector<uint64_t>* trace, uint64_t* n_blocks,
-                            uint8_t digest[32]) {
+uint64_t sha256_witness(const uint8_t* msg, uint64_t len, std::vector<sha::BlockWitness>* wit, uint8_t digest[32]) {
   using namespace sha;
   // FIPS 180-4 §5.1.1 padding
   std::vector<uint8_t> buf(msg, msg + len);
@@ -329,27 +344,61 @@ uint64_t sha256_build_trace(const uint8_t* msg, uint64_t len, std::vector<uint64
   const uint64_t bits = len * 8;
   for (int i = 7; i >= 0; --i) buf.push_back((uint8_t)(bits >> (8 * i)));
   const uint64_t nb = buf.size() / 64;
-  *n_blocks = nb;
-  const uint64_t useful = ROWS_PER_BLOCK * nb;
-  uint64_t h = ROWS_PER_BLOCK;
-  while (h < useful) h <<= 1;
-  trace->assign((uint64_t)WIDTH * h, 0);
+  wit->resize(nb);
   uint32_t iv[8];
   memcpy(iv, kIV, sizeof iv);
-  BlockState B;
   for (uint64_t b = 0; b < nb; ++b) {
-    run_block(buf.data() + 64 * b, iv, &B);
-    fill_rows(trace->data(), h, b * ROWS_PER_BLOCK, B, iv);
-    for (int k = 0; k < 8; ++k) iv[k] += B.st[64][k];
+    run_block(buf.data() + 64 * b, iv, &(*wit)[b]);
+    for (int k = 0; k < 8; ++k) iv[k] += (*wit)[b].st[64][k];
   }
   for (int k = 0; k < 8; ++k)
     for (int q = 0; q < 4; ++q) digest[4 * k + q] = (uint8_t)(iv[k] >> (24 - 8 * q));
-  // replicate the last useful row into the padding rows
-  for (uint64_t c = 0; c < WIDTH; ++c) {
-    uint64_t* col = trace->data() + c * h;
-    for (uint64_t r = useful; r < h; ++r) col[r] = col[useful - 1];
-  }
+  return sha256_height(nb);
+}
+
+uint64_t sha256_height(uint64_t n_blocks) {
+  uint64_t h = sha::ROWS_PER_BLOCK;
+  while (h < sha::ROWS_PER_BLOCK * n_blocks) h <<= 1;
   return h;
+}
+
+void sha256_fill_host(const sha::BlockWitness* wit, uint64_t n_blocks, uint64_t h, uint64_t* out) {
+  const uint64_t useful = sha::ROWS_PER_BLOCK * n_blocks;
+  auto rows = [&](uint64_t lo, uint64_t hi) {
+    for (uint64_t r = lo; r < hi; ++r) {
+      const uint64_t rr = r < useful ? r : useful - 1;  // padding rows repeat the last useful row
+      const uint32_t br = (uint32_t)(rr % sha::ROWS_PER_BLOCK);
+      uint64_t* col0 = out + r;
+      sha256_row_cells(wit[rr / sha::ROWS_PER_BLOCK], br, br < 64 ? kK_host[br] : 0u,
+                       [&](uint32_t c, uint64_t v) { col0[(uint64_t)c * h] = v; });
+    }
+  };
+  const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint64_t nt = std::min<uint64_t>({hw, 64, h / 1024});
+  if (nt <= 1) return rows(0, h);
+  std::vector<std::thread> th;
+  const uint64_t chunk = (h + nt - 1) / nt;
+  for (uint64_t t = 0; t < nt; ++t) th.emplace_back(rows, t * chunk, std::min(h, (t + 1) * chunk));
+  for (auto& x : th) x.join();
+}
+
+uint64_t sha256_build_trace(const uint8_t* msg, uint64_t len, std::vector<uint64_t>* trace, uint64_t* n_blocks,
+                            uint8_t digest[32]) {
+  std::vector<sha::BlockWitness> wit;
+  const uint64_t h = sha256_witness(msg, len, &wit, digest);
+  *n_blocks = wit.size();
+  trace->resize((uint64_t)sha::WIDTH * h);
+  sha256_fill_host(wit.data(), wit.size(), h, trace->data());
+  return h;
+}
+
+cudaError_t sha256_expand(const sha::BlockWitness* d_wit, uint64_t n_blocks, uint64_t h, uint64_t* d_trace,
+                          cudaStream_t s) {
+  cudaError_t e = upload_k();
+  if (e != cudaSuccess) return e;
+  SG_LAUNCH_SCOPE("sha256_expand", s);
+  sha256_expand_kernel<<<(unsigned)((h + 255) / 256), 256, 0, s>>>(d_wit, sha::ROWS_PER_BLOCK * n_blocks, h, d_trace);
+  return cudaGetLastError();
 }
 
 cudaError_t sha256_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, uint64_t n_blocks, const uint64_t* lambdas,
@@ -360,17 +409,8 @@ cudaError_t sha256_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, uint64_
 cudaError_t sha256_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, uint64_t row_div, uint64_t n_blocks,
                               const uint64_t* lambdas, uint64_t* phi, uint64_t out_stride, uint64_t out_off,
                               cudaStream_t s) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  {
-    std::lock_guard<std::mutex> g(g_k_mu);
-    if (!g_k_uploaded[dev]) {
-      cudaError_t e = cudaMemcpyToSymbol(kK, kK_host, sizeof kK_host);
-      if (e != cudaSuccess) return e;
-      g_k_uploaded[dev] = true;
-    }
-  }
+  cudaError_t e = upload_k();
+  if (e != cudaSuccess) return e;
   const unsigned T = 128;
   SG_LAUNCH_SCOPE("merge_phi", s);
   sha256_phi_kernel<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(evals, n, step, row_div, n_blocks, lambdas, phi,

@@ -28,7 +28,25 @@ enum : uint32_t {
   WIDTH = 756, NUM_CONSTRAINTS = 766, ROWS_PER_BLOCK = 128
 };
 
+// One compression of the trace: message schedule, the working state before each
+// of the 64 rounds plus the post-compression state, and the chaining value in.
+struct BlockWitness {
+  uint32_t w[64];
+  uint32_t st[65][8];
+  uint32_t iv[8];
+};
+
 }  // namespace sha
+
+// FIPS 180-4 padding and the compressions of msg: one witness per block, the
+// digest, and the trace height (128 rows per block, next power of two).
+uint64_t sha256_witness(const uint8_t* msg, uint64_t len, std::vector<sha::BlockWitness>* wit, uint8_t digest[32]);
+uint64_t sha256_height(uint64_t n_blocks);
+// Expands block witnesses into the 756 x h column-major trace on the host (threads).
+void sha256_fill_host(const sha::BlockWitness* wit, uint64_t n_blocks, uint64_t h, uint64_t* out);
+// The same expansion on the device: d_wit (n_blocks witnesses) -> d_trace (756 x h).
+cudaError_t sha256_expand(const sha::BlockWitness* d_wit, uint64_t n_blocks, uint64_t h, uint64_t* d_trace,
+                          cudaStream_t s);
 
 // Host: build_sha256_trace_multi (sha256_air.rs:429-472) into a column-major
 // WIDTH x height buffer (resized); returns height and sets n_blocks. The

@@ -73,3 +73,24 @@ def test_large_sha256_trace_proof(sgpu, ctx):
         ctx.set_option(sgpu.OPT_WIDE_MERGE, sgpu.WIDE_MERGE_AUTO)
     assert digest == hashlib.sha256(msg).digest()
     assert O.stir_verify(proof, O.build_params(1 << 19, fsb))
+
+
+@pytest.mark.parametrize("msg", [b"", b"abc", bytes(range(64)), bytes(range(256)) * 3, b"p" * 1000])
+def test_device_trace_expansion_matches_oracle(sgpu, ctx, msg):
+    # host compressions + device column expansion == the oracle's fill_block trace,
+    # padding rows included
+    want, wnb = O.sha256_trace(msg)
+    got, nb, dg = ctx.sha256_trace(msg)
+    assert nb == wnb and got.shape == want.shape
+    assert np.array_equal(got, want)
+    assert dg == hashlib.sha256(msg).digest()
+
+
+def test_device_trace_expansion_into_device_buffer(sgpu, ctx):
+    torch = pytest.importorskip("torch")
+    msg = bytes(np.random.default_rng(9).integers(0, 256, 700, dtype=np.uint8))
+    want, _ = O.sha256_trace(msg)
+    d = torch.empty(want.size, dtype=torch.int64, device="cuda")
+    ctx.sha256_trace(msg, out=d)
+    torch.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy().view(np.uint64).reshape(want.shape), want)
