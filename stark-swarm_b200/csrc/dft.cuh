@@ -36,9 +36,10 @@ __device__ __forceinline__ void dft_reg(uint64_t* v) {
         for (int j = 0; j < h; ++j) {
           uint64_t u = v[s + j], w = v[s + j + h];
           v[s + j] = gl::add(u, w);
-          uint64_t d = gl::sub(u, w);
+          // (u - w) w_R^t = (u - w) 2^e; for e >= 96 the sign of 2^96 = -1 is
+          // taken by swapping the subtraction
           const unsigned e = (ER * (unsigned)j * (unsigned)(R / (2 * h))) % 192u;
-          v[s + j + h] = (j == 0) ? d : gl::mul_pow2(d, e);
+          v[s + j + h] = e >= 96 ? gl::mul2e(gl::sub(w, u), e - 96) : gl::mul2e(gl::sub(u, w), e);
         }
       }
     }

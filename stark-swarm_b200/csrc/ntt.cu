@@ -30,6 +30,23 @@ namespace {
 
 __device__ __forceinline__ int padi(int m) { return m + (m >> 4); }
 
+// Lanes per CTA (2^pass_log_k): at least 4 (32-byte global rows), about 8192
+// elements per CTA, at most 1024 threads.
+__host__ __device__ constexpr int pass_log_k(int log_m) {
+  int lk = log_m >= 11 ? 2 : 13 - log_m;
+  while (((1 << lk) << log_m) / (log_m < 4 ? (1 << log_m) : 16) > 1024) --lk;
+  return lk;
+}
+// Shared-memory words between the rows of two lanes. Inside a row, one word of
+// padding per 16 keeps every Stockham stage conflict-free. The load and store
+// phases walk the lanes fastest (a half-warp covers K lanes x 16/K points), so
+// for M >= 256 the row stride is also padded to 16/K (mod 16) words; below that
+// a half-warp's stage accesses span several rows and the plain stride is kept.
+__host__ __device__ constexpr int row_stride(int log_m) {
+  const int M = 1 << log_m, Mp = M + (M >> 4), K = 1 << pass_log_k(log_m);
+  return M >= 256 ? Mp + (K < 16 ? 16 / K : 1) : Mp;
+}
+
 struct PassArgs {
   const uint64_t* in;
   uint64_t* out;
@@ -48,7 +65,6 @@ struct PassArgs {
   // 1 or 2 when only the first `sparse_nz` of the 16 inputs of every first-stage
   // radix-16 group can be non-zero (zero-padded forward transform); 0 = dense
   int sparse_nz;
-  int log_k;                  // lanes per CTA = 2^log_k
   int tw_log;                 // > 0: output (lane, i) *= w_{2^tw_log}^(i*lane)
   uint64_t scale;             // != 1: outputs *= scale
   const uint64_t* tw_st;      // w_4096^i (direction of the transform)
@@ -60,11 +76,10 @@ struct PassArgs {
 // One Stockham stage of radix R over all K lanes of the tile.
 // Each thread holds V values = V/R groups; group g -> lane g / G, j = g % G.
 template <int R, int V, bool INV>
-__device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int log_m, int log_ns,
+__device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int log_m, int Mp, int log_ns,
                                                const uint64_t* tw_st) {
   constexpr int GPT = V / R;
   constexpr int LR = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
-  const int M = 1 << log_m, Mp = M + (M >> 4);
   const int log_g = log_m - LR;
   const int G = 1 << log_g;
   const int Ns = 1 << log_ns;
@@ -101,8 +116,7 @@ __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int l
 // can be non-zero: X[k] = sum_{r<NZ} x_r w_16^{rk}. NZ = 1 is a broadcast,
 // NZ = 2 is X[k], X[k+8] = x0 +- w_16^k x1 (7 shift-multiplies, no full DFT).
 template <int NZ, bool INV>
-__device__ __forceinline__ void stockham_first_sparse(uint64_t* sm, int t, int T, int K, int log_m) {
-  const int M = 1 << log_m, Mp = M + (M >> 4);
+__device__ __forceinline__ void stockham_first_sparse(uint64_t* sm, int t, int T, int K, int log_m, int Mp) {
   const int log_g = log_m - 4, G = 1 << log_g;
   const int groups = K << log_g;
   constexpr unsigned E16 = exp16(INV);
@@ -142,12 +156,13 @@ template <int LOG_M, bool INV>
 __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   constexpr int M = 1 << LOG_M;
   constexpr int V = M < 16 ? M : 16;
-  constexpr int Mp = M + (M >> 4);
+  constexpr int Mp = row_stride(LOG_M);
+  constexpr int LOG_K = pass_log_k(LOG_M);
   extern __shared__ uint64_t sm[];
   const int t = threadIdx.x, T = blockDim.x;
-  const int K = 1 << a.log_k;
+  constexpr int K = 1 << LOG_K;
   const int E = K * M;
-  const uint64_t lane0 = (uint64_t)blockIdx.x << a.log_k;
+  const uint64_t lane0 = (uint64_t)blockIdx.x << LOG_K;
   const uint64_t y = (uint64_t)blockIdx.y + a.y_base;
   const uint64_t yc = y / a.y_sub, ys = y - yc * a.y_sub;
   const uint64_t* in = a.in + yc * a.in_col + ys * a.in_sub;
@@ -161,7 +176,7 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
     int l, m;
     if (lane_fast_in) {
       l = e & (K - 1);
-      m = e >> a.log_k;
+      m = e >> LOG_K;
     } else {
       m = e & (M - 1);
       l = e >> LOG_M;
@@ -184,28 +199,28 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
     int st0 = 0;
     if (sparse == 1 || sparse == 2) {
       if (sparse == 1)
-        stockham_first_sparse<1, INV>(sm, t, T, K, LOG_M);
+        stockham_first_sparse<1, INV>(sm, t, T, K, LOG_M, Mp);
       else
-        stockham_first_sparse<2, INV>(sm, t, T, K, LOG_M);
+        stockham_first_sparse<2, INV>(sm, t, T, K, LOG_M, Mp);
       log_ns = 4;
       st0 = 1;
     }
 #pragma unroll 1
     for (int st = st0; st < N16; ++st) {
-      stockham_stage<16, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
+      stockham_stage<16, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
       log_ns += 4;
     }
   }
-  if constexpr (REM == 1) stockham_stage<2, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
-  if constexpr (REM == 2) stockham_stage<4, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
-  if constexpr (REM == 3) stockham_stage<8, V, INV>(sm, t, T, LOG_M, log_ns, a.tw_st);
+  if constexpr (REM == 1) stockham_stage<2, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
+  if constexpr (REM == 2) stockham_stage<4, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
+  if constexpr (REM == 3) stockham_stage<8, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
 
   const bool lane_fast_out = a.out_lane == 1;
   for (int e = t; e < E; e += T) {
     int l, i;
     if (lane_fast_out) {
       l = e & (K - 1);
-      i = e >> a.log_k;
+      i = e >> LOG_K;
     } else {
       i = e & (M - 1);
       l = e >> LOG_M;
@@ -223,14 +238,11 @@ template <int LOG_M>
 cudaError_t launch_pass(const PassArgs& a0, bool inv, uint64_t n_rows, cudaStream_t s) {
   constexpr int M = 1 << LOG_M;
   constexpr int V = M < 16 ? M : 16;
-  PassArgs a = a0;
-  // lanes per CTA: at least 4 (32-byte rows), ~8192 elements per CTA, <= 1024 threads
-  int log_k = LOG_M >= 11 ? 2 : 13 - LOG_M;
-  while (((1 << log_k) * M / V) > 1024) --log_k;
-  a.log_k = log_k;
-  const int K = 1 << log_k;
-  const int T = K * M / V;
-  const size_t smem = (size_t)K * (M + M / 16) * sizeof(uint64_t);
+  const PassArgs& a = a0;
+  constexpr int K = 1 << pass_log_k(LOG_M);
+  constexpr int T = K * M / V;
+  static_assert(T <= 1024, "too many threads per CTA");
+  const size_t smem = (size_t)K * row_stride(LOG_M) * sizeof(uint64_t);
   const uint64_t blocks = (a.n_lanes + K - 1) / K;
   auto kern = inv ? ntt_pass_kernel<LOG_M, true> : ntt_pass_kernel<LOG_M, false>;
   if (smem > 48 * 1024) {

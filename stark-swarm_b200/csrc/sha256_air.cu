@@ -182,11 +182,12 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
   const bool past = blk >= n_blocks;
   const bool comp = !past && br < 64, fin = !past && br == 64, sched = !past && br >= 15 && br <= 62;
   Acc acc{lam, 0, 0};
+  // sum_b v_b 2^b over 32 columns: 96-bit terms summed exactly, one reduction
   auto pack = [&](uint32_t off) {
-    uint64_t s = 0;
-#pragma unroll 8
-    for (int b = 0; b < 32; ++b) s = gl::add(s, gl::mul_pow2_lt64(C(off + b), b));
-    return s;
+    gl::Acc128 a;
+#pragma unroll
+    for (int b = 0; b < 32; ++b) a.add_shl(C(off + b), b);
+    return a.reduce();
   };
   // bit booleanity: A, B, C, E, F, G, W_win[14], W_win[1]
   const uint32_t bool_offs[8] = {BIT_A, BIT_B, BIT_C, BIT_E, BIT_F, BIT_G, BIT_WW14, BIT_WW1};
