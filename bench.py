@@ -139,6 +139,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# DRAM bytes (read + write) per step of each kernel family on this workload (64
+# columns), from one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum over
+# the step's launches (profiles/ntt_pass_traffic_cfg2_64x2p20.md).
+MEASURED_TRAFFIC_PER_STEP = {"ntt_pass": 15.711e9}
+
 # ---------------------------------------------------------------- CPU side
 def load_oracle():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -197,7 +202,95 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def sha256_cpu_sample(threads, blocks=64):
+    """Oracle time for a SHA-256 AIR proof of a `blocks`-block message (756 columns,
+    blowup 32), the CPU side of the large-trace section."""
+    O = load_oracle()
+    O.set_threads(threads)
+    msg = np.random.default_rng(blocks).integers(0, 256, blocks * 64 - 9, dtype=np.uint8).tobytes()
+    t0 = time.perf_counter()
+    O.prove_sha256(msg, hashlib.sha3_256(b"cpu-sample").digest())
+    return time.perf_counter() - t0, 128 * blocks * 32
+
+
 # ---------------------------------------------------------------- GPU side
+def sha256_large(sg, ctx, blocks, reps, cpu_threads):
+    """One SHA-256 AIR proof of a `blocks`-block message (8192 blocks = a 2^20-row
+    trace, n0 = 2^25) through the public entry point: host message in, proof
+    bytes and digest out (trace expansion, coset-sliced LDE + constraint merge,
+    quotient, STIR and self-verification inside the timed call)."""
+    msg = np.random.default_rng(5).integers(0, 256, blocks * 64 - 9, dtype=np.uint8).tobytes()
+    fsb = hashlib.sha3_256(b"large-trace").digest()
+    n_trace = 128
+    while n_trace < 128 * blocks:
+        n_trace *= 2
+    n0 = 32 * n_trace
+    ref = ctx.prove_sha256(msg, fsb)  # warm-up: memory-pool growth
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = ctx.prove_sha256(msg, fsb)
+        times.append(time.perf_counter() - t0)
+        assert out == ref, "non-deterministic proof"
+    assert ref[1] == hashlib.sha256(msg).digest()
+    assert sg.deep_fri_verify(sg.build_params(n0, fsb), ref[0]), "proof rejected by the verifier"
+    sec = statistics.median(times)
+    res = {"workload": f"SHA-256 AIR proof of a {len(msg)}-byte message ({blocks} blocks, n_trace 2^{n_trace.bit_length() - 1}, "
+                       f"n0 2^{n0.bit_length() - 1}, 756 cols, 766 constraints, blowup 32), self-verified",
+           "s_per_proof": sec, "proofs_per_s": 1.0 / sec, "proof_bytes": len(ref[0]), "reps": reps}
+    if cpu_threads:
+        t_cpu, n0_s = sha256_cpu_sample(cpu_threads)
+        # prover work grows as n0 log n0 (LDE, quotient and STIR transforms dominate)
+        scale = (n0 * (n0.bit_length() - 1)) / (n0_s * (n0_s.bit_length() - 1))
+        est = t_cpu * scale
+        res["cpu_baseline"] = {"s_per_proof": est, "cores": cpu_threads, "kind": "port",
+                               "sample": f"oracle proof at n0 2^{n0_s.bit_length() - 1} took {t_cpu:.2f} s, "
+                                         f"scaled by n0 log n0 (x{scale:.0f}); the full size needs "
+                                         f"{756 * n0 * 8 / 2**30:.0f} GiB for the materialised LDE"}
+        res["gpu_over_cpu"] = est / sec
+    return res
+
+
+def serving(sg, ctx, rates, n_jobs, streams, seed=7):
+    """Poisson arrivals of SHA-256 AIR proof requests over record-length messages
+    (lognormal, median 120 B, clipped to 40-600 B: 1-10 blocks), admitted by the
+    continuous-batching server under a 160 GB HBM budget; p50/p99 latency from
+    submit to result, and throughput against one proof at a time."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.round(rng.lognormal(np.log(120), 0.6, n_jobs)), 40, 600).astype(int)
+    msgs = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in lens]
+    pis = [hashlib.sha3_256(b"serve-%d" % i).digest() for i in range(n_jobs)]
+    alone = {i: ctx.prove_sha256(msgs[i], pis[i])[0] for i in range(8)}  # reference bytes, one at a time
+    t0 = time.perf_counter()
+    for i in range(n_jobs):
+        ctx.prove_sha256(msgs[i], pis[i])
+    plain = n_jobs / (time.perf_counter() - t0)
+    out = {"workload": "SHA-256 AIR proofs, messages lognormal(median 120 B) clipped 40-600 B, Poisson arrivals",
+           "jobs_per_rate": n_jobs, "streams": streams, "hbm_budget_gb": 160, "plain_proofs_per_s": plain,
+           "rates": []}
+    for lam in rates:
+        gaps = rng.exponential(1.0 / lam, n_jobs)
+        with sg.Server(ctx, n_streams=streams, hbm_budget_bytes=160 << 30) as srv:
+            tickets = []
+            start = time.perf_counter()
+            due = start
+            for i in range(n_jobs):
+                due += gaps[i]
+                wait = due - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                tickets.append(srv.submit(sg.JOB_SHA256, msgs[i], pis[i]))
+            res = [srv.wait(t) for t in tickets]
+            wall = time.perf_counter() - start
+        for i, want in alone.items():
+            assert res[i][0] == want, "a proof in the mix differs from the same proof alone"
+        lat = np.array([r.latency_ms for _, r in res])
+        out["rates"].append({"offered_per_s": lam, "proofs_per_s": n_jobs / wall,
+                             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                             "over_plain": (n_jobs / wall) / plain})
+    return out
+
+
 def algorithmic_bytes():
     """Minimal HBM bytes per step for each kernel family (read inputs once, write outputs once)."""
     lde = (W * N + W * N0) * 8                       # read trace, write LDE
@@ -220,6 +313,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sha256-jobs", type=int, default=256,
                     help="SHA-256 AIR proofs for the plain-vs-batched section (0 skips it)")
+    ap.add_argument("--sha256-large-blocks", type=int, default=8192,
+                    help="blocks of the large SHA-256 trace proof (8192 = 2^20 rows; 0 skips it)")
+    ap.add_argument("--serve-jobs", type=int, default=200, help="jobs per arrival rate in the serving sweep (0 skips)")
+    ap.add_argument("--serve-rates", default="50,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--columns", type=int, default=64,
                     help="trace columns (64 = the benchmark workload; fewer for small profiling captures)")
     args = ap.parse_args()
@@ -346,7 +443,9 @@ def main():
             bytes_per_launch, achieved = None, None
         roofline = {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                     "frac": (achieved / hbm_peak) if achieved else None,
-                    "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                    "traffic": (MEASURED_TRAFFIC_PER_STEP[fam] / launches_per_step
+                                if fam in MEASURED_TRAFFIC_PER_STEP and W == 64 else None),
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                     "alg_bytes_per_launch": bytes_per_launch, "avg_launch_ms": per_launch_ms,
                     "launches_per_step": launches_per_step}
     kernels = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps} for k, v in prof.items()}
@@ -371,6 +470,12 @@ def main():
                            "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
         cfg1["batched_over_plain"] = cfg1["batched"]["proofs_per_s"] / cfg1["plain"]["proofs_per_s"]
 
+    cpu_threads = (os.cpu_count() or 1) if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else 0
+    large = sha256_large(sg, ctx, args.sha256_large_blocks, 3, cpu_threads) if args.sha256_large_blocks > 0 else None
+    serve = None
+    if args.serve_jobs > 0:
+        serve = serving(sg, ctx, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs, 16)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -394,6 +499,8 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "sha256_proofs": cfg1,
+            "sha256_large_trace": large,
+            "serving": serve,
             "proof_bytes": len(ref[1]),
             "root": ref[0].hex(),
         }

@@ -426,17 +426,18 @@ class Context:
             self._check(rc)
             return buf.raw[:ln.value], dg.raw
 
-    def prove_batch(self, jobs, n_streams: int = 8, hbm_budget_bytes: int = 0, cap_per_job: int = 1 << 21):
+    def prove_batch(self, jobs, n_streams: int = 8, hbm_budget_bytes: int = 0, cap_per_job: int = 1 << 20):
         """jobs: list of (kind, data, pi[, phi_mode]) -> list of (proof bytes, JobResult)."""
         made = [make_job(*j) for j in jobs]
         arr = (Job * len(made))(*[m[0] for m in made])
         res = (JobResult * len(made))()
-        buf = ctypes.create_string_buffer(cap_per_job * max(1, len(made)))
-        rc = self._lib.sg_prove_batch(self._h, arr, len(made), n_streams, hbm_budget_bytes, buf, cap_per_job, res)
+        # uninitialised result slots: only each proof's own bytes are touched and copied out
+        buf = np.empty(cap_per_job * max(1, len(made)), dtype=np.uint8)
+        rc = self._lib.sg_prove_batch(self._h, arr, len(made), n_streams, hbm_budget_bytes,
+                                      ctypes.cast(buf.ctypes.data, ctypes.c_char_p), cap_per_job, res)
         if rc != SG_OK:
             raise StarkGpuError(rc, "sg_prove_batch failed")
-        raw = buf.raw
-        return [(raw[i * cap_per_job: i * cap_per_job + res[i].proof_len], res[i]) for i in range(len(made))]
+        return [(buf[i * cap_per_job: i * cap_per_job + res[i].proof_len].tobytes(), res[i]) for i in range(len(made))]
 
     def deep_ali_merge_general(self, trace_evals_on_lde, combination_coeffs, air, omega, n_trace, blowup,
                                phi_mode=PHI_PARALLEL_GATE):
