@@ -159,9 +159,10 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   constexpr int Mp = row_stride(LOG_M);
   constexpr int LOG_K = pass_log_k(LOG_M);
   extern __shared__ uint64_t sm[];
-  const int t = threadIdx.x, T = blockDim.x;
   constexpr int K = 1 << LOG_K;
-  const int E = K * M;
+  constexpr int E = K * M;
+  constexpr int T = E / V;  // blockDim.x (launch_pass); every thread owns V elements
+  const int t = threadIdx.x;
   const uint64_t lane0 = (uint64_t)blockIdx.x << LOG_K;
   const uint64_t y = (uint64_t)blockIdx.y + a.y_base;
   const uint64_t yc = y / a.y_sub, ys = y - yc * a.y_sub;
@@ -172,8 +173,10 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   // a sparse first stage reads only points m < nz * M/16: skip the rest
   const int sparse = (LOG_M >= 4 && lane_fast_in) ? a.sparse_nz : 0;
   const int E_load = sparse ? K * sparse * (M >> 4) : E;
-  for (int e = t; e < E_load; e += T) {
-    int l, m;
+  // Global loads go out in batches of B before the batch's shared stores (a
+  // generic load may not pass a shared store, so the split is explicit).
+  constexpr int B = V < 8 ? V : 8;
+  auto in_pos = [&](int e, int& l, int& m) {
     if (lane_fast_in) {
       l = e & (K - 1);
       m = e >> LOG_K;
@@ -181,14 +184,30 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       m = e & (M - 1);
       l = e >> LOG_M;
     }
-    uint64_t lane = lane0 + l;
-    uint64_t x = 0;
-    const uint64_t flat = (uint64_t)m * a.in_m + lane * a.flat_lane;
-    if (lane < a.n_lanes && flat < a.in_valid) {
-      x = in[lane * a.in_lane + (uint64_t)m * a.in_m];
-      if (a.pre.lo) x = gl::mul(x, pow_at(a.pre, flat));
+  };
+#pragma unroll
+  for (int q0 = 0; q0 < V; q0 += B) {
+    uint64_t x[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int e = t + (q0 + q) * T;
+      int l, m;
+      in_pos(e, l, m);
+      const uint64_t lane = lane0 + l;
+      const uint64_t flat = (uint64_t)m * a.in_m + lane * a.flat_lane;
+      x[q] = 0;
+      if (e < E_load && lane < a.n_lanes && flat < a.in_valid) {
+        x[q] = __ldg(in + lane * a.in_lane + (uint64_t)m * a.in_m);
+        if (a.pre.lo) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
+      }
     }
-    sm[l * Mp + padi(m)] = x;
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const int e = t + (q0 + q) * T;
+      int l, m;
+      in_pos(e, l, m);
+      if (e < E_load) sm[l * Mp + padi(m)] = x[q];
+    }
   }
   __syncthreads();
 
@@ -216,8 +235,7 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   if constexpr (REM == 3) stockham_stage<8, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
 
   const bool lane_fast_out = a.out_lane == 1;
-  for (int e = t; e < E; e += T) {
-    int l, i;
+  auto out_pos = [&](int e, int& l, int& i) {
     if (lane_fast_out) {
       l = e & (K - 1);
       i = e >> LOG_K;
@@ -225,12 +243,26 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       i = e & (M - 1);
       l = e >> LOG_M;
     }
-    uint64_t lane = lane0 + l;
-    if (lane >= a.n_lanes) continue;
-    uint64_t x = sm[l * Mp + padi(i)];
-    if (a.tw_log > 0) x = gl::mul(x, tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * lane, a.tw_log));
-    if (a.scale != 1) x = gl::mul(x, a.scale);
-    out[lane * a.out_lane + (uint64_t)i * a.out_i] = x;
+  };
+  // shared reads and pass-twiddle loads of a batch before its global stores
+#pragma unroll
+  for (int q0 = 0; q0 < V; q0 += B) {
+    uint64_t x[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      int l, i;
+      out_pos(t + (q0 + q) * T, l, i);
+      x[q] = sm[l * Mp + padi(i)];
+      if (a.tw_log > 0) x[q] = gl::mul(x[q], tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log));
+      if (a.scale != 1) x[q] = gl::mul(x[q], a.scale);
+    }
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      int l, i;
+      out_pos(t + (q0 + q) * T, l, i);
+      const uint64_t lane = lane0 + l;
+      if (lane < a.n_lanes) out[lane * a.out_lane + (uint64_t)i * a.out_i] = x[q];
+    }
   }
 }
 
