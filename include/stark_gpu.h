@@ -70,8 +70,8 @@ void sg_ctx_destroy(sg_ctx* ctx);
 int sg_ctx_set_stream(sg_ctx* ctx, void* cuda_stream);
 const char* sg_last_error(const sg_ctx* ctx);
 /* Context options.
- * SG_OPT_WIDE_MERGE selects how sg_prove_sha256 evaluates the SHA-256 AIR over the LDE:
- *   SG_WIDE_MERGE_LDE     materialise the 756-column LDE, then evaluate (fewest launches);
+ * SG_OPT_WIDE_MERGE selects how sg_prove_sha256 / sg_prove_sha512 evaluate their AIR over the LDE:
+ *   SG_WIDE_MERGE_LDE     materialise the 756- (1510-) column LDE, then evaluate (fewest launches);
  *   SG_WIDE_MERGE_COSETS  never store the LDE: for each of the `blowup` cosets r, evaluate
  *                         all columns on r*<w_n0^blowup> (coefficients twisted by w_n0^{rk},
  *                         one n_trace-point NTT per column) and fold the constraints of that
@@ -103,7 +103,7 @@ void sg_profile_reset(void);
 
 /* Batched NTT with ark-poly Radix2EvaluationDomain semantics: forward = evaluations
  * at w^0..w^{n-1} (natural order), inverse includes 1/n; w = 7^((p-1)/2^32)
- * squared (32 - log_n) times. n_cols columns of 2^log_n, log_n <= 24.
+ * squared (32 - log_n) times. n_cols columns of 2^log_n, log_n <= 28.
  * Replaces the domain.fft / domain.ifft calls of trace_import.rs:276-279 and
  * lib.rs:402-410. in == out allowed. */
 int sg_ntt(sg_ctx* ctx, const uint64_t* in, uint64_t* out, size_t n_cols, size_t log_n, int inverse);
@@ -173,6 +173,33 @@ int sg_sha256_trace_gpu(sg_ctx* ctx, const uint8_t* msg, size_t len, uint64_t* t
 int sg_prove_sha256(sg_ctx* ctx, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,
                     uint8_t* proof, size_t cap, size_t* len_out, uint8_t digest[32]);
 
+/* Replaces deep_ali_merge_sha512 (deep_ali/src/lib.rs:561-641): the SHA-512 AIR
+ * (eval_sha512_constraints, sha512_air.rs:909-1270; 64-bit words as 32-bit limb
+ * pairs) with an explicit block count. lde: 1510 x (n_trace*blowup); lambdas:
+ * 1526 values (host). */
+int sg_merge_sha512(sg_ctx* ctx, const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas,
+                    size_t n_blocks, int phi_mode, uint64_t* c_eval);
+
+/* Replaces build_sha512_trace_multi (deep_ali/src/sha512_air.rs:551-578), host
+ * only: FIPS 180-4 §5.1.2 padding, 128 rows per block (80 rounds, post-state,
+ * finalisation, idle), height = next power of two, last useful row replicated.
+ * Writes 1510 x height column-major into `trace` (cap in elements), the block
+ * count, and the 64-byte digest carried in the H-state. */
+int sg_sha512_trace(const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height, size_t* n_blocks,
+                    uint8_t digest[64]);
+/* The same trace with the column expansion on the device (one 5888-byte witness
+ * per block crosses PCIe); `trace` is host or device memory. */
+int sg_sha512_trace_gpu(sg_ctx* ctx, const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height,
+                        size_t* n_blocks, uint8_t digest[64]);
+
+/* SHA-512 AIR proof of `msg`: trace -> LDE x32 -> merge_sha512 (lambda_j = j+1)
+ * -> STIR with build_params(n0, fs_binding), self-verified. The reference has
+ * the AIR and its merge but no SHA-512 prover yet (sha512_air.rs:16-19); this
+ * uses the SHA-256 binding's parameters (swarm-dns/src/prover.rs:512-585).
+ * `digest` receives the 64-byte digest read from the trace's H-state. */
+int sg_prove_sha512(sg_ctx* ctx, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,
+                    uint8_t* proof, size_t cap, size_t* len_out, uint8_t digest[64]);
+
 /* Merkle commitment over the rows of a column-major matrix (leaf i = the
  * `width` values of row i), with the reference channel's framing
  * (merkle/src/lib.rs:95-238, 391-476): per-level arities, tree label, last-node
@@ -216,6 +243,7 @@ int sg_prove_hash_rollup(sg_ctx* ctx, const uint64_t* leaves, size_t n_leaves, c
  * Every proof is self-verified and byte-identical to the single-proof call. */
 #define SG_JOB_SHA256 1      /* input = message bytes, input_len = bytes (sg_prove_sha256) */
 #define SG_JOB_HASH_ROLLUP 2 /* input = u64 rollup leaves, input_len = count (sg_prove_hash_rollup) */
+#define SG_JOB_SHA512 3      /* input = message bytes, input_len = bytes (sg_prove_sha512) */
 
 typedef struct {
   int32_t kind;
@@ -229,7 +257,7 @@ typedef struct {
   int32_t status; /* SG_OK or an SG_E* code */
   uint32_t reserved;
   size_t proof_len;
-  uint8_t digest[32]; /* SHA-256 jobs: the asserted digest */
+  uint8_t digest[64]; /* SHA-256 jobs: the asserted digest (32 bytes); SHA-512 jobs: 64 bytes */
   double queue_ms;    /* submit -> start */
   double run_ms;      /* start -> proof ready */
   double latency_ms;  /* submit -> proof ready */

@@ -11,15 +11,19 @@
 #include <cstddef>
 #include "gl.hpp"
 #include "sha256_air.hpp"
+#include "sha512_air.hpp"
 
 namespace orc {
 
-enum { AIR_HASH_ROLLUP = 4, AIR_SHA256 = 6 };
+// AIR_SHA512 has no registry variant in the reference (it is reached through
+// deep_ali_merge_sha512, lib.rs:561-641); its id here is internal to the oracle.
+enum { AIR_HASH_ROLLUP = 4, AIR_SHA256 = 6, AIR_SHA512 = 100 };
 
 inline size_t air_width(int air) {
   switch (air) {
     case AIR_HASH_ROLLUP: return 4;
     case AIR_SHA256: return sha::WIDTH;
+    case AIR_SHA512: return sha512::WIDTH;
     default: return 0;
   }
 }
@@ -27,6 +31,7 @@ inline size_t air_num_constraints(int air) {
   switch (air) {
     case AIR_HASH_ROLLUP: return 3;
     case AIR_SHA256: return sha::NUM_CONSTRAINTS;
+    case AIR_SHA512: return sha512::NUM_CONSTRAINTS;
     default: return 0;
   }
 }
@@ -54,6 +59,7 @@ inline void eval_constraints(int air, const Fp* cur, const Fp* nxt, size_t row, 
       out[2] = nxt[2] - cur[3] - cur[1];
       break;
     case AIR_SHA256: sha::eval(cur, nxt, row, n_blocks, out); break;
+    case AIR_SHA512: sha512::eval(cur, nxt, row, n_blocks, out); break;
     default: break;
   }
 }

@@ -859,6 +859,59 @@ int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32
   return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
 }
 
+// deep_ali_merge_sha512 (lib.rs:561-641): the SHA-512 AIR with an explicit block count.
+int orc_merge_sha512(const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas, size_t n_blocks,
+                     int phi_mode, uint64_t* c_eval) {
+  if (n_trace == 0 || (n_trace & (n_trace - 1)) || blowup == 0 || (blowup & (blowup - 1))) return -2;
+  auto c = merge(AIR_SHA512, (const Fp*)lde, sha512::WIDTH, n_trace, blowup, (const Fp*)lambdas,
+                 sha512::NUM_CONSTRAINTS, phi_mode, n_blocks);
+  memcpy(c_eval, c.data(), c.size() * 8);
+  return 0;
+}
+
+// build_sha512_trace_multi (sha512_air.rs:551-578): WIDTH x height column-major.
+int orc_sha512_trace(const uint8_t* msg, size_t len, uint64_t* out, size_t cap_elems, size_t* height,
+                     size_t* n_blocks) {
+  std::vector<Fp> tr;
+  *height = sha512::build_trace_multi(msg, len, &tr, n_blocks);
+  if (tr.size() > cap_elems) return -3;
+  memcpy(out, tr.data(), tr.size() * 8);
+  return 0;
+}
+
+// eval_sha512_constraints at one row (for known-answer / tamper tests).
+int orc_sha512_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_blocks, uint64_t* out) {
+  sha512::eval((const Fp*)cur, (const Fp*)nxt, row, n_blocks, (Fp*)out);
+  return 0;
+}
+
+// SHA-512 proof with the SHA-256 binding's parameters (the reference has no
+// SHA-512 prover yet, sha512_air.rs:16-19): trace -> LDE x32 -> merge_sha512
+// (lambda_j = j+1) -> STIR with build_params(n0, fs_binding). digest receives the
+// 64-byte digest read from the H-state (row 128 (n_blocks - 1) + 81).
+int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
+                     size_t cap, size_t* out_len, uint8_t digest[64]) {
+  std::vector<Fp> tr;
+  size_t n_blocks = 0;
+  const size_t n_trace = sha512::build_trace_multi(msg, len, &tr, &n_blocks);
+  const size_t digest_row = sha512::ROWS_PER_BLOCK * (n_blocks - 1) + 81;
+  for (int k = 0; k < 8; ++k) {
+    const uint64_t lo = tr[(sha512::H0_LO + 2 * k) * n_trace + digest_row].v;
+    const uint64_t hi = tr[(sha512::H0_LO + 2 * k + 1) * n_trace + digest_row].v;
+    const uint64_t wd = lo | hi << 32;
+    for (int b = 0; b < 8; ++b) digest[8 * k + b] = (uint8_t)(wd >> (56 - 8 * b));
+  }
+  const size_t blowup = 32, n0 = n_trace * blowup;
+  std::vector<uint64_t> lde(sha512::WIDTH * n0), c(n0);
+  orc_lde((const uint64_t*)tr.data(), sha512::WIDTH, n_trace, blowup, 1, lde.data());
+  std::vector<uint64_t> lam(sha512::NUM_CONSTRAINTS);
+  for (size_t j = 0; j < lam.size(); ++j) lam[j] = j + 1;
+  orc_merge_sha512(lde.data(), n_trace, blowup, lam.data(), n_blocks, phi_mode, c.data());
+  orc_fri_params p;
+  orc_build_params(n0, fs_binding, 1, &p);
+  return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
+}
+
 int orc_poly_div_zh(const uint64_t* coeffs, size_t n, size_t m, uint64_t* q) {
   std::vector<Fp> d((const Fp*)coeffs, (const Fp*)coeffs + n);
   auto r = poly_div_zh(d, m);

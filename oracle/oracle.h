@@ -70,6 +70,13 @@ int orc_merge_sha256(const uint64_t* lde, size_t n_trace, size_t blowup, const u
 int orc_sha256_trace(const uint8_t* msg, size_t len, uint64_t* out, size_t cap_elems, size_t* height,
                      size_t* n_blocks);
 int orc_sha256_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_blocks, uint64_t* out);
+int orc_merge_sha512(const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas, size_t n_blocks,
+                     int phi_mode, uint64_t* c_eval);
+int orc_sha512_trace(const uint8_t* msg, size_t len, uint64_t* out, size_t cap_elems, size_t* height,
+                     size_t* n_blocks);
+int orc_sha512_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_blocks, uint64_t* out);
+int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
+                     size_t cap, size_t* out_len, uint8_t digest[64]);
 int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
                      size_t cap, size_t* out_len, uint8_t digest[32]);
 void orc_build_params(size_t n0, const uint8_t pi[32], int stir, orc_fri_params* out);

@@ -10,6 +10,11 @@ C ABI is declared in include/stark_gpu.h:
   deep_fri_verify        deep_ali/src/fri.rs:2136-2521 (STIR branch)
   MerkleTreeChannel      merkle/src/lib.rs:356-512
   make_schedule / build_params / prove_hash_rollup   swarm-dns/src/prover.rs:53-304
+  deep_ali_merge_sha256 / prove_sha256 (prove_ds_ksk_binding core)
+                         deep_ali/src/lib.rs:453-545, swarm-dns/src/prover.rs:512-585
+  deep_ali_merge_sha512  deep_ali/src/lib.rs:561-641 (and a SHA-512 proof with the same parameters)
+  build_sha256_trace_multi / build_sha512_trace_multi
+                         deep_ali/src/sha256_air.rs:429-472, sha512_air.rs:551-578
 
 Field elements are canonical uint64 (numpy uint64 arrays on the host, or CUDA
 tensors / raw device pointers that the library uses in place). Errors that the
@@ -98,11 +103,12 @@ EXPORTS = (
     "sg_kernel_launches",
     "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
     "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_sha256_trace_gpu", "sg_prove_sha256",
+    "sg_merge_sha512", "sg_sha512_trace", "sg_sha512_trace_gpu", "sg_prove_sha512",
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
 )
-JOB_SHA256, JOB_HASH_ROLLUP = 1, 2
+JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512 = 1, 2, 3
 OPT_WIDE_MERGE = 1
 WIDE_MERGE_AUTO, WIDE_MERGE_LDE, WIDE_MERGE_COSETS = 0, 1, 2
 
@@ -114,10 +120,23 @@ class Job(ctypes.Structure):
 
 class JobResult(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int32), ("reserved", ctypes.c_uint32), ("proof_len", ctypes.c_size_t),
-                ("digest", ctypes.c_uint8 * 32), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("digest", ctypes.c_uint8 * 64), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
                 ("latency_ms", ctypes.c_double)]
 AIR_SHA256 = 6
 SHA256_WIDTH, SHA256_CONSTRAINTS = 756, 766
+SHA512_WIDTH, SHA512_CONSTRAINTS = 1510, 1526
+# per hash AIR: width, constraints, digest bytes, block bytes, padding overhead (0x80 + length field)
+_HASH = {"sha256": (SHA256_WIDTH, SHA256_CONSTRAINTS, 32, 64, 9),
+         "sha512": (SHA512_WIDTH, SHA512_CONSTRAINTS, 64, 128, 17)}
+
+
+def _trace_height(hash_name: str, message: bytes) -> int:
+    _, _, _, block, pad = _HASH[hash_name]
+    nb = (len(message) + pad + block - 1) // block
+    height = 128
+    while height < 128 * nb:
+        height *= 2
+    return height
 
 
 def lib():
@@ -160,6 +179,10 @@ def lib():
     L.sg_sha256_trace_gpu.argtypes = [vp] + L.sg_sha256_trace.argtypes
     L.sg_prove_sha256.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz,
                                   ctypes.POINTER(sz), ctypes.c_char_p]
+    L.sg_merge_sha512.argtypes = L.sg_merge_sha256.argtypes
+    L.sg_sha512_trace.argtypes = L.sg_sha256_trace.argtypes
+    L.sg_sha512_trace_gpu.argtypes = L.sg_sha256_trace_gpu.argtypes
+    L.sg_prove_sha512.argtypes = L.sg_prove_sha256.argtypes
     L.sg_merkle_commit.argtypes = [vp, vp, sz, sz, sz, vp, sz, u64, ctypes.c_char_p, ctypes.POINTER(vp)]
     L.sg_merkle_open.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
     L.sg_merkle_free.argtypes = [vp]
@@ -239,20 +262,27 @@ def ntt_noalloc(d_in, d_out, log_n: int, inverse: bool = False, stream_ptr: int 
     return lib().sg_ntt_noalloc(ip, op, max(1, count // n), log_n, int(inverse), stream_ptr or None)
 
 
+def _build_trace_multi(hash_name: str, message: bytes):
+    width, _, dbytes, _, _ = _HASH[hash_name]
+    height = _trace_height(hash_name, message)
+    out = np.zeros(width * height, dtype=np.uint64)
+    h, n = ctypes.c_size_t(), ctypes.c_size_t()
+    dg = ctypes.create_string_buffer(dbytes)
+    fn = getattr(lib(), f"sg_{hash_name}_trace")
+    rc = fn(message, len(message), out.ctypes.data, out.size, ctypes.byref(h), ctypes.byref(n), dg)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, f"sg_{hash_name}_trace failed")
+    return out[: width * h.value].reshape(width, h.value), n.value, dg.raw
+
+
 def build_sha256_trace_multi(message: bytes):
     """sha256_air.rs:429-472 on the host -> ((756, height) uint64 trace, n_blocks, asserted digest)."""
-    nb = (len(message) + 9 + 63) // 64
-    height = 128
-    while height < 128 * nb:
-        height *= 2
-    out = np.zeros(SHA256_WIDTH * height, dtype=np.uint64)
-    h, n = ctypes.c_size_t(), ctypes.c_size_t()
-    dg = ctypes.create_string_buffer(32)
-    rc = lib().sg_sha256_trace(message, len(message), out.ctypes.data, out.size, ctypes.byref(h), ctypes.byref(n),
-                               dg)
-    if rc != SG_OK:
-        raise StarkGpuError(rc, "sg_sha256_trace failed")
-    return out[: SHA256_WIDTH * h.value].reshape(SHA256_WIDTH, h.value), n.value, dg.raw
+    return _build_trace_multi("sha256", message)
+
+
+def build_sha512_trace_multi(message: bytes):
+    """sha512_air.rs:551-578 on the host -> ((1510, height) uint64 trace, n_blocks, 64-byte digest)."""
+    return _build_trace_multi("sha512", message)
 
 
 def deep_fri_verify(params: FriParams, proof: bytes) -> bool:
@@ -375,56 +405,79 @@ class Context:
                                        op))
         return out
 
-    def sha256_trace(self, message: bytes, out=None):
-        """build_sha256_trace_multi with the column expansion on the GPU ->
-        ((756, height) trace, n_blocks, asserted digest). `out`, if given, is a
-        device tensor of at least 756 * height elements and receives the trace."""
-        nb = (len(message) + 9 + 63) // 64
-        height = 128
-        while height < 128 * nb:
-            height *= 2
+    def _hash_trace(self, hash_name: str, message: bytes, out=None):
+        width, _, dbytes, _, _ = _HASH[hash_name]
+        height = _trace_height(hash_name, message)
         if out is None:
-            out = np.empty((SHA256_WIDTH, height), dtype=np.uint64)
+            out = np.empty((width, height), dtype=np.uint64)
         op, _ko, _ = _addr(out)
-        cap = SHA256_WIDTH * height
         h, n = ctypes.c_size_t(), ctypes.c_size_t()
-        dg = ctypes.create_string_buffer(32)
-        self._check(self._lib.sg_sha256_trace_gpu(self._h, message, len(message), op, cap, ctypes.byref(h),
-                                                  ctypes.byref(n), dg))
+        dg = ctypes.create_string_buffer(dbytes)
+        fn = getattr(self._lib, f"sg_{hash_name}_trace_gpu")
+        self._check(fn(self._h, message, len(message), op, width * height, ctypes.byref(h), ctypes.byref(n), dg))
         return out, n.value, dg.raw
 
-    def merge_sha256(self, lde, n_trace: int, blowup: int, lambdas, n_blocks: int, phi_mode=PHI_PARALLEL_GATE,
-                     out=None):
-        """deep_ali_merge_sha256 on a (756, n_trace*blowup) LDE."""
+    def _merge_hash(self, hash_name, lde, n_trace, blowup, lambdas, n_blocks, phi_mode, out):
+        _, k, _, _, _ = _HASH[hash_name]
         ip, _ki, host = _addr(lde)
         lam = np.ascontiguousarray(lambdas, dtype=np.uint64)
-        if lam.size != SHA256_CONSTRAINTS:
-            raise ValueError("need one combination coefficient per constraint (766)")
+        if lam.size != k:
+            raise ValueError(f"need one combination coefficient per constraint ({k})")
         n = n_trace * blowup
         if out is None:
             if not host:
                 raise ValueError("device input needs an explicit out buffer")
             out = np.empty(n, dtype=np.uint64)
         op, _ko, _ = _addr(out)
-        self._check(self._lib.sg_merge_sha256(self._h, ip, n_trace, blowup, lam.ctypes.data, n_blocks, phi_mode, op))
+        fn = getattr(self._lib, f"sg_merge_{hash_name}")
+        self._check(fn(self._h, ip, n_trace, blowup, lam.ctypes.data, n_blocks, phi_mode, op))
         return out
 
-    def prove_sha256(self, message: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
-        """prove_ds_ksk_binding core -> (proof bytes, asserted SHA-256 digest); self-verified."""
+    def _prove_hash(self, hash_name, message, fs_binding, phi_mode):
         if len(fs_binding) != 32:
             raise ValueError("fs_binding must be 32 bytes")
+        dbytes = _HASH[hash_name][2]
+        fn = getattr(self._lib, f"sg_prove_{hash_name}")
         cap = 1 << 24
         while True:
             buf = ctypes.create_string_buffer(cap)
             ln = ctypes.c_size_t()
-            dg = ctypes.create_string_buffer(32)
-            rc = self._lib.sg_prove_sha256(self._h, message, len(message), fs_binding, phi_mode, buf, cap,
-                                           ctypes.byref(ln), dg)
+            dg = ctypes.create_string_buffer(dbytes)
+            rc = fn(self._h, message, len(message), fs_binding, phi_mode, buf, cap, ctypes.byref(ln), dg)
             if rc == SG_ESPACE:
                 cap = ln.value
                 continue
             self._check(rc)
             return buf.raw[:ln.value], dg.raw
+
+    def sha256_trace(self, message: bytes, out=None):
+        """build_sha256_trace_multi with the column expansion on the GPU ->
+        ((756, height) trace, n_blocks, asserted digest). `out`, if given, is a
+        device tensor of at least 756 * height elements and receives the trace."""
+        return self._hash_trace("sha256", message, out)
+
+    def sha512_trace(self, message: bytes, out=None):
+        """build_sha512_trace_multi with the column expansion on the GPU ->
+        ((1510, height) trace, n_blocks, 64-byte digest)."""
+        return self._hash_trace("sha512", message, out)
+
+    def merge_sha256(self, lde, n_trace: int, blowup: int, lambdas, n_blocks: int, phi_mode=PHI_PARALLEL_GATE,
+                     out=None):
+        """deep_ali_merge_sha256 on a (756, n_trace*blowup) LDE."""
+        return self._merge_hash("sha256", lde, n_trace, blowup, lambdas, n_blocks, phi_mode, out)
+
+    def merge_sha512(self, lde, n_trace: int, blowup: int, lambdas, n_blocks: int, phi_mode=PHI_PARALLEL_GATE,
+                     out=None):
+        """deep_ali_merge_sha512 on a (1510, n_trace*blowup) LDE."""
+        return self._merge_hash("sha512", lde, n_trace, blowup, lambdas, n_blocks, phi_mode, out)
+
+    def prove_sha256(self, message: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
+        """prove_ds_ksk_binding core -> (proof bytes, asserted SHA-256 digest); self-verified."""
+        return self._prove_hash("sha256", message, fs_binding, phi_mode)
+
+    def prove_sha512(self, message: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
+        """SHA-512 AIR proof (LDE x32, lambda_j = j+1, STIR) -> (proof bytes, 64-byte digest); self-verified."""
+        return self._prove_hash("sha512", message, fs_binding, phi_mode)
 
     def prove_batch(self, jobs, n_streams: int = 8, hbm_budget_bytes: int = 0, cap_per_job: int = 1 << 20):
         """jobs: list of (kind, data, pi[, phi_mode]) -> list of (proof bytes, JobResult)."""
@@ -497,7 +550,7 @@ def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
     """A sg_job plus the buffer it points to (keep both alive until submitted)."""
     if len(pi) != 32:
         raise ValueError("pi must be 32 bytes")
-    if kind == JOB_SHA256:
+    if kind in (JOB_SHA256, JOB_SHA512):
         buf = ctypes.create_string_buffer(bytes(data), max(1, len(data)))
         n = len(data)
     elif kind == JOB_HASH_ROLLUP:
@@ -507,7 +560,7 @@ def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
         raise ValueError("unknown job kind")
     j = Job()
     j.kind, j.phi_mode = kind, phi_mode
-    j.input = ctypes.addressof(buf) if kind == JOB_SHA256 else (buf.ctypes.data if n else None)
+    j.input = ctypes.addressof(buf) if kind in (JOB_SHA256, JOB_SHA512) else (buf.ctypes.data if n else None)
     j.input_len = n
     ctypes.memmove(j.pi, pi, 32)
     return j, buf

@@ -6,6 +6,7 @@
 #include "merkle.cuh"
 #include "prover.hpp"
 #include "sha256_air.cuh"
+#include "sha512_air.cuh"
 #include "verifier.hpp"
 
 struct sg_tree {
@@ -258,6 +259,69 @@ int sg_prove_sha256(sg_ctx* c, const uint8_t* msg, size_t len, const uint8_t fs_
     std::vector<uint8_t> b = sg::prove_sha256_message(c, msg, len, fs_binding, phi_mode, true, digest);
     *len_out = b.size();
     if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_sha256: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+int sg_merge_sha512(sg_ctx* c, const uint64_t* lde, size_t n_trace, size_t blowup, const uint64_t* lambdas,
+                    size_t n_blocks, int phi_mode, uint64_t* c_eval) {
+  return guarded(c, [&] {
+    sg::require(lde && lambdas && c_eval, "merge_sha512: null buffer");
+    sg::require(n_trace > 0 && blowup > 0 && n_blocks > 0, "merge_sha512: empty input");
+    const size_t n = n_trace * blowup;
+    In di(lde, (size_t)sg::sha512::WIDTH * n, c->stream);
+    Out dout(c_eval, n, c->stream);
+    sg::merge_hash_device(c, sg::sha512_hash_air(), di.d, n_trace, blowup, lambdas, phi_mode, dout.d, n_blocks);
+    dout.finish();
+  });
+}
+
+int sg_sha512_trace(const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height, size_t* n_blocks,
+                    uint8_t digest[64]) {
+  if ((!msg && len) || !height || !n_blocks || !digest) return SG_EINVAL;
+  try {
+    std::vector<sg::sha512::BlockWitness> wit;
+    uint8_t dg[64];
+    const uint64_t h = sg::sha512_witness(msg, len, &wit, dg);
+    *height = (size_t)h;
+    *n_blocks = wit.size();
+    memcpy(digest, dg, 64);
+    if (!trace || (uint64_t)sg::sha512::WIDTH * h > cap) return SG_ESPACE;
+    sg::sha512_fill_host(wit.data(), wit.size(), h, trace);
+    return SG_OK;
+  } catch (const std::bad_alloc&) {
+    return SG_ENOMEM;
+  }
+}
+
+int sg_sha512_trace_gpu(sg_ctx* c, const uint8_t* msg, size_t len, uint64_t* trace, size_t cap, size_t* height,
+                        size_t* n_blocks, uint8_t digest[64]) {
+  return guarded(c, [&] {
+    sg::require((msg || !len) && height && n_blocks && digest, "sha512_trace_gpu: null argument");
+    std::vector<sg::sha512::BlockWitness> wit;
+    const uint64_t h = sg::sha512_witness(msg, len, &wit, digest);
+    *height = (size_t)h;
+    *n_blocks = wit.size();
+    const uint64_t cells = (uint64_t)sg::sha512::WIDTH * h;
+    if (!trace || cells > cap) throw sg::SgError{SG_ESPACE, "sha512_trace_gpu: trace buffer too small"};
+    Out dout(trace, cells, c->stream);
+    sg::DBuf d_wit((wit.size() * sizeof(sg::sha512::BlockWitness) + 7) / 8, c->stream);
+    sg::cuda_check(cudaMemcpyAsync(d_wit.p, wit.data(), wit.size() * sizeof(sg::sha512::BlockWitness),
+                                   cudaMemcpyHostToDevice, c->stream), "h2d");
+    sg::cuda_check(sg::sha512_expand((const sg::sha512::BlockWitness*)d_wit.p, wit.size(), h, dout.d, c->stream),
+                   "sha512_expand");
+    dout.finish();
+  });
+}
+
+int sg_prove_sha512(sg_ctx* c, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,
+                    uint8_t* proof, size_t cap, size_t* len_out, uint8_t digest[64]) {
+  return guarded(c, [&] {
+    sg::require((msg || !len) && fs_binding && len_out && digest, "prove_sha512: null argument");
+    std::vector<uint8_t> b =
+        sg::prove_hash_message(c, sg::sha512_hash_air(), msg, len, fs_binding, phi_mode, true, digest);
+    *len_out = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_sha512: proof buffer too small"};
     memcpy(proof, b.data(), b.size());
   });
 }

@@ -12,6 +12,7 @@
 #include "merge.cuh"
 #include "merkle.cuh"
 #include "prover.hpp"
+#include "hash_air.hpp"
 #include "sha256_air.cuh"
 #include "stir.cuh"
 #include "verifier.hpp"
@@ -94,18 +95,13 @@ void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_
     cuda_check(cudaMemsetAsync(d_c, 0, n * 8, s), "memset");
     return;
   }
+  if (air == SG_AIR_SHA256) {
+    merge_hash_device(c, sha256_hash_air(), d_lde, n_trace, blowup, lambdas, phi_mode, d_c, n_blocks);
+    return;
+  }
   DBuf phi(n, s);
   DBuf scratch(ntt_scratch_elems(1, log2_exact(n)), s);
-  if (air == SG_AIR_HASH_ROLLUP) {
-    cuda_check(hash_rollup_phi(d_lde, n, blowup, lambdas, phi.p, s), "phi");
-  } else {
-    std::vector<uint64_t> lam(lambdas, lambdas + k);
-    for (auto& x : lam) x %= gl::P;
-    DBuf d_lam(k, s);
-    cuda_check(cudaMemcpyAsync(d_lam.p, lam.data(), k * 8, cudaMemcpyHostToDevice, s), "h2d");
-    cuda_check(sha256_phi(d_lde, n, blowup, n_blocks, d_lam.p, phi.p, s), "sha256 phi");
-    cuda_check(cudaStreamSynchronize(s), "sync");  // lam (host) must outlive the copy
-  }
+  cuda_check(hash_rollup_phi(d_lde, n, blowup, lambdas, phi.p, s), "phi");
   ntt(c, phi.p, phi.p, 1, n, n, log2_exact(n), true, n, scratch.p);
   cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
   ntt(c, d_c, d_c, 1, n, n, log2_exact(n), false, n > n_trace ? n - n_trace : n, scratch.p);
@@ -389,17 +385,39 @@ std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* le
   return proof;
 }
 
-// ------------------------------------------------------------------ SHA-256 pipeline
-// prove_ds_ksk_binding (swarm-dns/src/prover.rs:512-585): multi-block trace on the
-// host (sha256_air.rs:429-472), then LDE x32 -> deep_ali_merge_sha256 with
-// lambda_j = j + 1 -> STIR with build_params(n0, fs_binding) on the device.
-// deep_ali_merge_sha256 without materialising the LDE: LDE point i = r + blowup a
-// lies on coset r, whose evaluations are NTT_{n_trace}(c_k w_n0^{rk}), and point
-// i + blowup is point a + 1 of the same coset. Each coset is produced, folded into
-// Phi[r + blowup a] by the constraint kernel, and dropped.
-void merge_sha256_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, uint64_t blowup, uint64_t n_blocks,
-                         const uint64_t* lambdas, int phi_mode, uint64_t* d_c) {
-  const uint64_t W = sha::WIDTH, n = n_trace * blowup;
+// ------------------------------------------------------------------ hash-AIR pipeline
+// Phi of a hash AIR on a materialised LDE (deep_ali_merge_sha256, lib.rs:453-545;
+// deep_ali_merge_sha512, lib.rs:561-641): point i reads rows i and i + blowup.
+void merge_hash_device(sg_ctx* c, const HashAir& air, const uint64_t* d_lde, uint64_t n_trace, uint64_t blowup,
+                       const uint64_t* lambdas, int phi_mode, uint64_t* d_c, uint64_t n_blocks) {
+  require(pow2(n_trace) && pow2(blowup), "merge: sizes must be powers of 2");
+  require(phi_mode >= 0 && phi_mode <= 2, "merge: bad phi mode");
+  const uint64_t n = n_trace * blowup;
+  const unsigned ln = log2_exact(n);
+  require(ln <= kMaxLogN, "merge: domain larger than 2^28");
+  cudaStream_t s = c->stream;
+  if (!phi_live(phi_mode, n)) {
+    cuda_check(cudaMemsetAsync(d_c, 0, n * 8, s), "memset");
+    return;
+  }
+  std::vector<uint64_t> lam(lambdas, lambdas + air.num_constraints);
+  for (auto& x : lam) x %= gl::P;
+  DBuf phi(n, s), d_lam(lam.size(), s), scratch(ntt_scratch_elems(1, ln), s);
+  cuda_check(cudaMemcpyAsync(d_lam.p, lam.data(), lam.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+  cuda_check(air.phi_points(d_lde, n, blowup, blowup, n_blocks, d_lam.p, phi.p, 1, 0, s), "phi");
+  ntt(c, phi.p, phi.p, 1, n, n, ln, true, n, scratch.p);
+  cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
+  ntt(c, d_c, d_c, 1, n, n, ln, false, n > n_trace ? n - n_trace : n, scratch.p);
+  cuda_check(cudaStreamSynchronize(s), "sync");  // lam (host) must outlive the copy
+}
+
+// The same merge without materialising the LDE: LDE point i = r + blowup a lies
+// on coset r, whose evaluations are NTT_{n_trace}(c_k w_n0^{rk}), and point
+// i + blowup is point a + 1 of the same coset. Each coset is produced, folded
+// into Phi[r + blowup a] by the constraint kernel, and dropped.
+void merge_hash_cosets(sg_ctx* c, const HashAir& air, const uint64_t* d_trace, uint64_t n_trace, uint64_t blowup,
+                       uint64_t n_blocks, const uint64_t* lambdas, int phi_mode, uint64_t* d_c) {
+  const uint64_t W = air.width, n = n_trace * blowup;
   const unsigned lt = log2_exact(n_trace), ln = log2_exact(n);
   require(pow2(n_trace) && pow2(blowup) && ln <= kMaxLogN, "merge: bad sizes");
   cudaStream_t s = c->stream;
@@ -407,7 +425,7 @@ void merge_sha256_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, u
     cuda_check(cudaMemsetAsync(d_c, 0, n * 8, s), "memset");
     return;
   }
-  std::vector<uint64_t> lam(lambdas, lambdas + sha::NUM_CONSTRAINTS);
+  std::vector<uint64_t> lam(lambdas, lambdas + air.num_constraints);
   for (auto& x : lam) x %= gl::P;
   DBuf d_lam(lam.size(), s), phi(n, s), coef(W * n_trace, s), ev(W * n_trace, s);
   DBuf scratch(std::max(ntt_scratch_elems(W, lt), ntt_scratch_elems(1, ln)), s);
@@ -425,7 +443,7 @@ void merge_sha256_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, u
       ntt(c, coef.p, ev.p, (uint32_t)W, n_trace, n_trace, lt, false, n_trace, scratch.p, &twist);
       evals = ev.p;
     }
-    cuda_check(sha256_phi_points(evals, n_trace, 1, 1, n_blocks, d_lam.p, phi.p, blowup, r, s), "coset phi");
+    cuda_check(air.phi_points(evals, n_trace, 1, 1, n_blocks, d_lam.p, phi.p, blowup, r, s), "coset phi");
   }
   ntt(c, phi.p, phi.p, 1, n, n, ln, true, n, scratch.p);
   cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
@@ -433,42 +451,51 @@ void merge_sha256_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, u
   cuda_check(cudaStreamSynchronize(s), "sync");  // lam (host) must outlive the copy
 }
 
-std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
-                                          int phi_mode, bool self_verify, uint8_t digest[32]) {
-  // the host runs the compressions; the 756 trace columns are expanded on the device
-  std::vector<sha::BlockWitness> wit;
-  const uint64_t n_trace = sha256_witness(msg, len, &wit, digest);
-  const uint64_t n_blocks = wit.size();
+// prove_ds_ksk_binding (swarm-dns/src/prover.rs:512-585) for SHA-256, and the
+// same pipeline for SHA-512 (whose reference prover is not written yet,
+// sha512_air.rs:16-19): the host runs the compressions, the trace columns are
+// expanded on the device, then LDE x32 -> merge with lambda_j = j + 1
+// (prover.rs:100-102) -> STIR with build_params(n0, fs_binding).
+std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uint8_t* msg, uint64_t len,
+                                        const uint8_t fs_binding[32], int phi_mode, bool self_verify,
+                                        uint8_t* digest) {
+  std::vector<uint8_t> wit;
+  uint64_t n_blocks = 0;
+  const uint64_t n_trace = air.witness(msg, len, &wit, &n_blocks, digest);
   const uint64_t blowup = 32, n0 = n_trace * blowup;
-  require(log2_exact(n0) <= kMaxLogN, "prove_sha256: message too long for a 2^28 domain");
+  require(log2_exact(n0) <= kMaxLogN, "prove: message too long for a 2^28 domain");
   cudaStream_t s = c->stream;
-  const uint64_t lde_bytes = (uint64_t)sha::WIDTH * n0 * 8;
+  const uint64_t lde_bytes = (uint64_t)air.width * n0 * 8;
   const bool cosets = c->wide_merge == SG_WIDE_MERGE_COSETS ||
                       (c->wide_merge == SG_WIDE_MERGE_AUTO && lde_bytes > (2ull << 30));
-  DBuf d_trace((uint64_t)sha::WIDTH * n_trace, s), d_c(n0, s);
+  DBuf d_trace((uint64_t)air.width * n_trace, s), d_c(n0, s);
   {
-    DBuf d_wit((n_blocks * sizeof(sha::BlockWitness) + 7) / 8, s);
-    cuda_check(cudaMemcpyAsync(d_wit.p, wit.data(), n_blocks * sizeof(sha::BlockWitness), cudaMemcpyHostToDevice, s),
-               "h2d");
-    cuda_check(sha256_expand((const sha::BlockWitness*)d_wit.p, n_blocks, n_trace, d_trace.p, s), "sha256_expand");
+    DBuf d_wit((wit.size() + 7) / 8, s);
+    cuda_check(cudaMemcpyAsync(d_wit.p, wit.data(), wit.size(), cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(air.expand(d_wit.p, n_blocks, n_trace, d_trace.p, s), "trace expand");
+    cuda_check(cudaStreamSynchronize(s), "sync");  // wit (host) must outlive its copy
   }
-  std::vector<uint64_t> lam(sha::NUM_CONSTRAINTS);
-  for (uint64_t j = 0; j < lam.size(); ++j) lam[j] = j + 1;  // comb_coeffs (prover.rs:100-102)
+  std::vector<uint64_t> lam(air.num_constraints);
+  for (uint64_t j = 0; j < lam.size(); ++j) lam[j] = j + 1;
   if (cosets) {
-    merge_sha256_cosets(c, d_trace.p, n_trace, blowup, n_blocks, lam.data(), phi_mode, d_c.p);
+    merge_hash_cosets(c, air, d_trace.p, n_trace, blowup, n_blocks, lam.data(), phi_mode, d_c.p);
   } else {
-    DBuf d_lde((uint64_t)sha::WIDTH * n0, s);
-    lde_device(c, d_trace.p, sha::WIDTH, n_trace, blowup, 1, d_lde.p);
-    merge_device(c, SG_AIR_SHA256, d_lde.p, sha::WIDTH, n_trace, blowup, lam.data(), lam.size(), phi_mode, d_c.p,
-                 n_blocks);
+    DBuf d_lde((uint64_t)air.width * n0, s);
+    lde_device(c, d_trace.p, air.width, n_trace, blowup, 1, d_lde.p);
+    merge_hash_device(c, air, d_lde.p, n_trace, blowup, lam.data(), phi_mode, d_c.p, n_blocks);
   }
-  cuda_check(cudaStreamSynchronize(s), "sync");  // wit (host) must outlive its copy
+  cuda_check(cudaStreamSynchronize(s), "sync");
   sg_fri_params p;
   sg_build_params(n0, fs_binding, 1, &p);
   std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
   if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
     throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
   return proof;
+}
+
+std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
+                                          int phi_mode, bool self_verify, uint8_t digest[32]) {
+  return prove_hash_message(c, sha256_hash_air(), msg, len, fs_binding, phi_mode, self_verify, digest);
 }
 
 }  // namespace sg

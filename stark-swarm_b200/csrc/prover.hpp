@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "context.hpp"
+#include "hash_air.hpp"
 #include "protocol.hpp"
 
 namespace sg {
@@ -13,6 +14,13 @@ void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace
 // lambdas are host values; n_blocks gates the SHA-256 AIR (the AIR registry uses 1)
 void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_t n_trace, uint64_t blowup,
                   const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c, uint64_t n_blocks = 1);
+// Phi + quotient of a hash AIR on a materialised LDE (lambdas: host values).
+void merge_hash_device(sg_ctx* c, const HashAir& air, const uint64_t* d_lde, uint64_t n_trace, uint64_t blowup,
+                       const uint64_t* lambdas, int phi_mode, uint64_t* d_c, uint64_t n_blocks);
+// message -> hash AIR trace -> LDE x32 -> merge -> STIR; digest gets air.digest_bytes.
+std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uint8_t* msg, uint64_t len,
+                                        const uint8_t fs_binding[32], int phi_mode, bool self_verify,
+                                        uint8_t* digest);
 // prove_ds_ksk_binding core: message -> SHA-256 AIR trace -> LDE x32 -> merge -> STIR.
 std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
                                           int phi_mode, bool self_verify, uint8_t digest[32]);

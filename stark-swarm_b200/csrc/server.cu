@@ -22,6 +22,7 @@
 #include "context.hpp"
 #include "prover.hpp"
 #include "sha256_air.cuh"
+#include "sha512_air.cuh"
 
 namespace {
 
@@ -37,7 +38,7 @@ struct Entry {
   int status = SG_OK;
   std::string err;
   std::vector<uint8_t> proof;
-  uint8_t digest[32] = {0};
+  uint8_t digest[64] = {0};
   Clock::time_point t_submit, t_start, t_end;
 };
 
@@ -53,6 +54,11 @@ uint64_t footprint_bytes(const sg_job& j) {
     const uint64_t blocks = (j.input_len + 9 + 63) / 64;
     const uint64_t nt = next_pow2(128 * blocks), n0 = nt * 32;
     return 8 * ((uint64_t)sg::sha::WIDTH * (n0 + 2 * nt) + 16 * n0);
+  }
+  if (j.kind == SG_JOB_SHA512) {
+    const uint64_t blocks = (j.input_len + 17 + 127) / 128;
+    const uint64_t nt = next_pow2(128 * blocks), n0 = nt * 32;
+    return 8 * ((uint64_t)sg::sha512::WIDTH * (n0 + 2 * nt) + 16 * n0);
   }
   const uint64_t nt = next_pow2(j.input_len < 8 ? 8 : j.input_len), n0 = nt * 32;
   return 8 * (4 * n0 + 8 * nt + 16 * n0);
@@ -112,6 +118,9 @@ struct sg_server {
     try {
       if (e->kind == SG_JOB_SHA256) {
         e->proof = sg::prove_sha256_message(c, e->input.data(), e->input.size(), e->pi, e->phi_mode, true, e->digest);
+      } else if (e->kind == SG_JOB_SHA512) {
+        e->proof = sg::prove_hash_message(c, sg::sha512_hash_air(), e->input.data(), e->input.size(), e->pi,
+                                          e->phi_mode, true, e->digest);
       } else {
         const uint64_t n = e->input.size() / 8;
         e->proof = sg::prove_hash_rollup_host_leaves(c, (const uint64_t*)e->input.data(), n, e->pi, e->phi_mode, true);
@@ -169,12 +178,12 @@ void sg_server_destroy(sg_server* s) {
 
 int sg_server_submit(sg_server* s, const sg_job* job, uint64_t* ticket) {
   if (!s || !job || !ticket) return SG_EINVAL;
-  if (job->kind != SG_JOB_SHA256 && job->kind != SG_JOB_HASH_ROLLUP) return SG_EINVAL;
+  if (job->kind != SG_JOB_SHA256 && job->kind != SG_JOB_SHA512 && job->kind != SG_JOB_HASH_ROLLUP) return SG_EINVAL;
   if (job->input_len && !job->input) return SG_EINVAL;
   Entry e;
   e.kind = job->kind;
   e.phi_mode = job->phi_mode;
-  const size_t bytes = job->kind == SG_JOB_SHA256 ? job->input_len : job->input_len * 8;
+  const size_t bytes = job->kind == SG_JOB_HASH_ROLLUP ? job->input_len * 8 : job->input_len;
   e.input.assign((const uint8_t*)job->input, (const uint8_t*)job->input + bytes);
   memcpy(e.pi, job->pi, 32);
   e.footprint = footprint_bytes(*job);
@@ -210,7 +219,7 @@ int sg_server_wait(sg_server* s, uint64_t ticket, sg_job_result* res, uint8_t* p
   memset(res, 0, sizeof *res);
   res->status = e.status;
   res->proof_len = e.proof.size();
-  memcpy(res->digest, e.digest, 32);
+  memcpy(res->digest, e.digest, 64);
   res->queue_ms = ms(e.t_submit, e.t_start);
   res->run_ms = ms(e.t_start, e.t_end);
   res->latency_ms = ms(e.t_submit, e.t_end);

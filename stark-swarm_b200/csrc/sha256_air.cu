@@ -402,11 +402,6 @@ cudaError_t sha256_expand(const sha::BlockWitness* d_wit, uint64_t n_blocks, uin
   return cudaGetLastError();
 }
 
-cudaError_t sha256_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, uint64_t n_blocks, const uint64_t* lambdas,
-                       uint64_t* phi, cudaStream_t s) {
-  return sha256_phi_points(lde, n, blowup, blowup, n_blocks, lambdas, phi, 1, 0, s);
-}
-
 cudaError_t sha256_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, uint64_t row_div, uint64_t n_blocks,
                               const uint64_t* lambdas, uint64_t* phi, uint64_t out_stride, uint64_t out_off,
                               cudaStream_t s) {
@@ -419,4 +414,27 @@ cudaError_t sha256_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, 
   return cudaGetLastError();
 }
 
+}  // namespace sg
+
+#include "hash_air.hpp"
+namespace sg {
+namespace {
+uint64_t sha256_witness_blob(const uint8_t* msg, uint64_t len, std::vector<uint8_t>* blob, uint64_t* n_blocks,
+                             uint8_t* digest) {
+  std::vector<sha::BlockWitness> wit;
+  const uint64_t h = sha256_witness(msg, len, &wit, digest);
+  *n_blocks = wit.size();
+  blob->resize(wit.size() * sizeof(sha::BlockWitness));
+  memcpy(blob->data(), wit.data(), blob->size());
+  return h;
+}
+cudaError_t sha256_expand_blob(const void* d_wit, uint64_t n_blocks, uint64_t h, uint64_t* d_trace, cudaStream_t s) {
+  return sha256_expand((const sha::BlockWitness*)d_wit, n_blocks, h, d_trace, s);
+}
+}  // namespace
+const HashAir& sha256_hash_air() {
+  static const HashAir a{"sha256", sha::WIDTH, sha::NUM_CONSTRAINTS, 32, sha256_witness_blob, sha256_expand_blob,
+                         sha256_phi_points};
+  return a;
+}
 }  // namespace sg

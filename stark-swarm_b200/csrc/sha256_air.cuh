@@ -54,15 +54,12 @@ cudaError_t sha256_expand(const sha::BlockWitness* d_wit, uint64_t n_blocks, uin
 uint64_t sha256_build_trace(const uint8_t* msg, uint64_t len, std::vector<uint64_t>* trace, uint64_t* n_blocks,
                             uint8_t digest[32]);
 
-// Phi(w^i) = sum_j lambda_j C_j(row i, row (i + blowup) mod n) for the SHA-256 AIR
-// (eval_sha256_constraints, sha256_air.rs:956-1294, with trace_row = i / blowup).
-// lde: WIDTH x n column-major on the device; lambdas: NUM_CONSTRAINTS values on the device.
-cudaError_t sha256_phi(const uint64_t* lde, uint64_t n, uint64_t blowup, uint64_t n_blocks, const uint64_t* lambdas,
-                       uint64_t* phi, cudaStream_t s);
-// General form: evals holds WIDTH columns of n points; point i pairs with
-// point (i + step) mod n, has trace row i / row_div, and its value goes to
-// phi[out_off + i * out_stride]. One coset r of the LDE (points r + blowup a)
-// is (step, row_div, out_stride, out_off) = (1, 1, blowup, r).
+// Phi = sum_j lambda_j C_j for the SHA-256 AIR (eval_sha256_constraints,
+// sha256_air.rs:956-1294) at the points of an evaluation buffer: evals holds
+// WIDTH columns of n points; point i pairs with point (i + step) mod n, has trace
+// row i / row_div, and its value goes to phi[out_off + i * out_stride]. The whole
+// LDE is (step, row_div, out_stride, out_off) = (blowup, blowup, 1, 0); one coset
+// r of it (points r + blowup a) is (1, 1, blowup, r). lambdas are on the device.
 cudaError_t sha256_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, uint64_t row_div, uint64_t n_blocks,
                               const uint64_t* lambdas, uint64_t* phi, uint64_t out_stride, uint64_t out_off,
                               cudaStream_t s);

@@ -88,6 +88,10 @@ def lib():
             L.orc_prove_sha256.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_int,
                                            ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
                                            ctypes.c_char_p]
+            L.orc_merge_sha512.argtypes = L.orc_merge_sha256.argtypes
+            L.orc_sha512_trace.argtypes = L.orc_sha256_trace.argtypes
+            L.orc_sha512_eval.argtypes = L.orc_sha256_eval.argtypes
+            L.orc_prove_sha512.argtypes = L.orc_prove_sha256.argtypes
             _lib = L
     return _lib
 
@@ -249,3 +253,48 @@ def fp6_inv(a):
     O = (ctypes.c_uint64 * 6)()
     assert lib().orc_fp6_inv(A, O) == 0
     return list(O)
+
+
+SHA512_WIDTH, SHA512_K = 1510, 1526
+SHA512_H0_LO = 1066
+
+
+def sha512_trace(msg: bytes):
+    """build_sha512_trace_multi -> ((1510, height) uint64, n_blocks)"""
+    nb = (len(msg) + 17 + 127) // 128
+    height = 128
+    while height < 128 * nb:
+        height *= 2
+    out = np.zeros(SHA512_WIDTH * height, dtype=np.uint64)
+    h, n = ctypes.c_size_t(), ctypes.c_size_t()
+    rc = lib().orc_sha512_trace(msg, len(msg), _ptr(out), out.size, ctypes.byref(h), ctypes.byref(n))
+    assert rc == 0, rc
+    return out[: SHA512_WIDTH * h.value].reshape(SHA512_WIDTH, h.value), n.value
+
+
+def sha512_eval(cur, nxt, row, n_blocks):
+    cur = np.ascontiguousarray(cur, dtype=np.uint64)
+    nxt = np.ascontiguousarray(nxt, dtype=np.uint64)
+    out = np.zeros(SHA512_K, dtype=np.uint64)
+    lib().orc_sha512_eval(_ptr(cur), _ptr(nxt), row, n_blocks, _ptr(out))
+    return out
+
+
+def merge_sha512(lde_cols, n_trace, blowup, lambdas, n_blocks, phi_mode=PHI_PARALLEL_GATE):
+    lde_cols = np.ascontiguousarray(lde_cols, dtype=np.uint64)
+    lam = np.ascontiguousarray(lambdas, dtype=np.uint64)
+    out = np.zeros(n_trace * blowup, dtype=np.uint64)
+    rc = lib().orc_merge_sha512(_ptr(lde_cols), n_trace, blowup, _ptr(lam), n_blocks, phi_mode, _ptr(out))
+    assert rc == 0, rc
+    return out
+
+
+def prove_sha512(msg: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
+    """SHA-512 AIR proof -> (proof bytes, 64-byte digest read from the H-state)"""
+    cap = 1 << 26
+    buf = ctypes.create_string_buffer(cap)
+    ln = ctypes.c_size_t()
+    dg = ctypes.create_string_buffer(64)
+    rc = lib().orc_prove_sha512(msg, len(msg), fs_binding, phi_mode, buf, cap, ctypes.byref(ln), dg)
+    assert rc == 0, rc
+    return buf.raw[:ln.value], dg.raw

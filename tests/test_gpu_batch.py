@@ -1,4 +1,5 @@
-"""Batched and served proving: every proof made in a mix of concurrent jobs is
+"""Batched and served proving: every proof made in a mix of concurrent jobs
+(SHA-256, SHA-512 and HashRollup) is
 byte-identical to the same job proved alone (oracle), under several stream
 counts and an HBM budget tight enough to serialise admission; the server
 accepts submissions while earlier jobs are running."""
@@ -18,10 +19,14 @@ def _mix(n, seed):
     jobs, want = [], []
     for i in range(n):
         pi = hashlib.sha3_256(b"job%d" % i).digest()
-        if i % 3 == 2:
+        if i % 4 == 2:
             leaves = rng.integers(0, O.P, int(rng.integers(1, 3000)), dtype=np.uint64)
             jobs.append((2, leaves, pi))
             want.append((O.prove_hash_rollup(leaves, pi), None))
+        elif i % 4 == 3:
+            msg = rng.integers(0, 256, int(rng.integers(1, 240)), dtype=np.uint8).tobytes()
+            jobs.append((3, msg, pi))
+            want.append(O.prove_sha512(msg, pi))
         else:
             ln = int(np.clip(rng.lognormal(np.log(120), 0.6), 40, 600))
             msg = rng.integers(0, 256, ln, dtype=np.uint8).tobytes()
@@ -39,7 +44,7 @@ def test_batch_matches_single_proofs(ctx, streams, budget):
         assert res.status == 0
         assert proof == wproof
         if wdg is not None:
-            assert bytes(res.digest) == wdg
+            assert bytes(res.digest)[:len(wdg)] == wdg
         assert res.latency_ms >= res.run_ms >= 0
 
 

@@ -109,3 +109,15 @@ def test_sha256_trace_builder_matches_oracle(msg):
     assert nb == onb
     assert np.array_equal(tr, otr)
     assert digest == hashlib.sha256(msg).digest()
+
+
+@pytest.mark.parametrize("msg", [b"abc", b"", b"a" * 111, b"b" * 112, bytes(range(256)) + b"z" * 50])
+def test_sha512_trace_builder_matches_oracle(msg):
+    # host-side trace builder (build_sha512_trace_multi) of the library vs the oracle
+    import hashlib
+    sg = load_sgpu()
+    tr, nb, digest = sg.build_sha512_trace_multi(msg)
+    otr, onb = O.sha512_trace(msg)
+    assert nb == onb
+    assert np.array_equal(tr, otr)
+    assert digest == hashlib.sha512(msg).digest()
