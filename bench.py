@@ -252,20 +252,27 @@ def sha256_large(sg, ctx, blocks, reps, cpu_threads):
 
 
 def serving(sg, ctx, rates, n_jobs, streams, seed=7):
-    """Poisson arrivals of SHA-256 AIR proof requests over record-length messages
-    (lognormal, median 120 B, clipped to 40-600 B: 1-10 blocks), admitted by the
-    continuous-batching server under a 160 GB HBM budget; p50/p99 latency from
-    submit to result, and throughput against one proof at a time."""
+    """Poisson arrivals of hash-AIR proof requests over record-length messages
+    (lognormal, median 120 B, clipped to 40-600 B), 80 % SHA-256 and 20 % SHA-512,
+    admitted by the continuous-batching server under a 160 GB HBM budget; p50/p99
+    latency from submit to result, and throughput against one proof at a time."""
     rng = np.random.default_rng(seed)
     lens = np.clip(np.round(rng.lognormal(np.log(120), 0.6, n_jobs)), 40, 600).astype(int)
     msgs = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in lens]
+    kinds = [sg.JOB_SHA512 if u < 0.2 else sg.JOB_SHA256 for u in rng.random(n_jobs)]
     pis = [hashlib.sha3_256(b"serve-%d" % i).digest() for i in range(n_jobs)]
-    alone = {i: ctx.prove_sha256(msgs[i], pis[i])[0] for i in range(8)}  # reference bytes, one at a time
+
+    def prove_one(i):
+        f = ctx.prove_sha512 if kinds[i] == sg.JOB_SHA512 else ctx.prove_sha256
+        return f(msgs[i], pis[i])[0]
+
+    alone = {i: prove_one(i) for i in range(12)}  # reference bytes, one at a time
     t0 = time.perf_counter()
     for i in range(n_jobs):
-        ctx.prove_sha256(msgs[i], pis[i])
+        prove_one(i)
     plain = n_jobs / (time.perf_counter() - t0)
-    out = {"workload": "SHA-256 AIR proofs, messages lognormal(median 120 B) clipped 40-600 B, Poisson arrivals",
+    out = {"workload": "hash-AIR proofs (80 % SHA-256, 20 % SHA-512), messages lognormal(median 120 B) "
+                       "clipped 40-600 B, Poisson arrivals",
            "jobs_per_rate": n_jobs, "streams": streams, "hbm_budget_gb": 160, "plain_proofs_per_s": plain,
            "rates": []}
     for lam in rates:
@@ -279,7 +286,7 @@ def serving(sg, ctx, rates, n_jobs, streams, seed=7):
                 wait = due - time.perf_counter()
                 if wait > 0:
                     time.sleep(wait)
-                tickets.append(srv.submit(sg.JOB_SHA256, msgs[i], pis[i]))
+                tickets.append(srv.submit(kinds[i], msgs[i], pis[i]))
             res = [srv.wait(t) for t in tickets]
             wall = time.perf_counter() - start
         for i, want in alone.items():
