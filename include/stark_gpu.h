@@ -46,7 +46,7 @@ typedef struct {
   uint64_t seed_z;
   uint64_t d_final;
   int32_t coeff_commit_final; /* bool */
-  int32_t stir;               /* bool; this library proves the STIR branch */
+  int32_t stir;               /* bool: STIR (1) or classic DEEP-FRI (0) */
   int32_t has_pi;             /* bool: public_inputs_hash is Some */
   uint8_t pi_hash[32];
 } sg_fri_params;
@@ -216,14 +216,16 @@ void sg_merkle_free(sg_tree* tree);
  * coeff_commit_final, d_final = 1, public_inputs_hash = pi (NULL = None). */
 void sg_build_params(size_t n0, const uint8_t* pi32, int stir, sg_fri_params* out);
 
-/* Replaces deep_fri_prove::<SexticExt> (deep_ali/src/fri.rs:1900-2055), STIR
- * branch: writes the exact ark-serialize (Compress::Yes) bytes of the
- * DeepFriProof. f0: n0 values. */
+/* Replaces deep_fri_prove::<SexticExt> (deep_ali/src/fri.rs:1900-2055) in both
+ * branches, selected by params->stir: STIR (s0 proximity queries against the
+ * coset-packed f0 tree) or classic DEEP-FRI (fri.rs:1724-1807: per-layer DEEP
+ * quotients, r fold queries through every layer). Writes the exact ark-serialize
+ * (Compress::Yes) bytes of the DeepFriProof. f0: n0 values. */
 int sg_stir_prove(sg_ctx* ctx, const uint64_t* f0, size_t n0, const sg_fri_params* params, uint8_t* proof,
                   size_t cap, size_t* len);
 
-/* Replaces deep_fri_verify::<SexticExt> (deep_ali/src/fri.rs:2136-2521), STIR
- * branch, on serialized proof bytes. Returns 1 accept, 0 reject. Host only. */
+/* Replaces deep_fri_verify::<SexticExt> (deep_ali/src/fri.rs:2136-2707), both
+ * branches, on serialized proof bytes. Returns 1 accept, 0 reject. Host only. */
 int sg_stir_verify(const uint8_t* proof, size_t len, const sg_fri_params* params);
 
 /* Core of prove_inner_shard / prove_outer_rollup (swarm-dns/src/prover.rs:148-304):

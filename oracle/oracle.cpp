@@ -10,6 +10,7 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -296,7 +297,20 @@ struct ProxQuery {
   MerkleOpening l1_open;
 };
 
+// classic FRI query (fri.rs:1236-1263): per-layer refs (i, child_pos,
+// parent_index, parent_pos), payloads (f, s, q), the f0 opening, final index
+struct ClassicQuery {
+  std::vector<std::array<uint64_t, 4>> refs;
+  std::vector<std::array<Fp6, 3>> pay;
+  MerkleOpening f0_open;
+  uint64_t final_index = 0;
+};
+
 struct StirProof {
+  bool stir = true;
+  std::vector<std::vector<MerkleOpening>> layer_open;  // classic: layer_proofs.layers[ell].openings
+  std::vector<MerkleOpening> f0_openings;               // classic
+  std::vector<ClassicQuery> queries;                    // classic
   Digest root_f0;
   std::vector<Digest> roots;
   std::vector<Fp6> fz;
@@ -311,13 +325,159 @@ struct StirProof {
   std::vector<ProxQuery> prox;
 };
 
+// ------------------------------------------------------------------ classic FRI
+// fri.rs:255-336 compute_q_layer_ext_on_ext: f(z) from the component iFFTs and
+// Horner, then q_i = (f_i - f(z)) / (w^i - z).
+void q_layer(const std::vector<Fp6>& f, const Fp6& z, Fp omega, std::vector<Fp6>* q, Fp6* fz) {
+  const size_t n = f.size();
+  std::vector<std::vector<Fp>> comp(6, std::vector<Fp>(n));
+  for (size_t i = 0; i < n; ++i)
+    for (int c = 0; c < 6; ++c) comp[c][i] = f[i].comp(c);
+  for (int c = 0; c < 6; ++c) ifft(comp[c].data(), n);
+  Fp6 r = e_zero();
+  for (size_t k = n; k-- > 0;) {
+    Fp6 ck;
+    for (int c = 0; c < 6; ++c) ck.set_comp(c, comp[c][k]);
+    r = e_add(e_mul(r, z), ck);
+  }
+  *fz = r;
+  q->assign(n, e_zero());
+#pragma omp parallel for schedule(static) if (n >= 1024)
+  for (long i = 0; i < (long)n; ++i) {
+    Fp6 d = e_sub(e_from(pow(omega, (uint64_t)i)), z), di;
+    if (!e_inv(d, &di)) throw std::runtime_error("DEEP point on the domain");
+    (*q)[i] = e_mul(e_sub(f[i], r), di);
+  }
+}
+
+// fri.rs:1356-1362 ext_leaf_fields: the 18 components of (f, s, q)
+std::vector<Fp> ext_leaf_rows(const std::vector<Fp6>& f, const std::vector<Fp6>& s, const std::vector<Fp6>& q) {
+  std::vector<Fp> rows(f.size() * 18);
+  for (size_t i = 0; i < f.size(); ++i)
+    for (int k = 0; k < 6; ++k) {
+      rows[i * 18 + k] = f[i].comp(k);
+      rows[i * 18 + 6 + k] = s[i].comp(k);
+      rows[i * 18 + 12 + k] = q[i].comp(k);
+    }
+  return rows;
+}
+
+// fri.rs:1900-2055 deep_fri_prove, classic branch: fri.rs:1398-1718
+// fri_build_transcript (stir = false) and fri.rs:1724-1807 fri_prove_queries.
+StirProof classic_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
+  const size_t n0 = f0.size(), L = p.schedule_len;
+  const bool use_cc = p.coeff_commit_final && L > 0;
+  const size_t normal = use_cc ? L - 1 : L;
+  StirProof pr;
+  pr.stir = false;
+  pr.n0 = n0;
+  pr.omega0 = root_of_unity(log2_exact(n0));
+  Transcript tr("FRI/FS");
+  bind_statement(tr, p, n0);
+  // f0 tree (fri.rs:1060-1076): one value per leaf, arity pick(n0, 16), label 0xFF
+  TreeCfg f0cfg = layer_cfg(n0, 16, 0xFF);
+  MerkleTree f0tree(f0cfg.ar, f0cfg.label);
+  f0tree.build(f0, 1);
+  pr.root_f0 = f0tree.root();
+  tr.absorb_bytes(pr.root_f0.data(), 32);
+  const Fp6 z = tr.challenge_ext("z_fp3");
+
+  std::vector<std::vector<Fp6>> layers, s_layers, q_layers;
+  layers.emplace_back(n0);
+  for (size_t i = 0; i < n0; ++i) layers[0][i] = e_from(f0[i]);
+  std::vector<MerkleTree> trees;
+  size_t cur = n0;
+  auto commit = [&](size_t ell, size_t m) {
+    TreeCfg c = layer_cfg(cur, m, ell);
+    MerkleTree t(c.ar, c.label);
+    t.build(ext_leaf_rows(layers[ell], s_layers[ell], q_layers[ell]), 18);
+    pr.roots.push_back(t.root());
+    trees.push_back(std::move(t));
+  };
+  for (size_t ell = 0; ell < normal; ++ell) {
+    const size_t m = p.schedule[ell], nn = cur / m;
+    const Fp6 alpha = tr.challenge_ext("alpha");
+    const Fp omega = root_of_unity(log2_exact(cur));
+    std::vector<Fp6> q;
+    Fp6 fz;
+    q_layer(layers[ell], z, omega, &q, &fz);
+    pr.fz.push_back(fz);
+    auto tuples = extract_coset_coeffs(layers[ell], omega, m);
+    std::vector<Fp6> next = fold(tuples, alpha);
+    std::vector<Fp6> sl(cur);  // compute_s_layer_from_coeffs (fri.rs:773-789)
+    for (size_t i = 0; i < cur; ++i) sl[i] = next[i % nn];
+    s_layers.push_back(std::move(sl));
+    q_layers.push_back(std::move(q));
+    commit(ell, m);
+    tr.absorb_ext(fz);
+    tr.absorb_bytes(pr.roots.back().data(), 32);
+    layers.push_back(std::move(next));
+    cur = nn;
+  }
+  pr.has_ct = pr.has_croot = false;
+  if (use_cc) {
+    const size_t ell = L - 1, m = p.schedule[ell], nf = cur / m;
+    const Fp omega = root_of_unity(log2_exact(cur));
+    std::vector<Fp6> q;
+    Fp6 fz;
+    q_layer(layers[ell], z, omega, &q, &fz);
+    pr.fz.push_back(fz);
+    s_layers.emplace_back(cur, e_zero());
+    q_layers.push_back(std::move(q));
+    commit(ell, m);
+    tr.absorb_ext(fz);
+    tr.absorb_bytes(pr.roots.back().data(), 32);
+    auto tuples = extract_coset_coeffs(layers[ell], omega, m);
+    TreeCfg cc = layer_cfg(nf, 16, 0xFE);
+    MerkleTree ct(cc.ar, cc.label);
+    std::vector<Fp> rows(nf * m * 6);
+    for (size_t b = 0; b < nf; ++b)
+      for (size_t i = 0; i < m; ++i)
+        for (int k = 0; k < 6; ++k) rows[(b * m + i) * 6 + k] = tuples[b][i].comp(k);
+    ct.build(rows, m * 6);
+    pr.coeff_root = ct.root();
+    tr.absorb_bytes(pr.coeff_root.data(), 32);
+    const Fp6 alpha = tr.challenge_ext("alpha");
+    (void)tr.challenge_ext("beta_deg");
+    layers.push_back(fold(tuples, alpha));
+    pr.coeff_tuples = std::move(tuples);
+    pr.has_ct = pr.has_croot = true;
+    cur = nf;
+  }
+  auto all = ext_evals_to_coeffs(layers[L]);
+  const size_t d_final = std::min<size_t>(p.d_final, all.size());
+  pr.final_coeffs.assign(all.begin(), all.begin() + d_final);
+  for (auto& c : pr.final_coeffs) tr.absorb_ext(c);
+  const Fp query_seed = tr.challenge_field("query_seed");
+
+  pr.layer_open.resize(L);
+  for (size_t qi = 0; qi < p.r; ++qi) {
+    ClassicQuery cq;
+    size_t i = query_index(query_seed, qi, n0), n = n0;
+    for (size_t ell = 0; ell < L; ++ell) {
+      const size_t m = p.schedule[ell], nn = n / m;
+      cq.refs.push_back({(uint64_t)i, (uint64_t)(i % m), (uint64_t)(i % nn), 0});
+      cq.pay.push_back({layers[ell][i], s_layers[ell][i], q_layers[ell][i]});
+      pr.layer_open[ell].push_back(trees[ell].open(i));
+      i %= nn;
+      n = nn;
+    }
+    cq.final_index = i;
+    cq.f0_open = f0tree.open(cq.refs[0][0]);
+    pr.f0_openings.push_back(cq.f0_open);
+    pr.queries.push_back(std::move(cq));
+  }
+  return pr;
+}
+
 // ------------------------------------------------------------------ prover
 // fri.rs:1900-2055 deep_fri_prove (STIR branch) with fri.rs:1398-1718
 // fri_build_transcript and fri.rs:1813-1893 stir_prove_proximity_queries.
 StirProof stir_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
   size_t n0 = f0.size();
   size_t L = p.schedule_len;
-  if (!p.stir || L == 0) throw std::runtime_error("oracle implements the STIR branch only");
+  if (L == 0) throw std::runtime_error("empty folding schedule");
+  if (!p.stir) return classic_prove(f0, p);
   bool use_cc = p.coeff_commit_final && L > 0;
   size_t normal = use_cc ? L - 1 : L;
   StirProof pr;
@@ -462,9 +622,24 @@ std::vector<uint8_t> serialize(const StirProof& pr) {
   w.dig(pr.root_f0);
   w.u64(pr.roots.size());
   for (auto& r : pr.roots) w.dig(r);
-  w.u64(0);  // layer_proofs.layers (classic FRI only)
-  w.u64(0);  // f0_openings
-  w.u64(0);  // queries
+  w.u64(pr.layer_open.size());  // layer_proofs.layers (classic FRI only)
+  for (auto& lo : pr.layer_open) {
+    w.u64(lo.size());
+    for (auto& o : lo) w.opening(o);
+  }
+  w.u64(pr.f0_openings.size());
+  for (auto& o : pr.f0_openings) w.opening(o);
+  w.u64(pr.queries.size());
+  for (auto& q : pr.queries) {
+    w.u64(q.refs.size());
+    for (auto& r : q.refs)
+      for (int k = 0; k < 4; ++k) w.u64(r[k]);
+    w.u64(q.pay.size());
+    for (auto& pl : q.pay)
+      for (int k = 0; k < 3; ++k) w.ext(pl[k]);
+    w.opening(q.f0_open);
+    w.u64(q.final_index);
+  }
   w.u64(pr.fz.size());
   for (auto& e : pr.fz) w.ext(e);
   w.u64(pr.final_coeffs.size());
@@ -481,7 +656,11 @@ std::vector<uint8_t> serialize(const StirProof& pr) {
   }
   w.u8(pr.has_croot);
   if (pr.has_croot) w.dig(pr.coeff_root);
-  w.u8(1);
+  w.u8(pr.stir);
+  if (!pr.stir) {
+    w.u8(0);  // stir_proximity_queries: None
+    return w.b;
+  }
   w.u64(pr.coset_evals.size());
   for (auto& v : pr.coset_evals) {
     w.u64(v.size());
@@ -557,7 +736,26 @@ StirProof deserialize(const uint8_t* b, size_t n) {
   pr.root_f0 = r.dig();
   uint64_t k = r.len();
   for (uint64_t i = 0; i < k; ++i) pr.roots.push_back(r.dig());
-  if (r.u64() != 0 || r.u64() != 0 || r.u64() != 0) throw std::runtime_error("classic FRI fields in STIR proof");
+  k = r.len();
+  for (uint64_t i = 0; i < k; ++i) {
+    uint64_t m = r.len();
+    std::vector<MerkleOpening> lo;
+    for (uint64_t j = 0; j < m; ++j) lo.push_back(r.opening());
+    pr.layer_open.push_back(std::move(lo));
+  }
+  k = r.len();
+  for (uint64_t i = 0; i < k; ++i) pr.f0_openings.push_back(r.opening());
+  k = r.len();
+  for (uint64_t i = 0; i < k; ++i) {
+    ClassicQuery q;
+    uint64_t m = r.len();
+    for (uint64_t j = 0; j < m; ++j) q.refs.push_back({r.u64(), r.u64(), r.u64(), r.u64()});
+    m = r.len();
+    for (uint64_t j = 0; j < m; ++j) q.pay.push_back({r.ext(), r.ext(), r.ext()});
+    q.f0_open = r.opening();
+    q.final_index = r.u64();
+    pr.queries.push_back(std::move(q));
+  }
   k = r.len();
   for (uint64_t i = 0; i < k; ++i) pr.fz.push_back(r.ext());
   k = r.len();
@@ -576,7 +774,12 @@ StirProof deserialize(const uint8_t* b, size_t n) {
   }
   pr.has_croot = r.flag();
   if (pr.has_croot) pr.coeff_root = r.dig();
-  if (!r.flag()) throw std::runtime_error("missing stir_coset_evals");
+  pr.stir = r.flag();
+  if (!pr.stir) {
+    if (r.flag()) throw std::runtime_error("proximity queries without coset evaluations");
+    if (r.o != n) throw std::runtime_error("trailing bytes");
+    return pr;
+  }
   k = r.len();
   for (uint64_t i = 0; i < k; ++i) {
     uint64_t m = r.len();
@@ -605,10 +808,124 @@ StirProof deserialize(const uint8_t* b, size_t n) {
 }
 
 // ------------------------------------------------------------------ verifier
+// coeff-commit checks shared by both branches (fri.rs:2275-2322): tuple shapes,
+// the recomputed coefficient root, and the batched degree check.
+bool coeff_commit_ok(const StirProof& pr, const orc_fri_params& p, const std::vector<size_t>& sizes,
+                     const Fp6& beta) {
+  const size_t L = p.schedule_len;
+  if (!pr.has_ct) return false;
+  const size_t nf = sizes[L], mf = p.schedule[L - 1];
+  if (pr.coeff_tuples.size() != nf) return false;
+  for (auto& t : pr.coeff_tuples)
+    if (t.size() != mf) return false;
+  TreeCfg cc = layer_cfg(nf, 16, 0xFE);
+  MerkleTree ct(cc.ar, cc.label);
+  std::vector<Fp> rows;
+  for (auto& t : pr.coeff_tuples)
+    for (auto& e : t)
+      for (int k = 0; k < 6; ++k) rows.push_back(e.comp(k));
+  ct.build(rows, mf * 6);
+  if (ct.root() != pr.coeff_root) return false;
+  return batched_degree_check(pr.coeff_tuples, beta, p.d_final);
+}
+
+// fri.rs:2136-2258 + 2517-2707 deep_fri_verify, classic branch.
+bool classic_verify(const StirProof& pr, const orc_fri_params& p) {
+  const size_t L = p.schedule_len;
+  if (L == 0 || pr.stir) return false;
+  std::vector<size_t> sizes{(size_t)pr.n0};
+  for (size_t i = 0; i < L; ++i) {
+    if (p.schedule[i] == 0 || sizes.back() % p.schedule[i]) return false;
+    sizes.push_back(sizes.back() / p.schedule[i]);
+  }
+  const bool use_cc = p.coeff_commit_final && L > 0;
+  if (pr.roots.size() < L || pr.fz.size() < L) return false;
+  Transcript tr("FRI/FS");
+  bind_statement(tr, p, pr.n0);
+  tr.absorb_bytes(pr.root_f0.data(), 32);
+  const Fp6 z = tr.challenge_ext("z_fp3");
+  std::vector<Fp6> alphas;
+  Fp6 beta;
+  for (size_t ell = 0; ell < L; ++ell) {
+    const bool last_cc = use_cc && ell == L - 1;
+    if (!last_cc) alphas.push_back(tr.challenge_ext("alpha"));
+    tr.absorb_ext(pr.fz[ell]);
+    tr.absorb_bytes(pr.roots[ell].data(), 32);
+    if (last_cc) {
+      if (!pr.has_croot) return false;
+      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      alphas.push_back(tr.challenge_ext("alpha"));
+      beta = tr.challenge_ext("beta_deg");
+    }
+  }
+  for (auto& c : pr.final_coeffs) tr.absorb_ext(c);
+  const Fp query_seed = tr.challenge_field("query_seed");
+  if (pr.final_coeffs.size() != p.d_final) return false;
+  if (use_cc && !coeff_commit_ok(pr, p, sizes, beta)) return false;
+  const Fp omega_final = sizes[L] >= 2 ? root_of_unity(log2_exact(sizes[L])) : Fp::raw(1);
+  if (pr.queries.size() < p.r || pr.layer_open.size() < L) return false;
+  TreeCfg f0cfg = layer_cfg(pr.n0, 16, 0xFF);
+  for (size_t qi = 0; qi < p.r; ++qi) {
+    const ClassicQuery& q = pr.queries[qi];
+    if (q.refs.size() < L || q.pay.size() < L) return false;
+    const size_t i0 = query_index(query_seed, qi, pr.n0);
+    size_t ei = i0;
+    for (size_t ell = 0; ell < L; ++ell) {
+      if (q.refs[ell][0] != ei) return false;
+      ei %= sizes[ell] / p.schedule[ell];
+    }
+    if (q.final_index != ei) return false;
+    if (!verify_opening(f0cfg.ar, f0cfg.label, pr.root_f0, q.f0_open)) return false;
+    for (int k = 1; k < 6; ++k)
+      if (!q.pay[0][0].comp(k).is_zero()) return false;  // layer 0 is in the base field
+    const Fp f0v = q.pay[0][0].comp(0);
+    if (leaf_hash(f0cfg.ar[0], f0cfg.label, q.f0_open.index, &f0v, 1) != q.f0_open.leaf) return false;
+    if (q.f0_open.index != i0) return false;
+    for (size_t ell = 0; ell < L; ++ell) {
+      if (pr.layer_open[ell].size() <= qi) return false;
+      const MerkleOpening& o = pr.layer_open[ell][qi];
+      const auto& pl = q.pay[ell];
+      const size_t i = q.refs[ell][0];
+      TreeCfg cfg = layer_cfg(sizes[ell], p.schedule[ell], ell);
+      if (!verify_opening(cfg.ar, cfg.label, pr.roots[ell], o)) return false;
+      if (o.index != i) return false;
+      Fp vals[18];
+      for (int t = 0; t < 3; ++t)
+        for (int k = 0; k < 6; ++k) vals[t * 6 + k] = pl[t].comp(k);
+      if (leaf_hash(cfg.ar[0], cfg.label, o.index, vals, 18) != o.leaf) return false;
+      const Fp omega = root_of_unity(log2_exact(sizes[ell]));
+      const Fp xi = pow(omega, i);
+      // DEEP check: q (x_i - z) = f - f(z)
+      if (e_mul(pl[2], e_sub(e_from(xi), z)) != e_sub(pl[0], pr.fz[ell])) return false;
+      const Fp6 x_final = e_from(pow(omega_final, q.final_index));
+      if (ell == L - 1 && use_cc) {
+        const size_t m = p.schedule[ell];
+        if (q.final_index >= pr.coeff_tuples.size()) return false;
+        const auto& t = pr.coeff_tuples[q.final_index];
+        Fp6 h = e_zero(), fv = e_zero(), ap = e_one();
+        Fp xp = Fp::raw(1);
+        for (size_t k = 0; k < m; ++k) {
+          h = e_add(h, e_scale(t[k], xp));
+          xp = xp * xi;
+          fv = e_add(fv, e_mul(t[k], ap));
+          ap = e_mul(ap, alphas[L - 1]);
+        }
+        if (pl[0] != h) return false;
+        if (fv != eval_poly_ext(pr.final_coeffs, x_final)) return false;
+      } else {
+        const Fp6 f_next = ell + 1 < L ? q.pay[ell + 1][0] : eval_poly_ext(pr.final_coeffs, x_final);
+        if (pl[1] != f_next) return false;
+      }
+    }
+  }
+  return true;
+}
+
 // fri.rs:2136-2521 deep_fri_verify, STIR branch.
 bool stir_verify(const StirProof& pr, const orc_fri_params& p) {
   size_t L = p.schedule_len;
-  if (!p.stir || L == 0) return false;
+  if (!p.stir) return classic_verify(pr, p);
+  if (L == 0 || !pr.stir) return false;
   std::vector<size_t> sizes{(size_t)pr.n0};
   for (size_t i = 0; i < L; ++i) {
     if (sizes.back() % p.schedule[i]) return false;

@@ -6,8 +6,8 @@ C ABI is declared in include/stark_gpu.h:
 
   lde_trace_columns      deep_ali/src/trace_import.rs:251-281
   deep_ali_merge_general deep_ali/src/lib.rs:343-437
-  deep_fri_prove         deep_ali/src/fri.rs:1900-2055 (STIR branch, SexticExt)
-  deep_fri_verify        deep_ali/src/fri.rs:2136-2521 (STIR branch)
+  deep_fri_prove         deep_ali/src/fri.rs:1900-2055 (STIR and classic branches, SexticExt)
+  deep_fri_verify        deep_ali/src/fri.rs:2136-2707 (STIR and classic branches)
   MerkleTreeChannel      merkle/src/lib.rs:356-512
   make_schedule / build_params / prove_hash_rollup   swarm-dns/src/prover.rs:53-304
   deep_ali_merge_sha256 / prove_sha256 (prove_ds_ksk_binding core)
@@ -514,7 +514,8 @@ class Context:
 
     # ---------------------------------------------------------------- STIR
     def deep_fri_prove(self, f0, domain0, params: FriParams) -> bytes:
-        """STIR prove; returns the ark-serialize (Compress::Yes) bytes of the DeepFriProof."""
+        """deep_fri_prove (STIR or classic DEEP-FRI, per params.stir); returns the
+        ark-serialize (Compress::Yes) bytes of the DeepFriProof."""
         ip, _ki, host = _addr(f0)
         n0 = domain0.size if isinstance(domain0, FriDomain) else int(domain0)
         cap = 1 << 24

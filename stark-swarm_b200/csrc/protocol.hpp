@@ -163,7 +163,23 @@ struct ProxQuery {
   Opening l1_open;
 };
 
+// classic FRI query (fri.rs:1236-1263): per-layer refs (i, child_pos,
+// parent_index, parent_pos), payloads (f, s, q), the f0 opening, final index
+struct ClassicQuery {
+  std::vector<std::array<uint64_t, 4>> refs;
+  std::vector<std::array<gl::Fp6, 3>> pay;
+  Opening f0_open;
+  uint64_t final_index = 0;
+};
+
+// DeepFriProof (fri.rs:1286-1300). `stir` selects which optional payload is
+// present: STIR coset evaluations + proximity queries, or the classic layer
+// openings, f0 openings and fold queries.
 struct StirProof {
+  bool stir = true;
+  std::vector<std::vector<Opening>> layer_open;
+  std::vector<Opening> f0_openings;
+  std::vector<ClassicQuery> queries;
   Digest root_f0{};
   std::vector<Digest> roots;
   std::vector<gl::Fp6> fz;
@@ -204,9 +220,24 @@ inline std::vector<uint8_t> encode_proof(const StirProof& pr) {
   w.dig(pr.root_f0);
   w.u64(pr.roots.size());
   for (auto& r : pr.roots) w.dig(r);
-  w.u64(0);  // layer_proofs.layers: classic FRI only
-  w.u64(0);  // f0_openings: classic FRI only
-  w.u64(0);  // queries: classic FRI only
+  w.u64(pr.layer_open.size());  // layer_proofs.layers (classic FRI)
+  for (auto& lo : pr.layer_open) {
+    w.u64(lo.size());
+    for (auto& o : lo) w.opening(o);
+  }
+  w.u64(pr.f0_openings.size());
+  for (auto& o : pr.f0_openings) w.opening(o);
+  w.u64(pr.queries.size());
+  for (auto& q : pr.queries) {
+    w.u64(q.refs.size());
+    for (auto& r : q.refs)
+      for (int k = 0; k < 4; ++k) w.u64(r[k]);
+    w.u64(q.pay.size());
+    for (auto& pl : q.pay)
+      for (int k = 0; k < 3; ++k) w.ext(pl[k]);
+    w.opening(q.f0_open);
+    w.u64(q.final_index);
+  }
   w.u64(pr.fz.size());
   for (auto& e : pr.fz) w.ext(e);
   w.u64(pr.final_coeffs.size());
@@ -223,7 +254,11 @@ inline std::vector<uint8_t> encode_proof(const StirProof& pr) {
   }
   w.u8(pr.has_croot);
   if (pr.has_croot) w.dig(pr.coeff_root);
-  w.u8(1);
+  w.u8(pr.stir);  // stir_coset_evals: Some only for STIR
+  if (!pr.stir) {
+    w.u8(0);  // stir_proximity_queries: None
+    return w.b;
+  }
   w.u64(pr.coset_evals.size());
   for (auto& v : pr.coset_evals) {
     w.u64(v.size());
@@ -312,7 +347,34 @@ inline StirProof decode_proof(const uint8_t* b, size_t n) {
   pr.root_f0 = r.dig();
   uint64_t k = r.len();
   for (uint64_t i = 0; i < k; ++i) pr.roots.push_back(r.dig());
-  if (r.u64() != 0 || r.u64() != 0 || r.u64() != 0) throw std::runtime_error("classic FRI payload in STIR proof");
+  k = r.len();
+  for (uint64_t i = 0; i < k; ++i) {
+    uint64_t m = r.len();
+    std::vector<Opening> lo;
+    for (uint64_t j = 0; j < m; ++j) lo.push_back(r.opening());
+    pr.layer_open.push_back(std::move(lo));
+  }
+  k = r.len();
+  for (uint64_t i = 0; i < k; ++i) pr.f0_openings.push_back(r.opening());
+  k = r.len();
+  for (uint64_t i = 0; i < k; ++i) {
+    ClassicQuery q;
+    uint64_t m = r.len();
+    for (uint64_t j = 0; j < m; ++j) {
+      std::array<uint64_t, 4> ref;
+      for (auto& x : ref) x = r.u64();
+      q.refs.push_back(ref);
+    }
+    m = r.len();
+    for (uint64_t j = 0; j < m; ++j) {
+      std::array<gl::Fp6, 3> pl;
+      for (auto& e : pl) e = r.ext();
+      q.pay.push_back(pl);
+    }
+    q.f0_open = r.opening();
+    q.final_index = r.u64();
+    pr.queries.push_back(std::move(q));
+  }
   k = r.len();
   for (uint64_t i = 0; i < k; ++i) pr.fz.push_back(r.ext());
   k = r.len();
@@ -331,7 +393,12 @@ inline StirProof decode_proof(const uint8_t* b, size_t n) {
   }
   pr.has_croot = r.flag();
   if (pr.has_croot) pr.coeff_root = r.dig();
-  if (!r.flag()) throw std::runtime_error("missing stir_coset_evals");
+  pr.stir = r.flag();
+  if (!pr.stir) {
+    if (r.flag()) throw std::runtime_error("proximity queries without coset evaluations");
+    if (r.o != n) throw std::runtime_error("trailing bytes");
+    return pr;
+  }
   k = r.len();
   for (uint64_t i = 0; i < k; ++i) {
     uint64_t m = r.len();

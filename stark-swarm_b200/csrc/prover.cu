@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "context.hpp"
+#include "fri_classic.cuh"
 #include "gl.cuh"
 #include "merge.cuh"
 #include "merkle.cuh"
@@ -134,13 +135,228 @@ Digest digest_at(const std::vector<uint64_t>& h, size_t lane0) {
 
 }  // namespace
 
+// fri.rs:1900-2055 deep_fri_prove, classic branch (stir = false): fri.rs:1398-1718
+// fri_build_transcript and fri.rs:1724-1807 fri_prove_queries. Per layer the
+// DEEP quotient q = (f - f(z)) / (x - z) and s (the folded next layer, broadcast
+// over its fibres) are committed with f as 18-component leaves; r fold queries
+// open every layer at i, i mod n_1, ... .
+std::vector<uint8_t> classic_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p,
+                                          const std::vector<uint64_t>& sizes) {
+  cudaStream_t s = c->stream;
+  const uint64_t L = p.schedule_len;
+  const bool use_cc = p.coeff_commit_final != 0;
+  StirProof pr;
+  pr.stir = false;
+  pr.n0 = n0;
+  pr.omega0 = gl::root_of_unity(log2_exact(n0));
+  HostTranscript tr("FRI/FS");
+  bind_statement(tr, p, n0);
+
+  // f0 tree (fri.rs:1060-1076): one value per leaf, arity pick(n0, 16), label 0xFF
+  Tree f0t;
+  f0t.make(n0, layer_arities(n0, 16), 0xFF, s);
+  cuda_check(tree_hash_leaves(f0t.t, d_f0, 1, n0, 0, s), "f0 leaves");
+  cuda_check(tree_hash_levels(f0t.t, s), "f0 levels");
+  std::vector<uint64_t> h;
+  d2h(&h, f0t.t.d + 4 * f0t.t.off.back(), 4, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+  pr.root_f0 = digest_at(h, 0);
+  tr.absorb_bytes(pr.root_f0.data(), 32);
+  const gl::Fp6 z = tr.challenge_ext("z_fp3");
+
+  const uint64_t work = std::max<uint64_t>(n0, 6 * sizes[1]);
+  uint64_t scratch_len = ntt_scratch_elems(1, log2_exact(n0));
+  for (uint64_t i = 1; i <= L; ++i) scratch_len = std::max(scratch_len, ntt_scratch_elems(6, log2_exact(sizes[i])));
+  DBuf coef(work, s), scratch(scratch_len, s), partials(ood_partials_len(n0, 2), s), evals(2 * 6, s);
+  std::vector<DBuf> planes(L + 1), mats(L);
+  std::vector<Tree> trees(L);
+  DBuf tuples;
+  Tree ctree;
+  std::vector<gl::Fp6> alphas;
+
+  const uint64_t* cur = d_f0;
+  bool base = true;
+  for (uint64_t ell = 0; ell < L; ++ell) {
+    const uint64_t m = p.schedule[ell], n = sizes[ell], nn = n / m;
+    const unsigned lg = log2_exact(n);
+    const bool last_cc = use_cc && ell == L - 1;
+    gl::Fp6 alpha = gl::e_zero();
+    if (!last_cc) alpha = tr.challenge_ext("alpha");
+    // f(z): component iNTT, then the first of the two OOD points z, -z
+    ntt(c, cur, coef.p, base ? 1 : 6, n, n, lg, true, n, scratch.p);
+    cuda_check(ood_evaluate(coef.p, base, n, 2, z, partials.p, evals.p, s), "f(z)");
+    std::vector<uint64_t> fzh;
+    d2h(&fzh, evals.p, 6, s);
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    gl::Fp6 fz;
+    for (int k = 0; k < 6; ++k) fz.c[k] = fzh[k];
+    pr.fz.push_back(fz);
+    // leaf matrix rows 12..17: the DEEP quotient
+    mats[ell].alloc(18 * n, s);
+    cuda_check(deep_quotient(cur, base, n, (int)lg, c->tw.d_fwd_lo, c->tw.d_fwd_hi, z, fz, mats[ell].p + 12 * n, s),
+               "deep quotient");
+    // coset coefficients -> next layer (or the committed tuples of the last layer)
+    FoldArgs fa{};
+    fa.f = cur;
+    fa.base = base;
+    fa.n = n;
+    fa.log_n = (int)lg;
+    fa.m = (int)m;
+    fa.alpha = alpha;
+    fa.tw_inv_lo = c->tw.d_inv_lo;
+    fa.tw_inv_hi = c->tw.d_inv_hi;
+    if (!last_cc) {
+      planes[ell + 1].alloc(6 * nn, s);
+      fa.next = planes[ell + 1].p;
+    } else {
+      tuples.alloc(6 * m * nn, s);
+      fa.tuples = tuples.p;
+    }
+    cuda_check(stir_fold(fa, s), "fold");
+    cuda_check(fill_leaf_rows(cur, base, last_cc ? nullptr : planes[ell + 1].p, nn, n, mats[ell].p, s), "leaf rows");
+    trees[ell].make(n, layer_arities(n, m), ell, s);
+    cuda_check(tree_hash_leaves(trees[ell].t, mats[ell].p, 18, n, 0, s), "layer leaves");
+    cuda_check(tree_hash_levels(trees[ell].t, s), "layer levels");
+    if (last_cc) {
+      ctree.make(nn, layer_arities(nn, 16), 0xFE, s);
+      cuda_check(tree_hash_leaves(ctree.t, tuples.p, (uint32_t)(6 * m), nn, 0, s), "coeff leaves");
+      cuda_check(tree_hash_levels(ctree.t, s), "coeff levels");
+    }
+    std::vector<uint64_t> root, croot, tup;
+    d2h(&root, trees[ell].t.d + 4 * trees[ell].t.off.back(), 4, s);
+    if (last_cc) {
+      d2h(&croot, ctree.t.d + 4 * ctree.t.off.back(), 4, s);
+      d2h(&tup, tuples.p, 6 * m * nn, s);
+    }
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    pr.roots.push_back(digest_at(root, 0));
+    tr.absorb_ext(fz);
+    tr.absorb_bytes(pr.roots.back().data(), 32);
+    if (last_cc) {
+      pr.has_ct = pr.has_croot = true;
+      pr.coeff_root = digest_at(croot, 0);
+      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      alpha = tr.challenge_ext("alpha");
+      (void)tr.challenge_ext("beta_deg");
+      pr.coeff_tuples.assign(nn, std::vector<gl::Fp6>(m));
+      for (uint64_t b = 0; b < nn; ++b)
+        for (uint64_t k = 0; k < m; ++k)
+          for (int q = 0; q < 6; ++q) pr.coeff_tuples[b][k].c[q] = tup[(k * 6 + q) * nn + b];
+      planes[ell + 1].alloc(6 * nn, s);
+      cuda_check(fold_tuples(tuples.p, nn, (int)m, alpha, planes[ell + 1].p, s), "final fold");
+    }
+    alphas.push_back(alpha);
+    cur = planes[ell + 1].p;
+    base = false;
+  }
+
+  // final polynomial coefficients (fri.rs:1915-1935) and the query seed
+  const uint64_t nf = sizes[L];
+  if (nf > 1) {
+    ntt(c, cur, coef.p, 6, nf, nf, log2_exact(nf), true, nf, scratch.p);
+  } else {
+    cuda_check(cudaMemcpyAsync(coef.p, cur, 6 * 8, cudaMemcpyDeviceToDevice, s), "copy");
+  }
+  std::vector<uint64_t> fc;
+  d2h(&fc, coef.p, 6 * nf, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+  for (uint64_t k = 0; k < std::min<uint64_t>(p.d_final, nf); ++k) {
+    gl::Fp6 e;
+    for (int q = 0; q < 6; ++q) e.c[q] = fc[q * nf + k];
+    pr.final_coeffs.push_back(e);
+    tr.absorb_ext(e);
+  }
+  const uint64_t query_seed = tr.challenge_field("query_seed");
+
+  // fri_prove_queries (fri.rs:1724-1807): index chains on the host, one gather per
+  // buffer for the payload values and the opening digests
+  std::vector<std::vector<uint64_t>> chain(p.r);
+  for (uint64_t q = 0; q < p.r; ++q) {
+    uint64_t i = query_index(query_seed, q, n0);
+    for (uint64_t ell = 0; ell < L; ++ell) {
+      chain[q].push_back(i);
+      i %= sizes[ell] / p.schedule[ell];
+    }
+    chain[q].push_back(i);  // final index
+  }
+  auto gather_openings = [&](const DevTree& t, const std::vector<uint64_t>& idx) {
+    std::vector<uint64_t> di;
+    for (uint64_t i : idx) opening_indices(t, i, &di);
+    DBuf d_i(di.size(), s), d_o(4 * di.size(), s);
+    std::vector<uint64_t> got;
+    if (!di.empty()) {
+      cuda_check(cudaMemcpyAsync(d_i.p, di.data(), di.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+      cuda_check(gather_digests(t.d, d_i.p, di.size(), d_o.p, s), "gather paths");
+      d2h(&got, d_o.p, 4 * di.size(), s);
+    }
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    std::vector<Opening> out;
+    size_t pos = 0;
+    for (uint64_t i : idx) {
+      Opening o;
+      o.index = i;
+      o.leaf = digest_at(got, pos);
+      pos += 4;
+      for (size_t l = 0; l + 1 < t.len.size(); ++l) {
+        std::vector<Digest> sib(t.arity[l] - 1);
+        for (auto& d : sib) {
+          d = digest_at(got, pos);
+          pos += 4;
+        }
+        o.path.push_back(std::move(sib));
+      }
+      out.push_back(std::move(o));
+    }
+    return out;
+  };
+  auto gather_values = [&](const uint64_t* src, const std::vector<uint64_t>& idx) {
+    DBuf d_i(idx.size(), s), d_o(idx.size(), s);
+    std::vector<uint64_t> got;
+    if (!idx.empty()) {
+      cuda_check(cudaMemcpyAsync(d_i.p, idx.data(), idx.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+      cuda_check(gather_u64(src, d_i.p, idx.size(), d_o.p, s), "gather values");
+      d2h(&got, d_o.p, idx.size(), s);
+    }
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    return got;
+  };
+  std::vector<uint64_t> i0s(p.r);
+  for (uint64_t q = 0; q < p.r; ++q) i0s[q] = chain[q][0];
+  const std::vector<Opening> f0_open = gather_openings(f0t.t, i0s);
+  pr.queries.resize(p.r);
+  pr.layer_open.resize(L);
+  for (uint64_t ell = 0; ell < L; ++ell) {
+    const uint64_t n = sizes[ell], m = p.schedule[ell], nn = n / m;
+    std::vector<uint64_t> idx(p.r), vidx;
+    for (uint64_t q = 0; q < p.r; ++q) {
+      idx[q] = chain[q][ell];
+      for (uint64_t k = 0; k < 18; ++k) vidx.push_back(k * n + idx[q]);
+    }
+    pr.layer_open[ell] = gather_openings(trees[ell].t, idx);
+    const std::vector<uint64_t> v = gather_values(mats[ell].p, vidx);
+    for (uint64_t q = 0; q < p.r; ++q) {
+      const uint64_t i = idx[q];
+      pr.queries[q].refs.push_back({i, i % m, i % nn, 0});
+      std::array<gl::Fp6, 3> pl;
+      for (int t = 0; t < 3; ++t)
+        for (int k = 0; k < 6; ++k) pl[t].c[k] = v[q * 18 + t * 6 + k];
+      pr.queries[q].pay.push_back(pl);
+    }
+  }
+  for (uint64_t q = 0; q < p.r; ++q) {
+    pr.queries[q].f0_open = f0_open[q];
+    pr.queries[q].final_index = chain[q][L];
+    pr.f0_openings.push_back(f0_open[q]);
+  }
+  return encode_proof(pr);
+}
+
 std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p) {
   cudaStream_t s = c->stream;
   const uint64_t L = p.schedule_len;
-  require(p.stir != 0, "stir_prove: only the STIR branch (params.stir = true) is implemented");
   require(L >= 1 && L <= SG_MAX_SCHEDULE, "stir_prove: empty or oversized schedule");
   require(pow2(n0) && n0 >= 2 && log2_exact(n0) <= kMaxLogN, "stir_prove: n0 must be a power of 2 in [2, 2^28]");
-  require(p.s0 <= (1u << 20), "stir_prove: s0 too large");
+  require(p.s0 <= (1u << 20) && p.r <= (1u << 20), "stir_prove: too many queries");
   std::vector<uint64_t> sizes{n0};
   for (uint64_t i = 0; i < L; ++i) {
     const uint64_t m = p.schedule[i];
@@ -148,6 +364,7 @@ std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t
     require(sizes.back() % m == 0, "stir_prove: schedule does not divide the domain");
     sizes.push_back(sizes.back() / m);
   }
+  if (!p.stir) return classic_prove_device(c, d_f0, n0, p, sizes);
   const bool use_cc = p.coeff_commit_final != 0;
 
   StirProof pr;

@@ -1,4 +1,5 @@
-// verifier.cpp — host STIR verifier (deep_ali/src/fri.rs:2136-2521, STIR branch).
+// verifier.cpp — host DEEP-FRI verifier (deep_ali/src/fri.rs:2136-2707), STIR and
+// classic branches.
 //
 // Used for the self-verification the reference worker performs before it
 // reports a proof (swarm-dns/src/prover.rs:189-192) and exported as
@@ -146,19 +147,140 @@ Digest tree_root_host(const std::vector<std::vector<uint64_t>>& leaves, const st
   return lv[0];
 }
 
+// coefficient commitment + batched degree check (fri.rs:816-856, 2275-2322)
+bool coeff_commit_ok(const StirProof& pr, const sg_fri_params& p, const std::vector<uint64_t>& sizes,
+                     const Fp6& beta) {
+  const uint64_t L = p.schedule_len;
+  if (!pr.has_ct) return false;
+  const uint64_t nf = sizes[L], mf = p.schedule[L - 1];
+  if (pr.coeff_tuples.size() != nf) return false;
+  std::vector<std::vector<uint64_t>> leaves;
+  for (auto& t : pr.coeff_tuples) {
+    if (t.size() != mf) return false;
+    std::vector<uint64_t> row;
+    for (auto& e : t)
+      for (int c = 0; c < 6; ++c) row.push_back(e.c[c]);
+    leaves.push_back(std::move(row));
+  }
+  if (tree_root_host(leaves, layer_arities(nf, 16), 0xFE) != pr.coeff_root) return false;
+  std::vector<Fp6> g(nf);
+  for (uint64_t b = 0; b < nf; ++b) {
+    Fp6 s = gl::e_zero(), bp = gl::e_one();
+    for (uint64_t i = 0; i < mf; ++i) {
+      s = gl::e_add(s, gl::e_mul(pr.coeff_tuples[b][i], bp));
+      bp = gl::e_mul(bp, beta);
+    }
+    g[b] = s;
+  }
+  if (nf > 1) {
+    uint64_t wi = gl::inv(gl::root_of_unity(log2u(nf))), ninv = gl::inv(nf);
+    for (int c = 0; c < 6; ++c) {
+      std::vector<uint64_t> col(nf);
+      for (uint64_t i = 0; i < nf; ++i) col[i] = g[i].c[c];
+      host_dft(col, wi);
+      for (uint64_t k = p.d_final; k < nf; ++k)
+        if (gl::mul(col[k], ninv) != 0) return false;
+    }
+  }
+  return true;
+}
+
+// fri.rs:2136-2258 + 2517-2707 deep_fri_verify, classic branch: fold queries
+// through every layer tree, the DEEP identity q (x - z) = f - f(z) at each
+// opened point, s against the next layer, and the final coefficient tuple.
+bool classic_verify(const StirProof& pr, const sg_fri_params& p, const std::vector<uint64_t>& sizes) {
+  const uint64_t L = p.schedule_len;
+  const bool use_cc = p.coeff_commit_final && L > 0;
+  if (pr.stir || pr.roots.size() < L || pr.fz.size() < L) return false;
+  HostTranscript tr("FRI/FS");
+  bind_statement(tr, p, pr.n0);
+  tr.absorb_bytes(pr.root_f0.data(), 32);
+  const Fp6 z = tr.challenge_ext("z_fp3");
+  Fp6 beta = gl::e_zero();
+  std::vector<Fp6> alphas;
+  for (uint64_t ell = 0; ell < L; ++ell) {
+    const bool last_cc = use_cc && ell == L - 1;
+    if (!last_cc) alphas.push_back(tr.challenge_ext("alpha"));
+    tr.absorb_ext(pr.fz[ell]);
+    tr.absorb_bytes(pr.roots[ell].data(), 32);
+    if (last_cc) {
+      if (!pr.has_croot) return false;
+      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      alphas.push_back(tr.challenge_ext("alpha"));
+      beta = tr.challenge_ext("beta_deg");
+    }
+  }
+  for (auto& c : pr.final_coeffs) tr.absorb_ext(c);
+  const uint64_t query_seed = tr.challenge_field("query_seed");
+  if (pr.final_coeffs.size() != p.d_final) return false;
+  if (use_cc && !coeff_commit_ok(pr, p, sizes, beta)) return false;
+  const uint64_t omega_final = sizes[L] >= 2 ? gl::root_of_unity(log2u(sizes[L])) : 1;
+  if (pr.queries.size() < p.r || pr.layer_open.size() < L) return false;
+  const auto f0_ar = layer_arities(pr.n0, 16);
+  for (uint64_t qi = 0; qi < p.r; ++qi) {
+    const ClassicQuery& q = pr.queries[qi];
+    if (q.refs.size() < L || q.pay.size() < L) return false;
+    const uint64_t i0 = query_index(query_seed, qi, pr.n0);
+    uint64_t ei = i0;
+    for (uint64_t ell = 0; ell < L; ++ell) {
+      if (q.refs[ell][0] != ei) return false;
+      ei %= sizes[ell] / p.schedule[ell];
+    }
+    if (q.final_index != ei) return false;
+    if (!verify_opening(f0_ar, 0xFF, pr.root_f0, q.f0_open) || q.f0_open.index != i0) return false;
+    for (int k = 1; k < 6; ++k)
+      if (q.pay[0][0].c[k] != 0) return false;  // layer 0 is in the base field
+    if (leaf_hash(f0_ar[0], 0xFF, q.f0_open.index, q.pay[0][0].c, 1) != q.f0_open.leaf) return false;
+    const Fp6 x_final = gl::e_from(gl::pow(omega_final, q.final_index));
+    for (uint64_t ell = 0; ell < L; ++ell) {
+      if (pr.layer_open[ell].size() <= qi) return false;
+      const Opening& o = pr.layer_open[ell][qi];
+      const auto& pl = q.pay[ell];
+      const uint64_t i = q.refs[ell][0];
+      const auto ar = layer_arities(sizes[ell], p.schedule[ell]);
+      if (!verify_opening(ar, ell, pr.roots[ell], o) || o.index != i) return false;
+      uint64_t vals[18];
+      for (int t = 0; t < 3; ++t)
+        for (int k = 0; k < 6; ++k) vals[t * 6 + k] = pl[t].c[k];
+      if (leaf_hash(ar[0], ell, o.index, vals, 18) != o.leaf) return false;
+      const uint64_t xi = gl::pow(gl::root_of_unity(log2u(sizes[ell])), i);
+      if (!gl::e_eq(gl::e_mul(pl[2], gl::e_sub(gl::e_from(xi), z)), gl::e_sub(pl[0], pr.fz[ell]))) return false;
+      if (ell == L - 1 && use_cc) {
+        const uint64_t m = p.schedule[ell];
+        if (q.final_index >= pr.coeff_tuples.size()) return false;
+        const auto& t = pr.coeff_tuples[q.final_index];
+        Fp6 h = gl::e_zero(), fv = gl::e_zero(), ap = gl::e_one();
+        uint64_t xp = 1;
+        for (uint64_t k = 0; k < m; ++k) {
+          h = gl::e_add(h, gl::e_scale(t[k], xp));
+          xp = gl::mul(xp, xi);
+          fv = gl::e_add(fv, gl::e_mul(t[k], ap));
+          ap = gl::e_mul(ap, alphas[L - 1]);
+        }
+        if (!gl::e_eq(pl[0], h) || !gl::e_eq(fv, eval_poly(pr.final_coeffs, x_final))) return false;
+      } else {
+        const Fp6 f_next = ell + 1 < L ? q.pay[ell + 1][0] : eval_poly(pr.final_coeffs, x_final);
+        if (!gl::e_eq(pl[1], f_next)) return false;
+      }
+    }
+  }
+  return true;
+}
+
 }  // namespace
 
 bool stir_verify(const StirProof& pr, const sg_fri_params& p) {
   const uint64_t L = p.schedule_len;
-  if (!p.stir || L == 0 || L > SG_MAX_SCHEDULE) return false;
+  if (L == 0 || L > SG_MAX_SCHEDULE) return false;
+  if (pr.n0 == 0 || (pr.n0 & (pr.n0 - 1)) || pr.n0 > (1ull << 32)) return false;
   std::vector<uint64_t> sizes{pr.n0};
   for (uint64_t i = 0; i < L; ++i) {
     if (p.schedule[i] < 2 || sizes.back() % p.schedule[i]) return false;
     sizes.push_back(sizes.back() / p.schedule[i]);
   }
-  if (pr.n0 == 0 || (pr.n0 & (pr.n0 - 1)) || pr.n0 > (1ull << 32)) return false;
+  if (!p.stir) return classic_verify(pr, p, sizes);
   const bool use_cc = p.coeff_commit_final && L > 0;
-  if (pr.roots.size() < L || pr.coset_evals.size() < L) return false;
+  if (!pr.stir || pr.roots.size() < L || pr.coset_evals.size() < L) return false;
   HostTranscript tr("FRI/FS");
   bind_statement(tr, p, pr.n0);
   tr.absorb_bytes(pr.root_f0.data(), 32);
@@ -209,40 +331,7 @@ bool stir_verify(const StirProof& pr, const sg_fri_params& p) {
     if (!gl::e_eq(acc, expect)) return false;
   }
 
-  // coefficient commitment + batched degree check (fri.rs:816-856)
-  if (use_cc) {
-    if (!pr.has_ct) return false;
-    const uint64_t nf = sizes[L], mf = p.schedule[L - 1];
-    if (pr.coeff_tuples.size() != nf) return false;
-    std::vector<std::vector<uint64_t>> leaves;
-    for (auto& t : pr.coeff_tuples) {
-      if (t.size() != mf) return false;
-      std::vector<uint64_t> row;
-      for (auto& e : t)
-        for (int c = 0; c < 6; ++c) row.push_back(e.c[c]);
-      leaves.push_back(std::move(row));
-    }
-    if (tree_root_host(leaves, layer_arities(nf, 16), 0xFE) != pr.coeff_root) return false;
-    std::vector<Fp6> g(nf);
-    for (uint64_t b = 0; b < nf; ++b) {
-      Fp6 s = gl::e_zero(), bp = gl::e_one();
-      for (uint64_t i = 0; i < mf; ++i) {
-        s = gl::e_add(s, gl::e_mul(pr.coeff_tuples[b][i], bp));
-        bp = gl::e_mul(bp, beta);
-      }
-      g[b] = s;
-    }
-    if (nf > 1) {
-      uint64_t wi = gl::inv(gl::root_of_unity(log2u(nf))), ninv = gl::inv(nf);
-      for (int c = 0; c < 6; ++c) {
-        std::vector<uint64_t> col(nf);
-        for (uint64_t i = 0; i < nf; ++i) col[i] = g[i].c[c];
-        host_dft(col, wi);
-        for (uint64_t k = p.d_final; k < nf; ++k)
-          if (gl::mul(col[k], ninv) != 0) return false;
-      }
-    }
-  }
+  if (use_cc && !coeff_commit_ok(pr, p, sizes, beta)) return false;
 
   // s0 proximity queries against the packed f0 tree and the layer-1 tree
   if (pr.prox.size() != p.s0) return false;

@@ -204,8 +204,8 @@ def test_stir_prove_rejects_bad_arguments(sgpu, ctx):
         ctx.deep_fri_prove(f0, 64, sgpu.FriParams.new([3, 2]))
     with pytest.raises(sgpu.StarkGpuError):
         ctx.deep_fri_prove(f0, 64, sgpu.FriParams.new([8, 8, 8]))
-    with pytest.raises(sgpu.StarkGpuError):
-        ctx.deep_fri_prove(f0, 64, sgpu.FriParams.new([8, 8], stir=False))
+    with pytest.raises(sgpu.StarkGpuError):  # classic branch: query count beyond the 2^20 bound
+        ctx.deep_fri_prove(f0, 64, sgpu.FriParams.new([8, 8], stir=False, r=1 << 21))
     with pytest.raises(sgpu.StarkGpuError):
         ctx.deep_fri_prove(f0[:48], 48, sgpu.FriParams.new([8, 2]))
 
@@ -276,3 +276,39 @@ def test_lde_into_three_pass_domain(ctx):
                 acc = (acc * x + cf) % P
             assert int(out[c, i]) == acc, (c, i)
     assert np.array_equal(out[:, ::4096], tr)  # coset 0 of the LDE is the trace itself
+
+
+def _classic_params(sg, n0, pi, sched=None, cc=True):
+    po = O.build_params(n0, pi, stir=False)
+    if sched is None:
+        return sg.build_params(n0, pi, stir=False), po
+    po.schedule_len = len(sched)
+    for i, m in enumerate(sched):
+        po.schedule[i] = m
+    po.coeff_commit_final = int(cc)
+    ps = sg.FriParams.new(sched, coeff_commit_final=cc, stir=False, public_inputs_hash=pi)
+    return ps, po
+
+
+@pytest.mark.parametrize("log_n0,sched,cc,low", [
+    (1, None, True, True), (3, None, True, True), (6, None, True, True), (10, None, True, True),
+    (13, None, True, True), (16, None, True, False), (8, [4, 2, 2, 2, 2], True, True),
+    (9, [8, 2, 2, 2, 2, 2, 2], False, True), (10, [16, 4, 2, 2, 2], True, True),
+])
+def test_classic_fri_matches_oracle(sgpu, ctx, log_n0, sched, cc, low):
+    # classic DEEP-FRI branch (params.stir = false): byte-identical to the oracle; a
+    # low-degree f0 also passes the library's verifier
+    rng = np.random.default_rng(1000 + log_n0)
+    n0 = 1 << log_n0
+    if low:
+        c = np.zeros(n0, dtype=np.uint64)
+        c[: max(1, n0 // 32)] = rand_field(rng, max(1, n0 // 32))
+        f0 = O.ntt(c)
+    else:
+        f0 = rand_field(rng, n0)
+    pi = rng.bytes(32)
+    ps, po = _classic_params(sgpu, n0, pi, sched, cc)
+    got = ctx.deep_fri_prove(f0, sgpu.FriDomain(n0), ps)
+    assert got == O.stir_prove(f0, po)
+    if low:
+        assert sgpu.deep_fri_verify(ps, got) and O.stir_verify(got, po)

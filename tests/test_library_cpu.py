@@ -121,3 +121,21 @@ def test_sha512_trace_builder_matches_oracle(msg):
     assert nb == onb
     assert np.array_equal(tr, otr)
     assert digest == hashlib.sha512(msg).digest()
+
+
+@pytest.mark.parametrize("log_n0", [3, 6, 9])
+def test_product_verifier_accepts_oracle_classic_fri(log_n0):
+    import hashlib
+    sg = load_sgpu()
+    n0 = 1 << log_n0
+    rng = np.random.default_rng(log_n0)
+    c = np.zeros(n0, dtype=np.uint64)
+    c[: max(1, n0 // 32)] = rng.integers(0, O.P, max(1, n0 // 32), dtype=np.uint64)
+    f0 = O.ntt(c)
+    pi = hashlib.sha3_256(b"cls").digest()
+    proof = O.stir_prove(f0, O.build_params(n0, pi, stir=False))
+    ps = sg.build_params(n0, pi, stir=False)
+    assert sg.deep_fri_verify(ps, proof)
+    bad = bytearray(proof)
+    bad[100] ^= 1
+    assert not sg.deep_fri_verify(ps, bytes(bad))

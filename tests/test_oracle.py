@@ -230,3 +230,30 @@ def test_prove_verify_round_trip_low_degree(lg):
     params = O.build_params(n0, os.urandom(32))
     proof = O.stir_prove(f0, params)
     assert O.stir_verify(proof, params)
+
+
+def _low_degree_f0(n0, seed):
+    rng = np.random.default_rng(seed)
+    c = np.zeros(n0, dtype=np.uint64)
+    k = max(1, n0 // 32)
+    c[:k] = rng.integers(0, O.P, k, dtype=np.uint64)
+    return O.ntt(c)
+
+
+@pytest.mark.parametrize("log_n0", [2, 4, 7, 10])
+def test_classic_fri_oracle_round_trip(log_n0):
+    # classic DEEP-FRI branch (params.stir = false): the oracle's proof verifies,
+    # and changing a checked byte (root, layer opening, payload, fz, final poly) is rejected
+    import hashlib
+    n0 = 1 << log_n0
+    f0 = _low_degree_f0(n0, log_n0)
+    p = O.build_params(n0, hashlib.sha3_256(b"classic").digest(), stir=False)
+    assert p.sched == [2] * log_n0
+    proof = O.stir_prove(f0, p)
+    assert O.stir_verify(proof, p)
+    for pos in (5, 40, 300, len(proof) - 60):
+        bad = bytearray(proof)
+        bad[pos] ^= 0x10
+        assert not O.stir_verify(bytes(bad), p), pos
+    p2 = O.build_params(n0, hashlib.sha3_256(b"other").digest(), stir=False)
+    assert not O.stir_verify(proof, p2)
