@@ -324,6 +324,8 @@ def main():
                     help="blocks of the large SHA-256 trace proof (8192 = 2^20 rows; 0 skips it)")
     ap.add_argument("--serve-jobs", type=int, default=200, help="jobs per arrival rate in the serving sweep (0 skips)")
     ap.add_argument("--serve-rates", default="50,200,500,1000,2000", help="Poisson arrival rates (req/s)")
+    ap.add_argument("--no-classic-fri", dest="classic_fri", action="store_false",
+                    help="skip the classic DEEP-FRI timing")
     ap.add_argument("--columns", type=int, default=64,
                     help="trace columns (64 = the benchmark workload; fewer for small profiling captures)")
     args = ap.parse_args()
@@ -477,6 +479,33 @@ def main():
                            "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
         cfg1["batched_over_plain"] = cfg1["batched"]["proofs_per_s"] / cfg1["plain"]["proofs_per_s"]
 
+    # classic DEEP-FRI (params.stir = false, the branch of the reference's published
+    # scaling numbers) on the same 2^23 column, beside the STIR proof of the step
+    classic = None
+    if args.classic_fri:
+        pc = sg.build_params(N0, PI_HASH, stir=False)
+        ref_c = ctx.deep_fri_prove(d_lde[0], N0, pc)
+        assert sg.deep_fri_verify(pc, ref_c), "classic proof rejected"
+        tc = []
+        for _ in range(3):
+            e0.record(stream)
+            out_c = ctx.deep_fri_prove(d_lde[0], N0, pc)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tc.append(e0.elapsed_time(e1))
+            assert out_c == ref_c
+        ts = []
+        for _ in range(3):
+            e0.record(stream)
+            ctx.deep_fri_prove(d_lde[0], N0, params)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        classic = {"workload": f"deep_fri_prove of LDE column 0 (n0 = 2^{N0.bit_length() - 1}), schedule [2]*"
+                               f"{N0.bit_length() - 1}, r = 54, coefficient-committed final layer",
+                   "classic_ms": statistics.median(tc), "stir_ms": statistics.median(ts),
+                   "classic_proof_bytes": len(ref_c)}
+
     cpu_threads = (os.cpu_count() or 1) if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else 0
     large = sha256_large(sg, ctx, args.sha256_large_blocks, 3, cpu_threads) if args.sha256_large_blocks > 0 else None
     serve = None
@@ -508,6 +537,7 @@ def main():
             "sha256_proofs": cfg1,
             "sha256_large_trace": large,
             "serving": serve,
+            "classic_fri": classic,
             "proof_bytes": len(ref[1]),
             "root": ref[0].hex(),
         }
