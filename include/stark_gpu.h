@@ -235,6 +235,40 @@ int sg_stir_verify(const uint8_t* proof, size_t len, const sg_fri_params* params
 int sg_prove_hash_rollup(sg_ctx* ctx, const uint64_t* leaves, size_t n_leaves, const uint8_t pi[32], int phi_mode,
                          uint8_t* proof, size_t cap, size_t* len);
 
+/* ---------------------------------------------------------------- DNS shards
+ * The steps either side of the prover in swarm-dns. Records are passed in
+ * canonical form (DnsRecord::canonical_bytes, swarm-dns/src/dns.rs:43-54):
+ * record i is canon[offsets[i] .. offsets[i+1]), offsets has n+1 entries. */
+
+/* DnsRecord::leaf_hash (dns.rs:56-79): SHA3("DNS-LEAF-DOUBLE-V1" || salt ||
+ * SHA3("DNS-LEAF-V1" || salt || canonical)); out: n x 32 bytes. Host. */
+int sg_dns_record_leaves(const uint8_t* canon, const size_t* offsets, size_t n, const uint8_t salt[16],
+                         uint8_t* out);
+/* merkle_build + merkle_root (dns.rs:85-102): binary SHA3 tree, parent =
+ * SHA3("DNS-NODE-V1" || left || right), an odd last node paired with itself. Host. */
+int sg_dns_merkle_root(const uint8_t* leaves, size_t n, uint8_t root[32]);
+/* merkle_path (dns.rs:104-114): one 32-byte sibling per level; *depth receives
+ * the level count (SG_ESPACE when cap < 32 * depth). Host. */
+int sg_dns_merkle_path(const uint8_t* leaves, size_t n, size_t index, uint8_t* path, size_t cap, size_t* depth);
+/* merkle_verify (dns.rs:116-131): 1 if the path leads from leaf to root. Host. */
+int sg_dns_merkle_verify(const uint8_t leaf[32], size_t index, const uint8_t* path, size_t depth,
+                         const uint8_t root[32]);
+/* pi_hash of an inner shard (swarm-dns/src/prover.rs:207-214):
+ * SHA3("DNS-SHARD-PIHASH-V1" || salt || le64(count) || merkle_root || root_f0 || fs_binding). Host. */
+void sg_shard_pi_hash(const uint8_t salt[16], uint64_t record_count, const uint8_t merkle_root[32],
+                      const uint8_t root_f0[32], const uint8_t fs_binding[32], uint8_t out[32]);
+/* prove_inner_shard (swarm-dns/src/prover.rs:148-225): record leaves -> DNS Merkle
+ * root -> leaves packed as 4 x le64 (pack_hash_to_leaves) -> HashRollup proof
+ * (stir = 1: STIR, 0: classic DEEP-FRI; fs_binding as public_inputs_hash),
+ * self-verified -> pi_hash. Outputs the proof bytes, pi_hash and merkle_root. */
+int sg_prove_inner_shard(sg_ctx* ctx, const uint8_t* canon, const size_t* offsets, size_t n_records,
+                         const uint8_t salt[16], const uint8_t fs_binding[32], int stir, uint8_t* proof, size_t cap,
+                         size_t* len, uint8_t pi_hash[32], uint8_t merkle_root[32]);
+/* prove_outer_rollup (swarm-dns/src/prover.rs:250-304): the inner pi_hashes
+ * (n x 32 bytes) packed as rollup leaves, HashRollup proof under pk_hash. */
+int sg_prove_outer_rollup(sg_ctx* ctx, const uint8_t* pi_hashes, size_t n, const uint8_t pk_hash[32], int stir,
+                          uint8_t* proof, size_t cap, size_t* len);
+
 /* ---------------------------------------------------------------- batched / served proving
  * No single reference function: the reference scales by running one proof per
  * worker process (swarm-worker/src/main.rs:341-355, driven by swarm-ctrl). Here

@@ -10,6 +10,8 @@ C ABI is declared in include/stark_gpu.h:
   deep_fri_verify        deep_ali/src/fri.rs:2136-2707 (STIR and classic branches)
   MerkleTreeChannel      merkle/src/lib.rs:356-512
   make_schedule / build_params / prove_hash_rollup   swarm-dns/src/prover.rs:53-304
+  prove_inner_shard / prove_outer_rollup             swarm-dns/src/prover.rs:148-304
+  DnsRecord::leaf_hash, merkle_build/path/verify     swarm-dns/src/dns.rs:43-131
   deep_ali_merge_sha256 / prove_sha256 (prove_ds_ksk_binding core)
                          deep_ali/src/lib.rs:453-545, swarm-dns/src/prover.rs:512-585
   deep_ali_merge_sha512  deep_ali/src/lib.rs:561-641 (and a SHA-512 proof with the same parameters)
@@ -104,6 +106,8 @@ EXPORTS = (
     "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
     "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_sha256_trace_gpu", "sg_prove_sha256",
     "sg_merge_sha512", "sg_sha512_trace", "sg_sha512_trace_gpu", "sg_prove_sha512",
+    "sg_dns_record_leaves", "sg_dns_merkle_root", "sg_dns_merkle_path", "sg_dns_merkle_verify", "sg_shard_pi_hash",
+    "sg_prove_inner_shard", "sg_prove_outer_rollup",
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
@@ -179,6 +183,17 @@ def lib():
     L.sg_sha256_trace_gpu.argtypes = [vp] + L.sg_sha256_trace.argtypes
     L.sg_prove_sha256.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz,
                                   ctypes.POINTER(sz), ctypes.c_char_p]
+    L.sg_dns_record_leaves.argtypes = [ctypes.c_char_p, ctypes.POINTER(sz), sz, ctypes.c_char_p, ctypes.c_char_p]
+    L.sg_dns_merkle_root.argtypes = [ctypes.c_char_p, sz, ctypes.c_char_p]
+    L.sg_dns_merkle_path.argtypes = [ctypes.c_char_p, sz, sz, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
+    L.sg_dns_merkle_verify.argtypes = [ctypes.c_char_p, sz, ctypes.c_char_p, sz, ctypes.c_char_p]
+    L.sg_shard_pi_hash.argtypes = [ctypes.c_char_p, u64, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                   ctypes.c_char_p]
+    L.sg_shard_pi_hash.restype = None
+    L.sg_prove_inner_shard.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(sz), sz, ctypes.c_char_p, ctypes.c_char_p,
+                                       i32, ctypes.c_char_p, sz, ctypes.POINTER(sz), ctypes.c_char_p, ctypes.c_char_p]
+    L.sg_prove_outer_rollup.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz,
+                                        ctypes.POINTER(sz)]
     L.sg_merge_sha512.argtypes = L.sg_merge_sha256.argtypes
     L.sg_sha512_trace.argtypes = L.sg_sha256_trace.argtypes
     L.sg_sha512_trace_gpu.argtypes = L.sg_sha256_trace_gpu.argtypes
@@ -283,6 +298,62 @@ def build_sha256_trace_multi(message: bytes):
 def build_sha512_trace_multi(message: bytes):
     """sha512_air.rs:551-578 on the host -> ((1510, height) uint64 trace, n_blocks, 64-byte digest)."""
     return _build_trace_multi("sha512", message)
+
+
+def _records(records):
+    """canonical record byte strings -> (concatenated bytes, offsets[n+1])"""
+    recs = [bytes(r) for r in records]
+    offs = (ctypes.c_size_t * (len(recs) + 1))()
+    o = 0
+    for i, r in enumerate(recs):
+        offs[i] = o
+        o += len(r)
+    offs[len(recs)] = o
+    return b"".join(recs), offs
+
+
+def dns_record_leaves(records, salt: bytes):
+    """DnsRecord::leaf_hash (swarm-dns/src/dns.rs:56-79) of canonical records -> list of 32-byte hashes."""
+    if len(salt) != 16:
+        raise ValueError("salt must be 16 bytes")
+    canon, offs = _records(records)
+    out = ctypes.create_string_buffer(32 * max(1, len(records)))
+    rc = lib().sg_dns_record_leaves(canon, offs, len(records), salt, out)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_dns_record_leaves failed")
+    return [out.raw[32 * i: 32 * i + 32] for i in range(len(records))]
+
+
+def dns_merkle_root(leaves) -> bytes:
+    """merkle_build + merkle_root (swarm-dns/src/dns.rs:85-102)."""
+    root = ctypes.create_string_buffer(32)
+    rc = lib().sg_dns_merkle_root(b"".join(leaves), len(leaves), root)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_dns_merkle_root failed")
+    return root.raw
+
+
+def dns_merkle_path(leaves, index: int):
+    """merkle_path (swarm-dns/src/dns.rs:104-114) -> list of 32-byte siblings."""
+    cap = 32 * 64
+    path = ctypes.create_string_buffer(cap)
+    depth = ctypes.c_size_t()
+    rc = lib().sg_dns_merkle_path(b"".join(leaves), len(leaves), index, path, cap, ctypes.byref(depth))
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_dns_merkle_path failed")
+    return [path.raw[32 * i: 32 * i + 32] for i in range(depth.value)]
+
+
+def dns_merkle_verify(leaf: bytes, index: int, path, root: bytes) -> bool:
+    """merkle_verify (swarm-dns/src/dns.rs:116-131)."""
+    return lib().sg_dns_merkle_verify(leaf, index, b"".join(path), len(path), root) == 1
+
+
+def shard_pi_hash(salt: bytes, record_count: int, merkle_root: bytes, root_f0: bytes, fs_binding: bytes) -> bytes:
+    """Inner-shard pi_hash (swarm-dns/src/prover.rs:207-214)."""
+    out = ctypes.create_string_buffer(32)
+    lib().sg_shard_pi_hash(salt, record_count, merkle_root, root_f0, fs_binding, out)
+    return out.raw
 
 
 def deep_fri_verify(params: FriParams, proof: bytes) -> bool:
@@ -478,6 +549,41 @@ class Context:
     def prove_sha512(self, message: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
         """SHA-512 AIR proof (LDE x32, lambda_j = j+1, STIR) -> (proof bytes, 64-byte digest); self-verified."""
         return self._prove_hash("sha512", message, fs_binding, phi_mode)
+
+    def prove_inner_shard(self, records, salt: bytes, fs_binding: bytes, stir: bool = True):
+        """prove_inner_shard (swarm-dns/src/prover.rs:148-225) on canonical records ->
+        (proof bytes, pi_hash, DNS merkle root); self-verified."""
+        if len(salt) != 16 or len(fs_binding) != 32:
+            raise ValueError("salt must be 16 bytes and fs_binding 32 bytes")
+        canon, offs = _records(records)
+        cap = 1 << 24
+        while True:
+            buf = ctypes.create_string_buffer(cap)
+            ln = ctypes.c_size_t()
+            pi, root = ctypes.create_string_buffer(32), ctypes.create_string_buffer(32)
+            rc = self._lib.sg_prove_inner_shard(self._h, canon, offs, len(records), salt, fs_binding, int(stir), buf,
+                                                cap, ctypes.byref(ln), pi, root)
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return buf.raw[:ln.value], pi.raw, root.raw
+
+    def prove_outer_rollup(self, pi_hashes, pk_hash: bytes, stir: bool = True) -> bytes:
+        """prove_outer_rollup (swarm-dns/src/prover.rs:250-304) -> proof bytes; self-verified."""
+        if len(pk_hash) != 32 or not pi_hashes:
+            raise ValueError("need pi hashes and a 32-byte pk_hash")
+        cap = 1 << 24
+        while True:
+            buf = ctypes.create_string_buffer(cap)
+            ln = ctypes.c_size_t()
+            rc = self._lib.sg_prove_outer_rollup(self._h, b"".join(pi_hashes), len(pi_hashes), pk_hash, int(stir),
+                                                 buf, cap, ctypes.byref(ln))
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return buf.raw[:ln.value]
 
     def prove_batch(self, jobs, n_streams: int = 8, hbm_budget_bytes: int = 0, cap_per_job: int = 1 << 20):
         """jobs: list of (kind, data, pi[, phi_mode]) -> list of (proof bytes, JobResult)."""

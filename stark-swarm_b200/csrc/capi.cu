@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "context.hpp"
+#include "dns.hpp"
 #include "merkle.cuh"
 #include "prover.hpp"
 #include "sha256_air.cuh"
@@ -322,6 +323,92 @@ int sg_prove_sha512(sg_ctx* c, const uint8_t* msg, size_t len, const uint8_t fs_
         sg::prove_hash_message(c, sg::sha512_hash_air(), msg, len, fs_binding, phi_mode, true, digest);
     *len_out = b.size();
     if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_sha512: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+int sg_dns_record_leaves(const uint8_t* canon, const size_t* offsets, size_t n, const uint8_t salt[16],
+                         uint8_t* out) {
+  if (!offsets || !salt || (n && (!canon || !out))) return SG_EINVAL;
+  for (size_t i = 0; i < n; ++i)
+    if (offsets[i + 1] < offsets[i]) return SG_EINVAL;
+  sg::dns_record_leaves(canon, offsets, n, salt, out);
+  return SG_OK;
+}
+
+int sg_dns_merkle_root(const uint8_t* leaves, size_t n, uint8_t root[32]) {
+  if (!leaves || !root || n == 0) return SG_EINVAL;
+  try {
+    const auto lv = sg::dns_merkle_levels(leaves, n);
+    memcpy(root, lv.back().data(), 32);
+    return SG_OK;
+  } catch (const std::bad_alloc&) {
+    return SG_ENOMEM;
+  }
+}
+
+int sg_dns_merkle_path(const uint8_t* leaves, size_t n, size_t index, uint8_t* path, size_t cap, size_t* depth) {
+  if (!leaves || !depth || n == 0 || index >= n) return SG_EINVAL;
+  try {
+    const auto p = sg::dns_merkle_path(sg::dns_merkle_levels(leaves, n), index);
+    *depth = p.size() / 32;
+    if (!path || cap < p.size()) return SG_ESPACE;
+    memcpy(path, p.data(), p.size());
+    return SG_OK;
+  } catch (const std::bad_alloc&) {
+    return SG_ENOMEM;
+  }
+}
+
+int sg_dns_merkle_verify(const uint8_t leaf[32], size_t index, const uint8_t* path, size_t depth,
+                         const uint8_t root[32]) {
+  if (!leaf || !root || (depth && !path)) return 0;
+  return sg::dns_merkle_verify(leaf, index, path, depth, root) ? 1 : 0;
+}
+
+void sg_shard_pi_hash(const uint8_t salt[16], uint64_t record_count, const uint8_t merkle_root[32],
+                      const uint8_t root_f0[32], const uint8_t fs_binding[32], uint8_t out[32]) {
+  sg::shard_pi_hash(salt, record_count, merkle_root, root_f0, fs_binding, out);
+}
+
+int sg_prove_inner_shard(sg_ctx* c, const uint8_t* canon, const size_t* offsets, size_t n_records,
+                         const uint8_t salt[16], const uint8_t fs_binding[32], int stir, uint8_t* proof, size_t cap,
+                         size_t* len, uint8_t pi_hash[32], uint8_t merkle_root[32]) {
+  return guarded(c, [&] {
+    sg::require(offsets && salt && fs_binding && len && pi_hash && merkle_root && n_records > 0 &&
+                    (canon || offsets[n_records] == 0),
+                "prove_inner_shard: null argument or no records");
+    for (size_t i = 0; i < n_records; ++i)
+      sg::require(offsets[i + 1] >= offsets[i], "prove_inner_shard: offsets must not decrease");
+    // 1-2. record leaves and the off-chain Merkle root committed in pi_hash
+    std::vector<uint8_t> lh(32 * n_records);
+    sg::dns_record_leaves(canon, offsets, n_records, salt, lh.data());
+    const auto lv = sg::dns_merkle_levels(lh.data(), n_records);
+    memcpy(merkle_root, lv.back().data(), 32);
+    // 3. every leaf hash as 4 little-endian u64 rollup leaves (pack_hash_to_leaves)
+    std::vector<uint64_t> leaves(4 * n_records);
+    memcpy(leaves.data(), lh.data(), lh.size());
+    std::vector<uint8_t> b =
+        sg::prove_hash_rollup_host_leaves(c, leaves.data(), leaves.size(), fs_binding, SG_PHI_PARALLEL_GATE, true,
+                                          stir != 0);
+    // 4. pi_hash binds salt, count, merkle root, the proof's root_f0 and the FS binding
+    sg::shard_pi_hash(salt, n_records, merkle_root, b.data(), fs_binding, pi_hash);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_inner_shard: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+int sg_prove_outer_rollup(sg_ctx* c, const uint8_t* pi_hashes, size_t n, const uint8_t pk_hash[32], int stir,
+                          uint8_t* proof, size_t cap, size_t* len) {
+  return guarded(c, [&] {
+    sg::require(pi_hashes && pk_hash && len && n > 0, "prove_outer_rollup: null argument or no shards");
+    std::vector<uint64_t> leaves(4 * n);
+    memcpy(leaves.data(), pi_hashes, 32 * n);
+    std::vector<uint8_t> b = sg::prove_hash_rollup_host_leaves(c, leaves.data(), leaves.size(), pk_hash,
+                                                               SG_PHI_PARALLEL_GATE, true, stir != 0);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_outer_rollup: proof buffer too small"};
     memcpy(proof, b.data(), b.size());
   });
 }

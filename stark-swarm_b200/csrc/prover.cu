@@ -571,7 +571,7 @@ std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t
 
 // ------------------------------------------------------------------ HashRollup pipeline
 std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* leaves, uint64_t n_leaves,
-                                                   const uint8_t pi[32], int phi_mode, bool self_verify) {
+                                                   const uint8_t pi[32], int phi_mode, bool self_verify, bool stir) {
   uint64_t n_trace = 8;
   while (n_trace < n_leaves) n_trace <<= 1;
   const uint64_t blowup = 32, n0 = n_trace * blowup;
@@ -595,7 +595,7 @@ std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* le
   const uint64_t lam[3] = {1, 2, 3};  // comb_coeffs (prover.rs:100-102)
   merge_device(c, SG_AIR_HASH_ROLLUP, d_lde.p, 4, n_trace, blowup, lam, 3, phi_mode, d_c.p);
   sg_fri_params p;
-  sg_build_params(n0, pi, 1, &p);
+  sg_build_params(n0, pi, stir ? 1 : 0, &p);
   std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
   if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
     throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};

@@ -25,7 +25,10 @@ std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uin
 std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
                                           int phi_mode, bool self_verify, uint8_t digest[32]);
 std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p);
+// prove_inner_shard / prove_outer_rollup core: HashRollup trace -> LDE x32 -> merge ->
+// STIR (stir) or classic DEEP-FRI, with build_params(n0, pi).
 std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* leaves, uint64_t n_leaves,
-                                                   const uint8_t pi[32], int phi_mode, bool self_verify);
+                                                   const uint8_t pi[32], int phi_mode, bool self_verify,
+                                                   bool stir = true);
 
 }  // namespace sg

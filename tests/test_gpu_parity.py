@@ -312,3 +312,37 @@ def test_classic_fri_matches_oracle(sgpu, ctx, log_n0, sched, cc, low):
     assert got == O.stir_prove(f0, po)
     if low:
         assert sgpu.deep_fri_verify(ps, got) and O.stir_verify(got, po)
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2])
+def test_prove_inner_shard_reproduces_golden_bundle(sgpu, ctx, golden, idx):
+    # prove_inner_shard from the zone's records: the proof file, pi_hash and DNS
+    # merkle root of each golden shard, end to end
+    sh = golden["shards"][idx]
+    salt = bytes.fromhex(golden["zone_salt_hex"])
+    recs = dnszone.split_evenly(dnszone.synthetic_zone(golden["record_count"]), golden["shard_count"])
+    canon = [dnszone.canonical_bytes(*r) for r in recs[sh["shard_id"] - 1]]
+    _, fsb, _, _ = dnszone.inner_shard_inputs(golden, sh)
+    proof, pi, root = ctx.prove_inner_shard(canon, salt, fsb)
+    assert len(proof) == sh["len"] and hashlib.sha3_256(proof).hexdigest() == sh["sha3_256"]
+    assert pi.hex() == sh["pi_hash_hex"] and root.hex() == sh["merkle_root_hex"]
+
+
+def test_prove_outer_rollup_reproduces_golden_bundle(sgpu, ctx, golden):
+    pis = [bytes.fromhex(h) for h in golden["inner_pi_hashes_hex"]]
+    proof = ctx.prove_outer_rollup(pis, bytes.fromhex(golden["authority_pk_hash_hex"]))
+    assert hashlib.sha3_256(proof).hexdigest() == golden["outer"]["sha3_256"]
+
+
+def test_prove_inner_shard_classic_fri(sgpu, ctx, golden):
+    # the same shard with the classic DEEP-FRI low-degree test (LdtMode::Fri)
+    sh = golden["shards"][0]
+    salt = bytes.fromhex(golden["zone_salt_hex"])
+    recs = dnszone.split_evenly(dnszone.synthetic_zone(golden["record_count"]), golden["shard_count"])
+    canon = [dnszone.canonical_bytes(*r) for r in recs[0]]
+    _, fsb, _, _ = dnszone.inner_shard_inputs(golden, sh)
+    proof, pi, root = ctx.prove_inner_shard(canon, salt, fsb, stir=False)
+    assert root.hex() == sh["merkle_root_hex"]
+    params = sgpu.build_params(sh["n0"], fsb, stir=False)
+    assert sgpu.deep_fri_verify(params, proof) and O.stir_verify(proof, O.build_params(sh["n0"], fsb, stir=False))
+    assert pi == dnszone.shard_pi_hash(salt, len(canon), root, proof[:32], fsb)

@@ -2,6 +2,7 @@
 and its host-only parts (parameter builder, STIR verifier) agree with the
 oracle. No kernel is launched here."""
 import ctypes
+import hashlib
 import os
 import random
 import re
@@ -139,3 +140,33 @@ def test_product_verifier_accepts_oracle_classic_fri(log_n0):
     bad = bytearray(proof)
     bad[100] ^= 1
     assert not sg.deep_fri_verify(ps, bytes(bad))
+
+
+def test_dns_shard_helpers_match_golden_bundle(golden):
+    # record leaf hashes, the DNS Merkle root and the shard pi_hash of every golden
+    # shard (merkle_root_hex, pi_hash_hex come from the reference's zone bundle)
+    sg = load_sgpu()
+    salt = bytes.fromhex(golden["zone_salt_hex"])
+    shards = dnszone.split_evenly(dnszone.synthetic_zone(golden["record_count"]), golden["shard_count"])
+    for sh in golden["shards"]:
+        recs = [dnszone.canonical_bytes(*r) for r in shards[sh["shard_id"] - 1]]
+        leaves = sg.dns_record_leaves(recs, salt)
+        assert leaves[:5] == [dnszone.record_leaf_hash(r, salt) for r in shards[sh["shard_id"] - 1][:5]]
+        root = sg.dns_merkle_root(leaves)
+        assert root.hex() == sh["merkle_root_hex"]
+        _, fsb, _, count = dnszone.inner_shard_inputs(golden, sh)
+        pi = sg.shard_pi_hash(salt, count, root, bytes.fromhex(sh["root_f0_hex"]), fsb)
+        assert pi.hex() == sh["pi_hash_hex"]
+        for idx in (0, 1, len(leaves) // 2, len(leaves) - 1):
+            path = sg.dns_merkle_path(leaves, idx)
+            assert sg.dns_merkle_verify(leaves[idx], idx, path, root)
+            assert not sg.dns_merkle_verify(leaves[idx], idx ^ 1, path, root)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 8, 33])
+def test_dns_merkle_root_small_trees(n):
+    sg = load_sgpu()
+    leaves = [hashlib.sha3_256(bytes([i])).digest() for i in range(n)]
+    assert sg.dns_merkle_root(leaves) == dnszone.dns_merkle_root(leaves)
+    for idx in range(n):
+        assert sg.dns_merkle_verify(leaves[idx], idx, sg.dns_merkle_path(leaves, idx), dnszone.dns_merkle_root(leaves))
