@@ -101,11 +101,17 @@ int sg_ctx_create(int device, sg_ctx** out) {
     delete c;
     return SG_ECUDA;
   }
-  // keep freed pool memory cached: repeated proofs reuse it without cudaMalloc
+  // Keep freed pool memory cached, so repeated proofs reuse it without cudaMalloc.
+  // Never let the pool satisfy an allocation on one stream with a block freed on
+  // another by making the first stream wait for the second: contexts proving
+  // concurrently (a Merkle commitment beside a STIR proof, server workers) would
+  // be serialised behind each other. The pool grows instead.
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
     uint64_t thr = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    int no = 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
   }
   *out = c;
   return SG_OK;
@@ -117,6 +123,11 @@ void sg_ctx_destroy(sg_ctx* c) {
   cudaStreamSynchronize(c->stream);
   if (c->owns_tables) sg::ntt_tables_free(&c->tw);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+  }
+  if (c->shift_tab) cudaFree(c->shift_tab);
   delete c;
 }
 
@@ -179,9 +190,12 @@ int sg_lde(sg_ctx* c, const uint64_t* trace, size_t w, size_t n_trace, size_t bl
   return guarded(c, [&] {
     sg::require(trace && out, "lde: null buffer");
     sg::require(w > 0 && n_trace > 0 && blowup > 0, "lde: empty input");
-    In di(trace, w * n_trace, c->stream);
     Out dout(out, w * n_trace * blowup, c->stream);
-    sg::lde_device(c, di.d, w, n_trace, blowup, shift, dout.d);
+    if (sg::is_device_ptr(trace)) {
+      sg::lde_device(c, trace, w, n_trace, blowup, shift, dout.d);
+    } else {
+      sg::lde_from_host(c, trace, w, n_trace, blowup, shift, dout.d);  // copy overlapped with the transform
+    }
     dout.finish();
   });
 }

@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "counters.hpp"
 #include "ntt.cuh"
@@ -14,6 +15,11 @@ struct sg_ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // created on first use: host-to-device copies overlapped with compute
+  // powers of the last LDE coset shift (two 2^14-entry tables), kept on the device
+  uint64_t shift_key = 0;
+  uint64_t* shift_tab = nullptr;
+  std::vector<uint64_t> shift_host;
   sg::NttTables tw;
   bool owns_tables = true;  // worker contexts of a server borrow the parent's tables
   int wide_merge = SG_WIDE_MERGE_AUTO;  // SG_OPT_WIDE_MERGE

@@ -44,34 +44,105 @@ static void ntt(sg_ctx* c, const uint64_t* in, uint64_t* out, uint32_t cols, uin
 }
 
 // ------------------------------------------------------------------ LDE
-void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
-                uint64_t* d_out) {
+namespace {
+
+void lde_check(uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift) {
   require(w > 0 && w < (1u << 31), "lde: bad column count");
   require(pow2(n_trace), "lde: trace_len must be a power of 2");
   require(pow2(blowup) && blowup >= 2, "lde: blowup must be a power of 2 >= 2");
-  const uint64_t n0 = n_trace * blowup;
-  require(log2_exact(n0) <= kMaxLogN, "lde: domain larger than 2^28");
-  shift %= gl::P;
-  require(shift != 0, "lde: shift must be nonzero");
-  cudaStream_t s = c->stream;
-  DBuf coef(w * n_trace, s);
-  DBuf scratch(std::max(ntt_scratch_elems(w, log2_exact(n0)), ntt_scratch_elems(w, log2_exact(n_trace))), s);
-  ntt(c, d_trace, coef.p, (uint32_t)w, n_trace, n_trace, log2_exact(n_trace), true, n_trace, scratch.p);
-  // coset shift: coefficient k times shift^k, applied as the forward transform loads it
-  PowSpec pre;
-  DBuf tab;
-  std::vector<uint64_t> h_tab;
-  if (shift != 1) {
-    h_tab.resize(2 * kTwEntries);
-    pow_tables_host(shift, 1, h_tab.data());
-    tab.alloc(h_tab.size(), s);
-    cuda_check(cudaMemcpyAsync(tab.p, h_tab.data(), h_tab.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
-    pre.lo = tab.p;
-    pre.hi = tab.p + kTwEntries;
+  require(log2_exact(n_trace * blowup) <= kMaxLogN, "lde: domain larger than 2^28");
+  require(shift % gl::P != 0, "lde: shift must be nonzero");
+}
+
+// Powers of the coset shift for the forward transform's first pass (none for
+// shift 1). The tables stay on the device in the context, so an LDE with the same
+// shift as the previous one uploads nothing; a new shift is copied in stream
+// order, after every earlier use of the old tables on this context.
+struct ShiftTables {
+  PowSpec spec;
+  bool active = false;
+  ShiftTables(sg_ctx* c, uint64_t shift, cudaStream_t s) {
+    shift %= gl::P;
+    if (shift == 1) return;
+    if (!c->shift_tab) cuda_check(cudaMalloc(&c->shift_tab, 2 * kTwEntries * 8), "shift tables");
+    if (c->shift_key != shift) {
+      cuda_check(cudaStreamSynchronize(s), "sync");  // the host copy below is reused across calls
+      c->shift_host.resize(2 * kTwEntries);
+      pow_tables_host(shift, 1, c->shift_host.data());
+      cuda_check(cudaMemcpyAsync(c->shift_tab, c->shift_host.data(), 2 * kTwEntries * 8, cudaMemcpyHostToDevice, s),
+                 "h2d");
+      c->shift_key = shift;
+    }
+    spec.lo = c->shift_tab;
+    spec.hi = c->shift_tab + kTwEntries;
+    active = true;
   }
-  ntt(c, coef.p, d_out, (uint32_t)w, n_trace, n0, log2_exact(n0), false, n_trace, scratch.p,
-      shift != 1 ? &pre : nullptr);
-  if (shift != 1) cuda_check(cudaStreamSynchronize(s), "sync");  // h_tab must outlive its copy
+};
+
+// iNTT of w columns into coef, then the zero-padded forward transform into d_out,
+// coefficient k times shift^k (applied as the forward transform loads it).
+void lde_core(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup,
+              const ShiftTables& sh, uint64_t* coef, uint64_t* scratch, uint64_t* d_out) {
+  const uint64_t n0 = n_trace * blowup;
+  ntt(c, d_trace, coef, (uint32_t)w, n_trace, n_trace, log2_exact(n_trace), true, n_trace, scratch);
+  ntt(c, coef, d_out, (uint32_t)w, n_trace, n0, log2_exact(n0), false, n_trace, scratch,
+      sh.active ? &sh.spec : nullptr);
+}
+
+uint64_t lde_scratch_elems(uint64_t w, uint64_t n_trace, uint64_t blowup) {
+  return std::max(ntt_scratch_elems(w, log2_exact(n_trace * blowup)), ntt_scratch_elems(w, log2_exact(n_trace)));
+}
+
+}  // namespace
+
+void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
+                uint64_t* d_out) {
+  lde_check(w, n_trace, blowup, shift);
+  cudaStream_t s = c->stream;
+  ShiftTables sh(c, shift, s);
+  DBuf coef(w * n_trace, s), scratch(lde_scratch_elems(w, n_trace, blowup), s);
+  lde_core(c, d_trace, w, n_trace, blowup, sh, coef.p, scratch.p, d_out);
+}
+
+// The same LDE from a host trace: column chunks of ~64 MB are copied on the
+// context's copy stream while earlier chunks are transformed on its compute
+// stream, so only the first chunk's copy is exposed (with pinned host memory;
+// a pageable buffer is staged by the driver and overlaps less).
+void lde_from_host(sg_ctx* c, const uint64_t* h_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
+                   uint64_t* d_out) {
+  lde_check(w, n_trace, blowup, shift);
+  cudaStream_t s = c->stream;
+  const uint64_t chunk = std::min<uint64_t>(w, std::max<uint64_t>(1, (uint64_t(8) << 20) / n_trace));
+  const uint64_t n_chunks = (w + chunk - 1) / chunk;
+  ShiftTables sh(c, shift, s);  // before the chunk copies take the copy engine
+  DBuf d_in(w * n_trace, s);
+  if (n_chunks == 1) {
+    cuda_check(cudaMemcpyAsync(d_in.p, h_trace, w * n_trace * 8, cudaMemcpyHostToDevice, s), "h2d");
+    lde_device(c, d_in.p, w, n_trace, blowup, shift, d_out);
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    return;
+  }
+  if (!c->copy_stream) cuda_check(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
+  std::vector<cudaEvent_t> ev(n_chunks + 1, nullptr);
+  for (auto& e : ev) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+  // the copy stream may only write d_in once its stream-ordered allocation exists
+  cuda_check(cudaEventRecord(ev[n_chunks], s), "event");
+  cuda_check(cudaStreamWaitEvent(c->copy_stream, ev[n_chunks], 0), "wait");
+  for (uint64_t k = 0; k < n_chunks; ++k) {
+    const uint64_t c0 = k * chunk, wk = std::min(chunk, w - c0);
+    cuda_check(cudaMemcpyAsync(d_in.p + c0 * n_trace, h_trace + c0 * n_trace, wk * n_trace * 8,
+                               cudaMemcpyHostToDevice, c->copy_stream),
+               "h2d");
+    cuda_check(cudaEventRecord(ev[k], c->copy_stream), "event");
+  }
+  DBuf coef(chunk * n_trace, s), scratch(lde_scratch_elems(chunk, n_trace, blowup), s);
+  for (uint64_t k = 0; k < n_chunks; ++k) {
+    const uint64_t c0 = k * chunk, wk = std::min(chunk, w - c0);
+    cuda_check(cudaStreamWaitEvent(s, ev[k], 0), "wait");
+    lde_core(c, d_in.p + c0 * n_trace, wk, n_trace, blowup, sh, coef.p, scratch.p, d_out + c0 * n_trace * blowup);
+  }
+  cuda_check(cudaStreamSynchronize(s), "sync");  // d_in's copies and the transforms are done
+  for (auto& e : ev) cudaEventDestroy(e);
 }
 
 // ------------------------------------------------------------------ merge

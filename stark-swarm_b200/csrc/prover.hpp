@@ -11,6 +11,9 @@ namespace sg {
 
 void lde_device(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
                 uint64_t* d_out);
+// lde_device from a host trace, its copy pipelined with the transform by column chunks.
+void lde_from_host(sg_ctx* c, const uint64_t* h_trace, uint64_t w, uint64_t n_trace, uint64_t blowup, uint64_t shift,
+                   uint64_t* d_out);
 // lambdas are host values; n_blocks gates the SHA-256 AIR (the AIR registry uses 1)
 void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_t n_trace, uint64_t blowup,
                   const uint64_t* lambdas, uint64_t k, int phi_mode, uint64_t* d_c, uint64_t n_blocks = 1);

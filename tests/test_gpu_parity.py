@@ -346,3 +346,28 @@ def test_prove_inner_shard_classic_fri(sgpu, ctx, golden):
     params = sgpu.build_params(sh["n0"], fsb, stir=False)
     assert sgpu.deep_fri_verify(params, proof) and O.stir_verify(proof, O.build_params(sh["n0"], fsb, stir=False))
     assert pi == dnszone.shard_pi_hash(salt, len(canon), root, proof[:32], fsb)
+
+
+def test_lde_host_input_pipelined_matches_device_input(ctx):
+    # a host trace large enough to be copied in column chunks overlapped with the
+    # transform (16-column chunks at 2^19 rows; 20 columns leave a partial chunk)
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(19)
+    tr = rand_field(rng, (20, 1 << 19))
+    pinned = torch.from_numpy(tr.view(np.int64)).pin_memory()
+    d_out_host = torch.empty((20, 1 << 22), dtype=torch.int64, device="cuda")
+    ctx.lde(pinned, 8, 7, out=d_out_host)
+    d_out_dev = torch.empty_like(d_out_host)
+    ctx.lde(pinned.cuda(), 8, 7, out=d_out_dev)
+    torch.cuda.synchronize()
+    assert torch.equal(d_out_host, d_out_dev)
+    got = ctx.lde(tr, 8, 7)  # pageable numpy input, host output
+    assert np.array_equal(got, d_out_dev.cpu().numpy().view(np.uint64))
+    # spot values against the oracle's coset evaluation of column 19
+    col = [int(v) for v in O.ntt(tr[19], inverse=True)]
+    w = int(O.lib().orc_root_of_unity(22))
+    for i in (0, 5, (1 << 22) - 1):
+        x, acc = 7 * pow(w, i, P) % P, 0
+        for cf in reversed(col):
+            acc = (acc * x + cf) % P
+        assert int(got[19, i]) == acc
