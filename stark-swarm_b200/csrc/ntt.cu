@@ -47,6 +47,26 @@ __host__ __device__ constexpr int row_stride(int log_m) {
   return M >= 256 ? Mp + (K < 16 ? 16 / K : 1) : Mp;
 }
 
+// Twiddles staged in shared memory after the tile. Stage twiddles w_M^j (j < M)
+// pay off while the tile is small (M <= 2^10); for the 2^11 and 2^12 passes the
+// extra 16-32 KB costs more residency than the L1-cached table loads it saves.
+// The pass twiddle w^{lane i} is the product of per-lane factors w^{lane (i mod 64)}
+// and w^{64 lane (i / 64)}, built once per CTA from the global w28 tables.
+__host__ __device__ constexpr bool stage_tw_in_smem(int log_m) { return log_m >= 5 && log_m <= 10; }
+// Pass-twiddle factors for the 2^11 and 2^12 passes (K = 4 lanes); below that the
+// per-lane build costs more than the table loads it replaces. A lane's factors
+// are padded to 16/K (mod 16) words, so the K lanes a half-warp's stores cover
+// start in distinct banks.
+__host__ __device__ constexpr bool pass_tw_in_smem(int log_m) { return log_m >= 11; }
+__host__ __device__ constexpr int pass_tw_stride(int log_m) {
+  const int K = 1 << pass_log_k(log_m), n = 64 + ((1 << log_m) >> 6), want = K < 16 ? 16 / K : 0;
+  return n + (((want - n) % 16) + 16) % 16;
+}
+__host__ __device__ constexpr size_t pass_table_bytes(int log_m) {
+  const int M = 1 << log_m, K = 1 << pass_log_k(log_m);
+  return 8 * ((stage_tw_in_smem(log_m) ? M : 0) + (pass_tw_in_smem(log_m) ? K * pass_tw_stride(log_m) : 0));
+}
+
 struct PassArgs {
   const uint64_t* in;
   uint64_t* out;
@@ -75,7 +95,7 @@ struct PassArgs {
 
 // One Stockham stage of radix R over all K lanes of the tile.
 // Each thread holds V values = V/R groups; group g -> lane g / G, j = g % G.
-template <int R, int V, bool INV>
+template <int R, int V, bool INV, int TWL, bool TW_SM>
 __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int log_m, int Mp, int log_ns,
                                                const uint64_t* tw_st) {
   constexpr int GPT = V / R;
@@ -99,9 +119,12 @@ __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int l
     int l = g >> log_g, j = g & (G - 1);
     int k = j & (Ns - 1);
     if (log_ns > 0) {
-      const int sh = 12 - log_ns - LR;  // w_{Ns R}^{rk} = w_4096^{rk 4096/(Ns R)}
+      const int sh = TWL - log_ns - LR;  // w_{Ns R}^{rk} = w_{2^TWL}^{rk 2^TWL/(Ns R)}
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[q * R + r] = gl::mul(v[q * R + r], __ldg(tw_st + (((r * k) << sh) & 4095)));
+      for (int r = 1; r < R; ++r) {
+        const int ix = ((r * k) << sh) & ((1 << TWL) - 1);
+        v[q * R + r] = gl::mul(v[q * R + r], TW_SM ? tw_st[ix] : __ldg(tw_st + ix));
+      }
     }
     dft_reg<R, INV>(v + q * R);
     int idx = ((j >> log_ns) << (log_ns + LR)) + k;
@@ -168,6 +191,22 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   const uint64_t yc = y / a.y_sub, ys = y - yc * a.y_sub;
   const uint64_t* in = a.in + yc * a.in_col + ys * a.in_sub;
   uint64_t* out = a.out + yc * a.out_col + ys * a.out_sub;
+  constexpr bool STW = stage_tw_in_smem(LOG_M);
+  constexpr bool PTW = pass_tw_in_smem(LOG_M);
+  constexpr int PT_PER = pass_tw_stride(LOG_M), PT_N = 64 + (M >> 6);
+  uint64_t* stw = sm + K * Mp;
+  uint64_t* ptw = stw + (STW ? M : 0);
+  if constexpr (STW)
+    for (int j = t; j < M; j += T) stw[j] = __ldg(a.tw_st + (j << (12 - LOG_M)));
+  if constexpr (PTW) {
+    if (a.tw_log > 0)
+      for (int x = t; x < K * PT_N; x += T) {
+        const int l = x / PT_N, r = x - l * PT_N;
+        const uint64_t lane = lane0 + l;
+        const uint64_t e = r < 64 ? lane * (uint64_t)r : lane * (uint64_t)(r - 64) * 64;
+        ptw[l * PT_PER + r] = tw_pow(a.tw_lo, a.tw_hi, e, a.tw_log);
+      }
+  }
 
   const bool lane_fast_in = a.in_lane == 1;
   // a sparse first stage reads only points m < nz * M/16: skip the rest
@@ -224,15 +263,21 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       log_ns = 4;
       st0 = 1;
     }
+    constexpr int TWL = STW ? LOG_M : 12;
+    const uint64_t* tws = STW ? stw : a.tw_st;
 #pragma unroll 1
     for (int st = st0; st < N16; ++st) {
-      stockham_stage<16, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
+      stockham_stage<16, V, INV, TWL, STW>(sm, t, T, LOG_M, Mp, log_ns, tws);
       log_ns += 4;
     }
   }
-  if constexpr (REM == 1) stockham_stage<2, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
-  if constexpr (REM == 2) stockham_stage<4, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
-  if constexpr (REM == 3) stockham_stage<8, V, INV>(sm, t, T, LOG_M, Mp, log_ns, a.tw_st);
+  {
+    constexpr int TWL = STW ? LOG_M : 12;
+    const uint64_t* tws = STW ? stw : a.tw_st;
+    if constexpr (REM == 1) stockham_stage<2, V, INV, TWL, STW>(sm, t, T, LOG_M, Mp, log_ns, tws);
+    if constexpr (REM == 2) stockham_stage<4, V, INV, TWL, STW>(sm, t, T, LOG_M, Mp, log_ns, tws);
+    if constexpr (REM == 3) stockham_stage<8, V, INV, TWL, STW>(sm, t, T, LOG_M, Mp, log_ns, tws);
+  }
 
   const bool lane_fast_out = a.out_lane == 1;
   auto out_pos = [&](int e, int& l, int& i) {
@@ -253,7 +298,14 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       int l, i;
       out_pos(t + (q0 + q) * T, l, i);
       x[q] = sm[l * Mp + padi(i)];
-      if (a.tw_log > 0) x[q] = gl::mul(x[q], tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log));
+      if (a.tw_log > 0) {
+        uint64_t w;
+        if constexpr (PTW)
+          w = gl::mul(ptw[l * PT_PER + (i & 63)], ptw[l * PT_PER + 64 + (i >> 6)]);
+        else
+          w = tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log);
+        x[q] = gl::mul(x[q], w);
+      }
       if (a.scale != 1) x[q] = gl::mul(x[q], a.scale);
     }
 #pragma unroll
@@ -274,7 +326,7 @@ cudaError_t launch_pass(const PassArgs& a0, bool inv, uint64_t n_rows, cudaStrea
   constexpr int K = 1 << pass_log_k(LOG_M);
   constexpr int T = K * M / V;
   static_assert(T <= 1024, "too many threads per CTA");
-  const size_t smem = (size_t)K * row_stride(LOG_M) * sizeof(uint64_t);
+  const size_t smem = (size_t)K * row_stride(LOG_M) * sizeof(uint64_t) + pass_table_bytes(LOG_M);
   const uint64_t blocks = (a.n_lanes + K - 1) / K;
   auto kern = inv ? ntt_pass_kernel<LOG_M, true> : ntt_pass_kernel<LOG_M, false>;
   if (smem > 48 * 1024) {
