@@ -83,10 +83,8 @@ __global__ void leaf_kernel_t(const uint64_t* __restrict__ cols, uint64_t cs, ui
 }
 
 template <int A>
-__global__ void node_kernel_t(const uint64_t* __restrict__ child, uint64_t n_child, uint64_t* __restrict__ parent,
-                              uint64_t n_parent, uint64_t level, uint64_t label) {
-  uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (p >= n_parent) return;
+__device__ __forceinline__ void node_hash(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t p,
+                                          uint64_t level, uint64_t label) {
   kc::LaneSponge sp;
   sp.init();
   sp.lane(A);
@@ -108,10 +106,15 @@ __global__ void node_kernel_t(const uint64_t* __restrict__ child, uint64_t n_chi
   for (int q = 0; q < 4; ++q) o[q] = d[q];
 }
 
-__global__ void node_kernel(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t n_parent,
-                            uint32_t arity, uint64_t level, uint64_t label) {
+template <int A>
+__global__ void node_kernel_t(const uint64_t* __restrict__ child, uint64_t n_child, uint64_t* __restrict__ parent,
+                              uint64_t n_parent, uint64_t level, uint64_t label) {
   uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (p >= n_parent) return;
+  if (p < n_parent) node_hash<A>(child, n_child, parent, p, level, label);
+}
+
+__device__ void node_hash_any(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t p, uint32_t arity,
+                              uint64_t level, uint64_t label) {
   kc::LaneSponge sp;
   sp.init();
   sp.lane(arity);
@@ -134,6 +137,42 @@ __global__ void node_kernel(const uint64_t* child, uint64_t n_child, uint64_t* p
   o[1] = d[1];
   o[2] = d[2];
   o[3] = d[3];
+}
+
+__global__ void node_kernel(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t n_parent,
+                            uint32_t arity, uint64_t level, uint64_t label) {
+  uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (p < n_parent) node_hash_any(child, n_child, parent, p, arity, level, label);
+}
+
+// The levels above the first one with at most kTopParents parents, in one CTA:
+// each level is a block-wide loop over its parents, then a barrier (which makes
+// the level's global writes visible to the whole block) before the next.
+constexpr int kTopThreads = 512;
+constexpr uint64_t kTopParents = 1024;
+constexpr int kMaxTopLevels = 24;
+struct TopLevels {
+  int n;
+  uint32_t arity[kMaxTopLevels];
+  uint64_t n_child[kMaxTopLevels], child_off[kMaxTopLevels], parent_off[kMaxTopLevels], n_parent[kMaxTopLevels];
+  uint64_t level[kMaxTopLevels];
+};
+
+__global__ void __launch_bounds__(kTopThreads) tree_top_kernel(uint64_t* d, TopLevels tl, uint64_t label) {
+  for (int k = 0; k < tl.n; ++k) {
+    const uint64_t* ch = d + 4 * tl.child_off[k];
+    uint64_t* par = d + 4 * tl.parent_off[k];
+    for (uint64_t p = threadIdx.x; p < tl.n_parent[k]; p += kTopThreads) {
+      switch (tl.arity[k]) {
+        case 2: node_hash<2>(ch, tl.n_child[k], par, p, tl.level[k], label); break;
+        case 4: node_hash<4>(ch, tl.n_child[k], par, p, tl.level[k], label); break;
+        case 8: node_hash<8>(ch, tl.n_child[k], par, p, tl.level[k], label); break;
+        case 16: node_hash<16>(ch, tl.n_child[k], par, p, tl.level[k], label); break;
+        default: node_hash_any(ch, tl.n_child[k], par, p, tl.arity[k], tl.level[k], label); break;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void gather_digests_kernel(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out) {
@@ -177,6 +216,20 @@ cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w,
 cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
   for (size_t l = 0; l + 1 < t.len.size(); ++l) {
     const uint64_t np = t.len[l + 1];
+    if (np <= kTopParents && t.len.size() - 1 - l <= (size_t)kMaxTopLevels) {
+      TopLevels tl{};
+      for (size_t k = l; k + 1 < t.len.size(); ++k, ++tl.n) {
+        tl.arity[tl.n] = t.arity[k];
+        tl.n_child[tl.n] = t.len[k];
+        tl.child_off[tl.n] = t.off[k];
+        tl.parent_off[tl.n] = t.off[k + 1];
+        tl.n_parent[tl.n] = t.len[k + 1];
+        tl.level[tl.n] = k + 1;
+      }
+      SG_LAUNCH_SCOPE("merkle_nodes", s);
+      tree_top_kernel<<<1, kTopThreads, 0, s>>>(t.d, tl, t.label);
+      return cudaGetLastError();
+    }
     const uint64_t* ch = t.d + 4 * t.off[l];
     uint64_t* par = t.d + 4 * t.off[l + 1];
     const unsigned B = blocks_for(np, 128);

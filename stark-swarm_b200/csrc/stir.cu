@@ -9,7 +9,6 @@ namespace sg {
 namespace {
 
 constexpr int kOodThreads = 256;
-constexpr uint64_t kOodGroupsPerThread = 16;
 
 __device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
 #pragma unroll
@@ -17,26 +16,41 @@ __device__ __forceinline__ uint64_t warp_sum(uint64_t v) {
   return v;
 }
 
+// Groups of M coefficients per thread: enough threads to fill the GPU (2^17),
+// and at most 16 groups each. Small layers thus spread over many CTAs instead of
+// running a long serial loop on a few.
 inline uint64_t ood_blocks(uint64_t n, int m) {
-  uint64_t groups = n / m;
-  uint64_t threads = (groups + kOodGroupsPerThread - 1) / kOodGroupsPerThread;
-  uint64_t b = (threads + kOodThreads - 1) / kOodThreads;
+  const uint64_t groups = n / m;
+  uint64_t gpt = groups >> 17;
+  gpt = gpt < 1 ? 1 : gpt > 16 ? 16 : gpt;
+  const uint64_t threads = (groups + gpt - 1) / gpt;
+  const uint64_t b = (threads + kOodThreads - 1) / kOodThreads;
   return b ? b : 1;
 }
 
 // Thread tid accumulates T_r over groups t = tid, tid + S, ... (S = all threads),
 // starting from w^tid and stepping by w^S: consecutive threads read consecutive
-// groups of M coefficients.
+// groups of M coefficients. w^tid = w^{256 block} w^{tid mod 16} w^{16 (tid / 16 mod 16)},
+// the 33 factors computed once per CTA by 33 threads.
 template <int M, bool BASE>
 __global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t* c, uint64_t n, gl::Fp6 w,
                                                                    gl::Fp6 w_stride, uint64_t* partials) {
+  static_assert(kOodThreads == 256, "the power table covers 256 threads");
   const uint64_t n_groups = n / M;
   const uint64_t S = (uint64_t)gridDim.x * kOodThreads;
   const uint64_t tid = (uint64_t)blockIdx.x * kOodThreads + threadIdx.x;
-  __shared__ gl::Fp6 blk_start;
-  if (threadIdx.x == 0) blk_start = gl::e_pow(w, (uint64_t)blockIdx.x * kOodThreads);
+  __shared__ gl::Fp6 pw[33];
+  {
+    const int t = threadIdx.x;
+    if (t < 16)
+      pw[t] = gl::e_pow(w, (uint64_t)t);
+    else if (t < 32)
+      pw[t] = gl::e_pow(w, (uint64_t)16 * (t - 16));
+    else if (t == 32)
+      pw[32] = gl::e_pow(w, (uint64_t)blockIdx.x * kOodThreads);
+  }
   __syncthreads();
-  gl::Fp6 wt = gl::e_mul(blk_start, gl::e_pow(w, threadIdx.x));
+  gl::Fp6 wt = gl::e_mul(pw[32], gl::e_mul(pw[threadIdx.x & 15], pw[16 + (threadIdx.x >> 4)]));
   uint64_t acc[M][6];
 #pragma unroll
   for (int r = 0; r < M; ++r)
@@ -83,10 +97,13 @@ __global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t
 template <int M>
 __global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, gl::Fp6 z, uint64_t* evals) {
   __shared__ uint64_t T[M * 6];
-  for (int e = threadIdx.x; e < M * 6; e += blockDim.x) {
+  // one warp per element: the lanes stride over the block partials
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
+  for (int e = warp; e < M * 6; e += n_warps) {
     uint64_t v = 0;
-    for (uint64_t b = 0; b < n_blocks; ++b) v = gl::add(v, partials[b * M * 6 + e]);
-    T[e] = v;
+    for (uint64_t b = lane; b < n_blocks; b += 32) v = gl::add(v, partials[b * M * 6 + e]);
+    v = warp_sum(v);
+    if (lane == 0) T[e] = v;
   }
   __syncthreads();
   const int j = threadIdx.x;
@@ -200,7 +217,7 @@ cudaError_t ood_launch(const uint64_t* c, bool base, uint64_t n, const gl::Fp6& 
       ood_partial_kernel<M, false><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
   }
   SG_LAUNCH_SCOPE("stir_ood_finish", s);
-  ood_finish_kernel<M><<<1, 128, 0, s>>>(partials, blocks, z, evals);
+  ood_finish_kernel<M><<<1, 256, 0, s>>>(partials, blocks, z, evals);
   return cudaGetLastError();
 }
 
