@@ -235,6 +235,53 @@ int sg_stir_verify(const uint8_t* proof, size_t len, const sg_fri_params* params
 int sg_prove_hash_rollup(sg_ctx* ctx, const uint64_t* leaves, size_t n_leaves, const uint8_t pi[32], int phi_mode,
                          uint8_t* proof, size_t cap, size_t* len);
 
+/* ---------------------------------------------------------------- RSA-2048 signature checks
+ * RSASSA-PKCS1-v1_5 / SHA-256 (DNSSEC algorithm 8) proved as the e = 65537
+ * exponentiation chain AIR (deep_ali/src/rsa2048_exp_air.rs): 32 rows of 11041
+ * cells, each row one witness-quotient multiply modulo n
+ * (rsa2048_field_air.rs), 16 squarings then the multiply by s on row 16, whose
+ * output is bound to the encoded message EM; 11280 constraints per row. Several
+ * records stack side by side in one trace (rsa2048_stacked_air.rs). All integers
+ * are 256-byte big-endian (n, s = signature, em); arrays of records are
+ * contiguous, 256 bytes per record. */
+
+/* EMSA-PKCS1-v1_5 encoding of SHA-256(msg) for a 256-byte modulus
+ * (deep_ali/src/rsa2048.rs:71-90, emsa_pkcs1_v1_5_encode_sha256). */
+int sg_rsa2048_em(const uint8_t* msg, size_t len, uint8_t em[256]);
+/* Native check s^65537 mod n == em with 0 < s < n (rsa2048.rs:92-127, verify).
+ * Returns 1 valid, 0 invalid. */
+int sg_rsa2048_verify(const uint8_t n_be[256], const uint8_t s_be[256], const uint8_t em[256]);
+/* pi_hash of one record: SHA3-256("RSA2048-V2-PI-PRE" || n || s || msg || em)
+ * (swarm-dns/examples/prove_rsa2048_record_v1.rs:178-187). */
+int sg_rsa2048_pi_record(const uint8_t n_be[256], const uint8_t s_be[256], const uint8_t* msg, size_t len,
+                         const uint8_t em[256], uint8_t out[32]);
+/* pi_hash of a stacked zone under one key: SHA3-256("RSA2048-STACKED-ZONE" || n ||
+ * le64(n_records) || em_0 || ... ) (swarm-dns/examples/stacked_rsa_zone_prover.rs:158-165). */
+int sg_rsa2048_pi_stacked(const uint8_t n_be[256], size_t n_records, const uint8_t* ems, uint8_t out[32]);
+/* fill_rsa_exp_multirow / fill_rsa_stacked (rsa2048_exp_air.rs:126-204,
+ * rsa2048_stacked_air.rs:40-54) on the host: (n_records * 11041) x 32
+ * column-major into `trace` (cap in elements). SG_EINVAL unless 1 < n and s < n. */
+int sg_rsa2048_trace(const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, size_t n_records,
+                     uint64_t* trace, size_t cap);
+/* The same trace with the cells expanded on the device from per-row witnesses
+ * (limbs, quotient, biased carries; 2.5 KB a row); `trace` is host or device memory. */
+int sg_rsa2048_trace_gpu(sg_ctx* ctx, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be,
+                         size_t n_records, uint64_t* trace, size_t cap);
+/* deep_ali_merge_rsa_exp_multirow(_streaming) / deep_ali_merge_rsa_stacked_streaming
+ * (deep_ali/src/lib.rs:1694-2070): Phi_i = sum_j (j + 1) C_j over the concatenated
+ * constraints at every LDE point (always evaluated: this merge has no
+ * parallel-build gate), then iFFT, poly_div_zh, FFT -> c_eval (n_trace * blowup
+ * values). lde: (n_records * 11041) columns of n_trace * blowup, host or device. */
+int sg_merge_rsa2048(sg_ctx* ctx, const uint64_t* lde, size_t n_records, size_t n_trace, size_t blowup,
+                     uint64_t* c_eval);
+/* RSA-2048 proof: witnesses (host) -> trace (device) -> LDE x32 -> RSA merge ->
+ * STIR with build_params(1024, pi) (schedule [8,8,8,2]), self-verified. One
+ * record is prove_rsa2048_record_v1.rs; several are stacked_rsa_zone_prover.rs.
+ * The proof binds em only through the constraints: pass EM from sg_rsa2048_em
+ * and check the signature with sg_rsa2048_verify first, as the reference does. */
+int sg_prove_rsa2048(sg_ctx* ctx, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, size_t n_records,
+                     const uint8_t pi[32], uint8_t* proof, size_t cap, size_t* len);
+
 /* ---------------------------------------------------------------- DNS shards
  * The steps either side of the prover in swarm-dns. Records are passed in
  * canonical form (DnsRecord::canonical_bytes, swarm-dns/src/dns.rs:43-54):

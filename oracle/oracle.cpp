@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "air.hpp"
+#include "rsa2048_air.hpp"
 #include "chacha.hpp"
 #include "gl.hpp"
 #include "keccak.hpp"
@@ -1226,6 +1227,66 @@ int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32
   orc_merge_sha512(lde.data(), n_trace, blowup, lam.data(), n_blocks, phi_mode, c.data());
   orc_fri_params p;
   orc_build_params(n0, fs_binding, 1, &p);
+  return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
+}
+
+// ------------------------------------------------------------------ RSA-2048
+// eval_rsa_stacked_per_row (rsa2048_stacked_air.rs:56-70): n_records records of
+// rsa2048_exp_air.rs side by side; cur/nxt hold n_records * 11041 cells.
+int orc_rsa_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_trace, size_t n_records,
+                 uint64_t* out) {
+  for (size_t r = 0; r < n_records; ++r)
+    rsa::eval_record((const Fp*)cur + r * rsa::WIDTH, (const Fp*)nxt + r * rsa::WIDTH, row, n_trace,
+                     (Fp*)out + r * rsa::CONSTRAINTS);
+  return 0;
+}
+
+// deep_ali_merge_rsa_exp_multirow(_streaming) / deep_ali_merge_rsa_stacked_streaming
+// (lib.rs:1694-1823, 1827-1945, 1949-2070): Phi is always evaluated (no
+// parallel-build gate), lambda_j = j + 1 over the concatenated constraints,
+// point i reads rows i and i + blowup, then iFFT, poly_div_zh, FFT.
+int orc_merge_rsa(const uint64_t* lde, size_t n_records, size_t n_trace, size_t blowup, uint64_t* c_eval) {
+  if (n_trace == 0 || (n_trace & (n_trace - 1)) || blowup == 0 || (blowup & (blowup - 1)) || n_records == 0)
+    return -2;
+  const size_t n = n_trace * blowup, w = n_records * rsa::WIDTH, k = n_records * rsa::CONSTRAINTS;
+  const Fp* L = (const Fp*)lde;
+  std::vector<Fp> phi(n);
+#pragma omp parallel
+  {
+    std::vector<Fp> cur(w), nxt(w), cv(k);
+#pragma omp for schedule(static)
+    for (long i = 0; i < (long)n; ++i) {
+      const size_t ni = (i + blowup) % n;
+      for (size_t c = 0; c < w; ++c) {
+        cur[c] = L[c * n + i];
+        nxt[c] = L[c * n + ni];
+      }
+      orc_rsa_eval((const uint64_t*)cur.data(), (const uint64_t*)nxt.data(), i / blowup, n_trace, n_records,
+                   (uint64_t*)cv.data());
+      Fp acc;
+      for (size_t j = 0; j < k; ++j) acc = acc + Fp(j + 1) * cv[j];
+      phi[i] = acc;
+    }
+  }
+  ifft(phi.data(), n);
+  std::vector<Fp> q = poly_div_zh(phi, n_trace);
+  q.resize(n);
+  fft(q.data(), n);
+  memcpy(c_eval, q.data(), n * 8);
+  return 0;
+}
+
+// prove_rsa2048_record_v1.rs:150-205 (one record) and stacked_rsa_zone_prover.rs:
+// 120-175 (n_records): trace (n_records * 11041 x n_trace, column-major) -> LDE x32
+// (shift 1) -> RSA merge -> STIR with build_params(n0, pi) (schedule [8,8,8,2] at n0 1024).
+int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const uint8_t pi[32], uint8_t* out,
+                  size_t cap, size_t* out_len) {
+  const size_t blowup = 32, n0 = n_trace * blowup, w = n_records * rsa::WIDTH;
+  std::vector<uint64_t> lde(w * n0), c(n0);
+  if (orc_lde(trace, w, n_trace, blowup, 1, lde.data()) != 0) return -2;
+  if (orc_merge_rsa(lde.data(), n_records, n_trace, blowup, c.data()) != 0) return -2;
+  orc_fri_params p;
+  orc_build_params(n0, pi, 1, &p);
   return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
 }
 

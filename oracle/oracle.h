@@ -79,6 +79,13 @@ int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32
                      size_t cap, size_t* out_len, uint8_t digest[64]);
 int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
                      size_t cap, size_t* out_len, uint8_t digest[32]);
+/* RSA-2048 exponentiation AIR (rsa2048_exp_air.rs), n_records records side by side
+ * (rsa2048_stacked_air.rs): 11041 cells and 11280 constraints per record. */
+int orc_rsa_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_trace, size_t n_records,
+                 uint64_t* out);
+int orc_merge_rsa(const uint64_t* lde, size_t n_records, size_t n_trace, size_t blowup, uint64_t* c_eval);
+int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const uint8_t pi[32], uint8_t* out,
+                  size_t cap, size_t* out_len);
 void orc_build_params(size_t n0, const uint8_t pi[32], int stir, orc_fri_params* out);
 int orc_stir_prove(const uint64_t* f0, size_t n0, const orc_fri_params* p, uint8_t* out, size_t cap, size_t* len);
 int orc_stir_verify(const uint8_t* proof, size_t len, const orc_fri_params* p);

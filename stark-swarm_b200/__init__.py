@@ -108,6 +108,8 @@ EXPORTS = (
     "sg_merge_sha512", "sg_sha512_trace", "sg_sha512_trace_gpu", "sg_prove_sha512",
     "sg_dns_record_leaves", "sg_dns_merkle_root", "sg_dns_merkle_path", "sg_dns_merkle_verify", "sg_shard_pi_hash",
     "sg_prove_inner_shard", "sg_prove_outer_rollup",
+    "sg_rsa2048_em", "sg_rsa2048_verify", "sg_rsa2048_pi_record", "sg_rsa2048_pi_stacked", "sg_rsa2048_trace",
+    "sg_rsa2048_trace_gpu", "sg_merge_rsa2048", "sg_prove_rsa2048",
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
@@ -194,6 +196,16 @@ def lib():
                                        i32, ctypes.c_char_p, sz, ctypes.POINTER(sz), ctypes.c_char_p, ctypes.c_char_p]
     L.sg_prove_outer_rollup.argtypes = [vp, ctypes.c_char_p, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz,
                                         ctypes.POINTER(sz)]
+    L.sg_rsa2048_em.argtypes = [ctypes.c_char_p, sz, ctypes.c_char_p]
+    L.sg_rsa2048_verify.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p]
+    L.sg_rsa2048_pi_record.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_char_p,
+                                       ctypes.c_char_p]
+    L.sg_rsa2048_pi_stacked.argtypes = [ctypes.c_char_p, sz, ctypes.c_char_p, ctypes.c_char_p]
+    L.sg_rsa2048_trace.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sz, vp, sz]
+    L.sg_rsa2048_trace_gpu.argtypes = [vp] + L.sg_rsa2048_trace.argtypes
+    L.sg_merge_rsa2048.argtypes = [vp, vp, sz, sz, sz, vp]
+    L.sg_prove_rsa2048.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_char_p,
+                                   ctypes.c_char_p, sz, ctypes.POINTER(sz)]
     L.sg_merge_sha512.argtypes = L.sg_merge_sha256.argtypes
     L.sg_sha512_trace.argtypes = L.sg_sha256_trace.argtypes
     L.sg_sha512_trace_gpu.argtypes = L.sg_sha256_trace_gpu.argtypes
@@ -298,6 +310,72 @@ def build_sha256_trace_multi(message: bytes):
 def build_sha512_trace_multi(message: bytes):
     """sha512_air.rs:551-578 on the host -> ((1510, height) uint64 trace, n_blocks, 64-byte digest)."""
     return _build_trace_multi("sha512", message)
+
+
+RSA_WIDTH, RSA_CONSTRAINTS, RSA_N_TRACE, RSA_BLOWUP = 11041, 11280, 32, 32
+
+
+def _be256(x) -> bytes:
+    """an int or a 256-byte big-endian string -> 256 bytes"""
+    if isinstance(x, int):
+        return x.to_bytes(256, "big")
+    b = bytes(x)
+    if len(b) != 256:
+        raise ValueError("RSA-2048 values are 256-byte big-endian strings")
+    return b
+
+
+def rsa2048_em(message: bytes) -> bytes:
+    """EMSA-PKCS1-v1_5 of SHA-256(message) for a 256-byte modulus (deep_ali/src/rsa2048.rs:71-90)."""
+    em = ctypes.create_string_buffer(256)
+    rc = lib().sg_rsa2048_em(message, len(message), em)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_rsa2048_em failed")
+    return em.raw
+
+
+def rsa2048_verify(n, s, em) -> bool:
+    """Native RSASSA-PKCS1-v1_5 check s^65537 mod n == em (deep_ali/src/rsa2048.rs:92-127)."""
+    return lib().sg_rsa2048_verify(_be256(n), _be256(s), _be256(em)) == 1
+
+
+def rsa2048_pi_record(n, s, message: bytes, em) -> bytes:
+    """pi_hash of one RSA record (prove_rsa2048_record_v1.rs:178-187)."""
+    out = ctypes.create_string_buffer(32)
+    rc = lib().sg_rsa2048_pi_record(_be256(n), _be256(s), message, len(message), _be256(em), out)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_rsa2048_pi_record failed")
+    return out.raw
+
+
+def rsa2048_pi_stacked(n, ems) -> bytes:
+    """pi_hash of a stacked zone under one modulus (stacked_rsa_zone_prover.rs:158-165)."""
+    out = ctypes.create_string_buffer(32)
+    blob = b"".join(_be256(e) for e in ems)
+    rc = lib().sg_rsa2048_pi_stacked(_be256(n), len(ems), blob, out)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_rsa2048_pi_stacked failed")
+    return out.raw
+
+
+def _rsa_records(records):
+    """[(n, s, em)] (ints or 256-byte strings) -> concatenated n, s, em arrays"""
+    if not records:
+        raise ValueError("need at least one RSA record")
+    ns = b"".join(_be256(r[0]) for r in records)
+    ss = b"".join(_be256(r[1]) for r in records)
+    es = b"".join(_be256(r[2]) for r in records)
+    return ns, ss, es
+
+
+def rsa2048_trace(records) -> np.ndarray:
+    """fill_rsa_exp_multirow / fill_rsa_stacked on the host -> (len(records) * 11041, 32) uint64."""
+    ns, ss, es = _rsa_records(records)
+    out = np.empty(len(records) * RSA_WIDTH * RSA_N_TRACE, dtype=np.uint64)
+    rc = lib().sg_rsa2048_trace(ns, ss, es, len(records), out.ctypes.data, out.size)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_rsa2048_trace failed")
+    return out.reshape(len(records) * RSA_WIDTH, RSA_N_TRACE)
 
 
 def _records(records):
@@ -549,6 +627,47 @@ class Context:
     def prove_sha512(self, message: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
         """SHA-512 AIR proof (LDE x32, lambda_j = j+1, STIR) -> (proof bytes, 64-byte digest); self-verified."""
         return self._prove_hash("sha512", message, fs_binding, phi_mode)
+
+    def rsa2048_trace(self, records, out=None):
+        """The RSA trace with the cells expanded on the GPU -> (len(records) * 11041, 32);
+        `out`, if given, is a device tensor of at least that many elements."""
+        ns, ss, es = _rsa_records(records)
+        cells = len(records) * RSA_WIDTH * RSA_N_TRACE
+        host = out is None
+        if host:
+            out = np.empty(cells, dtype=np.uint64)
+        op, _k, _ = _addr(out)
+        self._check(self._lib.sg_rsa2048_trace_gpu(self._h, ns, ss, es, len(records), op, cells))
+        return out.reshape(len(records) * RSA_WIDTH, RSA_N_TRACE) if host else out
+
+    def merge_rsa2048(self, lde, n_records: int, n_trace: int = RSA_N_TRACE, blowup: int = RSA_BLOWUP, out=None):
+        """deep_ali_merge_rsa_exp_multirow / _stacked on a (n_records * 11041, n_trace * blowup) LDE -> c_eval."""
+        n = n_trace * blowup
+        ip, _ki, is_np = _addr(lde)
+        if out is None:
+            if not is_np:
+                raise ValueError("device input needs an explicit out buffer")
+            out = np.empty(n, dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        self._check(self._lib.sg_merge_rsa2048(self._h, ip, n_records, n_trace, blowup, op))
+        return out
+
+    def prove_rsa2048(self, records, pi: bytes) -> bytes:
+        """RSA-2048 signature-check proof of [(n, s, em)] records (one record:
+        prove_rsa2048_record_v1.rs; several: stacked_rsa_zone_prover.rs) -> proof bytes; self-verified."""
+        if len(pi) != 32:
+            raise ValueError("pi must be 32 bytes")
+        ns, ss, es = _rsa_records(records)
+        cap = 1 << 20
+        while True:
+            buf = ctypes.create_string_buffer(cap)
+            ln = ctypes.c_size_t()
+            rc = self._lib.sg_prove_rsa2048(self._h, ns, ss, es, len(records), pi, buf, cap, ctypes.byref(ln))
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return buf.raw[:ln.value]
 
     def prove_inner_shard(self, records, salt: bytes, fs_binding: bytes, stir: bool = True):
         """prove_inner_shard (swarm-dns/src/prover.rs:148-225) on canonical records ->

@@ -4,8 +4,10 @@
 
 #include "context.hpp"
 #include "dns.hpp"
+#include "merge.cuh"
 #include "merkle.cuh"
 #include "prover.hpp"
+#include "rsa_air.cuh"
 #include "sha256_air.cuh"
 #include "sha512_air.cuh"
 #include "verifier.hpp"
@@ -337,6 +339,107 @@ int sg_prove_sha512(sg_ctx* c, const uint8_t* msg, size_t len, const uint8_t fs_
         sg::prove_hash_message(c, sg::sha512_hash_air(), msg, len, fs_binding, phi_mode, true, digest);
     *len_out = b.size();
     if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_sha512: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+// ------------------------------------------------------------------ RSA-2048
+int sg_rsa2048_em(const uint8_t* msg, size_t len, uint8_t em[256]) {
+  if ((!msg && len) || !em) return SG_EINVAL;
+  sg::rsa::em_encode(msg, len, em);
+  return SG_OK;
+}
+
+int sg_rsa2048_verify(const uint8_t n_be[256], const uint8_t s_be[256], const uint8_t em[256]) {
+  if (!n_be || !s_be || !em) return 0;
+  try {
+    return sg::rsa::verify_native(n_be, s_be, em) ? 1 : 0;
+  } catch (...) {
+    return 0;
+  }
+}
+
+int sg_rsa2048_pi_record(const uint8_t n_be[256], const uint8_t s_be[256], const uint8_t* msg, size_t len,
+                         const uint8_t em[256], uint8_t out[32]) {
+  if (!n_be || !s_be || (!msg && len) || !em || !out) return SG_EINVAL;
+  sg::rsa::pi_record(n_be, s_be, msg, len, em, out);
+  return SG_OK;
+}
+
+int sg_rsa2048_pi_stacked(const uint8_t n_be[256], size_t n_records, const uint8_t* ems, uint8_t out[32]) {
+  if (!n_be || (!ems && n_records) || !out) return SG_EINVAL;
+  sg::rsa::pi_stacked(n_be, n_records, ems, out);
+  return SG_OK;
+}
+
+int sg_rsa2048_trace(const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, size_t n_records,
+                     uint64_t* trace, size_t cap) {
+  if (!n_be || !s_be || !em_be || n_records == 0) return SG_EINVAL;
+  try {
+    std::vector<sg::rsa::RecordW> recs;
+    std::vector<sg::rsa::RowW> rows;
+    sg::rsa_witnesses(n_be, s_be, em_be, n_records, &recs, &rows);
+    if (!trace || (uint64_t)n_records * sg::rsa::WIDTH * sg::rsa::N_TRACE > cap) return SG_ESPACE;
+    sg::rsa::expand_host(recs.data(), rows.data(), n_records, trace);
+    return SG_OK;
+  } catch (const sg::SgError& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return SG_ENOMEM;
+  }
+}
+
+int sg_rsa2048_trace_gpu(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be,
+                         size_t n_records, uint64_t* trace, size_t cap) {
+  return guarded(c, [&] {
+    sg::require(n_be && s_be && em_be && n_records > 0, "rsa2048_trace_gpu: null argument");
+    std::vector<sg::rsa::RecordW> recs;
+    std::vector<sg::rsa::RowW> rows;
+    sg::rsa_witnesses(n_be, s_be, em_be, n_records, &recs, &rows);
+    const uint64_t cells = (uint64_t)n_records * sg::rsa::WIDTH * sg::rsa::N_TRACE;
+    if (!trace || cells > cap) throw sg::SgError{SG_ESPACE, "rsa2048_trace_gpu: trace buffer too small"};
+    Out dout(trace, cells, c->stream);
+    const size_t rb = recs.size() * sizeof(sg::rsa::RecordW), wb = rows.size() * sizeof(sg::rsa::RowW);
+    sg::DBuf d_wit((rb + wb + 7) / 8, c->stream);
+    uint8_t* base = (uint8_t*)d_wit.p;
+    sg::cuda_check(cudaMemcpyAsync(base, recs.data(), rb, cudaMemcpyHostToDevice, c->stream), "h2d");
+    sg::cuda_check(cudaMemcpyAsync(base + rb, rows.data(), wb, cudaMemcpyHostToDevice, c->stream), "h2d");
+    sg::cuda_check(sg::rsa_expand((const sg::rsa::RecordW*)base, (const sg::rsa::RowW*)(base + rb), n_records,
+                                  dout.d, c->stream),
+                   "rsa_expand");
+    dout.finish();
+  });
+}
+
+int sg_merge_rsa2048(sg_ctx* c, const uint64_t* lde, size_t n_records, size_t n_trace, size_t blowup,
+                     uint64_t* c_eval) {
+  return guarded(c, [&] {
+    sg::require(lde && c_eval && n_records > 0 && n_records <= 65535, "merge_rsa2048: bad argument");
+    sg::require(n_trace >= 2 && (n_trace & (n_trace - 1)) == 0 && blowup >= 4 && (blowup & (blowup - 1)) == 0,
+                "merge_rsa2048: n_trace and blowup must be powers of 2 (blowup >= 4)");
+    const size_t n = n_trace * blowup;
+    unsigned ln = 0;
+    while ((size_t(1) << ln) < n) ++ln;
+    sg::require(ln <= sg::kMaxLogN, "merge_rsa2048: domain larger than 2^28");
+    cudaStream_t s = c->stream;
+    In di(lde, n_records * sg::rsa::WIDTH * n, s);
+    Out dout(c_eval, n, s);
+    sg::DBuf phi(n, s), part(n_records > 1 ? n_records * n : 0, s), scratch(sg::ntt_scratch_elems(1, ln), s);
+    sg::cuda_check(sg::rsa_phi(di.d, n_records, n_trace, blowup, part.p, phi.p, s), "rsa phi");
+    sg::cuda_check(sg::ntt_batch(c->tw, phi.p, phi.p, 1, n, n, ln, true, n, scratch.p, s), "intt");
+    sg::cuda_check(sg::quotient_zh(phi.p, n, n_trace, dout.d, s), "quotient");
+    sg::cuda_check(sg::ntt_batch(c->tw, dout.d, dout.d, 1, n, n, ln, false, n - n_trace, scratch.p, s), "ntt");
+    dout.finish();
+  });
+}
+
+int sg_prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, size_t n_records,
+                     const uint8_t pi[32], uint8_t* proof, size_t cap, size_t* len) {
+  return guarded(c, [&] {
+    sg::require(n_be && s_be && em_be && pi && len, "prove_rsa2048: null argument");
+    std::vector<uint8_t> b = sg::prove_rsa2048(c, n_be, s_be, em_be, n_records, pi, true);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_rsa2048: proof buffer too small"};
     memcpy(proof, b.data(), b.size());
   });
 }

@@ -5,6 +5,7 @@
 // evaluations and the layer root (a few hundred bytes), derives the next
 // challenges, and finally gathers the s0 query openings in one copy.
 #include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "context.hpp"
@@ -12,6 +13,7 @@
 #include "gl.cuh"
 #include "merge.cuh"
 #include "merkle.cuh"
+#include "rsa_air.cuh"
 #include "prover.hpp"
 #include "hash_air.hpp"
 #include "sha256_air.cuh"
@@ -775,6 +777,74 @@ std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uin
   cuda_check(cudaStreamSynchronize(s), "sync");
   sg_fri_params p;
   sg_build_params(n0, fs_binding, 1, &p);
+  std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
+  if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
+    throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
+  return proof;
+}
+
+// ------------------------------------------------------------------ RSA-2048 pipeline
+void rsa_witnesses(const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, uint64_t n_records,
+                   std::vector<rsa::RecordW>* recs, std::vector<rsa::RowW>* rows) {
+  recs->resize(n_records);
+  rows->resize(n_records * rsa::N_TRACE);
+  const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint64_t nt = std::min<uint64_t>(n_records, std::min<uint64_t>(hw, 32));
+  std::vector<SgError> errs(nt);
+  std::vector<char> failed(nt, 0);
+  auto work = [&](uint64_t w) {
+    try {
+      for (uint64_t r = w; r < n_records; r += nt)
+        rsa::witness(n_be + 256 * r, s_be + 256 * r, em_be + 256 * r, &(*recs)[r], &(*rows)[r * rsa::N_TRACE]);
+    } catch (const SgError& e) {
+      errs[w] = e;
+      failed[w] = 1;
+    }
+  };
+  if (nt <= 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (uint64_t w = 0; w < nt; ++w) th.emplace_back(work, w);
+    for (auto& t : th) t.join();
+  }
+  for (uint64_t w = 0; w < nt; ++w)
+    if (failed[w]) throw errs[w];
+}
+
+std::vector<uint8_t> prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be,
+                                   uint64_t n_records, const uint8_t pi[32], bool self_verify) {
+  require(n_records >= 1 && n_records <= 65535, "prove_rsa2048: 1 to 65535 records");
+  std::vector<rsa::RecordW> recs;
+  std::vector<rsa::RowW> rows;
+  rsa_witnesses(n_be, s_be, em_be, n_records, &recs, &rows);
+  const uint64_t n_trace = rsa::N_TRACE, blowup = rsa::BLOWUP, n0 = n_trace * blowup;
+  const uint64_t W = n_records * rsa::WIDTH;
+  const unsigned ln = log2_exact(n0);
+  cudaStream_t s = c->stream;
+  const uint64_t rec_bytes = recs.size() * sizeof(rsa::RecordW), row_bytes = rows.size() * sizeof(rsa::RowW);
+  DBuf d_trace(W * n_trace, s), d_c(n0, s);
+  {
+    DBuf d_wit((rec_bytes + row_bytes + 7) / 8, s);
+    uint8_t* base = (uint8_t*)d_wit.p;
+    static_assert(sizeof(rsa::RecordW) % 8 == 0, "witness alignment");
+    cuda_check(cudaMemcpyAsync(base, recs.data(), rec_bytes, cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(cudaMemcpyAsync(base + rec_bytes, rows.data(), row_bytes, cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(rsa_expand((const rsa::RecordW*)base, (const rsa::RowW*)(base + rec_bytes), n_records, d_trace.p, s),
+               "rsa trace expand");
+    cuda_check(cudaStreamSynchronize(s), "sync");  // the host witnesses must outlive their copies
+  }
+  {
+    DBuf d_lde(W * n0, s), phi(n0, s), part(n_records > 1 ? n_records * n0 : 0, s);
+    DBuf scratch(ntt_scratch_elems(1, ln), s);
+    lde_device(c, d_trace.p, W, n_trace, blowup, 1, d_lde.p);
+    cuda_check(rsa_phi(d_lde.p, n_records, n_trace, blowup, part.p, phi.p, s), "rsa phi");
+    ntt(c, phi.p, phi.p, 1, n0, n0, ln, true, n0, scratch.p);
+    cuda_check(quotient_zh(phi.p, n0, n_trace, d_c.p, s), "quotient");
+    ntt(c, d_c.p, d_c.p, 1, n0, n0, ln, false, n0 - n_trace, scratch.p);
+  }
+  sg_fri_params p;
+  sg_build_params(n0, pi, 1, &p);
   std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
   if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
     throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};

@@ -6,6 +6,7 @@
 #include "context.hpp"
 #include "hash_air.hpp"
 #include "protocol.hpp"
+#include "rsa2048.hpp"
 
 namespace sg {
 
@@ -28,6 +29,15 @@ std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uin
 std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
                                           int phi_mode, bool self_verify, uint8_t digest[32]);
 std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p);
+// RSA-2048 signature-check proof (prove_rsa2048_record_v1.rs for one record,
+// stacked_rsa_zone_prover.rs for several): witnesses on the host, trace expanded
+// on the device -> LDE x32 -> RSA merge (Phi always evaluated) -> STIR with
+// build_params(1024, pi). Inputs: n_records 256-byte big-endian n, s, em each.
+std::vector<uint8_t> prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be,
+                                   uint64_t n_records, const uint8_t pi[32], bool self_verify);
+// The host witnesses of n_records records (threads over records).
+void rsa_witnesses(const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, uint64_t n_records,
+                   std::vector<rsa::RecordW>* recs, std::vector<rsa::RowW>* rows);
 // prove_inner_shard / prove_outer_rollup core: HashRollup trace -> LDE x32 -> merge ->
 // STIR (stir) or classic DEEP-FRI, with build_params(n0, pi).
 std::vector<uint8_t> prove_hash_rollup_host_leaves(sg_ctx* c, const uint64_t* leaves, uint64_t n_leaves,
