@@ -151,6 +151,12 @@ def load_oracle():
     return oracle_lib
 
 
+def load_oracle_rsa():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_rsa
+    return oracle_rsa
+
+
 def cpu_sample(trace, threads):
     """Time the oracle (C++ restatement of the reference CPU prover, OpenMP) on a
     bounded sample and scale to one full step: LDE of 8 of the 64 columns (x8),
@@ -251,18 +257,88 @@ def sha256_large(sg, ctx, blocks, reps, cpu_threads):
     return res
 
 
+def rsa_keys():
+    """Seeded RSA-2048 test keys (n, d) shipped with the tests (tests/golden/rsa2048_keys.json)."""
+    with open(os.path.join(ROOT, "tests", "golden", "rsa2048_keys.json")) as f:
+        return [(int(k["n"], 16), int(k["d"], 16)) for k in json.load(f)["keys"]]
+
+
+def rsa_record(sg, msg, key):
+    """(n, s, em) of an RSASSA-PKCS1-v1_5 / SHA-256 signature of msg, and its pi_hash
+    (prove_rsa2048_record_v1.rs recipe)."""
+    n, d = key
+    em = sg.rsa2048_em(msg)
+    s = pow(int.from_bytes(em, "big"), d, n)
+    assert sg.rsa2048_verify(n, s, em)
+    return (n, s, int.from_bytes(em, "big")), sg.rsa2048_pi_record(n, s, msg, em)
+
+
+def rsa2048(sg, ctx, n_jobs, stacked, cpu_threads):
+    """RSA-2048 signature-check proofs (prove_rsa2048_record_v1.rs: n_trace 32,
+    11041 columns, 11280 constraints, blowup 32, STIR [8,8,8,2]): one record per
+    proof one at a time vs 16 in flight, and `stacked` records in one proof
+    (stacked_rsa_zone_prover.rs). Inputs cross as bytes; proofs are self-verified."""
+    keys = rsa_keys()
+    recs = [rsa_record(sg, b"DNSSEC-RRSIG-V0|rec%05d.example.com.|A|10.0.%d.%d|epoch-0|alg-8" % (i, i // 256, i % 256),
+                       keys[i % len(keys)]) for i in range(max(n_jobs, stacked))]
+    jobs = [(sg.JOB_RSA2048, [r], pi) for r, pi in recs[:n_jobs]]
+    ctx.prove_batch(jobs[:16], n_streams=16)
+    out = {"workload": "RSA-2048 PKCS#1 v1.5 signature-check proof (e = 65537 chain, n_trace 32, 11041 cols, "
+                       "11280 constraints, blowup 32, n0 1024), self-verified", "jobs": n_jobs}
+    for label, streams in (("plain", 1), ("batched", 16)):
+        t0 = time.perf_counter()
+        res = ctx.prove_batch(jobs, n_streams=streams)
+        dt = time.perf_counter() - t0
+        assert all(r.status == 0 for _, r in res)
+        lat = sorted(r.latency_ms for _, r in res)
+        out[label] = {"streams": streams, "proofs_per_s": n_jobs / dt, "p50_ms": lat[len(lat) // 2],
+                      "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
+    out["batched_over_plain"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
+    if stacked:
+        zone = [r for r, _ in recs[:stacked]]
+        pi = hashlib.sha3_256(b"stacked zone").digest()
+        ctx.prove_rsa2048(zone, pi)
+        t0 = time.perf_counter()
+        ctx.prove_rsa2048(zone, pi)
+        dt = time.perf_counter() - t0
+        out["stacked"] = {"records": stacked, "ms_per_proof": dt * 1e3, "records_per_s": stacked / dt}
+    if cpu_threads:
+        R = load_oracle_rsa()
+        O = load_oracle()
+        O.set_threads(cpu_threads)
+        (rec, pi) = recs[0]
+        t0 = time.perf_counter()
+        tr = R.trace([rec])
+        cpu_proof = R.prove(tr, pi)
+        dt = time.perf_counter() - t0
+        assert cpu_proof == ctx.prove_rsa2048([rec], pi), "GPU and oracle RSA proofs differ"
+        out["cpu_baseline"] = {"proofs_per_s": 1.0 / dt, "cores": cpu_threads, "kind": "port",
+                               "sample": "one single-record proof by the oracle (trace, LDE, merge, STIR)"}
+        out["plain_over_cpu"] = out["plain"]["proofs_per_s"] * dt
+    return out
+
+
 def serving(sg, ctx, rates, n_jobs, streams, seed=7):
-    """Poisson arrivals of hash-AIR proof requests over record-length messages
-    (lognormal, median 120 B, clipped to 40-600 B), 80 % SHA-256 and 20 % SHA-512,
-    admitted by the continuous-batching server under a 160 GB HBM budget; p50/p99
-    latency from submit to result, and throughput against one proof at a time."""
+    """Poisson arrivals of proof requests admitted by the continuous-batching server
+    under a 160 GB HBM budget: 52 % SHA-256 record proofs and 20 % SHA-512 over
+    record-length messages (lognormal, median 120 B, clipped to 40-600 B), and 28 %
+    RSA-2048 signature checks; p50/p99 latency from submit to result, and
+    throughput against one proof at a time."""
     rng = np.random.default_rng(seed)
     lens = np.clip(np.round(rng.lognormal(np.log(120), 0.6, n_jobs)), 40, 600).astype(int)
     msgs = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in lens]
-    kinds = [sg.JOB_SHA512 if u < 0.2 else sg.JOB_SHA256 for u in rng.random(n_jobs)]
+    u = rng.random(n_jobs)
+    kinds = [sg.JOB_SHA512 if x < 0.2 else sg.JOB_RSA2048 if x < 0.48 else sg.JOB_SHA256 for x in u]
     pis = [hashlib.sha3_256(b"serve-%d" % i).digest() for i in range(n_jobs)]
+    keys = rsa_keys()
+    for i in range(n_jobs):
+        if kinds[i] == sg.JOB_RSA2048:
+            rec, pis[i] = rsa_record(sg, msgs[i], keys[i % len(keys)])
+            msgs[i] = [rec]
 
     def prove_one(i):
+        if kinds[i] == sg.JOB_RSA2048:
+            return ctx.prove_rsa2048(msgs[i], pis[i])
         f = ctx.prove_sha512 if kinds[i] == sg.JOB_SHA512 else ctx.prove_sha256
         return f(msgs[i], pis[i])[0]
 
@@ -271,8 +347,8 @@ def serving(sg, ctx, rates, n_jobs, streams, seed=7):
     for i in range(n_jobs):
         prove_one(i)
     plain = n_jobs / (time.perf_counter() - t0)
-    out = {"workload": "hash-AIR proofs (80 % SHA-256, 20 % SHA-512), messages lognormal(median 120 B) "
-                       "clipped 40-600 B, Poisson arrivals",
+    out = {"workload": "52 % SHA-256 and 20 % SHA-512 AIR proofs of messages lognormal(median 120 B) clipped "
+                       "40-600 B, 28 % RSA-2048 signature-check proofs; Poisson arrivals",
            "jobs_per_rate": n_jobs, "streams": streams, "hbm_budget_gb": 160, "plain_proofs_per_s": plain,
            "rates": []}
     for lam in rates:
@@ -323,6 +399,9 @@ def main():
     ap.add_argument("--sha256-large-blocks", type=int, default=8192,
                     help="blocks of the large SHA-256 trace proof (8192 = 2^20 rows; 0 skips it)")
     ap.add_argument("--serve-jobs", type=int, default=200, help="jobs per arrival rate in the serving sweep (0 skips)")
+    ap.add_argument("--rsa-jobs", type=int, default=256,
+                    help="single-record RSA-2048 proofs for the plain-vs-batched section (0 skips it)")
+    ap.add_argument("--rsa-stacked", type=int, default=64, help="records in the stacked RSA-2048 proof (0 skips)")
     ap.add_argument("--serve-rates", default="50,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--no-classic-fri", dest="classic_fri", action="store_false",
                     help="skip the classic DEEP-FRI timing")
@@ -508,6 +587,7 @@ def main():
 
     cpu_threads = (os.cpu_count() or 1) if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else 0
     large = sha256_large(sg, ctx, args.sha256_large_blocks, 3, cpu_threads) if args.sha256_large_blocks > 0 else None
+    rsa = rsa2048(sg, ctx, args.rsa_jobs, args.rsa_stacked, cpu_threads) if args.rsa_jobs > 0 else None
     serve = None
     if args.serve_jobs > 0:
         serve = serving(sg, ctx, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs, 16)
@@ -536,6 +616,7 @@ def main():
             "cpu_baseline": cpu,
             "sha256_proofs": cfg1,
             "sha256_large_trace": large,
+            "rsa2048": rsa,
             "serving": serve,
             "classic_fri": classic,
             "proof_bytes": len(ref[1]),

@@ -327,6 +327,8 @@ int sg_prove_outer_rollup(sg_ctx* ctx, const uint8_t* pi_hashes, size_t n, const
 #define SG_JOB_SHA256 1      /* input = message bytes, input_len = bytes (sg_prove_sha256) */
 #define SG_JOB_HASH_ROLLUP 2 /* input = u64 rollup leaves, input_len = count (sg_prove_hash_rollup) */
 #define SG_JOB_SHA512 3      /* input = message bytes, input_len = bytes (sg_prove_sha512) */
+#define SG_JOB_RSA2048 4     /* input = records of n || s || em (256 bytes each, big-endian), input_len =
+                                768 * records (sg_prove_rsa2048; pi = public_inputs_hash) */
 
 typedef struct {
   int32_t kind;
@@ -340,7 +342,7 @@ typedef struct {
   int32_t status; /* SG_OK or an SG_E* code */
   uint32_t reserved;
   size_t proof_len;
-  uint8_t digest[64]; /* SHA-256 jobs: the asserted digest (32 bytes); SHA-512 jobs: 64 bytes */
+  uint8_t digest[64]; /* SHA-256 jobs: the asserted digest (32 bytes); SHA-512 jobs: 64 bytes; others: zero */
   double queue_ms;    /* submit -> start */
   double run_ms;      /* start -> proof ready */
   double latency_ms;  /* submit -> proof ready */

@@ -114,7 +114,7 @@ EXPORTS = (
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
 )
-JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512 = 1, 2, 3
+JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048 = 1, 2, 3, 4
 OPT_WIDE_MERGE = 1
 WIDE_MERGE_AUTO, WIDE_MERGE_LDE, WIDE_MERGE_COSETS = 0, 1, 2
 
@@ -776,7 +776,12 @@ def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
     """A sg_job plus the buffer it points to (keep both alive until submitted)."""
     if len(pi) != 32:
         raise ValueError("pi must be 32 bytes")
-    if kind in (JOB_SHA256, JOB_SHA512):
+    if kind == JOB_RSA2048:
+        # data: [(n, s, em)] records (ints or 256-byte big-endian strings)
+        data = b"".join(_be256(r[0]) + _be256(r[1]) + _be256(r[2]) for r in data)
+        if not data:
+            raise ValueError("an RSA job needs at least one record")
+    if kind in (JOB_SHA256, JOB_SHA512, JOB_RSA2048):
         buf = ctypes.create_string_buffer(bytes(data), max(1, len(data)))
         n = len(data)
     elif kind == JOB_HASH_ROLLUP:
@@ -786,7 +791,7 @@ def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
         raise ValueError("unknown job kind")
     j = Job()
     j.kind, j.phi_mode = kind, phi_mode
-    j.input = ctypes.addressof(buf) if kind in (JOB_SHA256, JOB_SHA512) else (buf.ctypes.data if n else None)
+    j.input = ctypes.addressof(buf) if kind != JOB_HASH_ROLLUP else (buf.ctypes.data if n else None)
     j.input_len = n
     ctypes.memmove(j.pi, pi, 32)
     return j, buf

@@ -21,6 +21,7 @@
 
 #include "context.hpp"
 #include "prover.hpp"
+#include "rsa2048.hpp"
 #include "sha256_air.cuh"
 #include "sha512_air.cuh"
 
@@ -60,8 +61,24 @@ uint64_t footprint_bytes(const sg_job& j) {
     const uint64_t nt = next_pow2(128 * blocks), n0 = nt * 32;
     return 8 * ((uint64_t)sg::sha512::WIDTH * (n0 + 2 * nt) + 16 * n0);
   }
+  if (j.kind == SG_JOB_RSA2048) {
+    const uint64_t recs = j.input_len / 768, w = recs * sg::rsa::WIDTH;
+    return 8 * (w * (sg::rsa::N_TRACE + 1024) + (recs + 16) * 1024);
+  }
   const uint64_t nt = next_pow2(j.input_len < 8 ? 8 : j.input_len), n0 = nt * 32;
   return 8 * (4 * n0 + 8 * nt + 16 * n0);
+}
+
+// n || s || em per record (256 bytes each) -> the three contiguous arrays prove_rsa2048 takes
+std::vector<uint8_t> prove_rsa_job(sg_ctx* c, const std::vector<uint8_t>& in, const uint8_t pi[32]) {
+  const uint64_t recs = in.size() / 768;
+  std::vector<uint8_t> n(256 * recs), s(256 * recs), em(256 * recs);
+  for (uint64_t r = 0; r < recs; ++r) {
+    memcpy(&n[256 * r], &in[768 * r], 256);
+    memcpy(&s[256 * r], &in[768 * r + 256], 256);
+    memcpy(&em[256 * r], &in[768 * r + 512], 256);
+  }
+  return sg::prove_rsa2048(c, n.data(), s.data(), em.data(), recs, pi, true);
 }
 
 }  // namespace
@@ -121,6 +138,8 @@ struct sg_server {
       } else if (e->kind == SG_JOB_SHA512) {
         e->proof = sg::prove_hash_message(c, sg::sha512_hash_air(), e->input.data(), e->input.size(), e->pi,
                                           e->phi_mode, true, e->digest);
+      } else if (e->kind == SG_JOB_RSA2048) {
+        e->proof = prove_rsa_job(c, e->input, e->pi);
       } else {
         const uint64_t n = e->input.size() / 8;
         e->proof = sg::prove_hash_rollup_host_leaves(c, (const uint64_t*)e->input.data(), n, e->pi, e->phi_mode, true);
@@ -178,8 +197,11 @@ void sg_server_destroy(sg_server* s) {
 
 int sg_server_submit(sg_server* s, const sg_job* job, uint64_t* ticket) {
   if (!s || !job || !ticket) return SG_EINVAL;
-  if (job->kind != SG_JOB_SHA256 && job->kind != SG_JOB_SHA512 && job->kind != SG_JOB_HASH_ROLLUP) return SG_EINVAL;
+  if (job->kind != SG_JOB_SHA256 && job->kind != SG_JOB_SHA512 && job->kind != SG_JOB_HASH_ROLLUP &&
+      job->kind != SG_JOB_RSA2048)
+    return SG_EINVAL;
   if (job->input_len && !job->input) return SG_EINVAL;
+  if (job->kind == SG_JOB_RSA2048 && (job->input_len == 0 || job->input_len % 768)) return SG_EINVAL;
   Entry e;
   e.kind = job->kind;
   e.phi_mode = job->phi_mode;

@@ -1,5 +1,5 @@
 """Batched and served proving: every proof made in a mix of concurrent jobs
-(SHA-256, SHA-512 and HashRollup) is
+(SHA-256, SHA-512, HashRollup and RSA-2048 signature checks) is
 byte-identical to the same job proved alone (oracle), under several stream
 counts and an HBM budget tight enough to serialise admission; the server
 accepts submissions while earlier jobs are running."""
@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import oracle_lib as O
+import oracle_rsa as R
 
 pytestmark = pytest.mark.gpu
 
@@ -17,9 +18,15 @@ pytestmark = pytest.mark.gpu
 def _mix(n, seed):
     rng = np.random.default_rng(seed)
     jobs, want = [], []
+    keys = R.keys()
     for i in range(n):
         pi = hashlib.sha3_256(b"job%d" % i).digest()
-        if i % 4 == 2:
+        if i % 5 == 4:
+            k = 1 + i % 2
+            recs = [R.record(b"job%d rec%d" % (i, r), keys[(i + r) % 4])[0] for r in range(k)]
+            jobs.append((4, recs, pi))
+            want.append((R.prove(R.trace(recs), pi), None))
+        elif i % 4 == 2:
             leaves = rng.integers(0, O.P, int(rng.integers(1, 3000)), dtype=np.uint64)
             jobs.append((2, leaves, pi))
             want.append((O.prove_hash_rollup(leaves, pi), None))
