@@ -223,6 +223,17 @@ def lib():
     return L
 
 
+_PROOF_CAP = 1 << 24  # proof buffer size; untouched pages of np.empty cost nothing, a larger proof is retried
+
+
+def _out_buffer(cap):
+    """An uninitialised byte buffer for a C call to write into: (numpy array, char pointer).
+    Only the prefix the call reports as written is read back, so nothing is zero-filled
+    or copied beyond the proof itself."""
+    arr = np.empty(max(1, cap), dtype=np.uint8)
+    return arr, ctypes.cast(arr.ctypes.data, ctypes.c_char_p)
+
+
 def _addr(x):
     """(pointer, keepalive, is_numpy) for a numpy uint64 array, a CUDA tensor or an int device pointer."""
     if isinstance(x, np.ndarray):
@@ -587,9 +598,9 @@ class Context:
             raise ValueError("fs_binding must be 32 bytes")
         dbytes = _HASH[hash_name][2]
         fn = getattr(self._lib, f"sg_prove_{hash_name}")
-        cap = 1 << 24
+        cap = _PROOF_CAP
         while True:
-            buf = ctypes.create_string_buffer(cap)
+            arr, buf = _out_buffer(cap)
             ln = ctypes.c_size_t()
             dg = ctypes.create_string_buffer(dbytes)
             rc = fn(self._h, message, len(message), fs_binding, phi_mode, buf, cap, ctypes.byref(ln), dg)
@@ -597,7 +608,7 @@ class Context:
                 cap = ln.value
                 continue
             self._check(rc)
-            return buf.raw[:ln.value], dg.raw
+            return arr[:ln.value].tobytes(), dg.raw
 
     def sha256_trace(self, message: bytes, out=None):
         """build_sha256_trace_multi with the column expansion on the GPU ->
@@ -658,16 +669,16 @@ class Context:
         if len(pi) != 32:
             raise ValueError("pi must be 32 bytes")
         ns, ss, es = _rsa_records(records)
-        cap = 1 << 20
+        cap = _PROOF_CAP
         while True:
-            buf = ctypes.create_string_buffer(cap)
+            arr, buf = _out_buffer(cap)
             ln = ctypes.c_size_t()
             rc = self._lib.sg_prove_rsa2048(self._h, ns, ss, es, len(records), pi, buf, cap, ctypes.byref(ln))
             if rc == SG_ESPACE:
                 cap = ln.value
                 continue
             self._check(rc)
-            return buf.raw[:ln.value]
+            return arr[:ln.value].tobytes()
 
     def prove_inner_shard(self, records, salt: bytes, fs_binding: bytes, stir: bool = True):
         """prove_inner_shard (swarm-dns/src/prover.rs:148-225) on canonical records ->
@@ -675,9 +686,9 @@ class Context:
         if len(salt) != 16 or len(fs_binding) != 32:
             raise ValueError("salt must be 16 bytes and fs_binding 32 bytes")
         canon, offs = _records(records)
-        cap = 1 << 24
+        cap = _PROOF_CAP
         while True:
-            buf = ctypes.create_string_buffer(cap)
+            arr, buf = _out_buffer(cap)
             ln = ctypes.c_size_t()
             pi, root = ctypes.create_string_buffer(32), ctypes.create_string_buffer(32)
             rc = self._lib.sg_prove_inner_shard(self._h, canon, offs, len(records), salt, fs_binding, int(stir), buf,
@@ -686,15 +697,15 @@ class Context:
                 cap = ln.value
                 continue
             self._check(rc)
-            return buf.raw[:ln.value], pi.raw, root.raw
+            return arr[:ln.value].tobytes(), pi.raw, root.raw
 
     def prove_outer_rollup(self, pi_hashes, pk_hash: bytes, stir: bool = True) -> bytes:
         """prove_outer_rollup (swarm-dns/src/prover.rs:250-304) -> proof bytes; self-verified."""
         if len(pk_hash) != 32 or not pi_hashes:
             raise ValueError("need pi hashes and a 32-byte pk_hash")
-        cap = 1 << 24
+        cap = _PROOF_CAP
         while True:
-            buf = ctypes.create_string_buffer(cap)
+            arr, buf = _out_buffer(cap)
             ln = ctypes.c_size_t()
             rc = self._lib.sg_prove_outer_rollup(self._h, b"".join(pi_hashes), len(pi_hashes), pk_hash, int(stir),
                                                  buf, cap, ctypes.byref(ln))
@@ -702,7 +713,7 @@ class Context:
                 cap = ln.value
                 continue
             self._check(rc)
-            return buf.raw[:ln.value]
+            return arr[:ln.value].tobytes()
 
     def prove_batch(self, jobs, n_streams: int = 8, hbm_budget_bytes: int = 0, cap_per_job: int = 1 << 20):
         """jobs: list of (kind, data, pi[, phi_mode]) -> list of (proof bytes, JobResult)."""
@@ -743,25 +754,25 @@ class Context:
         ark-serialize (Compress::Yes) bytes of the DeepFriProof."""
         ip, _ki, host = _addr(f0)
         n0 = domain0.size if isinstance(domain0, FriDomain) else int(domain0)
-        cap = 1 << 24
+        cap = _PROOF_CAP
         while True:
-            buf = ctypes.create_string_buffer(cap)
+            arr, buf = _out_buffer(cap)
             ln = ctypes.c_size_t()
             rc = self._lib.sg_stir_prove(self._h, ip, n0, ctypes.byref(params), buf, cap, ctypes.byref(ln))
             if rc == SG_ESPACE:
                 cap = ln.value
                 continue
             self._check(rc)
-            return buf.raw[:ln.value]
+            return arr[:ln.value].tobytes()
 
     def prove_hash_rollup(self, leaves, pi: bytes, phi_mode=PHI_PARALLEL_GATE) -> bytes:
         """prove_inner_shard / prove_outer_rollup core on u64 rollup leaves; self-verified."""
         lv = np.ascontiguousarray(leaves, dtype=np.uint64)
         if len(pi) != 32:
             raise ValueError("pi must be 32 bytes")
-        cap = 1 << 24
+        cap = _PROOF_CAP
         while True:
-            buf = ctypes.create_string_buffer(cap)
+            arr, buf = _out_buffer(cap)
             ln = ctypes.c_size_t()
             rc = self._lib.sg_prove_hash_rollup(self._h, lv.ctypes.data if lv.size else None, lv.size, pi, phi_mode,
                                                 buf, cap, ctypes.byref(ln))
@@ -769,7 +780,7 @@ class Context:
                 cap = ln.value
                 continue
             self._check(rc)
-            return buf.raw[:ln.value]
+            return arr[:ln.value].tobytes()
 
 
 def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
@@ -821,17 +832,17 @@ class Server:
 
     def wait(self, ticket: int):
         """-> (proof bytes, JobResult)"""
-        cap = 1 << 22
+        cap = _PROOF_CAP
         while True:
             res = JobResult()
-            buf = ctypes.create_string_buffer(cap)
+            arr, buf = _out_buffer(cap)
             rc = self._ctx._lib.sg_server_wait(self._h, ticket, ctypes.byref(res), buf, cap)
             if rc == SG_ESPACE:
                 cap = res.proof_len
                 continue
             if rc != SG_OK:
                 raise StarkGpuError(rc, f"job {ticket} failed")
-            return buf.raw[:res.proof_len], res
+            return arr[:res.proof_len].tobytes(), res
 
     def close(self):
         if getattr(self, "_h", None):

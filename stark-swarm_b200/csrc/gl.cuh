@@ -290,6 +290,22 @@ GL_HD Fp6 e_mul(const Fp6& x, const Fp6& y) {
   for (int i = 0; i < 3; ++i) r.c[3 + i] = sub(sub(m[i], v0[i]), v1[i]);
   return r;
 }
+#if defined(__CUDACC__)
+// e_mul as a real call: one copy of its code per kernel. For kernels that run a
+// few CTAs once through (the small STIR layers), fully inlined Fp6 products make
+// the warps wait on instruction fetch; a call keeps the code small and cached.
+static __device__ __noinline__ Fp6 e_mul_call(const Fp6 x, const Fp6 y) { return e_mul(x, y); }
+static __device__ __forceinline__ Fp6 e_pow_call(Fp6 b, uint64_t e) {
+  Fp6 r = e_one();
+#pragma unroll 1
+  while (e) {
+    if (e & 1) r = e_mul_call(r, b);
+    b = e_mul_call(b, b);
+    e >>= 1;
+  }
+  return r;
+}
+#endif
 GL_HD Fp6 e_pow(Fp6 b, uint64_t e) {
   Fp6 r = e_one();
   while (e) {

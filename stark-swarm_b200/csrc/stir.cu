@@ -93,6 +93,62 @@ __global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t
   }
 }
 
+// Small layers (at most kOodSmallGroups groups): one CTA of M warps. Warp r sums
+// T_r = sum_t c_{tM+r} w^t with its lanes striding over t (lane l starts at w^l and
+// steps by w^32), then M threads form evals[j] = sum_r w_M^{jr} z^r T_r. Fp6
+// products go through e_mul_call so the kernel's code stays small: it runs once.
+constexpr uint64_t kOodSmallGroups = 4096;
+template <int M, bool BASE>
+__global__ void __launch_bounds__(M * 32) ood_small_kernel(const uint64_t* c, uint64_t n, gl::Fp6 w, gl::Fp6 w32,
+                                                           gl::Fp6 z, uint64_t* evals) {
+  const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+  const uint64_t n_groups = n / M;
+  __shared__ uint64_t T[M * 6];
+  gl::Fp6 wt = gl::e_pow_call(w, (uint64_t)lane);
+  uint64_t acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+  for (uint64_t t = lane; t < n_groups; t += 32) {
+    const uint64_t k = t * M + r;
+    if constexpr (BASE) {
+      const uint64_t ck = __ldg(c + k);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc[q] = gl::add(acc[q], gl::mul(wt.c[q], ck));
+    } else {
+      gl::Fp6 ck;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) ck.c[q] = __ldg(c + (uint64_t)q * n + k);
+      const gl::Fp6 p = gl::e_mul_call(ck, wt);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) acc[q] = gl::add(acc[q], p.c[q]);
+    }
+    wt = gl::e_mul_call(wt, w32);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const uint64_t v = warp_sum(acc[q]);
+    if (lane == 0) T[r * 6 + q] = v;
+  }
+  __syncthreads();
+  const int j = threadIdx.x;
+  if (j >= M) return;
+  constexpr unsigned EM = (exp16(false) * (16 / M)) % 192;  // w_M = 2^EM
+  gl::Fp6 out = gl::e_zero(), zr = gl::e_one();
+#pragma unroll 1
+  for (int rr = 0; rr < M; ++rr) {
+    gl::Fp6 tr;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) tr.c[q] = T[rr * 6 + q];
+    gl::Fp6 sv = gl::e_mul_call(zr, tr);
+    const unsigned e = (EM * (unsigned)((j * rr) % M)) % 192u;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sv.c[q] = gl::mul_pow2(sv.c[q], e);
+    out = gl::e_add(out, sv);
+    zr = gl::e_mul_call(zr, z);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) evals[j * 6 + q] = out.c[q];
+}
+
 // Sum block partials into T_r, then evals[j] = sum_r w_M^{jr} z^r T_r.
 template <int M>
 __global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, gl::Fp6 z, uint64_t* evals) {
@@ -110,16 +166,17 @@ __global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, g
   if (j >= M) return;
   constexpr unsigned EM = (exp16(false) * (16 / M)) % 192;  // w_M = 2^EM
   gl::Fp6 acc = gl::e_zero(), zr = gl::e_one();
+#pragma unroll 1
   for (int r = 0; r < M; ++r) {
     gl::Fp6 tr;
 #pragma unroll
     for (int q = 0; q < 6; ++q) tr.c[q] = T[r * 6 + q];
-    gl::Fp6 s = gl::e_mul(zr, tr);
+    gl::Fp6 s = gl::e_mul_call(zr, tr);
     const unsigned e = (EM * (unsigned)((j * r) % M)) % 192u;
 #pragma unroll
     for (int q = 0; q < 6; ++q) s.c[q] = gl::mul_pow2(s.c[q], e);
     acc = gl::e_add(acc, s);
-    zr = gl::e_mul(zr, z);
+    zr = gl::e_mul_call(zr, z);
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q) evals[j * 6 + q] = acc.c[q];
@@ -186,6 +243,74 @@ __global__ void fold_kernel(FoldArgs a) {
   }
 }
 
+// The fold for small layers (at most kFoldSmall cosets): the same arithmetic with
+// the per-component DFT in a rolled loop (results in a local array) and the Horner
+// products as calls, so a launch that runs once does not stream a large body of
+// inlined code through the instruction cache.
+constexpr uint64_t kFoldSmall = 4096;
+template <int M, bool BASE>
+__global__ void fold_small_kernel(FoldArgs a) {
+  constexpr int LM = M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : 4;
+  const uint64_t nn = a.n / M;
+  const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (b >= nn) return;
+  constexpr int NC = BASE ? 1 : 6;
+  uint64_t xs[NC][M];
+#pragma unroll 1
+  for (int q = 0; q < NC; ++q) {
+    uint64_t y[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) y[j] = __ldg(a.f + (uint64_t)q * a.n + b + (uint64_t)j * nn);
+    dft_reg<M, true>(y);
+#pragma unroll
+    for (int j = 0; j < M; ++j) xs[q][j] = y[j];
+  }
+  const uint64_t obinv = tw_pow(a.tw_inv_lo, a.tw_inv_hi, b, a.log_n);  // w_n^{-b}
+  constexpr unsigned MINV = 192u - LM;                                     // 1/M = 2^{-LM}
+  if (a.tuples) {
+    uint64_t p = 1;
+#pragma unroll 1
+    for (int k = 0; k < M; ++k) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const uint64_t v = q < NC ? gl::mul(gl::mul_pow2(xs[q][k], MINV), p) : 0;
+        a.tuples[(uint64_t)(k * 6 + q) * nn + b] = v;
+      }
+      p = gl::mul(p, obinv);
+    }
+  }
+  if (!a.next) return;
+  const gl::Fp6 beta = gl::e_scale(a.alpha, obinv);
+  gl::Fp6 acc;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) acc.c[q] = q < NC ? xs[q][M - 1] : 0;
+#pragma unroll 1
+  for (int k = M - 2; k >= 0; --k) {
+    acc = gl::e_mul_call(acc, beta);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) acc.c[q] = gl::add(acc.c[q], xs[q][k]);
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    acc.c[q] = gl::mul_pow2(acc.c[q], MINV);
+    a.next[(uint64_t)q * nn + b] = acc.c[q];
+  }
+  if (a.leaves) {
+    kc::LaneSponge sp;
+    sp.init();
+    sp.lane(a.leaf_arity0);
+    sp.lane(0xFFFFFFFFull);
+    sp.lane(b);
+    sp.lane(a.leaf_label);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sp.lane(acc.c[q]);
+    uint64_t d[4];
+    sp.finish(d);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a.leaves[4 * b + i] = d[i];
+  }
+}
+
 template <int M>
 __global__ void fold_tuples_kernel(const uint64_t* tup, uint64_t nf, gl::Fp6 alpha, uint64_t* next) {
   const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -206,8 +331,17 @@ __global__ void fold_tuples_kernel(const uint64_t* tup, uint64_t nf, gl::Fp6 alp
 template <int M>
 cudaError_t ood_launch(const uint64_t* c, bool base, uint64_t n, const gl::Fp6& z, uint64_t* partials,
                        uint64_t* evals, cudaStream_t s) {
-  const uint64_t blocks = ood_blocks(n, M);
   const gl::Fp6 w = gl::e_pow(z, M);
+  if (n / M <= kOodSmallGroups) {
+    const gl::Fp6 w32 = gl::e_pow(w, 32);
+    SG_LAUNCH_SCOPE("stir_ood", s);
+    if (base)
+      ood_small_kernel<M, true><<<1, M * 32, 0, s>>>(c, n, w, w32, z, evals);
+    else
+      ood_small_kernel<M, false><<<1, M * 32, 0, s>>>(c, n, w, w32, z, evals);
+    return cudaGetLastError();
+  }
+  const uint64_t blocks = ood_blocks(n, M);
   const gl::Fp6 ws = gl::e_pow(w, blocks * kOodThreads);
   {
     SG_LAUNCH_SCOPE("stir_ood", s);
@@ -227,10 +361,16 @@ cudaError_t fold_launch(const FoldArgs& a, cudaStream_t s) {
   const unsigned T = 128;
   const unsigned blocks = (unsigned)((nn + T - 1) / T);
   SG_LAUNCH_SCOPE("stir_fold", s);
-  if (a.base)
+  if (nn <= kFoldSmall) {
+    if (a.base)
+      fold_small_kernel<M, true><<<blocks, T, 0, s>>>(a);
+    else
+      fold_small_kernel<M, false><<<blocks, T, 0, s>>>(a);
+  } else if (a.base) {
     fold_kernel<M, true><<<blocks, T, 0, s>>>(a);
-  else
+  } else {
     fold_kernel<M, false><<<blocks, T, 0, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
