@@ -282,6 +282,61 @@ int sg_merge_rsa2048(sg_ctx* ctx, const uint64_t* lde, size_t n_records, size_t 
 int sg_prove_rsa2048(sg_ctx* ctx, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, size_t n_records,
                      const uint8_t pi[32], uint8_t* proof, size_t cap, size_t* len);
 
+/* ---------------------------------------------------------------- P-256 ECDSA signature checks
+ * ECDSA-P256 (DNSSEC algorithm 13) proved as the double-chain scalar
+ * multiplication AIR of deep_ali/src/p256_ecdsa_double_multirow_air.rs: each row
+ * carries one step of chain A (u1·G) and one of chain B (u2·Q), a step being a
+ * group double, an add of the chain's base point and a select on the row's bit
+ * (p256_scalar_mul_air.rs, p256_group_air.rs), all written as field gadgets over
+ * 10 limbs of 26 bits (p256_field_air.rs). 151,334 cells and 155,774 constraints
+ * per row; the last row binds each chain's output to constant r_proj columns.
+ * Coordinates, scalars and digests are 32-byte big-endian; bits are bytes 0/1. */
+
+/* The row layout as a gadget table in constraint order (8 u32 per gadget:
+ * kind 1 mul, 2 add, 3 sub, 4 freeze, 5 select, then its cell bases), and the 18
+ * tail bases (chain A accumulator x,y,z, A output x,y,z, the same for B, r_proj
+ * A x,y,z and B x,y,z). table may be NULL; cap is in gadgets. */
+int sg_p256_layout(uint32_t* width, uint32_t* n_gadgets, uint32_t* n_constraints, uint32_t* table, size_t cap,
+                   uint32_t tail[18]);
+/* u1 = e s^-1, u2 = r s^-1 mod n (e = digest mod n) as MSB-first bits, the
+ * chains' inputs (prove_ecdsa_record_v1.rs:97-118). SG_EINVAL unless 1 <= r, s < n. */
+int sg_p256_u_bits(const uint8_t digest[32], const uint8_t r[32], const uint8_t s[32], uint8_t u1[256],
+                   uint8_t u2[256]);
+/* pi_hash SHA3-256("ECDSA-V1-PI-PRE" || qx || qy || r || s || digest)
+ * (prove_ecdsa_record_v1.rs:213-222). */
+int sg_p256_ecdsa_pi(const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32], const uint8_t s[32],
+                     const uint8_t digest[32], uint8_t out[32]);
+/* fill_ecdsa_double_multirow (p256_ecdsa_double_multirow_air.rs:134-234) on the
+ * host: chain A starts at (ax, ay, 1) and takes a_bits, chain B at (bx, by, 1)
+ * with b_bits, one bit per row, k rows (a power of 2, 2..65536); the r_proj
+ * columns hold the chains' final points. width x k column-major into `trace`
+ * (cap in elements). SG_EINVAL for a coordinate >= p or a point off the curve. */
+int sg_p256_chain_trace(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits, const uint8_t bx[32],
+                        const uint8_t by[32], const uint8_t* b_bits, size_t k, uint64_t* trace, size_t cap);
+/* The same trace with the cells expanded on the device from per-row gadget
+ * witnesses (15 MB for k = 256 instead of the 310 MB trace); host or device output. */
+int sg_p256_chain_trace_gpu(sg_ctx* ctx, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
+                            const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, size_t k,
+                            uint64_t* trace, size_t cap);
+/* deep_ali_merge_ecdsa_double_multirow_streaming: Phi_i = sum_j (j + 1) C_j at every
+ * point of a (151,334 x n_trace*blowup) LDE (always evaluated), then iFFT,
+ * poly_div_zh, FFT -> c_eval. lde: host or device. */
+int sg_merge_p256_ecdsa(sg_ctx* ctx, const uint64_t* lde, size_t n_trace, size_t blowup, uint64_t* c_eval);
+/* Proof of two chains of k rows: trace -> LDE x32 -> merge -> STIR with
+ * build_params(32 k, pi), self-verified. */
+int sg_prove_p256_chains(sg_ctx* ctx, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
+                         const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, size_t k,
+                         const uint8_t pi[32], uint8_t* proof, size_t cap, size_t* len);
+/* prove_ecdsa_record_v1.rs:97-240: u1/u2 from (digest, r, s), chain A = u1 bits
+ * from G, chain B = u2 bits from the public key Q, K = 256 rows, blowup 32
+ * (n0 = 8192, 9.9 GB LDE on the device), STIR with build_params(8192, pi),
+ * self-verified. The reference checks the signature natively before proving
+ * and finishes the verification (R = chain outputs combined, x(R) = r mod n)
+ * natively; the caller does both here. */
+int sg_prove_p256_ecdsa(sg_ctx* ctx, const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32],
+                        const uint8_t s[32], const uint8_t digest[32], const uint8_t pi[32], uint8_t* proof,
+                        size_t cap, size_t* len);
+
 /* ---------------------------------------------------------------- DNS shards
  * The steps either side of the prover in swarm-dns. Records are passed in
  * canonical form (DnsRecord::canonical_bytes, swarm-dns/src/dns.rs:43-54):

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "air.hpp"
+#include "p256_air.hpp"
 #include "rsa2048_air.hpp"
 #include "chacha.hpp"
 #include "gl.hpp"
@@ -1285,6 +1286,70 @@ int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const
   std::vector<uint64_t> lde(w * n0), c(n0);
   if (orc_lde(trace, w, n_trace, blowup, 1, lde.data()) != 0) return -2;
   if (orc_merge_rsa(lde.data(), n_records, n_trace, blowup, c.data()) != 0) return -2;
+  orc_fri_params p;
+  orc_build_params(n0, pi, 1, &p);
+  return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
+}
+
+// ------------------------------------------------------------------ P-256 ECDSA double chain
+// The row is described by a gadget table (8 u64 per gadget, in constraint order)
+// and an 18-entry tail of chain bases (see p256_air.hpp).
+size_t p256_constraints(const uint64_t* table, size_t n_gadgets) {
+  size_t k = 180;
+  for (size_t g = 0; g < n_gadgets; ++g) k += p256::gadget_constraints(table[g * p256::REC]);
+  return k;
+}
+
+int orc_p256_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_trace, const uint64_t* table,
+                  size_t n_gadgets, const uint64_t* tail, uint64_t* out) {
+  Fp* o = (Fp*)out;
+  for (size_t g = 0; g < n_gadgets; ++g) p256::eval_gadget((const Fp*)cur, table + g * p256::REC, o);
+  p256::eval_tail((const Fp*)cur, (const Fp*)nxt, tail, row, n_trace, o);
+  return (int)(o - (Fp*)out);
+}
+
+// deep_ali_merge_ecdsa_double_multirow_streaming: lambda_j = j + 1 over the row's
+// constraints, Phi always evaluated, then iFFT, poly_div_zh, FFT.
+int orc_merge_p256(const uint64_t* lde, size_t width, const uint64_t* table, size_t n_gadgets,
+                   const uint64_t* tail, size_t n_trace, size_t blowup, uint64_t* c_eval) {
+  if (n_trace == 0 || (n_trace & (n_trace - 1)) || blowup == 0 || (blowup & (blowup - 1))) return -2;
+  const size_t n = n_trace * blowup, k = p256_constraints(table, n_gadgets);
+  const Fp* L = (const Fp*)lde;
+  std::vector<Fp> phi(n);
+#pragma omp parallel
+  {
+    std::vector<Fp> cur(width), nxt(width), cv(k);
+#pragma omp for schedule(dynamic, 4)
+    for (long i = 0; i < (long)n; ++i) {
+      const size_t ni = (i + blowup) % n;
+      for (size_t c = 0; c < width; ++c) {
+        cur[c] = L[c * n + i];
+        nxt[c] = L[c * n + ni];
+      }
+      orc_p256_eval((const uint64_t*)cur.data(), (const uint64_t*)nxt.data(), i / blowup, n_trace, table, n_gadgets,
+                    tail, (uint64_t*)cv.data());
+      Fp acc;
+      for (size_t j = 0; j < k; ++j) acc = acc + Fp(j + 1) * cv[j];
+      phi[i] = acc;
+    }
+  }
+  ifft(phi.data(), n);
+  std::vector<Fp> q = poly_div_zh(phi, n_trace);
+  q.resize(n);
+  fft(q.data(), n);
+  memcpy(c_eval, q.data(), n * 8);
+  return 0;
+}
+
+// prove_ecdsa_record_v1.rs:193-240: trace -> LDE x32 (shift 1) -> merge -> STIR with
+// build_params(n0, pi).
+int orc_prove_p256(const uint64_t* trace, size_t width, const uint64_t* table, size_t n_gadgets,
+                   const uint64_t* tail, size_t n_trace, const uint8_t pi[32], uint8_t* out, size_t cap,
+                   size_t* out_len) {
+  const size_t blowup = 32, n0 = n_trace * blowup;
+  std::vector<uint64_t> lde(width * n0), c(n0);
+  if (orc_lde(trace, width, n_trace, blowup, 1, lde.data()) != 0) return -2;
+  if (orc_merge_p256(lde.data(), width, table, n_gadgets, tail, n_trace, blowup, c.data()) != 0) return -2;
   orc_fri_params p;
   orc_build_params(n0, pi, 1, &p);
   return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);

@@ -86,6 +86,16 @@ int orc_rsa_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_
 int orc_merge_rsa(const uint64_t* lde, size_t n_records, size_t n_trace, size_t blowup, uint64_t* c_eval);
 int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const uint8_t pi[32], uint8_t* out,
                   size_t cap, size_t* out_len);
+/* P-256 ECDSA double-chain AIR (p256_ecdsa_double_multirow_air.rs): the row is a
+ * gadget table (8 u64 per gadget, constraint order) plus an 18-entry tail of chain
+ * bases. orc_p256_eval returns the number of constraint values written. */
+int orc_p256_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_trace, const uint64_t* table,
+                  size_t n_gadgets, const uint64_t* tail, uint64_t* out);
+int orc_merge_p256(const uint64_t* lde, size_t width, const uint64_t* table, size_t n_gadgets,
+                   const uint64_t* tail, size_t n_trace, size_t blowup, uint64_t* c_eval);
+int orc_prove_p256(const uint64_t* trace, size_t width, const uint64_t* table, size_t n_gadgets,
+                   const uint64_t* tail, size_t n_trace, const uint8_t pi[32], uint8_t* out, size_t cap,
+                   size_t* out_len);
 void orc_build_params(size_t n0, const uint8_t pi[32], int stir, orc_fri_params* out);
 int orc_stir_prove(const uint64_t* f0, size_t n0, const orc_fri_params* p, uint8_t* out, size_t cap, size_t* len);
 int orc_stir_verify(const uint8_t* proof, size_t len, const orc_fri_params* p);

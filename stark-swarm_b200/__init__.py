@@ -110,6 +110,8 @@ EXPORTS = (
     "sg_prove_inner_shard", "sg_prove_outer_rollup",
     "sg_rsa2048_em", "sg_rsa2048_verify", "sg_rsa2048_pi_record", "sg_rsa2048_pi_stacked", "sg_rsa2048_trace",
     "sg_rsa2048_trace_gpu", "sg_merge_rsa2048", "sg_prove_rsa2048",
+    "sg_p256_layout", "sg_p256_u_bits", "sg_p256_ecdsa_pi", "sg_p256_chain_trace", "sg_p256_chain_trace_gpu",
+    "sg_merge_p256_ecdsa", "sg_prove_p256_chains", "sg_prove_p256_ecdsa",
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
@@ -206,6 +208,15 @@ def lib():
     L.sg_merge_rsa2048.argtypes = [vp, vp, sz, sz, sz, vp]
     L.sg_prove_rsa2048.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, sz, ctypes.c_char_p,
                                    ctypes.c_char_p, sz, ctypes.POINTER(sz)]
+    cp = ctypes.c_char_p
+    L.sg_p256_layout.argtypes = [ctypes.POINTER(ctypes.c_uint32)] * 3 + [vp, sz, vp]
+    L.sg_p256_u_bits.argtypes = [cp, cp, cp, cp, cp]
+    L.sg_p256_ecdsa_pi.argtypes = [cp, cp, cp, cp, cp, cp]
+    L.sg_p256_chain_trace.argtypes = [cp, cp, cp, cp, cp, cp, sz, vp, sz]
+    L.sg_p256_chain_trace_gpu.argtypes = [vp] + L.sg_p256_chain_trace.argtypes
+    L.sg_merge_p256_ecdsa.argtypes = [vp, vp, sz, sz, vp]
+    L.sg_prove_p256_chains.argtypes = [vp, cp, cp, cp, cp, cp, cp, sz, cp, cp, sz, ctypes.POINTER(sz)]
+    L.sg_prove_p256_ecdsa.argtypes = [vp, cp, cp, cp, cp, cp, cp, cp, sz, ctypes.POINTER(sz)]
     L.sg_merge_sha512.argtypes = L.sg_merge_sha256.argtypes
     L.sg_sha512_trace.argtypes = L.sg_sha256_trace.argtypes
     L.sg_sha512_trace_gpu.argtypes = L.sg_sha256_trace_gpu.argtypes
@@ -387,6 +398,69 @@ def rsa2048_trace(records) -> np.ndarray:
     if rc != SG_OK:
         raise StarkGpuError(rc, "sg_rsa2048_trace failed")
     return out.reshape(len(records) * RSA_WIDTH, RSA_N_TRACE)
+
+
+P256_BLOWUP = 32
+
+
+def _be32(x) -> bytes:
+    if isinstance(x, int):
+        return x.to_bytes(32, "big")
+    b = bytes(x)
+    if len(b) != 32:
+        raise ValueError("P-256 values are 32-byte big-endian strings")
+    return b
+
+
+def _bits(bits) -> bytes:
+    return bytes(1 if b else 0 for b in bits)
+
+
+def p256_layout():
+    """-> (width, constraints per row, (n_gadgets, 8) uint32 table, 18 tail bases)."""
+    L = lib()
+    w, g, k = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    rc = L.sg_p256_layout(ctypes.byref(w), ctypes.byref(g), ctypes.byref(k), None, 0, None)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_p256_layout failed")
+    table = np.zeros((g.value, 8), dtype=np.uint32)
+    tail = np.zeros(18, dtype=np.uint32)
+    rc = L.sg_p256_layout(ctypes.byref(w), ctypes.byref(g), ctypes.byref(k), table.ctypes.data, g.value,
+                          tail.ctypes.data)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_p256_layout failed")
+    return w.value, k.value, table, tail
+
+
+def p256_u_bits(digest: bytes, r, s):
+    """u1 = e s^-1, u2 = r s^-1 mod n as MSB-first bit lists (prove_ecdsa_record_v1.rs:97-118)."""
+    u1, u2 = ctypes.create_string_buffer(256), ctypes.create_string_buffer(256)
+    rc = lib().sg_p256_u_bits(_be32(digest), _be32(r), _be32(s), u1, u2)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_p256_u_bits failed")
+    return list(u1.raw), list(u2.raw)
+
+
+def p256_ecdsa_pi(qx, qy, r, s, digest: bytes) -> bytes:
+    """pi_hash of prove_ecdsa_record_v1.rs:213-222."""
+    out = ctypes.create_string_buffer(32)
+    rc = lib().sg_p256_ecdsa_pi(_be32(qx), _be32(qy), _be32(r), _be32(s), _be32(digest), out)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_p256_ecdsa_pi failed")
+    return out.raw
+
+
+def p256_chain_trace(a_point, a_bits, b_point, b_bits) -> np.ndarray:
+    """fill_ecdsa_double_multirow on the host: chains from (x, y, 1) of two affine
+    points, one bit per row -> (151334, len(bits)) uint64."""
+    k = len(a_bits)
+    width = p256_layout()[0]
+    out = np.empty(width * k, dtype=np.uint64)
+    rc = lib().sg_p256_chain_trace(_be32(a_point[0]), _be32(a_point[1]), _bits(a_bits), _be32(b_point[0]),
+                                   _be32(b_point[1]), _bits(b_bits), k, out.ctypes.data, out.size)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_p256_chain_trace failed")
+    return out.reshape(width, k)
 
 
 def _records(records):
@@ -674,6 +748,59 @@ class Context:
             arr, buf = _out_buffer(cap)
             ln = ctypes.c_size_t()
             rc = self._lib.sg_prove_rsa2048(self._h, ns, ss, es, len(records), pi, buf, cap, ctypes.byref(ln))
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return arr[:ln.value].tobytes()
+
+    def p256_chain_trace(self, a_point, a_bits, b_point, b_bits, out=None):
+        """The double-chain trace with the cells expanded on the GPU -> (151334, len(bits))."""
+        k = len(a_bits)
+        width = p256_layout()[0]
+        host = out is None
+        if host:
+            out = np.empty(width * k, dtype=np.uint64)
+        op, _k, _ = _addr(out)
+        self._check(self._lib.sg_p256_chain_trace_gpu(self._h, _be32(a_point[0]), _be32(a_point[1]), _bits(a_bits),
+                                                      _be32(b_point[0]), _be32(b_point[1]), _bits(b_bits), k, op,
+                                                      width * k))
+        return out.reshape(width, k) if host else out
+
+    def merge_p256_ecdsa(self, lde, n_trace: int, blowup: int = P256_BLOWUP, out=None):
+        """deep_ali_merge_ecdsa_double_multirow_streaming on a (151334, n_trace * blowup) LDE -> c_eval."""
+        ip, _ki, is_np = _addr(lde)
+        if out is None:
+            if not is_np:
+                raise ValueError("device input needs an explicit out buffer")
+            out = np.empty(n_trace * blowup, dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        self._check(self._lib.sg_merge_p256_ecdsa(self._h, ip, n_trace, blowup, op))
+        return out
+
+    def prove_p256_chains(self, a_point, a_bits, b_point, b_bits, pi: bytes) -> bytes:
+        """Proof of two chains of len(bits) rows (LDE x32, STIR); self-verified."""
+        cap = _PROOF_CAP
+        while True:
+            arr, buf = _out_buffer(cap)
+            ln = ctypes.c_size_t()
+            rc = self._lib.sg_prove_p256_chains(self._h, _be32(a_point[0]), _be32(a_point[1]), _bits(a_bits),
+                                                _be32(b_point[0]), _be32(b_point[1]), _bits(b_bits), len(a_bits),
+                                                pi, buf, cap, ctypes.byref(ln))
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return arr[:ln.value].tobytes()
+
+    def prove_p256_ecdsa(self, q, r, s, digest: bytes, pi: bytes) -> bytes:
+        """ECDSA-P256 signature-check proof (prove_ecdsa_record_v1.rs: K = 256, n0 = 8192); self-verified."""
+        cap = _PROOF_CAP
+        while True:
+            arr, buf = _out_buffer(cap)
+            ln = ctypes.c_size_t()
+            rc = self._lib.sg_prove_p256_ecdsa(self._h, _be32(q[0]), _be32(q[1]), _be32(r), _be32(s), _be32(digest),
+                                               pi, buf, cap, ctypes.byref(ln))
             if rc == SG_ESPACE:
                 cap = ln.value
                 continue

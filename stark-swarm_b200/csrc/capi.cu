@@ -6,6 +6,8 @@
 #include "dns.hpp"
 #include "merge.cuh"
 #include "merkle.cuh"
+#include "p256.hpp"
+#include "p256_prover.hpp"
 #include "prover.hpp"
 #include "rsa_air.cuh"
 #include "sha256_air.cuh"
@@ -440,6 +442,110 @@ int sg_prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const 
     std::vector<uint8_t> b = sg::prove_rsa2048(c, n_be, s_be, em_be, n_records, pi, true);
     *len = b.size();
     if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_rsa2048: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+// ------------------------------------------------------------------ P-256 ECDSA
+int sg_p256_layout(uint32_t* width, uint32_t* n_gadgets, uint32_t* n_constraints, uint32_t* table, size_t cap,
+                   uint32_t tail[18]) {
+  if (!width || !n_gadgets || !n_constraints) return SG_EINVAL;
+  try {
+    const sg::p256::Layout& L = sg::p256::layout();
+    *width = L.width;
+    *n_gadgets = (uint32_t)L.table.size();
+    *n_constraints = L.n_constraints;
+    if (tail) memcpy(tail, L.tail, sizeof L.tail);
+    if (table) {
+      if (cap < L.table.size()) return SG_ESPACE;
+      memcpy(table, L.table.data(), L.table.size() * sizeof(sg::p256::Gadget));
+    }
+    return SG_OK;
+  } catch (const sg::SgError& e) {
+    return e.code;
+  }
+}
+
+int sg_p256_u_bits(const uint8_t digest[32], const uint8_t r[32], const uint8_t s[32], uint8_t u1[256],
+                   uint8_t u2[256]) {
+  if (!digest || !r || !s || !u1 || !u2) return SG_EINVAL;
+  try {
+    sg::p256::u_bits(digest, r, s, u1, u2);
+    return SG_OK;
+  } catch (const sg::SgError& e) {
+    return e.code;
+  }
+}
+
+int sg_p256_ecdsa_pi(const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32], const uint8_t s[32],
+                     const uint8_t digest[32], uint8_t out[32]) {
+  if (!qx || !qy || !r || !s || !digest || !out) return SG_EINVAL;
+  sg::p256::pi_hash(qx, qy, r, s, digest, out);
+  return SG_OK;
+}
+
+int sg_p256_chain_trace(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits, const uint8_t bx[32],
+                        const uint8_t by[32], const uint8_t* b_bits, size_t k, uint64_t* trace, size_t cap) {
+  if (!ax || !ay || !a_bits || !bx || !by || !b_bits || k < 2 || (k & (k - 1)) || k > 65536) return SG_EINVAL;
+  try {
+    std::vector<sg::p256::RowW> rows;
+    std::vector<sg::p256::GadgetW> gw;
+    uint32_t rproj[6][sg::p256::NL];
+    sg::p256::chain_witness(ax, ay, a_bits, bx, by, b_bits, k, &rows, &gw, rproj);
+    if (!trace || (uint64_t)sg::p256::layout().width * k > cap) return SG_ESPACE;
+    sg::p256::expand_host(rows.data(), gw.data(), rproj, k, trace);
+    return SG_OK;
+  } catch (const sg::SgError& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return SG_ENOMEM;
+  }
+}
+
+int sg_p256_chain_trace_gpu(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
+                            const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, size_t k,
+                            uint64_t* trace, size_t cap) {
+  return guarded(c, [&] {
+    sg::require(ax && ay && a_bits && bx && by && b_bits, "p256_chain_trace_gpu: null argument");
+    const uint64_t cells = (uint64_t)sg::p256::layout().width * k;
+    if (!trace || cells > cap) throw sg::SgError{SG_ESPACE, "p256_chain_trace_gpu: trace buffer too small"};
+    Out dout(trace, cells, c->stream);
+    sg::p256_trace_device(c, ax, ay, a_bits, bx, by, b_bits, k, dout.d);
+    dout.finish();
+  });
+}
+
+int sg_merge_p256_ecdsa(sg_ctx* c, const uint64_t* lde, size_t n_trace, size_t blowup, uint64_t* c_eval) {
+  return guarded(c, [&] {
+    sg::require(lde && c_eval && n_trace >= 2 && blowup >= 1, "merge_p256_ecdsa: bad argument");
+    const size_t n = n_trace * blowup;
+    In di(lde, (size_t)sg::p256::layout().width * n, c->stream);
+    Out dout(c_eval, n, c->stream);
+    sg::p256_merge_device(c, di.d, n_trace, blowup, dout.d);
+    dout.finish();
+  });
+}
+
+int sg_prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
+                         const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, size_t k,
+                         const uint8_t pi[32], uint8_t* proof, size_t cap, size_t* len) {
+  return guarded(c, [&] {
+    sg::require(ax && ay && a_bits && bx && by && b_bits && pi && len, "prove_p256_chains: null argument");
+    std::vector<uint8_t> b = sg::prove_p256_chains(c, ax, ay, a_bits, bx, by, b_bits, k, pi, true);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_p256_chains: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+int sg_prove_p256_ecdsa(sg_ctx* c, const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32],
+                        const uint8_t s[32], const uint8_t digest[32], const uint8_t pi[32], uint8_t* proof,
+                        size_t cap, size_t* len) {
+  return guarded(c, [&] {
+    sg::require(qx && qy && r && s && digest && pi && len, "prove_p256_ecdsa: null argument");
+    std::vector<uint8_t> b = sg::prove_p256_ecdsa(c, qx, qy, r, s, digest, pi, true);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_p256_ecdsa: proof buffer too small"};
     memcpy(proof, b.data(), b.size());
   });
 }

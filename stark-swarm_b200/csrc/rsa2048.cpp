@@ -1,16 +1,11 @@
 // rsa2048.cpp — host side of the RSA-2048 AIR: big-integer witness, EM encoding,
-// pi_hash recipes, host trace expansion.
-//
-// Big integers are little-endian arrays of 32-bit words. The product a * b of
-// two 2048-bit values is schoolbook; its division by n is Knuth's Algorithm D
-// (TAOCP vol. 2, 4.3.1): normalise so the divisor's top word has its high bit
-// set, estimate each quotient word from the top two dividend words and the top
-// divisor word, correct the estimate with the second divisor word, multiply and
-// subtract, and add back in the rare case the estimate was still one too large.
+// pi_hash recipes, host trace expansion. Big integers are little-endian arrays of
+// 32-bit words (bigint.hpp: schoolbook product, Knuth division).
 #include "rsa2048.hpp"
 
 #include <cstring>
 
+#include "bigint.hpp"
 #include "context.hpp"
 #include "keccak.cuh"
 #include "sha256_air.cuh"
@@ -28,88 +23,6 @@ void from_be(const uint8_t* b, uint32_t* w) {  // 256 bytes -> 64 words
   }
 }
 
-int top_word(const uint32_t* w, int n) {  // index of the highest non-zero word, -1 for zero
-  for (int i = n - 1; i >= 0; --i)
-    if (w[i]) return i;
-  return -1;
-}
-
-int cmp(const uint32_t* a, const uint32_t* b, int n) {
-  for (int i = n - 1; i >= 0; --i)
-    if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
-  return 0;
-}
-
-void mul(const uint32_t* a, const uint32_t* b, uint32_t* out) {  // 64 x 64 -> 128 words
-  memset(out, 0, 2 * W * 4);
-  for (int i = 0; i < W; ++i) {
-    uint64_t carry = 0;
-    for (int j = 0; j < W; ++j) {
-      const uint64_t t = (uint64_t)a[i] * b[j] + out[i + j] + carry;
-      out[i + j] = (uint32_t)t;
-      carry = t >> 32;
-    }
-    out[i + W] = (uint32_t)carry;
-  }
-}
-
-// u (m words) = q * v + r with v of n significant words (n >= 1, v[n-1] != 0);
-// q gets m - n + 1 words, r gets n words.
-void divmod(const uint32_t* u, int m, const uint32_t* v, int n, uint32_t* q, uint32_t* r) {
-  if (n == 1) {
-    uint64_t rem = 0;
-    for (int i = m - 1; i >= 0; --i) {
-      const uint64_t cur = rem << 32 | u[i];
-      q[i] = (uint32_t)(cur / v[0]);
-      rem = cur % v[0];
-    }
-    r[0] = (uint32_t)rem;
-    return;
-  }
-  // normalise: shift so the divisor's top bit is set
-  const int s = __builtin_clz(v[n - 1]);
-  std::vector<uint32_t> vn(n), un(m + 1);
-  for (int i = n - 1; i > 0; --i) vn[i] = s ? (v[i] << s | v[i - 1] >> (32 - s)) : v[i];
-  vn[0] = v[0] << s;
-  un[m] = s ? u[m - 1] >> (32 - s) : 0;
-  for (int i = m - 1; i > 0; --i) un[i] = s ? (u[i] << s | u[i - 1] >> (32 - s)) : u[i];
-  un[0] = u[0] << s;
-  const uint64_t B = 1ull << 32;
-  for (int j = m - n; j >= 0; --j) {
-    const uint64_t top = (uint64_t)un[j + n] << 32 | un[j + n - 1];
-    uint64_t qh = top / vn[n - 1], rh = top % vn[n - 1];
-    while (qh >= B || qh * vn[n - 2] > (rh << 32 | un[j + n - 2])) {
-      --qh;
-      rh += vn[n - 1];
-      if (rh >= B) break;
-    }
-    // un[j .. j+n] -= qh * vn
-    int64_t borrow = 0;
-    uint64_t carry = 0;
-    for (int i = 0; i < n; ++i) {
-      const uint64_t p = qh * vn[i] + carry;
-      carry = p >> 32;
-      const int64_t t = (int64_t)un[i + j] - (int64_t)(uint32_t)p + borrow;
-      un[i + j] = (uint32_t)t;
-      borrow = t >> 32;  // 0 or -1
-    }
-    int64_t t = (int64_t)un[j + n] - (int64_t)carry + borrow;
-    un[j + n] = (uint32_t)t;
-    if (t < 0) {  // estimate one too large: add the divisor back
-      --qh;
-      uint64_t c = 0;
-      for (int i = 0; i < n; ++i) {
-        const uint64_t s2 = (uint64_t)un[i + j] + vn[i] + c;
-        un[i + j] = (uint32_t)s2;
-        c = s2 >> 32;
-      }
-      un[j + n] += (uint32_t)c;
-    }
-    q[j] = (uint32_t)qh;
-  }
-  for (int i = 0; i < n; ++i) r[i] = s ? (un[i] >> s | un[i + 1] << (32 - s)) : un[i];
-}
-
 // biguint_to_limbs80 (rsa2048_field_air.rs:190-210): 26-bit limbs, least significant first.
 void limbs26(const uint32_t* w, int nw, uint32_t out[LIMBS]) {
   for (uint32_t i = 0; i < LIMBS; ++i) {
@@ -124,12 +37,12 @@ void limbs26(const uint32_t* w, int nw, uint32_t out[LIMBS]) {
 // slot identities (fill_rsa_mul_gadget, rsa2048_field_air.rs:241-326).
 void mul_gadget(const uint32_t* a, const uint32_t* b, const uint32_t* n, int nn, RowW* row, uint32_t* c_words) {
   uint32_t prod[2 * W], qw[2 * W] = {0}, rw[W] = {0};
-  mul(a, b, prod);
-  const int m = top_word(prod, 2 * W) + 1;
+  bn::mul(a, W, b, W, prod);
+  const int m = bn::top_word(prod, 2 * W) + 1;
   if (m < nn) {  // product below n: q = 0, c = product
     memcpy(rw, prod, 4 * (m > 0 ? m : 0));
   } else {
-    divmod(prod, m, n, nn, qw, rw);
+    bn::divmod(prod, m, n, nn, qw, rw);
   }
   memcpy(c_words, rw, 4 * W);
   uint32_t al[LIMBS], bl[LIMBS], nl[LIMBS];
@@ -185,9 +98,9 @@ void witness(const uint8_t n_be[256], const uint8_t s_be[256], const uint8_t em_
   from_be(n_be, n);
   from_be(s_be, s);
   from_be(em_be, em);
-  const int nn = top_word(n, W) + 1;
+  const int nn = bn::top_word(n, W) + 1;
   require(nn >= 1 && !(nn == 1 && n[0] < 2), "rsa: modulus must be > 1");
-  require(cmp(s, n, W) < 0, "rsa: signature value must be below the modulus");
+  require(bn::cmp(s, n, W) < 0, "rsa: signature value must be below the modulus");
   limbs26(s, W, rec->s);
   limbs26(n, W, rec->n);
   limbs26(em, W, rec->em);
@@ -207,9 +120,9 @@ bool verify_native(const uint8_t n_be[256], const uint8_t s_be[256], const uint8
   from_be(n_be, n);
   from_be(s_be, s);
   from_be(em_be, em);
-  const int nn = top_word(n, W) + 1;
-  if (nn < 1 || (nn == 1 && n[0] < 2) || cmp(s, n, W) >= 0) return false;
-  if (top_word(s, W) < 0) return false;  // rsa2048.rs:100-103 rejects s = 0
+  const int nn = bn::top_word(n, W) + 1;
+  if (nn < 1 || (nn == 1 && n[0] < 2) || bn::cmp(s, n, W) >= 0) return false;
+  if (bn::top_word(s, W) < 0) return false;  // rsa2048.rs:100-103 rejects s = 0
   RecordW rec;
   std::vector<RowW> rows(N_TRACE);
   witness(n_be, s_be, em_be, &rec, rows.data());
