@@ -151,6 +151,12 @@ def load_oracle():
     return oracle_lib
 
 
+def load_oracle_p256():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_p256
+    return oracle_p256
+
+
 def load_oracle_rsa():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_rsa
@@ -318,27 +324,116 @@ def rsa2048(sg, ctx, n_jobs, stacked, cpu_threads):
     return out
 
 
+# P-256 test signatures (affine arithmetic over p; test data only)
+P256_P = 0xFFFFFFFF00000001000000000000000000000000FFFFFFFFFFFFFFFFFFFFFFFF
+P256_N = 0xFFFFFFFF00000000FFFFFFFFFFFFFFFFBCE6FAADA7179E84F3B9CAC2FC632551
+P256_G = (0x6B17D1F2E12C4247F8BCE6E563A440F277037D812DEB33A0F4A13945D898C296,
+          0x4FE342E2FE1A7F9B8EE7EB4A7C0F9E162BCE33576B315ECECBB6406837BF51F5)
+
+
+def _p256_add(a, b):
+    if a is None:
+        return b
+    if b is None:
+        return a
+    if a[0] == b[0] and (a[1] + b[1]) % P256_P == 0:
+        return None
+    if a == b:
+        lam = (3 * a[0] * a[0] - 3) * pow(2 * a[1], -1, P256_P) % P256_P
+    else:
+        lam = (b[1] - a[1]) * pow(b[0] - a[0], -1, P256_P) % P256_P
+    x = (lam * lam - a[0] - b[0]) % P256_P
+    return x, (lam * (a[0] - x) - a[1]) % P256_P
+
+
+def _p256_mul(k, pt):
+    acc = None
+    for bit in bin(k)[2:]:
+        acc = _p256_add(acc, acc)
+        if bit == "1":
+            acc = _p256_add(acc, pt)
+    return acc
+
+
+def ecdsa_job(sg, i):
+    """(q, r, s, digest) of a seeded ECDSA-P256 / SHA-256 signature, and its pi_hash."""
+    rng = np.random.default_rng(1000 + i)
+    d = int.from_bytes(rng.bytes(32), "big") % (P256_N - 1) + 1
+    k = int.from_bytes(rng.bytes(32), "big") % (P256_N - 1) + 1
+    q = _p256_mul(d, P256_G)
+    digest = hashlib.sha256(b"DNSSEC-RRSIG-V0|rec%05d.example.com.|A|10.0.0.1|alg-13" % i).digest()
+    e = int.from_bytes(digest, "big") % P256_N
+    r = _p256_mul(k, P256_G)[0] % P256_N
+    s = pow(k, -1, P256_N) * (e + r * d) % P256_N
+    return (q, r, s, digest), sg.p256_ecdsa_pi(q[0], q[1], r, s, digest)
+
+
+def p256_ecdsa(sg, ctx, n_jobs, cpu_threads):
+    """ECDSA-P256 signature-check proofs (prove_ecdsa_record_v1.rs: the double-chain
+    AIR, 256 rows of 151,334 cells and 155,774 constraints, blowup 32, n0 8192,
+    STIR [8,8,8,8,2]) one at a time vs 4 in flight; each job is host signature in,
+    proof bytes out, self-verified."""
+    jobs = [(sg.JOB_P256_ECDSA,) + ecdsa_job(sg, i) for i in range(n_jobs)]
+    ctx.prove_batch(jobs[:2], n_streams=2)
+    out = {"workload": "ECDSA-P256 signature-check proof (double-chain scalar-mult AIR, n_trace 256, 151334 cols, "
+                       "155774 constraints, blowup 32, n0 8192), self-verified", "jobs": n_jobs}
+    for label, streams in (("plain", 1), ("batched", 4)):
+        t0 = time.perf_counter()
+        res = ctx.prove_batch(jobs, n_streams=streams, hbm_budget_bytes=160 << 30)
+        dt = time.perf_counter() - t0
+        assert all(r.status == 0 for _, r in res)
+        lat = sorted(r.latency_ms for _, r in res)
+        out[label] = {"streams": streams, "proofs_per_s": n_jobs / dt, "p50_ms": lat[len(lat) // 2],
+                      "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
+    out["batched_over_plain"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
+    if cpu_threads:
+        E = load_oracle_p256()
+        O = load_oracle()
+        O.set_threads(cpu_threads)
+        (q, r, s, digest), pi = jobs[0][1], jobs[0][2]
+        u1, u2 = sg.p256_u_bits(digest, r, s)
+        k = 64  # the bounded sample: the first 64 bits of each chain (n0 = 2048)
+        t0 = time.perf_counter()
+        tr, lay = E.trace(E.G, u1[:k], q, u2[:k])
+        cpu_proof = E.prove(lay, tr, pi)
+        dt = time.perf_counter() - t0
+        assert cpu_proof == ctx.prove_p256_chains(E.G, u1[:k], q, u2[:k], pi), "GPU and oracle chain proofs differ"
+        scale = 256 // k
+        out["cpu_baseline"] = {"proofs_per_s": 1.0 / (dt * scale), "cores": cpu_threads, "kind": "port",
+                               "sample": f"oracle proof of the first {k} rows of both chains (n0 {k * 32}) took "
+                                         f"{dt:.2f} s, scaled by n0 (x{scale}: the merge, linear in n0, dominates)"}
+        out["plain_over_cpu"] = out["plain"]["proofs_per_s"] * dt * scale
+    return out
+
+
 def serving(sg, ctx, rates, n_jobs, streams, seed=7):
     """Poisson arrivals of proof requests admitted by the continuous-batching server
-    under a 160 GB HBM budget: 52 % SHA-256 record proofs and 20 % SHA-512 over
-    record-length messages (lognormal, median 120 B, clipped to 40-600 B), and 28 %
-    RSA-2048 signature checks; p50/p99 latency from submit to result, and
-    throughput against one proof at a time."""
+    under a 160 GB HBM budget: 40 % SHA-256 record proofs and 20 % SHA-512 over
+    record-length messages (lognormal, median 120 B, clipped to 40-600 B), 24 %
+    ECDSA-P256 and 16 % RSA-2048 signature checks (the record checks' 60/40
+    signature split); p50/p99 latency from submit to result, and throughput
+    against one proof at a time."""
     rng = np.random.default_rng(seed)
     lens = np.clip(np.round(rng.lognormal(np.log(120), 0.6, n_jobs)), 40, 600).astype(int)
     msgs = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in lens]
     u = rng.random(n_jobs)
-    kinds = [sg.JOB_SHA512 if x < 0.2 else sg.JOB_RSA2048 if x < 0.48 else sg.JOB_SHA256 for x in u]
+    kinds = [sg.JOB_SHA512 if x < 0.2 else sg.JOB_P256_ECDSA if x < 0.44 else sg.JOB_RSA2048 if x < 0.6
+             else sg.JOB_SHA256 for x in u]
     pis = [hashlib.sha3_256(b"serve-%d" % i).digest() for i in range(n_jobs)]
     keys = rsa_keys()
     for i in range(n_jobs):
         if kinds[i] == sg.JOB_RSA2048:
             rec, pis[i] = rsa_record(sg, msgs[i], keys[i % len(keys)])
             msgs[i] = [rec]
+        elif kinds[i] == sg.JOB_P256_ECDSA:
+            msgs[i], pis[i] = ecdsa_job(sg, 50000 + i)
 
     def prove_one(i):
         if kinds[i] == sg.JOB_RSA2048:
             return ctx.prove_rsa2048(msgs[i], pis[i])
+        if kinds[i] == sg.JOB_P256_ECDSA:
+            q, r, s, dg = msgs[i]
+            return ctx.prove_p256_ecdsa(q, r, s, dg, pis[i])
         f = ctx.prove_sha512 if kinds[i] == sg.JOB_SHA512 else ctx.prove_sha256
         return f(msgs[i], pis[i])[0]
 
@@ -347,8 +442,8 @@ def serving(sg, ctx, rates, n_jobs, streams, seed=7):
     for i in range(n_jobs):
         prove_one(i)
     plain = n_jobs / (time.perf_counter() - t0)
-    out = {"workload": "52 % SHA-256 and 20 % SHA-512 AIR proofs of messages lognormal(median 120 B) clipped "
-                       "40-600 B, 28 % RSA-2048 signature-check proofs; Poisson arrivals",
+    out = {"workload": "40 % SHA-256 and 20 % SHA-512 AIR proofs of messages lognormal(median 120 B) clipped "
+                       "40-600 B, 24 % ECDSA-P256 and 16 % RSA-2048 signature-check proofs; Poisson arrivals",
            "jobs_per_rate": n_jobs, "streams": streams, "hbm_budget_gb": 160, "plain_proofs_per_s": plain,
            "rates": []}
     for lam in rates:
@@ -402,6 +497,8 @@ def main():
     ap.add_argument("--rsa-jobs", type=int, default=256,
                     help="single-record RSA-2048 proofs for the plain-vs-batched section (0 skips it)")
     ap.add_argument("--rsa-stacked", type=int, default=64, help="records in the stacked RSA-2048 proof (0 skips)")
+    ap.add_argument("--ecdsa-jobs", type=int, default=32,
+                    help="ECDSA-P256 proofs for the plain-vs-batched section (0 skips it)")
     ap.add_argument("--serve-rates", default="50,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--no-classic-fri", dest="classic_fri", action="store_false",
                     help="skip the classic DEEP-FRI timing")
@@ -593,6 +690,7 @@ def main():
     cpu_threads = (os.cpu_count() or 1) if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else 0
     large = sha256_large(sg, ctx, args.sha256_large_blocks, 3, cpu_threads) if args.sha256_large_blocks > 0 else None
     rsa = rsa2048(sg, ctx, args.rsa_jobs, args.rsa_stacked, cpu_threads) if args.rsa_jobs > 0 else None
+    ecdsa = p256_ecdsa(sg, ctx, args.ecdsa_jobs, cpu_threads) if args.ecdsa_jobs > 0 else None
     serve = None
     if args.serve_jobs > 0:
         serve = serving(sg, ctx, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs, 16)
@@ -622,6 +720,7 @@ def main():
             "sha256_proofs": cfg1,
             "sha256_large_trace": large,
             "rsa2048": rsa,
+            "p256_ecdsa": ecdsa,
             "serving": serve,
             "classic_fri": classic,
             "proof_bytes": len(ref[1]),

@@ -384,6 +384,8 @@ int sg_prove_outer_rollup(sg_ctx* ctx, const uint8_t* pi_hashes, size_t n, const
 #define SG_JOB_SHA512 3      /* input = message bytes, input_len = bytes (sg_prove_sha512) */
 #define SG_JOB_RSA2048 4     /* input = records of n || s || em (256 bytes each, big-endian), input_len =
                                 768 * records (sg_prove_rsa2048; pi = public_inputs_hash) */
+#define SG_JOB_P256_ECDSA 5  /* input = qx || qy || r || s || digest (32 bytes each), input_len = 160
+                                (sg_prove_p256_ecdsa; pi = public_inputs_hash) */
 
 typedef struct {
   int32_t kind;

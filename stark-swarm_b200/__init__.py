@@ -116,7 +116,7 @@ EXPORTS = (
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
 )
-JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048 = 1, 2, 3, 4
+JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA = 1, 2, 3, 4, 5
 OPT_WIDE_MERGE = 1
 WIDE_MERGE_AUTO, WIDE_MERGE_LDE, WIDE_MERGE_COSETS = 0, 1, 2
 
@@ -919,7 +919,11 @@ def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
         data = b"".join(_be256(r[0]) + _be256(r[1]) + _be256(r[2]) for r in data)
         if not data:
             raise ValueError("an RSA job needs at least one record")
-    if kind in (JOB_SHA256, JOB_SHA512, JOB_RSA2048):
+    if kind == JOB_P256_ECDSA and not isinstance(data, (bytes, bytearray)):
+        # data: (q, r, s, digest) with q = (x, y), or the 160 packed bytes
+        q, r, s_, dg = data
+        data = _be32(q[0]) + _be32(q[1]) + _be32(r) + _be32(s_) + _be32(dg)
+    if kind in (JOB_SHA256, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA):
         buf = ctypes.create_string_buffer(bytes(data), max(1, len(data)))
         n = len(data)
     elif kind == JOB_HASH_ROLLUP:

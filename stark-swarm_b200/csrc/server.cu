@@ -20,6 +20,8 @@
 #include <vector>
 
 #include "context.hpp"
+#include "p256.hpp"
+#include "p256_prover.hpp"
 #include "prover.hpp"
 #include "rsa2048.hpp"
 #include "sha256_air.cuh"
@@ -60,6 +62,10 @@ uint64_t footprint_bytes(const sg_job& j) {
     const uint64_t blocks = (j.input_len + 17 + 127) / 128;
     const uint64_t nt = next_pow2(128 * blocks), n0 = nt * 32;
     return 8 * ((uint64_t)sg::sha512::WIDTH * (n0 + 2 * nt) + 16 * n0);
+  }
+  if (j.kind == SG_JOB_P256_ECDSA) {
+    // trace, LDE and the LDE transform's scratch at 151,334 columns, n0 = 8192
+    return 8ull * sg::p256::layout().width * (sg::p256::K_ECDSA + 2 * 8192) + (64ull << 20);
   }
   if (j.kind == SG_JOB_RSA2048) {
     const uint64_t recs = j.input_len / 768, w = recs * sg::rsa::WIDTH;
@@ -138,6 +144,9 @@ struct sg_server {
       } else if (e->kind == SG_JOB_SHA512) {
         e->proof = sg::prove_hash_message(c, sg::sha512_hash_air(), e->input.data(), e->input.size(), e->pi,
                                           e->phi_mode, true, e->digest);
+      } else if (e->kind == SG_JOB_P256_ECDSA) {
+        const uint8_t* in = e->input.data();
+        e->proof = sg::prove_p256_ecdsa(c, in, in + 32, in + 64, in + 96, in + 128, e->pi, true);
       } else if (e->kind == SG_JOB_RSA2048) {
         e->proof = prove_rsa_job(c, e->input, e->pi);
       } else {
@@ -198,8 +207,9 @@ void sg_server_destroy(sg_server* s) {
 int sg_server_submit(sg_server* s, const sg_job* job, uint64_t* ticket) {
   if (!s || !job || !ticket) return SG_EINVAL;
   if (job->kind != SG_JOB_SHA256 && job->kind != SG_JOB_SHA512 && job->kind != SG_JOB_HASH_ROLLUP &&
-      job->kind != SG_JOB_RSA2048)
+      job->kind != SG_JOB_RSA2048 && job->kind != SG_JOB_P256_ECDSA)
     return SG_EINVAL;
+  if (job->kind == SG_JOB_P256_ECDSA && job->input_len != 160) return SG_EINVAL;
   if (job->input_len && !job->input) return SG_EINVAL;
   if (job->kind == SG_JOB_RSA2048 && (job->input_len == 0 || job->input_len % 768)) return SG_EINVAL;
   Entry e;

@@ -2,7 +2,9 @@
 (SHA-256, SHA-512, HashRollup and RSA-2048 signature checks) is
 byte-identical to the same job proved alone (oracle), under several stream
 counts and an HBM budget tight enough to serialise admission; the server
-accepts submissions while earlier jobs are running."""
+accepts submissions while earlier jobs are running. ECDSA-P256 jobs, whose
+full-size proof is beyond the oracle's reach, match the same job proved alone
+on the GPU (that path is pinned to the oracle at smaller chain lengths)."""
 import hashlib
 import time
 
@@ -10,6 +12,7 @@ import numpy as np
 import pytest
 
 import oracle_lib as O
+import oracle_p256 as E
 import oracle_rsa as R
 
 pytestmark = pytest.mark.gpu
@@ -66,3 +69,36 @@ def test_server_admits_while_running(sgpu, ctx):
         for i, t in enumerate(tickets[1:], start=1):
             proof, res = srv.wait(t)
             assert res.status == 0 and proof == want[i][0]
+
+
+def _ecdsa_jobs(sgpu, n):
+    out = []
+    for i in range(n):
+        d, q = E.keypair(0xEC0000 + i)
+        digest = hashlib.sha256(b"DNSSEC-RRSIG-V0|rec%03d.example.|A|10.0.0.%d" % (i, i)).digest()
+        r, s = E.sign(digest, d, 0x5000 + 7 * i)
+        out.append((sgpu.JOB_P256_ECDSA, (q, r, s, digest), sgpu.p256_ecdsa_pi(q[0], q[1], r, s, digest)))
+    return out
+
+
+def test_batch_with_ecdsa_jobs(sgpu, ctx):
+    ecdsa = _ecdsa_jobs(sgpu, 3)
+    alone = [ctx.prove_p256_ecdsa(q, r, s, dg, pi) for _, (q, r, s, dg), pi in ecdsa]
+    for proof, (_, _, pi) in zip(alone, ecdsa):
+        assert O.stir_verify(proof, O.build_params(256 * E.BLOWUP, pi))
+    jobs, want = _mix(5, 3)
+    jobs = [jobs[0], ecdsa[0], jobs[1], ecdsa[1], jobs[2], ecdsa[2], jobs[3], jobs[4]]
+    want = [want[0][0], alone[0], want[1][0], alone[1], want[2][0], alone[2], want[3][0], want[4][0]]
+    out = ctx.prove_batch(jobs, n_streams=4)
+    for (proof, res), w in zip(out, want):
+        assert res.status == 0 and proof == w
+    with sgpu.Server(ctx, n_streams=2) as srv:
+        tickets = [srv.submit(*j) for j in jobs]
+        for t, w in zip(tickets, want):
+            proof, res = srv.wait(t)
+            assert res.status == 0 and proof == w
+
+
+def test_ecdsa_job_rejects_bad_input(sgpu, ctx):
+    with pytest.raises(sgpu.StarkGpuError):
+        ctx.prove_batch([(sgpu.JOB_P256_ECDSA, b"\x00" * 159, bytes(32))])

@@ -65,3 +65,14 @@ def test_rejects_bad_inputs(sg):
     for r, s in ((0, 1), (1, 0), (E.N, 1), (1, E.N)):
         with pytest.raises(sg.StarkGpuError):
             sg.p256_u_bits(digest, r, s)
+
+
+def test_ecdsa_job_packing(sg):
+    d, q = E.keypair(0x77)
+    digest = hashlib.sha256(b"job").digest()
+    r, s = E.sign(digest, d, 0x99)
+    j, buf = sg.make_job(sg.JOB_P256_ECDSA, (q, r, s, digest), bytes(32))
+    want = b"".join(v.to_bytes(32, "big") for v in (q[0], q[1], r, s)) + digest
+    assert j.kind == sg.JOB_P256_ECDSA and j.input_len == 160 and bytes(buf)[:160] == want
+    j2, _ = sg.make_job(sg.JOB_P256_ECDSA, want, bytes(32))
+    assert j2.input_len == 160
