@@ -85,6 +85,14 @@ const char* sg_last_error(const sg_ctx* ctx);
 #define SG_WIDE_MERGE_COSETS 2
 int sg_ctx_set_option(sg_ctx* ctx, int option, int64_t value);
 
+/* Grow the device's stream-ordered memory pool (which keeps freed memory) to at
+ * least `bytes`, capped at the device's free memory less 2 GiB, with one
+ * allocation freed at once; later proofs sub-allocate from it instead of growing
+ * the pool while other streams' kernels run, which stalls them. Best effort:
+ * SG_OK also when the cap leaves nothing to reserve. sg_server_create calls it
+ * with the server's HBM budget. */
+int sg_pool_reserve(sg_ctx* ctx, uint64_t bytes);
+
 /* Number of kernels this library has launched in this process (instrumentation). */
 uint64_t sg_kernel_launches(const sg_ctx* ctx);
 

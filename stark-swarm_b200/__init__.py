@@ -115,6 +115,7 @@ EXPORTS = (
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
+    "sg_pool_reserve",
 )
 JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA = 1, 2, 3, 4, 5
 OPT_WIDE_MERGE = 1
@@ -161,6 +162,7 @@ def lib():
     L.sg_ctx_destroy.restype = None
     L.sg_ctx_set_stream.argtypes = [vp, vp]
     L.sg_ctx_set_option.argtypes = [vp, i32, ctypes.c_int64]
+    L.sg_pool_reserve.argtypes = [vp, u64]
     L.sg_last_error.argtypes = [vp]
     L.sg_last_error.restype = ctypes.c_char_p
     L.sg_kernel_launches.argtypes = [vp]
@@ -579,6 +581,10 @@ class Context:
 
     def set_option(self, option: int, value: int):
         self._check(self._lib.sg_ctx_set_option(self._h, option, value))
+
+    def pool_reserve(self, nbytes: int):
+        """sg_pool_reserve: grow the device memory pool to nbytes up front (best effort)."""
+        self._check(self._lib.sg_pool_reserve(self._h, nbytes))
 
     @property
     def kernel_launches(self) -> int:

@@ -1,4 +1,5 @@
 // capi.cu — extern "C" entry points declared in include/stark_gpu.h.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -81,6 +82,31 @@ struct Out {
 
 }  // namespace
 
+namespace sg {
+
+void pool_reserve(int device, uint64_t bytes, cudaStream_t s) {
+  cuda_check(cudaSetDevice(device), "set device");
+  cudaMemPool_t pool;
+  cuda_check(cudaDeviceGetDefaultMemPool(&pool, device), "memory pool");
+  uint64_t reserved = 0;
+  cuda_check(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved), "memory pool");
+  if (reserved >= bytes) return;
+  size_t free_b = 0, total_b = 0;
+  cuda_check(cudaMemGetInfo(&free_b, &total_b), "memory info");
+  const uint64_t margin = 2ull << 30;
+  if (free_b <= margin) return;
+  const uint64_t want = std::min<uint64_t>(bytes - reserved, free_b - margin);
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, want, s) != cudaSuccess) {
+    cudaGetLastError();  // nothing reserved; proofs grow the pool as they go
+    return;
+  }
+  cuda_check(cudaFreeAsync(p, s), "free");
+  cuda_check(cudaStreamSynchronize(s), "sync");
+}
+
+}  // namespace sg
+
 extern "C" {
 
 int sg_ctx_create(int device, sg_ctx** out) {
@@ -132,6 +158,12 @@ void sg_ctx_destroy(sg_ctx* c) {
     cudaStreamDestroy(c->copy_stream);
   }
   if (c->shift_tab) cudaFree(c->shift_tab);
+  if (c->stir_stream) {
+    cudaStreamSynchronize(c->stir_stream);
+    cudaStreamDestroy(c->stir_stream);
+  }
+  if (c->stir_in) cudaEventDestroy(c->stir_in);
+  if (c->stir_out) cudaEventDestroy(c->stir_out);
   delete c;
 }
 
@@ -151,6 +183,10 @@ int sg_ctx_set_option(sg_ctx* c, int option, int64_t value) {
     return SG_OK;
   }
   return SG_EINVAL;
+}
+
+int sg_pool_reserve(sg_ctx* c, uint64_t bytes) {
+  return guarded(c, [&] { sg::pool_reserve(c->device, bytes, c->stream); });
 }
 
 uint64_t sg_kernel_launches(const sg_ctx*) { return sg::g_kernel_launches.load(); }

@@ -23,6 +23,10 @@ struct sg_ctx {
   sg::NttTables tw;
   bool owns_tables = true;  // worker contexts of a server borrow the parent's tables
   int wide_merge = SG_WIDE_MERGE_AUTO;  // SG_OPT_WIDE_MERGE
+  // Server workers only (null elsewhere): a highest-priority stream for the STIR
+  // phase of a proof and the two events that order it after and before `stream`.
+  cudaStream_t stir_stream = nullptr;
+  cudaEvent_t stir_in = nullptr, stir_out = nullptr;
   std::string err;
 };
 
@@ -78,5 +82,8 @@ struct DBuf {
 };
 
 bool is_device_ptr(const void* p);
+
+// sg_pool_reserve: grow the device's default pool to `bytes` (best effort).
+void pool_reserve(int device, uint64_t bytes, cudaStream_t s);
 
 }  // namespace sg

@@ -86,6 +86,7 @@ struct PassArgs {
   // radix-16 group can be non-zero (zero-padded forward transform); 0 = dense
   int sparse_nz;
   int tw_log;                 // > 0: output (lane, i) *= w_{2^tw_log}^(i*lane)
+  int in_tw_log;              // > 0: input (lane, m) *= w_{2^in_tw_log}^(m*lane)
   uint64_t scale;             // != 1: outputs *= scale
   const uint64_t* tw_st;      // w_4096^i (direction of the transform)
   const uint64_t* tw_lo;      // w28^i
@@ -175,7 +176,9 @@ __device__ __forceinline__ void stockham_first_sparse(uint64_t* sm, int t, int T
   }
 }
 
-template <int LOG_M, bool INV>
+// COSET: the input twist w_{2^in_tw_log}^(m*lane) of ntt_coset_eval (a separate
+// instantiation, so the other passes' register allocation does not carry it).
+template <int LOG_M, bool INV, bool COSET = false>
 __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   constexpr int M = 1 << LOG_M;
   constexpr int V = M < 16 ? M : 16;
@@ -238,6 +241,7 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       if (e < E_load && lane < a.n_lanes && flat < a.in_valid) {
         x[q] = __ldg(in + lane * a.in_lane + (uint64_t)m * a.in_m);
         if (a.pre.lo) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
+        if constexpr (COSET) x[q] = gl::mul(x[q], tw_pow(a.tw_lo, a.tw_hi, (uint64_t)m * lane, a.in_tw_log));
       }
     }
 #pragma unroll
@@ -328,7 +332,8 @@ cudaError_t launch_pass(const PassArgs& a0, bool inv, uint64_t n_rows, cudaStrea
   static_assert(T <= 1024, "too many threads per CTA");
   const size_t smem = (size_t)K * row_stride(LOG_M) * sizeof(uint64_t) + pass_table_bytes(LOG_M);
   const uint64_t blocks = (a.n_lanes + K - 1) / K;
-  auto kern = inv ? ntt_pass_kernel<LOG_M, true> : ntt_pass_kernel<LOG_M, false>;
+  auto kern = a.in_tw_log > 0 ? ntt_pass_kernel<LOG_M, false, true>
+                              : inv ? ntt_pass_kernel<LOG_M, true> : ntt_pass_kernel<LOG_M, false>;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -458,6 +463,37 @@ cudaError_t ntt_tables_init(NttTables* t) {
 void ntt_tables_free(NttTables* t) {
   if (t->owned && t->d_fwd_st) cudaFree(t->d_fwd_st);
   *t = NttTables{};
+}
+
+bool ntt_coset_eval_ok(int log_m, int log_b) {
+  return log_m >= 1 && log_m <= 12 && log_b >= pass_log_k(log_m) && log_m + log_b <= kMaxLogN;
+}
+
+// Coset t < B of the evaluation domain is the DFT_M of c_m * g^m * w_N^{t m}:
+// f(g w_N^{B i + t}) = sum_m c_m g^m w_N^{t m} w_M^{i m}. One pass with one lane
+// per coset (a CTA's K lanes are K cosets of one column, so its stores of point
+// i are K adjacent outputs B i + t) and grid.y over the columns; every lane
+// reads the same M coefficients.
+cudaError_t ntt_coset_eval(const NttTables& t, const uint64_t* coef, uint64_t* out, uint32_t n_cols, int log_m,
+                           int log_b, cudaStream_t s, const PowSpec* pre) {
+  if (!ntt_coset_eval_ok(log_m, log_b)) return cudaErrorInvalidValue;
+  if (n_cols == 0) return cudaSuccess;
+  const uint64_t M = 1ull << log_m, B = 1ull << log_b;
+  PassArgs a = base_args(t, false);
+  a.pre = pre ? *pre : PowSpec{};
+  a.in = coef;
+  a.out = out;
+  a.in_col = M;
+  a.out_col = M * B;
+  a.in_lane = 0;
+  a.in_m = 1;
+  a.out_lane = 1;
+  a.out_i = B;
+  a.n_lanes = B;
+  a.flat_lane = 0;
+  a.in_valid = M;
+  a.in_tw_log = log_m + log_b;
+  return launch_pass_dyn(log_m, a, false, n_cols, s);
 }
 
 uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n) {

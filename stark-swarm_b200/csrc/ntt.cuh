@@ -64,6 +64,16 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
                       uint64_t out_stride, int log_n, bool inverse, uint64_t n_valid, uint64_t* scratch,
                       cudaStream_t s, const PowSpec* pre = nullptr);
 
+// Evaluate n_cols polynomials of degree < M = 2^log_m (coefficients contiguous,
+// column stride M) on the N = M * 2^log_b points g * w_N^j in natural order
+// (column stride N) in one pass, without scratch: a forward transform of the
+// zero-padded coefficients times g^k, as ntt_batch computes it with `pre`.
+// Needs ntt_coset_eval_ok(log_m, log_b): log_m <= 12 and at least as many
+// cosets as a pass's lanes per CTA.
+bool ntt_coset_eval_ok(int log_m, int log_b);
+cudaError_t ntt_coset_eval(const NttTables& t, const uint64_t* coef, uint64_t* out, uint32_t n_cols, int log_m,
+                           int log_b, cudaStream_t s, const PowSpec* pre = nullptr);
+
 }  // namespace sg
 
 #if defined(__CUDACC__)

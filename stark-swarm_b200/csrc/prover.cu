@@ -81,18 +81,34 @@ struct ShiftTables {
   }
 };
 
+// A domain above one pass (2^12) from a trace of at most 2^12 rows is evaluated
+// coset by coset in one pass (ntt_coset_eval): no scratch round trip, and no
+// scratch buffer the size of the LDE.
+bool lde_by_cosets(uint64_t n_trace, uint64_t blowup) {
+  const int lm = (int)log2_exact(n_trace), lb = (int)log2_exact(blowup);
+  return lm + lb > 12 && ntt_coset_eval_ok(lm, lb);
+}
+
 // iNTT of w columns into coef, then the zero-padded forward transform into d_out,
 // coefficient k times shift^k (applied as the forward transform loads it).
 void lde_core(sg_ctx* c, const uint64_t* d_trace, uint64_t w, uint64_t n_trace, uint64_t blowup,
               const ShiftTables& sh, uint64_t* coef, uint64_t* scratch, uint64_t* d_out) {
   const uint64_t n0 = n_trace * blowup;
   ntt(c, d_trace, coef, (uint32_t)w, n_trace, n_trace, log2_exact(n_trace), true, n_trace, scratch);
+  if (lde_by_cosets(n_trace, blowup)) {
+    cuda_check(ntt_coset_eval(c->tw, coef, d_out, (uint32_t)w, (int)log2_exact(n_trace), (int)log2_exact(blowup),
+                              c->stream, sh.active ? &sh.spec : nullptr),
+               "coset evaluation");
+    return;
+  }
   ntt(c, coef, d_out, (uint32_t)w, n_trace, n0, log2_exact(n0), false, n_trace, scratch,
       sh.active ? &sh.spec : nullptr);
 }
 
 uint64_t lde_scratch_elems(uint64_t w, uint64_t n_trace, uint64_t blowup) {
-  return std::max(ntt_scratch_elems(w, log2_exact(n_trace * blowup)), ntt_scratch_elems(w, log2_exact(n_trace)));
+  const uint64_t inv = ntt_scratch_elems(w, log2_exact(n_trace));
+  if (lde_by_cosets(n_trace, blowup)) return inv;
+  return std::max(ntt_scratch_elems(w, log2_exact(n_trace * blowup)), inv);
 }
 
 }  // namespace
@@ -424,7 +440,9 @@ std::vector<uint8_t> classic_prove_device(sg_ctx* c, const uint64_t* d_f0, uint6
   return encode_proof(pr);
 }
 
-std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p) {
+namespace {
+
+std::vector<uint8_t> stir_prove_on_stream(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p) {
   cudaStream_t s = c->stream;
   const uint64_t L = p.schedule_len;
   require(L >= 1 && L <= SG_MAX_SCHEDULE, "stir_prove: empty or oversized schedule");
@@ -640,6 +658,31 @@ std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t
   }
   pr.prox = std::move(qs);
   return encode_proof(pr);
+}
+
+// For the STIR phase, a context with a stir_stream (a server worker) moves to it:
+// the stream waits for everything queued so far, and `stream` waits for the STIR
+// work before the caller queues more (its buffers are freed in stream order).
+struct StirStreamScope {
+  sg_ctx* c;
+  cudaStream_t saved;
+  explicit StirStreamScope(sg_ctx* ctx) : c(ctx), saved(ctx->stream) {
+    cuda_check(cudaEventRecord(c->stir_in, saved), "event");
+    cuda_check(cudaStreamWaitEvent(c->stir_stream, c->stir_in, 0), "wait");
+    c->stream = c->stir_stream;
+  }
+  ~StirStreamScope() {
+    c->stream = saved;
+    if (cudaEventRecord(c->stir_out, c->stir_stream) == cudaSuccess) cudaStreamWaitEvent(saved, c->stir_out, 0);
+  }
+};
+
+}  // namespace
+
+std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t n0, const sg_fri_params& p) {
+  if (!c->stir_stream) return stir_prove_on_stream(c, d_f0, n0, p);
+  StirStreamScope scope(c);
+  return stir_prove_on_stream(c, d_f0, n0, p);
 }
 
 // ------------------------------------------------------------------ HashRollup pipeline

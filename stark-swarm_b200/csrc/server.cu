@@ -64,8 +64,9 @@ uint64_t footprint_bytes(const sg_job& j) {
     return 8 * ((uint64_t)sg::sha512::WIDTH * (n0 + 2 * nt) + 16 * n0);
   }
   if (j.kind == SG_JOB_P256_ECDSA) {
-    // trace, LDE and the LDE transform's scratch at 151,334 columns, n0 = 8192
-    return 8ull * sg::p256::layout().width * (sg::p256::K_ECDSA + 2 * 8192) + (64ull << 20);
+    // trace, coefficients and LDE at 151,334 columns, n0 = 8192 (the LDE is
+    // evaluated coset by coset, without a scratch copy)
+    return 8ull * sg::p256::layout().width * (2 * sg::p256::K_ECDSA + 8192) + (64ull << 20);
   }
   if (j.kind == SG_JOB_RSA2048) {
     const uint64_t recs = j.input_len / 768, w = recs * sg::rsa::WIDTH;
@@ -173,19 +174,40 @@ int sg_server_create(sg_ctx* ctx, int n_streams, uint64_t hbm_budget_bytes, sg_s
   s->parent = ctx;
   s->budget = hbm_budget_bytes ? hbm_budget_bytes : UINT64_MAX;
   cudaSetDevice(ctx->device);
+  int prio_low = 0, prio_high = 0;
+  if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) {
+    delete s;
+    return SG_ECUDA;
+  }
   for (int i = 0; i < n_streams; ++i) {
     sg_ctx* w = new sg_ctx;
     w->device = ctx->device;
     w->tw = ctx->tw;
     w->owns_tables = false;
     w->wide_merge = ctx->wide_merge;
-    if (cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
-      delete w;
+    s->wctx.push_back(w);
+    // The STIR phase (many small launches, each followed by a host round trip)
+    // runs on a highest-priority stream, so its CTAs are dispatched ahead of the
+    // remaining CTAs of other workers' LDE and constraint kernels.
+    if (cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&w->stir_stream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+        cudaEventCreateWithFlags(&w->stir_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&w->stir_out, cudaEventDisableTiming) != cudaSuccess) {
+      if (!w->stream) w->stream = w->own_stream;
       sg_server_destroy(s);
       return SG_ECUDA;
     }
     w->stream = w->own_stream;
-    s->wctx.push_back(w);
+  }
+  if (hbm_budget_bytes) {
+    // the pool's steady-state size up front: growing it piecemeal while other
+    // workers' kernels run stalls them
+    try {
+      sg::pool_reserve(ctx->device, hbm_budget_bytes, s->wctx[0]->stream);
+    } catch (const sg::SgError&) {
+      sg_server_destroy(s);
+      return SG_ECUDA;
+    }
   }
   for (sg_ctx* w : s->wctx) s->threads.emplace_back([s, w] { s->worker(w); });
   *out = s;

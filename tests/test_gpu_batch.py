@@ -102,3 +102,12 @@ def test_batch_with_ecdsa_jobs(sgpu, ctx):
 def test_ecdsa_job_rejects_bad_input(sgpu, ctx):
     with pytest.raises(sgpu.StarkGpuError):
         ctx.prove_batch([(sgpu.JOB_P256_ECDSA, b"\x00" * 159, bytes(32))])
+
+
+def test_pool_reserve_then_batch(ctx):
+    ctx.pool_reserve(2 << 30)
+    ctx.pool_reserve(1 << 30)  # already reserved: nothing to do
+    jobs, want = _mix(6, 17)
+    out = ctx.prove_batch(jobs, n_streams=4, hbm_budget_bytes=3 << 30)
+    for (proof, res), (wproof, _) in zip(out, want):
+        assert res.status == 0 and proof == wproof
