@@ -180,6 +180,21 @@ struct Acc128 {
     asm("add.cc.u32 %0, %0, %4;\n\taddc.cc.u32 %1, %1, %5;\n\taddc.cc.u32 %2, %2, %6;\n\taddc.u32 %3, %3, 0;"
         : "+r"(a0), "+r"(a1), "+r"(a2), "+r"(a3) : "r"(y0), "r"(y1), "r"(y2));
   }
+  // x 2^(32 + f), f < 32: the same three words one limb up (the sum must stay below 2^128)
+  __device__ __forceinline__ void add_shl32(uint64_t x, unsigned f) {
+    uint32_t y0, y1, y2;
+    shl96(x, f, y0, y1, y2);
+    asm("add.cc.u32 %0, %0, %3;\n\taddc.cc.u32 %1, %1, %4;\n\taddc.u32 %2, %2, %5;"
+        : "+r"(a1), "+r"(a2), "+r"(a3) : "r"(y0), "r"(y1), "r"(y2));
+  }
+  // lam * x for lam < 2^32: 4 IMADs and 3 adds
+  __device__ __forceinline__ void add_mul32(uint32_t lam, uint64_t x) {
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32);
+    asm("mad.lo.cc.u32 %0, %4, %6, %0;\n\tmadc.hi.cc.u32 %1, %4, %6, %1;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\taddc.u32 %3, %3, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\tmadc.hi.cc.u32 %2, %5, %6, %2;\n\taddc.u32 %3, %3, 0;"
+        : "+r"(a0), "+r"(a1), "+r"(a2), "+r"(a3) : "r"(x0), "r"(x1), "r"(lam));
+  }
   __device__ __forceinline__ uint64_t reduce() const {
     return reduce128((uint64_t)a3 << 32 | a2, (uint64_t)a1 << 32 | a0);
   }

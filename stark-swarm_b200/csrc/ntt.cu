@@ -241,7 +241,13 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       if (e < E_load && lane < a.n_lanes && flat < a.in_valid) {
         x[q] = __ldg(in + lane * a.in_lane + (uint64_t)m * a.in_m);
         if (a.pre.lo) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
-        if constexpr (COSET) x[q] = gl::mul(x[q], tw_pow(a.tw_lo, a.tw_hi, (uint64_t)m * lane, a.in_tw_log));
+        if constexpr (COSET) {
+          // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j)
+          const uint64_t e = (uint64_t)m * lane;
+          x[q] = gl::mul(x[q], a.in_tw_log <= kTwSplit
+                                   ? __ldg(a.tw_hi + ((e << (kTwSplit - a.in_tw_log)) & (kTwEntries - 1)))
+                                   : tw_pow(a.tw_lo, a.tw_hi, e, a.in_tw_log));
+        }
       }
     }
 #pragma unroll
