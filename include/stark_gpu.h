@@ -208,14 +208,23 @@ int sg_sha512_trace_gpu(sg_ctx* ctx, const uint8_t* msg, size_t len, uint64_t* t
 int sg_prove_sha512(sg_ctx* ctx, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,
                     uint8_t* proof, size_t cap, size_t* len_out, uint8_t digest[64]);
 
+/* Hash profile of this build, the counterpart of the reference's compile-time hash
+ * feature (hash/src/selected.rs:8-48): digest bytes of every Merkle node and of the
+ * Fiat-Shamir transcript, so of every root in a proof. libstarkgpu.so is the
+ * sha3-256 build (32), libstarkgpu_sha3_384.so 48, libstarkgpu_sha3_512.so 64.
+ * Record hashing and the pi_hash recipes are SHA3-256 in every build, and the
+ * swarm-dns shard entries (which bind 32-byte roots) need the sha3-256 build. */
+int sg_hash_bytes(void);
+
 /* Merkle commitment over the rows of a column-major matrix (leaf i = the
  * `width` values of row i), with the reference channel's framing
  * (merkle/src/lib.rs:95-238, 391-476): per-level arities, tree label, last-node
- * padding. `keep` (optional) receives a device-resident tree for sg_merkle_open. */
+ * padding. root: sg_hash_bytes() bytes. `keep` (optional) receives a
+ * device-resident tree for sg_merkle_open. */
 int sg_merkle_commit(sg_ctx* ctx, const uint64_t* cols, size_t n_leaves, size_t width, size_t col_stride,
-                     const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t root[32], sg_tree** keep);
-/* Serialized MerkleOpening (ark-serialize compressed: leaf[32], path Vec<Vec<[u8;32]>>,
- * index u64) for leaf `index` (merkle/src/lib.rs:478-512). */
+                     const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t* root, sg_tree** keep);
+/* Serialized MerkleOpening (ark-serialize compressed: leaf[HASH_BYTES], path
+ * Vec<Vec<[u8; HASH_BYTES]>>, index u64) for leaf `index` (merkle/src/lib.rs:478-512). */
 int sg_merkle_open(sg_ctx* ctx, const sg_tree* tree, size_t index, uint8_t* out, size_t cap, size_t* len);
 void sg_merkle_free(sg_tree* tree);
 

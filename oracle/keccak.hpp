@@ -1,10 +1,10 @@
-// oracle/keccak.hpp — CPU Keccak-f[1600] and streaming SHA3-256.
+// oracle/keccak.hpp — CPU Keccak-f[1600] and streaming SHA3-256/384/512.
 //
 // TEST INFRASTRUCTURE ONLY (part of the oracle; never linked into the product).
 //
 // sha3 0.10.8 / keccak 0.1.6 (pinned in stark-stir-swarm/Cargo.lock, not vendored)
-// implement FIPS 202; this restates FIPS 202 directly: rate 136 bytes for
-// SHA3-256, domain padding 0x06 ... 0x80. Callers in the reference:
+// implement FIPS 202; this restates FIPS 202 directly: rate 200 - 2d bytes for
+// a d-byte digest (136 for SHA3-256), domain padding 0x06 ... 0x80. Callers in the reference:
 // merkle/src/lib.rs:197-216,232-237 (tree nodes), transcript/src/lib.rs:158-213
 // (Fiat-Shamir), fri.rs:1035-1066 (tree-domain hashes). Pinned by
 // hashlib.sha3_256 in tests and by the golden proofs.
@@ -43,18 +43,21 @@ inline void keccak_f1600(uint64_t s[25]) {
   }
 }
 
-// Streaming SHA3-256 (copyable: the transcript clones it to squeeze).
-struct Sha3_256 {
+// Streaming SHA3 with an OUT-byte digest (rate 200 - 2 OUT bytes); copyable,
+// since the transcript clones it to squeeze.
+template <int OUT>
+struct Sha3 {
+  static constexpr int RATE = 200 - 2 * OUT;
   uint64_t st[25];
-  uint8_t buf[136];
+  uint8_t buf[RATE];
   size_t fill;
-  Sha3_256() { reset(); }
+  Sha3() { reset(); }
   void reset() {
     memset(st, 0, sizeof st);
     fill = 0;
   }
   void absorb_block(const uint8_t* blk) {
-    for (int i = 0; i < 17; ++i) {
+    for (int i = 0; i < RATE / 8; ++i) {
       uint64_t w;
       memcpy(&w, blk + 8 * i, 8);  // little-endian host assumed (x86-64)
       st[i] ^= w;
@@ -64,27 +67,38 @@ struct Sha3_256 {
   void update(const void* data, size_t len) {
     const uint8_t* p = (const uint8_t*)data;
     while (len) {
-      size_t take = 136 - fill;
+      size_t take = RATE - fill;
       if (take > len) take = len;
       memcpy(buf + fill, p, take);
       fill += take;
       p += take;
       len -= take;
-      if (fill == 136) {
+      if (fill == (size_t)RATE) {
         absorb_block(buf);
         fill = 0;
       }
     }
   }
-  void finalize(uint8_t out[32]) const {
-    Sha3_256 c = *this;
-    memset(c.buf + c.fill, 0, 136 - c.fill);
+  void finalize(uint8_t out[OUT]) const {
+    Sha3 c = *this;
+    memset(c.buf + c.fill, 0, RATE - c.fill);
     c.buf[c.fill] ^= 0x06;
-    c.buf[135] ^= 0x80;
+    c.buf[RATE - 1] ^= 0x80;
     c.absorb_block(c.buf);
-    memcpy(out, c.st, 32);
+    memcpy(out, c.st, OUT);
   }
 };
+using Sha3_256 = Sha3<32>;
+
+// The hash profile of the Merkle channel and the Fiat-Shamir transcript: the
+// reference picks it at compile time (hash/src/selected.rs:8-48, HASH_BYTES 32 /
+// 48 / 64 for the sha3-256 / sha3-384 / sha3-512 features); so does this build.
+#ifndef ORC_HASH_BYTES
+#define ORC_HASH_BYTES 32
+#endif
+static_assert(ORC_HASH_BYTES == 32 || ORC_HASH_BYTES == 48 || ORC_HASH_BYTES == 64, "SHA3-256/384/512 only");
+constexpr int HASH_BYTES = ORC_HASH_BYTES;
+using SelectedHasher = Sha3<HASH_BYTES>;
 
 inline void sha3_256(const void* data, size_t len, uint8_t out[32]) {
   Sha3_256 h;

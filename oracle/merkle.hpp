@@ -1,4 +1,4 @@
-// oracle/merkle.hpp — CPU restatement of the reference's SHA3-256 Merkle channel.
+// oracle/merkle.hpp — CPU restatement of the reference's SHA3 Merkle channel.
 //
 // TEST INFRASTRUCTURE ONLY (part of the oracle; never linked into the product).
 //
@@ -20,7 +20,7 @@
 
 namespace orc {
 
-using Digest = std::array<uint8_t, 32>;
+using Digest = std::array<uint8_t, HASH_BYTES>;
 
 inline size_t pick_arity_for_layer(size_t n, size_t m) {
   const size_t cands[] = {128, 64, 32, 16, 8, 4};
@@ -48,7 +48,7 @@ inline void ds_label(uint8_t out[32], uint64_t arity, uint64_t level, uint64_t p
 inline Digest leaf_hash(size_t arity0, uint64_t label, uint64_t pos, const Fp* vals, size_t n) {
   uint8_t ds[32];
   ds_label(ds, arity0, 0xFFFFFFFFull, pos, label);
-  Sha3_256 h;
+  SelectedHasher h;
   h.update(ds, 32);
   for (size_t i = 0; i < n; ++i) h.update(&vals[i].v, 8);
   Digest d;
@@ -59,9 +59,9 @@ inline Digest leaf_hash(size_t arity0, uint64_t label, uint64_t pos, const Fp* v
 inline Digest node_hash(size_t arity, uint64_t label, uint64_t level, uint64_t pos, const Digest* ch) {
   uint8_t ds[32];
   ds_label(ds, arity, level, pos, label);
-  Sha3_256 h;
+  SelectedHasher h;
   h.update(ds, 32);
-  for (size_t i = 0; i < arity; ++i) h.update(ch[i].data(), 32);
+  for (size_t i = 0; i < arity; ++i) h.update(ch[i].data(), HASH_BYTES);
   Digest d;
   h.finalize(d.data());
   return d;

@@ -381,7 +381,7 @@ StirProof classic_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
   MerkleTree f0tree(f0cfg.ar, f0cfg.label);
   f0tree.build(f0, 1);
   pr.root_f0 = f0tree.root();
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), HASH_BYTES);
   const Fp6 z = tr.challenge_ext("z_fp3");
 
   std::vector<std::vector<Fp6>> layers, s_layers, q_layers;
@@ -412,7 +412,7 @@ StirProof classic_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
     q_layers.push_back(std::move(q));
     commit(ell, m);
     tr.absorb_ext(fz);
-    tr.absorb_bytes(pr.roots.back().data(), 32);
+    tr.absorb_bytes(pr.roots.back().data(), HASH_BYTES);
     layers.push_back(std::move(next));
     cur = nn;
   }
@@ -428,7 +428,7 @@ StirProof classic_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
     q_layers.push_back(std::move(q));
     commit(ell, m);
     tr.absorb_ext(fz);
-    tr.absorb_bytes(pr.roots.back().data(), 32);
+    tr.absorb_bytes(pr.roots.back().data(), HASH_BYTES);
     auto tuples = extract_coset_coeffs(layers[ell], omega, m);
     TreeCfg cc = layer_cfg(nf, 16, 0xFE);
     MerkleTree ct(cc.ar, cc.label);
@@ -438,7 +438,7 @@ StirProof classic_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
         for (int k = 0; k < 6; ++k) rows[(b * m + i) * 6 + k] = tuples[b][i].comp(k);
     ct.build(rows, m * 6);
     pr.coeff_root = ct.root();
-    tr.absorb_bytes(pr.coeff_root.data(), 32);
+    tr.absorb_bytes(pr.coeff_root.data(), HASH_BYTES);
     const Fp6 alpha = tr.challenge_ext("alpha");
     (void)tr.challenge_ext("beta_deg");
     layers.push_back(fold(tuples, alpha));
@@ -500,7 +500,7 @@ StirProof stir_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
     f0tree.build(rows, m0);
   }
   pr.root_f0 = f0tree.root();
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), HASH_BYTES);
   Fp6 z = tr.challenge_ext("z_fp3");
 
   std::vector<std::vector<Fp6>> layers;
@@ -535,7 +535,7 @@ StirProof stir_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
     auto tuples = extract_coset_coeffs(layers[ell], omega, m);
     commit_layer(ell, m);
     for (auto& e : ev) tr.absorb_ext(e);
-    tr.absorb_bytes(pr.roots.back().data(), 32);
+    tr.absorb_bytes(pr.roots.back().data(), HASH_BYTES);
     pr.coset_evals.push_back(ev);
     layers.push_back(fold(tuples, alpha));
     cur /= m;
@@ -550,7 +550,7 @@ StirProof stir_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
     zc = e_pow(zc, m);
     commit_layer(ell, m);
     for (auto& e : ev) tr.absorb_ext(e);
-    tr.absorb_bytes(pr.roots.back().data(), 32);
+    tr.absorb_bytes(pr.roots.back().data(), HASH_BYTES);
     pr.coset_evals.push_back(ev);
     auto tuples = extract_coset_coeffs(layers[ell], omega, m);
     size_t nf = cur / m;
@@ -562,7 +562,7 @@ StirProof stir_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
         for (int k = 0; k < 6; ++k) rows[(b * m + i) * 6 + k] = tuples[b][i].comp(k);
     ct.build(rows, m * 6);
     pr.coeff_root = ct.root();
-    tr.absorb_bytes(pr.coeff_root.data(), 32);
+    tr.absorb_bytes(pr.coeff_root.data(), HASH_BYTES);
     Fp6 alpha = tr.challenge_ext("alpha");
     alphas.push_back(alpha);
     (void)tr.challenge_ext("beta_deg");
@@ -600,7 +600,7 @@ StirProof stir_prove(const std::vector<Fp>& f0, const orc_fri_params& p) {
 
 // ------------------------------------------------------------------ serializer
 // ark-serialize 0.4.2 Compress::Yes on DeepFriProof (fri.rs:1235-1300) and
-// MerkleOpening (merkle/src/lib.rs:135-140): [u8;32] raw, usize/len as le64,
+// MerkleOpening (merkle/src/lib.rs:135-140): [u8; HASH_BYTES] raw, usize/len as le64,
 // F as le64 canonical, Fp6 as 6 components, Option as one flag byte + payload.
 struct Writer {
   std::vector<uint8_t> b;
@@ -705,7 +705,7 @@ struct Reader {
     if (x > n) throw std::runtime_error("implausible length");
     return x;
   }
-  Digest dig() { need(32); Digest d; memcpy(d.data(), p + o, 32); o += 32; return d; }
+  Digest dig() { need(HASH_BYTES); Digest d; memcpy(d.data(), p + o, HASH_BYTES); o += HASH_BYTES; return d; }
   Fp fe() {
     uint64_t x = u64();
     if (x >= P) throw std::runtime_error("non-canonical field element");
@@ -844,7 +844,7 @@ bool classic_verify(const StirProof& pr, const orc_fri_params& p) {
   if (pr.roots.size() < L || pr.fz.size() < L) return false;
   Transcript tr("FRI/FS");
   bind_statement(tr, p, pr.n0);
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), HASH_BYTES);
   const Fp6 z = tr.challenge_ext("z_fp3");
   std::vector<Fp6> alphas;
   Fp6 beta;
@@ -852,10 +852,10 @@ bool classic_verify(const StirProof& pr, const orc_fri_params& p) {
     const bool last_cc = use_cc && ell == L - 1;
     if (!last_cc) alphas.push_back(tr.challenge_ext("alpha"));
     tr.absorb_ext(pr.fz[ell]);
-    tr.absorb_bytes(pr.roots[ell].data(), 32);
+    tr.absorb_bytes(pr.roots[ell].data(), HASH_BYTES);
     if (last_cc) {
       if (!pr.has_croot) return false;
-      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      tr.absorb_bytes(pr.coeff_root.data(), HASH_BYTES);
       alphas.push_back(tr.challenge_ext("alpha"));
       beta = tr.challenge_ext("beta_deg");
     }
@@ -938,7 +938,7 @@ bool stir_verify(const StirProof& pr, const orc_fri_params& p) {
   if (pr.roots.size() < L || pr.coset_evals.size() < L) return false;
   Transcript tr("FRI/FS");
   bind_statement(tr, p, pr.n0);
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), HASH_BYTES);
   Fp6 z = tr.challenge_ext("z_fp3");
   Fp6 zc = z;
   std::vector<std::vector<Fp6>> interps;
@@ -954,10 +954,10 @@ bool stir_verify(const StirProof& pr, const orc_fri_params& p) {
     interps.push_back(interp_stir_coset(ev, zc, zeta));
     zc = e_pow(zc, m);
     for (auto& e : ev) tr.absorb_ext(e);
-    tr.absorb_bytes(pr.roots[ell].data(), 32);
+    tr.absorb_bytes(pr.roots[ell].data(), HASH_BYTES);
     if (last_cc) {
       if (!pr.has_croot) return false;
-      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      tr.absorb_bytes(pr.coeff_root.data(), HASH_BYTES);
       alphas.push_back(tr.challenge_ext("alpha"));
       beta = tr.challenge_ext("beta_deg");
     }
@@ -1099,8 +1099,15 @@ void orc_sha3_256(const uint8_t* msg, size_t len, uint8_t out[32]) { sha3_256(ms
 uint64_t orc_stdrng_first_u64(const uint8_t seed[32]) { return stdrng_first_u64(seed); }
 uint64_t orc_root_of_unity(unsigned log_n) { return root_of_unity(log_n).v; }
 
+int orc_hash_bytes(void) { return HASH_BYTES; }
+void orc_sha3_selected(const uint8_t* msg, size_t len, uint8_t* out) {
+  SelectedHasher h;
+  h.update(msg, len);
+  h.finalize(out);
+}
+
 int orc_merkle_root(const uint64_t* rows, size_t n_leaves, size_t width, const uint64_t* arities, size_t depth,
-                    uint64_t label, uint8_t root[32]) {
+                    uint64_t label, uint8_t* root) {
   if (n_leaves == 0 || depth == 0) return -1;
   std::vector<size_t> ar(arities, arities + depth);
   MerkleTree t(ar, label);
@@ -1110,7 +1117,7 @@ int orc_merkle_root(const uint64_t* rows, size_t n_leaves, size_t width, const u
   } catch (...) {
     return -2;
   }
-  memcpy(root, t.root().data(), 32);
+  memcpy(root, t.root().data(), HASH_BYTES);
   return 0;
 }
 

@@ -59,8 +59,13 @@ int orc_lde(const uint64_t* trace, size_t w, size_t n_trace, size_t blowup, uint
 void orc_sha3_256(const uint8_t* msg, size_t len, uint8_t out[32]);
 uint64_t orc_stdrng_first_u64(const uint8_t seed[32]);
 uint64_t orc_root_of_unity(unsigned log_n);
+/* Digest bytes of this build's hash profile (32, 48 or 64: SHA3-256/384/512). */
+int orc_hash_bytes(void);
+/* SHA3 of this build's profile; out: orc_hash_bytes() bytes. */
+void orc_sha3_selected(const uint8_t* msg, size_t len, uint8_t* out);
+/* root: orc_hash_bytes() bytes */
 int orc_merkle_root(const uint64_t* rows, size_t n_leaves, size_t width, const uint64_t* arities, size_t depth,
-                    uint64_t label, uint8_t root[32]);
+                    uint64_t label, uint8_t* root);
 int orc_hash_rollup_trace(const uint64_t* leaves, size_t n_leaves, size_t n_trace, uint64_t* trace);
 int orc_merge(int air, const uint64_t* lde, size_t w, size_t n_trace, size_t blowup, const uint64_t* lambdas,
               size_t k, int phi_mode, uint64_t* c_eval);

@@ -18,7 +18,7 @@
 namespace orc {
 
 struct Transcript {
-  Sha3_256 h;
+  SelectedHasher h;
   explicit Transcript(const char* label) {
     static const char kInit[] = "FSv1-TRANSCRIPT-INIT";
     h.update(kInit, sizeof kInit - 1);
@@ -39,19 +39,19 @@ struct Transcript {
   void absorb_ext(const Fp6& e) {
     for (int i = 0; i < 6; ++i) absorb_field(e.comp(i));
   }
-  void challenge_bytes(const void* label, size_t n, uint8_t out[32]) const {
+  void challenge_bytes(const void* label, size_t n, uint8_t out[HASH_BYTES]) const {
     static const char kCh[] = "FSv1-CHALLENGE";
-    Sha3_256 c = h;
+    SelectedHasher c = h;
     c.update(kCh, sizeof kCh - 1);
     c.update(label, n);
     c.finalize(out);
   }
   // safe_field_challenge: fold the digest's 7-byte chunks taken from the END.
   Fp challenge_field(const std::string& label) const {
-    uint8_t d[32];
+    uint8_t d[HASH_BYTES];
     challenge_bytes(label.data(), label.size(), d);
     Fp acc;
-    int end = 32;
+    int end = HASH_BYTES;
     while (end > 0) {
       int start = end >= 7 ? end - 7 : 0;
       int len = end - start;

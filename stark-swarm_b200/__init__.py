@@ -29,7 +29,16 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libstarkgpu.so")
+# The hash profile is fixed per build, as the reference's hash feature is per
+# compile (hash/src/selected.rs:8-48); a process picks one with STARK_GPU_HASH
+# (sha3-256, the default, sha3-384 or sha3-512) before it first uses the library.
+HASH_PROFILE = os.environ.get("STARK_GPU_HASH", "sha3-256")
+_LIB_NAME = {"sha3-256": "libstarkgpu.so", "sha3-384": "libstarkgpu_sha3_384.so",
+             "sha3-512": "libstarkgpu_sha3_512.so"}
+if HASH_PROFILE not in _LIB_NAME:
+    raise ValueError(f"STARK_GPU_HASH must be one of {sorted(_LIB_NAME)}")
+HASH_BYTES = {"sha3-256": 32, "sha3-384": 48, "sha3-512": 64}[HASH_PROFILE]
+LIB_PATH = os.path.join(_HERE, _LIB_NAME[HASH_PROFILE])
 P = 0xFFFFFFFF00000001
 
 SG_OK, SG_EINVAL, SG_ECUDA, SG_ENOMEM, SG_ESPACE, SG_EVERIFY, SG_ELIMIT = 0, -1, -2, -3, -4, -5, -6
@@ -115,7 +124,7 @@ EXPORTS = (
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
-    "sg_pool_reserve",
+    "sg_pool_reserve", "sg_hash_bytes",
 )
 JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA = 1, 2, 3, 4, 5
 OPT_WIDE_MERGE = 1
@@ -154,8 +163,11 @@ def lib():
     if _lib is not None:
         return _lib
     if not os.path.exists(LIB_PATH):
-        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}`")
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE} all`")
     L = ctypes.CDLL(LIB_PATH)
+    L.sg_hash_bytes.restype = ctypes.c_int
+    if L.sg_hash_bytes() != HASH_BYTES:
+        raise ImportError(f"{LIB_PATH} is not a {HASH_PROFILE} build")
     vp, sz, u64, i32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int
     L.sg_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
     L.sg_ctx_destroy.argtypes = [vp]
@@ -875,7 +887,7 @@ class Context:
         n = cols.shape[1] if n_leaves is None else n_leaves
         cs = cols.shape[1] if col_stride is None else col_stride
         ar = np.ascontiguousarray(arities, dtype=np.uint64)
-        root = ctypes.create_string_buffer(32)
+        root = ctypes.create_string_buffer(HASH_BYTES)
         t = ctypes.c_void_p()
         self._check(self._lib.sg_merkle_commit(self._h, ip, n, width, cs, ar.ctypes.data, ar.size, tree_label, root,
                                                ctypes.byref(t) if keep else None))

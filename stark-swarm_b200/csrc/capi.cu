@@ -185,6 +185,8 @@ int sg_ctx_set_option(sg_ctx* c, int option, int64_t value) {
   return SG_EINVAL;
 }
 
+int sg_hash_bytes(void) { return kc::kHashBytes; }
+
 int sg_pool_reserve(sg_ctx* c, uint64_t bytes) {
   return guarded(c, [&] { sg::pool_reserve(c->device, bytes, c->stream); });
 }
@@ -634,6 +636,8 @@ int sg_prove_inner_shard(sg_ctx* c, const uint8_t* canon, const size_t* offsets,
                          const uint8_t salt[16], const uint8_t fs_binding[32], int stir, uint8_t* proof, size_t cap,
                          size_t* len, uint8_t pi_hash[32], uint8_t merkle_root[32]) {
   return guarded(c, [&] {
+    sg::require(kc::kHashBytes == 32, "prove_inner_shard: swarm-dns binds 32-byte proof roots; it builds with the "
+                                      "sha3-256 profile only");
     sg::require(offsets && salt && fs_binding && len && pi_hash && merkle_root && n_records > 0 &&
                     (canon || offsets[n_records] == 0),
                 "prove_inner_shard: null argument or no records");
@@ -661,6 +665,8 @@ int sg_prove_inner_shard(sg_ctx* c, const uint8_t* canon, const size_t* offsets,
 int sg_prove_outer_rollup(sg_ctx* c, const uint8_t* pi_hashes, size_t n, const uint8_t pk_hash[32], int stir,
                           uint8_t* proof, size_t cap, size_t* len) {
   return guarded(c, [&] {
+    sg::require(kc::kHashBytes == 32, "prove_outer_rollup: swarm-dns binds 32-byte proof roots; it builds with the "
+                                      "sha3-256 profile only");
     sg::require(pi_hashes && pk_hash && len && n > 0, "prove_outer_rollup: null argument or no shards");
     std::vector<uint64_t> leaves(4 * n);
     memcpy(leaves.data(), pi_hashes, 32 * n);
@@ -673,7 +679,7 @@ int sg_prove_outer_rollup(sg_ctx* c, const uint8_t* pi_hashes, size_t n, const u
 }
 
 int sg_merkle_commit(sg_ctx* c, const uint64_t* cols, size_t n_leaves, size_t width, size_t col_stride,
-                     const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t root[32], sg_tree** keep) {
+                     const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t* root, sg_tree** keep) {
   if (keep) *keep = nullptr;
   return guarded(c, [&] {
     sg::require(cols && root && arities && depth > 0 && n_leaves > 0, "merkle_commit: bad arguments");
@@ -687,11 +693,12 @@ int sg_merkle_commit(sg_ctx* c, const uint64_t* cols, size_t n_leaves, size_t wi
     sg_tree* t = new sg_tree;
     try {
       sg::require(sg::tree_plan(&t->t, n_leaves, ar, tree_label), "merkle_commit: arities do not reach the root");
-      t->buf.alloc(t->t.total_digests * 4, c->stream);
+      t->buf.alloc(t->t.total_digests * kc::kDigestLanes, c->stream);
       t->t.d = t->buf.p;
       sg::cuda_check(sg::tree_hash_leaves(t->t, di.d, (uint32_t)width, col_stride, 0, c->stream), "leaves");
       sg::cuda_check(sg::tree_hash_levels(t->t, c->stream), "levels");
-      sg::cuda_check(cudaMemcpyAsync(root, t->t.d + 4 * t->t.off.back(), 32, cudaMemcpyDeviceToHost, c->stream),
+      sg::cuda_check(cudaMemcpyAsync(root, t->t.d + kc::kDigestLanes * t->t.off.back(), kc::kHashBytes,
+                                     cudaMemcpyDeviceToHost, c->stream),
                      "d2h");
       sg::cuda_check(cudaStreamSynchronize(c->stream), "sync");
     } catch (...) {
@@ -711,18 +718,18 @@ int sg_merkle_open(sg_ctx* c, const sg_tree* tree, size_t index, uint8_t* out, s
     sg::require(index < tree->t.len[0], "merkle_open: index out of range");
     std::vector<uint64_t> idx;
     sg::opening_indices(tree->t, index, &idx);
-    sg::DBuf di(idx.size(), c->stream), dout(4 * idx.size(), c->stream);
+    sg::DBuf di(idx.size(), c->stream), dout(kc::kDigestLanes * idx.size(), c->stream);
     sg::cuda_check(cudaMemcpyAsync(di.p, idx.data(), idx.size() * 8, cudaMemcpyHostToDevice, c->stream), "h2d");
     sg::cuda_check(sg::gather_digests(tree->t.d, di.p, idx.size(), dout.p, c->stream), "gather");
-    std::vector<uint64_t> got(4 * idx.size());
+    std::vector<uint64_t> got(kc::kDigestLanes * idx.size());
     sg::cuda_check(cudaMemcpyAsync(got.data(), dout.p, got.size() * 8, cudaMemcpyDeviceToHost, c->stream), "d2h");
     sg::cuda_check(cudaStreamSynchronize(c->stream), "sync");
     sg::ByteWriter w;
     size_t pos = 0;
     auto dig = [&]() {
       sg::Digest d;
-      memcpy(d.data(), got.data() + pos, 32);
-      pos += 4;
+      memcpy(d.data(), got.data() + pos, kc::kHashBytes);
+      pos += kc::kDigestLanes;
       return d;
     };
     sg::Opening o;

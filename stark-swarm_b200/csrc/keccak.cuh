@@ -1,14 +1,18 @@
-// keccak.cuh — Keccak-f[1600] and SHA3-256 (FIPS 202) for host and device.
+// keccak.cuh — Keccak-f[1600] and SHA3-256/384/512 (FIPS 202) for host and device.
 //
 // The reference hashes every Merkle leaf/node, its transcript and its tree
-// domain tags with sha3 0.10.8's Sha3_256 (hash/src/selected.rs:100-112,
-// merkle/src/lib.rs:185-238, transcript/src/lib.rs:158-213). SHA3-256 absorbs
-// 136-byte blocks (17 lanes) and pads with 0x06 .. 0x80.
+// domain tags with the hasher its hash feature selects at compile time
+// (hash/src/selected.rs:8-48: Sha3_256, Sha3_384 or Sha3_512 from sha3 0.10.8;
+// merkle/src/lib.rs:185-238, transcript/src/lib.rs:162-212). This library does
+// the same with SG_HASH_BYTES (32, the default, 48 or 64): a d-byte SHA3 absorbs
+// 200 - 2d byte blocks (17, 13 or 9 lanes) and pads with 0x06 .. 0x80. DNS record
+// hashing and the pi_hash recipes use SHA3-256 in every build
+// (swarm-dns/src/dns.rs:17, prover.rs:207).
 //
 // On the device the 25-lane state lives in registers; each 64-bit XOR/rotate
 // lowers to 32-bit LOP3/SHF pairs, except half of the rho rotations, which are
 // written as IMAD products (4 % more permutations per second on B200). Messages in this library are built from
-// whole 64-bit lanes (32-byte labels, 8-byte field elements, 32-byte digests),
+// whole 64-bit lanes (32-byte labels, 8-byte field elements, whole-lane digests),
 // so lane-granular absorption is all the kernels need.
 #pragma once
 #include <cstdint>
@@ -20,7 +24,17 @@
 #define KC_HD inline
 #endif
 
+#ifndef SG_HASH_BYTES
+#define SG_HASH_BYTES 32
+#endif
+static_assert(SG_HASH_BYTES == 32 || SG_HASH_BYTES == 48 || SG_HASH_BYTES == 64, "SHA3-256, -384 or -512");
+
 namespace kc {
+
+// The Merkle / transcript hash profile of this build.
+constexpr int kHashBytes = SG_HASH_BYTES;
+constexpr int kDigestLanes = kHashBytes / 8;
+constexpr int kRateLanes = (200 - 2 * kHashBytes) / 8;
 
 KC_HD uint64_t rotl(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
 
@@ -155,13 +169,14 @@ KC_HD void keccak_f(uint64_t A[25]) {
 #endif
 }
 
-// Lane-granular SHA3-256 sponge: absorb whole 64-bit lanes, squeeze 4 lanes.
+// Lane-granular sponge of the build's profile: absorb whole 64-bit lanes, squeeze
+// kDigestLanes lanes.
 // The state is only ever indexed by constants (a switch on the block
 // position), so it stays in registers; when the caller's loop is unrolled the
 // position is a compile-time constant and the switch disappears.
 struct LaneSponge {
   uint64_t s[25];
-  int pos;  // lanes absorbed into the current block (0..16)
+  int pos;  // lanes absorbed into the current block (0 .. kRateLanes-1)
   KC_HD void init() {
 #pragma unroll
     for (int i = 0; i < 25; ++i) s[i] = 0;
@@ -190,34 +205,35 @@ struct LaneSponge {
   }
   KC_HD void lane(uint64_t w) {
     xor_at(pos, w);
-    if (++pos == 17) {
+    if (++pos == kRateLanes) {
       keccak_f(s);
       pos = 0;
     }
   }
-  KC_HD void finish(uint64_t out[4]) {
+  KC_HD void finish(uint64_t out[kDigestLanes]) {
     xor_at(pos, 0x06ull);
-    s[16] ^= 0x8000000000000000ull;
+    s[kRateLanes - 1] ^= 0x8000000000000000ull;
     keccak_f(s);
-    out[0] = s[0];
-    out[1] = s[1];
-    out[2] = s[2];
-    out[3] = s[3];
+#pragma unroll
+    for (int i = 0; i < kDigestLanes; ++i) out[i] = s[i];
   }
 };
 
-// Byte-granular streaming SHA3-256 for host code (transcript, domain tags).
-struct Sha3 {
+// Byte-granular streaming SHA3 with an OUT-byte digest for host code
+// (transcript, domain tags, record hashing).
+template <int OUT>
+struct Sha3T {
+  static constexpr int RATE = 200 - 2 * OUT;
   uint64_t st[25];
-  uint8_t buf[136];
+  uint8_t buf[RATE];
   size_t fill;
-  Sha3() { reset(); }
+  Sha3T() { reset(); }
   void reset() {
     memset(st, 0, sizeof st);
     fill = 0;
   }
   void block(const uint8_t* b) {
-    for (int i = 0; i < 17; ++i) {
+    for (int i = 0; i < RATE / 8; ++i) {
       uint64_t w;
       memcpy(&w, b + 8 * i, 8);
       st[i] ^= w;
@@ -227,25 +243,27 @@ struct Sha3 {
   void update(const void* data, size_t len) {
     const uint8_t* p = (const uint8_t*)data;
     while (len) {
-      size_t take = 136 - fill < len ? 136 - fill : len;
+      size_t take = RATE - fill < len ? RATE - fill : len;
       memcpy(buf + fill, p, take);
       fill += take;
       p += take;
       len -= take;
-      if (fill == 136) {
+      if (fill == (size_t)RATE) {
         block(buf);
         fill = 0;
       }
     }
   }
-  void finalize(uint8_t out[32]) const {
-    Sha3 c = *this;
-    memset(c.buf + c.fill, 0, 136 - c.fill);
+  void finalize(uint8_t out[OUT]) const {
+    Sha3T c = *this;
+    memset(c.buf + c.fill, 0, RATE - c.fill);
     c.buf[c.fill] ^= 0x06;
-    c.buf[135] ^= 0x80;
+    c.buf[RATE - 1] ^= 0x80;
     c.block(c.buf);
-    memcpy(out, c.st, 32);
+    memcpy(out, c.st, OUT);
   }
 };
+using Sha3 = Sha3T<32>;             // SHA3-256: records, pi_hash recipes
+using Sha3Sel = Sha3T<kHashBytes>;  // the profile: Merkle channel and transcript
 
 }  // namespace kc

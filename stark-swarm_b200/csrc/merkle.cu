@@ -1,4 +1,4 @@
-// merkle.cu — leaf and node hashing kernels for the SHA3-256 Merkle channel.
+// merkle.cu — leaf and node hashing kernels for the SHA3 Merkle channel.
 #include "keccak.cuh"
 #include "merkle.cuh"
 #include "counters.hpp"
@@ -29,7 +29,7 @@ bool tree_plan(DevTree* t, uint64_t n_leaves, const std::vector<uint32_t>& ariti
 }
 
 __device__ void leaf_digest_row(const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros, uint64_t i,
-                                uint64_t arity0, uint64_t label, uint64_t out[4]) {
+                                uint64_t arity0, uint64_t label, uint64_t out[kc::kDigestLanes]) {
   kc::LaneSponge sp;
   sp.init();
   sp.lane(arity0);
@@ -43,18 +43,21 @@ __device__ void leaf_digest_row(const uint64_t* cols, uint32_t w, uint64_t cs, u
 
 namespace {
 
+constexpr int DL = kc::kDigestLanes;
+
+__device__ __forceinline__ void put_digest(uint64_t* o, const uint64_t* d) {
+#pragma unroll
+  for (int q = 0; q < DL; ++q) o[q] = d[q];
+}
+
 // Generic width: runtime loop (positions resolved by the sponge's switch).
 __global__ void leaf_kernel(const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros, uint64_t n,
                             uint64_t arity0, uint64_t label, uint64_t* out) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  uint64_t d[4];
+  uint64_t d[DL];
   leaf_digest_row(cols, w, cs, zeros, i, arity0, label, d);
-  uint64_t* o = out + 4 * i;
-  o[0] = d[0];
-  o[1] = d[1];
-  o[2] = d[2];
-  o[3] = d[3];
+  put_digest(out + DL * i, d);
 }
 
 // Fixed width: fully unrolled, every lane position is a compile-time constant.
@@ -73,13 +76,9 @@ __global__ void leaf_kernel_t(const uint64_t* __restrict__ cols, uint64_t cs, ui
   for (int c = 0; c < W; ++c) sp.lane(__ldg(cols + (uint64_t)c * cs + i));
 #pragma unroll
   for (int c = 0; c < Z; ++c) sp.lane(0);
-  uint64_t d[4];
+  uint64_t d[DL];
   sp.finish(d);
-  uint64_t* o = out + 4 * i;
-  o[0] = d[0];
-  o[1] = d[1];
-  o[2] = d[2];
-  o[3] = d[3];
+  put_digest(out + DL * i, d);
 }
 
 template <int A>
@@ -95,15 +94,13 @@ __device__ __forceinline__ void node_hash(const uint64_t* child, uint64_t n_chil
   for (int k = 0; k < A; ++k) {
     uint64_t c = p * A + k;
     if (c >= n_child) c = n_child - 1;  // padding = copies of the last node
-    const uint64_t* cd = child + 4 * c;
+    const uint64_t* cd = child + DL * c;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) sp.lane(cd[q]);
+    for (int q = 0; q < DL; ++q) sp.lane(cd[q]);
   }
-  uint64_t d[4];
+  uint64_t d[DL];
   sp.finish(d);
-  uint64_t* o = parent + 4 * p;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) o[q] = d[q];
+  put_digest(parent + DL * p, d);
 }
 
 template <int A>
@@ -124,19 +121,13 @@ __device__ void node_hash_any(const uint64_t* child, uint64_t n_child, uint64_t*
   for (uint32_t k = 0; k < arity; ++k) {
     uint64_t c = p * arity + k;
     if (c >= n_child) c = n_child - 1;  // padding = copies of the last node
-    const uint64_t* cd = child + 4 * c;
-    sp.lane(cd[0]);
-    sp.lane(cd[1]);
-    sp.lane(cd[2]);
-    sp.lane(cd[3]);
+    const uint64_t* cd = child + DL * c;
+#pragma unroll
+    for (int q = 0; q < DL; ++q) sp.lane(cd[q]);
   }
-  uint64_t d[4];
+  uint64_t d[DL];
   sp.finish(d);
-  uint64_t* o = parent + 4 * p;
-  o[0] = d[0];
-  o[1] = d[1];
-  o[2] = d[2];
-  o[3] = d[3];
+  put_digest(parent + DL * p, d);
 }
 
 __global__ void node_kernel(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t n_parent,
@@ -160,8 +151,8 @@ struct TopLevels {
 
 __global__ void __launch_bounds__(kTopThreads) tree_top_kernel(uint64_t* d, TopLevels tl, uint64_t label) {
   for (int k = 0; k < tl.n; ++k) {
-    const uint64_t* ch = d + 4 * tl.child_off[k];
-    uint64_t* par = d + 4 * tl.parent_off[k];
+    const uint64_t* ch = d + DL * tl.child_off[k];
+    uint64_t* par = d + DL * tl.parent_off[k];
     for (uint64_t p = threadIdx.x; p < tl.n_parent[k]; p += kTopThreads) {
       switch (tl.arity[k]) {
         case 2: node_hash<2>(ch, tl.n_child[k], par, p, tl.level[k], label); break;
@@ -177,8 +168,8 @@ __global__ void __launch_bounds__(kTopThreads) tree_top_kernel(uint64_t* d, TopL
 
 __global__ void gather_digests_kernel(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out) {
   uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (e >= 4 * n) return;
-  out[e] = d[4 * idx[e >> 2] + (e & 3)];
+  if (e >= DL * n) return;
+  out[e] = d[DL * idx[e / DL] + e % DL];
 }
 
 __global__ void gather_u64_kernel(const uint64_t* src, const uint64_t* idx, uint64_t n, uint64_t* out) {
@@ -230,8 +221,8 @@ cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
       tree_top_kernel<<<1, kTopThreads, 0, s>>>(t.d, tl, t.label);
       return cudaGetLastError();
     }
-    const uint64_t* ch = t.d + 4 * t.off[l];
-    uint64_t* par = t.d + 4 * t.off[l + 1];
+    const uint64_t* ch = t.d + DL * t.off[l];
+    uint64_t* par = t.d + DL * t.off[l + 1];
     const unsigned B = blocks_for(np, 128);
     SG_LAUNCH_SCOPE("merkle_nodes", s);
     switch (t.arity[l]) {
@@ -248,7 +239,7 @@ cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
 cudaError_t gather_digests(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
   SG_LAUNCH_SCOPE("gather", s);
-  gather_digests_kernel<<<blocks_for(4 * n, 256), 256, 0, s>>>(d, idx, n, out);
+  gather_digests_kernel<<<blocks_for(DL * n, 256), 256, 0, s>>>(d, idx, n, out);
   return cudaGetLastError();
 }
 

@@ -1,4 +1,5 @@
-// merkle.cuh — device SHA3-256 Merkle trees with the reference's DsLabel framing.
+// merkle.cuh — device SHA3 Merkle trees (the build's hash profile) with the
+// reference's DsLabel framing.
 //
 // merkle/src/lib.rs:95-113 DsLabel = le64(arity) || le64(level) || le64(pos) || le64(label)
 //   leaf  = SHA3(DsLabel{arities[0], u32::MAX, i, label} || le64 values)      (:185-217)
@@ -13,6 +14,8 @@
 #include <vector>
 #include <cuda_runtime.h>
 
+#include "keccak.cuh"
+
 namespace sg {
 
 struct DevTree {
@@ -21,7 +24,7 @@ struct DevTree {
   std::vector<uint32_t> arity;       // arity[l]: children per parent from level l to l+1
   std::vector<uint64_t> len;         // logical length of each level (len.back() == 1)
   std::vector<uint64_t> off;         // digest offset of each level inside `d`
-  uint64_t* d = nullptr;             // all levels, 4 lanes (32 bytes) per digest
+  uint64_t* d = nullptr;             // all levels, kc::kDigestLanes lanes per digest
   uint64_t total_digests = 0;
   bool owns = false;
 };
@@ -37,7 +40,7 @@ cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w,
                              cudaStream_t s);
 // Hash levels 1..depth from level 0.
 cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s);
-// Copy digests at the given global digest indices into out (4 lanes each).
+// Copy digests at the given global digest indices into out (kc::kDigestLanes lanes each).
 cudaError_t gather_digests(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s);
 // Gather u64 values src[idx[i]] into out.
 cudaError_t gather_u64(const uint64_t* src, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s);
@@ -45,7 +48,7 @@ cudaError_t gather_u64(const uint64_t* src, const uint64_t* idx, uint64_t n, uin
 // Device-side leaf hash used by fused kernels (fold writes the next layer's leaves).
 #if defined(__CUDACC__)
 __device__ void leaf_digest_row(const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros, uint64_t i,
-                                uint64_t arity0, uint64_t label, uint64_t out[4]);
+                                uint64_t arity0, uint64_t label, uint64_t out[kc::kDigestLanes]);
 #endif
 
 // Host-side list of the global digest indices that make up opening `index`:

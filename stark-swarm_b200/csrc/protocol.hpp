@@ -24,10 +24,10 @@
 
 namespace sg {
 
-using Digest = std::array<uint8_t, 32>;
+using Digest = std::array<uint8_t, kc::kHashBytes>;  // the build's hash profile
 
 struct HostTranscript {
-  kc::Sha3 h;
+  kc::Sha3Sel h;  // new_matching_hash (transcript/src/lib.rs:338-344)
   explicit HostTranscript(const char* label) {
     static const char kInit[] = "FSv1-TRANSCRIPT-INIT";
     h.update(kInit, sizeof kInit - 1);
@@ -48,18 +48,18 @@ struct HostTranscript {
   void absorb_ext(const gl::Fp6& e) {
     for (int i = 0; i < 6; ++i) absorb_field(e.c[i]);
   }
-  void challenge_bytes(const std::string& label, uint8_t out[32]) const {
+  void challenge_bytes(const std::string& label, uint8_t out[kc::kHashBytes]) const {
     static const char kCh[] = "FSv1-CHALLENGE";
-    kc::Sha3 c = h;
+    kc::Sha3Sel c = h;
     c.update(kCh, sizeof kCh - 1);
     c.update(label.data(), label.size());
     c.finalize(out);
   }
   uint64_t challenge_field(const std::string& label) const {
-    uint8_t d[32];
+    uint8_t d[kc::kHashBytes];
     challenge_bytes(label, d);
     uint64_t acc = 0;
-    for (int end = 32; end > 0;) {
+    for (int end = kc::kHashBytes; end > 0;) {
       int start = end >= 7 ? end - 7 : 0, len = end - start;
       uint64_t v = 0;
       for (int i = 0; i < len; ++i) v |= (uint64_t)d[start + i] << (8 * i);
@@ -305,10 +305,10 @@ struct ByteReader {
     return x;
   }
   Digest dig() {
-    need(32);
+    need(kc::kHashBytes);
     Digest d;
-    memcpy(d.data(), p + o, 32);
-    o += 32;
+    memcpy(d.data(), p + o, kc::kHashBytes);
+    o += kc::kHashBytes;
     return d;
   }
   uint64_t fe() {

@@ -200,12 +200,15 @@ void merge_device(sg_ctx* c, int air, const uint64_t* d_lde, uint64_t w, uint64_
 // ------------------------------------------------------------------ STIR
 namespace {
 
+constexpr int DL = kc::kDigestLanes;  // u64 lanes per digest of the build's hash profile
+constexpr int HB = kc::kHashBytes;
+
 struct Tree {
   DevTree t;
   DBuf buf;
   void make(uint64_t n, const std::vector<uint32_t>& ar, uint64_t label, cudaStream_t s) {
     require(tree_plan(&t, n, ar, label), "merkle: arity schedule does not reach the root");
-    buf.alloc(t.total_digests * 4, s);
+    buf.alloc(t.total_digests * DL, s);
     t.d = buf.p;
   }
 };
@@ -218,7 +221,7 @@ void d2h(std::vector<T>* v, const uint64_t* src, size_t elems, cudaStream_t s) {
 
 Digest digest_at(const std::vector<uint64_t>& h, size_t lane0) {
   Digest d;
-  memcpy(d.data(), h.data() + lane0, 32);
+  memcpy(d.data(), h.data() + lane0, HB);
   return d;
 }
 
@@ -247,10 +250,10 @@ std::vector<uint8_t> classic_prove_device(sg_ctx* c, const uint64_t* d_f0, uint6
   cuda_check(tree_hash_leaves(f0t.t, d_f0, 1, n0, 0, s), "f0 leaves");
   cuda_check(tree_hash_levels(f0t.t, s), "f0 levels");
   std::vector<uint64_t> h;
-  d2h(&h, f0t.t.d + 4 * f0t.t.off.back(), 4, s);
+  d2h(&h, f0t.t.d + DL * f0t.t.off.back(), DL, s);
   cuda_check(cudaStreamSynchronize(s), "sync");
   pr.root_f0 = digest_at(h, 0);
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), HB);
   const gl::Fp6 z = tr.challenge_ext("z_fp3");
 
   const uint64_t work = std::max<uint64_t>(n0, 6 * sizes[1]);
@@ -312,19 +315,19 @@ std::vector<uint8_t> classic_prove_device(sg_ctx* c, const uint64_t* d_f0, uint6
       cuda_check(tree_hash_levels(ctree.t, s), "coeff levels");
     }
     std::vector<uint64_t> root, croot, tup;
-    d2h(&root, trees[ell].t.d + 4 * trees[ell].t.off.back(), 4, s);
+    d2h(&root, trees[ell].t.d + DL * trees[ell].t.off.back(), DL, s);
     if (last_cc) {
-      d2h(&croot, ctree.t.d + 4 * ctree.t.off.back(), 4, s);
+      d2h(&croot, ctree.t.d + DL * ctree.t.off.back(), DL, s);
       d2h(&tup, tuples.p, 6 * m * nn, s);
     }
     cuda_check(cudaStreamSynchronize(s), "sync");
     pr.roots.push_back(digest_at(root, 0));
     tr.absorb_ext(fz);
-    tr.absorb_bytes(pr.roots.back().data(), 32);
+    tr.absorb_bytes(pr.roots.back().data(), HB);
     if (last_cc) {
       pr.has_ct = pr.has_croot = true;
       pr.coeff_root = digest_at(croot, 0);
-      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      tr.absorb_bytes(pr.coeff_root.data(), HB);
       alpha = tr.challenge_ext("alpha");
       (void)tr.challenge_ext("beta_deg");
       pr.coeff_tuples.assign(nn, std::vector<gl::Fp6>(m));
@@ -371,12 +374,12 @@ std::vector<uint8_t> classic_prove_device(sg_ctx* c, const uint64_t* d_f0, uint6
   auto gather_openings = [&](const DevTree& t, const std::vector<uint64_t>& idx) {
     std::vector<uint64_t> di;
     for (uint64_t i : idx) opening_indices(t, i, &di);
-    DBuf d_i(di.size(), s), d_o(4 * di.size(), s);
+    DBuf d_i(di.size(), s), d_o(DL * di.size(), s);
     std::vector<uint64_t> got;
     if (!di.empty()) {
       cuda_check(cudaMemcpyAsync(d_i.p, di.data(), di.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
       cuda_check(gather_digests(t.d, d_i.p, di.size(), d_o.p, s), "gather paths");
-      d2h(&got, d_o.p, 4 * di.size(), s);
+      d2h(&got, d_o.p, DL * di.size(), s);
     }
     cuda_check(cudaStreamSynchronize(s), "sync");
     std::vector<Opening> out;
@@ -385,12 +388,12 @@ std::vector<uint8_t> classic_prove_device(sg_ctx* c, const uint64_t* d_f0, uint6
       Opening o;
       o.index = i;
       o.leaf = digest_at(got, pos);
-      pos += 4;
+      pos += DL;
       for (size_t l = 0; l + 1 < t.len.size(); ++l) {
         std::vector<Digest> sib(t.arity[l] - 1);
         for (auto& d : sib) {
           d = digest_at(got, pos);
-          pos += 4;
+          pos += DL;
         }
         o.path.push_back(std::move(sib));
       }
@@ -471,10 +474,10 @@ std::vector<uint8_t> stir_prove_on_stream(sg_ctx* c, const uint64_t* d_f0, uint6
   cuda_check(tree_hash_leaves(f0t.t, d_f0, (uint32_t)m0, nn0, 0, s), "f0 leaves");
   cuda_check(tree_hash_levels(f0t.t, s), "f0 levels");
   std::vector<uint64_t> h;
-  d2h(&h, f0t.t.d + 4 * f0t.t.off.back(), 4, s);
+  d2h(&h, f0t.t.d + DL * f0t.t.off.back(), DL, s);
   cuda_check(cudaStreamSynchronize(s), "sync");
   pr.root_f0 = digest_at(h, 0);
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), HB);
   const gl::Fp6 z = tr.challenge_ext("z_fp3");
 
   const uint64_t work = std::max<uint64_t>(n0, 6 * sizes[1]);
@@ -543,9 +546,9 @@ std::vector<uint8_t> stir_prove_on_stream(sg_ctx* c, const uint64_t* d_f0, uint6
 
     std::vector<uint64_t> ev, root, croot, tup;
     d2h(&ev, evals.p, m * 6, s);
-    d2h(&root, trees[ell].t.d + 4 * trees[ell].t.off.back(), 4, s);
+    d2h(&root, trees[ell].t.d + DL * trees[ell].t.off.back(), DL, s);
     if (last_cc) {
-      d2h(&croot, ctree.t.d + 4 * ctree.t.off.back(), 4, s);
+      d2h(&croot, ctree.t.d + DL * ctree.t.off.back(), DL, s);
       d2h(&tup, tuples.p, 6 * m * nn, s);
     }
     cuda_check(cudaStreamSynchronize(s), "sync");
@@ -556,12 +559,12 @@ std::vector<uint8_t> stir_prove_on_stream(sg_ctx* c, const uint64_t* d_f0, uint6
     for (auto& e : evs) tr.absorb_ext(e);
     pr.coset_evals.push_back(std::move(evs));
     pr.roots.push_back(digest_at(root, 0));
-    tr.absorb_bytes(pr.roots.back().data(), 32);
+    tr.absorb_bytes(pr.roots.back().data(), HB);
     zc = gl::e_pow(zc, m);
     if (last_cc) {
       pr.has_ct = pr.has_croot = true;
       pr.coeff_root = digest_at(croot, 0);
-      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      tr.absorb_bytes(pr.coeff_root.data(), HB);
       alpha = tr.challenge_ext("alpha");
       (void)tr.challenge_ext("beta_deg");
       pr.coeff_tuples.assign(nn, std::vector<gl::Fp6>(m));
@@ -616,14 +619,14 @@ std::vector<uint8_t> stir_prove_on_stream(sg_ctx* c, const uint64_t* d_f0, uint6
   idx_all.insert(idx_all.end(), dig_idx1.begin(), dig_idx1.end());
   for (uint64_t q = 0; q < (L >= 2 ? p.s0 : 0); ++q)
     for (int k = 0; k < 6; ++k) idx_all.push_back((uint64_t)k * sizes[1] + qs[q].base);
-  DBuf d_idx(idx_all.size(), s), d_out(nv + 4 * (nd0 + nd1) + n_next, s);
+  DBuf d_idx(idx_all.size(), s), d_out(nv + DL * (nd0 + nd1) + n_next, s);
   if (!idx_all.empty()) {
     cuda_check(cudaMemcpyAsync(d_idx.p, idx_all.data(), idx_all.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
     cuda_check(gather_u64(d_f0, d_idx.p, nv, d_out.p, s), "gather values");
     cuda_check(gather_digests(f0t.t.d, d_idx.p + nv, nd0, d_out.p + nv, s), "gather f0 paths");
     if (L >= 2) {
-      cuda_check(gather_digests(trees[1].t.d, d_idx.p + nv + nd0, nd1, d_out.p + nv + 4 * nd0, s), "gather l1");
-      cuda_check(gather_u64(planes[1].p, d_idx.p + nv + nd0 + nd1, n_next, d_out.p + nv + 4 * (nd0 + nd1), s),
+      cuda_check(gather_digests(trees[1].t.d, d_idx.p + nv + nd0, nd1, d_out.p + nv + DL * nd0, s), "gather l1");
+      cuda_check(gather_u64(planes[1].p, d_idx.p + nv + nd0 + nd1, n_next, d_out.p + nv + DL * (nd0 + nd1), s),
                  "gather f1");
     }
   }
@@ -631,17 +634,17 @@ std::vector<uint8_t> stir_prove_on_stream(sg_ctx* c, const uint64_t* d_f0, uint6
   d2h(&got, d_out.p, d_out.n, s);
   cuda_check(cudaStreamSynchronize(s), "sync");
 
-  size_t pv = 0, p0 = nv, p1 = nv + 4 * nd0, pn = nv + 4 * (nd0 + nd1);
+  size_t pv = 0, p0 = nv, p1 = nv + DL * nd0, pn = nv + DL * (nd0 + nd1);
   auto take_opening = [&](const DevTree& t, uint64_t index, size_t* pos) {
     Opening o;
     o.index = index;
     o.leaf = digest_at(got, *pos);
-    *pos += 4;
+    *pos += DL;
     for (size_t l = 0; l + 1 < t.len.size(); ++l) {
       std::vector<Digest> sib(t.arity[l] - 1);
       for (auto& d : sib) {
         d = digest_at(got, *pos);
-        *pos += 4;
+        *pos += DL;
       }
       o.path.push_back(std::move(sib));
     }

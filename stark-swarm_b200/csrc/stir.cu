@@ -236,10 +236,10 @@ __global__ void fold_kernel(FoldArgs a) {
     sp.lane(a.leaf_label);
 #pragma unroll
     for (int q = 0; q < 6; ++q) sp.lane(acc.c[q]);
-    uint64_t d[4];
+    uint64_t d[kc::kDigestLanes];
     sp.finish(d);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a.leaves[4 * b + i] = d[i];
+    for (int i = 0; i < kc::kDigestLanes; ++i) a.leaves[kc::kDigestLanes * b + i] = d[i];
   }
 }
 
@@ -304,10 +304,10 @@ __global__ void fold_small_kernel(FoldArgs a) {
     sp.lane(a.leaf_label);
 #pragma unroll
     for (int q = 0; q < 6; ++q) sp.lane(acc.c[q]);
-    uint64_t d[4];
+    uint64_t d[kc::kDigestLanes];
     sp.finish(d);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) a.leaves[4 * b + i] = d[i];
+    for (int i = 0; i < kc::kDigestLanes; ++i) a.leaves[kc::kDigestLanes * b + i] = d[i];
   }
 }
 

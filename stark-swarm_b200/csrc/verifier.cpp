@@ -92,7 +92,7 @@ Fp6 eval_poly(const std::vector<Fp6>& c, const Fp6& x) {
 }
 
 Digest leaf_hash(uint64_t arity0, uint64_t label, uint64_t pos, const uint64_t* v, size_t n) {
-  kc::Sha3 h;
+  kc::Sha3Sel h;
   uint64_t ds[4] = {arity0, 0xFFFFFFFFull, pos, label};
   h.update(ds, 32);
   h.update(v, 8 * n);
@@ -107,16 +107,16 @@ bool verify_opening(const std::vector<uint32_t>& ar, uint64_t label, const Diges
   for (size_t lv = 0; lv < o.path.size(); ++lv) {
     if (lv >= ar.size()) return false;
     uint64_t a = ar[lv], pos = idx % a;
-    kc::Sha3 h;
+    kc::Sha3Sel h;
     uint64_t ds[4] = {a, lv + 1, idx / a, label};
     h.update(ds, 32);
     size_t k = 0;
     for (uint64_t i = 0; i < a; ++i) {
       if (i == pos) {
-        h.update(cur.data(), 32);
+        h.update(cur.data(), kc::kHashBytes);
       } else {
         if (k >= o.path[lv].size()) return false;
-        h.update(o.path[lv][k++].data(), 32);
+        h.update(o.path[lv][k++].data(), kc::kHashBytes);
       }
     }
     h.finalize(cur.data());
@@ -135,10 +135,10 @@ Digest tree_root_host(const std::vector<std::vector<uint64_t>>& leaves, const st
     while (lv.size() % a) lv.push_back(lv.back());
     std::vector<Digest> par(lv.size() / a);
     for (size_t p = 0; p < par.size(); ++p) {
-      kc::Sha3 h;
+      kc::Sha3Sel h;
       uint64_t ds[4] = {a, level + 1, p, label};
       h.update(ds, 32);
-      for (uint64_t k = 0; k < a; ++k) h.update(lv[p * a + k].data(), 32);
+      for (uint64_t k = 0; k < a; ++k) h.update(lv[p * a + k].data(), kc::kHashBytes);
       h.finalize(par[p].data());
     }
     lv.swap(par);
@@ -194,7 +194,7 @@ bool classic_verify(const StirProof& pr, const sg_fri_params& p, const std::vect
   if (pr.stir || pr.roots.size() < L || pr.fz.size() < L) return false;
   HostTranscript tr("FRI/FS");
   bind_statement(tr, p, pr.n0);
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), kc::kHashBytes);
   const Fp6 z = tr.challenge_ext("z_fp3");
   Fp6 beta = gl::e_zero();
   std::vector<Fp6> alphas;
@@ -202,10 +202,10 @@ bool classic_verify(const StirProof& pr, const sg_fri_params& p, const std::vect
     const bool last_cc = use_cc && ell == L - 1;
     if (!last_cc) alphas.push_back(tr.challenge_ext("alpha"));
     tr.absorb_ext(pr.fz[ell]);
-    tr.absorb_bytes(pr.roots[ell].data(), 32);
+    tr.absorb_bytes(pr.roots[ell].data(), kc::kHashBytes);
     if (last_cc) {
       if (!pr.has_croot) return false;
-      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      tr.absorb_bytes(pr.coeff_root.data(), kc::kHashBytes);
       alphas.push_back(tr.challenge_ext("alpha"));
       beta = tr.challenge_ext("beta_deg");
     }
@@ -283,7 +283,7 @@ bool stir_verify(const StirProof& pr, const sg_fri_params& p) {
   if (!pr.stir || pr.roots.size() < L || pr.coset_evals.size() < L) return false;
   HostTranscript tr("FRI/FS");
   bind_statement(tr, p, pr.n0);
-  tr.absorb_bytes(pr.root_f0.data(), 32);
+  tr.absorb_bytes(pr.root_f0.data(), kc::kHashBytes);
   const Fp6 z = tr.challenge_ext("z_fp3");
   Fp6 zc = z, beta = gl::e_zero();
   std::vector<std::vector<Fp6>> interps;
@@ -300,10 +300,10 @@ bool stir_verify(const StirProof& pr, const sg_fri_params& p) {
     interps.push_back(std::move(ip));
     zc = gl::e_pow(zc, m);
     for (auto& e : ev) tr.absorb_ext(e);
-    tr.absorb_bytes(pr.roots[ell].data(), 32);
+    tr.absorb_bytes(pr.roots[ell].data(), kc::kHashBytes);
     if (last_cc) {
       if (!pr.has_croot) return false;
-      tr.absorb_bytes(pr.coeff_root.data(), 32);
+      tr.absorb_bytes(pr.coeff_root.data(), kc::kHashBytes);
       alphas.push_back(tr.challenge_ext("alpha"));
       beta = tr.challenge_ext("beta_deg");
     }

@@ -12,7 +12,12 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
-ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+# The hash profile (the reference's compile-time sha3-256 / sha3-384 / sha3-512
+# feature) is chosen per process, as the library's is: STARK_GPU_HASH.
+HASH_PROFILE = os.environ.get("STARK_GPU_HASH", "sha3-256")
+_SO_NAME = {"sha3-256": "liboracle.so", "sha3-384": "liboracle_sha3_384.so", "sha3-512": "liboracle_sha3_512.so"}
+ORACLE_SO = os.path.join(ORACLE_DIR, _SO_NAME[HASH_PROFILE])
+HASH_BYTES = {"sha3-256": 32, "sha3-384": 48, "sha3-512": 64}[HASH_PROFILE]
 P = 0xFFFFFFFF00000001
 
 PHI_PARALLEL_GATE, PHI_ALWAYS, PHI_NEVER = 0, 1, 2
@@ -55,6 +60,7 @@ def lib():
         if _lib is None:
             subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
             L = ctypes.CDLL(ORACLE_SO)
+            assert L.orc_hash_bytes() == HASH_BYTES, "oracle library of another hash profile"
             L.orc_fp_add.restype = L.orc_fp_sub.restype = L.orc_fp_mul.restype = ctypes.c_uint64
             L.orc_fp_pow.restype = L.orc_fp_inv.restype = ctypes.c_uint64
             for f in ("orc_fp_add", "orc_fp_sub", "orc_fp_mul", "orc_fp_pow"):
@@ -136,7 +142,7 @@ def poly_div_zh(coeffs, m):
 def merkle_root(rows: np.ndarray, arities, label: int) -> bytes:
     rows = np.ascontiguousarray(rows, dtype=np.uint64)
     ar = np.ascontiguousarray(arities, dtype=np.uint64)
-    out = ctypes.create_string_buffer(32)
+    out = ctypes.create_string_buffer(HASH_BYTES)
     rc = lib().orc_merkle_root(_ptr(rows), rows.shape[0], rows.shape[1], _ptr(ar), ar.size, label, out)
     assert rc == 0, rc
     return out.raw
