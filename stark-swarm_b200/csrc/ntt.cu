@@ -87,6 +87,7 @@ struct PassArgs {
   int sparse_nz;
   int tw_log;                 // > 0: output (lane, i) *= w_{2^tw_log}^(i*lane)
   int in_tw_log;              // > 0: input (lane, m) *= w_{2^in_tw_log}^(m*lane)
+  int out_i_log;              // coset evaluation: out_i = 2^out_i_log
   uint64_t scale;             // != 1: outputs *= scale
   const uint64_t* tw_st;      // w_4096^i (direction of the transform)
   const uint64_t* tw_lo;      // w28^i
@@ -238,16 +239,19 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       const uint64_t lane = lane0 + l;
       const uint64_t flat = (uint64_t)m * a.in_m + lane * a.flat_lane;
       x[q] = 0;
-      if (e < E_load && lane < a.n_lanes && flat < a.in_valid) {
+      if constexpr (COSET) {
+        // one column's cosets: point m of every lane is in[m], all lanes valid
+        // (ntt_coset_eval launches exactly B / K CTAs per column)
+        x[q] = __ldg(in + m);
+        if (a.pre.lo) x[q] = gl::mul(x[q], pow_at(a.pre, (uint64_t)m));
+        // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j)
+        const uint64_t ex = (uint64_t)m * lane;
+        x[q] = gl::mul(x[q], a.in_tw_log <= kTwSplit
+                                 ? __ldg(a.tw_hi + ((ex << (kTwSplit - a.in_tw_log)) & (kTwEntries - 1)))
+                                 : tw_pow(a.tw_lo, a.tw_hi, ex, a.in_tw_log));
+      } else if (e < E_load && lane < a.n_lanes && flat < a.in_valid) {
         x[q] = __ldg(in + lane * a.in_lane + (uint64_t)m * a.in_m);
         if (a.pre.lo) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
-        if constexpr (COSET) {
-          // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j)
-          const uint64_t e = (uint64_t)m * lane;
-          x[q] = gl::mul(x[q], a.in_tw_log <= kTwSplit
-                                   ? __ldg(a.tw_hi + ((e << (kTwSplit - a.in_tw_log)) & (kTwEntries - 1)))
-                                   : tw_pow(a.tw_lo, a.tw_hi, e, a.in_tw_log));
-        }
       }
     }
 #pragma unroll
@@ -323,7 +327,10 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       int l, i;
       out_pos(t + (q0 + q) * T, l, i);
       const uint64_t lane = lane0 + l;
-      if (lane < a.n_lanes) out[lane * a.out_lane + (uint64_t)i * a.out_i] = x[q];
+      if constexpr (COSET)
+        out[lane + ((uint64_t)i << a.out_i_log)] = x[q];  // point B i + t of the column
+      else if (lane < a.n_lanes)
+        out[lane * a.out_lane + (uint64_t)i * a.out_i] = x[q];
     }
   }
 }
@@ -495,6 +502,7 @@ cudaError_t ntt_coset_eval(const NttTables& t, const uint64_t* coef, uint64_t* o
   a.in_m = 1;
   a.out_lane = 1;
   a.out_i = B;
+  a.out_i_log = log_b;
   a.n_lanes = B;
   a.flat_lane = 0;
   a.in_valid = M;
