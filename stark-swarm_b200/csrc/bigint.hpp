@@ -55,7 +55,18 @@ inline void divmod(const uint32_t* u, int m, const uint32_t* v, int n, uint32_t*
     return;
   }
   const int s = __builtin_clz(v[n - 1]);
-  std::vector<uint32_t> vn(n), un(m + 1);
+  // normalised copies on the stack for the sizes the witness builders use
+  // (up to 4096-bit dividends), on the heap beyond
+  uint32_t vn_small[64], un_small[129];
+  std::vector<uint32_t> vn_big, un_big;
+  uint32_t* vn = vn_small;
+  uint32_t* un = un_small;
+  if (n > 64 || m + 1 > 129) {
+    vn_big.resize(n);
+    un_big.resize(m + 1);
+    vn = vn_big.data();
+    un = un_big.data();
+  }
   for (int i = n - 1; i > 0; --i) vn[i] = s ? (v[i] << s | v[i - 1] >> (32 - s)) : v[i];
   vn[0] = v[0] << s;
   un[m] = s ? u[m - 1] >> (32 - s) : 0;

@@ -11,7 +11,9 @@
 #include "p256.hpp"
 
 #include <cstring>
+#include <exception>
 #include <mutex>
+#include <thread>
 
 #include "bigint.hpp"
 #include "context.hpp"
@@ -436,14 +438,16 @@ void chain_witness(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_
   check_point(base[1][0], base[1][1]);
   rows->assign(k, RowW{});
   gw->assign(k * NG, GadgetW{});
-  std::vector<U> val(L.width);
   U acc[2][3];
   memcpy(acc, base, sizeof acc);
-  for (uint64_t r = 0; r < k; ++r) {
-    RowW& rw = (*rows)[r];
-    GadgetW* g = gw->data() + r * NG;
-    for (int c = 0; c < 2; ++c) {
-      const Chain& C = B.ch[c];
+  // The two chains share no cells or gadgets, so chain A runs on a second host
+  // thread while this one builds chain B (each fills its own fields of the rows).
+  auto run_chain = [&](int c) {
+    const Chain& C = B.ch[c];
+    std::vector<U> val(L.width);
+    for (uint64_t r = 0; r < k; ++r) {
+      RowW& rw = (*rows)[r];
+      GadgetW* g = gw->data() + r * NG;
       const uint8_t bit = (c == 0 ? a_bits : b_bits)[r] ? 1 : 0;
       rw.bit[c] = bit;
       for (int x = 0; x < 3; ++x) {
@@ -463,7 +467,24 @@ void chain_witness(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_
         acc[c][x] = chosen;
       }
     }
+  };
+  std::exception_ptr err_a;
+  std::thread ta([&] {
+    try {
+      run_chain(0);
+    } catch (...) {
+      err_a = std::current_exception();
+    }
+  });
+  std::exception_ptr err_b;
+  try {
+    run_chain(1);
+  } catch (...) {
+    err_b = std::current_exception();
   }
+  ta.join();
+  if (err_a) std::rethrow_exception(err_a);
+  if (err_b) std::rethrow_exception(err_b);
   for (int c = 0; c < 2; ++c)
     for (int x = 0; x < 3; ++x) limbs(acc[c][x], r_proj[3 * c + x]);
 }
