@@ -84,6 +84,17 @@ struct Out {
 
 namespace sg {
 
+void* pinned_host(sg_ctx* c, size_t bytes) {
+  if (c->pinned_bytes >= bytes) return c->pinned;
+  cuda_check(cudaStreamSynchronize(c->stream), "sync");  // no copy from the old buffer in flight
+  if (c->pinned) cudaFreeHost(c->pinned);
+  c->pinned = nullptr;
+  c->pinned_bytes = 0;
+  cuda_check(cudaHostAlloc(&c->pinned, bytes, cudaHostAllocDefault), "pinned host allocation");
+  c->pinned_bytes = bytes;
+  return c->pinned;
+}
+
 void pool_reserve(int device, uint64_t bytes, cudaStream_t s) {
   cuda_check(cudaSetDevice(device), "set device");
   cudaMemPool_t pool;
@@ -164,6 +175,7 @@ void sg_ctx_destroy(sg_ctx* c) {
   }
   if (c->stir_in) cudaEventDestroy(c->stir_in);
   if (c->stir_out) cudaEventDestroy(c->stir_out);
+  if (c->pinned) cudaFreeHost(c->pinned);
   delete c;
 }
 
@@ -526,10 +538,10 @@ int sg_p256_chain_trace(const uint8_t ax[32], const uint8_t ay[32], const uint8_
                         const uint8_t by[32], const uint8_t* b_bits, size_t k, uint64_t* trace, size_t cap) {
   if (!ax || !ay || !a_bits || !bx || !by || !b_bits || k < 2 || (k & (k - 1)) || k > 65536) return SG_EINVAL;
   try {
-    std::vector<sg::p256::RowW> rows;
-    std::vector<sg::p256::GadgetW> gw;
+    std::vector<sg::p256::RowW> rows(k);
+    std::vector<sg::p256::GadgetW> gw(k * sg::p256::layout().table.size());
     uint32_t rproj[6][sg::p256::NL];
-    sg::p256::chain_witness(ax, ay, a_bits, bx, by, b_bits, k, &rows, &gw, rproj);
+    sg::p256::chain_witness(ax, ay, a_bits, bx, by, b_bits, k, rows.data(), gw.data(), rproj);
     if (!trace || (uint64_t)sg::p256::layout().width * k > cap) return SG_ESPACE;
     sg::p256::expand_host(rows.data(), gw.data(), rproj, k, trace);
     return SG_OK;

@@ -27,6 +27,9 @@ struct sg_ctx {
   // phase of a proof and the two events that order it after and before `stream`.
   cudaStream_t stir_stream = nullptr;
   cudaEvent_t stir_in = nullptr, stir_out = nullptr;
+  // grow-only pinned host staging for witnesses copied to the device (pinned_host)
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
   std::string err;
 };
 
@@ -82,6 +85,10 @@ struct DBuf {
 };
 
 bool is_device_ptr(const void* p);
+
+// The context's pinned host staging buffer, grown to at least `bytes`. Earlier
+// contents are not kept; the caller synchronises its stream before the next use.
+void* pinned_host(sg_ctx* c, size_t bytes);
 
 // sg_pool_reserve: grow the device's default pool to `bytes` (best effort).
 void pool_reserve(int device, uint64_t bytes, cudaStream_t s);

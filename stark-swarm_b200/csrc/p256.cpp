@@ -428,16 +428,16 @@ void check_point(const U& x, const U& y) {
 const Layout& layout() { return built().L; }
 
 void chain_witness(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits, const uint8_t bx[32],
-                   const uint8_t by[32], const uint8_t* b_bits, uint64_t k, std::vector<RowW>* rows,
-                   std::vector<GadgetW>* gw, uint32_t r_proj[6][NL]) {
+                   const uint8_t by[32], const uint8_t* b_bits, uint64_t k, RowW* rows, GadgetW* gw,
+                   uint32_t r_proj[6][NL]) {
   const Built& B = built();
   const Layout& L = B.L;
   const uint32_t NG = (uint32_t)L.table.size();
   U base[2][3] = {{from_be(ax), from_be(ay), U{{1}}}, {from_be(bx), from_be(by), U{{1}}}};
   check_point(base[0][0], base[0][1]);
   check_point(base[1][0], base[1][1]);
-  rows->assign(k, RowW{});
-  gw->assign(k * NG, GadgetW{});
+  memset(rows, 0, k * sizeof(RowW));
+  memset(gw, 0, k * NG * sizeof(GadgetW));
   U acc[2][3];
   memcpy(acc, base, sizeof acc);
   // The two chains share no cells or gadgets, so chain A runs on a second host
@@ -446,8 +446,8 @@ void chain_witness(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_
     const Chain& C = B.ch[c];
     std::vector<U> val(L.width);
     for (uint64_t r = 0; r < k; ++r) {
-      RowW& rw = (*rows)[r];
-      GadgetW* g = gw->data() + r * NG;
+      RowW& rw = rows[r];
+      GadgetW* g = gw + r * NG;
       const uint8_t bit = (c == 0 ? a_bits : b_bits)[r] ? 1 : 0;
       rw.bit[c] = bit;
       for (int x = 0; x < 3; ++x) {

@@ -94,12 +94,13 @@ const Layout& layout();
 
 // The per-row witnesses of the two chains: each starts at (x, y, 1) of its affine
 // point (32-byte big-endian coordinates) and takes one bit per row (k rows).
-// Fills rows (k), gadget witnesses (k * 260, row-major) and the chains' final
-// projective outputs (r_proj: A x,y,z then B x,y,z as limbs). Throws SgError
+// Fills rows (k entries), gadget witnesses (k * 260, row-major) and the chains'
+// final projective outputs (r_proj: A x,y,z then B x,y,z as limbs); the caller
+// provides the buffers (pinned host memory on the proving path). Throws SgError
 // (SG_EINVAL) for a coordinate >= p or a point not on the curve.
 void chain_witness(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits, const uint8_t bx[32],
-                   const uint8_t by[32], const uint8_t* b_bits, uint64_t k, std::vector<RowW>* rows,
-                   std::vector<GadgetW>* gw, uint32_t r_proj[6][NL]);
+                   const uint8_t by[32], const uint8_t* b_bits, uint64_t k, RowW* rows, GadgetW* gw,
+                   uint32_t r_proj[6][NL]);
 // The column-major width x k trace on the host.
 void expand_host(const RowW* rows, const GadgetW* gw, const uint32_t r_proj[6][NL], uint64_t k, uint64_t* trace);
 // u1 = e s^-1, u2 = r s^-1 mod n as MSB-first bits (e = digest mod n); throws

@@ -2,6 +2,7 @@
 // host, trace expanded on the device, LDE x32, Phi by the gadget kernel, the
 // quotient by X^n_trace - 1, and the STIR proof (prove_ecdsa_record_v1.rs:97-240).
 #include <cstring>
+#include <mutex>
 
 #include "context.hpp"
 #include "merge.cuh"
@@ -20,10 +21,42 @@ unsigned lg2(uint64_t n) {
   return l;
 }
 
+// The layout's device tables (gadget table, cell codes, lambda bases, merge
+// chunks, tail bases, b), uploaded once per device and kept for the process.
+struct P256Tables {
+  const p256::Gadget* table = nullptr;
+  const uint32_t *code = nullptr, *lam = nullptr, *chunk = nullptr, *tail = nullptr, *b = nullptr;
+  uint32_t n_chunks = 0;
+};
+
 template <class T>
-void h2d(DBuf* d, const std::vector<T>& v, cudaStream_t s) {
-  d->alloc((v.size() * sizeof(T) + 7) / 8, s);
-  cuda_check(cudaMemcpyAsync(d->p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "h2d");
+const T* upload_const(const T* h, size_t n) {
+  void* d = nullptr;
+  cuda_check(cudaMalloc(&d, n * sizeof(T)), "p256 tables");
+  cuda_check(cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice), "p256 tables");
+  return (const T*)d;
+}
+
+const P256Tables& p256_tables() {
+  static std::mutex mu;
+  static P256Tables per_dev[64];
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "device");
+  require(dev >= 0 && dev < 64, "p256: device index");
+  std::lock_guard<std::mutex> g(mu);
+  P256Tables& t = per_dev[dev];
+  if (!t.table) {
+    const p256::Layout& L = p256::layout();
+    const std::vector<uint32_t> chunk = p256_chunks(2600);
+    t.code = upload_const(L.cell_code.data(), L.cell_code.size());
+    t.lam = upload_const(L.lam_base.data(), L.lam_base.size());
+    t.chunk = upload_const(chunk.data(), chunk.size());
+    t.tail = upload_const(L.tail, 18);
+    t.b = upload_const(L.b_limbs, p256::NL);
+    t.n_chunks = (uint32_t)chunk.size() - 1;
+    t.table = upload_const(L.table.data(), L.table.size());
+  }
+  return t;
 }
 
 }  // namespace
@@ -33,47 +66,40 @@ void p256_trace_device(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], co
                        uint64_t* d_trace) {
   require(k >= 2 && (k & (k - 1)) == 0 && k <= (1u << 16), "p256: rows must be a power of 2 in [2, 65536]");
   const p256::Layout& L = p256::layout();
-  std::vector<p256::RowW> rows;
-  std::vector<p256::GadgetW> gw;
-  uint32_t rproj[6][p256::NL];
-  p256::chain_witness(ax, ay, a_bits, bx, by, b_bits, k, &rows, &gw, rproj);
+  const P256Tables& T = p256_tables();
+  const uint64_t NG = L.table.size();
+  // witnesses straight into pinned staging, so the copy is one fast DMA
+  const size_t rows_bytes = k * sizeof(p256::RowW), gw_bytes = k * NG * sizeof(p256::GadgetW);
+  const size_t rp_bytes = 6 * p256::NL * sizeof(uint32_t);
+  uint8_t* pin = (uint8_t*)pinned_host(c, rows_bytes + gw_bytes + rp_bytes);
+  p256::RowW* rows = (p256::RowW*)pin;
+  p256::GadgetW* gw = (p256::GadgetW*)(pin + rows_bytes);
+  auto rproj = (uint32_t(*)[p256::NL])(pin + rows_bytes + gw_bytes);
+  p256::chain_witness(ax, ay, a_bits, bx, by, b_bits, k, rows, gw, rproj);
   cudaStream_t s = c->stream;
-  DBuf d_table, d_code, d_rows, d_gw, d_rp, d_b;
-  h2d(&d_table, L.table, s);
-  h2d(&d_code, L.cell_code, s);
-  h2d(&d_rows, rows, s);
-  h2d(&d_gw, gw, s);
-  h2d(&d_rp, std::vector<uint32_t>(&rproj[0][0], &rproj[0][0] + 6 * p256::NL), s);
-  h2d(&d_b, std::vector<uint32_t>(L.b_limbs, L.b_limbs + p256::NL), s);
-  P256Dev d{(const p256::Gadget*)d_table.p, (const uint32_t*)d_code.p, (const p256::RowW*)d_rows.p,
-            (const p256::GadgetW*)d_gw.p, (const uint32_t*)d_rp.p, (const uint32_t*)d_b.p, L.width,
-            (uint32_t)L.table.size()};
+  DBuf d_wit((rows_bytes + gw_bytes + rp_bytes + 7) / 8, s);
+  cuda_check(cudaMemcpyAsync(d_wit.p, pin, rows_bytes + gw_bytes + rp_bytes, cudaMemcpyHostToDevice, s), "h2d");
+  const uint8_t* dw = (const uint8_t*)d_wit.p;
+  P256Dev d{T.table, T.code, (const p256::RowW*)dw, (const p256::GadgetW*)(dw + rows_bytes),
+            (const uint32_t*)(dw + rows_bytes + gw_bytes), T.b, L.width, (uint32_t)NG};
   cuda_check(p256_expand(d, k, d_trace, s), "p256 trace expand");
-  cuda_check(cudaStreamSynchronize(s), "sync");  // host witnesses must outlive their copies
+  cuda_check(cudaStreamSynchronize(s), "sync");  // the staging buffer is reused by the next proof
 }
 
 void p256_merge_device(sg_ctx* c, const uint64_t* d_lde, uint64_t n_trace, uint64_t blowup, uint64_t* d_c) {
   const p256::Layout& L = p256::layout();
+  const P256Tables& T = p256_tables();
   const uint64_t n = n_trace * blowup;
   const unsigned ln = lg2(n);
   require((1ull << ln) == n && ln <= kMaxLogN && n_trace >= 2, "p256 merge: bad sizes");
   cudaStream_t s = c->stream;
-  const std::vector<uint32_t> chunk = p256_chunks(2600);
-  const uint32_t n_chunks = (uint32_t)chunk.size() - 1;
-  DBuf d_table, d_lam, d_chunk, d_tail;
-  h2d(&d_table, L.table, s);
-  h2d(&d_lam, L.lam_base, s);
-  h2d(&d_chunk, chunk, s);
-  h2d(&d_tail, std::vector<uint32_t>(L.tail, L.tail + 18), s);
-  DBuf part((uint64_t)n_chunks * n, s), phi(n, s), scratch(ntt_scratch_elems(1, ln), s);
-  P256Phi a{d_lde, n, blowup, n_trace, (const p256::Gadget*)d_table.p, (const uint32_t*)d_lam.p,
-            (const uint32_t*)d_chunk.p, (const uint32_t*)d_tail.p, (uint32_t)L.table.size(),
+  DBuf part((uint64_t)T.n_chunks * n, s), phi(n, s), scratch(ntt_scratch_elems(1, ln), s);
+  P256Phi a{d_lde, n, blowup, n_trace, T.table, T.lam, T.chunk, T.tail, (uint32_t)L.table.size(),
             L.n_constraints - p256::TAIL_CONSTRAINTS};
-  cuda_check(p256_phi(a, n_chunks, part.p, phi.p, s), "p256 phi");
+  cuda_check(p256_phi(a, T.n_chunks, part.p, phi.p, s), "p256 phi");
   cuda_check(ntt_batch(c->tw, phi.p, phi.p, 1, n, n, (int)ln, true, n, scratch.p, s), "intt");
   cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
   cuda_check(ntt_batch(c->tw, d_c, d_c, 1, n, n, (int)ln, false, n - n_trace, scratch.p, s), "ntt");
-  cuda_check(cudaStreamSynchronize(s), "sync");  // host tables must outlive their copies
 }
 
 std::vector<uint8_t> prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
