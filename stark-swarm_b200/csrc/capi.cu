@@ -1,6 +1,7 @@
 // capi.cu — extern "C" entry points declared in include/stark_gpu.h.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "context.hpp"
@@ -84,15 +85,51 @@ struct Out {
 
 namespace sg {
 
+// Pinned staging buffers are recycled process-wide: a context returns its buffer
+// when it is destroyed (server workers come and go with each batch), so page
+// locking happens once per peak concurrency, not once per worker.
+namespace {
+struct PinnedPool {
+  std::mutex mu;
+  std::vector<std::pair<void*, size_t>> free;
+};
+PinnedPool& pinned_pool() {
+  static PinnedPool* p = new PinnedPool;  // kept for the process
+  return *p;
+}
+}  // namespace
+
+void pinned_release(sg_ctx* c) {
+  if (!c->pinned) return;
+  PinnedPool& P = pinned_pool();
+  std::lock_guard<std::mutex> g(P.mu);
+  P.free.push_back({c->pinned, c->pinned_bytes});
+  c->pinned = nullptr;
+  c->pinned_bytes = 0;
+}
+
 void* pinned_host(sg_ctx* c, size_t bytes) {
   if (c->pinned_bytes >= bytes) return c->pinned;
   cuda_check(cudaStreamSynchronize(c->stream), "sync");  // no copy from the old buffer in flight
-  if (c->pinned) cudaFreeHost(c->pinned);
-  c->pinned = nullptr;
-  c->pinned_bytes = 0;
-  cuda_check(cudaHostAlloc(&c->pinned, bytes, cudaHostAllocDefault), "pinned host allocation");
+  pinned_release(c);
+  {
+    PinnedPool& P = pinned_pool();
+    std::lock_guard<std::mutex> g(P.mu);
+    size_t best = P.free.size();
+    for (size_t i = 0; i < P.free.size(); ++i)
+      if (P.free[i].second >= bytes && (best == P.free.size() || P.free[i].second < P.free[best].second)) best = i;
+    if (best < P.free.size()) {
+      c->pinned = P.free[best].first;
+      c->pinned_bytes = P.free[best].second;
+      P.free.erase(P.free.begin() + best);
+      return c->pinned;
+    }
+  }
+  void* p = nullptr;
+  cuda_check(cudaHostAlloc(&p, bytes, cudaHostAllocDefault), "pinned host allocation");
+  c->pinned = p;
   c->pinned_bytes = bytes;
-  return c->pinned;
+  return p;
 }
 
 void pool_reserve(int device, uint64_t bytes, cudaStream_t s) {
@@ -175,7 +212,7 @@ void sg_ctx_destroy(sg_ctx* c) {
   }
   if (c->stir_in) cudaEventDestroy(c->stir_in);
   if (c->stir_out) cudaEventDestroy(c->stir_out);
-  if (c->pinned) cudaFreeHost(c->pinned);
+  sg::pinned_release(c);
   delete c;
 }
 

@@ -89,6 +89,8 @@ bool is_device_ptr(const void* p);
 // The context's pinned host staging buffer, grown to at least `bytes`. Earlier
 // contents are not kept; the caller synchronises its stream before the next use.
 void* pinned_host(sg_ctx* c, size_t bytes);
+// Give the context's staging buffer back to the process-wide pool.
+void pinned_release(sg_ctx* c);
 
 // sg_pool_reserve: grow the device's default pool to `bytes` (best effort).
 void pool_reserve(int device, uint64_t bytes, cudaStream_t s);
