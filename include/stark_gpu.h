@@ -208,6 +208,18 @@ int sg_sha512_trace_gpu(sg_ctx* ctx, const uint8_t* msg, size_t len, uint64_t* t
 int sg_prove_sha512(sg_ctx* ctx, const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode,
                     uint8_t* proof, size_t cap, size_t* len_out, uint8_t digest[64]);
 
+/* Autotuner for the NTT's four-step split (sizes 2^13 .. 2^24, done in two passes
+ * N = N1 * N2 with N1, N2 <= 2^12): times every split on a scratch transform of
+ * min(n_cols, 2^26 / 2^log_n) columns (input zero-padded beyond n_valid, as in an
+ * LDE, when n_valid < 2^log_n; 0 = none) and keeps the fastest for that size and
+ * padding, for every later transform in the process (all splits give the same
+ * output). best_log_n1 (optional) receives log N1 of the chosen split. Call it
+ * before the timed or latency-sensitive work, like cuDNN's benchmark mode. */
+int sg_ntt_autotune(sg_ctx* ctx, size_t n_cols, size_t log_n, int inverse, size_t n_valid, int* best_log_n1);
+/* Set the split directly (a saved sg_ntt_autotune result; 0 = the default log N / 2):
+ * SG_EINVAL unless 13 <= log_n <= 24 and max(1, log_n - 12) <= log_n1 <= min(12, log_n - 1). */
+int sg_ntt_set_split(size_t log_n, int padded, int log_n1);
+
 /* Hash profile of this build, the counterpart of the reference's compile-time hash
  * feature (hash/src/selected.rs:8-48): digest bytes of every Merkle node and of the
  * Fiat-Shamir transcript, so of every root in a proof. libstarkgpu.so is the

@@ -124,7 +124,7 @@ EXPORTS = (
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
-    "sg_pool_reserve", "sg_hash_bytes",
+    "sg_pool_reserve", "sg_hash_bytes", "sg_ntt_autotune", "sg_ntt_set_split",
 )
 JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA = 1, 2, 3, 4, 5
 OPT_WIDE_MERGE = 1
@@ -175,6 +175,8 @@ def lib():
     L.sg_ctx_set_stream.argtypes = [vp, vp]
     L.sg_ctx_set_option.argtypes = [vp, i32, ctypes.c_int64]
     L.sg_pool_reserve.argtypes = [vp, u64]
+    L.sg_ntt_autotune.argtypes = [vp, sz, sz, i32, sz, ctypes.POINTER(ctypes.c_int)]
+    L.sg_ntt_set_split.argtypes = [sz, i32, i32]
     L.sg_last_error.argtypes = [vp]
     L.sg_last_error.restype = ctypes.c_char_p
     L.sg_kernel_launches.argtypes = [vp]
@@ -296,6 +298,13 @@ def build_params(n0: int, pk_hash_32: bytes = None, stir: bool = True) -> FriPar
     p = FriParams()
     lib().sg_build_params(n0, pk_hash_32, int(stir), ctypes.byref(p))
     return p
+
+
+def ntt_set_split(log_n: int, padded: bool, log_n1: int):
+    """sg_ntt_set_split: pin the four-step split of 2^log_n transforms (0 = default)."""
+    rc = lib().sg_ntt_set_split(log_n, int(padded), log_n1)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_ntt_set_split: size or split out of range")
 
 
 def profile_enable(on: bool = True):
@@ -593,6 +602,13 @@ class Context:
 
     def set_option(self, option: int, value: int):
         self._check(self._lib.sg_ctx_set_option(self._h, option, value))
+
+    def ntt_autotune(self, n_cols: int, log_n: int, inverse: bool = False, n_valid: int = 0) -> int:
+        """sg_ntt_autotune: measure the four-step splits of a 2^13..2^24 transform
+        (zero-padded beyond n_valid when given) and keep the fastest; returns its log N1."""
+        best = ctypes.c_int()
+        self._check(self._lib.sg_ntt_autotune(self._h, n_cols, log_n, int(inverse), n_valid, ctypes.byref(best)))
+        return best.value
 
     def pool_reserve(self, nbytes: int):
         """sg_pool_reserve: grow the device memory pool to nbytes up front (best effort)."""

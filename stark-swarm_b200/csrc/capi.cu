@@ -236,6 +236,69 @@ int sg_ctx_set_option(sg_ctx* c, int option, int64_t value) {
 
 int sg_hash_bytes(void) { return kc::kHashBytes; }
 
+int sg_ntt_set_split(size_t log_n, int padded, int log_n1) {
+  if (log_n < 13 || log_n > 24) return SG_EINVAL;
+  if (log_n1 != 0 && (log_n1 < std::max<int>(1, (int)log_n - 12) || log_n1 > std::min<int>(12, (int)log_n - 1)))
+    return SG_EINVAL;
+  sg::ntt_set_split((int)log_n, padded != 0, log_n1);
+  return SG_OK;
+}
+
+int sg_ntt_autotune(sg_ctx* c, size_t n_cols, size_t log_n, int inverse, size_t n_valid, int* best_log_n1) {
+  return guarded(c, [&] {
+    sg::require(log_n >= 13 && log_n <= 24 && n_cols > 0, "ntt_autotune: sizes 2^13 .. 2^24 (two passes) only");
+    const uint64_t N = 1ull << log_n;
+    if (n_valid == 0 || n_valid > N) n_valid = N;
+    const bool padded = n_valid < N;
+    // enough columns to fill the GPU (2^26 elements), at most the caller's
+    const uint64_t cols = std::min<uint64_t>(n_cols, std::max<uint64_t>(1, (1ull << 26) >> log_n));
+    cudaStream_t s = c->stream;
+    sg::DBuf in(cols * N, s), out(cols * N, s), scratch(sg::ntt_scratch_elems(cols, (int)log_n), s);
+    sg::cuda_check(cudaMemsetAsync(in.p, 0, cols * N * 8, s), "memset");  // the timing is data-independent
+    cudaEvent_t e0, e1;
+    sg::cuda_check(cudaEventCreate(&e0), "event");
+    sg::cuda_check(cudaEventCreate(&e1), "event");
+    const int lo = std::max<int>(1, (int)log_n - 12), hi = std::min<int>(12, (int)log_n - 1);
+    const int prior = sg::ntt_split((int)log_n, padded);
+    int best = prior;
+    float best_ms = 1e30f;
+    try {
+      for (int l1 = lo; l1 <= hi; ++l1) {
+        sg::ntt_set_split((int)log_n, padded, l1);
+        auto run = [&] {
+          sg::cuda_check(sg::ntt_batch(c->tw, in.p, out.p, (uint32_t)cols, N, N, (int)log_n, inverse != 0, n_valid,
+                                       scratch.p, s),
+                         "ntt");
+        };
+        run();  // warm-up
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+          sg::cuda_check(cudaEventRecord(e0, s), "event");
+          run();
+          sg::cuda_check(cudaEventRecord(e1, s), "event");
+          sg::cuda_check(cudaEventSynchronize(e1), "sync");
+          float t = 0;
+          sg::cuda_check(cudaEventElapsedTime(&t, e0, e1), "elapsed");
+          ms = std::min(ms, t);
+        }
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = l1;
+        }
+      }
+    } catch (...) {
+      sg::ntt_set_split((int)log_n, padded, prior);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      throw;
+    }
+    sg::ntt_set_split((int)log_n, padded, best);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best_log_n1) *best_log_n1 = best;
+  });
+}
+
 int sg_pool_reserve(sg_ctx* c, uint64_t bytes) {
   return guarded(c, [&] { sg::pool_reserve(c->device, bytes, c->stream); });
 }

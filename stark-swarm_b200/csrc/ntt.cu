@@ -18,6 +18,7 @@
 // is padded one word per 16 so every stage's stride pattern is conflict-free.
 // The radix-R butterflies use only powers of w_R <= w_16, which in Goldilocks
 // are powers of two (w_16 = 2^156 for ark's root chain).
+#include <atomic>
 #include <vector>
 
 #include "counters.hpp"
@@ -400,6 +401,7 @@ PassArgs base_args(const NttTables& t, bool inverse) {
 
 // sparse first stage for pass 1 over k_hi: points m >= ceil(n_valid / n_lo) are zero
 int sparse_nz_for(uint64_t n_valid, uint64_t N, uint64_t n_lo, uint64_t M) {
+  if (n_valid >= N || M < 16) return 0;  // dense, or a pass without a radix-16 first stage
   const uint64_t m_nz = (n_valid + n_lo - 1) / n_lo, G = M / 16;
   const uint64_t nz = (m_nz + G - 1) / G;
   return (n_valid < N && M >= 16 && nz <= 2) ? (int)(nz ? nz : 1) : 0;
@@ -516,6 +518,21 @@ uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n) {
   return (log_n <= 24 ? 1 : 2) * n_cols * N;
 }
 
+// Four-step split per (log N, zero-padded input): log N1 of the second pass.
+// 0 = the default, log N / 2; ntt_autotune stores measured choices.
+namespace {
+std::atomic<int> g_split[kMaxLogN + 1][2];
+}
+
+int ntt_split(int log_n, bool padded) {
+  const int tuned = (log_n >= 0 && log_n <= kMaxLogN) ? g_split[log_n][padded ? 1 : 0].load() : 0;
+  return tuned ? tuned : log_n / 2;
+}
+
+void ntt_set_split(int log_n, bool padded, int log_n1) {
+  if (log_n >= 13 && log_n <= 24) g_split[log_n][padded ? 1 : 0].store(log_n1);
+}
+
 cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uint32_t n_cols, uint64_t in_stride,
                       uint64_t out_stride, int log_n, bool inverse, uint64_t n_valid, uint64_t* scratch,
                       cudaStream_t s, const PowSpec* pre) {
@@ -550,7 +567,7 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
   }
   if (!scratch) return cudaErrorInvalidValue;
   if (log_n <= 24) {
-    const int l1 = log_n / 2, l2 = log_n - l1;
+    const int l1 = ntt_split(log_n, n_valid < N), l2 = log_n - l1;
     const uint64_t N1 = 1ull << l1, N2 = 1ull << l2;
     // pass 1: DFT_{N2} over k2 (stride N1), lanes k1; transposed store into scratch
     PassArgs a = base_args(t, inverse);

@@ -52,6 +52,13 @@ struct PowSpec {
 // Host: lo[i] = scale * g^i, hi[i] = g^(2^14 i) for i < 2^14 (out: 2 * 2^14 u64).
 void pow_tables_host(uint64_t g, uint64_t scale, uint64_t* out);
 
+// The four-step split ntt_batch uses for 2^13 .. 2^24 (log N1 of its second pass),
+// per size and for zero-padded (forward LDE) input; ntt_set_split overrides the
+// default log N / 2 (the measured choice of ntt_autotune), for every context.
+// Every split gives the same output.
+int ntt_split(int log_n, bool padded);
+void ntt_set_split(int log_n, bool padded, int log_n1);
+
 // Scratch (in elements) ntt_batch needs for n_cols columns of 2^log_n.
 uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n);
 

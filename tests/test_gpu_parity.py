@@ -373,3 +373,41 @@ def test_lde_host_input_pipelined_matches_device_input(ctx):
         for cf in reversed(col):
             acc = (acc * x + cf) % P
         assert int(got[19, i]) == acc
+
+
+@pytest.mark.parametrize("log_n", [13, 16, 20])
+def test_ntt_every_four_step_split_matches_oracle(sgpu, ctx, log_n):
+    # every split the autotuner may choose gives the oracle's transform, for dense
+    # input and for a zero-padded LDE
+    rng = np.random.default_rng(300 + log_n)
+    x = rand_field(rng, (2, 1 << log_n))
+    want = [O.ntt(x[c]) for c in range(2)]
+    tr = rand_field(rng, (2, 1 << (log_n - 3)))
+    want_lde = O.lde(tr, 8)
+    try:
+        for l1 in range(max(1, log_n - 12), min(12, log_n - 1) + 1):
+            sgpu.ntt_set_split(log_n, False, l1)
+            sgpu.ntt_set_split(log_n, True, l1)
+            got = ctx.ntt(x, log_n, False)
+            assert all(np.array_equal(got[c], want[c]) for c in range(2)), l1
+            assert np.array_equal(ctx.lde(tr, 8, 1), want_lde), l1
+    finally:
+        sgpu.ntt_set_split(log_n, False, 0)
+        sgpu.ntt_set_split(log_n, True, 0)
+    with pytest.raises(sgpu.StarkGpuError):
+        sgpu.ntt_set_split(log_n, False, 13)
+
+
+def test_ntt_autotune_keeps_results(sgpu, ctx):
+    rng = np.random.default_rng(9)
+    x = rand_field(rng, (4, 1 << 18))
+    want = ctx.ntt(x, 18, False)
+    try:
+        best = ctx.ntt_autotune(4, 18)
+        assert 6 <= best <= 12
+        assert np.array_equal(ctx.ntt(x, 18, False), want)
+        best_pad = ctx.ntt_autotune(4, 21, False, 1 << 18)
+        assert 9 <= best_pad <= 12
+    finally:
+        sgpu.ntt_set_split(18, False, 0)
+        sgpu.ntt_set_split(21, True, 0)
