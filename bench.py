@@ -646,10 +646,14 @@ def main():
                     "launches_per_step": launches_per_step}
     kernels = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps} for k, v in prof.items()}
 
+    # The sections below characterise one GPU; with N > 1 ranks (the weak-scaling
+    # run, one independent proof per GPU per step) only the main metric is taken.
+    single = ws == 1
+
     # SHA-256 AIR proofs of seeded 64-byte messages (prove_ds_ksk_binding shape:
     # 2 blocks, n_trace 256, n0 8192): one proof at a time vs 16 in flight
     cfg1 = None
-    if args.sha256_jobs > 0:
+    if single and args.sha256_jobs > 0:
         rng = np.random.default_rng(1)
         jobs = [(sg.JOB_SHA256, rng.integers(0, 256, 64, dtype=np.uint8).tobytes(),
                  hashlib.sha3_256(b"cfg1-%d" % i).digest()) for i in range(args.sha256_jobs)]
@@ -669,7 +673,7 @@ def main():
     # classic DEEP-FRI (params.stir = false, the branch of the reference's published
     # scaling numbers) on the same 2^23 column, beside the STIR proof of the step
     classic = None
-    if args.classic_fri:
+    if single and args.classic_fri:
         pc = sg.build_params(N0, PI_HASH, stir=False)
         ref_c = ctx.deep_fri_prove(d_lde[0], N0, pc)
         assert sg.deep_fri_verify(pc, ref_c), "classic proof rejected"
@@ -694,11 +698,12 @@ def main():
                    "classic_proof_bytes": len(ref_c)}
 
     cpu_threads = (os.cpu_count() or 1) if (rank == 0 and ws == 1 and not args.no_cpu_baseline) else 0
-    large = sha256_large(sg, ctx, args.sha256_large_blocks, 3, cpu_threads) if args.sha256_large_blocks > 0 else None
-    rsa = rsa2048(sg, ctx, args.rsa_jobs, args.rsa_stacked, cpu_threads) if args.rsa_jobs > 0 else None
-    ecdsa = p256_ecdsa(sg, ctx, args.ecdsa_jobs, cpu_threads) if args.ecdsa_jobs > 0 else None
+    large = sha256_large(sg, ctx, args.sha256_large_blocks, 3, cpu_threads) if single and args.sha256_large_blocks > 0 \
+        else None
+    rsa = rsa2048(sg, ctx, args.rsa_jobs, args.rsa_stacked, cpu_threads) if single and args.rsa_jobs > 0 else None
+    ecdsa = p256_ecdsa(sg, ctx, args.ecdsa_jobs, cpu_threads) if single and args.ecdsa_jobs > 0 else None
     serve = None
-    if args.serve_jobs > 0:
+    if single and args.serve_jobs > 0:
         serve = serving(sg, ctx, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs, 16)
 
     cpu = None
