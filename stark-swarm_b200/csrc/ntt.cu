@@ -19,6 +19,9 @@
 // The radix-R butterflies use only powers of w_R <= w_16, which in Goldilocks
 // are powers of two (w_16 = 2^156 for ark's root chain).
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "counters.hpp"
@@ -87,6 +90,7 @@ struct PassArgs {
   // radix-16 group can be non-zero (zero-padded forward transform); 0 = dense
   int sparse_nz;
   int tw_log;                 // > 0: output (lane, i) *= w_{2^tw_log}^(i*lane)
+  const uint64_t* tw_tab;     // if set, that twiddle is tw_tab[i * n_lanes + lane]
   int in_tw_log;              // > 0: input (lane, m) *= w_{2^in_tw_log}^(m*lane)
   int out_i_log;              // coset evaluation: out_i = 2^out_i_log
   uint64_t scale;             // != 1: outputs *= scale
@@ -315,10 +319,14 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       x[q] = sm[l * Mp + padi(i)];
       if (a.tw_log > 0) {
         uint64_t w;
-        if constexpr (PTW)
+        if constexpr (PTW) {
           w = gl::mul(ptw[l * PT_PER + (i & 63)], ptw[l * PT_PER + 64 + (i >> 6)]);
-        else
-          w = tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log);
+        } else {
+          if (a.tw_tab)  // (a CTA's lanes past n_lanes store nothing and read no table entry)
+            w = lane0 + l < a.n_lanes ? __ldg(a.tw_tab + (uint64_t)i * a.n_lanes + lane0 + l) : 0;
+          else
+            w = tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log);
+        }
         x[q] = gl::mul(x[q], w);
       }
       if (a.scale != 1) x[q] = gl::mul(x[q], a.scale);
@@ -400,6 +408,43 @@ PassArgs base_args(const NttTables& t, bool inverse) {
 }
 
 // sparse first stage for pass 1 over k_hi: points m >= ceil(n_valid / n_lo) are zero
+__global__ void pass_tw_kernel(const uint64_t* lo, const uint64_t* hi, int log_n, int log_n1, uint64_t* out) {
+  const uint64_t total = 1ull << log_n, n1 = 1ull << log_n1;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
+       e += (uint64_t)gridDim.x * blockDim.x)
+    out[e] = tw_pow(lo, hi, (e >> log_n1) * (e & (n1 - 1)), log_n);
+}
+
+// Pass-1 twiddles w_N^{i k} of the split N = N1 N2 as a table [i < N2][k < N1],
+// built once per (device, size, split, direction) and kept for the process: one
+// load per element instead of two table loads and a product, for first passes of
+// at most 2^10 points (8 MB for a 2^20 transform). Larger first passes keep their
+// per-CTA factor tables in shared memory: with a global table the 2^12 pass spilled
+// and read 64 MB per column, and the 64 x 2^23 LDE went from 16.3 to 18.0 ms.
+const uint64_t* pass_twiddle_table(const NttTables& t, int log_n, int log_n1, bool inverse, cudaStream_t s) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, int, int>, uint64_t*> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  const auto key = std::make_tuple(dev, log_n, log_n1, inverse ? 1 : 0);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  uint64_t* d = nullptr;
+  if (cudaMalloc(&d, 8ull << log_n) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;  // no room: the pass forms its twiddles itself
+  }
+  pass_tw_kernel<<<148 * 8, 256, 0, s>>>(inverse ? t.d_inv_lo : t.d_fwd_lo, inverse ? t.d_inv_hi : t.d_fwd_hi, log_n,
+                                          log_n1, d);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  cache[key] = d;
+  return d;
+}
+
 int sparse_nz_for(uint64_t n_valid, uint64_t N, uint64_t n_lo, uint64_t M) {
   if (n_valid >= N || M < 16) return 0;  // dense, or a pass without a radix-16 first stage
   const uint64_t m_nz = (n_valid + n_lo - 1) / n_lo, G = M / 16;
@@ -472,6 +517,7 @@ cudaError_t ntt_tables_init(NttTables* t) {
   }
   *t = ntt_tables_view(dev);
   t->owned = true;
+  t->pass_tables = true;
   return cudaSuccess;
 }
 
@@ -584,6 +630,8 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
     a.in_valid = n_valid;
     a.sparse_nz = sparse_nz_for(n_valid, N, N1, N2);
     a.tw_log = log_n;
+    // passes of 2^11 and 2^12 build their twiddle factors in shared memory instead
+    if (t.pass_tables && !pass_tw_in_smem(l2)) a.tw_tab = pass_twiddle_table(t, log_n, l1, inverse, s);
     a.pre = pre ? *pre : none;
     cudaError_t e = launch_pass_dyn(l2, a, inverse, n_cols, s);
     if (e != cudaSuccess) return e;

@@ -26,6 +26,10 @@ struct NttTables {
   uint64_t* d_inv_lo = nullptr;
   uint64_t* d_inv_hi = nullptr;
   bool owned = false;
+  // Two-pass transforms may read their pass twiddles w_N^{i k} from a per-size
+  // table kept for the process (pass_twiddle_table); off for tables made by
+  // ntt_tables_view (callers that must not allocate).
+  bool pass_tables = false;
 };
 
 // Elements of one direction's block: st (4096) + lo + hi.
