@@ -18,6 +18,7 @@
 // is padded one word per 16 so every stage's stride pattern is conflict-free.
 // The radix-R butterflies use only powers of w_R <= w_16, which in Goldilocks
 // are powers of two (w_16 = 2^156 for ark's root chain).
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
         // one column's cosets: point m of every lane is in[m], all lanes valid
         // (ntt_coset_eval launches exactly B / K CTAs per column)
         x[q] = __ldg(in + m);
-        if (a.pre.lo) x[q] = gl::mul(x[q], pow_at(a.pre, (uint64_t)m));
+        if (a.pre.active()) x[q] = gl::mul(x[q], pow_at(a.pre, (uint64_t)m));
         // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j)
         const uint64_t ex = (uint64_t)m * lane;
         x[q] = gl::mul(x[q], a.in_tw_log <= kTwSplit
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
                                  : tw_pow(a.tw_lo, a.tw_hi, ex, a.in_tw_log));
       } else if (e < E_load && lane < a.n_lanes && flat < a.in_valid) {
         x[q] = __ldg(in + lane * a.in_lane + (uint64_t)m * a.in_m);
-        if (a.pre.lo) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
+        if (a.pre.active()) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
       }
     }
 #pragma unroll
@@ -445,6 +446,12 @@ const uint64_t* pass_twiddle_table(const NttTables& t, int log_n, int log_n1, bo
   return d;
 }
 
+__global__ void pow_table_kernel(const uint64_t* lo, const uint64_t* hi, uint64_t mult, int log_n, uint64_t len,
+                                 uint64_t* tab) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < len; k += (uint64_t)gridDim.x * blockDim.x)
+    tab[k] = tw_pow(lo, hi, k * mult, log_n);
+}
+
 int sparse_nz_for(uint64_t n_valid, uint64_t N, uint64_t n_lo, uint64_t M) {
   if (n_valid >= N || M < 16) return 0;  // dense, or a pass without a radix-16 first stage
   const uint64_t m_nz = (n_valid + n_lo - 1) / n_lo, G = M / 16;
@@ -556,6 +563,16 @@ cudaError_t ntt_coset_eval(const NttTables& t, const uint64_t* coef, uint64_t* o
   a.in_valid = M;
   a.in_tw_log = log_m + log_b;
   return launch_pass_dyn(log_m, a, false, n_cols, s);
+}
+
+cudaError_t pow_table_device(const NttTables& t, uint64_t mult, int log_n, uint64_t len, uint64_t* tab,
+                             cudaStream_t s) {
+  if (len == 0) return cudaSuccess;
+  if (log_n < 0 || log_n > kMaxLogN || !tab) return cudaErrorInvalidValue;
+  SG_LAUNCH_SCOPE("pow_table", s);
+  pow_table_kernel<<<(unsigned)std::min<uint64_t>((len + 255) / 256, 148 * 16), 256, 0, s>>>(
+      t.d_fwd_lo, t.d_fwd_hi, mult, log_n, len, tab);
+  return cudaGetLastError();
 }
 
 uint64_t ntt_scratch_elems(uint64_t n_cols, int log_n) {

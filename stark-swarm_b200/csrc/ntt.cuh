@@ -52,7 +52,14 @@ struct PowSpec {
   const uint64_t* hi = nullptr;
   uint64_t mult = 1;
   int shl = 0;
+  // instead of lo/hi: g^k read from a full table (k below its length)
+  const uint64_t* tab = nullptr;
+  __host__ __device__ bool active() const { return lo || tab; }
 };
+// Host: tab[k] = w_{2^log_n}^(mult k) for k < len on the device (the NttTables'
+// forward direction), e.g. a coset twist applied by a transform's first pass.
+cudaError_t pow_table_device(const NttTables& t, uint64_t mult, int log_n, uint64_t len, uint64_t* tab,
+                             cudaStream_t s);
 // Host: lo[i] = scale * g^i, hi[i] = g^(2^14 i) for i < 2^14 (out: 2 * 2^14 u64).
 void pow_tables_host(uint64_t g, uint64_t scale, uint64_t* out);
 
@@ -96,6 +103,7 @@ __device__ __forceinline__ uint64_t tw_pow(const uint64_t* lo, const uint64_t* h
   return gl::mul(__ldg(lo + (E & (kTwEntries - 1))), __ldg(hi + (E >> kTwSplit)));
 }
 __device__ __forceinline__ uint64_t pow_at(const PowSpec& p, uint64_t k) {
+  if (p.tab) return __ldg(p.tab + k);
   const uint64_t E = ((k * p.mult) << p.shl) & ((1ull << kTwBaseLog) - 1);
   return gl::mul(__ldg(p.lo + (E & (kTwEntries - 1))), __ldg(p.hi + (E >> kTwSplit)));
 }

@@ -767,15 +767,15 @@ void merge_hash_cosets(sg_ctx* c, const HashAir& air, const uint64_t* d_trace, u
   DBuf scratch(std::max(ntt_scratch_elems(W, lt), ntt_scratch_elems(1, ln)), s);
   cuda_check(cudaMemcpyAsync(d_lam.p, lam.data(), lam.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
   ntt(c, d_trace, coef.p, (uint32_t)W, n_trace, n_trace, lt, true, n_trace, scratch.p);
+  DBuf twist_tab(n_trace, s);
   for (uint64_t r = 0; r < blowup; ++r) {
     const uint64_t* evals = d_trace;  // coset 0 holds the trace values themselves
     if (r > 0) {
-      // coefficient k times w_n^(r k), applied as the transform loads it
+      // coefficient k times w_n^(r k), applied as the transform loads it, from a
+      // table of the coset's n_trace powers (one load instead of two and a product)
+      cuda_check(pow_table_device(c->tw, r, (int)ln, n_trace, twist_tab.p, s), "twist table");
       PowSpec twist;
-      twist.lo = c->tw.d_fwd_lo;
-      twist.hi = c->tw.d_fwd_hi;
-      twist.mult = r;
-      twist.shl = kTwBaseLog - (int)ln;
+      twist.tab = twist_tab.p;
       ntt(c, coef.p, ev.p, (uint32_t)W, n_trace, n_trace, lt, false, n_trace, scratch.p, &twist);
       evals = ev.p;
     }
