@@ -136,11 +136,16 @@ __global__ void node_kernel(const uint64_t* child, uint64_t n_child, uint64_t* p
   if (p < n_parent) node_hash_any(child, n_child, parent, p, arity, level, label);
 }
 
-// The levels above the first one with at most kTopParents parents, in one CTA:
-// each level is a block-wide loop over its parents, then a barrier (which makes
-// the level's global writes visible to the whole block) before the next.
+// The levels from the first one of at most kTopWork Keccak-f (parents x
+// permutations per node: two per thread of the CTA) upward, in one CTA: each level
+// is a block-wide loop over its parents, then a barrier (which makes the level's
+// global writes visible to the whole block) before the next. Larger levels go to
+// the whole GPU: on one SM a level of 1024 arity-16 parents (4096 Keccak-f) took
+// about 0.2 ms, against a few microseconds spread over 148 SMs.
 constexpr int kTopThreads = 512;
-constexpr uint64_t kTopParents = 1024;
+constexpr uint64_t kTopWork = 2 * kTopThreads;
+// Keccak-f per node hash: the 4-lane label and `arity` digests, padded
+inline uint64_t node_perms(uint64_t arity) { return (4 + arity * DL) / kc::kRateLanes + 1; }
 constexpr int kMaxTopLevels = 24;
 struct TopLevels {
   int n;
@@ -207,7 +212,7 @@ cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w,
 cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
   for (size_t l = 0; l + 1 < t.len.size(); ++l) {
     const uint64_t np = t.len[l + 1];
-    if (np <= kTopParents && t.len.size() - 1 - l <= (size_t)kMaxTopLevels) {
+    if (np * node_perms(t.arity[l]) <= kTopWork && t.len.size() - 1 - l <= (size_t)kMaxTopLevels) {
       TopLevels tl{};
       for (size_t k = l; k + 1 < t.len.size(); ++k, ++tl.n) {
         tl.arity[tl.n] = t.arity[k];
