@@ -17,6 +17,17 @@ C ABI is declared in include/stark_gpu.h:
   deep_ali_merge_sha512  deep_ali/src/lib.rs:561-641 (and a SHA-512 proof with the same parameters)
   build_sha256_trace_multi / build_sha512_trace_multi
                          deep_ali/src/sha256_air.rs:429-472, sha512_air.rs:551-578
+  prove_rsa2048 / rsa2048_trace / merge_rsa2048
+                         swarm-dns/examples/prove_rsa2048_record_v1.rs, stacked_rsa_zone_prover.rs,
+                         deep_ali/src/rsa2048_exp_air.rs, lib.rs:1694-2070
+  prove_p256_ecdsa / p256_chain_trace / merge_p256_ecdsa
+                         swarm-dns/examples/prove_ecdsa_record_v1.rs:97-240,
+                         deep_ali/src/p256_ecdsa_double_multirow_air.rs, lib.rs:1421-1681
+  Server / prove_batch   many proofs in flight on one GPU (worker loop, swarm-worker/src/main.rs:355)
+
+The Merkle / transcript hash profile (sha3-256, sha3-384 or sha3-512: the
+reference's compile-time hash feature, hash/src/selected.rs) is one library build
+each, chosen per process with STARK_GPU_HASH.
 
 Field elements are canonical uint64 (numpy uint64 arrays on the host, or CUDA
 tensors / raw device pointers that the library uses in place). Errors that the
