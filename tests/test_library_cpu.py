@@ -170,3 +170,14 @@ def test_dns_merkle_root_small_trees(n):
     assert sg.dns_merkle_root(leaves) == dnszone.dns_merkle_root(leaves)
     for idx in range(n):
         assert sg.dns_merkle_verify(leaves[idx], idx, sg.dns_merkle_path(leaves, idx), dnszone.dns_merkle_root(leaves))
+
+
+def test_ntt_split_setter_bounds():
+    # the split table is host state: valid splits are accepted and reset, others refused
+    sg = load_sgpu()
+    sg.ntt_set_split(20, False, 12)
+    sg.ntt_set_split(20, False, 0)
+    for log_n, l1 in ((12, 6), (25, 12), (20, 7), (20, 13), (13, -1)):
+        with pytest.raises(sg.StarkGpuError):
+            sg.ntt_set_split(log_n, False, l1)
+    assert sg.lib().sg_hash_bytes() == sg.HASH_BYTES == 32
