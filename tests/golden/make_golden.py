@@ -7,7 +7,9 @@ length, SHA3-256 digest and a few decoded fields. The tests then check that
 the oracle and the GPU library reproduce each proof byte for byte without
 the reference being present.
 
-Usage: python tests/golden/make_golden.py [path/to/stark-stir-swarm]
+Usage: python tests/golden/make_golden.py path/to/stark-stir-swarm
+
+The path of the reference checkout is required.
 """
 import hashlib
 import json
@@ -18,7 +20,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/stark-stir-swarm"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py path/to/stark-stir-swarm")
+    root = sys.argv[1]
     state = os.path.join(root, "primary-state")
     b = json.load(open(os.path.join(state, "zone_bundle.json")))
 
