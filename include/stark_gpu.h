@@ -126,12 +126,16 @@ int sg_ntt(sg_ctx* ctx, const uint64_t* in, uint64_t* out, size_t n_cols, size_t
  * twiddle table are static device arrays (8 MiB + 576 KiB, held by every GPU
  * that loads the library until exit).
  *  - in/out: device pointers on the current device (in == out allowed);
- *    host pointers are rejected with SG_EINVAL.
+ *    host pointers and memory of another GPU are rejected with SG_EINVAL.
+ *    The library cannot see a buffer's length: in and out must each hold
+ *    n_cols * 2^log_n elements.
  *  - limit: for log_n > 12, n_cols * 2^log_n must be <= 2^20, else SG_ELIMIT;
  *    log_n <= 12 needs no scratch and has no limit.
  *  - the first call on a device sets it up (cudaGetSymbolAddress of the static
  *    arrays and a synchronous copy of the twiddle table), so make that first
- *    call before any stream capture.
+ *    call before any stream capture. Every call resolves the arrays' addresses
+ *    again and compares the current context's id with the one it set up in:
+ *    after cudaDeviceReset the next call repeats the set-up (and its copy).
  *  - every call shares the one static buffer: calls whose kernels can overlap
  *    on the GPU (different streams, no ordering between them) race; order
  *    them on one stream or synchronize between them.

@@ -334,15 +334,39 @@ def profile_read():
     return {arr[i].name.decode(): (arr[i].launches, arr[i].total_ms) for i in range(min(n.value, 64))}
 
 
-def ntt_noalloc(d_in, d_out, log_n: int, inverse: bool = False, stream_ptr: int = 0) -> int:
-    """sg_ntt_noalloc on device buffers (CUDA tensors or raw device pointers), for
-    callers that must not let the library allocate device memory. Returns the
-    SG_* code; the transform is ordered on `stream_ptr` (0 = default stream)."""
+def ntt_noalloc(d_in, d_out, log_n: int, inverse: bool = False, stream_ptr: int = 0, n_cols: int = None) -> int:
+    """sg_ntt_noalloc on device buffers, for callers that must not let the library
+    allocate device memory. `d_in` / `d_out` are CUDA tensors of 64-bit elements
+    holding n_cols columns of 2^log_n (a tensor's element count fixes n_cols), or
+    raw device pointers, in which case `n_cols` must be given. Sizes are checked
+    here before anything reaches the device: a buffer shorter than one column,
+    an element count that is not a whole number of columns, or an output
+    shorter than the input raises ValueError. Returns the SG_* code; the
+    transform is ordered on `stream_ptr` (0 = the legacy default stream)."""
+    if not 0 <= log_n <= 28:
+        raise ValueError("log_n must be in [0, 28]")
+    n = 1 << log_n
     ip, _ki, host_in = _addr(d_in)
     op, _ko, host_out = _addr(d_out)
-    n = 1 << log_n
-    count = d_in.size if host_in else (d_in.numel() if hasattr(d_in, "numel") else n)
-    return lib().sg_ntt_noalloc(ip, op, max(1, count // n), log_n, int(inverse), stream_ptr or None)
+    if host_in or host_out:
+        raise ValueError("sg_ntt_noalloc takes device buffers, not host arrays")
+    counts = [x.numel() if hasattr(x, "numel") else None for x in (d_in, d_out)]
+    if counts[0] is not None:
+        if counts[0] < n or counts[0] % n:
+            raise ValueError(f"input holds {counts[0]} elements, not a whole number of 2^{log_n}-point columns")
+        cols = counts[0] // n
+        if n_cols is not None and n_cols != cols:
+            raise ValueError(f"n_cols={n_cols} but the input holds {cols} columns")
+    elif n_cols is None:
+        raise ValueError("a raw device pointer needs an explicit n_cols")
+    else:
+        cols = n_cols
+    if cols < 1:
+        raise ValueError("n_cols must be at least 1")
+    for c in counts:
+        if c is not None and c < cols * n:
+            raise ValueError(f"a buffer holds {c} elements, fewer than n_cols * 2^log_n = {cols * n}")
+    return lib().sg_ntt_noalloc(ip, op, cols, log_n, int(inverse), stream_ptr or None)
 
 
 def _build_trace_multi(hash_name: str, message: bytes):

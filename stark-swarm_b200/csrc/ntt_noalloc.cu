@@ -10,6 +10,7 @@
 // file-scope static device arrays of fixed size, so nothing is allocated per
 // call. The arrays are created when the library is loaded and every GPU that
 // loads it keeps them (kNoAllocScratchElems * 8 bytes + 576 KiB) until exit.
+#include <cuda.h>  // CUcontext and CUresult types; no libcuda link
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -31,44 +32,88 @@ static __device__ __align__(256) uint64_t g_noalloc_twiddles[2 * sg::kTwDirElems
 
 struct DeviceSlot {
   bool ready = false;
-  uint64_t* scratch = nullptr;   // device address of g_noalloc_scratch on this device
-  uint64_t* twiddles = nullptr;  // device address of g_noalloc_twiddles on this device
+  unsigned long long ctx_id = 0;  // context the arrays were set up in (0: unknown)
+  uint64_t* scratch = nullptr;    // device address of g_noalloc_scratch on this device
+  uint64_t* twiddles = nullptr;   // device address of g_noalloc_twiddles on this device
 };
 DeviceSlot g_slots[kMaxDevices];
 std::mutex g_mu;
 uint64_t g_host_twiddles[2 * sg::kTwDirElems];  // layout of sg::ntt_tables_host
 bool g_host_twiddles_ready = false;
 
-// Once per device, with that device current: resolve the device addresses of
-// the static arrays (host code may not use the symbols' names as pointers) and
-// fill the twiddle table. Runs inside the first sg_ntt_noalloc call on a device.
-int setup_device(int dev) {
-  std::lock_guard<std::mutex> g(g_mu);
-  DeviceSlot& s = g_slots[dev];
-  if (s.ready) return SG_OK;
-  if (!g_host_twiddles_ready) {
-    sg::ntt_tables_host(g_host_twiddles);
-    g_host_twiddles_ready = true;
-  }
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// A process-unique id of the calling thread's current context, or 0 when the
+// driver cannot give one. A context created after cudaDeviceReset gets a new
+// id, and its module holds freshly loaded static arrays (no twiddles), so a
+// changed id means the set-up must run again. The two driver calls are reached
+// through the runtime's entry-point query: the library links cudart only.
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&c) != CUDA_SUCCESS || c == nullptr) return 0;
+  if (get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// With the device current: resolve the device addresses of the static arrays
+// (host code may not use the symbols' names as pointers) and, the first time
+// on a device or whenever its context or the arrays' addresses changed since
+// (cudaDeviceReset), fill the twiddle table with a synchronous copy. Resolving
+// the addresses runs on every call; it is a table lookup in the runtime.
+int setup_device(int dev, DeviceSlot* out) {
   uint64_t* scratch = nullptr;
   uint64_t* tw = nullptr;
   if (cudaGetSymbolAddress((void**)&scratch, g_noalloc_scratch) != cudaSuccess) return SG_ECUDA;
   if (cudaGetSymbolAddress((void**)&tw, g_noalloc_twiddles) != cudaSuccess) return SG_ECUDA;
-  if (cudaMemcpy(tw, g_host_twiddles, sizeof g_host_twiddles, cudaMemcpyHostToDevice) != cudaSuccess)
-    return SG_ECUDA;
-  s.scratch = scratch;
-  s.twiddles = tw;
-  s.ready = true;
+  const unsigned long long ctx_id = current_context_id();
+  std::lock_guard<std::mutex> g(g_mu);
+  DeviceSlot& s = g_slots[dev];
+  if (!s.ready || s.ctx_id != ctx_id || s.scratch != scratch || s.twiddles != tw) {
+    if (!g_host_twiddles_ready) {
+      sg::ntt_tables_host(g_host_twiddles);
+      g_host_twiddles_ready = true;
+    }
+    s.ready = false;
+    if (cudaMemcpy(tw, g_host_twiddles, sizeof g_host_twiddles, cudaMemcpyHostToDevice) != cudaSuccess)
+      return SG_ECUDA;
+    s.scratch = scratch;
+    s.twiddles = tw;
+    s.ctx_id = ctx_id;
+    s.ready = true;
+  }
+  *out = s;
   return SG_OK;
 }
 
-bool on_device(const void* p) {
+// True for device (or managed) memory that belongs to device `dev`. Memory of
+// another GPU is refused: without peer access enabled, a kernel that reads it
+// faults.
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -79,13 +124,13 @@ extern "C" int sg_ntt_noalloc(const uint64_t* d_in, uint64_t* d_out, size_t n_co
     return SG_EINVAL;
   const size_t n = size_t(1) << log_n;
   if (sg::ntt_scratch_elems(n_cols, (int)log_n) > kNoAllocScratchElems) return SG_ELIMIT;
-  if (!on_device(d_in) || !on_device(d_out)) return SG_EINVAL;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return SG_ECUDA;
   if (dev < 0 || dev >= kMaxDevices) return SG_EINVAL;
-  const int rc = setup_device(dev);
+  if (!on_device(d_in, dev) || !on_device(d_out, dev)) return SG_EINVAL;
+  DeviceSlot s;
+  const int rc = setup_device(dev, &s);
   if (rc != SG_OK) return rc;
-  const DeviceSlot& s = g_slots[dev];
   const sg::NttTables t = sg::ntt_tables_view(s.twiddles);
   // Pass 1 writes every scratch element that pass 2 reads, so the scratch left
   // by an earlier call needs no clearing.

@@ -181,3 +181,26 @@ def test_ntt_split_setter_bounds():
         with pytest.raises(sg.StarkGpuError):
             sg.ntt_set_split(log_n, False, l1)
     assert sg.lib().sg_hash_bytes() == sg.HASH_BYTES == 32
+
+
+def test_ntt_noalloc_wrapper_refuses_bad_buffers_before_the_call():
+    # the no-alloc NTT cannot see buffer lengths on the device, so its Python
+    # wrapper checks them first; every case below raises before the library is called
+    torch = pytest.importorskip("torch")
+    sg = load_sgpu()
+    n = 1 << 10
+    good = torch.zeros(2 * n, dtype=torch.int64)
+    with pytest.raises(ValueError):  # not a whole number of columns
+        sg.ntt_noalloc(torch.zeros(2 * n + 1, dtype=torch.int64), good, 10)
+    with pytest.raises(ValueError):  # shorter than one column
+        sg.ntt_noalloc(torch.zeros(n // 2, dtype=torch.int64), good, 10)
+    with pytest.raises(ValueError):  # output shorter than the input
+        sg.ntt_noalloc(good, torch.zeros(n, dtype=torch.int64), 10)
+    with pytest.raises(ValueError):  # raw pointers without a column count
+        sg.ntt_noalloc(good.data_ptr(), good.data_ptr(), 10)
+    with pytest.raises(ValueError):  # a raw output pointer cannot hold the tensor's 2 columns when n_cols says 3
+        sg.ntt_noalloc(good, good.data_ptr(), 10, n_cols=3)
+    with pytest.raises(ValueError):  # host arrays are refused
+        sg.ntt_noalloc(np.zeros(n, dtype=np.uint64), np.zeros(n, dtype=np.uint64), 10)
+    with pytest.raises(ValueError):
+        sg.ntt_noalloc(good, good, 29)
