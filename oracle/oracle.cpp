@@ -1164,8 +1164,9 @@ int orc_sha256_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t
 // prove_ds_ksk_binding core (swarm-dns/src/prover.rs:512-585): multi-block trace ->
 // LDE x32 -> merge_sha256 (lambda_j = j+1) -> STIR with build_params(n0, fs_binding).
 // digest receives the asserted SHA-256 digest read from the H-state.
-int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
-                     size_t cap, size_t* out_len, uint8_t digest[32]) {
+int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, size_t blowup,
+                     uint8_t* out, size_t cap, size_t* out_len, uint8_t digest[32]) {
+  if (blowup < 2 || (blowup & (blowup - 1))) return -2;
   std::vector<Fp> tr;
   size_t n_blocks = 0;
   const size_t n_trace = sha::build_trace_multi(msg, len, &tr, &n_blocks);
@@ -1174,7 +1175,7 @@ int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32
     uint32_t wd = (uint32_t)tr[(sha::H0 + k) * n_trace + digest_row].v;
     for (int b = 0; b < 4; ++b) digest[4 * k + b] = (uint8_t)(wd >> (24 - 8 * b));
   }
-  const size_t blowup = 32, n0 = n_trace * blowup;
+  const size_t n0 = n_trace * blowup;
   std::vector<uint64_t> lde(sha::WIDTH * n0), c(n0);
   orc_lde((const uint64_t*)tr.data(), sha::WIDTH, n_trace, blowup, 1, lde.data());
   std::vector<uint64_t> lam(sha::NUM_CONSTRAINTS);
@@ -1215,8 +1216,9 @@ int orc_sha512_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t
 // SHA-512 prover yet, sha512_air.rs:16-19): trace -> LDE x32 -> merge_sha512
 // (lambda_j = j+1) -> STIR with build_params(n0, fs_binding). digest receives the
 // 64-byte digest read from the H-state (row 128 (n_blocks - 1) + 81).
-int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
-                     size_t cap, size_t* out_len, uint8_t digest[64]) {
+int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, size_t blowup,
+                     uint8_t* out, size_t cap, size_t* out_len, uint8_t digest[64]) {
+  if (blowup < 2 || (blowup & (blowup - 1))) return -2;
   std::vector<Fp> tr;
   size_t n_blocks = 0;
   const size_t n_trace = sha512::build_trace_multi(msg, len, &tr, &n_blocks);
@@ -1227,7 +1229,7 @@ int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32
     const uint64_t wd = lo | hi << 32;
     for (int b = 0; b < 8; ++b) digest[8 * k + b] = (uint8_t)(wd >> (56 - 8 * b));
   }
-  const size_t blowup = 32, n0 = n_trace * blowup;
+  const size_t n0 = n_trace * blowup;
   std::vector<uint64_t> lde(sha512::WIDTH * n0), c(n0);
   orc_lde((const uint64_t*)tr.data(), sha512::WIDTH, n_trace, blowup, 1, lde.data());
   std::vector<uint64_t> lam(sha512::NUM_CONSTRAINTS);
@@ -1287,9 +1289,10 @@ int orc_merge_rsa(const uint64_t* lde, size_t n_records, size_t n_trace, size_t 
 // prove_rsa2048_record_v1.rs:150-205 (one record) and stacked_rsa_zone_prover.rs:
 // 120-175 (n_records): trace (n_records * 11041 x n_trace, column-major) -> LDE x32
 // (shift 1) -> RSA merge -> STIR with build_params(n0, pi) (schedule [8,8,8,2] at n0 1024).
-int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const uint8_t pi[32], uint8_t* out,
-                  size_t cap, size_t* out_len) {
-  const size_t blowup = 32, n0 = n_trace * blowup, w = n_records * rsa::WIDTH;
+int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const uint8_t pi[32], size_t blowup,
+                  uint8_t* out, size_t cap, size_t* out_len) {
+  if (blowup < 2 || (blowup & (blowup - 1))) return -2;
+  const size_t n0 = n_trace * blowup, w = n_records * rsa::WIDTH;
   std::vector<uint64_t> lde(w * n0), c(n0);
   if (orc_lde(trace, w, n_trace, blowup, 1, lde.data()) != 0) return -2;
   if (orc_merge_rsa(lde.data(), n_records, n_trace, blowup, c.data()) != 0) return -2;
@@ -1351,9 +1354,10 @@ int orc_merge_p256(const uint64_t* lde, size_t width, const uint64_t* table, siz
 // prove_ecdsa_record_v1.rs:193-240: trace -> LDE x32 (shift 1) -> merge -> STIR with
 // build_params(n0, pi).
 int orc_prove_p256(const uint64_t* trace, size_t width, const uint64_t* table, size_t n_gadgets,
-                   const uint64_t* tail, size_t n_trace, const uint8_t pi[32], uint8_t* out, size_t cap,
-                   size_t* out_len) {
-  const size_t blowup = 32, n0 = n_trace * blowup;
+                   const uint64_t* tail, size_t n_trace, const uint8_t pi[32], size_t blowup, uint8_t* out,
+                   size_t cap, size_t* out_len) {
+  if (blowup < 2 || (blowup & (blowup - 1))) return -2;
+  const size_t n0 = n_trace * blowup;
   std::vector<uint64_t> lde(width * n0), c(n0);
   if (orc_lde(trace, width, n_trace, blowup, 1, lde.data()) != 0) return -2;
   if (orc_merge_p256(lde.data(), width, table, n_gadgets, tail, n_trace, blowup, c.data()) != 0) return -2;

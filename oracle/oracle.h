@@ -80,17 +80,19 @@ int orc_merge_sha512(const uint64_t* lde, size_t n_trace, size_t blowup, const u
 int orc_sha512_trace(const uint8_t* msg, size_t len, uint64_t* out, size_t cap_elems, size_t* height,
                      size_t* n_blocks);
 int orc_sha512_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_blocks, uint64_t* out);
-int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
-                     size_t cap, size_t* out_len, uint8_t digest[64]);
-int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, uint8_t* out,
-                     size_t cap, size_t* out_len, uint8_t digest[32]);
+/* The SHA-256 / SHA-512 AIR proofs at LDE blowup `blowup` (32 in the reference's
+ * prove_ds_ksk_binding; any power of two >= 2). */
+int orc_prove_sha512(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, size_t blowup,
+                     uint8_t* out, size_t cap, size_t* out_len, uint8_t digest[64]);
+int orc_prove_sha256(const uint8_t* msg, size_t len, const uint8_t fs_binding[32], int phi_mode, size_t blowup,
+                     uint8_t* out, size_t cap, size_t* out_len, uint8_t digest[32]);
 /* RSA-2048 exponentiation AIR (rsa2048_exp_air.rs), n_records records side by side
  * (rsa2048_stacked_air.rs): 11041 cells and 11280 constraints per record. */
 int orc_rsa_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n_trace, size_t n_records,
                  uint64_t* out);
 int orc_merge_rsa(const uint64_t* lde, size_t n_records, size_t n_trace, size_t blowup, uint64_t* c_eval);
-int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const uint8_t pi[32], uint8_t* out,
-                  size_t cap, size_t* out_len);
+int orc_prove_rsa(const uint64_t* trace, size_t n_records, size_t n_trace, const uint8_t pi[32], size_t blowup,
+                  uint8_t* out, size_t cap, size_t* out_len);
 /* P-256 ECDSA double-chain AIR (p256_ecdsa_double_multirow_air.rs): the row is a
  * gadget table (8 u64 per gadget, constraint order) plus an 18-entry tail of chain
  * bases. orc_p256_eval returns the number of constraint values written. */
@@ -99,8 +101,8 @@ int orc_p256_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, size_t n
 int orc_merge_p256(const uint64_t* lde, size_t width, const uint64_t* table, size_t n_gadgets,
                    const uint64_t* tail, size_t n_trace, size_t blowup, uint64_t* c_eval);
 int orc_prove_p256(const uint64_t* trace, size_t width, const uint64_t* table, size_t n_gadgets,
-                   const uint64_t* tail, size_t n_trace, const uint8_t pi[32], uint8_t* out, size_t cap,
-                   size_t* out_len);
+                   const uint64_t* tail, size_t n_trace, const uint8_t pi[32], size_t blowup, uint8_t* out,
+                   size_t cap, size_t* out_len);
 void orc_build_params(size_t n0, const uint8_t pi[32], int stir, orc_fri_params* out);
 int orc_stir_prove(const uint64_t* f0, size_t n0, const orc_fri_params* p, uint8_t* out, size_t cap, size_t* len);
 int orc_stir_verify(const uint8_t* proof, size_t len, const orc_fri_params* p);

@@ -92,8 +92,8 @@ def lib():
                                            ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
             L.orc_sha256_eval.argtypes = [U64P, U64P, ctypes.c_size_t, ctypes.c_size_t, U64P]
             L.orc_prove_sha256.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_int,
-                                           ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
-                                           ctypes.c_char_p]
+                                           ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t,
+                                           ctypes.POINTER(ctypes.c_size_t), ctypes.c_char_p]
             L.orc_merge_sha512.argtypes = L.orc_merge_sha256.argtypes
             L.orc_sha512_trace.argtypes = L.orc_sha256_trace.argtypes
             L.orc_sha512_eval.argtypes = L.orc_sha256_eval.argtypes
@@ -219,13 +219,13 @@ def merge_sha256(lde_cols, n_trace, blowup, lambdas, n_blocks, phi_mode=PHI_PARA
     return out
 
 
-def prove_sha256(msg: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
+def prove_sha256(msg: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE, blowup: int = 32):
     """prove_ds_ksk_binding core -> (proof bytes, asserted digest)"""
     cap = 1 << 26
     buf = ctypes.create_string_buffer(cap)
     ln = ctypes.c_size_t()
     dg = ctypes.create_string_buffer(32)
-    rc = lib().orc_prove_sha256(msg, len(msg), fs_binding, phi_mode, buf, cap, ctypes.byref(ln), dg)
+    rc = lib().orc_prove_sha256(msg, len(msg), fs_binding, phi_mode, blowup, buf, cap, ctypes.byref(ln), dg)
     assert rc == 0, rc
     return buf.raw[:ln.value], dg.raw
 
@@ -295,12 +295,12 @@ def merge_sha512(lde_cols, n_trace, blowup, lambdas, n_blocks, phi_mode=PHI_PARA
     return out
 
 
-def prove_sha512(msg: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE):
+def prove_sha512(msg: bytes, fs_binding: bytes, phi_mode=PHI_PARALLEL_GATE, blowup: int = 32):
     """SHA-512 AIR proof -> (proof bytes, 64-byte digest read from the H-state)"""
     cap = 1 << 26
     buf = ctypes.create_string_buffer(cap)
     ln = ctypes.c_size_t()
     dg = ctypes.create_string_buffer(64)
-    rc = lib().orc_prove_sha512(msg, len(msg), fs_binding, phi_mode, buf, cap, ctypes.byref(ln), dg)
+    rc = lib().orc_prove_sha512(msg, len(msg), fs_binding, phi_mode, blowup, buf, cap, ctypes.byref(ln), dg)
     assert rc == 0, rc
     return buf.raw[:ln.value], dg.raw

@@ -430,7 +430,7 @@ def _lib():
         sz = ctypes.c_size_t
         L.orc_p256_eval.argtypes = [O.U64P, O.U64P, sz, sz, O.U64P, sz, O.U64P, O.U64P]
         L.orc_merge_p256.argtypes = [O.U64P, sz, O.U64P, sz, O.U64P, sz, sz, O.U64P]
-        L.orc_prove_p256.argtypes = [O.U64P, sz, O.U64P, sz, O.U64P, sz, ctypes.c_char_p, ctypes.c_char_p, sz,
+        L.orc_prove_p256.argtypes = [O.U64P, sz, O.U64P, sz, O.U64P, sz, ctypes.c_char_p, sz, ctypes.c_char_p, sz,
                                      ctypes.POINTER(sz)]
         L._p256_bound = True
     return L
@@ -457,13 +457,13 @@ def merge(lay, lde_cols, n_trace, blowup=BLOWUP):
     return out
 
 
-def prove(lay, tr, pi: bytes) -> bytes:
+def prove(lay, tr, pi: bytes, blowup: int = BLOWUP) -> bytes:
     tr = np.ascontiguousarray(tr, dtype=np.uint64)
     tab = np.ascontiguousarray(lay.table)
     cap = 1 << 24
     buf = ctypes.create_string_buffer(cap)
     ln = ctypes.c_size_t()
     rc = _lib().orc_prove_p256(O._ptr(tr), lay.width, O._ptr(tab), tab.shape[0], O._ptr(lay.tail), tr.shape[1], pi,
-                               buf, cap, ctypes.byref(ln))
+                               blowup, buf, cap, ctypes.byref(ln))
     assert rc == 0, rc
     return buf.raw[:ln.value]

@@ -120,8 +120,8 @@ def _lib():
     if not getattr(L, "_rsa_bound", False):
         L.orc_rsa_eval.argtypes = [O.U64P, O.U64P, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, O.U64P]
         L.orc_merge_rsa.argtypes = [O.U64P, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, O.U64P]
-        L.orc_prove_rsa.argtypes = [O.U64P, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_char_p,
-                                    ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+        L.orc_prove_rsa.argtypes = [O.U64P, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t,
+                                    ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
         L._rsa_bound = True
     return L
 
@@ -141,13 +141,13 @@ def merge(lde_cols, n_records, n_trace=N_TRACE, blowup=BLOWUP):
     return out
 
 
-def prove(tr: np.ndarray, pi: bytes, n_trace=N_TRACE) -> bytes:
+def prove(tr: np.ndarray, pi: bytes, n_trace=N_TRACE, blowup=BLOWUP) -> bytes:
     tr = np.ascontiguousarray(tr, dtype=np.uint64)
     n_records = tr.shape[0] // WIDTH
     cap = 1 << 24
     buf = ctypes.create_string_buffer(cap)
     ln = ctypes.c_size_t()
-    rc = _lib().orc_prove_rsa(O._ptr(tr), n_records, n_trace, pi, buf, cap, ctypes.byref(ln))
+    rc = _lib().orc_prove_rsa(O._ptr(tr), n_records, n_trace, pi, blowup, buf, cap, ctypes.byref(ln))
     assert rc == 0, rc
     return buf.raw[:ln.value]
 
