@@ -253,19 +253,20 @@ __global__ void __launch_bounds__(kPhiThreads, 4) p256_phi_kernel(P256Phi a, uin
     }
   }
   if (g1 == a.n_gadgets && ch + 1 == gridDim.y) {
-    const uint64_t row = i / a.blowup;
-    eval_tail(x, a.lde + (i + a.blowup) % a.n, a.tail, row + 1 == a.n_trace, row + 1 < a.n_trace,
+    const uint64_t row = i / a.row_div;
+    eval_tail(x, a.lde + (i + a.step) % a.n, a.tail, row + 1 == a.n_trace, row + 1 < a.n_trace,
               (uint64_t)a.lam_tail + 1);
   }
   part[(uint64_t)ch * a.n + i] = x.acc.reduce();
 }
 
-__global__ void p256_sum_kernel(const uint64_t* part, uint64_t n, uint32_t chunks, uint64_t* phi) {
+__global__ void p256_sum_kernel(const uint64_t* part, uint64_t n, uint32_t chunks, uint64_t* phi, uint64_t out_stride,
+                                uint64_t out_off) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint64_t s = 0;
   for (uint32_t c = 0; c < chunks; ++c) s = gl::add(s, part[(uint64_t)c * n + i]);
-  phi[i] = s;
+  phi[i * out_stride + out_off] = s;
 }
 
 }  // namespace
@@ -294,14 +295,16 @@ cudaError_t p256_expand(const P256Dev& d, uint64_t k, uint64_t* d_trace, cudaStr
 }
 
 cudaError_t p256_phi(const P256Phi& a, uint32_t n_chunks, uint64_t* d_part, uint64_t* d_phi, cudaStream_t s) {
-  if (a.n % a.blowup || n_chunks == 0 || n_chunks > 65535) return cudaErrorInvalidValue;
+  if (a.row_div == 0 || a.n % a.row_div || a.step == 0 || a.out_stride == 0 || n_chunks == 0 || n_chunks > 65535)
+    return cudaErrorInvalidValue;
   {
     SG_LAUNCH_SCOPE("p256_phi", s);
     p256_phi_kernel<<<dim3((unsigned)((a.n + kPhiThreads - 1) / kPhiThreads), n_chunks), kPhiThreads, 0, s>>>(
         a, d_part);
   }
   SG_LAUNCH_SCOPE("p256_phi_sum", s);
-  p256_sum_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(d_part, a.n, n_chunks, d_phi);
+  p256_sum_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(d_part, a.n, n_chunks, d_phi, a.out_stride,
+                                                                 a.out_off);
   return cudaGetLastError();
 }
 

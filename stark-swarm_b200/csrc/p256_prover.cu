@@ -94,9 +94,49 @@ void p256_merge_device(sg_ctx* c, const uint64_t* d_lde, uint64_t n_trace, uint6
   require((1ull << ln) == n && ln <= kMaxLogN && n_trace >= 2, "p256 merge: bad sizes");
   cudaStream_t s = c->stream;
   DBuf part((uint64_t)T.n_chunks * n, s), phi(n, s), scratch(ntt_scratch_elems(1, ln), s);
-  P256Phi a{d_lde, n, blowup, n_trace, T.table, T.lam, T.chunk, T.tail, (uint32_t)L.table.size(),
-            L.n_constraints - p256::TAIL_CONSTRAINTS};
+  P256Phi a{d_lde, n, blowup, n_trace, blowup, blowup, 1, 0, T.table, T.lam, T.chunk, T.tail,
+            (uint32_t)L.table.size(), L.n_constraints - p256::TAIL_CONSTRAINTS};
   cuda_check(p256_phi(a, T.n_chunks, part.p, phi.p, s), "p256 phi");
+  cuda_check(ntt_batch(c->tw, phi.p, phi.p, 1, n, n, (int)ln, true, n, scratch.p, s), "intt");
+  cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
+  cuda_check(ntt_batch(c->tw, d_c, d_c, 1, n, n, (int)ln, false, n - n_trace, scratch.p, s), "ntt");
+}
+
+// The same merge without materialising the LDE (the reference's streaming merge,
+// deep_ali_merge_ecdsa_double_multirow_streaming, lib.rs:1421-1681, which also
+// never holds the whole LDE): LDE point r + blowup a lies on coset r, whose
+// values are NTT_{n_trace}(c_k w_n^{r k}) of the trace coefficients c, and the
+// next row of that point is point a + 1 of the same coset. Each coset is
+// produced (coset 0 is the trace itself), its Phi values are written to
+// Phi[r + blowup a], and it is dropped: the device holds the trace, its
+// coefficients and one coset (3 x 310 MB for K = 256) instead of the 9.9 GB LDE.
+void p256_merge_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, uint64_t blowup, uint64_t* d_c) {
+  const p256::Layout& L = p256::layout();
+  const P256Tables& T = p256_tables();
+  const uint64_t n = n_trace * blowup, W = L.width;
+  const unsigned ln = lg2(n), lt = lg2(n_trace);
+  require((1ull << ln) == n && (1ull << lt) == n_trace && ln <= kMaxLogN && n_trace >= 2, "p256 merge: bad sizes");
+  cudaStream_t s = c->stream;
+  DBuf part((uint64_t)T.n_chunks * n_trace, s), phi(n, s), coef(W * n_trace, s), ev(W * n_trace, s);
+  DBuf scratch(std::max(ntt_scratch_elems((uint32_t)W, (int)lt), ntt_scratch_elems(1, (int)ln)), s);
+  DBuf twist_tab(n_trace, s);
+  cuda_check(ntt_batch(c->tw, d_trace, coef.p, (uint32_t)W, n_trace, n_trace, (int)lt, true, n_trace, scratch.p, s),
+             "p256 trace intt");
+  for (uint64_t r = 0; r < blowup; ++r) {
+    const uint64_t* evals = d_trace;
+    if (r > 0) {
+      cuda_check(pow_table_device(c->tw, r, (int)ln, n_trace, twist_tab.p, s), "twist table");
+      PowSpec twist;
+      twist.tab = twist_tab.p;
+      cuda_check(ntt_batch(c->tw, coef.p, ev.p, (uint32_t)W, n_trace, n_trace, (int)lt, false, n_trace, scratch.p, s,
+                           &twist),
+                 "p256 coset ntt");
+      evals = ev.p;
+    }
+    P256Phi a{evals, n_trace, blowup, n_trace, 1, 1, blowup, r, T.table, T.lam, T.chunk, T.tail,
+              (uint32_t)L.table.size(), L.n_constraints - p256::TAIL_CONSTRAINTS};
+    cuda_check(p256_phi(a, T.n_chunks, part.p, phi.p, s), "p256 coset phi");
+  }
   cuda_check(ntt_batch(c->tw, phi.p, phi.p, 1, n, n, (int)ln, true, n, scratch.p, s), "intt");
   cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
   cuda_check(ntt_batch(c->tw, d_c, d_c, 1, n, n, (int)ln, false, n - n_trace, scratch.p, s), "ntt");
@@ -104,18 +144,25 @@ void p256_merge_device(sg_ctx* c, const uint64_t* d_lde, uint64_t n_trace, uint6
 
 std::vector<uint8_t> prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
                                        const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, uint64_t k,
-                                       const uint8_t pi[32], bool self_verify) {
+                                       const uint8_t pi[32], bool self_verify, uint64_t blowup) {
   const p256::Layout& L = p256::layout();
-  const uint64_t blowup = p256::BLOWUP, n0 = k * blowup, W = L.width;
+  require(blowup >= 2 && blowup <= 1024 && !(blowup & (blowup - 1)), "prove: blowup must be a power of 2 in [2, 1024]");
+  const uint64_t n0 = k * blowup, W = L.width;
   cudaStream_t s = c->stream;
   DBuf d_c(n0, s);
   {
     DBuf d_trace(W * k, s);
     p256_trace_device(c, ax, ay, a_bits, bx, by, b_bits, k, d_trace.p);
-    DBuf d_lde(W * n0, s);
-    lde_device(c, d_trace.p, W, k, blowup, 1, d_lde.p);
-    d_trace = DBuf();
-    p256_merge_device(c, d_lde.p, k, blowup, d_c.p);
+    const bool cosets = c->wide_merge == SG_WIDE_MERGE_COSETS ||
+                        (c->wide_merge == SG_WIDE_MERGE_AUTO && W * n0 * 8 > (2ull << 30));
+    if (cosets) {
+      p256_merge_cosets(c, d_trace.p, k, blowup, d_c.p);
+    } else {
+      DBuf d_lde(W * n0, s);
+      lde_device(c, d_trace.p, W, k, blowup, 1, d_lde.p);
+      d_trace = DBuf();
+      p256_merge_device(c, d_lde.p, k, blowup, d_c.p);
+    }
   }
   sg_fri_params p;
   sg_build_params(n0, pi, 1, &p);
@@ -127,10 +174,10 @@ std::vector<uint8_t> prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const ui
 
 std::vector<uint8_t> prove_p256_ecdsa(sg_ctx* c, const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32],
                                       const uint8_t sgn[32], const uint8_t digest[32], const uint8_t pi[32],
-                                      bool self_verify) {
+                                      bool self_verify, uint64_t blowup) {
   uint8_t u1[256], u2[256];
   p256::u_bits(digest, r, sgn, u1, u2);
-  return prove_p256_chains(c, p256::GX, p256::GY, u1, qx, qy, u2, p256::K_ECDSA, pi, self_verify);
+  return prove_p256_chains(c, p256::GX, p256::GY, u1, qx, qy, u2, p256::K_ECDSA, pi, self_verify, blowup);
 }
 
 }  // namespace sg
