@@ -28,6 +28,7 @@
 #include "counters.hpp"
 #include "dft.cuh"
 #include "gl.cuh"
+#include "keccak.cuh"
 #include "ntt.cuh"
 
 namespace sg {
@@ -726,6 +727,179 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
   c.in_valid = N;
   c.scale = ninv;
   return launch_pass_dyn(la, c, inverse, n_cols, s);
+}
+
+// ------------------------------------------------------------------ fused LDE -> leaf hash
+// The forward transform of a zero-padded (LDE) column set whose last pass is a
+// 2^7-point DFT fused with the Merkle leaf hash of the LDE rows: leaf r =
+// SHA3(DsLabel{arity0, level 0xFFFFFFFF, position r, label} || row r of all
+// w columns) (merkle/src/lib.rs:95-113, 391-476 over trace_import.rs:251-281's
+// LDE). A CTA owns 4 consecutive last-pass lanes h (rows i1 * BC + h, i1 < 128):
+// 512 rows, one per thread, whose sponge states stay in registers while the CTA
+// walks the columns 16 at a time: it stages the 64 lanes' last-pass inputs of 16
+// columns in shared memory, runs the two Stockham stages (radix 16, radix 8) of
+// the 128-point DFT, and each thread absorbs its row's 16 values. The LDE itself
+// need not be written (only its first keep_cols columns are, e.g. the column a
+// STIR proof takes next): the 8 + 64 bytes per row that reach the tree replace the
+// LDE write and the leaf kernel's full re-read.
+namespace {
+
+constexpr int kFuseLogA = 7, kFuseA = 1 << kFuseLogA;
+constexpr int kFuseLanes = 4, kFuseCols = 16;
+constexpr int kFuseTileLanes = kFuseLanes * kFuseCols;          // 64 DFT lanes per tile
+constexpr int kFuseThreads = kFuseTileLanes * kFuseA / 16;      // 512 = rows per CTA
+constexpr int kFuseMp = kFuseA + (kFuseA >> 4);                 // padded lane stride in shared memory
+static_assert(kFuseThreads == kFuseLanes * kFuseA, "one hashing thread per row");
+static_assert(pass_log_k(kFuseLogA) == 6 && row_stride(kFuseLogA) == kFuseMp,
+              "the tile has the shape of a 2^7 pass");
+
+struct LeafFuse {
+  const uint64_t* in;  // last-pass input: column c, lane h, point m at in + c * N + h * 128 + m
+  uint64_t N, BC;      // LDE length; row of (i1, lane h) = i1 * BC + h
+  uint32_t w, keep_cols;
+  uint64_t arity0, label;
+  uint64_t* leaves;  // N digests (level 0 of the tree)
+  uint64_t* out;     // the LDE's first keep_cols columns (column stride N), or null
+  const uint64_t* tw_st;
+};
+
+__global__ void __launch_bounds__(kFuseThreads, 1) lde_leaf_kernel(LeafFuse a) {
+  extern __shared__ uint64_t sm[];
+  uint64_t* stw = sm + kFuseTileLanes * kFuseMp;
+  const int t = threadIdx.x;
+  const uint64_t lane0 = (uint64_t)blockIdx.x * kFuseLanes;
+  for (int j = t; j < kFuseA; j += kFuseThreads) stw[j] = __ldg(a.tw_st + (j << (12 - kFuseLogA)));
+  // this thread's row: lane hl, point hi1 (consecutive threads: consecutive points,
+  // conflict-free shared reads)
+  const int hl = t / kFuseA, hi1 = t % kFuseA;
+  const uint64_t row = (uint64_t)hi1 * a.BC + lane0 + hl;
+  kc::LaneSponge sp;
+  sp.init();
+  sp.lane(a.arity0);
+  sp.lane(0xFFFFFFFFull);
+  sp.lane(row);
+  sp.lane(a.label);
+#pragma unroll 1
+  for (uint32_t c0 = 0; c0 < a.w; c0 += kFuseCols) {
+    // tile lane L = cc * 4 + l: column c0 + cc, last-pass lane lane0 + l (128 contiguous inputs)
+#pragma unroll 4
+    for (int e = t; e < kFuseTileLanes * kFuseA; e += kFuseThreads) {
+      const int L = e >> kFuseLogA, m = e & (kFuseA - 1);
+      const int cc = L / kFuseLanes, l = L % kFuseLanes;
+      sm[L * kFuseMp + padi(m)] = __ldg(a.in + (uint64_t)(c0 + cc) * a.N + (lane0 + l) * kFuseA + m);
+    }
+    __syncthreads();
+    stockham_stage<16, 16, false, kFuseLogA, true>(sm, t, kFuseThreads, kFuseLogA, kFuseMp, 0, stw);
+    stockham_stage<8, 16, false, kFuseLogA, true>(sm, t, kFuseThreads, kFuseLogA, kFuseMp, 4, stw);
+#pragma unroll 1
+    for (int cc = 0; cc < kFuseCols; ++cc) {
+      const uint64_t v = sm[(cc * kFuseLanes + hl) * kFuseMp + padi(hi1)];
+      sp.lane(v);
+      if (c0 + cc < a.keep_cols) a.out[(uint64_t)(c0 + cc) * a.N + row] = v;
+    }
+    __syncthreads();  // the next tile overwrites the shared rows
+  }
+  uint64_t d[kc::kDigestLanes];
+  sp.finish(d);
+#pragma unroll
+  for (int q = 0; q < kc::kDigestLanes; ++q) a.leaves[(uint64_t)kc::kDigestLanes * row + q] = d[q];
+}
+
+}  // namespace
+
+bool lde_leaf_ok(uint32_t w, int log_n) {
+  return w >= kFuseCols && w % kFuseCols == 0 && log_n >= kFuseLogA + 2 && log_n <= kFuseLogA + 24;
+}
+
+uint64_t lde_leaf_scratch_elems(uint32_t w, int log_n) {
+  const int r = log_n - kFuseLogA;
+  return (r <= 12 ? 1ull : 2ull) * w * (1ull << log_n);
+}
+
+cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t in_stride, uint32_t w, int log_n,
+                               uint64_t n_valid, const PowSpec* pre, uint64_t* scratch, uint64_t arity0,
+                               uint64_t label, uint64_t* leaves, uint64_t* out, uint32_t keep_cols, cudaStream_t s) {
+  if (!lde_leaf_ok(w, log_n) || !scratch || !leaves || keep_cols > w || (keep_cols && !out))
+    return cudaErrorInvalidValue;
+  const uint64_t N = 1ull << log_n, A = kFuseA;
+  if (n_valid > N) n_valid = N;
+  const PowSpec none{};
+  const int r = log_n - kFuseLogA;
+  const uint64_t* last_in;
+  uint64_t BC;
+  if (r <= 12) {
+    // four-step with N1 = 2^7: pass 1 as ntt_batch's, transposed into scratch
+    const uint64_t N2 = 1ull << r;
+    PassArgs a = base_args(t, false);
+    a.in = in;
+    a.out = scratch;
+    a.in_col = in_stride;
+    a.out_col = N;
+    a.in_lane = 1;
+    a.in_m = A;
+    a.out_lane = 1;
+    a.out_i = A;
+    a.n_lanes = A;
+    a.flat_lane = 1;
+    a.in_valid = n_valid;
+    a.sparse_nz = sparse_nz_for(n_valid, N, A, N2);
+    a.tw_log = log_n;
+    a.pre = pre ? *pre : none;
+    cudaError_t e = launch_pass_dyn(r, a, false, w, s);
+    if (e != cudaSuccess) return e;
+    last_in = scratch;
+    BC = N2;
+  } else {
+    // three passes N = A * B * C with C = 2^12 and B = 2^(r - 12), as ntt_batch's
+    const int lc = 12, lb = r - 12;
+    const uint64_t B = 1ull << lb, C = 1ull << lc, AB = A * B;
+    uint64_t* s1 = scratch;
+    uint64_t* s2 = scratch + (uint64_t)w * N;
+    PassArgs a = base_args(t, false);
+    a.in = in;
+    a.out = s1;
+    a.in_col = in_stride;
+    a.out_col = N;
+    a.in_lane = 1;
+    a.in_m = AB;
+    a.out_lane = 1;
+    a.out_i = AB;
+    a.n_lanes = AB;
+    a.flat_lane = 1;
+    a.in_valid = n_valid;
+    a.sparse_nz = sparse_nz_for(n_valid, N, AB, C);
+    a.tw_log = log_n;
+    a.pre = pre ? *pre : none;
+    cudaError_t e = launch_pass_dyn(lc, a, false, w, s);
+    if (e != cudaSuccess) return e;
+    PassArgs b = base_args(t, false);
+    b.in = s1;
+    b.out = s2;
+    b.y_sub = (uint32_t)C;
+    b.in_col = N;
+    b.in_sub = AB;
+    b.out_col = N;
+    b.out_sub = A;
+    b.in_lane = 1;
+    b.in_m = A;
+    b.out_lane = 1;
+    b.out_i = C * A;
+    b.n_lanes = A;
+    b.flat_lane = 1;
+    b.in_valid = AB;
+    b.tw_log = kFuseLogA + lb;
+    e = launch_pass_dyn(lb, b, false, (uint64_t)w * C, s);
+    if (e != cudaSuccess) return e;
+    last_in = s2;
+    BC = B * C;
+  }
+  LeafFuse f{last_in, N, BC, w, keep_cols, arity0, label, leaves, out, t.d_fwd_st};
+  const size_t smem = ((size_t)kFuseTileLanes * kFuseMp + kFuseA) * sizeof(uint64_t);
+  cudaError_t e = cudaFuncSetAttribute(lde_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  SG_LAUNCH_SCOPE("lde_leaf", s);
+  lde_leaf_kernel<<<(unsigned)(BC / kFuseLanes), kFuseThreads, smem, s>>>(f);
+  return cudaGetLastError();
 }
 
 }  // namespace sg

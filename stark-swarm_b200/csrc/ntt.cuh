@@ -92,6 +92,20 @@ bool ntt_coset_eval_ok(int log_m, int log_b);
 cudaError_t ntt_coset_eval(const NttTables& t, const uint64_t* coef, uint64_t* out, uint32_t n_cols, int log_m,
                            int log_b, cudaStream_t s, const PowSpec* pre = nullptr);
 
+// Forward transform of w zero-padded columns (as ntt_batch with in_stride and
+// n_valid) whose last pass, a 2^7-point DFT, hashes the rows of the result into
+// Merkle leaves instead of storing them: leaf r (kc::kDigestLanes lanes at
+// leaves + r * kDigestLanes) = SHA3 of the build's profile of
+// {arity0, 0xFFFFFFFF, r, label} || row r of the w columns. Only the first
+// keep_cols columns of the result are written (to out, column stride 2^log_n).
+// Needs lde_leaf_ok (w a multiple of 16, 2^9 <= N <= 2^31) and
+// lde_leaf_scratch_elems(w, log_n) elements of scratch.
+bool lde_leaf_ok(uint32_t w, int log_n);
+uint64_t lde_leaf_scratch_elems(uint32_t w, int log_n);
+cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t in_stride, uint32_t w, int log_n,
+                               uint64_t n_valid, const PowSpec* pre, uint64_t* scratch, uint64_t arity0,
+                               uint64_t label, uint64_t* leaves, uint64_t* out, uint32_t keep_cols, cudaStream_t s);
+
 }  // namespace sg
 
 #if defined(__CUDACC__)

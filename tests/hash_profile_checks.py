@@ -144,6 +144,11 @@ def gpu_checks():
             assert got == O.merkle_root(rows, arities, label), n
             if n <= 100:
                 assert got == py_merkle(rows, arities, label), n
+        # LDE + row commitment in one call (the fused last pass hashes with this profile's SHA3)
+        tr = np.random.default_rng(9).integers(0, P, (32, 1 << 9), dtype=np.uint64)
+        lde = O.lde(tr, 8, 7)
+        assert ctx.lde_commit(tr, 8, 7, [16, 16, 16, 16], 3) == \
+            O.merkle_root(np.ascontiguousarray(lde.T), [16, 16, 16, 16], 3)
         for lg in (3, 8, 12, 16):
             n0 = 1 << lg
             f0 = low_degree(n0, lg)
