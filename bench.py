@@ -140,9 +140,21 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) per step of each kernel family on this workload (64
-# columns), from one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum over
-# the step's launches (profiles/ntt_pass_traffic_cfg2_64x2p20.md).
+# columns): one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum over
+# the 16 ntt_pass launches of one step (a single-pass metric set).
 MEASURED_TRAFFIC_PER_STEP = {"ntt_pass": 15.711e9}
+# From ncu summaries of the same kernels on the reduced (4-column, 2^20 -> 2^23) case,
+# scaled to 64 columns by the columns processed: ALU-pipe share of active cycles
+# (the integer roofline of these kernels) and DRAM bytes per 64-column LDE.
+MEASURED_NTT = {}
+
+
+def run_config(ws):
+    """The config dict of the JSON line, the same for both arms."""
+    return dict(CONFIG, parallelism=f"{ws} independent proofs (one per GPU), no collective")
+
+
+DTYPE = "u64 (Goldilocks) / Fp6"
 
 # ---------------------------------------------------------------- CPU side
 def load_oracle():
@@ -163,53 +175,74 @@ def load_oracle_rsa():
     return oracle_rsa
 
 
-def cpu_sample(trace, threads):
-    """Time the oracle (C++ restatement of the reference CPU prover, OpenMP) on a
-    bounded sample and scale to one full step: LDE of 8 of the 64 columns (x8),
-    Merkle leaf+tree hashing of 2^20 of the 2^23 rows of 64 columns (x8), and
-    STIR on a 2^21 domain (x4; STIR work is linear in the domain)."""
-    O = load_oracle()
-    O.set_threads(threads)
-    t0 = time.perf_counter()
-    O.lde(trace[:8], BLOWUP, SHIFT)
-    t_lde = time.perf_counter() - t0
-    rows = np.random.default_rng(9).integers(0, P, size=(1 << 20, W), dtype=np.uint64)
-    t0 = time.perf_counter()
-    O.merkle_root(rows, [16] * 5, TREE_LABEL)
-    t_mk = time.perf_counter() - t0
-    f0 = np.random.default_rng(10).integers(0, P, size=1 << 21, dtype=np.uint64)
-    t0 = time.perf_counter()
-    O.stir_prove(f0, O.build_params(1 << 21, PI_HASH))
-    t_stir = time.perf_counter() - t0
-    full = 8 * t_lde + 8 * t_mk + 4 * t_stir
-    sample = ("oracle on 8/64 LDE columns (x8), Merkle over 2^20/2^23 rows of 64 cols (x8), STIR at 2^21 (x4); "
-              f"measured {t_lde:.2f}+{t_mk:.2f}+{t_stir:.2f} s")
-    return 1.0 / full, sample, t_lde + t_mk + t_stir
+def cpu_sample_fraction(threads):
+    """The share of one proof that a CPU sample computes: 16 of the 64 LDE columns
+    (one per core on a 16-core host; 32 or all 64 on larger hosts, so that the
+    column-parallel LDE keeps every core busy), and the same share of the Merkle
+    rows and of the STIR domain."""
+    cols = 16 if threads <= 16 else 32 if threads <= 32 else 64
+    return cols / W if W == 64 else 1.0
+
+
+class CpuSample:
+    """A bounded sample of the step on the CPU oracle (the C++ restatement of the
+    reference CPU prover, OpenMP on every host core): the LDE of `frac` of the
+    trace columns, Merkle leaf + tree hashing of `frac` of the 2^23 LDE rows
+    (64 columns, arity 16), and the STIR proof of a domain `frac` as large. Each
+    part is `frac` of the work of the same part of the full step, so
+    frac / (measured seconds) is the CPU's proofs/s, measured rather than scaled
+    from a different shape."""
+
+    def __init__(self, trace, threads):
+        self.O = load_oracle()
+        self.threads = threads
+        self.frac = cpu_sample_fraction(threads)
+        cols = max(1, int(round(W * self.frac)))
+        self.lde_cols = trace[:cols]
+        rows = int(N0 * self.frac)
+        self.rows = np.random.default_rng(9).integers(0, P, size=(rows, W), dtype=np.uint64)
+        self.f0 = np.random.default_rng(10).integers(0, P, size=rows, dtype=np.uint64)
+        self.arities = [16] * max(1, (rows.bit_length() - 1 + 3) // 4)
+        self.params = self.O.build_params(rows, PI_HASH)
+        self.desc = (f"one {self.frac:g} share of the step per sample: oracle LDE of {cols}/{W} columns "
+                     f"(2^{LOG_N} -> 2^{LOG_N + 3}), Merkle over {rows}/{N0} LDE rows of {W} columns, "
+                     f"STIR at n0 {rows}")
+
+    def run(self):
+        """-> seconds for one sample"""
+        O = self.O
+        O.set_threads(self.threads)
+        t0 = time.perf_counter()
+        O.lde(self.lde_cols, BLOWUP, SHIFT)
+        O.merkle_root(self.rows, self.arities, TREE_LABEL)
+        O.stir_prove(self.f0, self.params)
+        return time.perf_counter() - t0
 
 
 def run_reference(args, ws, rank):
+    """The CPU arm: rank 0 times the oracle on all host cores, one bounded sample
+    per step; ms_per_step is the measured sample time and value = frac / time."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    trace = make_trace(0)
+    cs = CpuSample(make_trace(0), threads)
     for _ in range(args.warmup):
-        cpu_sample(trace, threads)
-    vals = []
+        cs.run()
     t_start = time.perf_counter()
-    for _ in range(args.steps):
-        v, sample, _ = cpu_sample(trace, threads)
-        vals.append(v)
+    times = [cs.run() for _ in range(args.steps)]
     wall = time.perf_counter() - t_start
-    value = statistics.median(vals)
+    value = args.steps * cs.frac / wall
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": "synthetic (seeded uniform)",
-        "config": dict(CONFIG, parallelism="rank 0 only, CPU"),
-        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port", "sample": sample},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPE,
+        "data": "synthetic (seeded uniform trace)", "config": run_config(ws),
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "port",
+                         "sample": cs.desc, "proofs_per_step": cs.frac},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "sample_wall_s": wall,
-        "note": "the reference is Rust (no toolchain here); this is the C++ oracle restatement of its CPU prover",
+        "sample_s": {"median": statistics.median(times), "min": min(times), "max": max(times)},
+        "note": "the reference is Rust (no toolchain here); this is the C++ oracle restatement of its CPU "
+                f"prover; each step proves a {cs.frac:g} share of one proof, and ms_per_step is that measured time",
     }
     print(json.dumps(line), flush=True)
 
@@ -255,8 +288,8 @@ def sha256_large(sg, ctx, blocks, reps, cpu_threads):
         # prover work grows as n0 log n0 (LDE, quotient and STIR transforms dominate)
         scale = (n0 * (n0.bit_length() - 1)) / (n0_s * (n0_s.bit_length() - 1))
         est = t_cpu * scale
-        res["cpu_baseline"] = {"s_per_proof": est, "cores": cpu_threads, "kind": "port",
-                               "sample": f"oracle proof at n0 2^{n0_s.bit_length() - 1} took {t_cpu:.2f} s, "
+        res["cpu_baseline"] = {"s_per_proof": est, "cores": cpu_threads, "kind": "port", "extrapolated": True,
+                               "sample": f"EXTRAPOLATED: oracle proof at n0 2^{n0_s.bit_length() - 1} took {t_cpu:.2f} s, "
                                          f"scaled by n0 log n0 (x{scale:.0f}); the full size needs "
                                          f"{756 * n0 * 8 / 2**30:.0f} GiB for the materialised LDE"}
         res["gpu_over_cpu"] = est / sec
@@ -402,7 +435,8 @@ def p256_ecdsa(sg, ctx, n_jobs, cpu_threads):
         assert cpu_proof == ctx.prove_p256_chains(E.G, u1[:k], q, u2[:k], pi), "GPU and oracle chain proofs differ"
         scale = 256 // k
         out["cpu_baseline"] = {"proofs_per_s": 1.0 / (dt * scale), "cores": cpu_threads, "kind": "port",
-                               "sample": f"oracle proof of the first {k} rows of both chains (n0 {k * 32}) took "
+                               "extrapolated": True,
+                               "sample": f"EXTRAPOLATED: oracle proof of the first {k} rows of both chains (n0 {k * 32}) took "
                                          f"{dt:.2f} s, scaled by n0 (x{scale}: the merge, linear in n0, dominates)"}
         out["plain_over_cpu"] = out["plain"]["proofs_per_s"] * dt * scale
     return out
@@ -475,6 +509,72 @@ def serving(sg, ctx, rates, n_jobs, streams, seed=7):
     return out
 
 
+def record_check_jobs(sg, n_jobs, seed=6, blowup=4):
+    """The batched mixed-proving workload: n_jobs synthetic DNS-zone record checks
+    (seeded). Each record is random bytes of lognormal length (median 120 B,
+    sigma 0.6, clipped to 40-600 B) and gets two independent proofs at LDE
+    blowup `blowup`: a SHA-256 AIR proof over the record bytes (1-10 blocks,
+    n_trace 128-2048, with the reference's parallel-build Phi gate: Phi = 0
+    below n0 = 4096) and a signature-check proof over SHA-256(record): ECDSA-P256
+    (60 %, K = 256 rows) or RSA-2048 PKCS#1 v1.5 (40 %, n_trace 32)."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.round(rng.lognormal(np.log(120), 0.6, n_jobs)), 40, 600).astype(int)
+    recs = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in lens]
+    alg = rng.random(n_jobs)
+    keys = rsa_keys()
+    ecdsa_keys = []
+    for i in range(16):
+        d = int.from_bytes(np.random.default_rng(7000 + i).bytes(32), "big") % (P256_N - 1) + 1
+        ecdsa_keys.append((d, _p256_mul(d, P256_G)))
+    jobs, kinds = [], []
+    for i in range(n_jobs):
+        jobs.append((sg.JOB_SHA256, recs[i], hashlib.sha3_256(b"record-check-%d" % i).digest(), 0, blowup))
+        kinds.append("sha256")
+        digest = hashlib.sha256(recs[i]).digest()
+        if alg[i] < 0.6:
+            d, q = ecdsa_keys[i % 16]
+            k = int.from_bytes(rng.bytes(32), "big") % (P256_N - 1) + 1
+            e = int.from_bytes(digest, "big") % P256_N
+            r = _p256_mul(k, P256_G)[0] % P256_N
+            s_ = pow(k, -1, P256_N) * (e + r * d) % P256_N
+            jobs.append((sg.JOB_P256_ECDSA, (q, r, s_, digest), sg.p256_ecdsa_pi(q[0], q[1], r, s_, digest), 0, blowup))
+            kinds.append("p256_ecdsa")
+        else:
+            rec, pi = rsa_record(sg, recs[i], keys[i % len(keys)])
+            jobs.append((sg.JOB_RSA2048, [rec], pi, 0, blowup))
+            kinds.append("rsa2048")
+    return jobs, kinds, lens
+
+
+def record_checks(sg, ctx, n_jobs, streams):
+    """Batched mixed proving: the record-check workload (2 proofs per record, blowup
+    4) proved one proof at a time on one stream (the plain GPU loop) and with
+    `streams` proofs in flight under a 160 GB HBM budget. Every proof of the
+    batched run must equal the same proof made alone."""
+    jobs, kinds, lens = record_check_jobs(sg, n_jobs)
+    ctx.prove_batch(jobs[:4 * streams], n_streams=streams, hbm_budget_bytes=160 << 30)  # pool warm-up
+    out = {"workload": f"{n_jobs} DNS-zone record checks (seed 6): SHA-256 AIR proof over lognormal(median 120 B, "
+                       "sigma 0.6, 40-600 B) record bytes + ECDSA-P256 (60 %) or RSA-2048 (40 %) signature-check "
+                       "proof, blowup 4, s0 = 54, STIR make_schedule(n0); every proof self-verified",
+           "records": n_jobs, "proofs": len(jobs),
+           "mix": {k: kinds.count(k) for k in sorted(set(kinds))},
+           "sha256_blocks": {"min": int((lens.min() + 9 + 63) // 64), "max": int((lens.max() + 9 + 63) // 64)}}
+    proofs = {}
+    for label, st in (("plain", 1), ("batched", streams)):
+        t0 = time.perf_counter()
+        res = ctx.prove_batch(jobs, n_streams=st, hbm_budget_bytes=160 << 30)
+        dt = time.perf_counter() - t0
+        assert all(r.status == 0 for _, r in res), "a record-check proof failed"
+        proofs[label] = [p for p, _ in res]
+        lat = sorted(r.latency_ms for _, r in res)
+        out[label] = {"streams": st, "proofs_per_s": len(jobs) / dt, "records_per_s": n_jobs / dt, "s": dt,
+                      "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
+    assert proofs["plain"] == proofs["batched"], "a proof in the batch differs from the same proof alone"
+    out["batched_over_plain"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
+    out["identical_alone_and_batched"] = True
+    return out
+
+
 def algorithmic_bytes():
     """Minimal HBM bytes per step for each kernel family (read inputs once, write outputs once)."""
     lde = (W * N + W * N0) * 8                       # read trace, write LDE
@@ -503,11 +603,16 @@ def main():
     ap.add_argument("--rsa-jobs", type=int, default=256,
                     help="single-record RSA-2048 proofs for the plain-vs-batched section (0 skips it)")
     ap.add_argument("--rsa-stacked", type=int, default=64, help="records in the stacked RSA-2048 proof (0 skips)")
+    ap.add_argument("--record-checks", type=int, default=1024,
+                    help="records of the batched mixed-proving section (2 proofs each, blowup 4; 0 skips it)")
     ap.add_argument("--ecdsa-jobs", type=int, default=32,
                     help="ECDSA-P256 proofs for the plain-vs-batched section (0 skips it)")
     ap.add_argument("--serve-rates", default="50,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--no-classic-fri", dest="classic_fri", action="store_false",
                     help="skip the classic DEEP-FRI timing")
+    ap.add_argument("--pipeline", choices=["fused", "split"], default="fused",
+                    help="fused: the LDE's last pass hashes the rows (sg_lde_commit) while column 0's LDE and its "
+                         "STIR proof run beside it; split: LDE, then Merkle and STIR concurrently")
     ap.add_argument("--columns", type=int, default=64,
                     help="trace columns (64 = the benchmark workload; fewer for small profiling captures)")
     args = ap.parse_args()
@@ -547,20 +652,45 @@ def main():
         root = ctx.merkle_commit(d_lde, ARITIES, TREE_LABEL)
         return root, fut.result()
 
-    def step_device():
+    def split_device():
         ctx.lde(d_trace, BLOWUP, SHIFT, out=d_lde)  # returns once the LDE is complete
         return commit_and_prove()
 
-    def step_e2e():
+    def split_e2e():
         ctx.lde(h_trace, BLOWUP, SHIFT, out=d_lde)  # host (pinned) input: H2D inside the call
         return commit_and_prove()
 
-    # warm-up, and a determinism check: every step must give the same bytes
+    # fused: column 0's LDE and its STIR proof on the second context, beside the
+    # LDE + row commitment of all columns whose last pass hashes the rows
+    d_col0 = torch.empty((1, N0), dtype=torch.int64, device="cuda")
+
+    def stir_col0(src):
+        ctx2.lde(src, BLOWUP, SHIFT, out=d_col0)
+        return ctx2.deep_fri_prove(d_col0[0], N0, params)
+
+    def fused_device():
+        fut = pool.submit(stir_col0, d_trace[0:1])
+        root = ctx.lde_commit(d_trace, BLOWUP, SHIFT, ARITIES, TREE_LABEL)
+        return root, fut.result()
+
+    def fused_e2e():
+        fut = pool.submit(stir_col0, h_trace[0:1])  # host (pinned) input: H2D inside the calls
+        root = ctx.lde_commit(h_trace, BLOWUP, SHIFT, ARITIES, TREE_LABEL)
+        return root, fut.result()
+
+    fused = args.pipeline == "fused"
+    step_device = fused_device if fused else split_device
+    step_e2e = fused_e2e if fused else split_e2e
+
+    # warm-up, and a determinism check: every step must give the same bytes, and
+    # the two pipelines the same root and proof
     ref = None
     for _ in range(max(1, args.warmup)):
         out = step_device()
         assert ref is None or out == ref, "non-deterministic proof"
         ref = out
+    other = split_device() if fused else fused_device()
+    assert other == ref, "the fused and split pipelines disagree"
     assert sg.deep_fri_verify(params, ref[1]), "proof rejected by the verifier"
     torch.cuda.synchronize()
 
@@ -605,13 +735,28 @@ def main():
     e2e_ms = dist_max(e0.elapsed_time(e1), ws)
     e2e_value = ws * args.steps / (e2e_ms / 1000.0)
 
+    # the other pipeline, timed the same way, for comparison
+    other_step = split_device if fused else fused_device
+    e0.record(stream)
+    for _ in range(args.steps):
+        out = other_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert out == ref
+    other_ms = dist_max(e0.elapsed_time(e1), ws) / args.steps
+
     # LDE stage alone (trace and LDE in HBM): the NTT/LDE GB/s of the metric,
-    # algorithmic bytes = read the trace once + write the LDE once
+    # algorithmic bytes = read the trace once + write the LDE once; the profiler
+    # gives ntt_pass's launches inside it
+    sg.profile_reset()
+    sg.profile_enable(True)
     e0.record(stream)
     for _ in range(args.steps):
         ctx.lde(d_trace, BLOWUP, SHIFT, out=d_lde)
     e1.record(stream)
     torch.cuda.synchronize()
+    sg.profile_enable(False)
+    prof_lde = sg.profile_read()
     lde_ms = dist_max(e0.elapsed_time(e1), ws) / args.steps
 
     # roofline of the dominant kernel family (CUDA events recorded on the launching stream)
@@ -621,30 +766,48 @@ def main():
     except (OSError, ValueError):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    alg = algorithmic_bytes()
-    # The LDE runs alone on the GPU; the Merkle commitment and the STIR proof run
-    # concurrently on two streams, so their event-bracketed times include time they
-    # share with each other (merkle_leaves alone: about 14 ms per step). The dominant
-    # family by device time is therefore taken among the kernels that run alone.
-    alone = [k for k in prof if k == "ntt_pass"]
-    fam = alone[0] if alone else (max(prof, key=lambda k: prof[k][1]) if prof else None)
-    roofline = None
-    if fam:
-        n_l, ms = prof[fam]
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    def roof(fam, profile, runs, alg_bytes_per_run, extra=None):
+        """roofline entry of one kernel family from its event-timed launches"""
+        if fam not in profile:
+            return None
+        n_l, ms = profile[fam]
         per_launch_ms = ms / n_l
-        launches_per_step = n_l / args.steps
-        if fam in alg:
-            bytes_per_launch = alg[fam] / launches_per_step
-            achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
-        else:
-            bytes_per_launch, achieved = None, None
-        roofline = {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": (achieved / hbm_peak) if achieved else None,
-                    "traffic": (MEASURED_TRAFFIC_PER_STEP[fam] / launches_per_step
-                                if fam in MEASURED_TRAFFIC_PER_STEP and W == 64 else None),
-                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                    "alg_bytes_per_launch": bytes_per_launch, "avg_launch_ms": per_launch_ms,
-                    "launches_per_step": launches_per_step}
+        per_run = n_l / runs
+        bytes_per_launch = alg_bytes_per_run / per_run
+        achieved = bytes_per_launch / (per_launch_ms / 1e3) / 1e9
+        r = {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+             "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+             "alg_bytes_per_launch": bytes_per_launch, "avg_launch_ms": per_launch_ms, "launches_per_step": per_run}
+        r.update(extra or {})
+        return r
+
+    # ntt_pass inside the LDE alone: 4 launches per LDE (inverse 2^20: 2 passes, forward
+    # 2^23: 2 passes); algorithmic bytes of the LDE = read the trace + write the LDE
+    ntt_extra = {}
+    if W == 64 and "ntt_pass" in MEASURED_NTT:
+        ntt_extra = dict(MEASURED_NTT["ntt_pass"])
+    roofline_ntt = roof("ntt_pass", prof_lde, args.steps, (W * N + W * N0) * 8, ntt_extra)
+    if roofline_ntt and W == 64 and "traffic_per_lde" in ntt_extra:
+        roofline_ntt["traffic"] = ntt_extra["traffic_per_lde"] / roofline_ntt["launches_per_step"]
+    # the dominant family of the timed step
+    roofline = None
+    if fused and "lde_leaf" in prof:
+        # reads the last pass's input once, writes one digest per row; 5 Keccak-f per
+        # 64-column row (4 + 64 lanes absorbed at 17 per block, then the pad block)
+        leaf_perms = N0 * ((4 + W) // 17 + 1)
+        n_l, ms = prof["lde_leaf"]
+        roofline = roof("lde_leaf", prof, args.steps, W * N0 * 8 + N0 * 32,
+                        {"keccak_f_per_s": leaf_perms * n_l / args.steps / (ms / 1e3)})
+        if W == 64 and "lde_leaf" in MEASURED_NTT:
+            roofline.update(MEASURED_NTT["lde_leaf"])
+    elif prof:
+        alg = algorithmic_bytes()
+        fam = "ntt_pass" if "ntt_pass" in prof else max(prof, key=lambda k: prof[k][1])
+        roofline = roof(fam, prof, args.steps, alg.get(fam, 0))
+        if roofline and fam in MEASURED_TRAFFIC_PER_STEP and W == 64:
+            roofline["traffic"] = MEASURED_TRAFFIC_PER_STEP[fam] / roofline["launches_per_step"]
     kernels = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps} for k, v in prof.items()}
 
     # The sections below characterise one GPU; with N > 1 ranks (the weak-scaling
@@ -703,6 +866,7 @@ def main():
         else None
     rsa = rsa2048(sg, ctx, args.rsa_jobs, args.rsa_stacked, cpu_threads) if single and args.rsa_jobs > 0 else None
     ecdsa = p256_ecdsa(sg, ctx, args.ecdsa_jobs, cpu_threads) if single and args.ecdsa_jobs > 0 else None
+    checks = record_checks(sg, ctx, args.record_checks, 16) if single and args.record_checks > 0 else None
     serve = None
     if single and args.serve_jobs > 0:
         serve = serving(sg, ctx, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs, 16)
@@ -710,19 +874,24 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, sample, _ = cpu_sample(trace, threads)
-        cpu = {"value": v, "unit": "proofs/s", "cores": threads, "kind": "port", "sample": sample}
+        cs = CpuSample(trace, threads)
+        t_cpu = min(cs.run() for _ in range(2))
+        cpu = {"value": cs.frac / t_cpu, "unit": "proofs/s", "cores": threads, "kind": "port",
+               "sample": cs.desc + f"; {t_cpu:.2f} s per sample", "proofs_per_sample": cs.frac}
 
     if rank == 0:
         ms_step = total_ms / args.steps
         line = {
             "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": ws, "steps": args.steps,
             "warmup": max(1, args.warmup), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64 (Goldilocks) / Fp6", "data": "synthetic (seeded uniform trace)",
-            "config": dict(CONFIG, parallelism=f"{ws} independent proofs (one per GPU), no collective"),
+            "vs_baseline": None, "dtype": DTYPE, "data": "synthetic (seeded uniform trace)",
+            "config": run_config(ws),
             "p50_ms": statistics.median(step_ms), "p99_ms": float(np.percentile(step_ms, 99)),
             "lde_ms": lde_ms, "lde_gbs": (W * N + W * N0) * 8 / 1e9 / (lde_ms / 1e3),
-            "e2e": {"value": e2e_value, "unit": "proofs/s", "h2d_bytes_per_step": W * N * 8,
+            "pipeline": args.pipeline,
+            "pipelines_ms_per_step": {args.pipeline: ms_step, ("split" if fused else "fused"): other_ms},
+            "roofline_ntt_pass": roofline_ntt,
+            "e2e": {"value": e2e_value, "unit": "proofs/s", "h2d_bytes_per_step": W * N * 8 + (N * 8 if fused else 0),
                     "d2h_bytes_per_step": 32 + len(ref[1])},
             "gpu_launches": launches_total,  # this library's kernels in the timed region
             "gpu_launches_per_step": launches,
@@ -734,6 +903,7 @@ def main():
             "sha256_large_trace": large,
             "rsa2048": rsa,
             "p256_ecdsa": ecdsa,
+            "record_checks": checks,
             "serving": serve,
             "classic_fri": classic,
             "proof_bytes": len(ref[1]),

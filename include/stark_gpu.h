@@ -34,6 +34,8 @@ extern "C" {
 #define SG_ESPACE -4    /* output buffer too small; *len holds the needed size */
 #define SG_EVERIFY -5   /* self-verification of a produced proof failed */
 #define SG_ELIMIT -6    /* request exceeds the fixed scratch of sg_ntt_noalloc */
+#define SG_ETIMEDOUT -7 /* sg_server_wait_for: the job did not finish within the time limit */
+#define SG_ECANCELED -8 /* the job was cancelled (sg_server_cancel) */
 
 #define SG_MAX_SCHEDULE 64
 
@@ -70,8 +72,9 @@ void sg_ctx_destroy(sg_ctx* ctx);
 int sg_ctx_set_stream(sg_ctx* ctx, void* cuda_stream);
 const char* sg_last_error(const sg_ctx* ctx);
 /* Context options.
- * SG_OPT_WIDE_MERGE selects how sg_prove_sha256 / sg_prove_sha512 evaluate their AIR over the LDE:
- *   SG_WIDE_MERGE_LDE     materialise the 756- (1510-) column LDE, then evaluate (fewest launches);
+ * SG_OPT_WIDE_MERGE selects how sg_prove_sha256 / sg_prove_sha512 / sg_prove_p256_ecdsa (and the
+ * server's jobs of those kinds) evaluate their AIR over the LDE:
+ *   SG_WIDE_MERGE_LDE     materialise the 756- (1510-, 151,334-) column LDE, then evaluate (fewest launches);
  *   SG_WIDE_MERGE_COSETS  never store the LDE: for each of the `blowup` cosets r, evaluate
  *                         all columns on r*<w_n0^blowup> (coefficients twisted by w_n0^{rk},
  *                         one n_trace-point NTT per column) and fold the constraints of that
@@ -243,6 +246,20 @@ int sg_merkle_commit(sg_ctx* ctx, const uint64_t* cols, size_t n_leaves, size_t 
  * Vec<Vec<[u8; HASH_BYTES]>>, index u64) for leaf `index` (merkle/src/lib.rs:478-512). */
 int sg_merkle_open(sg_ctx* ctx, const sg_tree* tree, size_t index, uint8_t* out, size_t cap, size_t* len);
 void sg_merkle_free(sg_tree* tree);
+
+/* lde_trace_columns (deep_ali/src/trace_import.rs:251-281, with sg_lde's coset
+ * shift) followed by the MerkleTreeChannel commitment to the rows of the LDE
+ * (merkle/src/lib.rs:391-476; leaf i = row i of the w LDE columns), in one call:
+ * the same root as sg_merkle_commit over sg_lde's output. With w a multiple of
+ * 16 and a domain of at least 2^9, the forward transform's
+ * last pass hashes the rows as it produces them and the LDE is never stored;
+ * otherwise it is materialised on the device first. `out` receives the LDE's
+ * first keep_cols columns (column stride n_trace * blowup; NULL when keep_cols is
+ * 0), e.g. the column a STIR proof takes next. root: sg_hash_bytes() bytes;
+ * `keep` (optional) receives the device-resident tree for sg_merkle_open. */
+int sg_lde_commit(sg_ctx* ctx, const uint64_t* trace, size_t w, size_t n_trace, size_t blowup, uint64_t shift,
+                  const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t* root, uint64_t* out,
+                  size_t keep_cols, sg_tree** keep);
 
 /* make_schedule + build_params (swarm-dns/src/prover.rs:53-98): schedule of 8s plus
  * a remainder for STIR (2s for FRI), r = s0 = 54, seed_z = 0xDEEF_BAAD,
@@ -426,7 +443,17 @@ typedef struct {
   const void* input;
   size_t input_len;
   uint8_t pi[32]; /* fs_binding / public_inputs_hash */
+  /* LDE blowup of the proof: 0 = the reference prover's own (32); otherwise a
+   * power of two in [2, 1024] (n0 = n_trace * blowup, STIR schedule
+   * make_schedule(n0)). HashRollup jobs always use 32. */
+  uint32_t blowup;
+  /* SG_JOB_FAULT_* bits: host-side fault injection for tests of the serving
+   * loop's failure handling (0 in production). No GPU work is made to fail:
+   * the fault is raised on the host where the named call would have failed. */
+  uint32_t flags;
 } sg_job;
+#define SG_JOB_FAULT_ALLOC 1u  /* the job's first attempt fails as if its device allocation had (SG_ENOMEM) */
+#define SG_JOB_FAULT_VERIFY 2u /* one byte of the proof is flipped before self-verification (SG_EVERIFY) */
 
 typedef struct {
   int32_t status; /* SG_OK or an SG_E* code */
@@ -446,6 +473,21 @@ int sg_server_poll(sg_server* srv, uint64_t ticket);                       /* 1 
 /* Blocks until the job is done; copies the proof (cap bytes available) and releases
  * the ticket, except on SG_ESPACE, which keeps it so the caller can retry. */
 int sg_server_wait(sg_server* srv, uint64_t ticket, sg_job_result* res, uint8_t* proof, size_t cap);
+/* sg_server_wait with a time limit, the per-shard deadline of the reference's
+ * controller (swarm-ctrl/src/main.rs:94-99): returns SG_ETIMEDOUT, keeping the
+ * ticket, if the job is not done within timeout_ms (0 = poll once). */
+int sg_server_wait_for(sg_server* srv, uint64_t ticket, int64_t timeout_ms, sg_job_result* res, uint8_t* proof,
+                       size_t cap);
+/* Cancels a job: a queued job is dropped before it starts (returns SG_OK); a
+ * running one finishes on the GPU but its result is discarded (returns 1).
+ * Either way its wait returns SG_ECANCELED. A job that had already finished
+ * keeps its result (returns 2). Unknown tickets: SG_EINVAL. */
+int sg_server_cancel(sg_server* srv, uint64_t ticket);
+/* Re-queue a job whose attempt failed with a transient error (SG_ENOMEM or
+ * SG_ECUDA) up to max_retries times, as the reference's controller reopens a
+ * failed shard (swarm-ctrl/src/main.rs:1085). Default 0. A proof that fails
+ * self-verification (SG_EVERIFY) is deterministic and is never retried. */
+int sg_server_set_retries(sg_server* srv, int max_retries);
 /* Proves n jobs with n_streams proofs in flight; proof i goes to proofs + i*cap_per_job. */
 int sg_prove_batch(sg_ctx* ctx, const sg_job* jobs, size_t n, int n_streams, uint64_t hbm_budget_bytes,
                    uint8_t* proofs, size_t cap_per_job, sg_job_result* results);

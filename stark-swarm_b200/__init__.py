@@ -53,6 +53,7 @@ LIB_PATH = os.path.join(_HERE, _LIB_NAME[HASH_PROFILE])
 P = 0xFFFFFFFF00000001
 
 SG_OK, SG_EINVAL, SG_ECUDA, SG_ENOMEM, SG_ESPACE, SG_EVERIFY, SG_ELIMIT = 0, -1, -2, -3, -4, -5, -6
+SG_ETIMEDOUT, SG_ECANCELED = -7, -8
 NOALLOC_MAX_ELEMS = 1 << 20  # sg_ntt_noalloc: n_cols * 2^log_n limit for log_n > 12
 PHI_PARALLEL_GATE, PHI_ALWAYS, PHI_NEVER = 0, 1, 2
 AIR_HASH_ROLLUP = 4
@@ -124,7 +125,7 @@ EXPORTS = (
     "sg_ctx_create", "sg_ctx_destroy", "sg_ctx_set_stream", "sg_ctx_set_option", "sg_last_error",
     "sg_kernel_launches",
     "sg_profile_enable", "sg_profile_read", "sg_profile_reset", "sg_ntt", "sg_ntt_noalloc",
-    "sg_lde", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_sha256_trace_gpu", "sg_prove_sha256",
+    "sg_lde", "sg_lde_commit", "sg_merge", "sg_merge_sha256", "sg_sha256_trace", "sg_sha256_trace_gpu", "sg_prove_sha256",
     "sg_merge_sha512", "sg_sha512_trace", "sg_sha512_trace_gpu", "sg_prove_sha512",
     "sg_dns_record_leaves", "sg_dns_merkle_root", "sg_dns_merkle_path", "sg_dns_merkle_verify", "sg_shard_pi_hash",
     "sg_prove_inner_shard", "sg_prove_outer_rollup",
@@ -135,16 +136,20 @@ EXPORTS = (
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
+    "sg_server_wait_for", "sg_server_cancel", "sg_server_set_retries",
     "sg_pool_reserve", "sg_hash_bytes", "sg_ntt_autotune", "sg_ntt_set_split",
 )
 JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA = 1, 2, 3, 4, 5
+# sg_job.flags: host-side fault injection for tests of the serving loop
+JOB_FAULT_ALLOC, JOB_FAULT_VERIFY = 1, 2
 OPT_WIDE_MERGE = 1
 WIDE_MERGE_AUTO, WIDE_MERGE_LDE, WIDE_MERGE_COSETS = 0, 1, 2
 
 
 class Job(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("phi_mode", ctypes.c_int32), ("input", ctypes.c_void_p),
-                ("input_len", ctypes.c_size_t), ("pi", ctypes.c_uint8 * 32)]
+                ("input_len", ctypes.c_size_t), ("pi", ctypes.c_uint8 * 32), ("blowup", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32)]
 
 
 class JobResult(ctypes.Structure):
@@ -207,6 +212,9 @@ def lib():
     L.sg_server_submit.argtypes = [vp, ctypes.POINTER(Job), ctypes.POINTER(u64)]
     L.sg_server_poll.argtypes = [vp, u64]
     L.sg_server_wait.argtypes = [vp, u64, ctypes.POINTER(JobResult), ctypes.c_char_p, sz]
+    L.sg_server_wait_for.argtypes = [vp, u64, ctypes.c_int64, ctypes.POINTER(JobResult), ctypes.c_char_p, sz]
+    L.sg_server_cancel.argtypes = [vp, u64]
+    L.sg_server_set_retries.argtypes = [vp, i32]
     L.sg_prove_batch.argtypes = [vp, ctypes.POINTER(Job), sz, i32, u64, ctypes.c_char_p, sz,
                                  ctypes.POINTER(JobResult)]
     L.sg_sha256_trace.argtypes = [ctypes.c_char_p, sz, vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz),
@@ -249,6 +257,7 @@ def lib():
     L.sg_sha512_trace_gpu.argtypes = L.sg_sha256_trace_gpu.argtypes
     L.sg_prove_sha512.argtypes = L.sg_prove_sha256.argtypes
     L.sg_merkle_commit.argtypes = [vp, vp, sz, sz, sz, vp, sz, u64, ctypes.c_char_p, ctypes.POINTER(vp)]
+    L.sg_lde_commit.argtypes = [vp, vp, sz, sz, sz, u64, vp, sz, u64, ctypes.c_char_p, vp, sz, ctypes.POINTER(vp)]
     L.sg_merkle_open.argtypes = [vp, vp, sz, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
     L.sg_merkle_free.argtypes = [vp]
     L.sg_merkle_free.restype = None
@@ -667,6 +676,29 @@ class Context:
         self._check(self._lib.sg_ntt(self._h, ip, op, cols, log_n, int(inverse)))
         return out
 
+    def lde_commit(self, trace, blowup: int, shift: int, arities, tree_label: int, keep_cols: int = 0, out=None,
+                   keep=False):
+        """lde_trace_columns then the Merkle commitment to the LDE's rows, in one call
+        (sg_lde_commit): returns the root, plus the first keep_cols LDE columns (a new
+        (keep_cols, n0) array unless `out` is given) and the tree handle if keep."""
+        ip, _ki, host = _addr(trace)
+        w, n = trace.shape
+        n0 = n * blowup
+        if keep_cols and out is None:
+            out = np.empty((keep_cols, n0), dtype=np.uint64)
+        op = _addr(out)[0] if keep_cols else None
+        ar = np.ascontiguousarray(arities, dtype=np.uint64)
+        root = ctypes.create_string_buffer(HASH_BYTES)
+        t = ctypes.c_void_p()
+        self._check(self._lib.sg_lde_commit(self._h, ip, w, n, blowup, shift, ar.ctypes.data, ar.size, tree_label, root,
+                                            op, keep_cols, ctypes.byref(t) if keep else None))
+        res = [root.raw]
+        if keep_cols:
+            res.append(out)
+        if keep:
+            res.append(MerkleTree(self, t))
+        return res[0] if len(res) == 1 else tuple(res)
+
     def lde(self, trace, blowup: int, shift: int = 1, out=None):
         """lde_trace_columns on a (w, n_trace) column-major buffer -> (w, n_trace*blowup)."""
         ip, _ki, host = _addr(trace)
@@ -912,7 +944,8 @@ class Context:
             return arr[:ln.value].tobytes()
 
     def prove_batch(self, jobs, n_streams: int = 8, hbm_budget_bytes: int = 0, cap_per_job: int = 1 << 20):
-        """jobs: list of (kind, data, pi[, phi_mode]) -> list of (proof bytes, JobResult)."""
+        """jobs: list of (kind, data, pi[, phi_mode[, blowup[, flags]]]) -> list of (proof bytes, JobResult).
+        blowup 0 (the default) is the reference prover's own, 32."""
         made = [make_job(*j) for j in jobs]
         arr = (Job * len(made))(*[m[0] for m in made])
         res = (JobResult * len(made))()
@@ -979,7 +1012,7 @@ class Context:
             return arr[:ln.value].tobytes()
 
 
-def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
+def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE, blowup: int = 0, flags: int = 0):
     """A sg_job plus the buffer it points to (keep both alive until submitted)."""
     if len(pi) != 32:
         raise ValueError("pi must be 32 bytes")
@@ -1001,7 +1034,7 @@ def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE):
     else:
         raise ValueError("unknown job kind")
     j = Job()
-    j.kind, j.phi_mode = kind, phi_mode
+    j.kind, j.phi_mode, j.blowup, j.flags = kind, phi_mode, blowup, flags
     j.input = ctypes.addressof(buf) if kind != JOB_HASH_ROLLUP else (buf.ctypes.data if n else None)
     j.input_len = n
     ctypes.memmove(j.pi, pi, 32)
@@ -1019,8 +1052,9 @@ class Server:
             raise StarkGpuError(rc, "sg_server_create failed")
         self._h = h
 
-    def submit(self, kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE) -> int:
-        j, _keep = make_job(kind, data, pi, phi_mode)
+    def submit(self, kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE, blowup: int = 0,
+               flags: int = 0) -> int:
+        j, _keep = make_job(kind, data, pi, phi_mode, blowup, flags)
         t = ctypes.c_uint64()
         rc = self._ctx._lib.sg_server_submit(self._h, ctypes.byref(j), ctypes.byref(t))
         if rc != SG_OK:
@@ -1030,19 +1064,36 @@ class Server:
     def poll(self, ticket: int) -> bool:
         return self._ctx._lib.sg_server_poll(self._h, ticket) == 1
 
-    def wait(self, ticket: int):
-        """-> (proof bytes, JobResult)"""
+    def wait(self, ticket: int, timeout_ms: int = None):
+        """-> (proof bytes, JobResult). With timeout_ms, raises StarkGpuError with code
+        SG_ETIMEDOUT (the ticket stays valid) when the job is not done in time."""
         cap = _PROOF_CAP
         while True:
             res = JobResult()
             arr, buf = _out_buffer(cap)
-            rc = self._ctx._lib.sg_server_wait(self._h, ticket, ctypes.byref(res), buf, cap)
+            if timeout_ms is None:
+                rc = self._ctx._lib.sg_server_wait(self._h, ticket, ctypes.byref(res), buf, cap)
+            else:
+                rc = self._ctx._lib.sg_server_wait_for(self._h, ticket, int(timeout_ms), ctypes.byref(res), buf, cap)
             if rc == SG_ESPACE:
                 cap = res.proof_len
                 continue
             if rc != SG_OK:
                 raise StarkGpuError(rc, f"job {ticket} failed")
             return arr[:res.proof_len].tobytes(), res
+
+    def cancel(self, ticket: int) -> int:
+        """0: dropped from the queue; 1: running, its result will be discarded; 2: already done."""
+        rc = self._ctx._lib.sg_server_cancel(self._h, ticket)
+        if rc < 0:
+            raise StarkGpuError(rc, f"sg_server_cancel({ticket}) failed")
+        return rc
+
+    def set_retries(self, max_retries: int):
+        """re-run a job whose attempt failed with SG_ENOMEM / SG_ECUDA up to max_retries times"""
+        rc = self._ctx._lib.sg_server_set_retries(self._h, max_retries)
+        if rc != SG_OK:
+            raise StarkGpuError(rc, "sg_server_set_retries failed")
 
     def close(self):
         if getattr(self, "_h", None):

@@ -824,6 +824,44 @@ int sg_merkle_commit(sg_ctx* c, const uint64_t* cols, size_t n_leaves, size_t wi
   });
 }
 
+int sg_lde_commit(sg_ctx* c, const uint64_t* trace, size_t w, size_t n_trace, size_t blowup, uint64_t shift,
+                  const uint64_t* arities, size_t depth, uint64_t tree_label, uint8_t* root, uint64_t* out,
+                  size_t keep_cols, sg_tree** keep) {
+  if (keep) *keep = nullptr;
+  return guarded(c, [&] {
+    sg::require(trace && root && arities && depth > 0, "lde_commit: null argument");
+    sg::require(w > 0 && n_trace > 0 && blowup > 0 && keep_cols <= w && (keep_cols == 0 || out),
+                "lde_commit: bad shape or kept columns");
+    std::vector<uint32_t> ar;
+    for (size_t i = 0; i < depth; ++i) {
+      sg::require(arities[i] >= 2 && arities[i] <= 1024, "lde_commit: arity out of range");
+      ar.push_back((uint32_t)arities[i]);
+    }
+    const size_t n0 = n_trace * blowup;
+    Out dout(out, keep_cols * n0, c->stream);
+    sg_tree* t = new sg_tree;
+    try {
+      sg::require(sg::tree_plan(&t->t, n0, ar, tree_label), "lde_commit: arities do not reach the root");
+      t->buf.alloc(t->t.total_digests * kc::kDigestLanes, c->stream);
+      t->t.d = t->buf.p;
+      sg::lde_commit(c, trace, !sg::is_device_ptr(trace), w, n_trace, blowup, shift, t->t, dout.d, keep_cols);
+      sg::cuda_check(sg::tree_hash_levels(t->t, c->stream), "levels");
+      sg::cuda_check(cudaMemcpyAsync(root, t->t.d + kc::kDigestLanes * t->t.off.back(), kc::kHashBytes,
+                                     cudaMemcpyDeviceToHost, c->stream),
+                     "d2h");
+      dout.finish();
+      sg::cuda_check(cudaStreamSynchronize(c->stream), "sync");
+    } catch (...) {
+      delete t;
+      throw;
+    }
+    if (keep)
+      *keep = t;
+    else
+      delete t;
+  });
+}
+
 int sg_merkle_open(sg_ctx* c, const sg_tree* tree, size_t index, uint8_t* out, size_t cap, size_t* len) {
   return guarded(c, [&] {
     sg::require(tree && len, "merkle_open: null tree or length");

@@ -163,6 +163,73 @@ void lde_from_host(sg_ctx* c, const uint64_t* h_trace, uint64_t w, uint64_t n_tr
   for (auto& e : ev) cudaEventDestroy(e);
 }
 
+// LDE of w columns (lde_trace_columns, trace_import.rs:251-281) and the Merkle
+// commitment to its rows (MerkleTreeChannel::push_leaves_parallel + finalize,
+// merkle/src/lib.rs:391-476) in one pipeline. When lde_leaf_ok, the forward
+// transform's last pass hashes the rows as it produces them, so the LDE is never
+// written (only its first keep_cols columns, into d_keep); otherwise the LDE is
+// materialised and hashed by the leaf kernel. A host trace is copied in column
+// chunks overlapped with their inverse transforms, as lde_from_host does.
+void lde_commit(sg_ctx* c, const uint64_t* trace, bool host_trace, uint64_t w, uint64_t n_trace, uint64_t blowup,
+                uint64_t shift, const DevTree& tree, uint64_t* d_keep, uint64_t keep_cols) {
+  lde_check(w, n_trace, blowup, shift);
+  require(keep_cols <= w && (keep_cols == 0 || d_keep), "lde_commit: bad kept columns");
+  require(tree.len[0] == n_trace * blowup, "lde_commit: the tree does not have one leaf per LDE row");
+  cudaStream_t s = c->stream;
+  const uint64_t n0 = n_trace * blowup;
+  const int ln = (int)log2_exact(n0), lt = (int)log2_exact(n_trace);
+  if (!lde_leaf_ok((uint32_t)w, ln)) {
+    DBuf lde(keep_cols == w ? 0 : w * n0, s);
+    uint64_t* dst = keep_cols == w ? d_keep : lde.p;
+    if (host_trace)
+      lde_from_host(c, trace, w, n_trace, blowup, shift, dst);
+    else
+      lde_device(c, trace, w, n_trace, blowup, shift, dst);
+    cuda_check(tree_hash_leaves(tree, dst, (uint32_t)w, n0, 0, s), "leaves");
+    if (keep_cols && dst != d_keep)
+      cuda_check(cudaMemcpyAsync(d_keep, dst, keep_cols * n0 * 8, cudaMemcpyDeviceToDevice, s), "copy");
+    return;
+  }
+  ShiftTables sh(c, shift, s);
+  DBuf coef(w * n_trace, s);
+  {
+    DBuf scratch(ntt_scratch_elems(w, lt), s);
+    if (!host_trace) {
+      ntt(c, trace, coef.p, (uint32_t)w, n_trace, n_trace, lt, true, n_trace, scratch.p);
+    } else {
+      // column chunks of ~64 MB: chunk k's copy overlaps chunk k-1's inverse transform
+      const uint64_t chunk = std::min<uint64_t>(w, std::max<uint64_t>(1, (uint64_t(8) << 20) / n_trace));
+      const uint64_t n_chunks = (w + chunk - 1) / chunk;
+      if (!c->copy_stream)
+        cuda_check(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "copy stream");
+      DBuf d_in(w * n_trace, s);
+      std::vector<cudaEvent_t> ev(n_chunks + 1, nullptr);
+      for (auto& e : ev) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      cuda_check(cudaEventRecord(ev[n_chunks], s), "event");
+      cuda_check(cudaStreamWaitEvent(c->copy_stream, ev[n_chunks], 0), "wait");
+      for (uint64_t k = 0; k < n_chunks; ++k) {
+        const uint64_t c0 = k * chunk, wk = std::min(chunk, w - c0);
+        cuda_check(cudaMemcpyAsync(d_in.p + c0 * n_trace, trace + c0 * n_trace, wk * n_trace * 8,
+                                   cudaMemcpyHostToDevice, c->copy_stream),
+                   "h2d");
+        cuda_check(cudaEventRecord(ev[k], c->copy_stream), "event");
+      }
+      for (uint64_t k = 0; k < n_chunks; ++k) {
+        const uint64_t c0 = k * chunk, wk = std::min(chunk, w - c0);
+        cuda_check(cudaStreamWaitEvent(s, ev[k], 0), "wait");
+        ntt(c, d_in.p + c0 * n_trace, coef.p + c0 * n_trace, (uint32_t)wk, n_trace, n_trace, lt, true, n_trace,
+            scratch.p);
+      }
+      cuda_check(cudaStreamSynchronize(s), "sync");  // the copies and transforms are done before d_in is freed
+      for (auto& e : ev) cudaEventDestroy(e);
+    }
+  }
+  DBuf scratch(lde_leaf_scratch_elems((uint32_t)w, ln), s);
+  cuda_check(lde_leaf_transform(c->tw, coef.p, n_trace, (uint32_t)w, ln, n_trace, sh.active ? &sh.spec : nullptr,
+                                scratch.p, tree.arity0, tree.label, tree.d, d_keep, (uint32_t)keep_cols, s),
+             "fused LDE and leaf hashing");
+}
+
 // ------------------------------------------------------------------ merge
 static bool phi_live(int mode, uint64_t n) {
   if (mode == SG_PHI_ALWAYS) return true;
@@ -792,13 +859,18 @@ void merge_hash_cosets(sg_ctx* c, const HashAir& air, const uint64_t* d_trace, u
 // sha512_air.rs:16-19): the host runs the compressions, the trace columns are
 // expanded on the device, then LDE x32 -> merge with lambda_j = j + 1
 // (prover.rs:100-102) -> STIR with build_params(n0, fs_binding).
+void check_blowup(uint64_t blowup) {
+  require(blowup >= 2 && blowup <= 1024 && pow2(blowup), "prove: blowup must be a power of 2 in [2, 1024]");
+}
+
 std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uint8_t* msg, uint64_t len,
                                         const uint8_t fs_binding[32], int phi_mode, bool self_verify,
-                                        uint8_t* digest) {
+                                        uint8_t* digest, uint64_t blowup) {
+  check_blowup(blowup);
   std::vector<uint8_t> wit;
   uint64_t n_blocks = 0;
   const uint64_t n_trace = air.witness(msg, len, &wit, &n_blocks, digest);
-  const uint64_t blowup = 32, n0 = n_trace * blowup;
+  const uint64_t n0 = n_trace * blowup;
   require(log2_exact(n0) <= kMaxLogN, "prove: message too long for a 2^28 domain");
   cudaStream_t s = c->stream;
   const uint64_t lde_bytes = (uint64_t)air.width * n0 * 8;
@@ -859,12 +931,13 @@ void rsa_witnesses(const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_b
 }
 
 std::vector<uint8_t> prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be,
-                                   uint64_t n_records, const uint8_t pi[32], bool self_verify) {
+                                   uint64_t n_records, const uint8_t pi[32], bool self_verify, uint64_t blowup) {
   require(n_records >= 1 && n_records <= 65535, "prove_rsa2048: 1 to 65535 records");
+  check_blowup(blowup);
   std::vector<rsa::RecordW> recs;
   std::vector<rsa::RowW> rows;
   rsa_witnesses(n_be, s_be, em_be, n_records, &recs, &rows);
-  const uint64_t n_trace = rsa::N_TRACE, blowup = rsa::BLOWUP, n0 = n_trace * blowup;
+  const uint64_t n_trace = rsa::N_TRACE, n0 = n_trace * blowup;
   const uint64_t W = n_records * rsa::WIDTH;
   const unsigned ln = log2_exact(n0);
   cudaStream_t s = c->stream;
@@ -898,8 +971,8 @@ std::vector<uint8_t> prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t
 }
 
 std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],
-                                          int phi_mode, bool self_verify, uint8_t digest[32]) {
-  return prove_hash_message(c, sha256_hash_air(), msg, len, fs_binding, phi_mode, self_verify, digest);
+                                          int phi_mode, bool self_verify, uint8_t digest[32], uint64_t blowup) {
+  return prove_hash_message(c, sha256_hash_air(), msg, len, fs_binding, phi_mode, self_verify, digest, blowup);
 }
 
 }  // namespace sg

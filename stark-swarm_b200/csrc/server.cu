@@ -26,6 +26,7 @@
 #include "rsa2048.hpp"
 #include "sha256_air.cuh"
 #include "sha512_air.cuh"
+#include "verifier.hpp"
 
 namespace {
 
@@ -34,6 +35,10 @@ using Clock = std::chrono::steady_clock;
 struct Entry {
   int32_t kind = 0;
   int32_t phi_mode = 0;
+  uint64_t blowup = 32;
+  uint32_t flags = 0;   // SG_JOB_FAULT_* (tests)
+  int attempts = 0;     // runs started
+  bool cancel = false;  // cancelled while running: the result is discarded
   std::vector<uint8_t> input;
   uint8_t pi[32];
   uint64_t footprint = 0;
@@ -51,33 +56,37 @@ uint64_t next_pow2(uint64_t x) {
   return p;
 }
 
+uint64_t job_blowup(const sg_job& j) { return j.blowup && j.kind != SG_JOB_HASH_ROLLUP ? j.blowup : 32; }
+
 // Device bytes a job holds at its peak (LDE + trace + quotient + STIR buffers), estimated.
 uint64_t footprint_bytes(const sg_job& j) {
+  const uint64_t bu = job_blowup(j);
   if (j.kind == SG_JOB_SHA256) {
     const uint64_t blocks = (j.input_len + 9 + 63) / 64;
-    const uint64_t nt = next_pow2(128 * blocks), n0 = nt * 32;
+    const uint64_t nt = next_pow2(128 * blocks), n0 = nt * bu;
     return 8 * ((uint64_t)sg::sha::WIDTH * (n0 + 2 * nt) + 16 * n0);
   }
   if (j.kind == SG_JOB_SHA512) {
     const uint64_t blocks = (j.input_len + 17 + 127) / 128;
-    const uint64_t nt = next_pow2(128 * blocks), n0 = nt * 32;
+    const uint64_t nt = next_pow2(128 * blocks), n0 = nt * bu;
     return 8 * ((uint64_t)sg::sha512::WIDTH * (n0 + 2 * nt) + 16 * n0);
   }
   if (j.kind == SG_JOB_P256_ECDSA) {
-    // trace, coefficients and LDE at 151,334 columns, n0 = 8192 (the LDE is
-    // evaluated coset by coset, without a scratch copy)
-    return 8ull * sg::p256::layout().width * (2 * sg::p256::K_ECDSA + 8192) + (64ull << 20);
+    // trace, coefficients and LDE at 151,334 columns (the LDE is evaluated
+    // coset by coset, without a scratch copy)
+    return 8ull * sg::p256::layout().width * (2 * sg::p256::K_ECDSA + sg::p256::K_ECDSA * bu) + (64ull << 20);
   }
   if (j.kind == SG_JOB_RSA2048) {
-    const uint64_t recs = j.input_len / 768, w = recs * sg::rsa::WIDTH;
-    return 8 * (w * (sg::rsa::N_TRACE + 1024) + (recs + 16) * 1024);
+    const uint64_t recs = j.input_len / 768, w = recs * sg::rsa::WIDTH, n0 = sg::rsa::N_TRACE * bu;
+    return 8 * (w * (sg::rsa::N_TRACE + n0) + (recs + 16) * n0);
   }
   const uint64_t nt = next_pow2(j.input_len < 8 ? 8 : j.input_len), n0 = nt * 32;
   return 8 * (4 * n0 + 8 * nt + 16 * n0);
 }
 
 // n || s || em per record (256 bytes each) -> the three contiguous arrays prove_rsa2048 takes
-std::vector<uint8_t> prove_rsa_job(sg_ctx* c, const std::vector<uint8_t>& in, const uint8_t pi[32]) {
+std::vector<uint8_t> prove_rsa_job(sg_ctx* c, const std::vector<uint8_t>& in, const uint8_t pi[32], uint64_t blowup,
+                                   bool self_verify) {
   const uint64_t recs = in.size() / 768;
   std::vector<uint8_t> n(256 * recs), s(256 * recs), em(256 * recs);
   for (uint64_t r = 0; r < recs; ++r) {
@@ -85,13 +94,14 @@ std::vector<uint8_t> prove_rsa_job(sg_ctx* c, const std::vector<uint8_t>& in, co
     memcpy(&s[256 * r], &in[768 * r + 256], 256);
     memcpy(&em[256 * r], &in[768 * r + 512], 256);
   }
-  return sg::prove_rsa2048(c, n.data(), s.data(), em.data(), recs, pi, true);
+  return sg::prove_rsa2048(c, n.data(), s.data(), em.data(), recs, pi, self_verify, blowup);
 }
 
 }  // namespace
 
 struct sg_server {
   sg_ctx* parent = nullptr;
+  int max_retries = 0;
   uint64_t budget = 0;
   uint64_t in_flight = 0;
   int running = 0;
@@ -123,15 +133,27 @@ struct sg_server {
         e = &entries.at(ticket);
         in_flight += e->footprint;
         ++running;
-        e->t_start = Clock::now();
+        ++e->attempts;
+        if (e->attempts == 1) e->t_start = Clock::now();
       }
       run(c, e);
       {
         std::lock_guard<std::mutex> lk(mu);
-        e->t_end = Clock::now();
-        e->done = true;
         in_flight -= e->footprint;
         --running;
+        const bool transient = e->status == SG_ENOMEM || e->status == SG_ECUDA;
+        if (e->cancel) {
+          e->status = SG_ECANCELED;
+          e->proof.clear();
+        } else if (transient && e->attempts <= max_retries) {
+          // reopened: back to the head of the queue for another attempt
+          queue.push_front(ticket);
+          e = nullptr;
+        }
+        if (e) {
+          e->t_end = Clock::now();
+          e->done = true;
+        }
       }
       cv_done.notify_all();
       cv_work.notify_all();
@@ -139,28 +161,53 @@ struct sg_server {
   }
 
   static void run(sg_ctx* c, Entry* e) {
+    e->proof.clear();
+    e->err.clear();
     try {
-      if (e->kind == SG_JOB_SHA256) {
-        e->proof = sg::prove_sha256_message(c, e->input.data(), e->input.size(), e->pi, e->phi_mode, true, e->digest);
-      } else if (e->kind == SG_JOB_SHA512) {
-        e->proof = sg::prove_hash_message(c, sg::sha512_hash_air(), e->input.data(), e->input.size(), e->pi,
-                                          e->phi_mode, true, e->digest);
-      } else if (e->kind == SG_JOB_P256_ECDSA) {
-        const uint8_t* in = e->input.data();
-        e->proof = sg::prove_p256_ecdsa(c, in, in + 32, in + 64, in + 96, in + 128, e->pi, true);
-      } else if (e->kind == SG_JOB_RSA2048) {
-        e->proof = prove_rsa_job(c, e->input, e->pi);
-      } else {
-        const uint64_t n = e->input.size() / 8;
-        e->proof = sg::prove_hash_rollup_host_leaves(c, (const uint64_t*)e->input.data(), n, e->pi, e->phi_mode, true);
+      if ((e->flags & SG_JOB_FAULT_ALLOC) && e->attempts == 1)
+        throw sg::SgError{SG_ENOMEM, "injected fault: device allocation failed"};
+      prove(c, e, !(e->flags & SG_JOB_FAULT_VERIFY));
+      if (e->flags & SG_JOB_FAULT_VERIFY) {
+        // a corrupted proof goes through the same self-verification as every proof
+        require_nonempty(e->proof);
+        e->proof[e->proof.size() / 2] ^= 0x40;
+        const sg::StirProof pr = sg::decode_proof(e->proof.data(), e->proof.size());
+        sg_fri_params p;
+        sg_build_params(pr.n0, e->pi, 1, &p);
+        if (!sg::stir_verify(pr, p)) throw sg::SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
       }
       e->status = SG_OK;
     } catch (const sg::SgError& x) {
       e->status = x.code;
       e->err = x.msg;
     } catch (const std::exception& x) {
-      e->status = SG_EINVAL;
+      e->status = SG_EVERIFY;
       e->err = x.what();
+    }
+  }
+
+  static void require_nonempty(const std::vector<uint8_t>& v) {
+    if (v.empty()) throw sg::SgError{SG_EINVAL, "empty proof"};
+  }
+
+  static void prove(sg_ctx* c, Entry* e, bool self_verify) {
+    {
+      if (e->kind == SG_JOB_SHA256) {
+        e->proof = sg::prove_sha256_message(c, e->input.data(), e->input.size(), e->pi, e->phi_mode, self_verify,
+                                            e->digest, e->blowup);
+      } else if (e->kind == SG_JOB_SHA512) {
+        e->proof = sg::prove_hash_message(c, sg::sha512_hash_air(), e->input.data(), e->input.size(), e->pi,
+                                          e->phi_mode, self_verify, e->digest, e->blowup);
+      } else if (e->kind == SG_JOB_P256_ECDSA) {
+        const uint8_t* in = e->input.data();
+        e->proof = sg::prove_p256_ecdsa(c, in, in + 32, in + 64, in + 96, in + 128, e->pi, self_verify, e->blowup);
+      } else if (e->kind == SG_JOB_RSA2048) {
+        e->proof = prove_rsa_job(c, e->input, e->pi, e->blowup, self_verify);
+      } else {
+        const uint64_t n = e->input.size() / 8;
+        e->proof = sg::prove_hash_rollup_host_leaves(c, (const uint64_t*)e->input.data(), n, e->pi, e->phi_mode,
+                                                     self_verify);
+      }
     }
   }
 };
@@ -234,9 +281,12 @@ int sg_server_submit(sg_server* s, const sg_job* job, uint64_t* ticket) {
   if (job->kind == SG_JOB_P256_ECDSA && job->input_len != 160) return SG_EINVAL;
   if (job->input_len && !job->input) return SG_EINVAL;
   if (job->kind == SG_JOB_RSA2048 && (job->input_len == 0 || job->input_len % 768)) return SG_EINVAL;
+  if (job->blowup && (job->blowup < 2 || job->blowup > 1024 || (job->blowup & (job->blowup - 1)))) return SG_EINVAL;
   Entry e;
   e.kind = job->kind;
   e.phi_mode = job->phi_mode;
+  e.blowup = job_blowup(*job);
+  e.flags = job->flags;
   const size_t bytes = job->kind == SG_JOB_HASH_ROLLUP ? job->input_len * 8 : job->input_len;
   e.input.assign((const uint8_t*)job->input, (const uint8_t*)job->input + bytes);
   memcpy(e.pi, job->pi, 32);
@@ -260,12 +310,12 @@ int sg_server_poll(sg_server* s, uint64_t ticket) {
   return it->second.done ? 1 : 0;
 }
 
-int sg_server_wait(sg_server* s, uint64_t ticket, sg_job_result* res, uint8_t* proof, size_t cap) {
-  if (!s || !res) return SG_EINVAL;
-  std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->entries.find(ticket);
-  if (it == s->entries.end()) return SG_EINVAL;
-  s->cv_done.wait(lk, [&] { return it->second.done; });
+namespace {
+
+// The result of a finished job (entries locked by the caller); erases the entry
+// unless the proof does not fit.
+int take_result(sg_server* s, std::map<uint64_t, Entry>::iterator it, sg_job_result* res, uint8_t* proof,
+                size_t cap) {
   Entry& e = it->second;
   auto ms = [](Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
@@ -284,6 +334,61 @@ int sg_server_wait(sg_server* s, uint64_t ticket, sg_job_result* res, uint8_t* p
   }
   s->entries.erase(it);
   return rc;
+}
+
+}  // namespace
+
+int sg_server_wait(sg_server* s, uint64_t ticket, sg_job_result* res, uint8_t* proof, size_t cap) {
+  if (!s || !res) return SG_EINVAL;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->entries.find(ticket);
+  if (it == s->entries.end()) return SG_EINVAL;
+  s->cv_done.wait(lk, [&] { return it->second.done; });
+  return take_result(s, it, res, proof, cap);
+}
+
+int sg_server_wait_for(sg_server* s, uint64_t ticket, int64_t timeout_ms, sg_job_result* res, uint8_t* proof,
+                       size_t cap) {
+  if (!s || !res || timeout_ms < 0) return SG_EINVAL;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->entries.find(ticket);
+  if (it == s->entries.end()) return SG_EINVAL;
+  if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return it->second.done; })) {
+    memset(res, 0, sizeof *res);
+    res->status = SG_ETIMEDOUT;
+    return SG_ETIMEDOUT;
+  }
+  return take_result(s, it, res, proof, cap);
+}
+
+int sg_server_cancel(sg_server* s, uint64_t ticket) {
+  if (!s) return SG_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->entries.find(ticket);
+  if (it == s->entries.end()) return SG_EINVAL;
+  Entry& e = it->second;
+  if (e.done) return 2;  // finished before the call: its result stands
+  for (auto q = s->queue.begin(); q != s->queue.end(); ++q) {
+    if (*q != ticket) continue;
+    // queued (never started, or waiting for a retry): dropped here
+    s->queue.erase(q);
+    e.status = SG_ECANCELED;
+    e.proof.clear();
+    if (e.attempts == 0) e.t_start = Clock::now();
+    e.t_end = Clock::now();
+    e.done = true;
+    s->cv_done.notify_all();
+    return SG_OK;
+  }
+  e.cancel = true;  // running: the worker discards its result
+  return 1;
+}
+
+int sg_server_set_retries(sg_server* s, int max_retries) {
+  if (!s || max_retries < 0 || max_retries > 100) return SG_EINVAL;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->max_retries = max_retries;
+  return SG_OK;
 }
 
 int sg_prove_batch(sg_ctx* ctx, const sg_job* jobs, size_t n, int n_streams, uint64_t hbm_budget_bytes,

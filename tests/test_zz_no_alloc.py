@@ -68,3 +68,29 @@ def test_noalloc_ntt_rejects_oversize_and_host_buffers(sgpu):
     # 2^29 is beyond the largest supported domain (2^28)
     assert L.sg_ntt_noalloc(ptr, ptr, 1, 25, 0, None) == sgpu.SG_ELIMIT
     assert L.sg_ntt_noalloc(ptr, ptr, 1, 29, 0, None) == sgpu.SG_EINVAL
+
+
+@pytest.mark.parametrize("cols,log_n", [(3, 14), (1, 9)])
+def test_noalloc_python_wrapper_matches_context_and_oracle(sgpu, ctx, cols, log_n):
+    # the package's wrapper on a (cols, 2^log_n) tensor: it derives n_cols from the
+    # tensor, and its result equals the context's sg_ntt and the oracle's transform
+    torch = pytest.importorskip("torch")
+    import oracle_lib as O
+    rng = np.random.default_rng(50 + log_n)
+    host = rng.integers(0, P, size=(cols, 1 << log_n), dtype=np.uint64)
+    x = torch.from_numpy(host.view(np.int64)).cuda()
+    want = torch.empty_like(x)
+    ctx.ntt(x, log_n, False, out=want)
+    for call in range(2):
+        out = torch.full_like(x, -1)
+        assert sgpu.ntt_noalloc(x, out, log_n) == sgpu.SG_OK
+        torch.cuda.synchronize()
+        assert torch.equal(out, want), f"call {call}"
+    got = out.cpu().numpy().view(np.uint64)
+    for c in range(cols):
+        assert np.array_equal(got[c], O.ntt(host[c])), c
+    # raw device pointers with an explicit column count
+    out2 = torch.full_like(x, -1)
+    assert sgpu.ntt_noalloc(x.data_ptr(), out2.data_ptr(), log_n, n_cols=cols) == sgpu.SG_OK
+    torch.cuda.synchronize()
+    assert torch.equal(out2, want)
