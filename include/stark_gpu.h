@@ -83,6 +83,13 @@ const char* sg_last_error(const sg_ctx* ctx);
  *   SG_WIDE_MERGE_AUTO    (default) cosets once the LDE would exceed 2 GiB.
  * Both give bit-identical results. */
 #define SG_OPT_WIDE_MERGE 1
+/* SG_OPT_STIR_GROUP (1 .. 64, default 1): servers (and sg_prove_batch) created
+ * from this context let a worker take up to this many queued jobs whose proofs
+ * have the same domain n0 (any kinds except HashRollup) and prove their STIR
+ * phase in lockstep (sg_stir_prove_group: one launch per stage for the group, one
+ * host round trip per fold layer). Each job's trace, LDE and constraint merge
+ * still run on their own; every proof's bytes are unchanged. */
+#define SG_OPT_STIR_GROUP 2
 #define SG_WIDE_MERGE_AUTO 0
 #define SG_WIDE_MERGE_LDE 1
 #define SG_WIDE_MERGE_COSETS 2
@@ -273,6 +280,15 @@ void sg_build_params(size_t n0, const uint8_t* pi32, int stir, sg_fri_params* ou
  * (Compress::Yes) bytes of the DeepFriProof. f0: n0 values. */
 int sg_stir_prove(sg_ctx* ctx, const uint64_t* f0, size_t n0, const sg_fri_params* params, uint8_t* proof,
                   size_t cap, size_t* len);
+
+/* n_proofs STIR proofs of one shape in lockstep (the reference proves one per
+ * call; its swarm runs many shards side by side): the same n0 and parameters
+ * except public_inputs_hash, f0 of proof g at f0 + g * n0. Every device stage is
+ * one launch over all the proofs and each fold layer has one host round trip for
+ * all of their transcripts. Proof g (the bytes of sg_stir_prove on its f0 and
+ * params[g]) goes to proofs + g * cap_per_proof, its length to lens[g]. */
+int sg_stir_prove_group(sg_ctx* ctx, const uint64_t* f0, size_t n0, size_t n_proofs, const sg_fri_params* params,
+                        uint8_t* proofs, size_t cap_per_proof, size_t* lens);
 
 /* Replaces deep_fri_verify::<SexticExt> (deep_ali/src/fri.rs:2136-2707), both
  * branches, on serialized proof bytes. Returns 1 accept, 0 reject. Host only. */

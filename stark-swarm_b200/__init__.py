@@ -134,7 +134,7 @@ EXPORTS = (
     "sg_p256_layout", "sg_p256_u_bits", "sg_p256_ecdsa_pi", "sg_p256_chain_trace", "sg_p256_chain_trace_gpu",
     "sg_merge_p256_ecdsa", "sg_prove_p256_chains", "sg_prove_p256_ecdsa",
     "sg_merkle_commit",
-    "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_verify", "sg_prove_hash_rollup",
+    "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_prove_group", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
     "sg_server_wait_for", "sg_server_cancel", "sg_server_set_retries",
     "sg_pool_reserve", "sg_hash_bytes", "sg_ntt_autotune", "sg_ntt_set_split",
@@ -143,6 +143,7 @@ JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA = 1, 2, 3, 
 # sg_job.flags: host-side fault injection for tests of the serving loop
 JOB_FAULT_ALLOC, JOB_FAULT_VERIFY = 1, 2
 OPT_WIDE_MERGE = 1
+OPT_STIR_GROUP = 2  # servers from this context prove up to this many same-n0 STIR phases in lockstep
 WIDE_MERGE_AUTO, WIDE_MERGE_LDE, WIDE_MERGE_COSETS = 0, 1, 2
 
 
@@ -264,6 +265,8 @@ def lib():
     L.sg_build_params.argtypes = [sz, ctypes.c_char_p, i32, ctypes.POINTER(FriParams)]
     L.sg_build_params.restype = None
     L.sg_stir_prove.argtypes = [vp, vp, sz, ctypes.POINTER(FriParams), ctypes.c_char_p, sz, ctypes.POINTER(sz)]
+    L.sg_stir_prove_group.argtypes = [vp, vp, sz, sz, ctypes.POINTER(FriParams), ctypes.c_char_p, sz,
+                                      ctypes.POINTER(sz)]
     L.sg_stir_verify.argtypes = [ctypes.c_char_p, sz, ctypes.POINTER(FriParams)]
     L.sg_prove_hash_rollup.argtypes = [vp, vp, sz, ctypes.c_char_p, i32, ctypes.c_char_p, sz, ctypes.POINTER(sz)]
     _lib = L
@@ -978,6 +981,26 @@ class Context:
         return (root.raw, MerkleTree(self, t)) if keep else root.raw
 
     # ---------------------------------------------------------------- STIR
+    def deep_fri_prove_group(self, f0s, params_list, cap_per_proof: int = 1 << 21):
+        """n STIR proofs of one shape in lockstep (sg_stir_prove_group): f0s is an (n, n0)
+        buffer, params_list n FriParams that differ only in their public-input hash.
+        Returns the n proofs' bytes, each equal to deep_fri_prove's."""
+        ip, _ki, host = _addr(f0s)
+        n, n0 = f0s.shape
+        if len(params_list) != n:
+            raise ValueError("one FriParams per proof")
+        ps = (FriParams * n)(*params_list)
+        while True:
+            buf = np.empty(cap_per_proof * n, dtype=np.uint8)
+            lens = (ctypes.c_size_t * n)()
+            rc = self._lib.sg_stir_prove_group(self._h, ip, n0, n, ps, ctypes.cast(buf.ctypes.data, ctypes.c_char_p),
+                                               cap_per_proof, lens)
+            if rc == SG_ESPACE:
+                cap_per_proof = max(lens)
+                continue
+            self._check(rc)
+            return [buf[g * cap_per_proof: g * cap_per_proof + lens[g]].tobytes() for g in range(n)]
+
     def deep_fri_prove(self, f0, domain0, params: FriParams) -> bytes:
         """deep_fri_prove (STIR or classic DEEP-FRI, per params.stir); returns the
         ark-serialize (Compress::Yes) bytes of the DeepFriProof."""

@@ -231,6 +231,11 @@ int sg_ctx_set_option(sg_ctx* c, int option, int64_t value) {
     c->wide_merge = (int)value;
     return SG_OK;
   }
+  if (option == SG_OPT_STIR_GROUP) {
+    if (value < 1 || value > 64) return SG_EINVAL;
+    c->stir_group = (int)value;
+    return SG_OK;
+  }
   return SG_EINVAL;
 }
 
@@ -931,6 +936,25 @@ int sg_stir_prove(sg_ctx* c, const uint64_t* f0, size_t n0, const sg_fri_params*
     *len = b.size();
     if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "stir_prove: proof buffer too small"};
     memcpy(proof, b.data(), b.size());
+  });
+}
+
+int sg_stir_prove_group(sg_ctx* c, const uint64_t* f0, size_t n0, size_t n_proofs, const sg_fri_params* params,
+                        uint8_t* proofs, size_t cap_per_proof, size_t* lens) {
+  return guarded(c, [&] {
+    sg::require(f0 && params && lens && proofs && n_proofs > 0 && n_proofs <= 4096,
+                "stir_prove_group: null argument or bad count");
+    sg::require(n0 > 0 && n0 <= (size_t(1) << sg::kMaxLogN), "stir_prove_group: bad n0");
+    In di(f0, n0 * n_proofs, c->stream);
+    std::vector<sg_fri_params> ps(params, params + n_proofs);
+    const auto out = sg::stir_prove_group(c, di.d, n0, n0, ps);
+    bool fits = true;
+    for (size_t g = 0; g < n_proofs; ++g) {
+      lens[g] = out[g].size();
+      if (out[g].size() > cap_per_proof) fits = false;
+    }
+    if (!fits) throw sg::SgError{SG_ESPACE, "stir_prove_group: proof buffer too small"};
+    for (size_t g = 0; g < n_proofs; ++g) memcpy(proofs + g * cap_per_proof, out[g].data(), out[g].size());
   });
 }
 

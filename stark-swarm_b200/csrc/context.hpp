@@ -23,6 +23,7 @@ struct sg_ctx {
   sg::NttTables tw;
   bool owns_tables = true;  // worker contexts of a server borrow the parent's tables
   int wide_merge = SG_WIDE_MERGE_AUTO;  // SG_OPT_WIDE_MERGE
+  int stir_group = 1;                   // SG_OPT_STIR_GROUP (servers created from this context)
   // Server workers only (null elsewhere): a highest-priority stream for the STIR
   // phase of a proof and the two events that order it after and before `stream`.
   cudaStream_t stir_stream = nullptr;

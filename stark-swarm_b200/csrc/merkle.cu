@@ -51,10 +51,14 @@ __device__ __forceinline__ void put_digest(uint64_t* o, const uint64_t* d) {
 }
 
 // Generic width: runtime loop (positions resolved by the sponge's switch).
+// Trees of one shape side by side (grid.y = tree g): tree g's rows start g_cols
+// elements and its digests g_out elements further on.
 __global__ void leaf_kernel(const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros, uint64_t n,
-                            uint64_t arity0, uint64_t label, uint64_t* out) {
+                            uint64_t arity0, uint64_t label, uint64_t* out, uint64_t g_cols, uint64_t g_out) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  cols += blockIdx.y * g_cols;
+  out += blockIdx.y * g_out;
   uint64_t d[DL];
   leaf_digest_row(cols, w, cs, zeros, i, arity0, label, d);
   put_digest(out + DL * i, d);
@@ -63,9 +67,11 @@ __global__ void leaf_kernel(const uint64_t* cols, uint32_t w, uint64_t cs, uint3
 // Fixed width: fully unrolled, every lane position is a compile-time constant.
 template <int W, int Z>
 __global__ void leaf_kernel_t(const uint64_t* __restrict__ cols, uint64_t cs, uint64_t n, uint64_t arity0,
-                              uint64_t label, uint64_t* __restrict__ out) {
+                              uint64_t label, uint64_t* __restrict__ out, uint64_t g_cols, uint64_t g_out) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  cols += blockIdx.y * g_cols;
+  out += blockIdx.y * g_out;
   kc::LaneSponge sp;
   sp.init();
   sp.lane(arity0);
@@ -105,9 +111,9 @@ __device__ __forceinline__ void node_hash(const uint64_t* child, uint64_t n_chil
 
 template <int A>
 __global__ void node_kernel_t(const uint64_t* __restrict__ child, uint64_t n_child, uint64_t* __restrict__ parent,
-                              uint64_t n_parent, uint64_t level, uint64_t label) {
+                              uint64_t n_parent, uint64_t level, uint64_t label, uint64_t g_tree) {
   uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (p < n_parent) node_hash<A>(child, n_child, parent, p, level, label);
+  if (p < n_parent) node_hash<A>(child + blockIdx.y * g_tree, n_child, parent + blockIdx.y * g_tree, p, level, label);
 }
 
 __device__ void node_hash_any(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t p, uint32_t arity,
@@ -131,9 +137,10 @@ __device__ void node_hash_any(const uint64_t* child, uint64_t n_child, uint64_t*
 }
 
 __global__ void node_kernel(const uint64_t* child, uint64_t n_child, uint64_t* parent, uint64_t n_parent,
-                            uint32_t arity, uint64_t level, uint64_t label) {
+                            uint32_t arity, uint64_t level, uint64_t label, uint64_t g_tree) {
   uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (p < n_parent) node_hash_any(child, n_child, parent, p, arity, level, label);
+  if (p < n_parent)
+    node_hash_any(child + blockIdx.y * g_tree, n_child, parent + blockIdx.y * g_tree, p, arity, level, label);
 }
 
 // The levels from the first one of at most kTopWork Keccak-f (parents x
@@ -154,7 +161,10 @@ struct TopLevels {
   uint64_t level[kMaxTopLevels];
 };
 
-__global__ void __launch_bounds__(kTopThreads) tree_top_kernel(uint64_t* d, TopLevels tl, uint64_t label) {
+// one CTA per tree of a group (tree g's digests at d + g g_tree)
+__global__ void __launch_bounds__(kTopThreads) tree_top_kernel(uint64_t* d, TopLevels tl, uint64_t label,
+                                                               uint64_t g_tree) {
+  d += blockIdx.x * g_tree;
   for (int k = 0; k < tl.n; ++k) {
     const uint64_t* ch = d + DL * tl.child_off[k];
     uint64_t* par = d + DL * tl.parent_off[k];
@@ -188,13 +198,20 @@ inline unsigned blocks_for(uint64_t n, unsigned t) { return (unsigned)((n + t - 
 
 cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros,
                              cudaStream_t s) {
+  return tree_hash_leaves_group(t, cols, w, cs, zeros, 0, 0, 1, s);
+}
+
+cudaError_t tree_hash_leaves_group(const DevTree& t, const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros,
+                                   uint64_t g_cols, uint64_t g_tree, uint32_t n_trees, cudaStream_t s) {
+  if (n_trees == 0 || n_trees > 65535) return cudaErrorInvalidValue;
   const uint64_t n = t.len[0];
-  const unsigned T = 128, B = blocks_for(n, T);
-#define SG_LEAF_CASE(WW, ZZ)                                                           \
-  if (w == WW && zeros == ZZ) {                                                        \
-    SG_LAUNCH_SCOPE("merkle_leaves", s);                                               \
-    leaf_kernel_t<WW, ZZ><<<B, T, 0, s>>>(cols, cs, n, t.arity0, t.label, t.d);        \
-    return cudaGetLastError();                                                         \
+  const unsigned T = 128;
+  const dim3 B(blocks_for(n, T), n_trees);
+#define SG_LEAF_CASE(WW, ZZ)                                                                   \
+  if (w == WW && zeros == ZZ) {                                                                \
+    SG_LAUNCH_SCOPE("merkle_leaves", s);                                                       \
+    leaf_kernel_t<WW, ZZ><<<B, T, 0, s>>>(cols, cs, n, t.arity0, t.label, t.d, g_cols, g_tree); \
+    return cudaGetLastError();                                                                 \
   }
   SG_LEAF_CASE(1, 5)
   SG_LEAF_CASE(2, 0)
@@ -205,11 +222,14 @@ cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w,
   SG_LEAF_CASE(64, 0)
 #undef SG_LEAF_CASE
   SG_LAUNCH_SCOPE("merkle_leaves", s);
-  leaf_kernel<<<B, T, 0, s>>>(cols, w, cs, zeros, n, t.arity0, t.label, t.d);
+  leaf_kernel<<<B, T, 0, s>>>(cols, w, cs, zeros, n, t.arity0, t.label, t.d, g_cols, g_tree);
   return cudaGetLastError();
 }
 
-cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
+cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) { return tree_hash_levels_group(t, 0, 1, s); }
+
+cudaError_t tree_hash_levels_group(const DevTree& t, uint64_t g_tree, uint32_t n_trees, cudaStream_t s) {
+  if (n_trees == 0 || n_trees > 65535) return cudaErrorInvalidValue;
   for (size_t l = 0; l + 1 < t.len.size(); ++l) {
     const uint64_t np = t.len[l + 1];
     if (np * node_perms(t.arity[l]) <= kTopWork && t.len.size() - 1 - l <= (size_t)kMaxTopLevels) {
@@ -223,19 +243,19 @@ cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s) {
         tl.level[tl.n] = k + 1;
       }
       SG_LAUNCH_SCOPE("merkle_nodes", s);
-      tree_top_kernel<<<1, kTopThreads, 0, s>>>(t.d, tl, t.label);
+      tree_top_kernel<<<n_trees, kTopThreads, 0, s>>>(t.d, tl, t.label, g_tree);
       return cudaGetLastError();
     }
     const uint64_t* ch = t.d + DL * t.off[l];
     uint64_t* par = t.d + DL * t.off[l + 1];
-    const unsigned B = blocks_for(np, 128);
+    const dim3 B(blocks_for(np, 128), n_trees);
     SG_LAUNCH_SCOPE("merkle_nodes", s);
     switch (t.arity[l]) {
-      case 2: node_kernel_t<2><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
-      case 4: node_kernel_t<4><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
-      case 8: node_kernel_t<8><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
-      case 16: node_kernel_t<16><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label); break;
-      default: node_kernel<<<B, 128, 0, s>>>(ch, t.len[l], par, np, t.arity[l], l + 1, t.label); break;
+      case 2: node_kernel_t<2><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label, g_tree); break;
+      case 4: node_kernel_t<4><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label, g_tree); break;
+      case 8: node_kernel_t<8><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label, g_tree); break;
+      case 16: node_kernel_t<16><<<B, 128, 0, s>>>(ch, t.len[l], par, np, l + 1, t.label, g_tree); break;
+      default: node_kernel<<<B, 128, 0, s>>>(ch, t.len[l], par, np, t.arity[l], l + 1, t.label, g_tree); break;
     }
   }
   return cudaGetLastError();

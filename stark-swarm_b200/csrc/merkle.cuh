@@ -40,6 +40,11 @@ cudaError_t tree_hash_leaves(const DevTree& t, const uint64_t* cols, uint32_t w,
                              cudaStream_t s);
 // Hash levels 1..depth from level 0.
 cudaError_t tree_hash_levels(const DevTree& t, cudaStream_t s);
+// The same for n_trees trees of t's shape side by side: tree g's digests at
+// t.d + g * g_tree (u64) and, for the leaves, its rows at cols + g * g_cols.
+cudaError_t tree_hash_leaves_group(const DevTree& t, const uint64_t* cols, uint32_t w, uint64_t cs, uint32_t zeros,
+                                   uint64_t g_cols, uint64_t g_tree, uint32_t n_trees, cudaStream_t s);
+cudaError_t tree_hash_levels_group(const DevTree& t, uint64_t g_tree, uint32_t n_trees, cudaStream_t s);
 // Copy digests at the given global digest indices into out (kc::kDigestLanes lanes each).
 cudaError_t gather_digests(const uint64_t* d, const uint64_t* idx, uint64_t n, uint64_t* out, cudaStream_t s);
 // Gather u64 values src[idx[i]] into out.

@@ -850,8 +850,10 @@ cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t 
     last_in = scratch;
     BC = N2;
   } else {
-    // three passes N = A * B * C with C = 2^12 and B = 2^(r - 12), as ntt_batch's
-    const int lc = 12, lb = r - 12;
+    // three passes N = A * B * C, as ntt_batch's, with C and B as even as possible
+    // (2^8 x 2^8 for a 2^23 domain): every pass then fills its CTAs' lanes, where
+    // C = 2^12 would leave a 2^(r - 12)-point middle pass with mostly idle lanes
+    const int lc = (r + 1) / 2, lb = r - lc;
     const uint64_t B = 1ull << lb, C = 1ull << lc, AB = A * B;
     uint64_t* s1 = scratch;
     uint64_t* s2 = scratch + (uint64_t)w * N;

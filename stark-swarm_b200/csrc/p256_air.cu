@@ -253,20 +253,32 @@ __global__ void __launch_bounds__(kPhiThreads, 4) p256_phi_kernel(P256Phi a, uin
     }
   }
   if (g1 == a.n_gadgets && ch + 1 == gridDim.y) {
-    const uint64_t row = i / a.row_div;
-    eval_tail(x, a.lde + (i + a.step) % a.n, a.tail, row + 1 == a.n_trace, row + 1 < a.n_trace,
-              (uint64_t)a.lam_tail + 1);
+    uint64_t row, nx;
+    if (a.coset_len == 0) {
+      row = i / a.blowup;
+      nx = (i + a.blowup) % a.n;
+    } else {
+      const uint64_t c = i / a.coset_len, p = i - c * a.coset_len;
+      row = p;
+      nx = c * a.coset_len + (p + 1 == a.coset_len ? 0 : p + 1);
+    }
+    eval_tail(x, a.lde + nx, a.tail, row + 1 == a.n_trace, row + 1 < a.n_trace, (uint64_t)a.lam_tail + 1);
   }
   part[(uint64_t)ch * a.n + i] = x.acc.reduce();
 }
 
-__global__ void p256_sum_kernel(const uint64_t* part, uint64_t n, uint32_t chunks, uint64_t* phi, uint64_t out_stride,
-                                uint64_t out_off) {
+__global__ void p256_sum_kernel(const uint64_t* part, uint64_t n, uint32_t chunks, uint64_t* phi, uint64_t coset_len,
+                                uint64_t out_stride, uint64_t out_off) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint64_t s = 0;
   for (uint32_t c = 0; c < chunks; ++c) s = gl::add(s, part[(uint64_t)c * n + i]);
-  phi[i * out_stride + out_off] = s;
+  if (coset_len == 0) {
+    phi[i] = s;
+  } else {
+    const uint64_t c = i / coset_len;
+    phi[out_off + c + out_stride * (i - c * coset_len)] = s;
+  }
 }
 
 }  // namespace
@@ -295,7 +307,7 @@ cudaError_t p256_expand(const P256Dev& d, uint64_t k, uint64_t* d_trace, cudaStr
 }
 
 cudaError_t p256_phi(const P256Phi& a, uint32_t n_chunks, uint64_t* d_part, uint64_t* d_phi, cudaStream_t s) {
-  if (a.row_div == 0 || a.n % a.row_div || a.step == 0 || a.out_stride == 0 || n_chunks == 0 || n_chunks > 65535)
+  if (a.blowup == 0 || a.n % (a.coset_len ? a.coset_len : a.blowup) || n_chunks == 0 || n_chunks > 65535)
     return cudaErrorInvalidValue;
   {
     SG_LAUNCH_SCOPE("p256_phi", s);
@@ -303,8 +315,8 @@ cudaError_t p256_phi(const P256Phi& a, uint32_t n_chunks, uint64_t* d_part, uint
         a, d_part);
   }
   SG_LAUNCH_SCOPE("p256_phi_sum", s);
-  p256_sum_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(d_part, a.n, n_chunks, d_phi, a.out_stride,
-                                                                 a.out_off);
+  p256_sum_kernel<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(d_part, a.n, n_chunks, d_phi, a.coset_len,
+                                                                 a.out_stride, a.out_off);
   return cudaGetLastError();
 }
 

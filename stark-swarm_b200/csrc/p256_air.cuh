@@ -26,12 +26,13 @@ cudaError_t p256_expand(const P256Dev& d, uint64_t k, uint64_t* d_trace, cudaStr
 struct P256Phi {
   const uint64_t* lde;  // width columns of n points
   uint64_t n, blowup, n_trace;
-  // Point i of the buffer is trace row i / row_div; the next row's point is
-  // (i + step) mod n. A materialised LDE has row_div = step = blowup; one coset
-  // of it (point a = LDE point r + blowup a) has row_div = step = 1.
-  uint64_t row_div, step;
-  // Phi of point i goes to d_phi[i * out_stride + out_off] (1, 0 for an LDE; blowup, r for coset r)
-  uint64_t out_stride, out_off;
+  // coset_len = 0: `lde` is the materialised LDE; point i is trace row i / blowup,
+  // its next row is point (i + blowup) mod n, and Phi goes to d_phi[i].
+  // coset_len = L > 0: `lde` holds n / L whole cosets of the LDE one after
+  // another (coset out_off + c at c L .. c L + L - 1, point a = LDE point
+  // out_off + c + out_stride a): point i = c L + a is trace row a, its next row is
+  // point c L + (a + 1) mod L, and Phi goes to d_phi[out_off + c + out_stride a].
+  uint64_t coset_len, out_stride, out_off;
   const p256::Gadget* table;
   const uint32_t* lam_base;  // first constraint index of each gadget
   const uint32_t* chunk;     // n_chunks + 1 gadget boundaries

@@ -94,8 +94,8 @@ void p256_merge_device(sg_ctx* c, const uint64_t* d_lde, uint64_t n_trace, uint6
   require((1ull << ln) == n && ln <= kMaxLogN && n_trace >= 2, "p256 merge: bad sizes");
   cudaStream_t s = c->stream;
   DBuf part((uint64_t)T.n_chunks * n, s), phi(n, s), scratch(ntt_scratch_elems(1, ln), s);
-  P256Phi a{d_lde, n, blowup, n_trace, blowup, blowup, 1, 0, T.table, T.lam, T.chunk, T.tail,
-            (uint32_t)L.table.size(), L.n_constraints - p256::TAIL_CONSTRAINTS};
+  P256Phi a{d_lde, n, blowup, n_trace, 0, 1, 0, T.table, T.lam, T.chunk, T.tail, (uint32_t)L.table.size(),
+            L.n_constraints - p256::TAIL_CONSTRAINTS};
   cuda_check(p256_phi(a, T.n_chunks, part.p, phi.p, s), "p256 phi");
   cuda_check(ntt_batch(c->tw, phi.p, phi.p, 1, n, n, (int)ln, true, n, scratch.p, s), "intt");
   cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
@@ -107,33 +107,39 @@ void p256_merge_device(sg_ctx* c, const uint64_t* d_lde, uint64_t n_trace, uint6
 // never holds the whole LDE): LDE point r + blowup a lies on coset r, whose
 // values are NTT_{n_trace}(c_k w_n^{r k}) of the trace coefficients c, and the
 // next row of that point is point a + 1 of the same coset. Each coset is
-// produced (coset 0 is the trace itself), its Phi values are written to
-// Phi[r + blowup a], and it is dropped: the device holds the trace, its
-// coefficients and one coset (3 x 310 MB for K = 256) instead of the 9.9 GB LDE.
+// produced, its Phi values are written to Phi[r + blowup a], and it is dropped.
+// Cosets go kCosetGroup at a time (their evaluations one after another), so each
+// Phi launch covers kCosetGroup x n_trace points: one coset alone (256 points for
+// K = 256) gives the constraint kernel too few CTAs to fill the GPU. The device
+// holds the trace, its coefficients and one group (2 x 310 MB + 2.5 GB for K = 256)
+// instead of the 9.9 GB LDE.
 void p256_merge_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, uint64_t blowup, uint64_t* d_c) {
+  constexpr uint64_t kCosetGroup = 8;
   const p256::Layout& L = p256::layout();
   const P256Tables& T = p256_tables();
-  const uint64_t n = n_trace * blowup, W = L.width;
+  const uint64_t n = n_trace * blowup, W = L.width, G = std::min<uint64_t>(kCosetGroup, blowup);
   const unsigned ln = lg2(n), lt = lg2(n_trace);
   require((1ull << ln) == n && (1ull << lt) == n_trace && ln <= kMaxLogN && n_trace >= 2, "p256 merge: bad sizes");
   cudaStream_t s = c->stream;
-  DBuf part((uint64_t)T.n_chunks * n_trace, s), phi(n, s), coef(W * n_trace, s), ev(W * n_trace, s);
+  DBuf part((uint64_t)T.n_chunks * G * n_trace, s), phi(n, s), coef(W * n_trace, s), ev(W * G * n_trace, s);
   DBuf scratch(std::max(ntt_scratch_elems((uint32_t)W, (int)lt), ntt_scratch_elems(1, (int)ln)), s);
   DBuf twist_tab(n_trace, s);
   cuda_check(ntt_batch(c->tw, d_trace, coef.p, (uint32_t)W, n_trace, n_trace, (int)lt, true, n_trace, scratch.p, s),
              "p256 trace intt");
-  for (uint64_t r = 0; r < blowup; ++r) {
-    const uint64_t* evals = d_trace;
-    if (r > 0) {
-      cuda_check(pow_table_device(c->tw, r, (int)ln, n_trace, twist_tab.p, s), "twist table");
+  for (uint64_t r0 = 0; r0 < blowup; r0 += G) {
+    // column col of coset r0 + g at ev[col * G n_trace + g n_trace]
+    for (uint64_t g = 0; g < G; ++g) {
+      const uint64_t r = r0 + g;
       PowSpec twist;
-      twist.tab = twist_tab.p;
-      cuda_check(ntt_batch(c->tw, coef.p, ev.p, (uint32_t)W, n_trace, n_trace, (int)lt, false, n_trace, scratch.p, s,
-                           &twist),
+      if (r > 0) {
+        cuda_check(pow_table_device(c->tw, r, (int)ln, n_trace, twist_tab.p, s), "twist table");
+        twist.tab = twist_tab.p;
+      }
+      cuda_check(ntt_batch(c->tw, coef.p, ev.p + g * n_trace, (uint32_t)W, n_trace, G * n_trace, (int)lt, false,
+                           n_trace, scratch.p, s, r > 0 ? &twist : nullptr),
                  "p256 coset ntt");
-      evals = ev.p;
     }
-    P256Phi a{evals, n_trace, blowup, n_trace, 1, 1, blowup, r, T.table, T.lam, T.chunk, T.tail,
+    P256Phi a{ev.p, G * n_trace, blowup, n_trace, n_trace, blowup, r0, T.table, T.lam, T.chunk, T.tail,
               (uint32_t)L.table.size(), L.n_constraints - p256::TAIL_CONSTRAINTS};
     cuda_check(p256_phi(a, T.n_chunks, part.p, phi.p, s), "p256 coset phi");
   }
@@ -142,9 +148,9 @@ void p256_merge_cosets(sg_ctx* c, const uint64_t* d_trace, uint64_t n_trace, uin
   cuda_check(ntt_batch(c->tw, d_c, d_c, 1, n, n, (int)ln, false, n - n_trace, scratch.p, s), "ntt");
 }
 
-std::vector<uint8_t> prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
-                                       const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, uint64_t k,
-                                       const uint8_t pi[32], bool self_verify, uint64_t blowup) {
+CEval p256_chains_ceval(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
+                        const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, uint64_t k,
+                        const uint8_t pi[32], uint64_t blowup) {
   const p256::Layout& L = p256::layout();
   require(blowup >= 2 && blowup <= 1024 && !(blowup & (blowup - 1)), "prove: blowup must be a power of 2 in [2, 1024]");
   const uint64_t n0 = k * blowup, W = L.width;
@@ -164,12 +170,24 @@ std::vector<uint8_t> prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const ui
       p256_merge_device(c, d_lde.p, k, blowup, d_c.p);
     }
   }
-  sg_fri_params p;
-  sg_build_params(n0, pi, 1, &p);
-  std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
-  if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
-    throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
-  return proof;
+  CEval r;
+  r.d_c = std::move(d_c);
+  r.n0 = n0;
+  sg_build_params(n0, pi, 1, &r.params);
+  return r;
+}
+
+std::vector<uint8_t> prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
+                                       const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, uint64_t k,
+                                       const uint8_t pi[32], bool self_verify, uint64_t blowup) {
+  return prove_from_ceval(c, p256_chains_ceval(c, ax, ay, a_bits, bx, by, b_bits, k, pi, blowup), self_verify);
+}
+
+CEval p256_ecdsa_ceval(sg_ctx* c, const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32],
+                       const uint8_t sgn[32], const uint8_t digest[32], const uint8_t pi[32], uint64_t blowup) {
+  uint8_t u1[256], u2[256];
+  p256::u_bits(digest, r, sgn, u1, u2);
+  return p256_chains_ceval(c, p256::GX, p256::GY, u1, qx, qy, u2, p256::K_ECDSA, pi, blowup);
 }
 
 std::vector<uint8_t> prove_p256_ecdsa(sg_ctx* c, const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32],

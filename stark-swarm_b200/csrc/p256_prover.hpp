@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "context.hpp"
+#include "prover.hpp"
 
 namespace sg {
 
@@ -18,6 +19,12 @@ void p256_merge_device(sg_ctx* c, const uint64_t* d_lde, uint64_t n_trace, uint6
 std::vector<uint8_t> prove_p256_chains(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
                                        const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, uint64_t k,
                                        const uint8_t pi[32], bool self_verify, uint64_t blowup = 32);
+// c_eval of the same proofs (everything before the STIR phase).
+CEval p256_chains_ceval(sg_ctx* c, const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits,
+                        const uint8_t bx[32], const uint8_t by[32], const uint8_t* b_bits, uint64_t k,
+                        const uint8_t pi[32], uint64_t blowup = 32);
+CEval p256_ecdsa_ceval(sg_ctx* c, const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32],
+                       const uint8_t s[32], const uint8_t digest[32], const uint8_t pi[32], uint64_t blowup = 32);
 // prove_ecdsa_record_v1.rs:97-240: chain A = u1 bits from G, chain B = u2 bits from Q, K = 256.
 std::vector<uint8_t> prove_p256_ecdsa(sg_ctx* c, const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32],
                                       const uint8_t s[32], const uint8_t digest[32], const uint8_t pi[32],

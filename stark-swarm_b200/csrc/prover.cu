@@ -730,6 +730,307 @@ std::vector<uint8_t> stir_prove_on_stream(sg_ctx* c, const uint64_t* d_f0, uint6
   return encode_proof(pr);
 }
 
+// Trees of one shape, one per proof of a group, side by side in one buffer.
+struct GroupTree {
+  DevTree t;
+  DBuf buf;
+  uint64_t stride = 0;  // u64 between two trees' digests
+  void make(uint64_t n, const std::vector<uint32_t>& ar, uint64_t label, uint32_t G, cudaStream_t s) {
+    require(tree_plan(&t, n, ar, label), "merkle: arity schedule does not reach the root");
+    stride = t.total_digests * DL;
+    buf.alloc(stride * G, s);
+    t.d = buf.p;
+  }
+  // the G roots (DL lanes each, one after another) into h
+  void roots(std::vector<uint64_t>* h, uint32_t G, cudaStream_t s) const {
+    h->resize((size_t)G * DL);
+    cuda_check(cudaMemcpy2DAsync(h->data(), DL * 8, t.d + DL * t.off.back(), stride * 8, DL * 8, G,
+                                 cudaMemcpyDeviceToHost, s),
+               "d2h roots");
+  }
+};
+
+// G STIR proofs of one shape in lockstep (fri.rs:1398-1718, 1813-1893, 1900-2055,
+// as stir_prove_on_stream): the same n0 and parameters except the public-input
+// hash, proof g's f0 at d_f0 + g * g_f0. Every device stage is one launch over
+// all G proofs (trees side by side, transforms over 6G columns, grid.y = proof
+// for the OOD and fold kernels), and each layer's one host synchronisation serves
+// all G transcripts. The bytes of proof g are those of stir_prove_on_stream.
+std::vector<std::vector<uint8_t>> stir_prove_group_on_stream(sg_ctx* c, const uint64_t* d_f0, uint64_t g_f0,
+                                                             uint64_t n0, const std::vector<sg_fri_params>& ps) {
+  cudaStream_t s = c->stream;
+  const uint32_t G = (uint32_t)ps.size();
+  require(G >= 1 && G <= 4096, "stir_prove_group: 1 to 4096 proofs");
+  const sg_fri_params& p = ps[0];
+  for (const auto& q : ps)
+    require(q.schedule_len == p.schedule_len && q.s0 == p.s0 && q.r == p.r && q.seed_z == p.seed_z &&
+                q.d_final == p.d_final && q.coeff_commit_final == p.coeff_commit_final && q.stir == p.stir &&
+                !memcmp(q.schedule, p.schedule, sizeof p.schedule[0] * p.schedule_len),
+            "stir_prove_group: the proofs differ in more than their public-input hash");
+  const uint64_t L = p.schedule_len;
+  require(p.stir, "stir_prove_group: STIR parameters only");
+  require(L >= 1 && L <= SG_MAX_SCHEDULE, "stir_prove: empty or oversized schedule");
+  require(pow2(n0) && n0 >= 2 && log2_exact(n0) <= kMaxLogN, "stir_prove: n0 must be a power of 2 in [2, 2^28]");
+  require(p.s0 <= (1u << 20), "stir_prove: too many queries");
+  require(g_f0 >= n0, "stir_prove_group: f0 stride below n0");
+  std::vector<uint64_t> sizes{n0};
+  for (uint64_t i = 0; i < L; ++i) {
+    const uint64_t m = p.schedule[i];
+    require(m == 2 || m == 4 || m == 8 || m == 16, "stir_prove: fold arities must be 2, 4, 8 or 16");
+    require(sizes.back() % m == 0, "stir_prove: schedule does not divide the domain");
+    sizes.push_back(sizes.back() / m);
+  }
+  const bool use_cc = p.coeff_commit_final != 0;
+  std::vector<StirProof> pr(G);
+  std::vector<HostTranscript> tr;
+  tr.reserve(G);
+  for (uint32_t g = 0; g < G; ++g) {
+    pr[g].n0 = n0;
+    pr[g].omega0 = gl::root_of_unity(log2_exact(n0));
+    tr.emplace_back("FRI/FS");
+    bind_statement(tr[g], ps[g], n0);
+  }
+
+  const uint64_t m0 = p.schedule[0], nn0 = n0 / m0;
+  GroupTree f0t;
+  f0t.make(nn0, layer_arities(nn0, 16), 0xFF, G, s);
+  cuda_check(tree_hash_leaves_group(f0t.t, d_f0, (uint32_t)m0, nn0, 0, g_f0, f0t.stride, G, s), "f0 leaves");
+  cuda_check(tree_hash_levels_group(f0t.t, f0t.stride, G, s), "f0 levels");
+  std::vector<uint64_t> h;
+  f0t.roots(&h, G, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+  std::vector<gl::Fp6> zc(G);
+  for (uint32_t g = 0; g < G; ++g) {
+    pr[g].root_f0 = digest_at(h, (size_t)g * DL);
+    tr[g].absorb_bytes(pr[g].root_f0.data(), HB);
+    zc[g] = tr[g].challenge_ext("z_fp3");
+  }
+
+  const uint64_t work = std::max<uint64_t>(n0, 6 * sizes[1]);
+  uint64_t scratch_len = ntt_scratch_elems(G, log2_exact(n0));
+  for (uint64_t i = 1; i <= L; ++i)
+    scratch_len = std::max(scratch_len, ntt_scratch_elems(6ull * G, log2_exact(sizes[i])));
+  DBuf coef(work * G, s), scratch(scratch_len, s);
+  uint64_t part_len = 0;
+  for (uint64_t i = 0; i < L; ++i) part_len = std::max<uint64_t>(part_len, ood_partials_len(sizes[i], (int)p.schedule[i]));
+  DBuf partials(part_len * G, s), evals(16 * 6 * (uint64_t)G, s);
+  // per-proof OOD scalars and fold challenges, uploaded before each layer's launches
+  const size_t sc_words = sizeof(OodScalars) / 8, al_words = sizeof(gl::Fp6) / 8;
+  DBuf d_sc(sc_words * G, s), d_al(al_words * G, s);
+  std::vector<OodScalars> h_sc(G);
+  std::vector<gl::Fp6> h_al(G);
+  std::vector<DBuf> planes(L + 1);
+  std::vector<GroupTree> trees(L);
+  DBuf tuples;
+  GroupTree ctree;
+
+  const uint64_t* cur = d_f0;
+  uint64_t g_cur = g_f0;
+  bool base = true;
+  for (uint64_t ell = 0; ell < L; ++ell) {
+    const uint64_t m = p.schedule[ell], n = sizes[ell], nn = n / m;
+    const unsigned lg = log2_exact(n);
+    const bool last_cc = use_cc && ell == L - 1;
+    for (uint32_t g = 0; g < G; ++g) h_al[g] = last_cc ? gl::e_zero() : tr[g].challenge_ext("alpha");
+    if (ell == 0) {
+      trees[0].make(n, layer_arities(n, m), 0, G, s);
+      cuda_check(tree_hash_leaves_group(trees[0].t, d_f0, 1, n, 5, g_f0, trees[0].stride, G, s), "layer-0 leaves");
+    }
+    cuda_check(tree_hash_levels_group(trees[ell].t, trees[ell].stride, G, s), "layer levels");
+
+    const uint32_t cols = base ? 1 : 6;
+    // proof g's component c at cur + g g_cur + c n; coefficients at coef + (g cols + c) n
+    if (base)
+      ntt(c, cur, coef.p, G, g_cur, n, lg, true, n, scratch.p);
+    else
+      ntt(c, cur, coef.p, 6 * G, n, n, lg, true, n, scratch.p);
+    for (uint32_t g = 0; g < G; ++g) h_sc[g] = ood_scalars(zc[g], n, (int)m);
+    cuda_check(cudaMemcpyAsync(d_sc.p, h_sc.data(), G * sizeof(OodScalars), cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(cudaMemcpyAsync(d_al.p, h_al.data(), G * sizeof(gl::Fp6), cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(ood_evaluate_group(coef.p, (uint64_t)cols * n, base, n, (int)m, (const OodScalars*)d_sc.p, partials.p,
+                                  evals.p, 16 * 6, G, s),
+               "ood");
+
+    FoldArgs fa{};
+    fa.f = cur;
+    fa.base = base;
+    fa.n = n;
+    fa.log_n = (int)lg;
+    fa.m = (int)m;
+    fa.alpha = gl::e_zero();
+    fa.tw_inv_lo = c->tw.d_inv_lo;
+    fa.tw_inv_hi = c->tw.d_inv_hi;
+    fa.n_proofs = G;
+    fa.g_f = g_cur;
+    fa.alphas = (const gl::Fp6*)d_al.p;
+    if (!last_cc) {
+      planes[ell + 1].alloc(6 * nn * G, s);
+      fa.next = planes[ell + 1].p;
+      fa.g_next = 6 * nn;
+      if (ell + 1 < L) {
+        trees[ell + 1].make(nn, layer_arities(nn, p.schedule[ell + 1]), ell + 1, G, s);
+        fa.leaves = trees[ell + 1].t.d;
+        fa.g_leaves = trees[ell + 1].stride;
+        fa.leaf_label = ell + 1;
+        fa.leaf_arity0 = trees[ell + 1].t.arity0;
+      }
+      cuda_check(stir_fold(fa, s), "fold");
+    } else {
+      tuples.alloc(6 * m * nn * G, s);
+      fa.tuples = tuples.p;
+      fa.g_tuples = 6 * m * nn;
+      cuda_check(stir_fold(fa, s), "coefficient tuples");
+      ctree.make(nn, layer_arities(nn, 16), 0xFE, G, s);
+      cuda_check(tree_hash_leaves_group(ctree.t, tuples.p, (uint32_t)(6 * m), nn, 0, 6 * m * nn, ctree.stride, G, s),
+                 "coeff leaves");
+      cuda_check(tree_hash_levels_group(ctree.t, ctree.stride, G, s), "coeff levels");
+    }
+
+    std::vector<uint64_t> ev, root, croot, tup;
+    d2h(&ev, evals.p, 16 * 6 * (uint64_t)G, s);
+    trees[ell].roots(&root, G, s);
+    if (last_cc) {
+      ctree.roots(&croot, G, s);
+      d2h(&tup, tuples.p, 6 * m * nn * G, s);
+    }
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    for (uint32_t g = 0; g < G; ++g) {
+      std::vector<gl::Fp6> evs(m);
+      for (uint64_t j = 0; j < m; ++j)
+        for (int q = 0; q < 6; ++q) evs[j].c[q] = ev[(uint64_t)g * 96 + j * 6 + q];
+      pr[g].fz.push_back(evs[0]);
+      for (auto& e : evs) tr[g].absorb_ext(e);
+      pr[g].coset_evals.push_back(std::move(evs));
+      pr[g].roots.push_back(digest_at(root, (size_t)g * DL));
+      tr[g].absorb_bytes(pr[g].roots.back().data(), HB);
+      zc[g] = gl::e_pow(zc[g], m);
+      if (last_cc) {
+        pr[g].has_ct = pr[g].has_croot = true;
+        pr[g].coeff_root = digest_at(croot, (size_t)g * DL);
+        tr[g].absorb_bytes(pr[g].coeff_root.data(), HB);
+        h_al[g] = tr[g].challenge_ext("alpha");
+        (void)tr[g].challenge_ext("beta_deg");
+        const uint64_t* tg = tup.data() + (uint64_t)g * 6 * m * nn;
+        pr[g].coeff_tuples.assign(nn, std::vector<gl::Fp6>(m));
+        for (uint64_t b = 0; b < nn; ++b)
+          for (uint64_t k = 0; k < m; ++k)
+            for (int q = 0; q < 6; ++q) pr[g].coeff_tuples[b][k].c[q] = tg[(k * 6 + q) * nn + b];
+      }
+    }
+    if (last_cc) {
+      planes[ell + 1].alloc(6 * nn * G, s);
+      cuda_check(cudaMemcpyAsync(d_al.p, h_al.data(), G * sizeof(gl::Fp6), cudaMemcpyHostToDevice, s), "h2d");
+      cuda_check(fold_tuples_group(tuples.p, 6 * m * nn, nn, (int)m, (const gl::Fp6*)d_al.p, planes[ell + 1].p,
+                                   6 * nn, G, s),
+                 "final fold");
+    }
+    cur = planes[ell + 1].p;
+    g_cur = 6 * nn;
+    base = false;
+  }
+
+  // final polynomial coefficients (fri.rs:1915-1935), proof g's at coef + 6 g nf
+  const uint64_t nf = sizes[L];
+  const unsigned lgf = log2_exact(nf);
+  if (nf > 1) {
+    ntt(c, cur, coef.p, 6 * G, nf, nf, lgf, true, nf, scratch.p);
+  } else {
+    cuda_check(cudaMemcpyAsync(coef.p, cur, 6 * 8 * (uint64_t)G, cudaMemcpyDeviceToDevice, s), "copy");
+  }
+  std::vector<uint64_t> fc;
+  d2h(&fc, coef.p, 6 * nf * G, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+  const uint64_t d_final = std::min<uint64_t>(p.d_final, nf);
+  std::vector<uint64_t> query_seed(G);
+  for (uint32_t g = 0; g < G; ++g) {
+    for (uint64_t k = 0; k < d_final; ++k) {
+      gl::Fp6 e;
+      for (int q = 0; q < 6; ++q) e.c[q] = fc[(uint64_t)g * 6 * nf + q * nf + k];
+      pr[g].final_coeffs.push_back(e);
+      tr[g].absorb_ext(e);
+    }
+    query_seed[g] = tr[g].challenge_field("query_seed");
+  }
+
+  // proximity queries of every proof: one gather per kind of value
+  std::vector<uint64_t> val_idx, dig_idx0, dig_idx1, next_idx;
+  std::vector<std::vector<ProxQuery>> qs(G, std::vector<ProxQuery>(p.s0));
+  const uint64_t td0 = f0t.t.total_digests, td1 = L >= 2 ? trees[1].t.total_digests : 0;
+  for (uint32_t g = 0; g < G; ++g) {
+    for (uint64_t q = 0; q < p.s0; ++q) {
+      ProxQuery& x = qs[g][q];
+      x.raw = query_index(query_seed[g], q, n0);
+      x.base = x.raw % nn0;
+      for (uint64_t j = 0; j < m0; ++j) {
+        x.fib_idx.push_back(x.base + j * nn0);
+        val_idx.push_back((uint64_t)g * g_f0 + x.base + j * nn0);
+      }
+      const size_t a0 = dig_idx0.size();
+      opening_indices(f0t.t, x.base, &dig_idx0);
+      for (size_t i = a0; i < dig_idx0.size(); ++i) dig_idx0[i] += (uint64_t)g * td0;
+      if (L >= 2) {
+        const size_t a1 = dig_idx1.size();
+        opening_indices(trees[1].t, x.base, &dig_idx1);
+        for (size_t i = a1; i < dig_idx1.size(); ++i) dig_idx1[i] += (uint64_t)g * td1;
+        for (int k = 0; k < 6; ++k) next_idx.push_back((uint64_t)g * 6 * sizes[1] + (uint64_t)k * sizes[1] + x.base);
+      }
+    }
+  }
+  const size_t nv = val_idx.size(), nd0 = dig_idx0.size(), nd1 = dig_idx1.size(), nx = next_idx.size();
+  std::vector<uint64_t> idx_all;
+  idx_all.insert(idx_all.end(), val_idx.begin(), val_idx.end());
+  idx_all.insert(idx_all.end(), dig_idx0.begin(), dig_idx0.end());
+  idx_all.insert(idx_all.end(), dig_idx1.begin(), dig_idx1.end());
+  idx_all.insert(idx_all.end(), next_idx.begin(), next_idx.end());
+  DBuf d_idx(idx_all.size(), s), d_out(nv + DL * (nd0 + nd1) + nx, s);
+  if (!idx_all.empty()) {
+    cuda_check(cudaMemcpyAsync(d_idx.p, idx_all.data(), idx_all.size() * 8, cudaMemcpyHostToDevice, s), "h2d");
+    cuda_check(gather_u64(d_f0, d_idx.p, nv, d_out.p, s), "gather values");
+    cuda_check(gather_digests(f0t.t.d, d_idx.p + nv, nd0, d_out.p + nv, s), "gather f0 paths");
+    if (L >= 2) {
+      cuda_check(gather_digests(trees[1].t.d, d_idx.p + nv + nd0, nd1, d_out.p + nv + DL * nd0, s), "gather l1");
+      cuda_check(gather_u64(planes[1].p, d_idx.p + nv + nd0 + nd1, nx, d_out.p + nv + DL * (nd0 + nd1), s),
+                 "gather f1");
+    }
+  }
+  std::vector<uint64_t> got;
+  d2h(&got, d_out.p, d_out.n, s);
+  cuda_check(cudaStreamSynchronize(s), "sync");
+
+  size_t pv = 0, p0 = nv, p1 = nv + DL * nd0, pn = nv + DL * (nd0 + nd1);
+  auto take_opening = [&](const DevTree& t, uint64_t index, size_t* pos) {
+    Opening o;
+    o.index = index;
+    o.leaf = digest_at(got, *pos);
+    *pos += DL;
+    for (size_t l = 0; l + 1 < t.len.size(); ++l) {
+      std::vector<Digest> sib(t.arity[l] - 1);
+      for (auto& d : sib) {
+        d = digest_at(got, *pos);
+        *pos += DL;
+      }
+      o.path.push_back(std::move(sib));
+    }
+    return o;
+  };
+  std::vector<std::vector<uint8_t>> out(G);
+  for (uint32_t g = 0; g < G; ++g) {
+    for (uint64_t q = 0; q < p.s0; ++q) {
+      ProxQuery& x = qs[g][q];
+      for (uint64_t j = 0; j < m0; ++j) x.fib_vals.push_back(got[pv++]);
+      x.f0_open = take_opening(f0t.t, x.base, &p0);
+      x.has_l1 = L >= 2;
+      if (L >= 2) {
+        x.l1_open = take_opening(trees[1].t, x.base, &p1);
+        for (int k = 0; k < 6; ++k) x.f_next.c[k] = got[pn++];
+      }
+    }
+    pr[g].prox = std::move(qs[g]);
+    out[g] = encode_proof(pr[g]);
+  }
+  return out;
+}
+
 // For the STIR phase, a context with a stir_stream (a server worker) moves to it:
 // the stream waits for everything queued so far, and `stream` waits for the STIR
 // work before the caller queues more (its buffers are freed in stream order).
@@ -753,6 +1054,13 @@ std::vector<uint8_t> stir_prove_device(sg_ctx* c, const uint64_t* d_f0, uint64_t
   if (!c->stir_stream) return stir_prove_on_stream(c, d_f0, n0, p);
   StirStreamScope scope(c);
   return stir_prove_on_stream(c, d_f0, n0, p);
+}
+
+std::vector<std::vector<uint8_t>> stir_prove_group(sg_ctx* c, const uint64_t* d_f0, uint64_t g_f0, uint64_t n0,
+                                                   const std::vector<sg_fri_params>& ps) {
+  if (!c->stir_stream) return stir_prove_group_on_stream(c, d_f0, g_f0, n0, ps);
+  StirStreamScope scope(c);
+  return stir_prove_group_on_stream(c, d_f0, g_f0, n0, ps);
 }
 
 // ------------------------------------------------------------------ HashRollup pipeline
@@ -863,9 +1171,8 @@ void check_blowup(uint64_t blowup) {
   require(blowup >= 2 && blowup <= 1024 && pow2(blowup), "prove: blowup must be a power of 2 in [2, 1024]");
 }
 
-std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uint8_t* msg, uint64_t len,
-                                        const uint8_t fs_binding[32], int phi_mode, bool self_verify,
-                                        uint8_t* digest, uint64_t blowup) {
+CEval hash_message_ceval(sg_ctx* c, const HashAir& air, const uint8_t* msg, uint64_t len,
+                         const uint8_t fs_binding[32], int phi_mode, uint8_t* digest, uint64_t blowup) {
   check_blowup(blowup);
   std::vector<uint8_t> wit;
   uint64_t n_blocks = 0;
@@ -893,12 +1200,25 @@ std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uin
     merge_hash_device(c, air, d_lde.p, n_trace, blowup, lam.data(), phi_mode, d_c.p, n_blocks);
   }
   cuda_check(cudaStreamSynchronize(s), "sync");
-  sg_fri_params p;
-  sg_build_params(n0, fs_binding, 1, &p);
-  std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
-  if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
+  CEval r;
+  r.d_c = std::move(d_c);
+  r.n0 = n0;
+  sg_build_params(n0, fs_binding, 1, &r.params);
+  return r;
+}
+
+std::vector<uint8_t> prove_from_ceval(sg_ctx* c, const CEval& ce, bool self_verify) {
+  std::vector<uint8_t> proof = stir_prove_device(c, ce.d_c.p, ce.n0, ce.params);
+  if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), ce.params))
     throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
   return proof;
+}
+
+std::vector<uint8_t> prove_hash_message(sg_ctx* c, const HashAir& air, const uint8_t* msg, uint64_t len,
+                                        const uint8_t fs_binding[32], int phi_mode, bool self_verify,
+                                        uint8_t* digest, uint64_t blowup) {
+  return prove_from_ceval(c, hash_message_ceval(c, air, msg, len, fs_binding, phi_mode, digest, blowup),
+                          self_verify);
 }
 
 // ------------------------------------------------------------------ RSA-2048 pipeline
@@ -930,8 +1250,8 @@ void rsa_witnesses(const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_b
     if (failed[w]) throw errs[w];
 }
 
-std::vector<uint8_t> prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be,
-                                   uint64_t n_records, const uint8_t pi[32], bool self_verify, uint64_t blowup) {
+CEval rsa2048_ceval(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, uint64_t n_records,
+                    const uint8_t pi[32], uint64_t blowup) {
   require(n_records >= 1 && n_records <= 65535, "prove_rsa2048: 1 to 65535 records");
   check_blowup(blowup);
   std::vector<rsa::RecordW> recs;
@@ -962,12 +1282,16 @@ std::vector<uint8_t> prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t
     cuda_check(quotient_zh(phi.p, n0, n_trace, d_c.p, s), "quotient");
     ntt(c, d_c.p, d_c.p, 1, n0, n0, ln, false, n0 - n_trace, scratch.p);
   }
-  sg_fri_params p;
-  sg_build_params(n0, pi, 1, &p);
-  std::vector<uint8_t> proof = stir_prove_device(c, d_c.p, n0, p);
-  if (self_verify && !stir_verify(decode_proof(proof.data(), proof.size()), p))
-    throw SgError{SG_EVERIFY, "self-verification of the produced proof failed"};
-  return proof;
+  CEval r;
+  r.d_c = std::move(d_c);
+  r.n0 = n0;
+  sg_build_params(n0, pi, 1, &r.params);
+  return r;
+}
+
+std::vector<uint8_t> prove_rsa2048(sg_ctx* c, const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be,
+                                   uint64_t n_records, const uint8_t pi[32], bool self_verify, uint64_t blowup) {
+  return prove_from_ceval(c, rsa2048_ceval(c, n_be, s_be, em_be, n_records, pi, blowup), self_verify);
 }
 
 std::vector<uint8_t> prove_sha256_message(sg_ctx* c, const uint8_t* msg, uint64_t len, const uint8_t fs_binding[32],

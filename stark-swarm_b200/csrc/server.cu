@@ -102,6 +102,7 @@ std::vector<uint8_t> prove_rsa_job(sg_ctx* c, const std::vector<uint8_t>& in, co
 struct sg_server {
   sg_ctx* parent = nullptr;
   int max_retries = 0;
+  int group_max = 1;  // SG_OPT_STIR_GROUP of the parent context
   uint64_t budget = 0;
   uint64_t in_flight = 0;
   int running = 0;
@@ -117,8 +118,8 @@ struct sg_server {
   void worker(sg_ctx* c) {
     cudaSetDevice(c->device);
     for (;;) {
-      uint64_t ticket = 0;
-      Entry* e = nullptr;
+      std::vector<uint64_t> tickets;
+      std::vector<Entry*> es;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv_work.wait(lk, [&] {
@@ -128,35 +129,148 @@ struct sg_server {
           return running == 0 || in_flight + f.footprint <= budget;
         });
         if (stop) return;
-        ticket = queue.front();
+        auto take = [&](uint64_t t) {
+          Entry* x = &entries.at(t);
+          tickets.push_back(t);
+          es.push_back(x);
+          in_flight += x->footprint;
+          ++x->attempts;
+          if (x->attempts == 1) x->t_start = Clock::now();
+        };
+        take(queue.front());
         queue.pop_front();
-        e = &entries.at(ticket);
-        in_flight += e->footprint;
+        // lockstep STIR: further queued jobs with the same n0, as far as the budget allows
+        const uint64_t n0 = job_n0(*es[0]);
+        if (group_max > 1 && n0) {
+          for (auto q = queue.begin(); q != queue.end() && (int)es.size() < group_max;) {
+            const Entry& f = entries.at(*q);
+            if (job_n0(f) == n0 && in_flight + f.footprint <= budget) {
+              take(*q);
+              q = queue.erase(q);
+            } else {
+              ++q;
+            }
+          }
+        }
         ++running;
-        ++e->attempts;
-        if (e->attempts == 1) e->t_start = Clock::now();
       }
-      run(c, e);
+      if (es.size() == 1)
+        run(c, es[0]);
+      else
+        run_group(c, es);
       {
         std::lock_guard<std::mutex> lk(mu);
-        in_flight -= e->footprint;
         --running;
-        const bool transient = e->status == SG_ENOMEM || e->status == SG_ECUDA;
-        if (e->cancel) {
-          e->status = SG_ECANCELED;
-          e->proof.clear();
-        } else if (transient && e->attempts <= max_retries) {
-          // reopened: back to the head of the queue for another attempt
-          queue.push_front(ticket);
-          e = nullptr;
-        }
-        if (e) {
+        for (size_t i = 0; i < es.size(); ++i) {
+          Entry* e = es[i];
+          in_flight -= e->footprint;
+          const bool transient = e->status == SG_ENOMEM || e->status == SG_ECUDA;
+          if (e->cancel) {
+            e->status = SG_ECANCELED;
+            e->proof.clear();
+          } else if (transient && e->attempts <= max_retries) {
+            // reopened: back to the head of the queue for another attempt
+            queue.push_front(tickets[i]);
+            continue;
+          }
           e->t_end = Clock::now();
           e->done = true;
         }
       }
       cv_done.notify_all();
       cv_work.notify_all();
+    }
+  }
+
+  // The proof domain of a job that can join a lockstep STIR group (0: it cannot).
+  static uint64_t job_n0(const Entry& e) {
+    if (e.kind == SG_JOB_SHA256)
+      return next_pow2(128 * ((e.input.size() + 9 + 63) / 64)) * e.blowup;
+    if (e.kind == SG_JOB_SHA512)
+      return next_pow2(128 * ((e.input.size() + 17 + 127) / 128)) * e.blowup;
+    if (e.kind == SG_JOB_P256_ECDSA) return sg::p256::K_ECDSA * e.blowup;
+    if (e.kind == SG_JOB_RSA2048) return sg::rsa::N_TRACE * e.blowup;
+    return 0;
+  }
+
+  // A job's c_eval (everything before its STIR phase).
+  static sg::CEval ceval(sg_ctx* c, Entry* e) {
+    const uint8_t* in = e->input.data();
+    if (e->kind == SG_JOB_SHA256)
+      return sg::hash_message_ceval(c, sg::sha256_hash_air(), in, e->input.size(), e->pi, e->phi_mode, e->digest,
+                                    e->blowup);
+    if (e->kind == SG_JOB_SHA512)
+      return sg::hash_message_ceval(c, sg::sha512_hash_air(), in, e->input.size(), e->pi, e->phi_mode, e->digest,
+                                    e->blowup);
+    if (e->kind == SG_JOB_P256_ECDSA)
+      return sg::p256_ecdsa_ceval(c, in, in + 32, in + 64, in + 96, in + 128, e->pi, e->blowup);
+    const uint64_t recs = e->input.size() / 768;
+    std::vector<uint8_t> n(256 * recs), s(256 * recs), em(256 * recs);
+    for (uint64_t r = 0; r < recs; ++r) {
+      memcpy(&n[256 * r], &in[768 * r], 256);
+      memcpy(&s[256 * r], &in[768 * r + 256], 256);
+      memcpy(&em[256 * r], &in[768 * r + 512], 256);
+    }
+    return sg::rsa2048_ceval(c, n.data(), s.data(), em.data(), recs, e->pi, e->blowup);
+  }
+
+  // Jobs with one n0: each c_eval on its own, then one lockstep STIR phase for all
+  // of them, then each proof's self-verification. A job that fails before the STIR
+  // phase leaves the group; a failure of the group's STIR phase fails its jobs.
+  static void run_group(sg_ctx* c, const std::vector<Entry*>& es) {
+    std::vector<Entry*> ok;
+    std::vector<sg::CEval> ce;
+    for (Entry* e : es) {
+      e->proof.clear();
+      e->err.clear();
+      try {
+        if ((e->flags & SG_JOB_FAULT_ALLOC) && e->attempts == 1)
+          throw sg::SgError{SG_ENOMEM, "injected fault: device allocation failed"};
+        ce.push_back(ceval(c, e));
+        ok.push_back(e);
+      } catch (const sg::SgError& x) {
+        e->status = x.code;
+        e->err = x.msg;
+      } catch (const std::exception& x) {
+        e->status = SG_EINVAL;
+        e->err = x.what();
+      }
+    }
+    if (ok.empty()) return;
+    try {
+      const uint64_t n0 = ce[0].n0;
+      sg::DBuf f0(n0 * ok.size(), c->stream);
+      std::vector<sg_fri_params> ps;
+      for (size_t g = 0; g < ok.size(); ++g) {
+        sg::require(ce[g].n0 == n0, "stir group: mixed domains");
+        sg::cuda_check(cudaMemcpyAsync(f0.p + g * n0, ce[g].d_c.p, n0 * 8, cudaMemcpyDeviceToDevice, c->stream),
+                       "copy");
+        ps.push_back(ce[g].params);
+      }
+      ce.clear();
+      std::vector<std::vector<uint8_t>> proofs = sg::stir_prove_group(c, f0.p, n0, n0, ps);
+      for (size_t g = 0; g < ok.size(); ++g) {
+        Entry* e = ok[g];
+        e->proof = std::move(proofs[g]);
+        if (e->flags & SG_JOB_FAULT_VERIFY) e->proof[e->proof.size() / 2] ^= 0x40;
+        try {
+          const sg::StirProof pr = sg::decode_proof(e->proof.data(), e->proof.size());
+          e->status = sg::stir_verify(pr, ps[g]) ? SG_OK : SG_EVERIFY;
+        } catch (const std::exception&) {
+          e->status = SG_EVERIFY;
+        }
+        if (e->status != SG_OK) e->err = "self-verification of the produced proof failed";
+      }
+    } catch (const sg::SgError& x) {
+      for (Entry* e : ok) {
+        e->status = x.code;
+        e->err = x.msg;
+      }
+    } catch (const std::exception& x) {
+      for (Entry* e : ok) {
+        e->status = SG_EINVAL;
+        e->err = x.what();
+      }
     }
   }
 
@@ -219,6 +333,7 @@ int sg_server_create(sg_ctx* ctx, int n_streams, uint64_t hbm_budget_bytes, sg_s
   *out = nullptr;
   sg_server* s = new sg_server;
   s->parent = ctx;
+  s->group_max = ctx->stir_group;
   s->budget = hbm_budget_bytes ? hbm_budget_bytes : UINT64_MAX;
   cudaSetDevice(ctx->device);
   int prio_low = 0, prio_high = 0;

@@ -32,10 +32,21 @@ inline uint64_t ood_blocks(uint64_t n, int m) {
 // starting from w^tid and stepping by w^S: consecutive threads read consecutive
 // groups of M coefficients. w^tid = w^{256 block} w^{tid mod 16} w^{16 (tid / 16 mod 16)},
 // the 33 factors computed once per CTA by 33 threads.
+// Proof groups (grid.y = proof g): with sc set, proof g's powers come from sc[g]
+// and its coefficients / partials start g_c / g_p elements further on.
 template <int M, bool BASE>
 __global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t* c, uint64_t n, gl::Fp6 w,
-                                                                   gl::Fp6 w_stride, uint64_t* partials) {
+                                                                   gl::Fp6 w_stride, uint64_t* partials,
+                                                                   const OodScalars* sc, uint64_t g_c,
+                                                                   uint64_t g_p) {
   static_assert(kOodThreads == 256, "the power table covers 256 threads");
+  if (sc) {
+    const uint32_t g = blockIdx.y;
+    w = sc[g].w;
+    w_stride = sc[g].ws;
+    c += g * g_c;
+    partials += g * g_p;
+  }
   const uint64_t n_groups = n / M;
   const uint64_t S = (uint64_t)gridDim.x * kOodThreads;
   const uint64_t tid = (uint64_t)blockIdx.x * kOodThreads + threadIdx.x;
@@ -100,7 +111,16 @@ __global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t
 constexpr uint64_t kOodSmallGroups = 4096;
 template <int M, bool BASE>
 __global__ void __launch_bounds__(M * 32) ood_small_kernel(const uint64_t* c, uint64_t n, gl::Fp6 w, gl::Fp6 w32,
-                                                           gl::Fp6 z, uint64_t* evals) {
+                                                           gl::Fp6 z, uint64_t* evals, const OodScalars* sc,
+                                                           uint64_t g_c, uint64_t g_e) {
+  if (sc) {
+    const uint32_t g = blockIdx.x;  // one CTA per proof
+    w = sc[g].w;
+    w32 = sc[g].w32;
+    z = sc[g].z;
+    c += g * g_c;
+    evals += g * g_e;
+  }
   const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
   const uint64_t n_groups = n / M;
   __shared__ uint64_t T[M * 6];
@@ -151,7 +171,14 @@ __global__ void __launch_bounds__(M * 32) ood_small_kernel(const uint64_t* c, ui
 
 // Sum block partials into T_r, then evals[j] = sum_r w_M^{jr} z^r T_r.
 template <int M>
-__global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, gl::Fp6 z, uint64_t* evals) {
+__global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, gl::Fp6 z, uint64_t* evals,
+                                  const OodScalars* sc, uint64_t g_p, uint64_t g_e) {
+  if (sc) {
+    const uint32_t g = blockIdx.x;  // one CTA per proof
+    z = sc[g].z;
+    partials += g * g_p;
+    evals += g * g_e;
+  }
   __shared__ uint64_t T[M * 6];
   // one warp per element: the lanes stride over the block partials
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
@@ -182,12 +209,24 @@ __global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, g
   for (int q = 0; q < 6; ++q) evals[j * 6 + q] = acc.c[q];
 }
 
+// proof g = blockIdx.y of a group: its buffers and challenge (FoldArgs' g_* strides)
+__device__ __forceinline__ void fold_select(FoldArgs& a) {
+  const uint32_t g = blockIdx.y;
+  if (g == 0 && !a.alphas) return;
+  a.f += g * a.g_f;
+  if (a.next) a.next += g * a.g_next;
+  if (a.tuples) a.tuples += g * a.g_tuples;
+  if (a.leaves) a.leaves += g * a.g_leaves;
+  if (a.alphas) a.alpha = a.alphas[g];
+}
+
 template <int M, bool BASE>
 __global__ void fold_kernel(FoldArgs a) {
   constexpr int LM = M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : 4;
   const uint64_t nn = a.n / M;
   const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (b >= nn) return;
+  fold_select(a);
   constexpr int NC = BASE ? 1 : 6;
   uint64_t x[NC][M];
 #pragma unroll
@@ -254,6 +293,7 @@ __global__ void fold_small_kernel(FoldArgs a) {
   const uint64_t nn = a.n / M;
   const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (b >= nn) return;
+  fold_select(a);
   constexpr int NC = BASE ? 1 : 6;
   uint64_t xs[NC][M];
 #pragma unroll 1
@@ -312,9 +352,16 @@ __global__ void fold_small_kernel(FoldArgs a) {
 }
 
 template <int M>
-__global__ void fold_tuples_kernel(const uint64_t* tup, uint64_t nf, gl::Fp6 alpha, uint64_t* next) {
+__global__ void fold_tuples_kernel(const uint64_t* tup, uint64_t nf, gl::Fp6 alpha, uint64_t* next,
+                                   const gl::Fp6* alphas, uint64_t g_tup, uint64_t g_next) {
   const uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (b >= nf) return;
+  if (alphas) {
+    const uint32_t g = blockIdx.y;
+    alpha = alphas[g];
+    tup += g * g_tup;
+    next += g * g_next;
+  }
   gl::Fp6 acc;
 #pragma unroll
   for (int q = 0; q < 6; ++q) acc.c[q] = tup[(uint64_t)((M - 1) * 6 + q) * nf + b];
@@ -328,30 +375,35 @@ __global__ void fold_tuples_kernel(const uint64_t* tup, uint64_t nf, gl::Fp6 alp
   for (int q = 0; q < 6; ++q) next[(uint64_t)q * nf + b] = acc.c[q];
 }
 
+// One proof (sc null: powers from z on the host) or a group of G proofs (sc set).
 template <int M>
-cudaError_t ood_launch(const uint64_t* c, bool base, uint64_t n, const gl::Fp6& z, uint64_t* partials,
-                       uint64_t* evals, cudaStream_t s) {
-  const gl::Fp6 w = gl::e_pow(z, M);
+cudaError_t ood_launch(const uint64_t* c, uint64_t g_c, bool base, uint64_t n, const gl::Fp6& z,
+                       const OodScalars* sc, uint64_t* partials, uint64_t* evals, uint64_t g_e, uint32_t G,
+                       cudaStream_t s) {
+  gl::Fp6 w = gl::e_zero(), w32 = w, ws = w;
+  if (!sc) w = gl::e_pow(z, M);
   if (n / M <= kOodSmallGroups) {
-    const gl::Fp6 w32 = gl::e_pow(w, 32);
+    if (!sc) w32 = gl::e_pow(w, 32);
     SG_LAUNCH_SCOPE("stir_ood", s);
     if (base)
-      ood_small_kernel<M, true><<<1, M * 32, 0, s>>>(c, n, w, w32, z, evals);
+      ood_small_kernel<M, true><<<G, M * 32, 0, s>>>(c, n, w, w32, z, evals, sc, g_c, g_e);
     else
-      ood_small_kernel<M, false><<<1, M * 32, 0, s>>>(c, n, w, w32, z, evals);
+      ood_small_kernel<M, false><<<G, M * 32, 0, s>>>(c, n, w, w32, z, evals, sc, g_c, g_e);
     return cudaGetLastError();
   }
-  const uint64_t blocks = ood_blocks(n, M);
-  const gl::Fp6 ws = gl::e_pow(w, blocks * kOodThreads);
+  const uint64_t blocks = ood_blocks(n, M), g_p = blocks * M * 6;
+  if (!sc) ws = gl::e_pow(w, blocks * kOodThreads);
   {
     SG_LAUNCH_SCOPE("stir_ood", s);
     if (base)
-      ood_partial_kernel<M, true><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
+      ood_partial_kernel<M, true><<<dim3((unsigned)blocks, G), kOodThreads, 0, s>>>(c, n, w, ws, partials, sc, g_c,
+                                                                                     g_p);
     else
-      ood_partial_kernel<M, false><<<(unsigned)blocks, kOodThreads, 0, s>>>(c, n, w, ws, partials);
+      ood_partial_kernel<M, false><<<dim3((unsigned)blocks, G), kOodThreads, 0, s>>>(c, n, w, ws, partials, sc,
+                                                                                      g_c, g_p);
   }
   SG_LAUNCH_SCOPE("stir_ood_finish", s);
-  ood_finish_kernel<M><<<1, 256, 0, s>>>(partials, blocks, z, evals);
+  ood_finish_kernel<M><<<G, 256, 0, s>>>(partials, blocks, z, evals, sc, g_p, g_e);
   return cudaGetLastError();
 }
 
@@ -360,16 +412,17 @@ cudaError_t fold_launch(const FoldArgs& a, cudaStream_t s) {
   const uint64_t nn = a.n / M;
   const unsigned T = 128;
   const unsigned blocks = (unsigned)((nn + T - 1) / T);
+  const dim3 grid(blocks, a.n_proofs ? a.n_proofs : 1);
   SG_LAUNCH_SCOPE("stir_fold", s);
   if (nn <= kFoldSmall) {
     if (a.base)
-      fold_small_kernel<M, true><<<blocks, T, 0, s>>>(a);
+      fold_small_kernel<M, true><<<grid, T, 0, s>>>(a);
     else
-      fold_small_kernel<M, false><<<blocks, T, 0, s>>>(a);
+      fold_small_kernel<M, false><<<grid, T, 0, s>>>(a);
   } else if (a.base) {
-    fold_kernel<M, true><<<blocks, T, 0, s>>>(a);
+    fold_kernel<M, true><<<grid, T, 0, s>>>(a);
   } else {
-    fold_kernel<M, false><<<blocks, T, 0, s>>>(a);
+    fold_kernel<M, false><<<grid, T, 0, s>>>(a);
   }
   return cudaGetLastError();
 }
@@ -382,16 +435,39 @@ cudaError_t ood_evaluate(const uint64_t* coeffs, bool base, uint64_t n, int m, c
                          uint64_t* partials, uint64_t* evals, cudaStream_t s) {
   if (n % m) return cudaErrorInvalidValue;
   switch (m) {
-    case 2: return ood_launch<2>(coeffs, base, n, z, partials, evals, s);
-    case 4: return ood_launch<4>(coeffs, base, n, z, partials, evals, s);
-    case 8: return ood_launch<8>(coeffs, base, n, z, partials, evals, s);
-    case 16: return ood_launch<16>(coeffs, base, n, z, partials, evals, s);
+    case 2: return ood_launch<2>(coeffs, 0, base, n, z, nullptr, partials, evals, 0, 1, s);
+    case 4: return ood_launch<4>(coeffs, 0, base, n, z, nullptr, partials, evals, 0, 1, s);
+    case 8: return ood_launch<8>(coeffs, 0, base, n, z, nullptr, partials, evals, 0, 1, s);
+    case 16: return ood_launch<16>(coeffs, 0, base, n, z, nullptr, partials, evals, 0, 1, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+OodScalars ood_scalars(const gl::Fp6& z, uint64_t n, int m) {
+  OodScalars r;
+  r.z = z;
+  r.w = gl::e_pow(z, (uint64_t)m);
+  r.w32 = gl::e_pow(r.w, 32);
+  r.ws = gl::e_pow(r.w, ood_blocks(n, m) * kOodThreads);
+  return r;
+}
+
+cudaError_t ood_evaluate_group(const uint64_t* coeffs, uint64_t g_c, bool base, uint64_t n, int m,
+                               const OodScalars* sc, uint64_t* partials, uint64_t* evals, uint64_t g_e,
+                               uint32_t n_proofs, cudaStream_t s) {
+  if (n % m || !sc || n_proofs == 0 || n_proofs > 65535) return cudaErrorInvalidValue;
+  const gl::Fp6 z = gl::e_zero();
+  switch (m) {
+    case 2: return ood_launch<2>(coeffs, g_c, base, n, z, sc, partials, evals, g_e, n_proofs, s);
+    case 4: return ood_launch<4>(coeffs, g_c, base, n, z, sc, partials, evals, g_e, n_proofs, s);
+    case 8: return ood_launch<8>(coeffs, g_c, base, n, z, sc, partials, evals, g_e, n_proofs, s);
+    case 16: return ood_launch<16>(coeffs, g_c, base, n, z, sc, partials, evals, g_e, n_proofs, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
 cudaError_t stir_fold(const FoldArgs& a, cudaStream_t s) {
-  if (a.n % a.m || a.log_n > kMaxLogN) return cudaErrorInvalidValue;
+  if (a.n % a.m || a.log_n > kMaxLogN || a.n_proofs > 65535) return cudaErrorInvalidValue;
   switch (a.m) {
     case 2: return fold_launch<2>(a, s);
     case 4: return fold_launch<4>(a, s);
@@ -406,10 +482,27 @@ cudaError_t fold_tuples(const uint64_t* tuples, uint64_t n_final, int m, const g
   const unsigned blocks = (unsigned)((n_final + 127) / 128);
   SG_LAUNCH_SCOPE("stir_fold_tuples", s);
   switch (m) {
-    case 2: fold_tuples_kernel<2><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
-    case 4: fold_tuples_kernel<4><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
-    case 8: fold_tuples_kernel<8><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
-    case 16: fold_tuples_kernel<16><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next); break;
+    case 2: fold_tuples_kernel<2><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next, nullptr, 0, 0); break;
+    case 4: fold_tuples_kernel<4><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next, nullptr, 0, 0); break;
+    case 8: fold_tuples_kernel<8><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next, nullptr, 0, 0); break;
+    case 16: fold_tuples_kernel<16><<<blocks, 128, 0, s>>>(tuples, n_final, alpha, next, nullptr, 0, 0); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t fold_tuples_group(const uint64_t* tuples, uint64_t g_tup, uint64_t n_final, int m,
+                              const gl::Fp6* alphas, uint64_t* next, uint64_t g_next, uint32_t n_proofs,
+                              cudaStream_t s) {
+  if (!alphas || n_proofs == 0 || n_proofs > 65535) return cudaErrorInvalidValue;
+  const dim3 grid((unsigned)((n_final + 127) / 128), n_proofs);
+  const gl::Fp6 z = gl::e_zero();
+  SG_LAUNCH_SCOPE("stir_fold_tuples", s);
+  switch (m) {
+    case 2: fold_tuples_kernel<2><<<grid, 128, 0, s>>>(tuples, n_final, z, next, alphas, g_tup, g_next); break;
+    case 4: fold_tuples_kernel<4><<<grid, 128, 0, s>>>(tuples, n_final, z, next, alphas, g_tup, g_next); break;
+    case 8: fold_tuples_kernel<8><<<grid, 128, 0, s>>>(tuples, n_final, z, next, alphas, g_tup, g_next); break;
+    case 16: fold_tuples_kernel<16><<<grid, 128, 0, s>>>(tuples, n_final, z, next, alphas, g_tup, g_next); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -37,11 +37,36 @@ struct FoldArgs {
   uint64_t leaf_arity0;
   const uint64_t* tw_inv_lo;
   const uint64_t* tw_inv_hi;
+  // Several proofs of one shape in one launch (grid.y = proof g): each pointer
+  // above advances by its g_* stride (u64 elements) per proof, and the fold
+  // challenge is alphas[g] (device memory) when alphas is set. The defaults
+  // describe one proof.
+  uint32_t n_proofs = 1;
+  uint64_t g_f = 0, g_next = 0, g_tuples = 0, g_leaves = 0;
+  const gl::Fp6* alphas = nullptr;
 };
 cudaError_t stir_fold(const FoldArgs& a, cudaStream_t s);
 
 // next[b] = sum_k tuple_k alpha^k over n_final tuples of m (planes as above).
 cudaError_t fold_tuples(const uint64_t* tuples, uint64_t n_final, int m, const gl::Fp6& alpha, uint64_t* next,
                         cudaStream_t s);
+
+// The same for n_proofs proofs of one shape (tuples and next advance by g_tup /
+// g_next per proof; alpha of proof g = alphas[g], device memory).
+cudaError_t fold_tuples_group(const uint64_t* tuples, uint64_t g_tup, uint64_t n_final, int m,
+                              const gl::Fp6* alphas, uint64_t* next, uint64_t g_next, uint32_t n_proofs,
+                              cudaStream_t s);
+
+// Out-of-domain evaluation of n_proofs proofs of one shape in one launch set:
+// proof g's coefficients at coeffs + g g_c, its evaluations at evals + g g_e,
+// its point and the powers the kernels use in sc[g] (device memory, filled
+// from ood_scalars). partials: n_proofs * ood_partials_len(n, m).
+struct OodScalars {
+  gl::Fp6 z, w, w32, ws;  // z, w = z^m, w^32, w^(threads of the partial pass)
+};
+OodScalars ood_scalars(const gl::Fp6& z, uint64_t n, int m);
+cudaError_t ood_evaluate_group(const uint64_t* coeffs, uint64_t g_c, bool base, uint64_t n, int m,
+                               const OodScalars* sc, uint64_t* partials, uint64_t* evals, uint64_t g_e,
+                               uint32_t n_proofs, cudaStream_t s);
 
 }  // namespace sg
