@@ -560,17 +560,27 @@ def record_checks(sg, ctx, n_jobs, streams):
            "mix": {k: kinds.count(k) for k in sorted(set(kinds))},
            "sha256_blocks": {"min": int((lens.min() + 9 + 63) // 64), "max": int((lens.max() + 9 + 63) // 64)}}
     proofs = {}
-    for label, st in (("plain", 1), ("batched", streams)):
-        t0 = time.perf_counter()
-        res = ctx.prove_batch(jobs, n_streams=st, hbm_budget_bytes=160 << 30)
-        dt = time.perf_counter() - t0
+    # plain: one proof at a time; batched: `streams` proofs in flight; grouped: the
+    # same, and each worker proves the STIR phases of up to 8 queued jobs of one n0
+    # in lockstep (one launch per stage for the group)
+    for label, st, group in (("plain", 1, 1), ("batched", streams, 1), ("grouped", streams, 8)):
+        ctx.set_option(sg.OPT_STIR_GROUP, group)
+        try:
+            t0 = time.perf_counter()
+            res = ctx.prove_batch(jobs, n_streams=st, hbm_budget_bytes=160 << 30)
+            dt = time.perf_counter() - t0
+        finally:
+            ctx.set_option(sg.OPT_STIR_GROUP, 1)
         assert all(r.status == 0 for _, r in res), "a record-check proof failed"
         proofs[label] = [p for p, _ in res]
         lat = sorted(r.latency_ms for _, r in res)
-        out[label] = {"streams": st, "proofs_per_s": len(jobs) / dt, "records_per_s": n_jobs / dt, "s": dt,
+        out[label] = {"streams": st, "stir_group": group, "proofs_per_s": len(jobs) / dt,
+                      "records_per_s": n_jobs / dt, "s": dt,
                       "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(len(lat) * 0.99))]}
-    assert proofs["plain"] == proofs["batched"], "a proof in the batch differs from the same proof alone"
+    assert proofs["plain"] == proofs["batched"] == proofs["grouped"], \
+        "a proof in the batch differs from the same proof alone"
     out["batched_over_plain"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
+    out["grouped_over_plain"] = out["grouped"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
     out["identical_alone_and_batched"] = True
     return out
 
