@@ -164,24 +164,29 @@ __device__ __forceinline__ uint64_t xor_poly(uint64_t x, uint64_t y) {
 }
 
 // Point i of a column-major evaluation buffer (n points per column): cur = point
-// i, nxt = point (i + step) mod n, trace_row = i / row_div, result to
-// phi[out_off + i * out_stride]. The full LDE uses (step, row_div) = (blowup,
-// blowup); one coset r of it (points r + blowup a) uses (1, 1) with
-// out_off = r, out_stride = blowup.
-__global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n, uint64_t step,
+// i, nxt = point (i + step) mod n, trace_row = i / row_div. The full LDE uses
+// (step, row_div) = (blowup, blowup); one coset of it uses (1, 1).
+// The 766 constraints are split into kPhiChunks chunks (grid.y): constraints
+// 0-263 (bit booleanity, bit -> word packs), 264-523 (the four Sigma / sigma
+// blocks) and 524-765 (Ch, Maj, carries, register shifts, H, W window,
+// schedule). Chunk c writes its part of Phi at part[c n + i]; sha256_phi_sum adds
+// them. Three shorter threads per point keep more warps in flight than one long
+// one: a thread of the unsplit kernel spent most of its time waiting on loads.
+constexpr int kPhiChunks = 3;
+__global__ void __launch_bounds__(128, 4) sha256_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n, uint64_t step,
                                                          uint64_t row_div, uint64_t n_blocks,
-                                                         const uint64_t* __restrict__ lam, uint64_t* __restrict__ phi,
-                                                         uint64_t out_stride, uint64_t out_off) {
+                                                         const uint64_t* __restrict__ lam, uint64_t* __restrict__ part) {
   using namespace sha;
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const uint32_t chunk = blockIdx.y;
   const uint64_t j = (i + step) & (n - 1);
   auto C = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + i); };
   auto X = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + j); };
   const uint64_t row = i / row_div, blk = row / ROWS_PER_BLOCK, br = row % ROWS_PER_BLOCK;
   const bool past = blk >= n_blocks;
   const bool comp = !past && br < 64, fin = !past && br == 64, sched = !past && br >= 15 && br <= 62;
-  Acc acc{lam, 0, 0};
+  Acc acc{lam, 0, chunk == 0 ? 0u : chunk == 1 ? 264u : 524u};
   // sum_b v_b 2^b over 32 columns: 96-bit terms summed exactly, one reduction
   auto pack = [&](uint32_t off) {
     gl::Acc128 a;
@@ -189,6 +194,7 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
     for (int b = 0; b < 32; ++b) a.add_shl(C(off + b), b);
     return a.reduce();
   };
+  if (chunk == 0) {
   // bit booleanity: A, B, C, E, F, G, W_win[14], W_win[1]
   const uint32_t bool_offs[8] = {BIT_A, BIT_B, BIT_C, BIT_E, BIT_F, BIT_G, BIT_WW14, BIT_WW1};
 #pragma unroll 1
@@ -207,6 +213,10 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
   acc.push(gl::sub(C(A_g), pack(BIT_G)));
   acc.push(gl::sub(C(WW0 + 14), pack(BIT_WW14)));
   acc.push(gl::sub(C(WW0 + 1), pack(BIT_WW1)));
+  part[i] = acc.phi;
+  return;
+  }
+  if (chunk == 1) {
   // Sigma0(a), Sigma1(e) (rotations), sigma0(W[t-14]), sigma1(W[t-1]) (two rotations + a shift)
   struct Sg {
     uint32_t bits, t, bit, w;
@@ -229,6 +239,9 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
       acc.push(gl::sub(C(g.bit + b), xor_poly(C(g.t + b), r)));
     }
     acc.push(gl::sub(C(g.w), pack(g.bit)));
+  }
+  part[n + i] = acc.phi;
+  return;
   }
   // Ch(e, f, g) = e f + g - e g
 #pragma unroll 4
@@ -314,7 +327,14 @@ __global__ void __launch_bounds__(128) sha256_phi_kernel(const uint64_t* __restr
   } else {
     acc.zeros(4);
   }
-  phi[out_off + i * out_stride] = acc.phi;
+  part[2 * n + i] = acc.phi;
+}
+
+__global__ void sha256_phi_sum(const uint64_t* __restrict__ part, uint64_t n, uint64_t* __restrict__ phi,
+                               uint64_t out_stride, uint64_t out_off) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  phi[out_off + i * out_stride] = gl::add(gl::add(part[i], part[n + i]), part[2 * n + i]);
 }
 
 bool g_k_uploaded[64] = {false};
@@ -408,10 +428,21 @@ cudaError_t sha256_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, 
   cudaError_t e = upload_k();
   if (e != cudaSuccess) return e;
   const unsigned T = 128;
-  SG_LAUNCH_SCOPE("merge_phi", s);
-  sha256_phi_kernel<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(evals, n, step, row_div, n_blocks, lambdas, phi,
-                                                                out_stride, out_off);
-  return cudaGetLastError();
+  uint64_t* part = nullptr;
+  e = cudaMallocAsync((void**)&part, kPhiChunks * n * sizeof(uint64_t), s);
+  if (e != cudaSuccess) return e;
+  {
+    SG_LAUNCH_SCOPE("merge_phi", s);
+    sha256_phi_kernel<<<dim3((unsigned)((n + T - 1) / T), kPhiChunks), T, 0, s>>>(evals, n, step, row_div, n_blocks,
+                                                                                   lambdas, part);
+  }
+  {
+    SG_LAUNCH_SCOPE("merge_phi_sum", s);
+    sha256_phi_sum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part, n, phi, out_stride, out_off);
+  }
+  e = cudaGetLastError();
+  cudaFreeAsync(part, s);
+  return e;
 }
 
 }  // namespace sg
