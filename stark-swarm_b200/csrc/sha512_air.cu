@@ -212,20 +212,25 @@ __device__ __forceinline__ uint64_t xor_poly(uint64_t x, uint64_t y) {
   return gl::sub(gl::add(x, y), gl::add(m, m));
 }
 
-__global__ void __launch_bounds__(128) sha512_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n, uint64_t step,
-                                                         uint64_t row_div, uint64_t n_blocks,
-                                                         const uint64_t* __restrict__ lam, uint64_t* __restrict__ phi,
-                                                         uint64_t out_stride, uint64_t out_off) {
+// The 1526 constraints in kPhiChunks chunks (grid.y), as in the SHA-256 kernel:
+// 0-527 (bit booleanity, limb packs), 528-1047 (the four Sigma / sigma blocks),
+// 1048-1525 (the rest); chunk c writes its part of Phi at part[c n + i].
+constexpr int kPhiChunks = 3;
+__global__ void __launch_bounds__(128, 4) sha512_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n,
+                                                            uint64_t step, uint64_t row_div, uint64_t n_blocks,
+                                                            const uint64_t* __restrict__ lam,
+                                                            uint64_t* __restrict__ part) {
   using namespace sha512;
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const uint32_t chunk = blockIdx.y;
   const uint64_t j = (i + step) & (n - 1);
   auto C = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + i); };
   auto X = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + j); };
   const uint64_t row = i / row_div, blk = row / ROWS_PER_BLOCK, br = row % ROWS_PER_BLOCK;
   const bool past = blk >= n_blocks;
   const bool comp = !past && br < ROUNDS, fin = !past && br == ROUNDS, sched = !past && br >= 15 && br <= 78;
-  Acc acc{lam, 0, 0};
+  Acc acc{lam, 0, chunk == 0 ? 0u : chunk == 1 ? 528u : 1048u};
   // sum_{b<32} v_b 2^b over 32 columns: 96-bit terms summed exactly, one reduction
   auto pack = [&](uint32_t off) {
     gl::Acc128 a;
@@ -234,6 +239,7 @@ __global__ void __launch_bounds__(128) sha512_phi_kernel(const uint64_t* __restr
     return a.reduce();
   };
   const uint64_t P32 = 1ull << 32;
+  if (chunk == 0) {
   // bit booleanity: A, B, C, E, F, G, W_win[14], W_win[1]
   const uint32_t bool_offs[8] = {BIT_A, BIT_B, BIT_C, BIT_E, BIT_F, BIT_G, BIT_WW14, BIT_WW1};
 #pragma unroll 1
@@ -252,6 +258,10 @@ __global__ void __launch_bounds__(128) sha512_phi_kernel(const uint64_t* __restr
     acc.push(gl::sub(C(limb_words[q][0]), pack(limb_words[q][1])));
     acc.push(gl::sub(C(limb_words[q][0] + 1), pack(limb_words[q][1] + 32)));
   }
+  part[i] = acc.phi;
+  return;
+  }
+  if (chunk == 1) {
   // Sigma0(a), Sigma1(e) (rotations), sigma0(W_win[1]), sigma1(W_win[14]) (two rotations + a shift)
   struct Sg {
     uint32_t bits, t, bit, lo;
@@ -275,6 +285,9 @@ __global__ void __launch_bounds__(128) sha512_phi_kernel(const uint64_t* __restr
     }
     acc.push(gl::sub(C(g.lo), pack(g.bit)));
     acc.push(gl::sub(C(g.lo + 1), pack(g.bit + 32)));
+  }
+  part[n + i] = acc.phi;
+  return;
   }
   // Ch(e, f, g) = e f + g - e g
 #pragma unroll 4
@@ -393,7 +406,14 @@ __global__ void __launch_bounds__(128) sha512_phi_kernel(const uint64_t* __restr
   } else {
     acc.zeros(8);
   }
-  phi[out_off + i * out_stride] = acc.phi;
+  part[2 * n + i] = acc.phi;
+}
+
+__global__ void sha512_phi_sum(const uint64_t* __restrict__ part, uint64_t n, uint64_t* __restrict__ phi,
+                               uint64_t out_stride, uint64_t out_off) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  phi[out_off + i * out_stride] = gl::add(gl::add(part[i], part[n + i]), part[2 * n + i]);
 }
 
 bool g_k_uploaded[64] = {false};
@@ -475,10 +495,21 @@ cudaError_t sha512_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, 
   cudaError_t e = upload_k();
   if (e != cudaSuccess) return e;
   const unsigned T = 128;
-  SG_LAUNCH_SCOPE("merge_phi", s);
-  sha512_phi_kernel<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(evals, n, step, row_div, n_blocks, lambdas, phi,
-                                                                out_stride, out_off);
-  return cudaGetLastError();
+  uint64_t* part = nullptr;
+  e = cudaMallocAsync((void**)&part, kPhiChunks * n * sizeof(uint64_t), s);
+  if (e != cudaSuccess) return e;
+  {
+    SG_LAUNCH_SCOPE("merge_phi", s);
+    sha512_phi_kernel<<<dim3((unsigned)((n + T - 1) / T), kPhiChunks), T, 0, s>>>(evals, n, step, row_div, n_blocks,
+                                                                                   lambdas, part);
+  }
+  {
+    SG_LAUNCH_SCOPE("merge_phi_sum", s);
+    sha512_phi_sum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part, n, phi, out_stride, out_off);
+  }
+  e = cudaGetLastError();
+  cudaFreeAsync(part, s);
+  return e;
 }
 
 }  // namespace sg
