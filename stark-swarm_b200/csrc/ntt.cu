@@ -816,17 +816,20 @@ uint64_t lde_leaf_scratch_elems(uint32_t w, int log_n) {
   return (r <= 12 ? 1ull : 2ull) * w * (1ull << log_n);
 }
 
-cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t in_stride, uint32_t w, int log_n,
-                               uint64_t n_valid, const PowSpec* pre, uint64_t* scratch, uint64_t arity0,
-                               uint64_t label, uint64_t* leaves, uint64_t* out, uint32_t keep_cols, cudaStream_t s) {
-  if (!lde_leaf_ok(w, log_n) || !scratch || !leaves || keep_cols > w || (keep_cols && !out))
-    return cudaErrorInvalidValue;
+// The passes before the fused one, for columns c0 .. c0 + wc - 1 of a w-column
+// transform (column c's input at in + c in_stride; scratch as lde_leaf_transform's).
+// Every pass works column by column, so a host-input pipeline can run them
+// chunk by chunk as the chunks arrive.
+cudaError_t lde_leaf_prepasses(const NttTables& t, const uint64_t* in, uint64_t in_stride, uint32_t w, uint32_t c0,
+                               uint32_t wc, int log_n, uint64_t n_valid, const PowSpec* pre, uint64_t* scratch,
+                               cudaStream_t s) {
+  if (!lde_leaf_ok(w, log_n) || !scratch || c0 + wc > w) return cudaErrorInvalidValue;
+  if (wc == 0) return cudaSuccess;
   const uint64_t N = 1ull << log_n, A = kFuseA;
   if (n_valid > N) n_valid = N;
   const PowSpec none{};
   const int r = log_n - kFuseLogA;
-  const uint64_t* last_in;
-  uint64_t BC;
+  in += (uint64_t)c0 * in_stride;
   if (r <= 12) {
     // four-step with N1 = 2^7: pass 1 as ntt_batch's, transposed into scratch
     const uint64_t N2 = 1ull << r;
@@ -845,18 +848,16 @@ cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t 
     a.sparse_nz = sparse_nz_for(n_valid, N, A, N2);
     a.tw_log = log_n;
     a.pre = pre ? *pre : none;
-    cudaError_t e = launch_pass_dyn(r, a, false, w, s);
-    if (e != cudaSuccess) return e;
-    last_in = scratch;
-    BC = N2;
+    a.out = scratch + (uint64_t)c0 * N;
+    return launch_pass_dyn(r, a, false, wc, s);
   } else {
     // three passes N = A * B * C, as ntt_batch's, with C and B as even as possible
     // (2^8 x 2^8 for a 2^23 domain): every pass then fills its CTAs' lanes, where
     // C = 2^12 would leave a 2^(r - 12)-point middle pass with mostly idle lanes
     const int lc = (r + 1) / 2, lb = r - lc;
     const uint64_t B = 1ull << lb, C = 1ull << lc, AB = A * B;
-    uint64_t* s1 = scratch;
-    uint64_t* s2 = scratch + (uint64_t)w * N;
+    uint64_t* s1 = scratch + (uint64_t)c0 * N;
+    uint64_t* s2 = scratch + (uint64_t)w * N + (uint64_t)c0 * N;
     PassArgs a = base_args(t, false);
     a.in = in;
     a.out = s1;
@@ -872,7 +873,7 @@ cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t 
     a.sparse_nz = sparse_nz_for(n_valid, N, AB, C);
     a.tw_log = log_n;
     a.pre = pre ? *pre : none;
-    cudaError_t e = launch_pass_dyn(lc, a, false, w, s);
+    cudaError_t e = launch_pass_dyn(lc, a, false, wc, s);
     if (e != cudaSuccess) return e;
     PassArgs b = base_args(t, false);
     b.in = s1;
@@ -890,11 +891,19 @@ cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t 
     b.flat_lane = 1;
     b.in_valid = AB;
     b.tw_log = kFuseLogA + lb;
-    e = launch_pass_dyn(lb, b, false, (uint64_t)w * C, s);
-    if (e != cudaSuccess) return e;
-    last_in = s2;
-    BC = B * C;
+    return launch_pass_dyn(lb, b, false, (uint64_t)wc * C, s);
   }
+}
+
+// The fused last pass over all w columns, after lde_leaf_prepasses covered them.
+cudaError_t lde_leaf_final(const NttTables& t, uint32_t w, int log_n, const uint64_t* scratch, uint64_t arity0,
+                           uint64_t label, uint64_t* leaves, uint64_t* out, uint32_t keep_cols, cudaStream_t s) {
+  if (!lde_leaf_ok(w, log_n) || !scratch || !leaves || keep_cols > w || (keep_cols && !out))
+    return cudaErrorInvalidValue;
+  const uint64_t N = 1ull << log_n;
+  const int r = log_n - kFuseLogA;
+  const uint64_t* last_in = r <= 12 ? scratch : scratch + (uint64_t)w * N;
+  const uint64_t BC = N >> kFuseLogA;
   LeafFuse f{last_in, N, BC, w, keep_cols, arity0, label, leaves, out, t.d_fwd_st};
   const size_t smem = ((size_t)kFuseTileLanes * kFuseMp + kFuseA) * sizeof(uint64_t);
   cudaError_t e = cudaFuncSetAttribute(lde_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -902,6 +911,14 @@ cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t 
   SG_LAUNCH_SCOPE("lde_leaf", s);
   lde_leaf_kernel<<<(unsigned)(BC / kFuseLanes), kFuseThreads, smem, s>>>(f);
   return cudaGetLastError();
+}
+
+cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t in_stride, uint32_t w, int log_n,
+                               uint64_t n_valid, const PowSpec* pre, uint64_t* scratch, uint64_t arity0,
+                               uint64_t label, uint64_t* leaves, uint64_t* out, uint32_t keep_cols, cudaStream_t s) {
+  cudaError_t e = lde_leaf_prepasses(t, in, in_stride, w, 0, w, log_n, n_valid, pre, scratch, s);
+  if (e != cudaSuccess) return e;
+  return lde_leaf_final(t, w, log_n, scratch, arity0, label, leaves, out, keep_cols, s);
 }
 
 }  // namespace sg

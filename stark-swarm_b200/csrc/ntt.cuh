@@ -105,6 +105,14 @@ uint64_t lde_leaf_scratch_elems(uint32_t w, int log_n);
 cudaError_t lde_leaf_transform(const NttTables& t, const uint64_t* in, uint64_t in_stride, uint32_t w, int log_n,
                                uint64_t n_valid, const PowSpec* pre, uint64_t* scratch, uint64_t arity0,
                                uint64_t label, uint64_t* leaves, uint64_t* out, uint32_t keep_cols, cudaStream_t s);
+// lde_leaf_transform in two steps: the passes before the fused one for columns
+// c0 .. c0 + wc - 1 (column by column, so chunks can go as they arrive), then the
+// fused pass over all w columns.
+cudaError_t lde_leaf_prepasses(const NttTables& t, const uint64_t* in, uint64_t in_stride, uint32_t w, uint32_t c0,
+                               uint32_t wc, int log_n, uint64_t n_valid, const PowSpec* pre, uint64_t* scratch,
+                               cudaStream_t s);
+cudaError_t lde_leaf_final(const NttTables& t, uint32_t w, int log_n, const uint64_t* scratch, uint64_t arity0,
+                           uint64_t label, uint64_t* leaves, uint64_t* out, uint32_t keep_cols, cudaStream_t s);
 
 }  // namespace sg
 

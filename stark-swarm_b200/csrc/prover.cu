@@ -191,13 +191,18 @@ void lde_commit(sg_ctx* c, const uint64_t* trace, bool host_trace, uint64_t w, u
     return;
   }
   ShiftTables sh(c, shift, s);
-  DBuf coef(w * n_trace, s);
+  const PowSpec* pre = sh.active ? &sh.spec : nullptr;
+  DBuf coef(w * n_trace, s), fscratch(lde_leaf_scratch_elems((uint32_t)w, ln), s);
   {
     DBuf scratch(ntt_scratch_elems(w, lt), s);
     if (!host_trace) {
       ntt(c, trace, coef.p, (uint32_t)w, n_trace, n_trace, lt, true, n_trace, scratch.p);
+      cuda_check(lde_leaf_prepasses(c->tw, coef.p, n_trace, (uint32_t)w, 0, (uint32_t)w, ln, n_trace, pre,
+                                    fscratch.p, s),
+                 "LDE passes");
     } else {
-      // column chunks of ~64 MB: chunk k's copy overlaps chunk k-1's inverse transform
+      // column chunks of ~64 MB: chunk k's copy overlaps chunk k-1's inverse
+      // transform and the passes before the fused one
       const uint64_t chunk = std::min<uint64_t>(w, std::max<uint64_t>(1, (uint64_t(8) << 20) / n_trace));
       const uint64_t n_chunks = (w + chunk - 1) / chunk;
       if (!c->copy_stream)
@@ -219,14 +224,17 @@ void lde_commit(sg_ctx* c, const uint64_t* trace, bool host_trace, uint64_t w, u
         cuda_check(cudaStreamWaitEvent(s, ev[k], 0), "wait");
         ntt(c, d_in.p + c0 * n_trace, coef.p + c0 * n_trace, (uint32_t)wk, n_trace, n_trace, lt, true, n_trace,
             scratch.p);
+        cuda_check(lde_leaf_prepasses(c->tw, coef.p, n_trace, (uint32_t)w, (uint32_t)c0, (uint32_t)wk, ln, n_trace,
+                                      pre, fscratch.p, s),
+                   "LDE passes");
       }
       cuda_check(cudaStreamSynchronize(s), "sync");  // the copies and transforms are done before d_in is freed
       for (auto& e : ev) cudaEventDestroy(e);
     }
   }
-  DBuf scratch(lde_leaf_scratch_elems((uint32_t)w, ln), s);
-  cuda_check(lde_leaf_transform(c->tw, coef.p, n_trace, (uint32_t)w, ln, n_trace, sh.active ? &sh.spec : nullptr,
-                                scratch.p, tree.arity0, tree.label, tree.d, d_keep, (uint32_t)keep_cols, s),
+  coef = DBuf();
+  cuda_check(lde_leaf_final(c->tw, (uint32_t)w, ln, fscratch.p, tree.arity0, tree.label, tree.d, d_keep,
+                            (uint32_t)keep_cols, s),
              "fused LDE and leaf hashing");
 }
 
