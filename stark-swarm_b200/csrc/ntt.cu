@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "counters.hpp"
@@ -112,14 +113,24 @@ __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int l
   const int log_g = log_m - LR;
   const int G = 1 << log_g;
   const int Ns = 1 << log_ns;
+  // Padded offsets as base + r * stride: when G (or Ns) is a multiple of 16,
+  // padi(j + r G) = padi(j) + r (G + G/16), so the R accesses of a group are one
+  // address and R immediate (or one-register) offsets.
+  const int gstride = G + (G >> 4);
   uint64_t v[V];
 #pragma unroll
   for (int q = 0; q < GPT; ++q) {
     int g = t + q * T;
     int l = g >> log_g, j = g & (G - 1);
     uint64_t* row = sm + l * Mp;
+    if (G % 16 == 0) {
+      const uint64_t* p = row + padi(j);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[q * R + r] = row[padi(j + r * G)];
+      for (int r = 0; r < R; ++r) v[q * R + r] = p[r * gstride];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q * R + r] = row[padi(j + r * G)];
+    }
   }
   __syncthreads();
 #pragma unroll
@@ -128,18 +139,30 @@ __device__ __forceinline__ void stockham_stage(uint64_t* sm, int t, int T, int l
     int l = g >> log_g, j = g & (G - 1);
     int k = j & (Ns - 1);
     if (log_ns > 0) {
-      const int sh = TWL - log_ns - LR;  // w_{Ns R}^{rk} = w_{2^TWL}^{rk 2^TWL/(Ns R)}
+      // w_{Ns R}^{rk} = w_{2^TWL}^{rk 2^TWL/(Ns R)}; r k < Ns R, so the index
+      // r (k << sh) stays below 2^TWL
+      const int kk = k << (TWL - log_ns - LR);
+      int ix = 0;
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        const int ix = ((r * k) << sh) & ((1 << TWL) - 1);
+        ix += kk;
         v[q * R + r] = gl::mul(v[q * R + r], TW_SM ? tw_st[ix] : __ldg(tw_st + ix));
       }
     }
     dft_reg<R, INV>(v + q * R);
     int idx = ((j >> log_ns) << (log_ns + LR)) + k;
     uint64_t* row = sm + l * Mp;
+    // stages run with Ns = 1 (idx a multiple of R, the R outputs in one padded
+    // 16-word block) or Ns >= 16 (every r Ns a multiple of 16)
+    if (log_ns == 0 || log_ns >= 4) {
+      uint64_t* p = row + padi(idx);
+      const int ostride = log_ns == 0 ? 1 : Ns + (Ns >> 4);
 #pragma unroll
-    for (int r = 0; r < R; ++r) row[padi(idx + r * Ns)] = v[q * R + r];
+      for (int r = 0; r < R; ++r) p[r * ostride] = v[q * R + r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) row[padi(idx + r * Ns)] = v[q * R + r];
+    }
   }
   __syncthreads();
 }
@@ -197,6 +220,9 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   constexpr int E = K * M;
   constexpr int T = E / V;  // blockDim.x (launch_pass); every thread owns V elements
   const int t = threadIdx.x;
+  // the launch has exactly T threads: with t < T known, the (lane, point) split of
+  // t + q T folds into per-thread constants plus compile-time offsets
+  __builtin_assume(t < T);
   const uint64_t lane0 = (uint64_t)blockIdx.x << LOG_K;
   const uint64_t y = (uint64_t)blockIdx.y + a.y_base;
   const uint64_t yc = y / a.y_sub, ys = y - yc * a.y_sub;
@@ -226,8 +252,9 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   // Global loads go out in batches of B before the batch's shared stores (a
   // generic load may not pass a shared store, so the split is explicit).
   constexpr int B = V < 8 ? V : 8;
-  auto in_pos = [&](int e, int& l, int& m) {
-    if (lane_fast_in) {
+  // element e of the tile -> (lane l, point m): lanes fastest or points fastest
+  auto in_pos = [&](auto lf_c, int e, int& l, int& m) {
+    if constexpr (decltype(lf_c)::value) {
       l = e & (K - 1);
       m = e >> LOG_K;
     } else {
@@ -235,40 +262,66 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       l = e >> LOG_M;
     }
   };
+  // The uniform choices (pre-multiplication, a tile with every lane valid and no
+  // zero padding) are taken once per CTA outside the element loops, so that each
+  // loop is straight-line code without per-element predicates or selects.
+  auto load_tile = [&](auto pre_c, auto full_c, auto lf_c) {
+    constexpr bool PRE = decltype(pre_c)::value, FULL = decltype(full_c)::value;
 #pragma unroll
-  for (int q0 = 0; q0 < V; q0 += B) {
-    uint64_t x[B];
+    for (int q0 = 0; q0 < V; q0 += B) {
+      uint64_t x[B];
 #pragma unroll
-    for (int q = 0; q < B; ++q) {
-      const int e = t + (q0 + q) * T;
-      int l, m;
-      in_pos(e, l, m);
-      const uint64_t lane = lane0 + l;
-      const uint64_t flat = (uint64_t)m * a.in_m + lane * a.flat_lane;
-      x[q] = 0;
-      if constexpr (COSET) {
-        // one column's cosets: point m of every lane is in[m], all lanes valid
-        // (ntt_coset_eval launches exactly B / K CTAs per column)
-        x[q] = __ldg(in + m);
-        if (a.pre.active()) x[q] = gl::mul(x[q], pow_at(a.pre, (uint64_t)m));
-        // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j)
-        const uint64_t ex = (uint64_t)m * lane;
-        x[q] = gl::mul(x[q], a.in_tw_log <= kTwSplit
-                                 ? __ldg(a.tw_hi + ((ex << (kTwSplit - a.in_tw_log)) & (kTwEntries - 1)))
-                                 : tw_pow(a.tw_lo, a.tw_hi, ex, a.in_tw_log));
-      } else if (e < E_load && lane < a.n_lanes && flat < a.in_valid) {
-        x[q] = __ldg(in + lane * a.in_lane + (uint64_t)m * a.in_m);
-        if (a.pre.active()) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
+      for (int q = 0; q < B; ++q) {
+        const int e = t + (q0 + q) * T;
+        int l, m;
+        in_pos(lf_c, e, l, m);
+        const uint64_t lane = lane0 + l;
+        x[q] = 0;
+        if constexpr (COSET) {
+          // one column's cosets: point m of every lane is in[m], all lanes valid
+          // (ntt_coset_eval launches exactly B / K CTAs per column)
+          x[q] = __ldg(in + m);
+          if (PRE) x[q] = gl::mul(x[q], pow_at(a.pre, (uint64_t)m));
+          // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j)
+          const uint64_t ex = (uint64_t)m * lane;
+          x[q] = gl::mul(x[q], a.in_tw_log <= kTwSplit
+                                   ? __ldg(a.tw_hi + ((ex << (kTwSplit - a.in_tw_log)) & (kTwEntries - 1)))
+                                   : tw_pow(a.tw_lo, a.tw_hi, ex, a.in_tw_log));
+        } else {
+          const uint64_t flat = (uint64_t)m * a.in_m + lane * a.flat_lane;
+          if (FULL || (e < E_load && lane < a.n_lanes && flat < a.in_valid)) {
+            x[q] = __ldg(in + lane * a.in_lane + (uint64_t)m * a.in_m);
+            if (PRE) x[q] = gl::mul(x[q], pow_at(a.pre, flat));
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < B; ++q) {
+        const int e = t + (q0 + q) * T;
+        int l, m;
+        in_pos(lf_c, e, l, m);
+        if (FULL || e < E_load) sm[l * Mp + padi(m)] = x[q];
       }
     }
-#pragma unroll
-    for (int q = 0; q < B; ++q) {
-      const int e = t + (q0 + q) * T;
-      int l, m;
-      in_pos(e, l, m);
-      if (e < E_load) sm[l * Mp + padi(m)] = x[q];
+  };
+  using yes = std::true_type;
+  using no = std::false_type;
+  auto load_dispatch = [&](auto lf_c) {
+    if (a.pre.active()) {
+      load_tile(yes{}, no{}, lf_c);
+    } else {
+      // largest flat index of the tile: point M-1 of its last lane
+      const uint64_t flat_max = (uint64_t)(M - 1) * a.in_m + (lane0 + K - 1) * a.flat_lane;
+      if (!COSET && E_load == E && lane0 + K <= a.n_lanes && flat_max < a.in_valid)
+        load_tile(no{}, yes{}, lf_c);
+      else
+        load_tile(no{}, no{}, lf_c);
     }
-  }
+  };
+  if (lane_fast_in)
+    load_dispatch(yes{});
+  else
+    load_dispatch(no{});
   __syncthreads();
 
   // Stage sequence: radix-16 stages, then one radix 2/4/8 stage for the remainder.
@@ -301,8 +354,8 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   }
 
   const bool lane_fast_out = a.out_lane == 1;
-  auto out_pos = [&](int e, int& l, int& i) {
-    if (lane_fast_out) {
+  auto out_pos = [&](auto lf_c, int e, int& l, int& i) {
+    if constexpr (decltype(lf_c)::value) {
       l = e & (K - 1);
       i = e >> LOG_K;
     } else {
@@ -310,40 +363,60 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
       l = e >> LOG_M;
     }
   };
-  // shared reads and pass-twiddle loads of a batch before its global stores
+  // shared reads and pass-twiddle loads of a batch before its global stores;
+  // the twiddle / scale choice is uniform and taken outside the loops
+  auto store_tile = [&](auto tw_c, auto sc_c, auto lf_c) {
+    constexpr bool TW = decltype(tw_c)::value, SC = decltype(sc_c)::value;
 #pragma unroll
-  for (int q0 = 0; q0 < V; q0 += B) {
-    uint64_t x[B];
+    for (int q0 = 0; q0 < V; q0 += B) {
+      uint64_t x[B];
 #pragma unroll
-    for (int q = 0; q < B; ++q) {
-      int l, i;
-      out_pos(t + (q0 + q) * T, l, i);
-      x[q] = sm[l * Mp + padi(i)];
-      if (a.tw_log > 0) {
-        uint64_t w;
-        if constexpr (PTW) {
-          w = gl::mul(ptw[l * PT_PER + (i & 63)], ptw[l * PT_PER + 64 + (i >> 6)]);
-        } else {
-          if (a.tw_tab)  // (a CTA's lanes past n_lanes store nothing and read no table entry)
-            w = lane0 + l < a.n_lanes ? __ldg(a.tw_tab + (uint64_t)i * a.n_lanes + lane0 + l) : 0;
-          else
-            w = tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log);
+      for (int q = 0; q < B; ++q) {
+        int l, i;
+        out_pos(lf_c, t + (q0 + q) * T, l, i);
+        x[q] = sm[l * Mp + padi(i)];
+        if constexpr (TW) {
+          uint64_t w;
+          if constexpr (PTW) {
+            w = gl::mul(ptw[l * PT_PER + (i & 63)], ptw[l * PT_PER + 64 + (i >> 6)]);
+          } else {
+            if (a.tw_tab)  // (a CTA's lanes past n_lanes store nothing and read no table entry)
+              w = lane0 + l < a.n_lanes ? __ldg(a.tw_tab + (uint64_t)i * a.n_lanes + lane0 + l) : 0;
+            else
+              w = tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log);
+          }
+          x[q] = gl::mul(x[q], w);
         }
-        x[q] = gl::mul(x[q], w);
+        if constexpr (SC) x[q] = gl::mul(x[q], a.scale);
       }
-      if (a.scale != 1) x[q] = gl::mul(x[q], a.scale);
-    }
 #pragma unroll
-    for (int q = 0; q < B; ++q) {
-      int l, i;
-      out_pos(t + (q0 + q) * T, l, i);
-      const uint64_t lane = lane0 + l;
-      if constexpr (COSET)
-        out[lane + ((uint64_t)i << a.out_i_log)] = x[q];  // point B i + t of the column
-      else if (lane < a.n_lanes)
-        out[lane * a.out_lane + (uint64_t)i * a.out_i] = x[q];
+      for (int q = 0; q < B; ++q) {
+        int l, i;
+        out_pos(lf_c, t + (q0 + q) * T, l, i);
+        const uint64_t lane = lane0 + l;
+        if constexpr (COSET)
+          out[lane + ((uint64_t)i << a.out_i_log)] = x[q];  // point B i + t of the column
+        else if (lane < a.n_lanes)
+          out[lane * a.out_lane + (uint64_t)i * a.out_i] = x[q];
+      }
     }
-  }
+  };
+  auto store_dispatch = [&](auto lf_c) {
+    if (a.tw_log > 0) {
+      if (a.scale != 1)
+        store_tile(yes{}, yes{}, lf_c);
+      else
+        store_tile(yes{}, no{}, lf_c);
+    } else if (a.scale != 1) {
+      store_tile(no{}, yes{}, lf_c);
+    } else {
+      store_tile(no{}, no{}, lf_c);
+    }
+  };
+  if (lane_fast_out)
+    store_dispatch(yes{});
+  else
+    store_dispatch(no{});
 }
 
 template <int LOG_M>
@@ -767,6 +840,7 @@ __global__ void __launch_bounds__(kFuseThreads, 1) lde_leaf_kernel(LeafFuse a) {
   extern __shared__ uint64_t sm[];
   uint64_t* stw = sm + kFuseTileLanes * kFuseMp;
   const int t = threadIdx.x;
+  __builtin_assume(t < kFuseThreads);
   const uint64_t lane0 = (uint64_t)blockIdx.x * kFuseLanes;
   for (int j = t; j < kFuseA; j += kFuseThreads) stw[j] = __ldg(a.tw_st + (j << (12 - kFuseLogA)));
   // this thread's row: lane hl, point hi1 (consecutive threads: consecutive points,

@@ -70,4 +70,4 @@ def test_lde_commit_edge_values_match_oracle(ctx):
     arities = [16, 16, 16, 8]
     root = ctx.lde_commit(tr, blowup, 7, arities, 0)
     assert root == ctx.merkle_commit(lde, arities, 0)
-    assert root == O.merkle_root(lde, arities, 0)
+    assert root == O.merkle_root(np.ascontiguousarray(lde.T), arities, 0)
