@@ -96,68 +96,99 @@ __device__ __forceinline__ uint64_t rotl_fma(uint64_t x) {
 #define KC_ROT_B(x, R) kc::rotl(x, R)
 #endif
 
-// One round on a register-resident state (theta, rho+pi, chi, iota). The rho
-// rotations of B2, B4, ..., B24 go through KC_ROT_B (see above).
-#define KC_ROUND(A, rc)                                                               \
-  {                                                                                   \
-    uint64_t C0 = A[0] ^ A[5] ^ A[10] ^ A[15] ^ A[20];                                \
-    uint64_t C1 = A[1] ^ A[6] ^ A[11] ^ A[16] ^ A[21];                                \
-    uint64_t C2 = A[2] ^ A[7] ^ A[12] ^ A[17] ^ A[22];                                \
-    uint64_t C3 = A[3] ^ A[8] ^ A[13] ^ A[18] ^ A[23];                                \
-    uint64_t C4 = A[4] ^ A[9] ^ A[14] ^ A[19] ^ A[24];                                \
-    uint64_t D0 = C4 ^ kc::rotl(C1, 1), D1 = C0 ^ kc::rotl(C2, 1);                    \
-    uint64_t D2 = C1 ^ kc::rotl(C3, 1), D3 = C2 ^ kc::rotl(C4, 1);                    \
-    uint64_t D4 = C3 ^ kc::rotl(C0, 1);                                               \
-    uint64_t B0 = A[0] ^ D0;                                                          \
-    uint64_t B1 = kc::rotl(A[6] ^ D1, 44);                                            \
-    uint64_t B2 = KC_ROT_B(A[12] ^ D2, 43);                                           \
-    uint64_t B3 = kc::rotl(A[18] ^ D3, 21);                                           \
-    uint64_t B4 = KC_ROT_B(A[24] ^ D4, 14);                                           \
-    uint64_t B5 = kc::rotl(A[3] ^ D3, 28);                                            \
-    uint64_t B6 = KC_ROT_B(A[9] ^ D4, 20);                                            \
-    uint64_t B7 = kc::rotl(A[10] ^ D0, 3);                                            \
-    uint64_t B8 = KC_ROT_B(A[16] ^ D1, 45);                                           \
-    uint64_t B9 = kc::rotl(A[22] ^ D2, 61);                                           \
-    uint64_t B10 = KC_ROT_B(A[1] ^ D1, 1);                                            \
-    uint64_t B11 = kc::rotl(A[7] ^ D2, 6);                                            \
-    uint64_t B12 = KC_ROT_B(A[13] ^ D3, 25);                                          \
-    uint64_t B13 = kc::rotl(A[19] ^ D4, 8);                                           \
-    uint64_t B14 = KC_ROT_B(A[20] ^ D0, 18);                                          \
-    uint64_t B15 = kc::rotl(A[4] ^ D4, 27);                                           \
-    uint64_t B16 = KC_ROT_B(A[5] ^ D0, 36);                                           \
-    uint64_t B17 = kc::rotl(A[11] ^ D1, 10);                                          \
-    uint64_t B18 = KC_ROT_B(A[17] ^ D2, 15);                                          \
-    uint64_t B19 = kc::rotl(A[23] ^ D3, 56);                                          \
-    uint64_t B20 = KC_ROT_B(A[2] ^ D2, 62);                                           \
-    uint64_t B21 = kc::rotl(A[8] ^ D3, 55);                                           \
-    uint64_t B22 = KC_ROT_B(A[14] ^ D4, 39);                                          \
-    uint64_t B23 = kc::rotl(A[15] ^ D0, 41);                                          \
-    uint64_t B24 = KC_ROT_B(A[21] ^ D1, 2);                                           \
-    A[0] = B0 ^ (~B1 & B2) ^ (rc);                                                    \
-    A[1] = B1 ^ (~B2 & B3);                                                           \
-    A[2] = B2 ^ (~B3 & B4);                                                           \
-    A[3] = B3 ^ (~B4 & B0);                                                           \
-    A[4] = B4 ^ (~B0 & B1);                                                           \
-    A[5] = B5 ^ (~B6 & B7);                                                           \
-    A[6] = B6 ^ (~B7 & B8);                                                           \
-    A[7] = B7 ^ (~B8 & B9);                                                           \
-    A[8] = B8 ^ (~B9 & B5);                                                           \
-    A[9] = B9 ^ (~B5 & B6);                                                           \
-    A[10] = B10 ^ (~B11 & B12);                                                       \
-    A[11] = B11 ^ (~B12 & B13);                                                       \
-    A[12] = B12 ^ (~B13 & B14);                                                       \
-    A[13] = B13 ^ (~B14 & B10);                                                       \
-    A[14] = B14 ^ (~B10 & B11);                                                       \
-    A[15] = B15 ^ (~B16 & B17);                                                       \
-    A[16] = B16 ^ (~B17 & B18);                                                       \
-    A[17] = B17 ^ (~B18 & B19);                                                       \
-    A[18] = B18 ^ (~B19 & B15);                                                       \
-    A[19] = B19 ^ (~B15 & B16);                                                       \
-    A[20] = B20 ^ (~B21 & B22);                                                       \
-    A[21] = B21 ^ (~B22 & B23);                                                       \
-    A[22] = B22 ^ (~B23 & B24);                                                       \
-    A[23] = B23 ^ (~B24 & B20);                                                       \
-    A[24] = B24 ^ (~B20 & B21);                                                       \
+// a ^ b ^ c. On the device each 32-bit half is one three-input LOP3, so theta's
+// "A[x][y] ^= C[x-1] ^ rot(C[x+1], 1)" costs one instruction per half and lane
+// (the two-step form, D[x] first, costs 10 more per round).
+KC_HD uint64_t xor3(uint64_t a, uint64_t b, uint64_t c) {
+#if defined(__CUDA_ARCH__)
+  uint32_t lo, hi;
+  asm("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(lo) : "r"((uint32_t)a), "r"((uint32_t)b), "r"((uint32_t)c));
+  asm("lop3.b32 %0, %1, %2, %3, 0x96;"
+      : "=r"(hi)
+      : "r"((uint32_t)(a >> 32)), "r"((uint32_t)(b >> 32)), "r"((uint32_t)(c >> 32)));
+  return (uint64_t)hi << 32 | lo;
+#else
+  return a ^ b ^ c;
+#endif
+}
+
+// a ^ (~b & c), Keccak's chi, as one LOP3 per 32-bit half on the device.
+KC_HD uint64_t chi(uint64_t a, uint64_t b, uint64_t c) {
+#if defined(__CUDA_ARCH__)
+  uint32_t lo, hi;
+  asm("lop3.b32 %0, %1, %2, %3, 0xD2;" : "=r"(lo) : "r"((uint32_t)a), "r"((uint32_t)b), "r"((uint32_t)c));
+  asm("lop3.b32 %0, %1, %2, %3, 0xD2;"
+      : "=r"(hi)
+      : "r"((uint32_t)(a >> 32)), "r"((uint32_t)(b >> 32)), "r"((uint32_t)(c >> 32)));
+  return (uint64_t)hi << 32 | lo;
+#else
+  return a ^ (~b & c);
+#endif
+}
+
+// One round on a register-resident state (theta, rho+pi, chi, iota). With
+// R[x] = rot(C[x], 1), theta's D[x] = C[x-1] ^ R[x+1] is folded into each lane's
+// update as xor3(A, C[x-1], R[x+1]). The rho rotations of B2, B4, ..., B24 go
+// through KC_ROT_B (see above).
+#define KC_ROUND(A, rc)                                                         \
+  {                                                                             \
+    uint64_t C0 = kc::xor3(kc::xor3(A[0], A[5], A[10]), A[15], A[20]);          \
+    uint64_t C1 = kc::xor3(kc::xor3(A[1], A[6], A[11]), A[16], A[21]);          \
+    uint64_t C2 = kc::xor3(kc::xor3(A[2], A[7], A[12]), A[17], A[22]);          \
+    uint64_t C3 = kc::xor3(kc::xor3(A[3], A[8], A[13]), A[18], A[23]);          \
+    uint64_t C4 = kc::xor3(kc::xor3(A[4], A[9], A[14]), A[19], A[24]);          \
+    uint64_t R0 = kc::rotl(C0, 1), R1 = kc::rotl(C1, 1), R2 = kc::rotl(C2, 1);  \
+    uint64_t R3 = kc::rotl(C3, 1), R4 = kc::rotl(C4, 1);                        \
+    uint64_t B0 = kc::xor3(A[0], C4, R1);                                       \
+    uint64_t B1 = kc::rotl(kc::xor3(A[6], C0, R2), 44);                         \
+    uint64_t B2 = KC_ROT_B(kc::xor3(A[12], C1, R3), 43);                        \
+    uint64_t B3 = kc::rotl(kc::xor3(A[18], C2, R4), 21);                        \
+    uint64_t B4 = KC_ROT_B(kc::xor3(A[24], C3, R0), 14);                        \
+    uint64_t B5 = kc::rotl(kc::xor3(A[3], C2, R4), 28);                         \
+    uint64_t B6 = KC_ROT_B(kc::xor3(A[9], C3, R0), 20);                         \
+    uint64_t B7 = kc::rotl(kc::xor3(A[10], C4, R1), 3);                         \
+    uint64_t B8 = KC_ROT_B(kc::xor3(A[16], C0, R2), 45);                        \
+    uint64_t B9 = kc::rotl(kc::xor3(A[22], C1, R3), 61);                        \
+    uint64_t B10 = KC_ROT_B(kc::xor3(A[1], C0, R2), 1);                         \
+    uint64_t B11 = kc::rotl(kc::xor3(A[7], C1, R3), 6);                         \
+    uint64_t B12 = KC_ROT_B(kc::xor3(A[13], C2, R4), 25);                       \
+    uint64_t B13 = kc::rotl(kc::xor3(A[19], C3, R0), 8);                        \
+    uint64_t B14 = KC_ROT_B(kc::xor3(A[20], C4, R1), 18);                       \
+    uint64_t B15 = kc::rotl(kc::xor3(A[4], C3, R0), 27);                        \
+    uint64_t B16 = KC_ROT_B(kc::xor3(A[5], C4, R1), 36);                        \
+    uint64_t B17 = kc::rotl(kc::xor3(A[11], C0, R2), 10);                       \
+    uint64_t B18 = KC_ROT_B(kc::xor3(A[17], C1, R3), 15);                       \
+    uint64_t B19 = kc::rotl(kc::xor3(A[23], C2, R4), 56);                       \
+    uint64_t B20 = KC_ROT_B(kc::xor3(A[2], C1, R3), 62);                        \
+    uint64_t B21 = kc::rotl(kc::xor3(A[8], C2, R4), 55);                        \
+    uint64_t B22 = KC_ROT_B(kc::xor3(A[14], C3, R0), 39);                       \
+    uint64_t B23 = kc::rotl(kc::xor3(A[15], C4, R1), 41);                       \
+    uint64_t B24 = KC_ROT_B(kc::xor3(A[21], C0, R2), 2);                        \
+    A[0] = kc::chi(B0, B1, B2) ^ (rc);                                          \
+    A[1] = kc::chi(B1, B2, B3);                                                 \
+    A[2] = kc::chi(B2, B3, B4);                                                 \
+    A[3] = kc::chi(B3, B4, B0);                                                 \
+    A[4] = kc::chi(B4, B0, B1);                                                 \
+    A[5] = kc::chi(B5, B6, B7);                                                 \
+    A[6] = kc::chi(B6, B7, B8);                                                 \
+    A[7] = kc::chi(B7, B8, B9);                                                 \
+    A[8] = kc::chi(B8, B9, B5);                                                 \
+    A[9] = kc::chi(B9, B5, B6);                                                 \
+    A[10] = kc::chi(B10, B11, B12);                                             \
+    A[11] = kc::chi(B11, B12, B13);                                             \
+    A[12] = kc::chi(B12, B13, B14);                                             \
+    A[13] = kc::chi(B13, B14, B10);                                             \
+    A[14] = kc::chi(B14, B10, B11);                                             \
+    A[15] = kc::chi(B15, B16, B17);                                             \
+    A[16] = kc::chi(B16, B17, B18);                                             \
+    A[17] = kc::chi(B17, B18, B19);                                             \
+    A[18] = kc::chi(B18, B19, B15);                                             \
+    A[19] = kc::chi(B19, B15, B16);                                             \
+    A[20] = kc::chi(B20, B21, B22);                                             \
+    A[21] = kc::chi(B21, B22, B23);                                             \
+    A[22] = kc::chi(B22, B23, B24);                                             \
+    A[23] = kc::chi(B23, B24, B20);                                             \
+    A[24] = kc::chi(B24, B20, B21);                                             \
   }
 
 KC_HD void keccak_f(uint64_t A[25]) {

@@ -94,6 +94,9 @@ struct PassArgs {
   int sparse_nz;
   int tw_log;                 // > 0: output (lane, i) *= w_{2^tw_log}^(i*lane)
   const uint64_t* tw_tab;     // if set, that twiddle is tw_tab[i * n_lanes + lane]
+  // grid x = grid row (column), y = lane group: the CTAs of one lane group run
+  // back to back over all columns, so they share its tw_tab entries through L2
+  bool cols_fast;
   int in_tw_log;              // > 0: input (lane, m) *= w_{2^in_tw_log}^(m*lane)
   int out_i_log;              // coset evaluation: out_i = 2^out_i_log
   uint64_t scale;             // != 1: outputs *= scale
@@ -223,8 +226,8 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   // the launch has exactly T threads: with t < T known, the (lane, point) split of
   // t + q T folds into per-thread constants plus compile-time offsets
   __builtin_assume(t < T);
-  const uint64_t lane0 = (uint64_t)blockIdx.x << LOG_K;
-  const uint64_t y = (uint64_t)blockIdx.y + a.y_base;
+  const uint64_t lane0 = (uint64_t)(a.cols_fast ? blockIdx.y : blockIdx.x) << LOG_K;
+  const uint64_t y = (uint64_t)(a.cols_fast ? blockIdx.x : blockIdx.y) + a.y_base;
   const uint64_t yc = y / a.y_sub, ys = y - yc * a.y_sub;
   const uint64_t* in = a.in + yc * a.in_col + ys * a.in_sub;
   uint64_t* out = a.out + yc * a.out_col + ys * a.out_sub;
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   if constexpr (STW)
     for (int j = t; j < M; j += T) stw[j] = __ldg(a.tw_st + (j << (12 - LOG_M)));
   if constexpr (PTW) {
-    if (a.tw_log > 0)
+    if (a.tw_log > 0 && !a.tw_tab)
       for (int x = t; x < K * PT_N; x += T) {
         const int l = x / PT_N, r = x - l * PT_N;
         const uint64_t lane = lane0 + l;
@@ -365,8 +368,8 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   };
   // shared reads and pass-twiddle loads of a batch before its global stores;
   // the twiddle / scale choice is uniform and taken outside the loops
-  auto store_tile = [&](auto tw_c, auto sc_c, auto lf_c) {
-    constexpr bool TW = decltype(tw_c)::value, SC = decltype(sc_c)::value;
+  auto store_tile = [&](auto tw_c, auto sc_c, auto lf_c, auto tab_c) {
+    constexpr bool TW = decltype(tw_c)::value, SC = decltype(sc_c)::value, TAB = decltype(tab_c)::value;
 #pragma unroll
     for (int q0 = 0; q0 < V; q0 += B) {
       uint64_t x[B];
@@ -377,10 +380,11 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
         x[q] = sm[l * Mp + padi(i)];
         if constexpr (TW) {
           uint64_t w;
-          if constexpr (PTW) {
+          if constexpr (PTW && !TAB) {
             w = gl::mul(ptw[l * PT_PER + (i & 63)], ptw[l * PT_PER + 64 + (i >> 6)]);
           } else {
-            if (a.tw_tab)  // (a CTA's lanes past n_lanes store nothing and read no table entry)
+            // (a CTA's lanes past n_lanes store nothing and read no table entry)
+            if (TAB || a.tw_tab)
               w = lane0 + l < a.n_lanes ? __ldg(a.tw_tab + (uint64_t)i * a.n_lanes + lane0 + l) : 0;
             else
               w = tw_pow(a.tw_lo, a.tw_hi, (uint64_t)i * (lane0 + l), a.tw_log);
@@ -404,13 +408,15 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
   auto store_dispatch = [&](auto lf_c) {
     if (a.tw_log > 0) {
       if (a.scale != 1)
-        store_tile(yes{}, yes{}, lf_c);
+        store_tile(yes{}, yes{}, lf_c, no{});
+      else if (PTW && a.tw_tab)  // (smaller passes take the table inside the one variant)
+        store_tile(yes{}, no{}, lf_c, yes{});
       else
-        store_tile(yes{}, no{}, lf_c);
+        store_tile(yes{}, no{}, lf_c, no{});
     } else if (a.scale != 1) {
-      store_tile(no{}, yes{}, lf_c);
+      store_tile(no{}, yes{}, lf_c, no{});
     } else {
-      store_tile(no{}, no{}, lf_c);
+      store_tile(no{}, no{}, lf_c, no{});
     }
   };
   if (lane_fast_out)
@@ -434,6 +440,15 @@ cudaError_t launch_pass(const PassArgs& a0, bool inv, uint64_t n_rows, cudaStrea
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+  }
+  if (a.cols_fast) {
+    // rows on grid x (up to 2^31 - 1), lane groups on grid y
+    if (blocks > 65535 || n_rows > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+    PassArgs b = a;
+    b.y_base = 0;
+    SG_LAUNCH_SCOPE("ntt_pass", s);
+    kern<<<dim3((unsigned)n_rows, (unsigned)blocks), T, smem, s>>>(b);
+    return cudaGetLastError();
   }
   for (uint64_t y0 = 0; y0 < n_rows; y0 += 65535) {
     const uint32_t ny = (uint32_t)(n_rows - y0 < 65535 ? n_rows - y0 : 65535);
@@ -525,6 +540,10 @@ __global__ void pow_table_kernel(const uint64_t* lo, const uint64_t* hi, uint64_
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < len; k += (uint64_t)gridDim.x * blockDim.x)
     tab[k] = tw_pow(lo, hi, k * mult, log_n);
 }
+
+// columns from which a 2^11 / 2^12 first pass reads its twiddles from the
+// per-size table (shared through L2) instead of building per-CTA factors
+constexpr uint32_t kPassTabMinCols = 8;
 
 int sparse_nz_for(uint64_t n_valid, uint64_t N, uint64_t n_lo, uint64_t M) {
   if (n_valid >= N || M < 16) return 0;  // dense, or a pass without a radix-16 first stage
@@ -721,8 +740,14 @@ cudaError_t ntt_batch(const NttTables& t, const uint64_t* in, uint64_t* out, uin
     a.in_valid = n_valid;
     a.sparse_nz = sparse_nz_for(n_valid, N, N1, N2);
     a.tw_log = log_n;
-    // passes of 2^11 and 2^12 build their twiddle factors in shared memory instead
-    if (t.pass_tables && !pass_tw_in_smem(l2)) a.tw_tab = pass_twiddle_table(t, log_n, l1, inverse, s);
+    // Passes of 2^11 and 2^12 build their twiddle factors in shared memory, unless
+    // enough columns share the table: then the CTAs of one lane group run over all
+    // columns back to back and read its entries from L2 (one load and one product
+    // per element instead of two shared loads and two products).
+    if (t.pass_tables && (!pass_tw_in_smem(l2) || n_cols >= kPassTabMinCols)) {
+      a.tw_tab = pass_twiddle_table(t, log_n, l1, inverse, s);
+      a.cols_fast = a.tw_tab && pass_tw_in_smem(l2) && (N1 >> pass_log_k(l2)) <= 65535;
+    }
     a.pre = pre ? *pre : none;
     cudaError_t e = launch_pass_dyn(l2, a, inverse, n_cols, s);
     if (e != cudaSuccess) return e;
