@@ -139,14 +139,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# DRAM bytes (read + write) per step of each kernel family on this workload (64
-# columns): one ncu capture of dram__bytes_read.sum + dram__bytes_write.sum over
-# the 16 ntt_pass launches of one step (a single-pass metric set).
-MEASURED_TRAFFIC_PER_STEP = {"ntt_pass": 15.711e9}
-# From ncu summaries of the same kernels on the reduced (4-column, 2^20 -> 2^23) case,
-# scaled to 64 columns by the columns processed: ALU-pipe share of active cycles
-# (the integer roofline of these kernels) and DRAM bytes per 64-column LDE.
-MEASURED_NTT = {}
+# Integer-pipe roofline and DRAM traffic of the dominant kernels, from ncu on the
+# reduced case (4 columns, 2^20 -> 2^23; 256 MiB LDE, larger than L2), scaled to 64
+# columns by the columns processed. int_frac = ALU-pipe instructions issued / peak
+# over the kernel's active cycles (sm__inst_executed_pipe_alu.avg.pct_of_peak_
+# sustained_active): these kernels are bound by integer issue, not by HBM.
+#   ntt_pass <12,fwd> 500.6 us: ALU 64.2 %, DRAM 0.498 TB/s -> 249 MB per 4 columns
+#   ntt_pass <11,fwd> 386.1 us: ALU 64.2 %, DRAM 1.275 TB/s -> 492 MB per 4 columns
+#   ntt_pass <10,inv> x 2 (trace iNTT, 16-column capture): 471 MB per 16 columns
+#   leaf_kernel_t<64> (2^20 rows of 64 columns) 1.489 ms: ALU 83.2 %
+_LDE_TRAFFIC = (249e6 + 492e6) * 16 + 471e6 * 4  # bytes per 64-column LDE (4 launches)
+MEASURED_NTT = {
+    "ntt_pass": {"int_frac": 0.642, "int_metric": "ALU-pipe share of active cycles (ncu, 4-column case)",
+                 "traffic_per_lde": _LDE_TRAFFIC},
+    "merkle_leaves": {"int_frac": 0.832, "int_metric": "ALU-pipe share of active cycles (ncu, 2^20 x 64 leaves)"},
+}
+# DRAM bytes per step of the ntt_pass family: the LDE's (above) plus the STIR
+# proof's transforms, taken at their algorithmic bytes times the LDE's
+# measured/algorithmic ratio (their own traffic was not captured).
+MEASURED_TRAFFIC_PER_STEP = {"ntt_pass": _LDE_TRAFFIC * (1 + 0.249e9 / 4.832e9)}
 
 
 def run_config(ws):
@@ -778,6 +789,19 @@ def main():
     prof_lde = sg.profile_read()
     lde_ms = dist_max(e0.elapsed_time(e1), ws) / args.steps
 
+    # Merkle commitment of the LDE rows alone (the leaf kernel without the STIR
+    # proof beside it): algorithmic bytes = read the LDE once + write the digests
+    sg.profile_reset()
+    sg.profile_enable(True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.merkle_commit(d_lde, ARITIES, TREE_LABEL)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sg.profile_enable(False)
+    prof_commit = sg.profile_read()
+    commit_ms = dist_max(e0.elapsed_time(e1), ws) / args.steps
+
     # roofline of the dominant kernel family (CUDA events recorded on the launching stream)
     peaks = {}
     try:
@@ -810,12 +834,19 @@ def main():
     roofline_ntt = roof("ntt_pass", prof_lde, args.steps, (W * N + W * N0) * 8, ntt_extra)
     if roofline_ntt and W == 64 and "traffic_per_lde" in ntt_extra:
         roofline_ntt["traffic"] = ntt_extra["traffic_per_lde"] / roofline_ntt["launches_per_step"]
+    leaf_perms = N0 * ((4 + W) // 17 + 1)  # Keccak-f per commitment: 4 + W lanes at 17 per block, then the pad
+    roofline_leaves = None
+    if "merkle_leaves" in prof_commit:
+        n_l, ms = prof_commit["merkle_leaves"]
+        roofline_leaves = roof("merkle_leaves", prof_commit, args.steps, W * N0 * 8 + N0 * 32,
+                               {"keccak_f_per_s": leaf_perms * n_l / args.steps / (ms / 1e3)})
+        if W == 64:
+            roofline_leaves.update(MEASURED_NTT["merkle_leaves"])
     # the dominant family of the timed step
     roofline = None
     if fused and "lde_leaf" in prof:
         # reads the last pass's input once, writes one digest per row; 5 Keccak-f per
         # 64-column row (4 + 64 lanes absorbed at 17 per block, then the pad block)
-        leaf_perms = N0 * ((4 + W) // 17 + 1)
         n_l, ms = prof["lde_leaf"]
         roofline = roof("lde_leaf", prof, args.steps, W * N0 * 8 + N0 * 32,
                         {"keccak_f_per_s": leaf_perms * n_l / args.steps / (ms / 1e3)})
@@ -827,6 +858,8 @@ def main():
         roofline = roof(fam, prof, args.steps, alg.get(fam, 0))
         if roofline and fam in MEASURED_TRAFFIC_PER_STEP and W == 64:
             roofline["traffic"] = MEASURED_TRAFFIC_PER_STEP[fam] / roofline["launches_per_step"]
+        if roofline and fam in MEASURED_NTT and W == 64:
+            roofline.update({k: v for k, v in MEASURED_NTT[fam].items() if k.startswith("int_")})
     kernels = {k: {"launches_per_step": v[0] / args.steps, "ms_per_step": v[1] / args.steps} for k, v in prof.items()}
 
     # The sections below characterise one GPU; with N > 1 ranks (the weak-scaling
@@ -911,6 +944,8 @@ def main():
             "pipelines_ms_per_step": {args.pipeline: ms_step, ("split" if fused else "fused"): other_ms},
             "pipelines_e2e_proofs_per_s": {args.pipeline: e2e_value, ("split" if fused else "fused"): other_e2e_value},
             "roofline_ntt_pass": roofline_ntt,
+            "commit_ms": commit_ms,
+            "roofline_merkle_leaves": roofline_leaves,
             "e2e": {"value": e2e_value, "unit": "proofs/s", "h2d_bytes_per_step": W * N * 8 + (N * 8 if fused else 0),
                     "d2h_bytes_per_step": 32 + len(ref[1])},
             "gpu_launches": launches_total,  # this library's kernels in the timed region
