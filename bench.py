@@ -839,7 +839,7 @@ def main():
     if "merkle_leaves" in prof_commit:
         n_l, ms = prof_commit["merkle_leaves"]
         roofline_leaves = roof("merkle_leaves", prof_commit, args.steps, W * N0 * 8 + N0 * 32,
-                               {"keccak_f_per_s": leaf_perms * n_l / args.steps / (ms / 1e3)})
+                               {"keccak_f_per_s": leaf_perms * n_l / (ms / 1e3)})
         if W == 64:
             roofline_leaves.update(MEASURED_NTT["merkle_leaves"])
     # the dominant family of the timed step
@@ -849,7 +849,7 @@ def main():
         # 64-column row (4 + 64 lanes absorbed at 17 per block, then the pad block)
         n_l, ms = prof["lde_leaf"]
         roofline = roof("lde_leaf", prof, args.steps, W * N0 * 8 + N0 * 32,
-                        {"keccak_f_per_s": leaf_perms * n_l / args.steps / (ms / 1e3)})
+                        {"keccak_f_per_s": leaf_perms * n_l / (ms / 1e3)})
         if W == 64 and "lde_leaf" in MEASURED_NTT:
             roofline.update(MEASURED_NTT["lde_leaf"])
     elif prof:
