@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "air.hpp"
+#include "ed25519_air.hpp"
 #include "p256_air.hpp"
 #include "rsa2048_air.hpp"
 #include "chacha.hpp"
@@ -1363,6 +1364,70 @@ int orc_prove_p256(const uint64_t* trace, size_t width, const uint64_t* table, s
   if (orc_merge_p256(lde.data(), width, table, n_gadgets, tail, n_trace, blowup, c.data()) != 0) return -2;
   orc_fri_params p;
   orc_build_params(n0, pi, 1, &p);
+  return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
+}
+
+// ------------------------------------------------------------------ Ed25519 verify AIR v16
+int orc_ed25519_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, const uint64_t* recs, size_t n_recs,
+                     const uint64_t* pairs, size_t n_pairs, uint64_t* out) {
+  (void)n_pairs;
+  return (int)ed25519::eval_row((const Fp*)cur, (const Fp*)nxt, row, recs, n_recs, pairs, (Fp*)out);
+}
+
+// deep_ali_merge_ed25519_verify(_streaming) (lib.rs:707-974): trace row i / blowup,
+// next row (i + blowup) mod n, lambda_j = j + 1, then iFFT, poly_div_zh, FFT.
+int orc_merge_ed25519(const uint64_t* lde, size_t width, const uint64_t* recs, size_t n_recs, const uint64_t* pairs,
+                      size_t n_pairs, size_t n_constraints, size_t n_trace, size_t blowup, uint64_t* c_eval) {
+  if (n_trace == 0 || (n_trace & (n_trace - 1)) || blowup == 0 || (blowup & (blowup - 1))) return -2;
+  const size_t n = n_trace * blowup, k = n_constraints;
+  const Fp* L = (const Fp*)lde;
+  std::vector<Fp> phi(n);
+  int bad = 0;
+#pragma omp parallel
+  {
+    std::vector<Fp> cur(width), nxt(width), cv(k);
+#pragma omp for schedule(dynamic, 4)
+    for (long i = 0; i < (long)n; ++i) {
+      const size_t ni = (i + blowup) % n;
+      for (size_t c = 0; c < width; ++c) {
+        cur[c] = L[c * n + i];
+        nxt[c] = L[c * n + ni];
+      }
+      if (orc_ed25519_eval((const uint64_t*)cur.data(), (const uint64_t*)nxt.data(), i / blowup, recs, n_recs, pairs,
+                           n_pairs, (uint64_t*)cv.data()) != (int)k) {
+#pragma omp atomic write
+        bad = 1;
+      }
+      Fp acc;
+      for (size_t j = 0; j < k; ++j)
+        if (!cv[j].is_zero()) acc = acc + Fp(j + 1) * cv[j];
+      phi[i] = acc;
+    }
+  }
+  if (bad) return -3;
+  ifft(phi.data(), n);
+  std::vector<Fp> q = poly_div_zh(phi, n_trace);
+  q.resize(n);
+  fft(q.data(), n);
+  memcpy(c_eval, q.data(), n * 8);
+  return 0;
+}
+
+// prove_zsk_ksk_binding_v2 (swarm-dns/src/prover.rs:856-951): trace -> LDE (shift 1)
+// -> merge -> STIR with build_params(n0, fs_binding).
+int orc_prove_ed25519(const uint64_t* trace, size_t width, const uint64_t* recs, size_t n_recs,
+                      const uint64_t* pairs, size_t n_pairs, size_t n_constraints, size_t n_trace,
+                      const uint8_t fs_binding[32], size_t blowup, uint8_t* out, size_t cap, size_t* out_len) {
+  if (blowup < 2 || (blowup & (blowup - 1))) return -2;
+  const size_t n0 = n_trace * blowup;
+  std::vector<uint64_t> lde(width * n0), c(n0);
+  if (orc_lde(trace, width, n_trace, blowup, 1, lde.data()) != 0) return -2;
+  const int rc = orc_merge_ed25519(lde.data(), width, recs, n_recs, pairs, n_pairs, n_constraints, n_trace, blowup,
+                                   c.data());
+  if (rc != 0) return rc;
+  std::vector<uint64_t>().swap(lde);
+  orc_fri_params p;
+  orc_build_params(n0, fs_binding, 1, &p);
   return orc_stir_prove(c.data(), n0, &p, out, cap, out_len);
 }
 

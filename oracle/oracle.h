@@ -103,6 +103,16 @@ int orc_merge_p256(const uint64_t* lde, size_t width, const uint64_t* table, siz
 int orc_prove_p256(const uint64_t* trace, size_t width, const uint64_t* table, size_t n_gadgets,
                    const uint64_t* tail, size_t n_trace, const uint8_t pi[32], size_t blowup, uint8_t* out,
                    size_t cap, size_t* out_len);
+/* Ed25519 verify AIR v16 (ed25519_verify_air.rs): the row's constraint vector is a
+ * program of 16-u64 block records (row gate, kind, cell bases) plus a table of
+ * A - B pairs (see ed25519_air.hpp); n_constraints is its length. */
+int orc_ed25519_eval(const uint64_t* cur, const uint64_t* nxt, size_t row, const uint64_t* recs, size_t n_recs,
+                     const uint64_t* pairs, size_t n_pairs, uint64_t* out);
+int orc_merge_ed25519(const uint64_t* lde, size_t width, const uint64_t* recs, size_t n_recs, const uint64_t* pairs,
+                      size_t n_pairs, size_t n_constraints, size_t n_trace, size_t blowup, uint64_t* c_eval);
+int orc_prove_ed25519(const uint64_t* trace, size_t width, const uint64_t* recs, size_t n_recs,
+                      const uint64_t* pairs, size_t n_pairs, size_t n_constraints, size_t n_trace,
+                      const uint8_t fs_binding[32], size_t blowup, uint8_t* out, size_t cap, size_t* out_len);
 void orc_build_params(size_t n0, const uint8_t pi[32], int stir, orc_fri_params* out);
 int orc_stir_prove(const uint64_t* f0, size_t n0, const orc_fri_params* p, uint8_t* out, size_t cap, size_t* len);
 int orc_stir_verify(const uint8_t* proof, size_t len, const orc_fri_params* p);

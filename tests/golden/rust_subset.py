@@ -1,8 +1,9 @@
 """An interpreter for the subset of Rust that the reference's AIR source files use.
 
 Fixture generation only (tests/golden/make_air_vectors.py): it parses the
-reference's `.rs` files (free functions, constants, structs; no traits or
-impl blocks) and evaluates their constraint evaluators on seeded inputs, so
+reference's `.rs` files (free functions, constants, structs, inherent `impl`
+blocks and `Lazy` statics; trait impls are skipped) and evaluates their
+constraint evaluators and layout builders on seeded inputs, so
 that the golden vectors come from the reference's own code rather than from a
 restatement of it. Nothing at test time imports this module.
 
@@ -132,12 +133,14 @@ class Ret(Exception):
 
 
 class Brk(Exception):
-    def __init__(self, v=None):
+    def __init__(self, v=None, label=None):
         self.v = v
+        self.label = label
 
 
 class Cont(Exception):
-    pass
+    def __init__(self, label=None):
+        self.label = label
 
 
 # ---------------------------------------------------------------- lexer
@@ -212,6 +215,7 @@ class Parser:
         self.t = toks
         self.i = 0
         self.macros = {}
+        self._impl_type = None
 
     # -- token helpers
     def peek(self, k=0):
@@ -277,6 +281,12 @@ class Parser:
                     break
                 depth -= 1
             elif v == ">>":
+                if depth == 1:
+                    # closes this generic and the enclosing one: split the token
+                    self.t[self.i:self.i + 1] = [("op", ">"), ("op", ">")]
+                    depth -= 1
+                    self.next()
+                    continue
                 if depth < 2:
                     break
                 depth -= 2
@@ -320,9 +330,13 @@ class Parser:
         tk = self.peek()
         v = tk[1]
         if v == "use" or v == "extern":
+            toks = []
             while not self.at(";"):
-                self.next()
+                toks.append(self.next())
             self.next()
+            for j in range(1, len(toks) - 1):  # `use path::{X as Y}`: Y names X
+                if toks[j][1] == "as" and toks[j - 1][0] == "id" and toks[j + 1][0] == "id":
+                    env.aliases[toks[j + 1][1]] = toks[j - 1][1]
         elif v == "mod":
             self.next()
             self.ident()
@@ -360,10 +374,17 @@ class Parser:
             self.expect("(")
             params = []
             while not self.at(")"):
-                pat = self.parse_pattern()
-                self.expect(":")
-                ty = self.parse_type({",", ")"})
-                params.append((pat, ty))
+                j = 0
+                while self.peek(j)[1] in ("&", "mut"):
+                    j += 1
+                if self.peek(j)[1] == "self" and self.peek(j + 1)[1] in (",", ")"):
+                    self.i += j + 1
+                    params.append((("pid", "self"), None))
+                else:
+                    pat = self.parse_pattern()
+                    self.expect(":")
+                    ty = self.parse_type({",", ")"})
+                    params.append((pat, ty))
                 if self.at(","):
                     self.next()
             self.expect(")")
@@ -394,14 +415,41 @@ class Parser:
                     self.next()
             else:
                 self.skip_balanced()
-        elif v in ("impl", "trait"):
+        elif v == "trait":
             self.next()
             while not self.at("{"):
                 self.next()
             self.skip_balanced()
+        elif v == "impl":
+            # inherent impl: its functions are registered as "Type::name"; trait impls are skipped
+            self.next()
+            if self.at("<"):
+                self.next()
+                self.parse_type({">"})
+                self.expect(">")
+            head = []
+            while not self.at("{"):
+                head.append(self.next())
+            if skip or any(t[1] == "for" for t in head):
+                self.skip_balanced()
+            else:
+                tname = head[0][1]
+                self.expect("{")
+                sub = Module()
+                old = self._impl_type
+                self._impl_type = tname
+                try:
+                    self.parse_items(sub, until_brace=True)
+                finally:
+                    self._impl_type = old
+                self.expect("}")
+                for fname, f in sub.fns.items():
+                    env.fns[f"{tname}::{fname}"] = f[:4] + (tname,)
+                for cname, c in sub.consts.items():
+                    env.consts[f"{tname}::{cname}"] = c
         elif v == "type":
             while not self.at(";"):
-                self.next()
+                self.skip_balanced()
             self.next()
         elif v == "macro_rules":
             self.next()
@@ -544,6 +592,11 @@ class Parser:
             self.next()
             self.parse_macro_rules()
             return None, False
+        if self.peek()[0] == "life" and self.at(":", 1):
+            e = self.parse_primary()
+            if self.at(";"):
+                self.next()
+            return ("expr", e), False
         if self.peek()[1] in ("if", "for", "while", "loop", "match", "unsafe", "{") and self.peek()[0] in ("id", "op"):
             # a block-like expression in statement position ends at its closing brace
             e = self.parse_primary()
@@ -711,6 +764,14 @@ class Parser:
     def parse_primary(self):
         tk = self.peek()
         k, v = tk
+        if k == "life" and self.at(":", 1):
+            label = v
+            self.next()
+            self.next()
+            e = self.parse_primary()
+            if e[0] not in ("for", "while", "loop"):
+                raise RustError(f"label on {e[0]}")
+            return ("label", label, e)
         if k == "num":
             self.next()
             return ("lit", v)
@@ -808,12 +869,14 @@ class Parser:
                 return ("return", self.parse_expr())
             if v == "break":
                 self.next()
+                label = self.next()[1] if self.peek()[0] == "life" else None
                 if self.at(";") or self.at("}"):
-                    return ("break", None)
-                return ("break", self.parse_expr())
+                    return ("break", None, label)
+                return ("break", self.parse_expr(), label)
             if v == "continue":
                 self.next()
-                return ("continue",)
+                label = self.next()[1] if self.peek()[0] == "life" else None
+                return ("continue", label)
             if v in ("true", "false"):
                 self.next()
                 return ("lit", v == "true")
@@ -980,6 +1043,7 @@ class Module:
     def __init__(self):
         self.fns = {}
         self.consts = {}
+        self.aliases = {}
         self.local_items = self
 
 
@@ -1051,10 +1115,12 @@ class Interp:
         return v
 
     def call_fn(self, f, args):
-        _, name, params, body = f
+        _, name, params, body = f[:4]
         if len(params) != len(args):
             raise RustError(f"{name}: {len(args)} args for {len(params)} params")
         sc = Scope()
+        if len(f) > 4:
+            sc.vars["Self"] = ("type", f[4])
         for (pat, ty), a in zip(params, args):
             self.bind(pat, a, sc)
         try:
@@ -1196,6 +1262,7 @@ class Interp:
             s = sc.lookup(name)
             if s is not None:
                 return s.vars[name]
+        name = self.mod.aliases.get(name, name)
         if name in self.mod.consts:
             return self.const(name)
         if name in self.mod.fns:
@@ -1212,8 +1279,17 @@ class Interp:
             return None
         raise RustError(f"unknown name {'::'.join(path)}")
 
+    def _self_type(self, name, sc):
+        if name == "Self":
+            s2 = sc.lookup("Self")
+            if s2 is None:
+                raise RustError("Self outside an impl")
+            return s2.vars["Self"][1]
+        return name
+
     def e_struct(self, e, sc):
         _, name, fields, base = e
+        name = self._self_type(name, sc)
         d = {}
         if base is not None:
             b = self.eval(base, sc)
@@ -1273,7 +1349,7 @@ class Interp:
             if isinstance(v, bool):
                 return not v
             return ~v & U64
-        return v  # deref
+        return _clone(v)  # deref: `let mut x = *fe;` copies (arrays and Copy structs)
 
     def e_bin(self, e, sc):
         op = e[1]
@@ -1354,46 +1430,62 @@ class Interp:
             return list(v)
         raise RustError(f"cannot iterate {type(v).__name__}")
 
-    def e_for(self, e, sc):
+    def e_label(self, e, sc):
+        inner = e[2]
+        return getattr(self, "e_" + inner[0])(inner, sc, e[1])
+
+    def e_for(self, e, sc, label=None):
         _, pat, it, body = e
         for x in self._iter(self.eval(it, sc)):
             inner = Scope(sc)
             self.bind(pat, x, inner)
             try:
                 self.eval(body, inner)
-            except Cont:
-                continue
-            except Brk:
-                break
+            except Cont as c:
+                if c.label is None or c.label == label:
+                    continue
+                raise
+            except Brk as b:
+                if b.label is None or b.label == label:
+                    break
+                raise
         return ()
 
-    def e_while(self, e, sc):
+    def e_while(self, e, sc, label=None):
         while self.eval(e[1], sc):
             try:
                 self.eval(e[2], sc)
-            except Cont:
-                continue
-            except Brk:
-                break
+            except Cont as c:
+                if c.label is None or c.label == label:
+                    continue
+                raise
+            except Brk as b:
+                if b.label is None or b.label == label:
+                    break
+                raise
         return ()
 
-    def e_loop(self, e, sc):
+    def e_loop(self, e, sc, label=None):
         while True:
             try:
                 self.eval(e[1], sc)
-            except Cont:
-                continue
+            except Cont as c:
+                if c.label is None or c.label == label:
+                    continue
+                raise
             except Brk as b:
-                return b.v
+                if b.label is None or b.label == label:
+                    return b.v
+                raise
 
     def e_return(self, e, sc):
         raise Ret(self.eval(e[1], sc) if e[1] is not None else ())
 
     def e_break(self, e, sc):
-        raise Brk(self.eval(e[1], sc) if e[1] is not None else None)
+        raise Brk(self.eval(e[1], sc) if e[1] is not None else None, e[2] if len(e) > 2 else None)
 
     def e_continue(self, e, sc):
-        raise Cont()
+        raise Cont(e[1] if len(e) > 1 else None)
 
     def e_try(self, e, sc):
         v = self.eval(e[1], sc)
@@ -1426,6 +1518,12 @@ class Interp:
                 s = sc.lookup(name)
                 if s is not None:
                     return s.vars[name](*args)
+            if len(path) >= 2:
+                key = f"{self._self_type(path[-2], sc)}::{name}"
+                if key in self.builtins:
+                    return self.builtins[key](*args)
+                if key in self.mod.fns:
+                    return self.call_fn(self.mod.fns[key], args)
             if name in self.mod.fns and (len(path) == 1 or path[-2] not in ("F", "Vec", "std", "core", "cmp")):
                 return self.call_fn(self.mod.fns[name], args)
             if name == "Some" or name == "Ok":
@@ -1434,9 +1532,28 @@ class Interp:
         return f(*args)
 
     def e_mcall(self, e, sc):
-        recv = self.eval(e[1], sc)
         name = e[2]
+        if name == "copy_from_slice" and e[1][0] == "index":
+            # dst[a..b].copy_from_slice(src) writes through to dst
+            arr = dv(self.eval(e[1][1], sc))
+            i = self.eval(e[1][2], sc)
+            src = list(dv(self.eval(e[3][0], sc)))
+            if isinstance(i, RRange):
+                lo = 0 if i.lo is None else i.lo
+                hi = len(arr) if i.hi is None else (i.hi + 1 if i.inclusive else i.hi)
+                if hi - lo != len(src):
+                    raise RustError("copy_from_slice length mismatch")
+                arr[lo:hi] = src
+                return ()
+        recv = self.eval(e[1], sc)
         args = [self.eval(a, sc) for a in e[3]]
+        r = dv(recv)
+        if isinstance(r, Struct):
+            key = f"{r._name}::{name}"
+            if key in self.builtins:
+                return self.builtins[key](r, *args)
+            if key in self.mod.fns:
+                return self.call_fn(self.mod.fns[key], [r] + args)
         return method(recv, name, args)
 
 
@@ -1504,7 +1621,22 @@ def _f_from(x):
     return Fe(x)
 
 
+def _from_le(bs):
+    bs = list(bs)
+    return sum(int(b) << (8 * i) for i, b in enumerate(bs))
+
+
+def _from_be(bs):
+    bs = list(bs)
+    return sum(int(b) << (8 * (len(bs) - 1 - i)) for i, b in enumerate(bs))
+
+
 BUILTIN_PATHS = {
+    "Lazy::new": lambda f: f(),
+    "u64::from_le_bytes": _from_le,
+    "u64::from_be_bytes": _from_be,
+    "u32::from_le_bytes": _from_le,
+    "u32::from_be_bytes": _from_be,
     "F::one": lambda: Fe(1),
     "F::zero": lambda: Fe(0),
     "F::from": _f_from,
@@ -1590,12 +1722,23 @@ def method(recv, name, args):
             return n
         if name == "abs":
             return abs(recv)
+        if name == "rem_euclid":
+            return recv % abs(args[0])
+        if name == "div_euclid":
+            q = recv // abs(args[0])
+            return q if args[0] > 0 else -q
+        if name == "to_le_bytes":
+            return [(recv >> (8 * i)) & 0xFF for i in range(8)]
+        if name == "to_be_bytes":
+            return [(recv >> (8 * (7 - i))) & 0xFF for i in range(8)]
         if name in ("clone",):
             return recv
         raise RustError(f"int.{name}")
     if isinstance(recv, Struct):
         if name == "clone":
             return recv.clone()
+        if name in ("unwrap", "expect"):
+            return recv
         raise RustError(f"struct.{name}")
     if isinstance(recv, tuple):
         recv = list(recv)
@@ -1670,7 +1813,7 @@ def method(recv, name, args):
             return [recv[i:i + k] for i in range(0, len(recv), k)]
         if name == "contains":
             return args[0] in recv
-        if name == "unwrap" or name == "expect":
+        if name in ("unwrap", "expect", "try_into"):
             return recv
         if name == "get":
             i = args[0]

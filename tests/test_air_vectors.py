@@ -18,6 +18,7 @@ import os
 import numpy as np
 import pytest
 
+import oracle_ed25519 as OE
 import oracle_lib as O
 import oracle_p256 as E
 import oracle_rsa as ORSA
@@ -75,9 +76,46 @@ def test_p256_ecdsa_evaluator_matches_reference(case):
     check(E.eval_row(lay, cur, nxt, case["row"], case["n_trace"]), case)
 
 
+_ED_PROGRAMS = {}
+
+
+def _ed25519_program(li):
+    """the oracle's layout and constraint program for the fixture's li-th signature"""
+    if li not in _ED_PROGRAMS:
+        L = FIX["airs"]["ed25519"]["layouts"][li]
+        seed = hashlib.sha256(L["key_tag"].encode()).digest()
+        msg = bytes.fromhex(L["msg_hex"])
+        _, _, pub = OE.keypair(seed)
+        sig = OE.sign(seed, msg)
+        _ED_PROGRAMS[li] = OE.layout_program(pub, sig, msg, L["k_scalar"])[:2]
+    return _ED_PROGRAMS[li]
+
+
+@pytest.mark.parametrize("li", range(len(FIX["airs"]["ed25519"]["layouts"])))
+def test_ed25519_layout_matches_reference(li):
+    L = FIX["airs"]["ed25519"]["layouts"][li]
+    lay, pr = _ed25519_program(li)
+    assert (lay.width, lay.height, pr.n) == (L["width"], L["height"], L["constraints"])
+    assert pr.n == OE.n_constraints(L["k_scalar"])
+    rows = L["rows"]
+    assert (lay.k_hash, lay.reduce_row, lay.decomp_R_row, lay.decomp_A_row) == (
+        rows["k_hash"], rows["reduce_row"], rows["decompress_R_row"], rows["decompress_A_row"])
+    assert (lay.sB_first, lay.kA_first, lay.residual_row, lay.result_row) == (
+        rows["sB_first_row"], rows["kA_first_row"], rows["residual_row"], rows["result_row"])
+    assert lay.dbl_rows == (rows["dbl_1_row"], rows["dbl_2_row"], rows["dbl_3_row"])
+
+
+@pytest.mark.parametrize("case", FIX["airs"]["ed25519"]["cases"], ids=_ids("ed25519"))
+def test_ed25519_evaluator_matches_reference(case):
+    lay, pr = _ed25519_program(case["layout"])
+    cur, nxt = rows_for(case["seed"], lay.width)
+    check(OE.eval_row(pr, cur, nxt, case["row"]), case)
+
+
 def test_fixture_shapes():
     # the fixture itself: one case per gating phase, digests of full-length vectors
     assert FIX["airs"]["sha256"]["constraints"] == 766 and FIX["airs"]["sha512"]["constraints"] == 1526
     assert FIX["airs"]["p256_ecdsa"]["constraints"] == 155774
+    assert [L["constraints"] for L in FIX["airs"]["ed25519"]["layouts"]] == [68870, 70606, 68926]
     for a in FIX["airs"].values():
         assert len({c["sha3_256"] for c in a["cases"]}) == len(a["cases"])
