@@ -403,6 +403,75 @@ int sg_prove_p256_ecdsa(sg_ctx* ctx, const uint8_t qx[32], const uint8_t qy[32],
                         const uint8_t s[32], const uint8_t digest[32], const uint8_t pi[32], uint8_t* proof,
                         size_t cap, size_t* len);
 
+/* ---------------------------------------------------------------- Ed25519 signature checks
+ * Ed25519 (RFC 8032) verification proved as the v16 verify AIR of
+ * deep_ali/src/ed25519_verify_air.rs: the SHA-512 rows of R || A || M, the
+ * reduction k = digest mod L, the decompressions of R and A, the [s]B and [k]A
+ * ladders (k_scalar rows each), the residual [s]B - R - [k]A as two point
+ * additions, three doublings and the identity verdict on [8] residual. Field
+ * elements of 2^255 - 19 are 10 limbs of 26/25 bits with range bits and carries
+ * (ed25519_field_air.rs). For k_scalar = 256 and a 32-byte message: 1024 rows,
+ * 41,519 cells and 70,606 constraints per row; the proof's domain is 1024 x 32.
+ * pub is the 32-byte public key A, sig the 64-byte signature R || S, msg the
+ * signed data (the SHA-512 input is R || A || msg). Every entry refuses, with
+ * SG_EINVAL, an R or A that does not decode (y >= p, off the curve, or x = 0 with
+ * the sign bit set) and k_scalar outside [2, 256]. */
+
+/* verify_air_layout_v16 (ed25519_verify_air.rs:4741-4814) for a msg_len-byte
+ * message: trace width and height, constraints per row, and the rows of its
+ * phases (k_hash, reduction, decompress R, decompress A, first [s]B row, first
+ * [k]A row, residual, doubling 1, 2, 3, verdict). */
+int sg_ed25519_layout(uint32_t k_scalar, size_t msg_len, uint32_t* width, uint32_t* height, uint32_t* n_constraints,
+                      uint32_t rows[11]);
+/* The row's constraint vector as a program (eval_verify_air_v16_per_row,
+ * ed25519_verify_air.rs:4870-4960, through the v15 .. v0 evaluators): per block 16
+ * u64 (row gate kind 0 every row / 1 row == g0 / 2 g0 <= row < g1 / 3 row in {g0,
+ * g1, g2}; g0..g2; block kind 1 SHA-512, 2 scalar reduction, 3 digest format,
+ * 4 mul, 5 add, 6 sub, 7 select, 8 range check, 9 sign bit, 10 A - B pairs; its
+ * cell bases; ~0 in unused slots) and the pairs (2 u64 each: src << 62 | cell, src
+ * 0 this row, 1 next row, 2 a constant). The public inputs fix the pinned
+ * constants. recs / pairs may be NULL to read the counts (caps in records / pairs). */
+int sg_ed25519_program(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                       uint32_t k_scalar, uint64_t* recs, size_t cap_recs, size_t* n_recs, uint64_t* pairs,
+                       size_t cap_pairs, size_t* n_pairs);
+/* fill_verify_air_v16 (ed25519_verify_air.rs:4820-4868) for the signature on the
+ * host: width x height column-major into `trace` (cap in elements). */
+int sg_ed25519_trace(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                     uint32_t k_scalar, uint64_t* trace, size_t cap);
+/* The same trace with the cells expanded on the device from per-row words (about
+ * 4 MB for k_scalar = 256 instead of the 340 MB trace); host or device output. */
+int sg_ed25519_trace_gpu(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg,
+                         size_t msg_len, uint32_t k_scalar, uint64_t* trace, size_t cap);
+/* deep_ali_merge_ed25519_verify (lib.rs:707-838): Phi_i = sum_j (j + 1) C_j at every
+ * point of a (width x height*blowup) LDE, each point evaluating the blocks its row
+ * opens, then iFFT, poly_div_zh, FFT -> c_eval. The signature fixes the program's
+ * constants. lde: host or device. */
+int sg_merge_ed25519(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                     uint32_t k_scalar, const uint64_t* lde, size_t blowup, uint64_t* c_eval);
+/* Proof: witness (host) -> trace (device) -> LDE x blowup -> merge (coset by coset
+ * above a 2 GiB LDE unless SG_OPT_WIDE_MERGE says otherwise) -> STIR with
+ * build_params(height * blowup, fs_binding), self-verified (prove_zsk_ksk_binding_v2,
+ * swarm-dns/src/prover.rs:856-951, with blowup 32 and k_scalar 256). */
+int sg_prove_ed25519(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                     const uint8_t fs_binding[32], uint32_t k_scalar, size_t blowup, uint8_t* proof, size_t cap,
+                     size_t* len);
+/* RFC 8032 §5.1.7 cofactored verification (ed25519_verify.rs:54-117): 1 valid, 0 not. */
+int sg_ed25519_verify(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len);
+/* zsk_ksk_pi_hash_v2_stark (swarm-dns/src/prover.rs:763-780): SHA3-256 of
+ * "ZSK-KSK-PIHASH-V2-ST" || pub || sig || le64(msg_len) || msg || fs_binding ||
+ * merkle_root || root_f0. */
+int sg_ed25519_pi_hash(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                       const uint8_t fs_binding[32], const uint8_t merkle_root[32], const uint8_t root_f0[32],
+                       uint8_t out[32]);
+/* prove_zsk_ksk_binding_v2 (swarm-dns/src/prover.rs:856-951): the signature is
+ * checked natively first (SG_EVERIFY when it does not verify, before any proving),
+ * then proved with k_scalar rows per ladder at blowup 32 and self-verified; pi_hash
+ * binds the proof's root_f0. SHA3-256 hash profile only (the bundle holds 32-byte
+ * roots), SG_EINVAL otherwise. */
+int sg_prove_zsk_ksk_binding_v2(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg,
+                                size_t msg_len, const uint8_t fs_binding[32], const uint8_t merkle_root[32],
+                                uint32_t k_scalar, uint8_t* proof, size_t cap, size_t* len, uint8_t pi_hash[32]);
+
 /* ---------------------------------------------------------------- DNS shards
  * The steps either side of the prover in swarm-dns. Records are passed in
  * canonical form (DnsRecord::canonical_bytes, swarm-dns/src/dns.rs:43-54):

@@ -23,6 +23,9 @@ C ABI is declared in include/stark_gpu.h:
   prove_p256_ecdsa / p256_chain_trace / merge_p256_ecdsa
                          swarm-dns/examples/prove_ecdsa_record_v1.rs:97-240,
                          deep_ali/src/p256_ecdsa_double_multirow_air.rs, lib.rs:1421-1681
+  prove_ed25519 / ed25519_trace / merge_ed25519 / prove_zsk_ksk_binding_v2
+                         deep_ali/src/ed25519_verify_air.rs (v16), lib.rs:707-974,
+                         swarm-dns/src/prover.rs:763-951
   Server / prove_batch   many proofs in flight on one GPU (worker loop, swarm-worker/src/main.rs:355)
 
 The Merkle / transcript hash profile (sha3-256, sha3-384 or sha3-512: the
@@ -133,6 +136,8 @@ EXPORTS = (
     "sg_rsa2048_trace_gpu", "sg_merge_rsa2048", "sg_prove_rsa2048",
     "sg_p256_layout", "sg_p256_u_bits", "sg_p256_ecdsa_pi", "sg_p256_chain_trace", "sg_p256_chain_trace_gpu",
     "sg_merge_p256_ecdsa", "sg_prove_p256_chains", "sg_prove_p256_ecdsa",
+    "sg_ed25519_layout", "sg_ed25519_program", "sg_ed25519_trace", "sg_ed25519_trace_gpu", "sg_merge_ed25519",
+    "sg_prove_ed25519", "sg_ed25519_verify", "sg_ed25519_pi_hash", "sg_prove_zsk_ksk_binding_v2",
     "sg_merkle_commit",
     "sg_merkle_open", "sg_merkle_free", "sg_build_params", "sg_stir_prove", "sg_stir_prove_group", "sg_stir_verify", "sg_prove_hash_rollup",
     "sg_server_create", "sg_server_destroy", "sg_server_submit", "sg_server_poll", "sg_server_wait", "sg_prove_batch",
@@ -253,6 +258,17 @@ def lib():
     L.sg_merge_p256_ecdsa.argtypes = [vp, vp, sz, sz, vp]
     L.sg_prove_p256_chains.argtypes = [vp, cp, cp, cp, cp, cp, cp, sz, cp, cp, sz, ctypes.POINTER(sz)]
     L.sg_prove_p256_ecdsa.argtypes = [vp, cp, cp, cp, cp, cp, cp, cp, sz, ctypes.POINTER(sz)]
+    u32 = ctypes.c_uint32
+    u32p = ctypes.POINTER(u32)
+    L.sg_ed25519_layout.argtypes = [u32, sz, u32p, u32p, u32p, vp]
+    L.sg_ed25519_program.argtypes = [cp, cp, cp, sz, u32, vp, sz, ctypes.POINTER(sz), vp, sz, ctypes.POINTER(sz)]
+    L.sg_ed25519_trace.argtypes = [cp, cp, cp, sz, u32, vp, sz]
+    L.sg_ed25519_trace_gpu.argtypes = [vp] + L.sg_ed25519_trace.argtypes
+    L.sg_merge_ed25519.argtypes = [vp, cp, cp, cp, sz, u32, vp, sz, vp]
+    L.sg_prove_ed25519.argtypes = [vp, cp, cp, cp, sz, cp, u32, sz, cp, sz, ctypes.POINTER(sz)]
+    L.sg_ed25519_verify.argtypes = [cp, cp, cp, sz]
+    L.sg_ed25519_pi_hash.argtypes = [cp, cp, cp, sz, cp, cp, cp, cp]
+    L.sg_prove_zsk_ksk_binding_v2.argtypes = [vp, cp, cp, cp, sz, cp, cp, u32, cp, sz, ctypes.POINTER(sz), cp]
     L.sg_merge_sha512.argtypes = L.sg_merge_sha256.argtypes
     L.sg_sha512_trace.argtypes = L.sg_sha256_trace.argtypes
     L.sg_sha512_trace_gpu.argtypes = L.sg_sha256_trace_gpu.argtypes
@@ -531,6 +547,80 @@ def p256_chain_trace(a_point, a_bits, b_point, b_bits) -> np.ndarray:
     if rc != SG_OK:
         raise StarkGpuError(rc, "sg_p256_chain_trace failed")
     return out.reshape(width, k)
+
+
+ED25519_K = 256
+ED25519_BLOWUP = 32
+
+
+def _ed_args(pub, sig, msg):
+    pub, sig, msg = bytes(pub), bytes(sig), bytes(msg)
+    if len(pub) != 32 or len(sig) != 64:
+        raise ValueError("Ed25519 keys are 32 bytes and signatures 64 bytes (R || S)")
+    return pub, sig, msg
+
+
+def ed25519_layout(msg_len: int, k_scalar: int = ED25519_K):
+    """verify_air_layout_v16 -> (width, height, constraints per row, dict of phase rows)."""
+    w, h, k = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    rows = (ctypes.c_uint32 * 11)()
+    rc = lib().sg_ed25519_layout(k_scalar, msg_len, ctypes.byref(w), ctypes.byref(h), ctypes.byref(k), rows)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_ed25519_layout failed")
+    names = ("k_hash", "reduce_row", "decompress_R_row", "decompress_A_row", "sB_first_row", "kA_first_row",
+             "residual_row", "dbl_1_row", "dbl_2_row", "dbl_3_row", "result_row")
+    return w.value, h.value, k.value, dict(zip(names, list(rows)))
+
+
+def ed25519_program(pub: bytes, sig: bytes, msg: bytes, k_scalar: int = ED25519_K):
+    """The row's constraint program -> ((n_blocks, 16) uint64 records, (n_pairs, 2) uint64 pairs)."""
+    pub, sig, msg = _ed_args(pub, sig, msg)
+    L = lib()
+    nr, npr = ctypes.c_size_t(), ctypes.c_size_t()
+    rc = L.sg_ed25519_program(pub, sig, msg, len(msg), k_scalar, None, 0, ctypes.byref(nr), None, 0,
+                              ctypes.byref(npr))
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_ed25519_program failed")
+    recs = np.zeros((nr.value, 16), dtype=np.uint64)
+    pairs = np.zeros((npr.value, 2), dtype=np.uint64)
+    rc = L.sg_ed25519_program(pub, sig, msg, len(msg), k_scalar, recs.ctypes.data, nr.value, ctypes.byref(nr),
+                              pairs.ctypes.data, npr.value, ctypes.byref(npr))
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_ed25519_program failed")
+    return recs, pairs
+
+
+def ed25519_trace(pub: bytes, sig: bytes, msg: bytes, k_scalar: int = ED25519_K) -> np.ndarray:
+    """fill_verify_air_v16 on the host -> (width, height) uint64."""
+    pub, sig, msg = _ed_args(pub, sig, msg)
+    w, h, _k, _r = ed25519_layout(len(msg), k_scalar)
+    out = np.empty(w * h, dtype=np.uint64)
+    rc = lib().sg_ed25519_trace(pub, sig, msg, len(msg), k_scalar, out.ctypes.data, out.size)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_ed25519_trace failed")
+    return out.reshape(w, h)
+
+
+def ed25519_verify(pub: bytes, sig: bytes, msg: bytes) -> bool:
+    """RFC 8032 cofactored verification (ed25519_verify.rs:54-117)."""
+    pub, sig, msg = _ed_args(pub, sig, msg)
+    rc = lib().sg_ed25519_verify(pub, sig, msg, len(msg))
+    if rc < 0:
+        raise StarkGpuError(rc, "sg_ed25519_verify failed")
+    return rc == 1
+
+
+def ed25519_pi_hash(pub: bytes, sig: bytes, msg: bytes, fs_binding: bytes, merkle_root: bytes,
+                    root_f0: bytes) -> bytes:
+    """zsk_ksk_pi_hash_v2_stark (swarm-dns/src/prover.rs:763-780)."""
+    pub, sig, msg = _ed_args(pub, sig, msg)
+    if len(fs_binding) != 32 or len(merkle_root) != 32 or len(root_f0) != 32:
+        raise ValueError("fs_binding, merkle_root and root_f0 are 32 bytes")
+    out = ctypes.create_string_buffer(32)
+    rc = lib().sg_ed25519_pi_hash(pub, sig, msg, len(msg), fs_binding, merkle_root, root_f0, out)
+    if rc != SG_OK:
+        raise StarkGpuError(rc, "sg_ed25519_pi_hash failed")
+    return out.raw
 
 
 def _records(records):
@@ -910,6 +1000,69 @@ class Context:
                 continue
             self._check(rc)
             return arr[:ln.value].tobytes()
+
+    def ed25519_trace(self, pub: bytes, sig: bytes, msg: bytes, k_scalar: int = ED25519_K, out=None):
+        """The verify AIR trace with the cells expanded on the GPU -> (width, height)."""
+        pub, sig, msg = _ed_args(pub, sig, msg)
+        w, h, _k, _r = ed25519_layout(len(msg), k_scalar)
+        host = out is None
+        if host:
+            out = np.empty(w * h, dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        self._check(self._lib.sg_ed25519_trace_gpu(self._h, pub, sig, msg, len(msg), k_scalar, op, w * h))
+        return out.reshape(w, h) if host else out
+
+    def merge_ed25519(self, pub: bytes, sig: bytes, msg: bytes, lde, blowup: int = ED25519_BLOWUP,
+                      k_scalar: int = ED25519_K, out=None):
+        """deep_ali_merge_ed25519_verify on a (width, height * blowup) LDE -> c_eval."""
+        pub, sig, msg = _ed_args(pub, sig, msg)
+        ip, _ki, is_np = _addr(lde)
+        if out is None:
+            if not is_np:
+                raise ValueError("device input needs an explicit out buffer")
+            out = np.empty(ed25519_layout(len(msg), k_scalar)[1] * blowup, dtype=np.uint64)
+        op, _ko, _ = _addr(out)
+        self._check(self._lib.sg_merge_ed25519(self._h, pub, sig, msg, len(msg), k_scalar, ip, blowup, op))
+        return out
+
+    def prove_ed25519(self, pub: bytes, sig: bytes, msg: bytes, fs_binding: bytes, k_scalar: int = ED25519_K,
+                      blowup: int = ED25519_BLOWUP) -> bytes:
+        """Ed25519 verify AIR proof (LDE x blowup, STIR with build_params(height * blowup, fs_binding));
+        self-verified."""
+        pub, sig, msg = _ed_args(pub, sig, msg)
+        if len(fs_binding) != 32:
+            raise ValueError("fs_binding must be 32 bytes")
+        cap = _PROOF_CAP
+        while True:
+            arr, buf = _out_buffer(cap)
+            ln = ctypes.c_size_t()
+            rc = self._lib.sg_prove_ed25519(self._h, pub, sig, msg, len(msg), fs_binding, k_scalar, blowup, buf, cap,
+                                            ctypes.byref(ln))
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return arr[:ln.value].tobytes()
+
+    def prove_zsk_ksk_binding_v2(self, pub: bytes, sig: bytes, msg: bytes, fs_binding: bytes, merkle_root: bytes,
+                                 k_scalar: int = ED25519_K):
+        """prove_zsk_ksk_binding_v2 (swarm-dns/src/prover.rs:856-951) -> (proof bytes, pi_hash); the
+        signature is verified natively first (SG_EVERIFY if it does not verify)."""
+        pub, sig, msg = _ed_args(pub, sig, msg)
+        if len(fs_binding) != 32 or len(merkle_root) != 32:
+            raise ValueError("fs_binding and merkle_root must be 32 bytes")
+        cap = _PROOF_CAP
+        while True:
+            arr, buf = _out_buffer(cap)
+            ln = ctypes.c_size_t()
+            pi = ctypes.create_string_buffer(32)
+            rc = self._lib.sg_prove_zsk_ksk_binding_v2(self._h, pub, sig, msg, len(msg), fs_binding, merkle_root,
+                                                       k_scalar, buf, cap, ctypes.byref(ln), pi)
+            if rc == SG_ESPACE:
+                cap = ln.value
+                continue
+            self._check(rc)
+            return arr[:ln.value].tobytes(), pi.raw
 
     def prove_inner_shard(self, records, salt: bytes, fs_binding: bytes, stir: bool = True):
         """prove_inner_shard (swarm-dns/src/prover.rs:148-225) on canonical records ->

@@ -6,6 +6,8 @@
 
 #include "context.hpp"
 #include "dns.hpp"
+#include "ed25519.hpp"
+#include "ed25519_prover.hpp"
 #include "merge.cuh"
 #include "merkle.cuh"
 #include "p256.hpp"
@@ -43,6 +45,21 @@ int guarded(sg_ctx* c, F&& f) {
   } catch (const std::exception& e) {
     return fail(c, SG_EINVAL, e.what());
   }
+}
+
+template <class F>
+int host_guarded(F&& f) {
+  try {
+    f();
+    return SG_OK;
+  } catch (const sg::SgError& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return SG_ENOMEM;
+  }
+}
+bool ed_args(const uint8_t* pub, const uint8_t* sig, const uint8_t* msg, size_t len) {
+  return pub && sig && (msg || len == 0);
 }
 
 // A caller buffer on the device is used in place; a host buffer is staged.
@@ -702,6 +719,137 @@ int sg_prove_p256_ecdsa(sg_ctx* c, const uint8_t qx[32], const uint8_t qy[32], c
     *len = b.size();
     if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_p256_ecdsa: proof buffer too small"};
     memcpy(proof, b.data(), b.size());
+  });
+}
+
+// ------------------------------------------------------------------ Ed25519
+int sg_ed25519_layout(uint32_t k_scalar, size_t msg_len, uint32_t* width, uint32_t* height, uint32_t* n_constraints,
+                      uint32_t rows[11]) {
+  if (!width || !height || !n_constraints) return SG_EINVAL;
+  return host_guarded([&] {
+    const sg::ed25519::Layout L = sg::ed25519::make_layout(64 + (uint64_t)msg_len, k_scalar);
+    *width = L.width;
+    *height = L.height;
+    *n_constraints = L.n_constraints;
+    if (rows) {
+      const uint32_t r[11] = {L.k_hash,   L.reduce_row,   L.decomp_R_row, L.decomp_A_row, L.sB_first, L.kA_first,
+                              L.residual_row, L.dbl_row[0], L.dbl_row[1], L.dbl_row[2], L.result_row};
+      memcpy(rows, r, sizeof r);
+    }
+  });
+}
+
+int sg_ed25519_program(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                       uint32_t k_scalar, uint64_t* recs, size_t cap_recs, size_t* n_recs, uint64_t* pairs,
+                       size_t cap_pairs, size_t* n_pairs) {
+  if (!ed_args(pub, sig, msg, msg_len) || !n_recs || !n_pairs) return SG_EINVAL;
+  return host_guarded([&] {
+    sg::ed25519::Witness w;
+    sg::ed25519::build_witness(pub, sig, msg, msg_len, k_scalar, &w);
+    const auto& P = w.prog;
+    *n_recs = P.blocks.size();
+    *n_pairs = P.pairs.size() / 2;
+    if (recs) {
+      if (cap_recs < P.blocks.size()) throw sg::SgError{SG_ESPACE, "ed25519_program: record buffer too small"};
+      for (size_t i = 0; i < P.blocks.size(); ++i) {
+        const sg::ed25519::Block& b = P.blocks[i];
+        uint64_t* r = recs + 16 * i;
+        for (int j = 0; j < 16; ++j) r[j] = ~0ull;
+        r[0] = b.gate;
+        for (int j = 0; j < 3; ++j) r[1 + j] = b.g[j] == ~0u ? ~0ull : b.g[j];
+        r[4] = b.kind;
+        static const int n_params[11] = {0, 1, 8, 3, 5, 5, 6, 4, 2, 2, 2};
+        for (int j = 0; j < n_params[b.kind]; ++j) r[5 + j] = b.p[j];
+      }
+    }
+    if (pairs) {
+      if (cap_pairs < P.pairs.size() / 2) throw sg::SgError{SG_ESPACE, "ed25519_program: pair buffer too small"};
+      memcpy(pairs, P.pairs.data(), P.pairs.size() * 8);
+    }
+  });
+}
+
+int sg_ed25519_trace(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                     uint32_t k_scalar, uint64_t* trace, size_t cap) {
+  if (!ed_args(pub, sig, msg, msg_len)) return SG_EINVAL;
+  return host_guarded([&] {
+    sg::ed25519::Witness w;
+    sg::ed25519::build_witness(pub, sig, msg, msg_len, k_scalar, &w);
+    if (!trace || (uint64_t)w.L.width * w.L.height > cap)
+      throw sg::SgError{SG_ESPACE, "ed25519_trace: trace buffer too small"};
+    sg::ed25519::expand_host(w, trace);
+  });
+}
+
+int sg_ed25519_trace_gpu(sg_ctx* c, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg,
+                         size_t msg_len, uint32_t k_scalar, uint64_t* trace, size_t cap) {
+  return guarded(c, [&] {
+    sg::require(ed_args(pub, sig, msg, msg_len), "ed25519_trace_gpu: null argument");
+    sg::ed25519::Witness w;
+    sg::ed25519::build_witness(pub, sig, msg, msg_len, k_scalar, &w);
+    const uint64_t cells = (uint64_t)w.L.width * w.L.height;
+    if (!trace || cells > cap) throw sg::SgError{SG_ESPACE, "ed25519_trace_gpu: trace buffer too small"};
+    Out dout(trace, cells, c->stream);
+    sg::ed25519_trace_device(c, w, dout.d);
+    dout.finish();
+  });
+}
+
+int sg_merge_ed25519(sg_ctx* c, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                     uint32_t k_scalar, const uint64_t* lde, size_t blowup, uint64_t* c_eval) {
+  return guarded(c, [&] {
+    sg::require(ed_args(pub, sig, msg, msg_len) && lde && c_eval, "merge_ed25519: null argument");
+    sg::check_blowup(blowup);
+    sg::ed25519::Witness w;
+    sg::ed25519::build_witness(pub, sig, msg, msg_len, k_scalar, &w);
+    const size_t n = (size_t)w.L.height * blowup;
+    In di(lde, (size_t)w.L.width * n, c->stream);
+    Out dout(c_eval, n, c->stream);
+    sg::ed25519_merge_device(c, w, di.d, blowup, dout.d);
+    dout.finish();
+  });
+}
+
+int sg_prove_ed25519(sg_ctx* c, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                     const uint8_t fs_binding[32], uint32_t k_scalar, size_t blowup, uint8_t* proof, size_t cap,
+                     size_t* len) {
+  return guarded(c, [&] {
+    sg::require(ed_args(pub, sig, msg, msg_len) && fs_binding && len, "prove_ed25519: null argument");
+    std::vector<uint8_t> b = sg::prove_ed25519(c, pub, sig, msg, msg_len, fs_binding, k_scalar, true, blowup);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_ed25519: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+  });
+}
+
+int sg_ed25519_verify(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len) {
+  if (!ed_args(pub, sig, msg, msg_len)) return SG_EINVAL;
+  return sg::ed25519::verify(pub, sig, msg, msg_len) ? 1 : 0;
+}
+
+int sg_ed25519_pi_hash(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
+                       const uint8_t fs_binding[32], const uint8_t merkle_root[32], const uint8_t root_f0[32],
+                       uint8_t out[32]) {
+  if (!ed_args(pub, sig, msg, msg_len) || !fs_binding || !merkle_root || !root_f0 || !out) return SG_EINVAL;
+  sg::ed25519::pi_hash(pub, sig, msg, msg_len, fs_binding, merkle_root, root_f0, out);
+  return SG_OK;
+}
+
+int sg_prove_zsk_ksk_binding_v2(sg_ctx* c, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg,
+                                size_t msg_len, const uint8_t fs_binding[32], const uint8_t merkle_root[32],
+                                uint32_t k_scalar, uint8_t* proof, size_t cap, size_t* len, uint8_t pi_hash[32]) {
+  return guarded(c, [&] {
+    sg::require(ed_args(pub, sig, msg, msg_len) && fs_binding && merkle_root && len && pi_hash,
+                "prove_zsk_ksk_binding_v2: null argument");
+    sg::require(SG_HASH_BYTES == 32, "prove_zsk_ksk_binding_v2: the bundle binds 32-byte roots (SHA3-256 profile)");
+    if (!sg::ed25519::verify(pub, sig, msg, msg_len))
+      throw sg::SgError{SG_EVERIFY, "prove_zsk_ksk_binding_v2: native Ed25519 verification failed"};
+    std::vector<uint8_t> b =
+        sg::prove_ed25519(c, pub, sig, msg, msg_len, fs_binding, k_scalar, true, sg::ed25519::BLOWUP);
+    *len = b.size();
+    if (b.size() > cap || !proof) throw sg::SgError{SG_ESPACE, "prove_zsk_ksk_binding_v2: proof buffer too small"};
+    memcpy(proof, b.data(), b.size());
+    sg::ed25519::pi_hash(pub, sig, msg, msg_len, fs_binding, merkle_root, b.data(), pi_hash);
   });
 }
 

@@ -185,13 +185,14 @@ __host__ __device__ __forceinline__ void sha512_row_cells(const sha512::BlockWit
 }
 
 __global__ void __launch_bounds__(256) sha512_expand_kernel(const sha512::BlockWitness* __restrict__ wit,
-                                                            uint64_t useful, uint64_t h, uint64_t* __restrict__ out) {
+                                                            uint64_t useful, uint64_t h, uint64_t stride,
+                                                            uint64_t* __restrict__ out) {
   const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= h) return;
   const uint64_t rr = r < useful ? r : useful - 1;
   const uint32_t br = (uint32_t)(rr % sha512::ROWS_PER_BLOCK);
   sha512_row_cells(wit[rr / sha512::ROWS_PER_BLOCK], br, br < 80 ? kK512[br] : 0ull,
-                   [&](uint32_t c, uint64_t v) { out[(uint64_t)c * h + r] = v; });
+                   [&](uint32_t c, uint64_t v) { out[(uint64_t)c * stride + r] = v; });
 }
 
 // ------------------------------------------------------------------ device Phi
@@ -216,17 +217,20 @@ __device__ __forceinline__ uint64_t xor_poly(uint64_t x, uint64_t y) {
 // 0-527 (bit booleanity, limb packs), 528-1047 (the four Sigma / sigma blocks),
 // 1048-1525 (the rest); chunk c writes its part of Phi at part[c n + i].
 constexpr int kPhiChunks = 3;
+// Points 0 .. count-1 of n (a power of two): cell col of point i at lde[col * stride + i],
+// its next row at point (i + step) mod n; chunk c writes part[c * count + i].
 __global__ void __launch_bounds__(128, 4) sha512_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n,
-                                                            uint64_t step, uint64_t row_div, uint64_t n_blocks,
+                                                            uint64_t stride, uint64_t count, uint64_t step,
+                                                            uint64_t row_div, uint64_t n_blocks,
                                                             const uint64_t* __restrict__ lam,
                                                             uint64_t* __restrict__ part) {
   using namespace sha512;
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= count) return;
   const uint32_t chunk = blockIdx.y;
   const uint64_t j = (i + step) & (n - 1);
-  auto C = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + i); };
-  auto X = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * n + j); };
+  auto C = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * stride + i); };
+  auto X = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * stride + j); };
   const uint64_t row = i / row_div, blk = row / ROWS_PER_BLOCK, br = row % ROWS_PER_BLOCK;
   const bool past = blk >= n_blocks;
   const bool comp = !past && br < ROUNDS, fin = !past && br == ROUNDS, sched = !past && br >= 15 && br <= 78;
@@ -286,7 +290,7 @@ __global__ void __launch_bounds__(128, 4) sha512_phi_kernel(const uint64_t* __re
     acc.push(gl::sub(C(g.lo), pack(g.bit)));
     acc.push(gl::sub(C(g.lo + 1), pack(g.bit + 32)));
   }
-  part[n + i] = acc.phi;
+  part[count + i] = acc.phi;
   return;
   }
   // Ch(e, f, g) = e f + g - e g
@@ -406,7 +410,7 @@ __global__ void __launch_bounds__(128, 4) sha512_phi_kernel(const uint64_t* __re
   } else {
     acc.zeros(8);
   }
-  part[2 * n + i] = acc.phi;
+  part[2 * count + i] = acc.phi;
 }
 
 __global__ void sha512_phi_sum(const uint64_t* __restrict__ part, uint64_t n, uint64_t* __restrict__ phi,
@@ -481,31 +485,45 @@ void sha512_fill_host(const sha512::BlockWitness* wit, uint64_t n_blocks, uint64
 
 cudaError_t sha512_expand(const sha512::BlockWitness* d_wit, uint64_t n_blocks, uint64_t h, uint64_t* d_trace,
                           cudaStream_t s) {
+  return sha512_expand_strided(d_wit, n_blocks, h, h, d_trace, s);
+}
+
+cudaError_t sha512_expand_strided(const sha512::BlockWitness* d_wit, uint64_t n_blocks, uint64_t h, uint64_t stride,
+                                  uint64_t* d_trace, cudaStream_t s) {
+  if (stride < h) return cudaErrorInvalidValue;
   cudaError_t e = upload_k();
   if (e != cudaSuccess) return e;
   SG_LAUNCH_SCOPE("sha512_expand", s);
   sha512_expand_kernel<<<(unsigned)((h + 255) / 256), 256, 0, s>>>(d_wit, sha512::ROWS_PER_BLOCK * n_blocks, h,
-                                                                     d_trace);
+                                                                     stride, d_trace);
   return cudaGetLastError();
 }
 
 cudaError_t sha512_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, uint64_t row_div, uint64_t n_blocks,
                               const uint64_t* lambdas, uint64_t* phi, uint64_t out_stride, uint64_t out_off,
                               cudaStream_t s) {
+  return sha512_phi_points_ex(evals, n, n, n, step, row_div, n_blocks, lambdas, phi, out_stride, out_off, s);
+}
+
+cudaError_t sha512_phi_points_ex(const uint64_t* evals, uint64_t n, uint64_t stride, uint64_t count, uint64_t step,
+                                 uint64_t row_div, uint64_t n_blocks, const uint64_t* lambdas, uint64_t* phi,
+                                 uint64_t out_stride, uint64_t out_off, cudaStream_t s) {
+  if (count == 0) return cudaSuccess;
+  if (count > n || stride < count || (n & (n - 1))) return cudaErrorInvalidValue;
   cudaError_t e = upload_k();
   if (e != cudaSuccess) return e;
   const unsigned T = 128;
   uint64_t* part = nullptr;
-  e = cudaMallocAsync((void**)&part, kPhiChunks * n * sizeof(uint64_t), s);
+  e = cudaMallocAsync((void**)&part, kPhiChunks * count * sizeof(uint64_t), s);
   if (e != cudaSuccess) return e;
   {
     SG_LAUNCH_SCOPE("merge_phi", s);
-    sha512_phi_kernel<<<dim3((unsigned)((n + T - 1) / T), kPhiChunks), T, 0, s>>>(evals, n, step, row_div, n_blocks,
-                                                                                   lambdas, part);
+    sha512_phi_kernel<<<dim3((unsigned)((count + T - 1) / T), kPhiChunks), T, 0, s>>>(
+        evals, n, stride, count, step, row_div, n_blocks, lambdas, part);
   }
   {
     SG_LAUNCH_SCOPE("merge_phi_sum", s);
-    sha512_phi_sum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part, n, phi, out_stride, out_off);
+    sha512_phi_sum<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(part, count, phi, out_stride, out_off);
   }
   e = cudaGetLastError();
   cudaFreeAsync(part, s);

@@ -51,11 +51,19 @@ void sha512_fill_host(const sha512::BlockWitness* wit, uint64_t n_blocks, uint64
 // The same expansion on the device.
 cudaError_t sha512_expand(const sha512::BlockWitness* d_wit, uint64_t n_blocks, uint64_t h, uint64_t* d_trace,
                           cudaStream_t s);
+// The h rows into a wider trace whose columns are `stride` rows apart.
+cudaError_t sha512_expand_strided(const sha512::BlockWitness* d_wit, uint64_t n_blocks, uint64_t h, uint64_t stride,
+                                  uint64_t* d_trace, cudaStream_t s);
 // Phi at the points of a column-major evaluation buffer (n points per column):
 // cur = point i, nxt = point (i + step) mod n, trace row i / row_div; result to
 // phi[out_off + i * out_stride] (eval_sha512_constraints, sha512_air.rs:909-1270).
 cudaError_t sha512_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, uint64_t row_div, uint64_t n_blocks,
                               const uint64_t* lambdas, uint64_t* phi, uint64_t out_stride, uint64_t out_off,
                               cudaStream_t s);
+// The same for points 0 .. count-1 only, with cell col of point i at evals[col * stride + i]
+// (the next row is still point (i + step) mod n): the SHA-512 rows at the top of a wider AIR.
+cudaError_t sha512_phi_points_ex(const uint64_t* evals, uint64_t n, uint64_t stride, uint64_t count, uint64_t step,
+                                 uint64_t row_div, uint64_t n_blocks, const uint64_t* lambdas, uint64_t* phi,
+                                 uint64_t out_stride, uint64_t out_off, cudaStream_t s);
 
 }  // namespace sg
