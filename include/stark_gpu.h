@@ -80,7 +80,9 @@ const char* sg_last_error(const sg_ctx* ctx);
  *                         one n_trace-point NTT per column) and fold the constraints of that
  *                         coset straight into Phi (row i+blowup of the LDE is the next point
  *                         of the same coset) -- memory 3 x trace instead of blowup x trace;
- *   SG_WIDE_MERGE_AUTO    (default) cosets once the LDE would exceed 2 GiB.
+ *   SG_WIDE_MERGE_AUTO    (default) cosets once the LDE would exceed 2 GiB; for
+ *                         sg_prove_ed25519 always the LDE, of which only the
+ *                         columns read on most rows are transformed.
  * Both give bit-identical results. */
 #define SG_OPT_WIDE_MERGE 1
 /* SG_OPT_STIR_GROUP (1 .. 64, default 1): servers (and sg_prove_batch) created
@@ -521,6 +523,9 @@ int sg_prove_outer_rollup(sg_ctx* ctx, const uint8_t* pi_hashes, size_t n, const
                                 768 * records (sg_prove_rsa2048; pi = public_inputs_hash) */
 #define SG_JOB_P256_ECDSA 5  /* input = qx || qy || r || s || digest (32 bytes each), input_len = 160
                                 (sg_prove_p256_ecdsa; pi = public_inputs_hash) */
+#define SG_JOB_ED25519 6     /* input = pub (32) || sig (64) || msg, input_len = 96 + message bytes
+                                (sg_prove_ed25519 with k_scalar 256; pi = fs_binding); the signature
+                                is verified natively first (SG_EVERIFY when it does not verify) */
 
 typedef struct {
   int32_t kind;

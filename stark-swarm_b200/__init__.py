@@ -144,7 +144,7 @@ EXPORTS = (
     "sg_server_wait_for", "sg_server_cancel", "sg_server_set_retries",
     "sg_pool_reserve", "sg_hash_bytes", "sg_ntt_autotune", "sg_ntt_set_split",
 )
-JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA = 1, 2, 3, 4, 5
+JOB_SHA256, JOB_HASH_ROLLUP, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA, JOB_ED25519 = 1, 2, 3, 4, 5, 6
 # sg_job.flags: host-side fault injection for tests of the serving loop
 JOB_FAULT_ALLOC, JOB_FAULT_VERIFY = 1, 2
 OPT_WIDE_MERGE = 1
@@ -1201,7 +1201,11 @@ def make_job(kind: int, data, pi: bytes, phi_mode: int = PHI_PARALLEL_GATE, blow
         # data: (q, r, s, digest) with q = (x, y), or the 160 packed bytes
         q, r, s_, dg = data
         data = _be32(q[0]) + _be32(q[1]) + _be32(r) + _be32(s_) + _be32(dg)
-    if kind in (JOB_SHA256, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA):
+    if kind == JOB_ED25519 and not isinstance(data, (bytes, bytearray)):
+        # data: (pub, sig, msg), or the packed pub || sig || msg
+        pub, sig, msg = _ed_args(*data)
+        data = pub + sig + msg
+    if kind in (JOB_SHA256, JOB_SHA512, JOB_RSA2048, JOB_P256_ECDSA, JOB_ED25519):
         buf = ctypes.create_string_buffer(bytes(data), max(1, len(data)))
         n = len(data)
     elif kind == JOB_HASH_ROLLUP:

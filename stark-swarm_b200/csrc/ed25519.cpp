@@ -11,6 +11,7 @@
 #include "ed25519.hpp"
 
 #include <algorithm>
+#include <map>
 #include <cstring>
 #include <thread>
 
@@ -1191,6 +1192,115 @@ void expand_host(const Witness& w, uint64_t* trace) {
   std::vector<uint64_t> sha((size_t)SHA_W * L.k_hash);
   sha512_fill_host(w.sha.data(), L.n_blocks, L.k_hash, sha.data());
   for (uint32_t c = 0; c < SHA_W; ++c) memcpy(trace + c * H, sha.data() + (size_t)c * L.k_hash, 8 * L.k_hash);
+}
+
+namespace {
+
+// The cells a block reads at this row (cur) and at the next row (nxt).
+template <class Cur, class Nxt>
+void block_cells(const Block& b, const Program& P, Cur cur, Nxt nxt) {
+  auto span = [&](uint32_t base, uint32_t n) {
+    for (uint32_t i = 0; i < n; ++i) cur(base + i);
+  };
+  const uint32_t* p = b.p;
+  switch (b.kind) {
+    case B_SHA512:
+      for (uint32_t c = 0; c < SHA_W; ++c) cur(c), nxt(c);
+      break;
+    case B_REDUCE:
+      span(p[0], RED_IN), span(p[1], RED_Q), span(p[2], RED_Q * RED_LB), span(p[3], RED_R);
+      span(p[4], RED_R * RED_LB), span(p[5], RED_R), span(p[6], RED_R * RED_LB), span(p[7], RED_PROD * RED_CB);
+      break;
+    case B_FORMAT:
+      span(p[0], 512), span(p[2], 16);
+      for (uint32_t i = 0; i < RED_IN; ++i) nxt(p[1] + i);
+      break;
+    case B_MUL: span(p[0], NL), span(p[1], NL), span(p[2], NL), span(p[3], 255), span(p[4], MUL_CB * NL); break;
+    case B_ADD: span(p[0], NL), span(p[1], NL), span(p[2], NL), span(p[3], 255), span(p[4], NL); break;
+    case B_SUB: span(p[0], NL), span(p[1], NL), span(p[2], NL), span(p[3], 255), span(p[4], NL), span(p[5], NL); break;
+    case B_SEL: span(p[0], NL), span(p[1], NL), cur(p[2]), span(p[3], NL); break;
+    case B_RANGE: span(p[0], NL), span(p[1], 255); break;
+    case B_SIGN: cur(p[0]), cur(p[1]); break;
+    default:
+      for (uint32_t i = 0; i < p[1]; ++i)
+        for (int h = 0; h < 2; ++h) {
+          const uint64_t r = P.pairs[2 * (p[0] + i) + h], src = r >> 62;
+          if (src == SRC_CUR) cur((uint32_t)(r & 0xFFFFFFFFu));
+          if (src == SRC_NXT) nxt((uint32_t)(r & 0xFFFFFFFFu));
+        }
+  }
+}
+
+}  // namespace
+
+LdePlan make_lde_plan(const Witness& w) {
+  const Layout& L = w.L;
+  const uint32_t W = L.width, H = L.height, D = L.r_thread, K = LdePlan::kSparseRows;
+  LdePlan plan;
+  plan.dense = D;
+  // row sets of the columns at and above D, capped: more than K rows marks a column wide
+  std::vector<std::vector<uint32_t>> nz(W - D), rd(W - D);
+  std::vector<char> nz_wide(W - D, 0), rd_wide(W - D, 0);
+  auto add = [&](std::vector<uint32_t>& set, char& wide, uint32_t row) {
+    if (wide) return;
+    if (std::find(set.begin(), set.end(), row) != set.end()) return;
+    if (set.size() == K) {
+      wide = 1;
+      return;
+    }
+    set.push_back(row);
+  };
+  std::vector<std::vector<uint32_t>> phase_rows(N_PHASES);
+  for (uint32_t r = 0; r < H; ++r) phase_rows[w.row_phase[r]].push_back(r);
+  // constant columns: the same global word in every phase that has rows
+  std::vector<char> is_const(W - D, 1);
+  for (uint32_t c = D; c < W; ++c) {
+    uint32_t code0 = ~0u;
+    for (uint32_t ph = 0; ph < N_PHASES; ++ph) {
+      if (phase_rows[ph].empty()) continue;
+      const uint32_t cd = w.codes[(size_t)ph * W + c];
+      if (code0 == ~0u) code0 = cd;
+      if (cd != code0 || (cd >> 29) != OP_GLOBAL) is_const[c - D] = 0;
+      if (cd != 0)
+        for (uint32_t r : phase_rows[ph]) add(nz[c - D], nz_wide[c - D], r);
+    }
+  }
+  for (const Block& b : w.prog.blocks) {
+    std::vector<uint32_t> rows;
+    for (uint32_t r = 0; r < H; ++r)
+      if (gate_open(b, r)) rows.push_back(r);
+    if (rows.empty()) continue;
+    block_cells(
+        b, w.prog,
+        [&](uint32_t c) {
+          if (c >= D)
+            for (uint32_t r : rows) add(rd[c - D], rd_wide[c - D], r);
+        },
+        [&](uint32_t c) {
+          if (c >= D)
+            for (uint32_t r : rows) add(rd[c - D], rd_wide[c - D], (r + 1) % H);
+        });
+  }
+  std::map<std::pair<std::vector<uint32_t>, std::vector<uint32_t>>, size_t> gid;
+  for (uint32_t c = D; c < W; ++c) {
+    const uint32_t i = c - D;
+    if (is_const[i]) {
+      plan.const_cols.push_back(c);
+      continue;
+    }
+    if (nz_wide[i] || rd_wide[i]) return LdePlan{};  // a column outside the plan: full LDE
+    std::sort(nz[i].begin(), nz[i].end());
+    std::sort(rd[i].begin(), rd[i].end());
+    auto key = std::make_pair(nz[i], rd[i]);
+    auto it = gid.find(key);
+    if (it == gid.end()) {
+      it = gid.emplace(key, plan.groups.size()).first;
+      plan.groups.push_back(LdePlan::Group{nz[i], rd[i], {}});
+    }
+    plan.groups[it->second].cols.push_back(c);
+  }
+  plan.ok = true;
+  return plan;
 }
 
 bool verify(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, uint64_t len) {

@@ -183,6 +183,27 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
                    Witness* w);
 // The column-major width x height trace on the host.
 void expand_host(const Witness& w, uint64_t* trace);
+
+// Which LDE values the merge reads. The trace LDE feeds only the merge (the proof
+// commits to c_eval alone, swarm-dns/src/prover.rs:904-916), and a point reads a
+// cell only when a block open on its row (or, through a next-row reference, on the
+// row before) names it. Columns below `dense` are read on most rows and get the
+// full LDE; a constant column's LDE is its value; a sparse column is non-zero on at
+// most kSparseRows trace rows and read on at most kSparseRows rows, so its LDE at
+// the points of a read row a (point a blowup + j) is sum over its non-zero rows r
+// of v_r L_r(w_N^(a blowup + j)), with L_r the Lagrange basis of the trace domain.
+struct LdePlan {
+  static constexpr uint32_t kSparseRows = 8;
+  uint32_t dense = 0;           // columns [0, dense) take the NTT LDE
+  bool ok = false;              // false: every column takes the NTT LDE
+  std::vector<uint32_t> const_cols;
+  // sparse columns in groups with the same non-zero and read rows
+  struct Group {
+    std::vector<uint32_t> nz, read, cols;
+  };
+  std::vector<Group> groups;
+};
+LdePlan make_lde_plan(const Witness& w);
 // RFC 8032 §5.1.7 cofactored verification (ed25519_verify.rs:54-117).
 bool verify(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, uint64_t len);
 // zsk_ksk_pi_hash_v2_stark (swarm-dns/src/prover.rs:763-780).

@@ -309,6 +309,47 @@ __global__ void ed25519_phi_sum(EdPhi a, const uint64_t* part, uint64_t* phi) {
     phi[a.out_off + c + a.out_stride * row] = s;
 }
 
+// L_r(x) = w_n^r (x^n - 1) / (n (x - w_n^r)) at x = w_N^(a B + j); on the trace
+// domain (j = 0) it is 1 when a = r and 0 otherwise.
+__global__ void ed25519_lagrange_kernel(const uint32_t* ar, uint32_t n_pairs, uint64_t B, unsigned log_n0,
+                                        uint64_t n_trace, uint64_t* lval) {
+  const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t >= (uint64_t)n_pairs * B) return;
+  const uint64_t p = t / B, j = t - p * B;
+  const uint64_t a = ar[2 * p], r = ar[2 * p + 1];
+  if (j == 0) {
+    lval[t] = a == r;
+    return;
+  }
+  const uint64_t wN = gl::root_of_unity(log_n0);
+  const uint64_t x = gl::pow(wN, a * B + j), wr = gl::pow(wN, r * B);
+  const uint64_t num = gl::mul(gl::mul(wr, gl::inv(n_trace % gl::P)), gl::sub(gl::pow(x, n_trace), 1));
+  lval[t] = gl::mul(num, gl::inv(gl::sub(x, wr)));
+}
+
+// one CTA per task: the B points of read row a of column c
+__global__ void ed25519_sparse_fill_kernel(EdLdeFill f, const uint64_t* trace, uint64_t H, uint64_t B,
+                                           const uint64_t* lval, uint64_t* lde) {
+  const uint32_t* t = f.tasks + 5 * (uint64_t)blockIdx.x;
+  const uint64_t c = t[0], a = t[1], lb = t[2], off = t[3], nnz = t[4], n0 = H * B;
+  for (uint64_t j = threadIdx.x; j < B; j += blockDim.x) {
+    uint64_t v = 0;
+    for (uint64_t k = 0; k < nnz; ++k)
+      v = gl::add(v, gl::mul(__ldg(trace + c * H + f.nz_rows[off + k]), __ldg(lval + (lb + k) * B + j)));
+    lde[c * n0 + a * B + j] = v;
+  }
+}
+
+__global__ void ed25519_const_fill_kernel(EdLdeFill f, const uint64_t* trace, uint64_t H, uint64_t n0,
+                                          uint64_t* lde) {
+  const uint64_t total = (uint64_t)f.n_const * n0;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = e / n0, c = f.const_cols[k];
+    lde[c * n0 + (e - k * n0)] = __ldg(trace + c * H);
+  }
+}
+
 }  // namespace
 
 EdPhiPlan ed25519_phi_plan(const Program& prog, uint32_t n_trace, uint32_t chunk_constraints) {
@@ -358,6 +399,28 @@ EdPhiPlan ed25519_phi_plan(const Program& prog, uint32_t n_trace, uint32_t chunk
     P.row_class[row] = (uint8_t)it->second;
   }
   return P;
+}
+
+cudaError_t ed25519_lde_fill(const EdLdeFill& f, const uint64_t* d_trace, uint64_t height, uint64_t blowup,
+                             uint64_t* d_lval, uint64_t* d_lde, cudaStream_t s) {
+  unsigned log_n0 = 0;
+  while ((1ull << log_n0) < height * blowup) ++log_n0;
+  if ((1ull << log_n0) != height * blowup) return cudaErrorInvalidValue;
+  SG_LAUNCH_SCOPE("ed25519_lde_fill", s);
+  if (f.n_pairs) {
+    const uint64_t t = (uint64_t)f.n_pairs * blowup;
+    ed25519_lagrange_kernel<<<(unsigned)((t + 127) / 128), 128, 0, s>>>(f.ar, f.n_pairs, blowup, log_n0, height,
+                                                                       d_lval);
+  }
+  if (f.n_tasks)
+    ed25519_sparse_fill_kernel<<<f.n_tasks, (unsigned)std::min<uint64_t>(blowup, 128), 0, s>>>(
+        f, d_trace, height, blowup, d_lval, d_lde);
+  if (f.n_const) {
+    const uint64_t total = (uint64_t)f.n_const * height * blowup;
+    ed25519_const_fill_kernel<<<(unsigned)std::min<uint64_t>((total + 255) / 256, 148ull * 32), 256, 0, s>>>(
+        f, d_trace, height, height * blowup, d_lde);
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t ed25519_expand(const EdExpand& d, uint64_t* d_trace, cudaStream_t s) {

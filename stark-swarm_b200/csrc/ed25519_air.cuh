@@ -23,6 +23,23 @@ struct EdExpand {
 // sha512_expand_strided) of the width x height column-major trace.
 cudaError_t ed25519_expand(const EdExpand& d, uint64_t* d_trace, cudaStream_t s);
 
+// The LDE values the merge reads in the columns an LdePlan does not transform
+// (device pointers): Lagrange basis values L_r at the points of read rows
+// (ar: read row a and non-zero row r per pair), sparse tasks (5 u32 each: column,
+// read row, first pair, offset into nz_rows, number of non-zero rows) and the
+// constant columns. The trace is width x height column-major, the LDE width x n0.
+struct EdLdeFill {
+  const uint32_t* ar;
+  uint32_t n_pairs;
+  const uint32_t* tasks;
+  uint32_t n_tasks;
+  const uint32_t* nz_rows;
+  const uint32_t* const_cols;
+  uint32_t n_const;
+};
+cudaError_t ed25519_lde_fill(const EdLdeFill& f, const uint64_t* d_trace, uint64_t height, uint64_t blowup,
+                             uint64_t* d_lval, uint64_t* d_lde, cudaStream_t s);
+
 // A block of the constraint program on the device: kind, index of its first
 // constraint, cell bases (B_PAIRS: first pair, count).
 struct EdBlock {

@@ -85,6 +85,34 @@ void ed25519_trace_device(sg_ctx* c, const ed25519::Witness& w, uint64_t* d_trac
              "ed25519 sha512 rows");
 }
 
+void ed25519_lde_device(sg_ctx* c, const ed25519::Witness& w, const uint64_t* d_trace, uint64_t blowup,
+                        uint64_t* d_lde) {
+  const ed25519::Layout& L = w.L;
+  const ed25519::LdePlan plan = ed25519::make_lde_plan(w);
+  if (!plan.ok) {
+    lde_device(c, d_trace, L.width, L.height, blowup, 1, d_lde);
+    return;
+  }
+  cudaStream_t s = c->stream;
+  lde_device(c, d_trace, plan.dense, L.height, blowup, 1, d_lde);
+  std::vector<uint32_t> ar, tasks, nz_rows;
+  for (const auto& g : plan.groups) {
+    const uint32_t off = (uint32_t)nz_rows.size();
+    nz_rows.insert(nz_rows.end(), g.nz.begin(), g.nz.end());
+    for (uint32_t a : g.read) {
+      const uint32_t lb = (uint32_t)(ar.size() / 2);
+      for (uint32_t r : g.nz) ar.push_back(a), ar.push_back(r);
+      for (uint32_t col : g.cols) tasks.insert(tasks.end(), {col, a, lb, off, (uint32_t)g.nz.size()});
+    }
+  }
+  DBuf d_ar = upload(ar, s), d_tasks = upload(tasks, s), d_nz = upload(nz_rows, s);
+  DBuf d_const = upload(plan.const_cols, s), d_lval(std::max<uint64_t>(1, ar.size() / 2 * blowup), s);
+  EdLdeFill f{(const uint32_t*)d_ar.p,    (uint32_t)(ar.size() / 2), (const uint32_t*)d_tasks.p,
+              (uint32_t)(tasks.size() / 5), (const uint32_t*)d_nz.p, (const uint32_t*)d_const.p,
+              (uint32_t)plan.const_cols.size()};
+  cuda_check(ed25519_lde_fill(f, d_trace, L.height, blowup, d_lval.p, d_lde, s), "ed25519 sparse LDE");
+}
+
 void ed25519_merge_device(sg_ctx* c, const ed25519::Witness& w, const uint64_t* d_lde, uint64_t blowup,
                           uint64_t* d_c) {
   const ed25519::Layout& L = w.L;
@@ -136,10 +164,9 @@ void ed25519_merge_cosets(sg_ctx* c, const ed25519::Witness& w, const uint64_t* 
       cuda_check(ntt_batch(c->tw, coef.p, ev.p + g * n_trace, (uint32_t)W, n_trace, G * n_trace, (int)lt, false,
                            n_trace, scratch.p, s, r > 0 ? &twist : nullptr),
                  "ed25519 coset ntt");
-      cuda_check(sha512_phi_points_ex(ev.p + g * n_trace, n_trace, G * n_trace, sha_rows, 1, 1, L.n_blocks,
-                                      pd.sha_lam.p, phi_sha.p, 1, g * n_trace, s),
-                 "ed25519 sha512 phi");
     }
+    cuda_check(sha512_phi_cosets(ev.p, G, n_trace, sha_rows, L.n_blocks, pd.sha_lam.p, phi_sha.p, s),
+               "ed25519 sha512 phi");
     cuda_check(ed25519_phi(pd.args(ev.p, G * n_trace, blowup, n_trace, n_trace, blowup, r0, phi_sha.p, sha_rows),
                            part.p, phi.p, s),
                "ed25519 coset phi");
@@ -160,13 +187,14 @@ CEval ed25519_ceval(sg_ctx* c, const uint8_t pub[32], const uint8_t sig[64], con
   {
     DBuf d_trace(W * w.L.height, s);
     ed25519_trace_device(c, w, d_trace.p);
-    const bool cosets = c->wide_merge == SG_WIDE_MERGE_COSETS ||
-                        (c->wide_merge == SG_WIDE_MERGE_AUTO && W * n0 * 8 > (2ull << 30));
+    // The materialised path transforms only the dense columns (ed25519_lde_device) and
+    // is the faster one; streaming by cosets is for callers that cannot hold the LDE.
+    const bool cosets = c->wide_merge == SG_WIDE_MERGE_COSETS;
     if (cosets) {
       ed25519_merge_cosets(c, w, d_trace.p, blowup, d_c.p);
     } else {
       DBuf d_lde(W * n0, s);
-      lde_device(c, d_trace.p, W, w.L.height, blowup, 1, d_lde.p);
+      ed25519_lde_device(c, w, d_trace.p, blowup, d_lde.p);
       d_trace = DBuf();
       ed25519_merge_device(c, w, d_lde.p, blowup, d_c.p);
     }

@@ -11,6 +11,11 @@ namespace sg {
 
 // The width x height trace of a witness, expanded on the device.
 void ed25519_trace_device(sg_ctx* c, const ed25519::Witness& w, uint64_t* d_trace);
+// The LDE values the merge reads (make_lde_plan): the transform of the dense
+// columns, then the constant and sparse columns filled where they are read; the
+// other cells of d_lde (width x height*blowup) are left unwritten.
+void ed25519_lde_device(sg_ctx* c, const ed25519::Witness& w, const uint64_t* d_trace, uint64_t blowup,
+                        uint64_t* d_lde);
 // Phi + quotient on a materialised (width x height*blowup) LDE.
 void ed25519_merge_device(sg_ctx* c, const ed25519::Witness& w, const uint64_t* d_lde, uint64_t blowup,
                           uint64_t* d_c);

@@ -20,6 +20,8 @@
 #include <vector>
 
 #include "context.hpp"
+#include "ed25519.hpp"
+#include "ed25519_prover.hpp"
 #include "p256.hpp"
 #include "p256_prover.hpp"
 #include "prover.hpp"
@@ -80,8 +82,21 @@ uint64_t footprint_bytes(const sg_job& j) {
     const uint64_t recs = j.input_len / 768, w = recs * sg::rsa::WIDTH, n0 = sg::rsa::N_TRACE * bu;
     return 8 * (w * (sg::rsa::N_TRACE + n0) + (recs + 16) * n0);
   }
+  if (j.kind == SG_JOB_ED25519) {
+    // trace and the materialised LDE at the layout's width, quotient and STIR buffers
+    const sg::ed25519::Layout L = sg::ed25519::make_layout(j.input_len - 32, sg::ed25519::K_FULL);
+    const uint64_t n0 = (uint64_t)L.height * bu;
+    return 8 * ((uint64_t)L.width * (L.height + n0) + 16 * n0) + (64ull << 20);
+  }
   const uint64_t nt = next_pow2(j.input_len < 8 ? 8 : j.input_len), n0 = nt * 32;
   return 8 * (4 * n0 + 8 * nt + 16 * n0);
+}
+
+// pub || sig || msg: the native check first (prove_zsk_ksk_binding_v2 refuses an
+// invalid signature before proving, swarm-dns/src/prover.rs:870-876)
+void check_ed25519_job(const std::vector<uint8_t>& in) {
+  if (!sg::ed25519::verify(in.data(), in.data() + 32, in.data() + 96, in.size() - 96))
+    throw sg::SgError{SG_EVERIFY, "ed25519 job: the signature does not verify"};
 }
 
 // n || s || em per record (256 bytes each) -> the three contiguous arrays prove_rsa2048 takes
@@ -190,6 +205,8 @@ struct sg_server {
       return next_pow2(128 * ((e.input.size() + 17 + 127) / 128)) * e.blowup;
     if (e.kind == SG_JOB_P256_ECDSA) return sg::p256::K_ECDSA * e.blowup;
     if (e.kind == SG_JOB_RSA2048) return sg::rsa::N_TRACE * e.blowup;
+    if (e.kind == SG_JOB_ED25519)
+      return (uint64_t)sg::ed25519::make_layout(e.input.size() - 32, sg::ed25519::K_FULL).height * e.blowup;
     return 0;
   }
 
@@ -204,6 +221,11 @@ struct sg_server {
                                     e->blowup);
     if (e->kind == SG_JOB_P256_ECDSA)
       return sg::p256_ecdsa_ceval(c, in, in + 32, in + 64, in + 96, in + 128, e->pi, e->blowup);
+    if (e->kind == SG_JOB_ED25519) {
+      check_ed25519_job(e->input);
+      return sg::ed25519_ceval(c, in, in + 32, in + 96, e->input.size() - 96, e->pi, sg::ed25519::K_FULL,
+                               e->blowup);
+    }
     const uint64_t recs = e->input.size() / 768;
     std::vector<uint8_t> n(256 * recs), s(256 * recs), em(256 * recs);
     for (uint64_t r = 0; r < recs; ++r) {
@@ -317,6 +339,11 @@ struct sg_server {
         e->proof = sg::prove_p256_ecdsa(c, in, in + 32, in + 64, in + 96, in + 128, e->pi, self_verify, e->blowup);
       } else if (e->kind == SG_JOB_RSA2048) {
         e->proof = prove_rsa_job(c, e->input, e->pi, e->blowup, self_verify);
+      } else if (e->kind == SG_JOB_ED25519) {
+        const uint8_t* in = e->input.data();
+        check_ed25519_job(e->input);
+        e->proof = sg::prove_ed25519(c, in, in + 32, in + 96, e->input.size() - 96, e->pi, sg::ed25519::K_FULL,
+                                     self_verify, e->blowup);
       } else {
         const uint64_t n = e->input.size() / 8;
         e->proof = sg::prove_hash_rollup_host_leaves(c, (const uint64_t*)e->input.data(), n, e->pi, e->phi_mode,
@@ -391,8 +418,9 @@ void sg_server_destroy(sg_server* s) {
 int sg_server_submit(sg_server* s, const sg_job* job, uint64_t* ticket) {
   if (!s || !job || !ticket) return SG_EINVAL;
   if (job->kind != SG_JOB_SHA256 && job->kind != SG_JOB_SHA512 && job->kind != SG_JOB_HASH_ROLLUP &&
-      job->kind != SG_JOB_RSA2048 && job->kind != SG_JOB_P256_ECDSA)
+      job->kind != SG_JOB_RSA2048 && job->kind != SG_JOB_P256_ECDSA && job->kind != SG_JOB_ED25519)
     return SG_EINVAL;
+  if (job->kind == SG_JOB_ED25519 && job->input_len < 96) return SG_EINVAL;
   if (job->kind == SG_JOB_P256_ECDSA && job->input_len != 160) return SG_EINVAL;
   if (job->input_len && !job->input) return SG_EINVAL;
   if (job->kind == SG_JOB_RSA2048 && (job->input_len == 0 || job->input_len % 768)) return SG_EINVAL;

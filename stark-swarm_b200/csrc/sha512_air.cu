@@ -217,21 +217,35 @@ __device__ __forceinline__ uint64_t xor_poly(uint64_t x, uint64_t y) {
 // 0-527 (bit booleanity, limb packs), 528-1047 (the four Sigma / sigma blocks),
 // 1048-1525 (the rest); chunk c writes its part of Phi at part[c n + i].
 constexpr int kPhiChunks = 3;
-// Points 0 .. count-1 of n (a power of two): cell col of point i at lde[col * stride + i],
-// its next row at point (i + step) mod n; chunk c writes part[c * count + i].
+// Work item i < count. Without cosets (coset_len = 0) it is point i of n (a power of
+// two), cell col at lde[col * stride + i], its next row at point (i + step) mod n,
+// trace row i / row_div. With cosets it is row a = i mod rows_pc of coset c = i / rows_pc:
+// point c coset_len + a, next row c coset_len + (a + 1) mod coset_len. Chunk ch writes
+// part[ch * count + i].
 __global__ void __launch_bounds__(128, 4) sha512_phi_kernel(const uint64_t* __restrict__ lde, uint64_t n,
                                                             uint64_t stride, uint64_t count, uint64_t step,
                                                             uint64_t row_div, uint64_t n_blocks,
                                                             const uint64_t* __restrict__ lam,
-                                                            uint64_t* __restrict__ part) {
+                                                            uint64_t* __restrict__ part, uint64_t coset_len,
+                                                            uint64_t rows_pc) {
   using namespace sha512;
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= count) return;
   const uint32_t chunk = blockIdx.y;
-  const uint64_t j = (i + step) & (n - 1);
-  auto C = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * stride + i); };
+  uint64_t pt, j, row;
+  if (coset_len == 0) {
+    pt = i;
+    j = (i + step) & (n - 1);
+    row = i / row_div;
+  } else {
+    const uint64_t c = i / rows_pc;
+    row = i - c * rows_pc;
+    pt = c * coset_len + row;
+    j = c * coset_len + (row + 1 == coset_len ? 0 : row + 1);
+  }
+  auto C = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * stride + pt); };
   auto X = [&](uint32_t col) { return __ldg(lde + (uint64_t)col * stride + j); };
-  const uint64_t row = i / row_div, blk = row / ROWS_PER_BLOCK, br = row % ROWS_PER_BLOCK;
+  const uint64_t blk = row / ROWS_PER_BLOCK, br = row % ROWS_PER_BLOCK;
   const bool past = blk >= n_blocks;
   const bool comp = !past && br < ROUNDS, fin = !past && br == ROUNDS, sched = !past && br >= 15 && br <= 78;
   Acc acc{lam, 0, chunk == 0 ? 0u : chunk == 1 ? 528u : 1048u};
@@ -414,10 +428,11 @@ __global__ void __launch_bounds__(128, 4) sha512_phi_kernel(const uint64_t* __re
 }
 
 __global__ void sha512_phi_sum(const uint64_t* __restrict__ part, uint64_t n, uint64_t* __restrict__ phi,
-                               uint64_t out_stride, uint64_t out_off) {
+                               uint64_t out_stride, uint64_t out_off, uint64_t coset_len, uint64_t rows_pc) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  phi[out_off + i * out_stride] = gl::add(gl::add(part[i], part[n + i]), part[2 * n + i]);
+  const uint64_t o = coset_len ? (i / rows_pc) * coset_len + i % rows_pc : out_off + i * out_stride;
+  phi[o] = gl::add(gl::add(part[i], part[n + i]), part[2 * n + i]);
 }
 
 bool g_k_uploaded[64] = {false};
@@ -519,11 +534,36 @@ cudaError_t sha512_phi_points_ex(const uint64_t* evals, uint64_t n, uint64_t str
   {
     SG_LAUNCH_SCOPE("merge_phi", s);
     sha512_phi_kernel<<<dim3((unsigned)((count + T - 1) / T), kPhiChunks), T, 0, s>>>(
-        evals, n, stride, count, step, row_div, n_blocks, lambdas, part);
+        evals, n, stride, count, step, row_div, n_blocks, lambdas, part, 0, 0);
   }
   {
     SG_LAUNCH_SCOPE("merge_phi_sum", s);
-    sha512_phi_sum<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(part, count, phi, out_stride, out_off);
+    sha512_phi_sum<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(part, count, phi, out_stride, out_off, 0, 0);
+  }
+  e = cudaGetLastError();
+  cudaFreeAsync(part, s);
+  return e;
+}
+
+cudaError_t sha512_phi_cosets(const uint64_t* evals, uint64_t n_cosets, uint64_t coset_len, uint64_t rows,
+                              uint64_t n_blocks, const uint64_t* lambdas, uint64_t* phi, cudaStream_t s) {
+  const uint64_t count = n_cosets * rows;
+  if (count == 0) return cudaSuccess;
+  if (rows > coset_len) return cudaErrorInvalidValue;
+  cudaError_t e = upload_k();
+  if (e != cudaSuccess) return e;
+  const unsigned T = 128;
+  uint64_t* part = nullptr;
+  e = cudaMallocAsync((void**)&part, kPhiChunks * count * sizeof(uint64_t), s);
+  if (e != cudaSuccess) return e;
+  {
+    SG_LAUNCH_SCOPE("merge_phi", s);
+    sha512_phi_kernel<<<dim3((unsigned)((count + T - 1) / T), kPhiChunks), T, 0, s>>>(
+        evals, coset_len, n_cosets * coset_len, count, 1, 1, n_blocks, lambdas, part, coset_len, rows);
+  }
+  {
+    SG_LAUNCH_SCOPE("merge_phi_sum", s);
+    sha512_phi_sum<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(part, count, phi, 0, 0, coset_len, rows);
   }
   e = cudaGetLastError();
   cudaFreeAsync(part, s);

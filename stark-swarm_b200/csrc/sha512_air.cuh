@@ -65,5 +65,10 @@ cudaError_t sha512_phi_points(const uint64_t* evals, uint64_t n, uint64_t step, 
 cudaError_t sha512_phi_points_ex(const uint64_t* evals, uint64_t n, uint64_t stride, uint64_t count, uint64_t step,
                                  uint64_t row_div, uint64_t n_blocks, const uint64_t* lambdas, uint64_t* phi,
                                  uint64_t out_stride, uint64_t out_off, cudaStream_t s);
+// The first `rows` rows of each of n_cosets cosets held one after another (coset c's
+// point a at evals[col * n_cosets * coset_len + c * coset_len + a], its next row
+// point (a + 1) mod coset_len), in one launch; Phi of that point to phi[c coset_len + a].
+cudaError_t sha512_phi_cosets(const uint64_t* evals, uint64_t n_cosets, uint64_t coset_len, uint64_t rows,
+                              uint64_t n_blocks, const uint64_t* lambdas, uint64_t* phi, cudaStream_t s);
 
 }  // namespace sg

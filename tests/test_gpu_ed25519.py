@@ -108,3 +108,26 @@ def test_binding_refuses_an_invalid_signature(sgpu, ctx):
     with pytest.raises(sgpu.StarkGpuError) as e:
         ctx.prove_zsk_ksk_binding_v2(pub, bytes(bad), msg, fs, mr)
     assert e.value.code == sgpu.SG_EVERIFY
+
+
+def test_batch_and_server_jobs(sgpu, ctx):
+    # SG_JOB_ED25519 (k_scalar 256) in a batch beside a SHA-256 job, and in the server,
+    # where a signature that does not verify is refused (SG_EVERIFY) without blocking the queue
+    signed = [_signed(b"srv%d" % i, b"zone record %d" % i) for i in range(3)]
+    fs = [hashlib.sha3_256(b"fs%d" % i).digest() for i in range(3)]
+    want = [ctx.prove_ed25519(p, s, m, f, 256, 4) for (p, s, m), f in zip(signed, fs)]
+    jobs = [(sgpu.JOB_ED25519, psm, f, sgpu.PHI_PARALLEL_GATE, 4) for psm, f in zip(signed, fs)]
+    jobs.append((sgpu.JOB_SHA256, b"record bytes", fs[0]))
+    out = ctx.prove_batch(jobs, n_streams=4)
+    for i in range(3):
+        assert out[i][1].status == sgpu.SG_OK and out[i][0] == want[i]
+    pub, sig, msg = signed[0]
+    bad = bytearray(sig)
+    bad[40] ^= 1
+    with sgpu.Server(ctx, n_streams=2) as srv:
+        t_bad = srv.submit(sgpu.JOB_ED25519, (pub, bytes(bad), msg), fs[0], blowup=4)
+        t_ok = srv.submit(sgpu.JOB_ED25519, signed[1], fs[1], blowup=4)
+        with pytest.raises(sgpu.StarkGpuError) as ei:
+            srv.wait(t_bad)
+        assert ei.value.code == sgpu.SG_EVERIFY
+        assert srv.wait(t_ok)[0] == want[1]
