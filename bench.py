@@ -453,6 +453,136 @@ def p256_ecdsa(sg, ctx, n_jobs, cpu_threads):
     return out
 
 
+# ---------------------------------------------------------------- Ed25519 inputs
+# RFC 8032 section 5.1.5-5.1.6 signing, to make the benchmark's signatures (input
+# generation only; the library proves and checks them).
+ED_P = 2 ** 255 - 19
+ED_L = 2 ** 252 + 27742317777372353535851937790883648493
+ED_D = (-121665 * pow(121666, ED_P - 2, ED_P)) % ED_P
+
+
+def _ed_add(p, q):
+    (X1, Y1, Z1, T1), (X2, Y2, Z2, T2) = p, q
+    a, b = (Y1 - X1) * (Y2 - X2) % ED_P, (Y1 + X1) * (Y2 + X2) % ED_P
+    c, d = 2 * ED_D * T1 * T2 % ED_P, 2 * Z1 * Z2 % ED_P
+    e, f, g, h = b - a, d - c, d + c, b + a
+    return (e * f % ED_P, g * h % ED_P, f * g % ED_P, e * h % ED_P)
+
+
+def _ed_mul(k, p):
+    acc = (0, 1, 1, 0)
+    for i in range(k.bit_length() - 1, -1, -1):
+        acc = _ed_add(acc, acc)
+        if (k >> i) & 1:
+            acc = _ed_add(acc, p)
+    return acc
+
+
+def _ed_base():
+    y = 4 * pow(5, ED_P - 2, ED_P) % ED_P
+    x2 = (y * y - 1) * pow(ED_D * y * y + 1, ED_P - 2, ED_P) % ED_P
+    x = pow(x2, (ED_P + 3) // 8, ED_P)
+    if x * x % ED_P != x2:
+        x = x * pow(2, (ED_P - 1) // 4, ED_P) % ED_P
+    if x & 1:
+        x = ED_P - x
+    return (x, y, 1, x * y % ED_P)
+
+
+ED_B = _ed_base()
+
+
+def _ed_compress(p):
+    zi = pow(p[2], ED_P - 2, ED_P)
+    x, y = p[0] * zi % ED_P, p[1] * zi % ED_P
+    return (y | (x & 1) << 255).to_bytes(32, "little")
+
+
+def ed25519_signature(seed: bytes, msg: bytes):
+    """(public key, signature R || S) of msg under the RFC 8032 key made from a 32-byte seed"""
+    h = hashlib.sha512(seed).digest()
+    a = (int.from_bytes(h[:32], "little") & ((1 << 254) - 8)) | (1 << 254)
+    pub = _ed_compress(_ed_mul(a, ED_B))
+    r = int.from_bytes(hashlib.sha512(h[32:] + msg).digest(), "little") % ED_L
+    R = _ed_compress(_ed_mul(r, ED_B))
+    k = int.from_bytes(hashlib.sha512(R + pub + msg).digest(), "little") % ED_L
+    return pub, R + ((r + k * a) % ED_L).to_bytes(32, "little")
+
+
+def ed25519_inputs(n, seed):
+    """n (pub, sig, 32-byte message) with keys and messages from a seeded generator"""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        key, msg = rng.bytes(32), rng.bytes(32)
+        pub, sig = ed25519_signature(key, msg)
+        out.append((pub, sig, msg))
+    return out
+
+
+def load_oracle_ed25519():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ed25519
+    return oracle_ed25519
+
+
+def ed25519(sg, ctx, n_jobs, cpu_threads):
+    """Ed25519 signature-verification proofs (prove_zsk_ksk_binding_v2: the v16 verify
+    AIR, k_scalar 256, 1024 rows of 41,519 cells and 70,606 constraints, blowup 32,
+    n0 32768): n_jobs signatures of 32-byte messages (keys and messages from seed 5),
+    one STARK per signature as in the reference, one at a time vs 8 in flight; each
+    job is host signature in, proof bytes out, natively checked first and self-verified.
+    Beside it: one proof's latency and kernel breakdown, and the CPU oracle's full-size
+    proof of the same signature (measured, not scaled) next to the reference's published
+    105.01 s per proof."""
+    sigs = ed25519_inputs(n_jobs, 5)
+    fs = hashlib.sha3_256(b"stark-swarm-b200 ed25519 fs binding").digest()
+    jobs = [(sg.JOB_ED25519, s, fs) for s in sigs]
+    ctx.prove_batch(jobs[:16], n_streams=8, hbm_budget_bytes=160 << 30)
+    w, h, k, _rows = sg.ed25519_layout(32)
+    out = {"workload": f"Ed25519 signature-verification proof (v16 verify AIR, k_scalar 256, n_trace {h}, {w} cols, "
+                       f"{k} constraints, blowup 32, n0 {h * 32}), one proof per signature, self-verified",
+           "jobs": n_jobs, "published_reference_s_per_proof": 105.01}
+    pub, sig, msg = sigs[0]
+    lat = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        proof, _pi = ctx.prove_zsk_ksk_binding_v2(pub, sig, msg, fs, bytes(32))
+        lat.append((time.perf_counter() - t0) * 1e3)
+    out["single_ms"] = statistics.median(lat)
+    out["proof_bytes"] = len(proof)
+    sg.profile_enable(True)
+    sg.profile_reset()
+    ctx.prove_ed25519(pub, sig, msg, fs)
+    prof = sg.profile_read()
+    sg.profile_enable(False)
+    out["kernels_ms"] = {kname: round(v[1], 3) for kname, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:10]}
+    for label, streams in (("plain", 1), ("batched", 8)):
+        t0 = time.perf_counter()
+        res = ctx.prove_batch(jobs, n_streams=streams, hbm_budget_bytes=160 << 30)
+        dt = time.perf_counter() - t0
+        assert all(r.status == 0 for _, r in res)
+        ls = sorted(r.latency_ms for _, r in res)
+        out[label] = {"streams": streams, "proofs_per_s": n_jobs / dt, "p50_ms": ls[len(ls) // 2],
+                      "p99_ms": ls[min(len(ls) - 1, int(len(ls) * 0.99))]}
+    out["batched_over_plain"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
+    out["plain_over_published_reference"] = out["plain"]["proofs_per_s"] * 105.01
+    if cpu_threads:
+        E = load_oracle_ed25519()
+        O = load_oracle()
+        O.set_threads(cpu_threads)
+        t0 = time.perf_counter()
+        lay, pr, tr = E.build(pub, sig, msg, 256)
+        cpu_proof = E.prove(lay, pr, tr, fs, 32)
+        dt = time.perf_counter() - t0
+        assert cpu_proof == proof, "GPU and oracle Ed25519 proofs differ"
+        out["cpu_baseline"] = {"proofs_per_s": 1.0 / dt, "cores": cpu_threads, "kind": "port",
+                               "sample": f"one full-size oracle proof of the first signature ({dt:.1f} s: trace, "
+                                         f"LDE x32, merge, STIR), byte-identical to the GPU's"}
+        out["plain_over_cpu"] = out["plain"]["proofs_per_s"] * dt
+    return out
+
+
 def serving(sg, ctx, rates, n_jobs, streams, seed=7):
     """Poisson arrivals of proof requests admitted by the continuous-batching server
     under a 160 GB HBM budget: 40 % SHA-256 record proofs and 20 % SHA-512 over
@@ -628,6 +758,8 @@ def main():
                     help="records of the batched mixed-proving section (2 proofs each, blowup 4; 0 skips it)")
     ap.add_argument("--ecdsa-jobs", type=int, default=32,
                     help="ECDSA-P256 proofs for the plain-vs-batched section (0 skips it)")
+    ap.add_argument("--ed25519-jobs", type=int, default=256,
+                    help="Ed25519 signature proofs (config 3: 256 signatures, one proof each; 0 skips)")
     ap.add_argument("--serve-rates", default="50,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--no-classic-fri", dest="classic_fri", action="store_false",
                     help="skip the classic DEEP-FRI timing")
@@ -918,6 +1050,7 @@ def main():
         else None
     rsa = rsa2048(sg, ctx, args.rsa_jobs, args.rsa_stacked, cpu_threads) if single and args.rsa_jobs > 0 else None
     ecdsa = p256_ecdsa(sg, ctx, args.ecdsa_jobs, cpu_threads) if single and args.ecdsa_jobs > 0 else None
+    ed = ed25519(sg, ctx, args.ed25519_jobs, cpu_threads) if single and args.ed25519_jobs > 0 else None
     checks = record_checks(sg, ctx, args.record_checks, 16) if single and args.record_checks > 0 else None
     serve = None
     if single and args.serve_jobs > 0:
@@ -958,6 +1091,7 @@ def main():
             "sha256_large_trace": large,
             "rsa2048": rsa,
             "p256_ecdsa": ecdsa,
+            "ed25519": ed,
             "record_checks": checks,
             "serving": serve,
             "classic_fri": classic,
