@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <map>
 #include <cstring>
+#include <exception>
 #include <thread>
 
 #include "bigint.hpp"
@@ -749,11 +750,11 @@ Program make_program(const Layout& L, const uint8_t* s_bits, const uint8_t* k_bi
 // of the row's phase are recorded on the phase's first row (every row of a phase
 // emits the same cells in the same order).
 struct Emit {
-  Witness& W;
+  std::vector<uint64_t>& words;
   uint32_t* codes;  // this phase's width codes, or null once recorded
   uint32_t nw = 0;
   uint32_t word(uint64_t v) {
-    W.words.push_back(v);
+    words.push_back(v);
     return nw++;
   }
   void set(uint32_t col, uint32_t c) {
@@ -950,6 +951,15 @@ Pt fill_point_double(Emit& e, const PDbl& g, const Pt& p) {
 
 }  // namespace
 
+namespace {
+// The words of consecutive ladder rows and where each row's words start.
+struct LadderChunk {
+  std::vector<uint64_t> words;
+  std::vector<uint32_t> start;
+  std::exception_ptr err;
+};
+}  // namespace
+
 void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, uint64_t len, uint32_t k,
                    Witness* w) {
   require(pub && sig && (msg || len == 0), "ed25519: null argument");
@@ -979,8 +989,20 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
   ladder_bits(k_can, k, k_bits.data());
   W.prog = make_program(L, s_bits.data(), k_bits.data(), r_y, r_sign, a_y, a_sign, A);
 
-  // natively computed points (fill_verify_air_v11..v16)
-  const Pt sB = ladder(basepoint(), s_bits.data(), k), kA = ladder(A, k_bits.data(), k);
+  // natively computed points (fill_verify_air_v11..v16): the accumulator entering each
+  // of the 2k ladder rows (padd and pdbl follow the gadgets' formulas, so the points
+  // are the ones the rows compute), sB = [s]B and kA = [k]A
+  const uint32_t n_lad = 2 * k;
+  std::vector<Pt> acc_in(n_lad);
+  Pt sB = identity(), kA = identity();
+  for (uint32_t j = 0; j < k; ++j) {
+    acc_in[j] = sB;
+    acc_in[k + j] = kA;
+    sB = pdbl(sB);
+    if (s_bits[j]) sB = padd(sB, basepoint());
+    kA = pdbl(kA);
+    if (k_bits[j]) kA = padd(kA, A);
+  }
   const Pt Rt{R.X, R.Y, fe(1), mul(R.X, R.Y)};
   const Pt res1 = padd(sB, pneg(Rt)), res2 = padd(res1, pneg(kA));
 
@@ -1006,13 +1028,61 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
   W.row_phase.assign(L.height, PH_IDLE);
   W.row_off.assign(L.height + 1, 0);
   W.words.clear();
-  W.words.reserve((size_t)2 * k * 800 + 8192);
   std::vector<bool> recorded(N_PHASES, false);
   uint32_t d[NL], d2[NL], one[NL], zero[NL] = {0};
   limbs_of(D(), d);
   for (int i = 0; i < NL; ++i) d2[i] = 2 * d[i];
   limbs_of(fe(1), one);
-  Pt acc_s = identity(), acc_k = identity();
+  // The 2k ladder rows (fill_scalar_mult_trace, ed25519_scalar_mult_air.rs:133-171,
+  // and the v6 shift chain) in parallel chunks, each emitting its rows' words into
+  // its own buffer from the accumulators computed above.
+  require(L.kA_first == L.sB_first + k && L.kA_last == L.kA_first + k - 1, "ed25519: ladder rows");
+  const uint32_t n_thr = std::max(1u, std::min({16u, std::thread::hardware_concurrency(), n_lad / 16}));
+  const uint32_t per_chunk = (n_lad + n_thr - 1) / n_thr;
+  std::vector<LadderChunk> chunks((n_lad + per_chunk - 1) / per_chunk);
+  auto run_chunk = [&](uint32_t ci) {
+    LadderChunk& ch = chunks[ci];
+    try {
+      const uint32_t g0 = ci * per_chunk, g1 = std::min(n_lad, g0 + per_chunk);
+      ch.words.reserve((size_t)(g1 - g0) * (k + 1024));
+      for (uint32_t g = g0; g < g1; ++g) {
+        const bool sb = g < k;
+        const uint32_t j = sb ? g : g - k;
+        const uint32_t ph = sb ? PH_SB : PH_KA;
+        ch.start.push_back((uint32_t)ch.words.size());
+        Emit e{ch.words, j == 0 ? &W.codes[(size_t)ph * L.width] : nullptr};
+        const Pt& base = sb ? basepoint() : A;
+        const uint8_t* bits = sb ? s_bits.data() : k_bits.data();
+        const Pt& acc = acc_in[g];
+        const PtL bl = limbs_pt(base), al = limbs_pt(acc);
+        for (int q = 0; q < 4; ++q) e.limbs(L.base[q], bl.l[q]);
+        for (int q = 0; q < 4; ++q) e.limbs(L.acc[q], al.l[q]);
+        const Pt dbl = fill_point_double(e, L.mdbl, acc);
+        const Pt tmp = fill_point_add(e, L.cadd.add, dbl, base, d2);
+        const PtL dl = limbs_pt(dbl), tl = limbs_pt(tmp);
+        for (int q = 0; q < 4; ++q) fill_sel(e, L.cadd.sel[q], dl.l[q], tl.l[q], bits[j]);
+        const uint32_t blk = sb ? L.sblock_sB : L.sblock_kA;
+        for (uint32_t i = 0; i < k; ++i) e.value(blk + i, j + i < k ? bits[j + i] : 0);
+      }
+      ch.start.push_back((uint32_t)ch.words.size());
+    } catch (...) {
+      ch.err = std::current_exception();
+    }
+  };
+  {
+    std::vector<std::thread> th;
+    for (uint32_t ci = 1; ci < chunks.size(); ++ci) th.emplace_back(run_chunk, ci);
+    run_chunk(0);
+    for (auto& t : th) t.join();
+    for (const LadderChunk& ch : chunks)
+      if (ch.err) std::rethrow_exception(ch.err);
+  }
+  recorded[PH_SB] = recorded[PH_KA] = true;
+  {
+    size_t lad_words = 0;
+    for (const LadderChunk& ch : chunks) lad_words += ch.words.size();
+    W.words.reserve(lad_words + 65536);
+  }
   for (uint32_t row = 0; row < L.height; ++row) {
     W.row_off[row] = (uint32_t)W.words.size();
     uint32_t ph = PH_IDLE;
@@ -1027,7 +1097,7 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
     else if (row >= L.dbl_row[0] && row <= L.dbl_row[2]) ph = PH_DBL;
     else if (row == L.result_row) ph = PH_RESULT;
     W.row_phase[row] = (uint8_t)ph;
-    Emit e{W, recorded[ph] ? nullptr : &W.codes[(size_t)ph * L.width]};
+    Emit e{W.words, recorded[ph] ? nullptr : &W.codes[(size_t)ph * L.width]};
     recorded[ph] = true;
     switch (ph) {
       case PH_DIGEST:  // v1: the digest's bits, LSB first within each big-endian word
@@ -1112,22 +1182,11 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
         break;
       }
       case PH_SB:
-      case PH_KA: {  // fill_scalar_mult_trace (ed25519_scalar_mult_air.rs:133-171) and the v6 shift chain
-        const bool sb = ph == PH_SB;
-        const uint32_t j = row - (sb ? L.sB_first : L.kA_first);
-        const Pt& base = sb ? basepoint() : A;
-        Pt& acc = sb ? acc_s : acc_k;
-        const uint8_t* bits = sb ? s_bits.data() : k_bits.data();
-        const PtL bl = limbs_pt(base), al = limbs_pt(acc);
-        for (int q = 0; q < 4; ++q) e.limbs(L.base[q], bl.l[q]);
-        for (int q = 0; q < 4; ++q) e.limbs(L.acc[q], al.l[q]);
-        const Pt dbl = fill_point_double(e, L.mdbl, acc);
-        const Pt tmp = fill_point_add(e, L.cadd.add, dbl, base, d2);
-        const PtL dl = limbs_pt(dbl), tl = limbs_pt(tmp);
-        for (int q = 0; q < 4; ++q) fill_sel(e, L.cadd.sel[q], dl.l[q], tl.l[q], bits[j]);
-        acc = bits[j] ? tmp : dbl;
-        const uint32_t blk = sb ? L.sblock_sB : L.sblock_kA;
-        for (uint32_t i = 0; i < k; ++i) e.value(blk + i, j + i < k ? bits[j + i] : 0);
+      case PH_KA: {  // filled by the ladder chunks: copy this row's words
+        const uint32_t g = row - L.sB_first;  // sB rows, then kA rows, contiguous
+        const LadderChunk& ch = chunks[g / per_chunk];
+        const uint32_t r = g % per_chunk;
+        W.words.insert(W.words.end(), ch.words.begin() + ch.start[r], ch.words.begin() + ch.start[r + 1]);
         break;
       }
       case PH_RESIDUAL: {  // v14, v15
