@@ -583,19 +583,21 @@ def ed25519(sg, ctx, n_jobs, cpu_threads):
     return out
 
 
-def serving(sg, ctx, rates, n_jobs, streams, seed=7):
+def serving(sg, ctx, rates, n_jobs, streams, seed=7, ed_max=32):
     """Poisson arrivals of proof requests admitted by the continuous-batching server
-    under a 160 GB HBM budget: 40 % SHA-256 record proofs and 20 % SHA-512 over
-    record-length messages (lognormal, median 120 B, clipped to 40-600 B), 24 %
-    ECDSA-P256 and 16 % RSA-2048 signature checks (the record checks' 60/40
-    signature split); p50/p99 latency from submit to result, and throughput
-    against one proof at a time."""
+    under a 160 GB HBM budget: 35 % SHA-256 record proofs and 20 % SHA-512 over
+    record-length messages (lognormal, median 120 B, clipped to 40-600 B), 21 %
+    ECDSA-P256 and 14 % RSA-2048 signature checks (the record checks' 60/40
+    signature split) and 10 % Ed25519 batches of 16-ed_max signatures (one proof
+    per signature; a batch's latency is its slowest proof's); p50/p99 latency from
+    submit to result, and throughput in requests and proofs against one proof at a
+    time."""
     rng = np.random.default_rng(seed)
     lens = np.clip(np.round(rng.lognormal(np.log(120), 0.6, n_jobs)), 40, 600).astype(int)
     msgs = [rng.integers(0, 256, int(n), dtype=np.uint8).tobytes() for n in lens]
     u = rng.random(n_jobs)
-    kinds = [sg.JOB_SHA512 if x < 0.2 else sg.JOB_P256_ECDSA if x < 0.44 else sg.JOB_RSA2048 if x < 0.6
-             else sg.JOB_SHA256 for x in u]
+    kinds = [sg.JOB_SHA512 if x < 0.2 else sg.JOB_ED25519 if x < 0.3 else sg.JOB_P256_ECDSA if x < 0.51
+             else sg.JOB_RSA2048 if x < 0.65 else sg.JOB_SHA256 for x in u]
     pis = [hashlib.sha3_256(b"serve-%d" % i).digest() for i in range(n_jobs)]
     keys = rsa_keys()
     for i in range(n_jobs):
@@ -604,8 +606,13 @@ def serving(sg, ctx, rates, n_jobs, streams, seed=7):
             msgs[i] = [rec]
         elif kinds[i] == sg.JOB_P256_ECDSA:
             msgs[i], pis[i] = ecdsa_job(sg, 50000 + i)
+        elif kinds[i] == sg.JOB_ED25519:
+            msgs[i] = ed25519_inputs(int(rng.integers(16, ed_max + 1)), 70000 + i)
+    n_proofs = sum(len(m) if k == sg.JOB_ED25519 else 1 for k, m in zip(kinds, msgs))
 
     def prove_one(i):
+        if kinds[i] == sg.JOB_ED25519:
+            return [ctx.prove_ed25519(p, s, m, pis[i]) for p, s, m in msgs[i]]
         if kinds[i] == sg.JOB_RSA2048:
             return ctx.prove_rsa2048(msgs[i], pis[i])
         if kinds[i] == sg.JOB_P256_ECDSA:
@@ -614,19 +621,26 @@ def serving(sg, ctx, rates, n_jobs, streams, seed=7):
         f = ctx.prove_sha512 if kinds[i] == sg.JOB_SHA512 else ctx.prove_sha256
         return f(msgs[i], pis[i])[0]
 
+    def flat_jobs(i):
+        if kinds[i] == sg.JOB_ED25519:
+            return [(kinds[i], psm, pis[i]) for psm in msgs[i]]
+        return [(kinds[i], msgs[i], pis[i])]
+
     alone = {i: prove_one(i) for i in range(12)}  # reference bytes, one at a time
     # one burst at the serving concurrency grows the device memory pool to its
     # steady-state size before anything is timed
-    ctx.prove_batch([(kinds[i], msgs[i], pis[i]) for i in range(min(n_jobs, 4 * streams))], n_streams=streams,
-                    hbm_budget_bytes=160 << 30)
+    burst = [j for i in range(n_jobs) for j in flat_jobs(i)][:4 * streams]
+    ctx.prove_batch(burst, n_streams=streams, hbm_budget_bytes=160 << 30)
     t0 = time.perf_counter()
     for i in range(n_jobs):
         prove_one(i)
-    plain = n_jobs / (time.perf_counter() - t0)
-    out = {"workload": "40 % SHA-256 and 20 % SHA-512 AIR proofs of messages lognormal(median 120 B) clipped "
-                       "40-600 B, 24 % ECDSA-P256 and 16 % RSA-2048 signature-check proofs; Poisson arrivals",
-           "jobs_per_rate": n_jobs, "streams": streams, "hbm_budget_gb": 160, "plain_proofs_per_s": plain,
-           "rates": []}
+    plain_s = time.perf_counter() - t0
+    plain = n_jobs / plain_s
+    out = {"workload": "35 % SHA-256 and 20 % SHA-512 AIR proofs of messages lognormal(median 120 B) clipped "
+                       "40-600 B, 21 % ECDSA-P256 and 14 % RSA-2048 signature-check proofs, 10 % Ed25519 batches "
+                       f"of 16-{ed_max} signatures (one proof each); Poisson arrivals",
+           "jobs_per_rate": n_jobs, "proofs_per_rate": n_proofs, "streams": streams, "hbm_budget_gb": 160,
+           "plain_proofs_per_s": n_proofs / plain_s, "plain_requests_per_s": plain, "rates": []}
     for lam in rates:
         gaps = rng.exponential(1.0 / lam, n_jobs)
         with sg.Server(ctx, n_streams=streams, hbm_budget_bytes=160 << 30) as srv:
@@ -638,13 +652,19 @@ def serving(sg, ctx, rates, n_jobs, streams, seed=7):
                 wait = due - time.perf_counter()
                 if wait > 0:
                     time.sleep(wait)
-                tickets.append(srv.submit(kinds[i], msgs[i], pis[i]))
-            res = [srv.wait(t) for t in tickets]
+                tickets.append([(time.perf_counter(), srv.submit(*j)) for j in flat_jobs(i)])
+            res, lat = [], []
+            for group in tickets:
+                got = [srv.wait(t) for _, t in group]
+                res.append([p for p, _ in got])
+                # a batch request ends with its last proof: its latency is its slowest job's
+                lat.append(max((ts - group[0][0]) * 1e3 + r.latency_ms for (ts, _), (_, r) in zip(group, got)))
             wall = time.perf_counter() - start
         for i, want in alone.items():
-            assert res[i][0] == want, "a proof in the mix differs from the same proof alone"
-        lat = np.array([r.latency_ms for _, r in res])
-        out["rates"].append({"offered_per_s": lam, "proofs_per_s": n_jobs / wall,
+            got = res[i] if kinds[i] == sg.JOB_ED25519 else res[i][0]
+            assert got == want, "a proof in the mix differs from the same proof alone"
+        lat = np.array(lat)
+        out["rates"].append({"offered_per_s": lam, "requests_per_s": n_jobs / wall, "proofs_per_s": n_proofs / wall,
                              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                              "over_plain": (n_jobs / wall) / plain})
     return out
@@ -760,6 +780,8 @@ def main():
                     help="ECDSA-P256 proofs for the plain-vs-batched section (0 skips it)")
     ap.add_argument("--ed25519-jobs", type=int, default=256,
                     help="Ed25519 signature proofs (config 3: 256 signatures, one proof each; 0 skips)")
+    ap.add_argument("--serve-ed25519-max", type=int, default=32,
+                    help="largest Ed25519 batch (signatures) in the serving mix; the full mix uses 256")
     ap.add_argument("--serve-rates", default="50,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     ap.add_argument("--no-classic-fri", dest="classic_fri", action="store_false",
                     help="skip the classic DEEP-FRI timing")
@@ -1054,7 +1076,8 @@ def main():
     checks = record_checks(sg, ctx, args.record_checks, 16) if single and args.record_checks > 0 else None
     serve = None
     if single and args.serve_jobs > 0:
-        serve = serving(sg, ctx, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs, 16)
+        serve = serving(sg, ctx, [float(r) for r in args.serve_rates.split(",")], args.serve_jobs, 16,
+                        ed_max=args.serve_ed25519_max)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
