@@ -450,10 +450,13 @@ int sg_ed25519_trace_gpu(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[6
  * constants. lde: host or device. */
 int sg_merge_ed25519(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
                      uint32_t k_scalar, const uint64_t* lde, size_t blowup, uint64_t* c_eval);
-/* Proof: witness (host) -> trace (device) -> LDE x blowup -> merge (coset by coset
- * above a 2 GiB LDE unless SG_OPT_WIDE_MERGE says otherwise) -> STIR with
- * build_params(height * blowup, fs_binding), self-verified (prove_zsk_ksk_binding_v2,
- * swarm-dns/src/prover.rs:856-951, with blowup 32 and k_scalar 256). */
+/* Proof: witness (host) -> trace (device) -> LDE x blowup of the columns the merge
+ * reads (the others are filled only at the points that read them) -> merge ->
+ * STIR with build_params(height * blowup, fs_binding), self-verified
+ * (prove_zsk_ksk_binding_v2, swarm-dns/src/prover.rs:856-951, with blowup 32 and
+ * k_scalar 256). The LDE buffer is width x height*blowup (10.9 GB for k_scalar
+ * 256); SG_OPT_WIDE_MERGE = SG_WIDE_MERGE_COSETS streams the merge coset by coset
+ * instead (about 1 GB, twice the time). */
 int sg_prove_ed25519(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
                      const uint8_t fs_binding[32], uint32_t k_scalar, size_t blowup, uint8_t* proof, size_t cap,
                      size_t* len);
