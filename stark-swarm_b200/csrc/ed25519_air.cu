@@ -134,19 +134,30 @@ __device__ void eval_mul(Ctx& x, const EdBlock& g) {
   }
 }
 
+// The loops below load a gadget's cells five limbs at a time before using them,
+// so a warp has tens of loads in flight instead of waiting on each limb's few.
+// Constraint values go into an exact 128-bit sum, so their order is free.
+
 // eval_add_gadget (ed25519_field_air.rs:431-486)
 __device__ void eval_add(Ctx& x, const EdBlock& g) {
   const uint32_t a = g.p[0], b = g.p[1], c = g.p[2], cr = g.p[4], lam = g.lam;
   range(x, c, g.p[3], lam);
-  uint64_t prev = mul_small(x.v(cr + NL - 1), 19);
-#pragma unroll 1
-  for (uint32_t k = 0; k < NL; ++k) {
-    const uint64_t ck = x.v(cr + k);
-    const uint64_t v = gl::sub(gl::add(gl::add(x.v(a + k), x.v(b + k)), prev),
-                               gl::add(x.v(c + k), gl::mul_pow2(ck, (k & 1) ? 25u : 26u)));
-    x.put(lam + 266 + k, v);
-    x.put(lam + 276 + k, gl::mul(ck, gl::sub(1, ck)));
-    prev = ck;
+  uint64_t ck[NL];
+#pragma unroll
+  for (uint32_t k = 0; k < NL; ++k) ck[k] = x.v(cr + k);
+#pragma unroll
+  for (uint32_t h = 0; h < NL; h += 5) {
+    uint64_t av[5], bv[5], cv[5];
+#pragma unroll
+    for (uint32_t j = 0; j < 5; ++j) av[j] = x.v(a + h + j), bv[j] = x.v(b + h + j), cv[j] = x.v(c + h + j);
+#pragma unroll
+    for (uint32_t j = 0; j < 5; ++j) {
+      const uint32_t k = h + j;
+      const uint64_t prev = k == 0 ? mul_small(ck[NL - 1], 19) : ck[k - 1];
+      const uint64_t v = gl::sub(gl::add(gl::add(av[j], bv[j]), prev), gl::add(cv[j], gl::mul_pow2(ck[k], (k & 1) ? 25u : 26u)));
+      x.put(lam + 266 + k, v);
+      x.put(lam + 276 + k, gl::mul(ck[k], gl::sub(1, ck[k])));
+    }
   }
 }
 
@@ -154,17 +165,32 @@ __device__ void eval_add(Ctx& x, const EdBlock& g) {
 __device__ void eval_sub(Ctx& x, const EdBlock& g) {
   const uint32_t a = g.p[0], b = g.p[1], c = g.p[2], pos = g.p[4], neg = g.p[5], lam = g.lam;
   range(x, c, g.p[3], lam);
-  uint64_t prev = mul_small(gl::sub(x.v(pos + NL - 1), x.v(neg + NL - 1)), 19);
-#pragma unroll 1
-  for (uint32_t k = 0; k < NL; ++k) {
-    const uint64_t cp = x.v(pos + k), cn = x.v(neg + k), net = gl::sub(cp, cn);
-    const uint64_t v = gl::add(gl::sub(gl::sub(gl::sub(x.v(a + k), x.v(b + k)), prev), x.v(c + k)),
-                               gl::mul_pow2(net, (k & 1) ? 25u : 26u));
-    x.put(lam + 266 + k, v);
-    x.put(lam + 276 + k, gl::mul(cp, gl::sub(1, cp)));
-    x.put(lam + 286 + k, gl::mul(cn, gl::sub(1, cn)));
-    x.put(lam + 296 + k, gl::mul(cp, cn));
-    prev = net;
+  uint64_t net[NL];
+  {
+    uint64_t cp[NL], cn[NL];
+#pragma unroll
+    for (uint32_t k = 0; k < NL; ++k) cp[k] = x.v(pos + k), cn[k] = x.v(neg + k);
+#pragma unroll
+    for (uint32_t k = 0; k < NL; ++k) {
+      net[k] = gl::sub(cp[k], cn[k]);
+      x.put(lam + 276 + k, gl::mul(cp[k], gl::sub(1, cp[k])));
+      x.put(lam + 286 + k, gl::mul(cn[k], gl::sub(1, cn[k])));
+      x.put(lam + 296 + k, gl::mul(cp[k], cn[k]));
+    }
+  }
+#pragma unroll
+  for (uint32_t h = 0; h < NL; h += 5) {
+    uint64_t av[5], bv[5], cv[5];
+#pragma unroll
+    for (uint32_t j = 0; j < 5; ++j) av[j] = x.v(a + h + j), bv[j] = x.v(b + h + j), cv[j] = x.v(c + h + j);
+#pragma unroll
+    for (uint32_t j = 0; j < 5; ++j) {
+      const uint32_t k = h + j;
+      const uint64_t prev = k == 0 ? mul_small(net[NL - 1], 19) : net[k - 1];
+      const uint64_t v = gl::add(gl::sub(gl::sub(gl::sub(av[j], bv[j]), prev), cv[j]),
+                                 gl::mul_pow2(net[k], (k & 1) ? 25u : 26u));
+      x.put(lam + 266 + k, v);
+    }
   }
 }
 
@@ -173,10 +199,14 @@ __device__ void eval_sel(Ctx& x, const EdBlock& g) {
   const uint32_t a = g.p[0], b = g.p[1], c = g.p[3], lam = g.lam;
   const uint64_t s = x.v(g.p[2]);
   x.put(lam + 1, gl::mul(s, gl::sub(1, s)));
-#pragma unroll 1
-  for (uint32_t k = 0; k < NL; ++k) {
-    const uint64_t ak = x.v(a + k);
-    x.put(lam + 2 + k, gl::sub(gl::sub(x.v(c + k), ak), gl::mul(s, gl::sub(x.v(b + k), ak))));
+#pragma unroll
+  for (uint32_t h = 0; h < NL; h += 5) {
+    uint64_t av[5], bv[5], cv[5];
+#pragma unroll
+    for (uint32_t j = 0; j < 5; ++j) av[j] = x.v(a + h + j), bv[j] = x.v(b + h + j), cv[j] = x.v(c + h + j);
+#pragma unroll
+    for (uint32_t j = 0; j < 5; ++j)
+      x.put(lam + 2 + h + j, gl::sub(gl::sub(cv[j], av[j]), gl::mul(s, gl::sub(bv[j], av[j]))));
   }
 }
 
@@ -186,10 +216,22 @@ __device__ __forceinline__ uint64_t ref(const Ctx& x, uint64_t r) {
   return src == SRC_CUR ? x.v(v) : src == SRC_NXT ? x.w(v) : (r & ((1ull << 62) - 1));
 }
 
+// Pairs go in batches of 8: the batch's 16 references (the same for the whole warp)
+// are read first, then its up to 16 cells, then the 8 differences.
 __device__ void eval_pairs(Ctx& x, const EdBlock& g, const uint64_t* pairs) {
+  constexpr uint32_t kB = 8;
   const uint32_t off = g.p[0], cnt = g.p[1];
-#pragma unroll 4
-  for (uint32_t i = 0; i < cnt; ++i) {
+  uint32_t i = 0;
+  for (; i + kB <= cnt; i += kB) {
+    uint64_t r[2 * kB], v[2 * kB];
+#pragma unroll
+    for (uint32_t j = 0; j < 2 * kB; ++j) r[j] = __ldg(pairs + 2 * (off + i) + j);
+#pragma unroll
+    for (uint32_t j = 0; j < 2 * kB; ++j) v[j] = ref(x, r[j]);
+#pragma unroll
+    for (uint32_t j = 0; j < kB; ++j) x.put(g.lam + 1 + i + j, gl::sub(v[2 * j], v[2 * j + 1]));
+  }
+  for (; i < cnt; ++i) {
     const uint64_t ra = __ldg(pairs + 2 * (off + i)), rb = __ldg(pairs + 2 * (off + i) + 1);
     x.put(g.lam + 1 + i, gl::sub(ref(x, ra), ref(x, rb)));
   }

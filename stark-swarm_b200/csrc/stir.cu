@@ -29,39 +29,36 @@ inline uint64_t ood_blocks(uint64_t n, int m) {
 }
 
 // Thread tid accumulates T_r over groups t = tid, tid + S, ... (S = all threads),
-// starting from w^tid and stepping by w^S: consecutive threads read consecutive
-// groups of M coefficients. w^tid = w^{256 block} w^{tid mod 16} w^{16 (tid / 16 mod 16)},
-// the 33 factors computed once per CTA by 33 threads.
-// Proof groups (grid.y = proof g): with sc set, proof g's powers come from sc[g]
-// and its coefficients / partials start g_c / g_p elements further on.
+// starting from w^tid = w^(256 block) w^(tid mod 256) and stepping by w^S:
+// consecutive threads read consecutive groups of M coefficients. The factors come
+// from the scalars' tables (three products deep).
+// Proof groups (grid.y = proof g): with sc set, proof g's scalars are sc[g] and its
+// coefficients / partials start g_c / g_p elements further on; else they are `one`.
 template <int M, bool BASE>
-__global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t* c, uint64_t n, gl::Fp6 w,
-                                                                   gl::Fp6 w_stride, uint64_t* partials,
+__global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t* c, uint64_t n,
+                                                                   const OodScalars one, uint64_t* partials,
                                                                    const OodScalars* sc, uint64_t g_c,
                                                                    uint64_t g_p) {
-  static_assert(kOodThreads == 256, "the power table covers 256 threads");
+  static_assert(kOodThreads == 256, "the factor tables cover 256 threads");
+  const uint32_t b = blockIdx.x, t = threadIdx.x;
+  gl::Fp6 tl, tm, bl, bm, w_stride, w64;
   if (sc) {
     const uint32_t g = blockIdx.y;
-    w = sc[g].w;
-    w_stride = sc[g].ws;
+    const OodScalars& S = sc[g];
+    tl = S.lo[t & 15], tm = S.mid[t >> 4], bl = S.blo[b & 15], bm = S.bmid[(b >> 4) & 15];
+    w_stride = S.ws, w64 = S.w65536;
     c += g * g_c;
     partials += g * g_p;
+  } else {
+    tl = one.lo[t & 15], tm = one.mid[t >> 4], bl = one.blo[b & 15], bm = one.bmid[(b >> 4) & 15];
+    w_stride = one.ws, w64 = one.w65536;
   }
   const uint64_t n_groups = n / M;
   const uint64_t S = (uint64_t)gridDim.x * kOodThreads;
-  const uint64_t tid = (uint64_t)blockIdx.x * kOodThreads + threadIdx.x;
-  __shared__ gl::Fp6 pw[33];
-  {
-    const int t = threadIdx.x;
-    if (t < 16)
-      pw[t] = gl::e_pow(w, (uint64_t)t);
-    else if (t < 32)
-      pw[t] = gl::e_pow(w, (uint64_t)16 * (t - 16));
-    else if (t == 32)
-      pw[32] = gl::e_pow(w, (uint64_t)blockIdx.x * kOodThreads);
-  }
-  __syncthreads();
-  gl::Fp6 wt = gl::e_mul(pw[32], gl::e_mul(pw[threadIdx.x & 15], pw[16 + (threadIdx.x >> 4)]));
+  const uint64_t tid = (uint64_t)b * kOodThreads + t;
+  gl::Fp6 bf = gl::e_mul(bl, bm);
+  if (b >= 256) bf = gl::e_mul(bf, gl::e_pow(w64, b >> 8));
+  gl::Fp6 wt = gl::e_mul(bf, gl::e_mul(tl, tm));
   uint64_t acc[M][6];
 #pragma unroll
   for (int r = 0; r < M; ++r)
@@ -104,27 +101,61 @@ __global__ void __launch_bounds__(kOodThreads) ood_partial_kernel(const uint64_t
   }
 }
 
+// evals[j] = sum_r w_M^{jr} z^r T_r for j < M, with T (M x 6 words) in shared
+// memory: thread r < M forms z^r T_r into U (zt = its z^r), then thread j adds
+// the M terms times powers of two (w_M = 2^EM).
+// Every thread of the block calls it (it holds a barrier).
+template <int M>
+__device__ __forceinline__ void ood_evals(const uint64_t* T, uint64_t* U, const gl::Fp6& zt, uint64_t* evals) {
+  const int t = threadIdx.x;
+  if (t < M) {
+    gl::Fp6 tr;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) tr.c[q] = T[t * 6 + q];
+    const gl::Fp6 u = gl::e_mul(zt, tr);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) U[t * 6 + q] = u.c[q];
+  }
+  __syncthreads();
+  if (t >= M) return;
+  constexpr unsigned EM = (exp16(false) * (16 / M)) % 192;
+  gl::Fp6 acc = gl::e_zero();
+#pragma unroll
+  for (int r = 0; r < M; ++r) {
+    const unsigned e = (EM * (unsigned)((t * r) % M)) % 192u;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc.c[q] = gl::add(acc.c[q], gl::mul_pow2(U[r * 6 + q], e));
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) evals[t * 6 + q] = acc.c[q];
+}
+
 // Small layers (at most kOodSmallGroups groups): one CTA of M warps. Warp r sums
 // T_r = sum_t c_{tM+r} w^t with its lanes striding over t (lane l starts at w^l and
-// steps by w^32), then M threads form evals[j] = sum_r w_M^{jr} z^r T_r. Fp6
-// products go through e_mul_call so the kernel's code stays small: it runs once.
-constexpr uint64_t kOodSmallGroups = 4096;
+// steps by w^32), then ood_evals forms evals[j] = sum_r w_M^{jr} z^r T_r.
+// Each lane's loop waits on its loads every iteration with only M warps on the SM,
+// so the bound is kept at 8 iterations: a 4096-group layer took 0.14 ms here and
+// takes a few microseconds through the partial and finish kernels.
+constexpr uint64_t kOodSmallGroups = 256;
 template <int M, bool BASE>
-__global__ void __launch_bounds__(M * 32) ood_small_kernel(const uint64_t* c, uint64_t n, gl::Fp6 w, gl::Fp6 w32,
-                                                           gl::Fp6 z, uint64_t* evals, const OodScalars* sc,
-                                                           uint64_t g_c, uint64_t g_e) {
+__global__ void __launch_bounds__(M * 32) ood_small_kernel(const uint64_t* c, uint64_t n, const OodScalars one,
+                                                           uint64_t* evals, const OodScalars* sc, uint64_t g_c,
+                                                           uint64_t g_e) {
+  const int lane0 = threadIdx.x & 31, t0 = threadIdx.x < M ? threadIdx.x : 0;
+  gl::Fp6 tl, tm, w32, zt;
   if (sc) {
     const uint32_t g = blockIdx.x;  // one CTA per proof
-    w = sc[g].w;
-    w32 = sc[g].w32;
-    z = sc[g].z;
+    const OodScalars& S = sc[g];
+    tl = S.lo[lane0 & 15], tm = S.mid[lane0 >> 4], w32 = S.w32, zt = S.zr[t0];
     c += g * g_c;
     evals += g * g_e;
+  } else {
+    tl = one.lo[lane0 & 15], tm = one.mid[lane0 >> 4], w32 = one.w32, zt = one.zr[t0];
   }
   const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
   const uint64_t n_groups = n / M;
   __shared__ uint64_t T[M * 6];
-  gl::Fp6 wt = gl::e_pow_call(w, (uint64_t)lane);
+  gl::Fp6 wt = gl::e_mul(tl, tm);
   uint64_t acc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll 1
   for (uint64_t t = lane; t < n_groups; t += 32) {
@@ -137,11 +168,11 @@ __global__ void __launch_bounds__(M * 32) ood_small_kernel(const uint64_t* c, ui
       gl::Fp6 ck;
 #pragma unroll
       for (int q = 0; q < 6; ++q) ck.c[q] = __ldg(c + (uint64_t)q * n + k);
-      const gl::Fp6 p = gl::e_mul_call(ck, wt);
+      const gl::Fp6 p = gl::e_mul(ck, wt);
 #pragma unroll
       for (int q = 0; q < 6; ++q) acc[q] = gl::add(acc[q], p.c[q]);
     }
-    wt = gl::e_mul_call(wt, w32);
+    wt = gl::e_mul(wt, w32);
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
@@ -149,35 +180,23 @@ __global__ void __launch_bounds__(M * 32) ood_small_kernel(const uint64_t* c, ui
     if (lane == 0) T[r * 6 + q] = v;
   }
   __syncthreads();
-  const int j = threadIdx.x;
-  if (j >= M) return;
-  constexpr unsigned EM = (exp16(false) * (16 / M)) % 192;  // w_M = 2^EM
-  gl::Fp6 out = gl::e_zero(), zr = gl::e_one();
-#pragma unroll 1
-  for (int rr = 0; rr < M; ++rr) {
-    gl::Fp6 tr;
-#pragma unroll
-    for (int q = 0; q < 6; ++q) tr.c[q] = T[rr * 6 + q];
-    gl::Fp6 sv = gl::e_mul_call(zr, tr);
-    const unsigned e = (EM * (unsigned)((j * rr) % M)) % 192u;
-#pragma unroll
-    for (int q = 0; q < 6; ++q) sv.c[q] = gl::mul_pow2(sv.c[q], e);
-    out = gl::e_add(out, sv);
-    zr = gl::e_mul_call(zr, z);
-  }
-#pragma unroll
-  for (int q = 0; q < 6; ++q) evals[j * 6 + q] = out.c[q];
+  __shared__ uint64_t U[M * 6];
+  ood_evals<M>(T, U, zt, evals);
 }
 
 // Sum block partials into T_r, then evals[j] = sum_r w_M^{jr} z^r T_r.
 template <int M>
-__global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, gl::Fp6 z, uint64_t* evals,
-                                  const OodScalars* sc, uint64_t g_p, uint64_t g_e) {
+__global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, const OodScalars one,
+                                  uint64_t* evals, const OodScalars* sc, uint64_t g_p, uint64_t g_e) {
+  const int t0 = threadIdx.x < M ? threadIdx.x : 0;
+  gl::Fp6 zt;
   if (sc) {
     const uint32_t g = blockIdx.x;  // one CTA per proof
-    z = sc[g].z;
+    zt = sc[g].zr[t0];
     partials += g * g_p;
     evals += g * g_e;
+  } else {
+    zt = one.zr[t0];
   }
   __shared__ uint64_t T[M * 6];
   // one warp per element: the lanes stride over the block partials
@@ -189,24 +208,8 @@ __global__ void ood_finish_kernel(const uint64_t* partials, uint64_t n_blocks, g
     if (lane == 0) T[e] = v;
   }
   __syncthreads();
-  const int j = threadIdx.x;
-  if (j >= M) return;
-  constexpr unsigned EM = (exp16(false) * (16 / M)) % 192;  // w_M = 2^EM
-  gl::Fp6 acc = gl::e_zero(), zr = gl::e_one();
-#pragma unroll 1
-  for (int r = 0; r < M; ++r) {
-    gl::Fp6 tr;
-#pragma unroll
-    for (int q = 0; q < 6; ++q) tr.c[q] = T[r * 6 + q];
-    gl::Fp6 s = gl::e_mul_call(zr, tr);
-    const unsigned e = (EM * (unsigned)((j * r) % M)) % 192u;
-#pragma unroll
-    for (int q = 0; q < 6; ++q) s.c[q] = gl::mul_pow2(s.c[q], e);
-    acc = gl::e_add(acc, s);
-    zr = gl::e_mul_call(zr, z);
-  }
-#pragma unroll
-  for (int q = 0; q < 6; ++q) evals[j * 6 + q] = acc.c[q];
+  __shared__ uint64_t U[M * 6];
+  ood_evals<M>(T, U, zt, evals);
 }
 
 // proof g = blockIdx.y of a group: its buffers and challenge (FoldArgs' g_* strides)
@@ -375,35 +378,34 @@ __global__ void fold_tuples_kernel(const uint64_t* tup, uint64_t nf, gl::Fp6 alp
   for (int q = 0; q < 6; ++q) next[(uint64_t)q * nf + b] = acc.c[q];
 }
 
-// One proof (sc null: powers from z on the host) or a group of G proofs (sc set).
+// One proof (sc null: its scalars built here from z and passed by value) or a
+// group of G proofs (sc set: their scalars in device memory).
 template <int M>
 cudaError_t ood_launch(const uint64_t* c, uint64_t g_c, bool base, uint64_t n, const gl::Fp6& z,
                        const OodScalars* sc, uint64_t* partials, uint64_t* evals, uint64_t g_e, uint32_t G,
                        cudaStream_t s) {
-  gl::Fp6 w = gl::e_zero(), w32 = w, ws = w;
-  if (!sc) w = gl::e_pow(z, M);
+  const OodScalars one = sc ? OodScalars{} : ood_scalars(z, n, M);
   if (n / M <= kOodSmallGroups) {
-    if (!sc) w32 = gl::e_pow(w, 32);
     SG_LAUNCH_SCOPE("stir_ood", s);
     if (base)
-      ood_small_kernel<M, true><<<G, M * 32, 0, s>>>(c, n, w, w32, z, evals, sc, g_c, g_e);
+      ood_small_kernel<M, true><<<G, M * 32, 0, s>>>(c, n, one, evals, sc, g_c, g_e);
     else
-      ood_small_kernel<M, false><<<G, M * 32, 0, s>>>(c, n, w, w32, z, evals, sc, g_c, g_e);
+      ood_small_kernel<M, false><<<G, M * 32, 0, s>>>(c, n, one, evals, sc, g_c, g_e);
     return cudaGetLastError();
   }
   const uint64_t blocks = ood_blocks(n, M), g_p = blocks * M * 6;
-  if (!sc) ws = gl::e_pow(w, blocks * kOodThreads);
+  if (blocks > 65535) return cudaErrorInvalidValue;
   {
     SG_LAUNCH_SCOPE("stir_ood", s);
     if (base)
-      ood_partial_kernel<M, true><<<dim3((unsigned)blocks, G), kOodThreads, 0, s>>>(c, n, w, ws, partials, sc, g_c,
+      ood_partial_kernel<M, true><<<dim3((unsigned)blocks, G), kOodThreads, 0, s>>>(c, n, one, partials, sc, g_c,
                                                                                      g_p);
     else
-      ood_partial_kernel<M, false><<<dim3((unsigned)blocks, G), kOodThreads, 0, s>>>(c, n, w, ws, partials, sc,
+      ood_partial_kernel<M, false><<<dim3((unsigned)blocks, G), kOodThreads, 0, s>>>(c, n, one, partials, sc,
                                                                                       g_c, g_p);
   }
   SG_LAUNCH_SCOPE("stir_ood_finish", s);
-  ood_finish_kernel<M><<<G, 256, 0, s>>>(partials, blocks, z, evals, sc, g_p, g_e);
+  ood_finish_kernel<M><<<G, 256, 0, s>>>(partials, blocks, one, evals, sc, g_p, g_e);
   return cudaGetLastError();
 }
 
@@ -446,9 +448,21 @@ cudaError_t ood_evaluate(const uint64_t* coeffs, bool base, uint64_t n, int m, c
 OodScalars ood_scalars(const gl::Fp6& z, uint64_t n, int m) {
   OodScalars r;
   r.z = z;
-  r.w = gl::e_pow(z, (uint64_t)m);
-  r.w32 = gl::e_pow(r.w, 32);
-  r.ws = gl::e_pow(r.w, ood_blocks(n, m) * kOodThreads);
+  // t-th powers of x for t < 16, and x^16
+  auto powers = [](const gl::Fp6& x, gl::Fp6* out) {
+    out[0] = gl::e_one();
+    for (int t = 1; t < 16; ++t) out[t] = gl::e_mul(out[t - 1], x);
+    return gl::e_mul(out[15], x);
+  };
+  const gl::Fp6 z16 = powers(z, r.zr);
+  r.w = m == 16 ? z16 : r.zr[m];
+  const gl::Fp6 w16 = powers(r.w, r.lo);
+  const gl::Fp6 w256 = powers(w16, r.mid);
+  const gl::Fp6 w4096 = powers(w256, r.blo);
+  r.w65536 = powers(w4096, r.bmid);
+  r.w32 = r.mid[2];
+  const uint64_t S = ood_blocks(n, m) * kOodThreads;  // w^S = w^(256 b) for b = S / 256 blocks
+  r.ws = gl::e_mul(gl::e_mul(r.blo[(S >> 8) & 15], r.bmid[(S >> 12) & 15]), gl::e_pow(r.w65536, S >> 16));
   return r;
 }
 

@@ -61,8 +61,15 @@ cudaError_t fold_tuples_group(const uint64_t* tuples, uint64_t g_tup, uint64_t n
 // proof g's coefficients at coeffs + g g_c, its evaluations at evals + g g_e,
 // its point and the powers the kernels use in sc[g] (device memory, filled
 // from ood_scalars). partials: n_proofs * ood_partials_len(n, m).
+// Beside z and w = z^m, the powers the kernels read instead of forming them by
+// chains of Fp6 products (a dependent Fp6 product costs microseconds on one
+// thread): z^r (r < m); a thread's factor w^t (t < 256) = lo[t & 15] mid[t >> 4];
+// a partial-pass block's factor w^(256 b) = blo[b & 15] bmid[(b >> 4) & 15]
+// (b < 256), times w65536^(b >> 8) beyond.
 struct OodScalars {
   gl::Fp6 z, w, w32, ws;  // z, w = z^m, w^32, w^(threads of the partial pass)
+  gl::Fp6 w65536;
+  gl::Fp6 zr[16], lo[16], mid[16], blo[16], bmid[16];
 };
 OodScalars ood_scalars(const gl::Fp6& z, uint64_t n, int m);
 cudaError_t ood_evaluate_group(const uint64_t* coeffs, uint64_t g_c, bool base, uint64_t n, int m,
