@@ -2,8 +2,9 @@
 library allocate device memory (its buffers come from file-scope static
 device arrays). Checked through the C ABI against sg_ntt, the allocating entry
 point, on two calls in a row -- the second call reuses the static scratch the
-first one left behind. Results are exact field elements, so the tolerance is
-zero. This file is named to be collected last."""
+first one left behind -- and against the oracle's transform in both directions.
+Results are exact field elements, so the tolerance is zero. This file is named
+to be collected last."""
 import ctypes
 
 import numpy as np
@@ -36,6 +37,25 @@ def test_noalloc_ntt_matches_allocating_entry_point(sgpu, ctx, cols, log_n, inve
         assert rc == sgpu.SG_OK, rc
         torch.cuda.synchronize()
         assert torch.equal(out, want), f"call {call}"
+
+
+@pytest.mark.parametrize("cols,log_n", [(2, 16), (1, 20), (3, 11)])
+@pytest.mark.parametrize("inverse", [0, 1])
+def test_noalloc_ntt_matches_oracle(sgpu, cols, log_n, inverse):
+    # each column against the oracle's transform (ark-poly radix-2 domain semantics)
+    import oracle_lib as O
+    torch = pytest.importorskip("torch")
+    L = sgpu.lib()
+    x = _rand(torch, cols, log_n, 77 + 10 * cols + log_n)
+    out = torch.full_like(x, -1)
+    rc = L.sg_ntt_noalloc(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), cols, log_n, inverse,
+                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == sgpu.SG_OK, rc
+    torch.cuda.synchronize()
+    xh = x.cpu().numpy().view(np.uint64)
+    got = out.cpu().numpy().view(np.uint64)
+    for c in range(cols):
+        assert np.array_equal(got[c], O.ntt(xh[c], bool(inverse))), c
 
 
 def test_noalloc_ntt_in_place_round_trip(sgpu):
