@@ -530,8 +530,9 @@ def ed25519(sg, ctx, n_jobs, cpu_threads):
     """Ed25519 signature-verification proofs (prove_zsk_ksk_binding_v2: the v16 verify
     AIR, k_scalar 256, 1024 rows of 41,519 cells and 70,606 constraints, blowup 32,
     n0 32768): n_jobs signatures of 32-byte messages (keys and messages from seed 5),
-    one STARK per signature as in the reference, one at a time vs 8 in flight; each
-    job is host signature in, proof bytes out, natively checked first and self-verified.
+    one STARK per signature as in the reference, one at a time vs 8 in flight (and 8
+    in flight with lockstep STIR groups of 8); each job is host signature in, proof
+    bytes out, natively checked first and self-verified.
     Beside it: one proof's latency and kernel breakdown, and the CPU oracle's full-size
     proof of the same signature (measured, not scaled) next to the reference's published
     105.01 s per proof."""
@@ -557,15 +558,25 @@ def ed25519(sg, ctx, n_jobs, cpu_threads):
     prof = sg.profile_read()
     sg.profile_enable(False)
     out["kernels_ms"] = {kname: round(v[1], 3) for kname, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:10]}
-    for label, streams in (("plain", 1), ("batched", 8)):
-        t0 = time.perf_counter()
-        res = ctx.prove_batch(jobs, n_streams=streams, hbm_budget_bytes=160 << 30)
-        dt = time.perf_counter() - t0
+    # grouped: 8 in flight, and each worker proves the STIR phases of up to 8 queued
+    # proofs (all of n0 32768) in lockstep
+    got = {}
+    for label, streams, group in (("plain", 1, 1), ("batched", 8, 1), ("grouped", 8, 8)):
+        ctx.set_option(sg.OPT_STIR_GROUP, group)
+        try:
+            t0 = time.perf_counter()
+            res = ctx.prove_batch(jobs, n_streams=streams, hbm_budget_bytes=160 << 30)
+            dt = time.perf_counter() - t0
+        finally:
+            ctx.set_option(sg.OPT_STIR_GROUP, 1)
         assert all(r.status == 0 for _, r in res)
+        got[label] = [p for p, _ in res]
         ls = sorted(r.latency_ms for _, r in res)
-        out[label] = {"streams": streams, "proofs_per_s": n_jobs / dt, "p50_ms": ls[len(ls) // 2],
-                      "p99_ms": ls[min(len(ls) - 1, int(len(ls) * 0.99))]}
+        out[label] = {"streams": streams, "stir_group": group, "proofs_per_s": n_jobs / dt,
+                      "p50_ms": ls[len(ls) // 2], "p99_ms": ls[min(len(ls) - 1, int(len(ls) * 0.99))]}
+    assert got["plain"] == got["batched"] == got["grouped"], "a batched Ed25519 proof differs from the same proof alone"
     out["batched_over_plain"] = out["batched"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
+    out["grouped_over_plain"] = out["grouped"]["proofs_per_s"] / out["plain"]["proofs_per_s"]
     out["plain_over_published_reference"] = out["plain"]["proofs_per_s"] * 105.01
     if cpu_threads:
         E = load_oracle_ed25519()
