@@ -98,6 +98,7 @@ struct PassArgs {
   // back to back over all columns, so they share its tw_tab entries through L2
   bool cols_fast;
   int in_tw_log;              // > 0: input (lane, m) *= w_{2^in_tw_log}^(m*lane)
+  const uint64_t* in_tw_tab;  // if set, that twist is in_tw_tab[m * lane] (m * lane < 2^in_tw_log)
   int out_i_log;              // coset evaluation: out_i = 2^out_i_log
   uint64_t scale;             // != 1: outputs *= scale
   const uint64_t* tw_st;      // w_4096^i (direction of the transform)
@@ -285,11 +286,13 @@ __global__ void __launch_bounds__(1024) ntt_pass_kernel(PassArgs a) {
           // (ntt_coset_eval launches exactly B / K CTAs per column)
           x[q] = __ldg(in + m);
           if (PRE) x[q] = gl::mul(x[q], pow_at(a.pre, (uint64_t)m));
-          // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j)
+          // w_N^e for N <= 2^14 is one entry of the hi table (hi[j] = w_{2^14}^j); above,
+          // one entry of the per-size table when there is one
           const uint64_t ex = (uint64_t)m * lane;
           x[q] = gl::mul(x[q], a.in_tw_log <= kTwSplit
                                    ? __ldg(a.tw_hi + ((ex << (kTwSplit - a.in_tw_log)) & (kTwEntries - 1)))
-                                   : tw_pow(a.tw_lo, a.tw_hi, ex, a.in_tw_log));
+                               : a.in_tw_tab ? __ldg(a.in_tw_tab + ex)
+                                             : tw_pow(a.tw_lo, a.tw_hi, ex, a.in_tw_log));
         } else {
           const uint64_t flat = (uint64_t)m * a.in_m + lane * a.flat_lane;
           if (FULL || (e < E_load && lane < a.n_lanes && flat < a.in_valid)) {
@@ -541,6 +544,36 @@ __global__ void pow_table_kernel(const uint64_t* lo, const uint64_t* hi, uint64_
     tab[k] = tw_pow(lo, hi, k * mult, log_n);
 }
 
+// w_N^j for j < N = 2^log_n (forward), built once per (device, size) and kept for
+// the process: the coset twist w_N^(m t) of ntt_coset_eval above 2^14 points is then
+// one load instead of two table loads and a product (m t < N). Up to 2^20 points
+// (8 MB); none for table views of callers that must not allocate.
+const uint64_t* coset_twist_table(const NttTables& t, int log_n, cudaStream_t s) {
+  if (!t.pass_tables || log_n <= kTwSplit || log_n > 20) return nullptr;
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, uint64_t*> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  const auto key = std::make_pair(dev, log_n);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  uint64_t* d = nullptr;
+  if (cudaMalloc(&d, 8ull << log_n) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;  // no room: the pass forms its twist itself
+  }
+  const uint64_t len = 1ull << log_n;
+  pow_table_kernel<<<(unsigned)std::min<uint64_t>((len + 255) / 256, 148 * 16), 256, 0, s>>>(t.d_fwd_lo, t.d_fwd_hi,
+                                                                                          1, log_n, len, d);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaFree(d);
+    return nullptr;
+  }
+  cache[key] = d;
+  return d;
+}
+
 // columns from which a 2^11 / 2^12 first pass reads its twiddles from the
 // per-size table (shared through L2) instead of building per-CTA factors
 constexpr uint32_t kPassTabMinCols = 8;
@@ -655,6 +688,7 @@ cudaError_t ntt_coset_eval(const NttTables& t, const uint64_t* coef, uint64_t* o
   a.flat_lane = 0;
   a.in_valid = M;
   a.in_tw_log = log_m + log_b;
+  a.in_tw_tab = coset_twist_table(t, log_m + log_b, s);
   return launch_pass_dyn(log_m, a, false, n_cols, s);
 }
 

@@ -70,6 +70,8 @@ def test_ntt_linearity_at_2p23(ctx):
     (3, 3, 4, 1), (4, 7, 32, 1), (4, 12, 32, 1), (5, 10, 8, 7), (2, 16, 8, 7), (1, 1, 2, 1), (3, 13, 2, 3),
     # domains above 2^12 from at most 2^12 rows: one pass per coset
     (3, 8, 32, 1), (2, 9, 16, 5), (3, 11, 4, 3), (2, 6, 128, 1), (1, 12, 1024, 3), (2, 8, 8, 1),
+    # above 2^14 points the coset twist comes from a per-size table (up to 2^20)
+    (2, 10, 32, 1), (2, 11, 32, 7), (1, 10, 1024, 3),
 ])
 def test_lde_matches_oracle(ctx, w, log_n, blowup, shift):
     rng = np.random.default_rng(w * 100 + log_n)
