@@ -764,13 +764,18 @@ struct Emit {
   void limbs(uint32_t base, const uint32_t l[NL]) {
     for (int i = 0; i < NL; ++i) value(base + i, l[i]);
   }
+  // the nb bit cells of word w at col (codes of the phase's first row only)
+  void bits(uint32_t col, uint32_t w, uint32_t nb) {
+    if (codes)
+      for (uint32_t b = 0; b < nb; ++b) codes[col + b] = code(OP_BIT, w, b);
+  }
   // limbs and their 255 range bits
-  void elem(uint32_t c, uint32_t bits, const uint32_t l[NL]) {
+  void elem(uint32_t c, uint32_t bit_cells, const uint32_t l[NL]) {
     uint32_t off = 0;
     for (int i = 0; i < NL; ++i) {
       const uint32_t w = word(l[i]);
       set(c + i, code(OP_WORD, w));
-      for (uint32_t b = 0; b < LW[i]; ++b) set(bits + off + b, code(OP_BIT, w, b));
+      bits(bit_cells + off, w, LW[i]);
       off += LW[i];
     }
   }
@@ -837,14 +842,18 @@ F fill_mul(Emit& e, const GMul& g, const uint32_t a[NL], const uint32_t b[NL]) {
   uint32_t cl[NL];
   limbs_of(c, cl);
   e.elem(g.c, g.bits, cl);
-  __int128 t[NL] = {0};
+  // limbs below 2^27 (the unreduced 2d constant; the others below 2^26): a sum of ten
+  // products times at most 38 stays below 10 * 38 * 2^54 < 2^63
+  int64_t t64[NL] = {0};
   for (int i = 0; i < NL; ++i)
     for (int j = 0; j < NL; ++j) {
-      __int128 f = ((i & 1) && (j & 1)) ? 2 : 1;
+      int64_t f = ((i & 1) && (j & 1)) ? 2 : 1;
       int s = i + j;
       if (s >= NL) s -= NL, f *= 19;
-      t[s] += f * (__int128)a[i] * b[j];
+      t64[s] += f * ((int64_t)a[i] * (int64_t)b[j]);
     }
+  __int128 t[NL];
+  for (int k = 0; k < NL; ++k) t[k] = t64[k];
   // S = sum (T[k] - c[k]) 2^off_k in a 320-bit two's-complement accumulator; S = x p
   uint64_t acc[5] = {0};
   for (int k = 0; k < NL; ++k) {
@@ -875,7 +884,7 @@ F fill_mul(Emit& e, const GMul& g, const uint32_t a[NL], const uint32_t b[NL]) {
     const __int128 cy = d >> LW[k];
     require(cy * ((__int128)1 << LW[k]) == d && cy >= -half && cy < half, "ed25519 witness: mul carry");
     const uint32_t w = e.word((uint64_t)(cy + half));
-    for (uint32_t bb = 0; bb < MUL_CB; ++bb) e.set(g.carry + k * MUL_CB + bb, code(OP_BIT, w, bb));
+    e.bits(g.carry + k * MUL_CB, w, MUL_CB);
     prev = cy;
   }
   require(prev == x, "ed25519 witness: mul chain");
