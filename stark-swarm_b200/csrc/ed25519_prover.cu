@@ -99,7 +99,7 @@ std::shared_ptr<EdShape> make_shape(const ed25519::Witness& w, bool resident, cu
   S.row_phase = w.row_phase;
   S.blocks = w.prog.blocks;
   S.pair_refs = pair_refs(w.prog);
-  S.phi = ed25519_phi_plan(w.prog, w.L.height, 2048);
+  S.phi = ed25519_phi_plan(w.prog, w.L.height, 1024);
   S.lde = ed25519::make_lde_plan(w);
   for (const auto& g : S.lde.groups) {
     const uint32_t off = (uint32_t)S.nz_rows.size();
