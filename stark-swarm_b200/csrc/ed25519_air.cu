@@ -418,10 +418,16 @@ EdPhiPlan ed25519_phi_plan(const Program& prog, uint32_t n_trace, uint32_t chunk
       const uint32_t id = (uint32_t)classes.size();
       require(id < 255, "ed25519: too many row classes");
       it = classes.emplace(open, id).first;
-      // the class's blocks in program order, cut into chunks of about chunk_constraints
+      // the class's blocks grouped by kind (program order within a kind), cut into chunks
+      // of about chunk_constraints: most chunks then run one gadget evaluator, so a CTA's
+      // instruction footprint is one evaluator's code. Every block carries its own
+      // lambda and the sum is exact, so the order changes no value.
+      std::vector<uint32_t> order(open);
+      std::stable_sort(order.begin(), order.end(),
+                       [&](uint32_t x, uint32_t y) { return P.blocks[x].kind < P.blocks[y].kind; });
       const uint32_t start = (uint32_t)P.cls_list.size();
       uint32_t first = start, acc = 0;
-      for (uint32_t bi : open) {
+      for (uint32_t bi : order) {
         P.cls_list.push_back(bi);
         acc += count[bi];
         if (acc >= chunk_constraints) {
