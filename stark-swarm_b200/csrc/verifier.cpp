@@ -5,6 +5,9 @@
 // reports a proof (swarm-dns/src/prover.rs:189-192) and exported as
 // sg_stir_verify. Verification is a few hundred hashes and small
 // interpolations, so it runs on the host.
+#include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "protocol.hpp"
@@ -349,7 +352,9 @@ bool stir_verify(const StirProof& pr, const sg_fri_params& p) {
       a = gl::e_mul(a, alphas[0]);
     }
   }
-  for (uint64_t qi = 0; qi < pr.prox.size(); ++qi) {
+  // Each query reads only the proof: they are checked on up to 8 threads, a strided
+  // share each (about 20 us a query, mostly its two Merkle openings).
+  auto query_ok = [&](uint64_t qi) -> bool {
     const ProxQuery& q = pr.prox[qi];
     const uint64_t raw = query_index(query_seed, qi, n0);
     if (q.raw != raw || q.base != raw % nn) return false;
@@ -367,12 +372,23 @@ bool stir_verify(const StirProof& pr, const sg_fri_params& p) {
       if (!q.has_l1) return false;
       if (!verify_opening(l1_ar, 1, pr.roots[1], q.l1_open) || q.l1_open.index != q.base) return false;
       if (leaf_hash(l1_ar[0], 1, q.l1_open.index, q.f_next.c, 6) != q.l1_open.leaf) return false;
-      if (!gl::e_eq(fv, q.f_next)) return false;
-    } else {
-      if (!gl::e_eq(fv, eval_poly(pr.final_coeffs, gl::e_from(gl::pow(omega_final, q.base))))) return false;
+      return gl::e_eq(fv, q.f_next);
     }
-  }
-  return true;
+    return gl::e_eq(fv, eval_poly(pr.final_coeffs, gl::e_from(gl::pow(omega_final, q.base))));
+  };
+  const uint64_t nq = pr.prox.size();
+  const unsigned nt = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>({8, std::max(1u, std::thread::hardware_concurrency()), nq / 8}));
+  std::atomic<bool> ok{true};
+  auto share = [&](unsigned t) {
+    for (uint64_t qi = t; qi < nq && ok.load(std::memory_order_relaxed); qi += nt)
+      if (!query_ok(qi)) ok = false;
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t) th.emplace_back(share, t);
+  share(0);
+  for (auto& x : th) x.join();
+  return ok.load();
 }
 
 }  // namespace sg
