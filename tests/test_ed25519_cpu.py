@@ -87,7 +87,8 @@ def test_tampered_trace_fires():
         assert v.any(), (row, col)
 
 
-@pytest.mark.parametrize("tag,msg,k", [(b"a", b"m" * 32, 8), (b"b", bytes(range(100)), 16), (b"c", b"", 4)])
+@pytest.mark.parametrize("tag,msg,k", [(b"a", b"m" * 32, 8), (b"b", bytes(range(100)), 16), (b"c", b"", 4),
+                                       (b"e", bytes(range(250)), 8)])
 def test_library_program_matches_oracle(sg, tag, msg, k):
     pub, sig, msg = _signed(tag, msg)
     lay, pr, _s, _k = OE.layout_program(pub, sig, msg, k)
@@ -99,7 +100,8 @@ def test_library_program_matches_oracle(sg, tag, msg, k):
     assert (rows["residual_row"], rows["result_row"]) == (lay.residual_row, lay.result_row)
 
 
-@pytest.mark.parametrize("tag,msg,k", [(b"a", b"m" * 32, 8), (b"b", bytes(range(100)), 16), (b"d", b"", 256)])
+@pytest.mark.parametrize("tag,msg,k", [(b"a", b"m" * 32, 8), (b"b", bytes(range(100)), 16), (b"d", b"", 256),
+                                       (b"e", bytes(range(250)), 8)])
 def test_library_host_trace_matches_oracle(sg, tag, msg, k):
     pub, sig, msg = _signed(tag, msg)
     _lay, _pr, want = OE.build(pub, sig, msg, k)

@@ -43,7 +43,8 @@ def test_merge_of_random_lde_matches_oracle(sgpu, ctx):
     assert np.array_equal(got, OE.merge(lay, pr, lde, lay.height, blowup))
 
 
-@pytest.mark.parametrize("tag,msg,k", [(b"h1", b"h" * 32, 8), (b"h2", bytes(range(120)), 8)])
+@pytest.mark.parametrize("tag,msg,k", [(b"h1", b"h" * 32, 8), (b"h2", bytes(range(120)), 8),
+                                       (b"h3", bytes(range(250)), 8)])
 def test_merge_of_honest_lde_matches_oracle(sgpu, ctx, tag, msg, k):
     pub, sig, msg = _signed(tag, msg)
     lay, pr, tr = OE.build(pub, sig, msg, k)
