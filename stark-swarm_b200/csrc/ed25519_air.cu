@@ -479,17 +479,24 @@ cudaError_t ed25519_expand(const EdExpand& d, uint64_t* d_trace, cudaStream_t s)
   return cudaGetLastError();
 }
 
-cudaError_t ed25519_phi(const EdPhi& a, uint64_t* d_part, uint64_t* d_phi, cudaStream_t s) {
+cudaError_t ed25519_phi_blocks(const EdPhi& a, uint64_t* d_part, cudaStream_t s) {
   if (a.blowup == 0 || a.n % (a.coset_len ? a.coset_len : a.blowup) || a.max_chunks == 0 || a.max_chunks > 65535)
     return cudaErrorInvalidValue;
-  {
-    SG_LAUNCH_SCOPE("ed25519_phi", s);
-    ed25519_phi_kernel<<<dim3((unsigned)((a.n + kPhiThreads - 1) / kPhiThreads), a.max_chunks), kPhiThreads, 0,
-                         s>>>(a, d_part);
-  }
+  SG_LAUNCH_SCOPE("ed25519_phi", s);
+  ed25519_phi_kernel<<<dim3((unsigned)((a.n + kPhiThreads - 1) / kPhiThreads), a.max_chunks), kPhiThreads, 0, s>>>(
+      a, d_part);
+  return cudaGetLastError();
+}
+
+cudaError_t ed25519_phi_add(const EdPhi& a, const uint64_t* d_part, uint64_t* d_phi, cudaStream_t s) {
   SG_LAUNCH_SCOPE("ed25519_phi_sum", s);
   ed25519_phi_sum<<<(unsigned)((a.n + 255) / 256), 256, 0, s>>>(a, d_part, d_phi);
   return cudaGetLastError();
+}
+
+cudaError_t ed25519_phi(const EdPhi& a, uint64_t* d_part, uint64_t* d_phi, cudaStream_t s) {
+  const cudaError_t e = ed25519_phi_blocks(a, d_part, s);
+  return e != cudaSuccess ? e : ed25519_phi_add(a, d_part, d_phi, s);
 }
 
 }  // namespace sg

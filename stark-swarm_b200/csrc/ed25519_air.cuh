@@ -77,5 +77,9 @@ struct EdPhi {
 };
 // Phi = sum_j (j + 1) C_j at the n points; d_part holds max_chunks * n values.
 cudaError_t ed25519_phi(const EdPhi& a, uint64_t* d_part, uint64_t* d_phi, cudaStream_t s);
+// The same in its two launches: the block kernel's per-chunk partial sums into
+// d_part, then their sum (with the SHA-512 part, a.phi_sha, for the hash rows).
+cudaError_t ed25519_phi_blocks(const EdPhi& a, uint64_t* d_part, cudaStream_t s);
+cudaError_t ed25519_phi_add(const EdPhi& a, const uint64_t* d_part, uint64_t* d_phi, cudaStream_t s);
 
 }  // namespace sg

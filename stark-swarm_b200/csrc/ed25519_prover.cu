@@ -221,11 +221,31 @@ void merge_on_device(sg_ctx* c, const ed25519::Witness& w, const EdShape& S, con
   const uint64_t sha_rows = L.k_hash - 1;
   DBuf part((uint64_t)S.phi.max_chunks * n, s), phi(n, s), phi_sha(sha_rows * blowup, s);
   DBuf scratch(ntt_scratch_elems(1, ln), s);
-  cuda_check(sha512_phi_points_ex(d_lde, n, n, sha_rows * blowup, blowup, blowup, L.n_blocks, S.d_sha_lam, phi_sha.p,
-                                  1, 0, s),
-             "ed25519 sha512 phi");
-  cuda_check(ed25519_phi(phi_args(S, pairs, d_lde, n, blowup, n_trace, 0, 1, 0, phi_sha.p, sha_rows), part.p, phi.p, s),
-             "ed25519 phi");
+  // The SHA-512 block's Phi on the hash rows (a few dozen CTAs, latency-bound) runs on
+  // the context's second stream beside the block kernel; the sum waits for both.
+  if (!c->copy_stream) cuda_check(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "side stream");
+  cudaEvent_t fork = nullptr, join = nullptr;
+  cuda_check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+  cuda_check(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), "event");
+  try {
+    cuda_check(cudaEventRecord(fork, s), "event");
+    cuda_check(cudaStreamWaitEvent(c->copy_stream, fork, 0), "wait");
+    cuda_check(sha512_phi_points_ex(d_lde, n, n, sha_rows * blowup, blowup, blowup, L.n_blocks, S.d_sha_lam,
+                                    phi_sha.p, 1, 0, c->copy_stream),
+               "ed25519 sha512 phi");
+    cuda_check(cudaEventRecord(join, c->copy_stream), "event");
+    const EdPhi a = phi_args(S, pairs, d_lde, n, blowup, n_trace, 0, 1, 0, phi_sha.p, sha_rows);
+    cuda_check(ed25519_phi_blocks(a, part.p, s), "ed25519 phi");
+    cuda_check(cudaStreamWaitEvent(s, join, 0), "wait");
+    cuda_check(ed25519_phi_add(a, part.p, phi.p, s), "ed25519 phi sum");
+  } catch (...) {
+    cudaStreamWaitEvent(s, join, 0);
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
+    throw;
+  }
+  cudaEventDestroy(fork);
+  cudaEventDestroy(join);
   cuda_check(ntt_batch(c->tw, phi.p, phi.p, 1, n, n, (int)ln, true, n, scratch.p, s), "intt");
   cuda_check(quotient_zh(phi.p, n, n_trace, d_c, s), "quotient");
   cuda_check(ntt_batch(c->tw, d_c, d_c, 1, n, n, (int)ln, false, n - n_trace, scratch.p, s), "ntt");
