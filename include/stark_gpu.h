@@ -460,7 +460,8 @@ int sg_merge_ed25519(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], 
 int sg_prove_ed25519(sg_ctx* ctx, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
                      const uint8_t fs_binding[32], uint32_t k_scalar, size_t blowup, uint8_t* proof, size_t cap,
                      size_t* len);
-/* RFC 8032 §5.1.7 cofactored verification (ed25519_verify.rs:54-117): 1 valid, 0 not. */
+/* RFC 8032 §5.1.7 cofactored verification (ed25519_verify.rs:54-117): 1 valid, 0 not,
+ * a negative error code (SG_EINVAL, SG_ENOMEM) on a bad argument or failed allocation. */
 int sg_ed25519_verify(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len);
 /* zsk_ksk_pi_hash_v2_stark (swarm-dns/src/prover.rs:763-780): SHA3-256 of
  * "ZSK-KSK-PIHASH-V2-ST" || pub || sig || le64(msg_len) || msg || fs_binding ||

@@ -824,15 +824,16 @@ int sg_prove_ed25519(sg_ctx* c, const uint8_t pub[32], const uint8_t sig[64], co
 
 int sg_ed25519_verify(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len) {
   if (!ed_args(pub, sig, msg, msg_len)) return SG_EINVAL;
-  return sg::ed25519::verify(pub, sig, msg, msg_len) ? 1 : 0;
+  bool ok = false;
+  const int rc = host_guarded([&] { ok = sg::ed25519::verify(pub, sig, msg, msg_len); });
+  return rc != SG_OK ? rc : ok ? 1 : 0;
 }
 
 int sg_ed25519_pi_hash(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg, size_t msg_len,
                        const uint8_t fs_binding[32], const uint8_t merkle_root[32], const uint8_t root_f0[32],
                        uint8_t out[32]) {
   if (!ed_args(pub, sig, msg, msg_len) || !fs_binding || !merkle_root || !root_f0 || !out) return SG_EINVAL;
-  sg::ed25519::pi_hash(pub, sig, msg, msg_len, fs_binding, merkle_root, root_f0, out);
-  return SG_OK;
+  return host_guarded([&] { sg::ed25519::pi_hash(pub, sig, msg, msg_len, fs_binding, merkle_root, root_f0, out); });
 }
 
 int sg_prove_zsk_ksk_binding_v2(sg_ctx* c, const uint8_t pub[32], const uint8_t sig[64], const uint8_t* msg,
