@@ -520,8 +520,7 @@ int sg_prove_sha512(sg_ctx* c, const uint8_t* msg, size_t len, const uint8_t fs_
 // ------------------------------------------------------------------ RSA-2048
 int sg_rsa2048_em(const uint8_t* msg, size_t len, uint8_t em[256]) {
   if ((!msg && len) || !em) return SG_EINVAL;
-  sg::rsa::em_encode(msg, len, em);
-  return SG_OK;
+  return host_guarded([&] { sg::rsa::em_encode(msg, len, em); });
 }
 
 int sg_rsa2048_verify(const uint8_t n_be[256], const uint8_t s_be[256], const uint8_t em[256]) {
@@ -536,14 +535,12 @@ int sg_rsa2048_verify(const uint8_t n_be[256], const uint8_t s_be[256], const ui
 int sg_rsa2048_pi_record(const uint8_t n_be[256], const uint8_t s_be[256], const uint8_t* msg, size_t len,
                          const uint8_t em[256], uint8_t out[32]) {
   if (!n_be || !s_be || (!msg && len) || !em || !out) return SG_EINVAL;
-  sg::rsa::pi_record(n_be, s_be, msg, len, em, out);
-  return SG_OK;
+  return host_guarded([&] { sg::rsa::pi_record(n_be, s_be, msg, len, em, out); });
 }
 
 int sg_rsa2048_pi_stacked(const uint8_t n_be[256], size_t n_records, const uint8_t* ems, uint8_t out[32]) {
   if (!n_be || (!ems && n_records) || !out) return SG_EINVAL;
-  sg::rsa::pi_stacked(n_be, n_records, ems, out);
-  return SG_OK;
+  return host_guarded([&] { sg::rsa::pi_stacked(n_be, n_records, ems, out); });
 }
 
 int sg_rsa2048_trace(const uint8_t* n_be, const uint8_t* s_be, const uint8_t* em_be, size_t n_records,
@@ -652,8 +649,7 @@ int sg_p256_u_bits(const uint8_t digest[32], const uint8_t r[32], const uint8_t 
 int sg_p256_ecdsa_pi(const uint8_t qx[32], const uint8_t qy[32], const uint8_t r[32], const uint8_t s[32],
                      const uint8_t digest[32], uint8_t out[32]) {
   if (!qx || !qy || !r || !s || !digest || !out) return SG_EINVAL;
-  sg::p256::pi_hash(qx, qy, r, s, digest, out);
-  return SG_OK;
+  return host_guarded([&] { sg::p256::pi_hash(qx, qy, r, s, digest, out); });
 }
 
 int sg_p256_chain_trace(const uint8_t ax[32], const uint8_t ay[32], const uint8_t* a_bits, const uint8_t bx[32],
@@ -859,8 +855,7 @@ int sg_dns_record_leaves(const uint8_t* canon, const size_t* offsets, size_t n, 
   if (!offsets || !salt || (n && (!canon || !out))) return SG_EINVAL;
   for (size_t i = 0; i < n; ++i)
     if (offsets[i + 1] < offsets[i]) return SG_EINVAL;
-  sg::dns_record_leaves(canon, offsets, n, salt, out);
-  return SG_OK;
+  return host_guarded([&] { sg::dns_record_leaves(canon, offsets, n, salt, out); });
 }
 
 int sg_dns_merkle_root(const uint8_t* leaves, size_t n, uint8_t root[32]) {
