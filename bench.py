@@ -18,6 +18,7 @@ back. `--impl reference` times the CPU restatement of the reference prover
 (the reference is Rust and cannot be built here) on a bounded sample.
 """
 import argparse
+import gc
 import hashlib
 import importlib
 import json
@@ -881,7 +882,10 @@ def main():
     assert sg.deep_fri_verify(params, ref[1]), "proof rejected by the verifier"
     torch.cuda.synchronize()
 
-    # timed region (device-resident inputs)
+    # timed region (device-resident inputs); the STIR transcript's host round trips
+    # sit inside each step, so no garbage-collector pause may land there
+    gc.collect()
+    gc.disable()
     barrier(ws)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -966,6 +970,7 @@ def main():
     sg.profile_enable(False)
     prof_commit = sg.profile_read()
     commit_ms = dist_max(e0.elapsed_time(e1), ws) / args.steps
+    gc.enable()
 
     # roofline of the dominant kernel family (CUDA events recorded on the launching stream)
     peaks = {}
