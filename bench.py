@@ -107,6 +107,11 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's start-up (its NVML initialisation) must not overlap the
+            # timed steps: wait for its first sample, then keep sampling through them
+            t0 = time.time()
+            while not self.lines and self.proc.poll() is None and time.time() - t0 < 3.0:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
 

@@ -132,3 +132,21 @@ def test_batch_and_server_jobs(sgpu, ctx):
             srv.wait(t_bad)
         assert ei.value.code == sgpu.SG_EVERIFY
         assert srv.wait(t_ok)[0] == want[1]
+
+
+def test_grouped_batch_equals_proofs_alone(sgpu, ctx):
+    # Ed25519 jobs (k_scalar 256, blowup 4: n0 = 4096) beside SHA-256 jobs of the same
+    # n0 (480-byte messages: 8 blocks, 1024 rows) proved with lockstep STIR groups:
+    # every proof equals the same job proved alone
+    signed = [_signed(b"grp%d" % i, b"grouped zone record %d" % i) for i in range(4)]
+    fs = [hashlib.sha3_256(b"gfs%d" % i).digest() for i in range(4)]
+    jobs = [(sgpu.JOB_ED25519, psm, f, sgpu.PHI_PARALLEL_GATE, 4) for psm, f in zip(signed, fs)]
+    jobs += [(sgpu.JOB_SHA256, bytes([7 + i]) * 480, fs[i], sgpu.PHI_PARALLEL_GATE, 4) for i in range(2)]
+    alone = [p for p, _ in ctx.prove_batch(jobs, n_streams=1)]
+    try:
+        ctx.set_option(sgpu.OPT_STIR_GROUP, 8)
+        got = ctx.prove_batch(jobs, n_streams=2, hbm_budget_bytes=48 << 30)
+    finally:
+        ctx.set_option(sgpu.OPT_STIR_GROUP, 1)
+    assert all(r.status == sgpu.SG_OK for _, r in got)
+    assert [p for p, _ in got] == alone
