@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <map>
 #include <cstring>
+#include <atomic>
 #include <exception>
 #include <thread>
 
@@ -998,41 +999,20 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
   ladder_bits(k_can, k, k_bits.data());
   W.prog = make_program(L, s_bits.data(), k_bits.data(), r_y, r_sign, a_y, a_sign, A);
 
-  // natively computed points (fill_verify_air_v11..v16): the accumulator entering each
-  // of the 2k ladder rows (padd and pdbl follow the gadgets' formulas, so the points
-  // are the ones the rows compute), sB = [s]B and kA = [k]A
+  // globals: the r thread (k bits) and the sB, kA and R threads (4 x 10 limbs each).
+  // Their codes go into every phase's codes first (the ladder threads then record
+  // their phases' other cells), their values once the ladders are done.
   const uint32_t n_lad = 2 * k;
-  std::vector<Pt> acc_in(n_lad);
-  Pt sB = identity(), kA = identity();
-  for (uint32_t j = 0; j < k; ++j) {
-    acc_in[j] = sB;
-    acc_in[k + j] = kA;
-    sB = pdbl(sB);
-    if (s_bits[j]) sB = padd(sB, basepoint());
-    kA = pdbl(kA);
-    if (k_bits[j]) kA = padd(kA, A);
-  }
-  const Pt Rt{R.X, R.Y, fe(1), mul(R.X, R.Y)};
-  const Pt res1 = padd(sB, pneg(Rt)), res2 = padd(res1, pneg(kA));
-
-  // globals: the r thread (k bits) and the sB, kA and R threads (4 x 10 limbs each)
-  W.globals.clear();
   W.codes.assign((size_t)N_PHASES * L.width, 0);
-  std::vector<uint32_t> gcodes(L.width, 0);
-  for (uint32_t i = 0; i < k; ++i) {
-    gcodes[L.r_thread + i] = code(OP_GLOBAL, (uint32_t)W.globals.size());
-    W.globals.push_back(k_bits[i]);
+  {
+    std::vector<uint32_t> gcodes(L.width, 0);
+    uint32_t gi = 0;
+    for (uint32_t i = 0; i < k; ++i) gcodes[L.r_thread + i] = code(OP_GLOBAL, gi++);
+    for (const uint32_t* thr : {L.thr_sB, L.thr_kA, L.thr_R})
+      for (int q = 0; q < 4; ++q)
+        for (int i = 0; i < NL; ++i) gcodes[thr[q] + i] = code(OP_GLOBAL, gi++);
+    for (uint32_t ph = 0; ph < N_PHASES; ++ph) memcpy(&W.codes[(size_t)ph * L.width], gcodes.data(), 4 * L.width);
   }
-  for (int t = 0; t < 3; ++t) {
-    const PtL p = limbs_pt(t == 0 ? sB : t == 1 ? kA : Rt);
-    const uint32_t* thr = t == 0 ? L.thr_sB : t == 1 ? L.thr_kA : L.thr_R;
-    for (int q = 0; q < 4; ++q)
-      for (int i = 0; i < NL; ++i) {
-        gcodes[thr[q] + i] = code(OP_GLOBAL, (uint32_t)W.globals.size());
-        W.globals.push_back(p.l[q][i]);
-      }
-  }
-  for (uint32_t ph = 0; ph < N_PHASES; ++ph) memcpy(&W.codes[(size_t)ph * L.width], gcodes.data(), 4 * L.width);
 
   W.row_phase.assign(L.height, PH_IDLE);
   W.row_off.assign(L.height + 1, 0);
@@ -1044,8 +1024,14 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
   limbs_of(fe(1), one);
   // The 2k ladder rows (fill_scalar_mult_trace, ed25519_scalar_mult_air.rs:133-171,
   // and the v6 shift chain) in parallel chunks, each emitting its rows' words into
-  // its own buffer from the accumulators computed above.
+  // its own buffer. A row needs the accumulator entering it; this thread computes
+  // them natively (padd and pdbl follow the gadgets' formulas, so the points are the
+  // ones the rows compute) and publishes them step by step in acc_ready, so the
+  // chunks start at once instead of after the whole pass (about 1 us a step against
+  // some 20 us for a row's gadgets).
   require(L.kA_first == L.sB_first + k && L.kA_last == L.kA_first + k - 1, "ed25519: ladder rows");
+  std::vector<Pt> acc_in(n_lad);
+  std::atomic<uint32_t> acc_ready{0};  // steps j done: acc_in[j] and acc_in[k + j] are set
   const uint32_t n_thr = std::max(1u, std::min({16u, std::thread::hardware_concurrency(), n_lad / 16}));
   const uint32_t per_chunk = (n_lad + n_thr - 1) / n_thr;
   std::vector<LadderChunk> chunks((n_lad + per_chunk - 1) / per_chunk);
@@ -1057,6 +1043,7 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
       for (uint32_t g = g0; g < g1; ++g) {
         const bool sb = g < k;
         const uint32_t j = sb ? g : g - k;
+        while (acc_ready.load(std::memory_order_acquire) <= j) std::this_thread::yield();
         const uint32_t ph = sb ? PH_SB : PH_KA;
         ch.start.push_back((uint32_t)ch.words.size());
         Emit e{ch.words, j == 0 ? &W.codes[(size_t)ph * L.width] : nullptr};
@@ -1078,13 +1065,38 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
       ch.err = std::current_exception();
     }
   };
+  Pt sB = identity(), kA = identity();
   {
     std::vector<std::thread> th;
-    for (uint32_t ci = 1; ci < chunks.size(); ++ci) th.emplace_back(run_chunk, ci);
-    run_chunk(0);
+    try {
+      for (uint32_t ci = 0; ci < chunks.size(); ++ci) th.emplace_back(run_chunk, ci);
+      for (uint32_t j = 0; j < k; ++j) {
+        acc_in[j] = sB;
+        acc_in[k + j] = kA;
+        acc_ready.store(j + 1, std::memory_order_release);
+        sB = pdbl(sB);
+        if (s_bits[j]) sB = padd(sB, basepoint());
+        kA = pdbl(kA);
+        if (k_bits[j]) kA = padd(kA, A);
+      }
+    } catch (...) {
+      acc_ready.store(k, std::memory_order_release);  // no thread may wait for ever
+      for (auto& t : th) t.join();
+      throw;
+    }
     for (auto& t : th) t.join();
     for (const LadderChunk& ch : chunks)
       if (ch.err) std::rethrow_exception(ch.err);
+  }
+  const Pt Rt{R.X, R.Y, fe(1), mul(R.X, R.Y)};
+  const Pt res1 = padd(sB, pneg(Rt)), res2 = padd(res1, pneg(kA));
+  W.globals.clear();
+  for (uint32_t i = 0; i < k; ++i) W.globals.push_back(k_bits[i]);
+  const Pt* const thread_pts[3] = {&sB, &kA, &Rt};
+  for (const Pt* pt : thread_pts) {
+    const PtL p = limbs_pt(*pt);
+    for (int q = 0; q < 4; ++q)
+      for (int i = 0; i < NL; ++i) W.globals.push_back(p.l[q][i]);
   }
   recorded[PH_SB] = recorded[PH_KA] = true;
   {
