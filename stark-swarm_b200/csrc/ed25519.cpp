@@ -1032,7 +1032,16 @@ void build_witness(const uint8_t pub[32], const uint8_t sig[64], const uint8_t* 
   require(L.kA_first == L.sB_first + k && L.kA_last == L.kA_first + k - 1, "ed25519: ladder rows");
   std::vector<Pt> acc_in(n_lad);
   std::atomic<uint32_t> acc_ready{0};  // steps j done: acc_in[j] and acc_in[k + j] are set
-  const uint32_t n_thr = std::max(1u, std::min({16u, std::thread::hardware_concurrency(), n_lad / 16}));
+  // the host's threads shared among the witnesses being built at once (server workers
+  // build theirs concurrently)
+  static std::atomic<uint32_t> g_building{0};
+  struct Building {
+    uint32_t n;
+    Building() : n(g_building.fetch_add(1) + 1) {}
+    ~Building() { g_building.fetch_sub(1); }
+  } building;
+  const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t n_thr = std::max(1u, std::min({16u, hw / building.n, n_lad / 16}));
   const uint32_t per_chunk = (n_lad + n_thr - 1) / n_thr;
   std::vector<LadderChunk> chunks((n_lad + per_chunk - 1) / per_chunk);
   auto run_chunk = [&](uint32_t ci) {

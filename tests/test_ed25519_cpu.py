@@ -108,6 +108,28 @@ def test_library_host_trace_matches_oracle(sg, tag, msg, k):
     assert np.array_equal(sg.ed25519_trace(pub, sig, msg, k), want)
 
 
+def test_concurrent_host_traces_match_oracle(sg):
+    # witnesses built at once from several host threads (as server workers do) share
+    # the host's threads and wait row by row for their accumulators: each trace still
+    # equals the oracle's
+    import threading
+    cases = [_signed(b"conc%d" % i, bytes(range(i, i + 40))) for i in range(6)]
+    want = [OE.build(p, s, m, 16)[2] for p, s, m in cases]
+    got = [None] * len(cases)
+
+    def work(i):
+        p, s, m = cases[i]
+        got[i] = sg.ed25519_trace(p, s, m, 16)
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(len(cases))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for i in range(len(cases)):
+        assert np.array_equal(got[i], want[i]), i
+
+
 @pytest.mark.parametrize("i", range(len(VEC)))
 def test_library_verify(sg, i):
     pub, sig, msg = _vec(VEC[i])
