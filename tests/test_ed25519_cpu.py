@@ -138,6 +138,10 @@ def test_library_verify(sg, i):
     bad = bytearray(pub)
     bad[3] ^= 1
     assert not sg.ed25519_verify(bytes(bad), sig, msg)
+    bad_s = bytearray(sig)  # a flipped bit of S (the reference's tamper test)
+    bad_s[40] ^= 1
+    assert not sg.ed25519_verify(pub, bytes(bad_s), msg)
+    assert not OE.verify(pub, bytes(bad_s), msg)
     # S >= L is refused (ed25519_verify.rs:80)
     s = int.from_bytes(sig[32:], "little") + OE.L_ORDER
     if s < 1 << 256:
